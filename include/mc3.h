@@ -1,0 +1,181 @@
+/*
+ * libmc3 -- B200-native motion correction of cryo-EM movie stacks.
+ *
+ * C ABI of the MotionCor3 hot path: gain application, hot-pixel / defect
+ * correction, iterative full-frame alignment, patch alignment, local-motion
+ * correction, dose weighting and summation.  Plain pointers and sizes
+ * only; device pointers are CUDA device addresses on the context's GPU and
+ * `stream` arguments are cudaStream_t values passed as void*.
+ *
+ * Every entry point returns an mc3 status code (MC3_OK on success) and
+ * never aborts the process or resets the device.  A context is
+ * thread-compatible: one host thread at a time per context.
+ *
+ * Each declaration names the reference (MotionCor3 1.2.1) interface it
+ * replaces, as path:line within the reference project.
+ */
+#ifndef MC3_H
+#define MC3_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MC3_OK 0
+#define MC3_EINVAL 1      /* bad argument or unsupported size */
+#define MC3_ENOMEM 2      /* device or host allocation failed */
+#define MC3_ECUDA 3       /* CUDA runtime error (sticky errors included) */
+#define MC3_ETIMEOUT 4    /* a bounded device wait gave up */
+#define MC3_EIO 5         /* file could not be read or written */
+#define MC3_EUNSUPPORTED 6 /* option or size outside the implemented path */
+
+typedef struct mc3_ctx mc3_ctx;
+
+/* Options of the in-scope command-line tags; defaults as CInput::CInput
+ * (CInput.cpp:82-127). */
+typedef struct {
+  int patch[3];        /* -Patch nx ny overlap; patch alignment needs nx,ny > 1 */
+  int iter;            /* -Iter (15)                                           */
+  float tol;           /* -Tol (0.1 px)                                        */
+  float bft[2];        /* -Bft global, patch (500, 100)                        */
+  int phase_only;      /* -PhaseOnly (0)                                       */
+  float ft_bin;        /* -FtBin (1; only 1 is implemented)                    */
+  float init_dose;     /* -InitDose (accepted, unused by the reference path)  */
+  float fm_dose;       /* -FmDose e/A^2 per frame (0 = no dose weighting)      */
+  float pix_size;      /* -PixSize A (0)                                       */
+  int kv;              /* -kV (300)                                            */
+  int group[2];        /* -Group global, patch (1, 4)                          */
+  int fm_ref;          /* -FmRef, 1-based; <0 = central frame (-1)             */
+  float sum_range[2];  /* -SumRange e/A^2 (3, 25)                              */
+  int align;           /* -Align (1; 0 = simple sum is not implemented)        */
+  int correct_bad;     /* hot-pixel / defect detection + fill (1, as the
+                          reference's CProcessThread.cpp:94-99 always runs)    */
+  int gpu;             /* CUDA device ordinal (-Gpu first entry)               */
+} mc3_params;
+
+/* Sizes a movie will use (CBufferPool::CreateBuffers, CBufferPool.cpp:95-270). */
+typedef struct {
+  int n_sums;          /* 1 + DW + DWS                                        */
+  int n_patches;       /* px*py in patch mode, else 0                         */
+  int xcf_size[2];     /* alignment (Fourier-binned) image size               */
+  int patch_size[2];   /* patch image size (0 in global mode)                 */
+  float xcf_bin[2];    /* binning factors of the alignment image             */
+  size_t device_bytes; /* device memory the context holds for this movie     */
+} mc3_plan_info;
+
+typedef struct {
+  const void* frames;  /* [nz][ny][nx] pixels, MRC mode `mode`               */
+  int mode;            /* 0 uint8, 1 int16, 2 float32, 6 uint16               */
+  int nx, ny, nz;
+  int on_device;       /* 1: frames is a device pointer                       */
+} mc3_movie;
+
+/* Caller-allocated outputs; any pointer may be NULL to skip it. */
+typedef struct {
+  float* sums;             /* [n_sums][ny][nx]: plain, DW, DWS               */
+  int sums_on_device;      /* 1: `sums` is a device pointer                   */
+  float* global_shifts;    /* [nz][2]: full-frame shifts as logged            */
+  float* patch_shifts;     /* [nz][n_patches][2]                              */
+  float* patch_centers;    /* [n_patches][2]                                  */
+  unsigned char* patch_bad;/* [nz][n_patches]                                 */
+  int* iterations;         /* [1 + n_patches]: global, then per patch         */
+  float* errors;           /* [iter * (1 + n_patches)] max group shift per iteration */
+  int n_sums;              /* out                                             */
+  int n_patches;           /* out                                             */
+  double time_ms;          /* out: device time of the call                    */
+} mc3_result;
+
+/* ---- library ---- */
+const char* mc3_version(void);
+const char* mc3_strerror(int code);
+/* CInput::CInput defaults (CInput.cpp:82-127). */
+void mc3_params_default(mc3_params* p);
+
+/* ---- context ---- */
+/* Replaces the CInput/CBufferPool/CAlignParam singletons set up in
+ * CMain::DoIt (CMain.cpp:37-91) and CMain::mCreateBufferPool (:400-427). */
+int mc3_create(const mc3_params* p, mc3_ctx** out);
+int mc3_destroy(mc3_ctx* ctx);
+/* Work stream (cudaStream_t); NULL = the context's own stream. */
+int mc3_set_stream(mc3_ctx* ctx, void* stream);
+/* Buffer geometry for a movie size (CBufferPool.cpp:185-270). */
+int mc3_plan(mc3_ctx* ctx, int nx, int ny, int nz, mc3_plan_info* info);
+/* Gain reference [ny][nx] float (CLoadRefs::LoadGain, CLoadRefs.cpp:82-95);
+ * NULL clears it. */
+int mc3_set_gain(mc3_ctx* ctx, const float* gain, int nx, int ny, int on_device);
+
+/* ---- whole path ---- */
+/* One movie from raw frames to sums and shift tables: replaces
+ * CProcessThread::mProcess from mApplyRefs through mAlignStack
+ * (CProcessThread.cpp:82-107, 136-182), i.e. CApplyRefs::DoIt,
+ * BadPixel::CDetectMain::DoIt, BadPixel::CCorrectMain::DoIt and
+ * Align::CAlignMain::DoIt (Align/CAlignMain.cpp:39-75). */
+int mc3_process_movie(mc3_ctx* ctx, const mc3_movie* movie, mc3_result* out);
+
+/* ---- components (device pointers unless stated) ---- */
+/* Util::CCufft2D::Forward (Util/CCufft2D.cpp:65-87): in-place R2C of nz
+ * padded real frames [nz][ny][2*(nx/2+1)], optionally x 1/(nx*ny). */
+int mc3_fft_forward(float* frames, int nx, int ny, int nz, int normalise, void* stream);
+/* Util::CCufft2D::Inverse (Util/CCufft2D.cpp:105-120): in-place,
+ * unnormalised C2R of nz half spectra [nz][ny][nx/2+1] complex. */
+int mc3_fft_inverse(float* frames, int nx, int ny, int nz, void* stream);
+/* Util::GPhaseShift2D::DoIt (Util/GPhaseShift2D.cu:48-66): out (+)= in *
+ * e^{i 2pi (kx sx/Nx + ky sy/Ny)} on a [cmp_y][cmp_x] half spectrum. */
+int mc3_phase_shift(const float* in, float* out, int cmp_x, int cmp_y, float sx, float sy,
+                    int accumulate, void* stream);
+/* Util::GFourierResize2D::DoIt (Util/GFourierResize2D.cu:110-126), copy mode. */
+int mc3_fourier_crop(const float* in, int in_cmp_x, int in_cmp_y, float* out, int out_cmp_x,
+                     int out_cmp_y, void* stream);
+/* Align::GCorrelateSum2D::DoIt + Align::CPeak2D::DoIt
+ * (Align/GCorrelateSum2D.cu:108-140, Align/CPeak2D.cpp:39-109): correlation
+ * window [sea_y][sea_x] of a group spectrum against (sum - group) and its
+ * sub-pixel peak (host float[2]). */
+int mc3_correlate(const float* group, const float* sum, int cmp_x, int cmp_y, float bfactor,
+                  int phase_only, int sea_x, int sea_y, float* window, float* shift_host,
+                  void* stream);
+/* Align::CIterativeAlign::DoIt (Align/CIterativeAlign.cpp:55-156) on a
+ * device stack of n half spectra [n][cmp_y][cmp_x]; shifts_host [n][2];
+ * returns iterations through *iters. */
+int mc3_iterative_align(mc3_ctx* ctx, const float* stack, int cmp_x, int cmp_y, int n,
+                        int group, int max_iter, float tol, float bfactor, int phase_only,
+                        float* shifts_host, int* iters);
+/* BadPixel::CDetectMain::DoIt detection part (BadPixel/CDetectMain.cpp:54-123)
+ * on a padded frame sum [ny][2*(nx/2+1)] -> bad map [ny][nx] (device). */
+int mc3_detect_bad_pixels(const float* sum, int nx, int ny, unsigned char* bad, void* stream);
+/* BadPixel::GCorrectBad::GDoIt (BadPixel/GCorrectBad.cu:167-185) on nz
+ * padded frames. */
+int mc3_correct_bad_pixels(float* frames, int nx, int ny, int nz, const unsigned char* bad,
+                           void* stream);
+/* Correct::mGCorrect3D (Correct/GCorrectPatchShift.cu:17-66) on one padded
+ * real frame; centers [P][2], shifts [P][2], bad [P] (device, bad may be NULL). */
+int mc3_local_gather(const float* in, float* out, int nx, int ny, const float* centers,
+                     const float* shifts, const unsigned char* bad, int n_patches, void* stream);
+/* Correct::GWeightFrame (Correct/GWeightFrame.cu:90-147) + the sums of
+ * CCorrectFullShift::mGenSums (Correct/CCorrectFullShift.cpp:271-300):
+ * sums of nz half spectra after the phase shift by -shifts (host [nz][2],
+ * |s| < 0.1 px skipped) with dose weighting when fm_dose > 0. */
+int mc3_dose_weighted_sums(mc3_ctx* ctx, const float* spectra, int nx, int ny, int nz,
+                           const float* shifts_host, float* sums, int* n_sums);
+
+/* ---- host-side bookkeeping (host pointers) ---- */
+/* Align::CPeak2D::DoIt (Align/CPeak2D.cpp:39-109). */
+void mc3_peak2d(const float* window, int sea_x, int sea_y, float* shift);
+/* Util::CRemoveSpikes1D::DoIt(x, y, false) (Util/CRemoveSpikes1D.cpp:59-105). */
+void mc3_remove_spikes(float* sx, float* sy, int n);
+/* Util_LinEqs::DoIt (LibSrc/Util/Util_LinEqs.cpp:19-41); returns 1 on success. */
+int mc3_lin_eqs(float* coeff, float* vals, int dim);
+/* Align::CStackShift::Smooth (Align/CStackShift.cpp:180-198). */
+void mc3_smooth_shifts(float* sx, float* sy, int n, float weight);
+/* Align::CPatchShifts::MakeRelative (Align/CPatchShifts.cpp:263-286),
+ * shifts [nz][P][2] in place. */
+void mc3_patch_make_relative(float* shifts, int nz, int n_patches);
+/* Align::CPatchShifts::DetectBads (Align/CPatchShifts.cpp:288-355). */
+void mc3_patch_detect_bads(const float* shifts, const float* centers, int nz, int n_patches,
+                           int nx, int ny, unsigned char* bad);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MC3_H */

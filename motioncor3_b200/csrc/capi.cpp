@@ -1,0 +1,378 @@
+// extern "C" entry points declared in include/mc3.h.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "engine.h"
+
+struct mc3_ctx {
+  mc3::Engine* eng;
+};
+
+using namespace mc3;
+
+namespace {
+cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+}  // namespace
+
+extern "C" {
+
+const char* mc3_version(void) { return "mc3-b200 0.1.0 (MotionCor3 1.2.1 hot path, sm_100a)"; }
+
+const char* mc3_strerror(int code) {
+  switch (code) {
+    case MC3_OK: return "ok";
+    case MC3_EINVAL: return "invalid argument or size";
+    case MC3_ENOMEM: return "out of memory";
+    case MC3_ECUDA: return "CUDA runtime error";
+    case MC3_ETIMEOUT: return "device wait timed out";
+    case MC3_EIO: return "file I/O error";
+    case MC3_EUNSUPPORTED: return "unsupported option or size";
+    default: return "unknown error";
+  }
+}
+
+void mc3_params_default(mc3_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  // CInput::CInput (CInput.cpp:82-127)
+  p->patch[0] = p->patch[1] = p->patch[2] = 0;
+  p->iter = 15;
+  p->tol = 0.1f;
+  p->bft[0] = 500.0f;
+  p->bft[1] = 100.0f;
+  p->phase_only = 0;
+  p->ft_bin = 1.0f;
+  p->init_dose = 0.0f;
+  p->fm_dose = 0.0f;
+  p->pix_size = 0.0f;
+  p->kv = 300;
+  p->group[0] = 1;
+  p->group[1] = 4;
+  p->fm_ref = -1;
+  p->sum_range[0] = 3.0f;
+  p->sum_range[1] = 25.0f;
+  p->align = 1;
+  p->correct_bad = 1;
+  p->gpu = 0;
+}
+
+int mc3_create(const mc3_params* p, mc3_ctx** out) {
+  if (!p || !out) return MC3_EINVAL;
+  *out = nullptr;
+  if (p->iter < 1 || p->group[0] < 1 || p->group[1] < 1) return MC3_EINVAL;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return MC3_ECUDA;
+  }
+  if (p->gpu < 0 || p->gpu >= ndev) return MC3_EINVAL;
+  mc3_ctx* c = new (std::nothrow) mc3_ctx;
+  if (!c) return MC3_ENOMEM;
+  c->eng = new (std::nothrow) Engine(*p);
+  if (!c->eng) {
+    delete c;
+    return MC3_ENOMEM;
+  }
+  int s = c->eng->init();
+  if (s != kOk) {
+    delete c->eng;
+    delete c;
+    return s;
+  }
+  *out = c;
+  return MC3_OK;
+}
+
+int mc3_destroy(mc3_ctx* ctx) {
+  if (!ctx) return MC3_EINVAL;
+  delete ctx->eng;
+  delete ctx;
+  return MC3_OK;
+}
+
+int mc3_set_stream(mc3_ctx* ctx, void* stream) {
+  if (!ctx) return MC3_EINVAL;
+  return ctx->eng->set_stream(as_stream(stream));
+}
+
+int mc3_plan(mc3_ctx* ctx, int nx, int ny, int nz, mc3_plan_info* info) {
+  if (!ctx || !info) return MC3_EINVAL;
+  return ctx->eng->plan(nx, ny, nz, info);
+}
+
+int mc3_set_gain(mc3_ctx* ctx, const float* gain, int nx, int ny, int on_device) {
+  if (!ctx) return MC3_EINVAL;
+  return ctx->eng->set_gain(gain, nx, ny, on_device != 0);
+}
+
+int mc3_process_movie(mc3_ctx* ctx, const mc3_movie* movie, mc3_result* out) {
+  if (!ctx || !movie) return MC3_EINVAL;
+  return ctx->eng->process(*movie, out);
+}
+
+// ---- components ----
+int mc3_fft_forward(float* frames, int nx, int ny, int nz, int normalise, void* stream) {
+  if (!frames || nx < 2 || (nx & 1) || ny < 1 || nz < 1) return MC3_EINVAL;
+  const int cmpX = nx / 2 + 1;
+  const long ncmp = (long)cmpX * ny;
+  cudaStream_t st = as_stream(stream);
+  Batch b{nz, nz, ncmp * 2, nullptr, ncmp};
+  int s = row_r2c(frames, 2 * cmpX, reinterpret_cast<float2*>(frames), cmpX, nx, ny, b, 1.0f, st);
+  if (s) return s;
+  Batch bc{nz, nz, ncmp, nullptr, ncmp};
+  ColOps ops{};
+  ops.dir = -1;
+  ops.scale = normalise ? (float)(1.0 / nx / ny) : 1.0f;
+  float2* c = reinterpret_cast<float2*>(frames);
+  return col_fft(c, c, cmpX, cmpX, ny, bc, ops, st);
+}
+
+int mc3_fft_inverse(float* frames, int nx, int ny, int nz, void* stream) {
+  if (!frames || nx < 2 || (nx & 1) || ny < 1 || nz < 1) return MC3_EINVAL;
+  const int cmpX = nx / 2 + 1;
+  const long ncmp = (long)cmpX * ny;
+  cudaStream_t st = as_stream(stream);
+  float2* c = reinterpret_cast<float2*>(frames);
+  Batch bc{nz, nz, ncmp, nullptr, ncmp};
+  ColOps ops{};
+  ops.dir = 1;
+  ops.scale = 1.0f;
+  int s = col_fft(c, c, cmpX, cmpX, ny, bc, ops, st);
+  if (s) return s;
+  Batch br{nz, nz, ncmp, nullptr, ncmp * 2};
+  return row_c2r(c, cmpX, frames, 2 * cmpX, nx, ny, br, st);
+}
+
+int mc3_fourier_crop(const float* in, int in_cmp_x, int in_cmp_y, float* out, int out_cmp_x,
+                     int out_cmp_y, void* stream) {
+  if (!in || !out || out_cmp_x > in_cmp_x || out_cmp_y > in_cmp_y) return MC3_EINVAL;
+  return fourier_crop(reinterpret_cast<const float2*>(in), in_cmp_x, in_cmp_y,
+                      reinterpret_cast<float2*>(out), out_cmp_x, out_cmp_y, as_stream(stream));
+}
+
+int mc3_detect_bad_pixels(const float* sum, int nx, int ny, unsigned char* bad, void* stream) {
+  if (!sum || !bad || nx < 8 || ny < 8 || (nx & 1)) return MC3_EINVAL;
+  const long pad = 2 * (nx / 2 + 1);
+  float *cc = nullptr, *part = nullptr, *mom = nullptr;
+  if (cudaMalloc(&cc, sizeof(float) * pad * ny) != cudaSuccess) return MC3_ENOMEM;
+  if (cudaMalloc(&part, sizeof(float) * 1024) != cudaSuccess) { cudaFree(cc); return MC3_ENOMEM; }
+  if (cudaMalloc(&mom, sizeof(float) * 16) != cudaSuccess) { cudaFree(cc); cudaFree(part); return MC3_ENOMEM; }
+  float tpl[36];
+  host::defect_template(6, tpl);
+  cudaStream_t st = as_stream(stream);
+  int s = detect_bad_pixels(sum, nx, ny, cc, part, mom, bad, tpl, 6, st);
+  if (s == kOk && cudaStreamSynchronize(st) != cudaSuccess) s = MC3_ECUDA;
+  cudaFree(cc);
+  cudaFree(part);
+  cudaFree(mom);
+  return s;
+}
+
+int mc3_correct_bad_pixels(float* frames, int nx, int ny, int nz, const unsigned char* bad,
+                           void* stream) {
+  if (!frames || !bad || nx < 2 || (nx & 1) || ny < 1 || nz < 1) return MC3_EINVAL;
+  const long pad = 2 * (nx / 2 + 1);
+  return correct_bad_pixels(frames, pad * ny, nz, bad, nx, ny, as_stream(stream));
+}
+
+int mc3_local_gather(const float* in, float* out, int nx, int ny, const float* centers,
+                     const float* shifts, const unsigned char* bad, int n_patches, void* stream) {
+  if (!in || !out || !centers || !shifts || n_patches < 1) return MC3_EINVAL;
+  const long pad = 2 * (nx / 2 + 1);
+  return local_gather(in, pad * ny, out, pad * ny, 1, nx, ny, centers,
+                      reinterpret_cast<const float2*>(shifts), bad, n_patches, as_stream(stream));
+}
+
+int mc3_phase_shift(const float* in, float* out, int cmp_x, int cmp_y, float sx, float sy,
+                    int accumulate, void* stream) {
+  if (!in || !out || cmp_x < 2 || cmp_y < 1) return MC3_EINVAL;
+  cudaStream_t st = as_stream(stream);
+  float2 *sh = nullptr, *ex = nullptr, *ey = nullptr;
+  int s = MC3_OK;
+  if (cudaMalloc(&sh, sizeof(float2)) != cudaSuccess || cudaMalloc(&ex, sizeof(float2) * cmp_x) != cudaSuccess ||
+      cudaMalloc(&ey, sizeof(float2) * cmp_y) != cudaSuccess) {
+    s = MC3_ENOMEM;
+  }
+  if (s == MC3_OK) {
+    float2 h;
+    h.x = sx;
+    h.y = sy;
+    if (cudaMemcpyAsync(sh, &h, sizeof(float2), cudaMemcpyHostToDevice, st) != cudaSuccess) s = MC3_ECUDA;
+    if (s == MC3_OK) s = phase_tables(sh, 1, cmp_x, cmp_y, ex, ey, false, st);
+    if (s == MC3_OK)
+      s = phase_apply(reinterpret_cast<const float2*>(in), reinterpret_cast<float2*>(out), cmp_x, cmp_y,
+                      ex, ey, accumulate != 0, st);
+    if (s == MC3_OK && cudaStreamSynchronize(st) != cudaSuccess) s = MC3_ECUDA;
+  }
+  cudaFree(sh);
+  cudaFree(ex);
+  cudaFree(ey);
+  return s;
+}
+
+int mc3_correlate(const float* group, const float* sum, int cmp_x, int cmp_y, float bfactor,
+                  int phase_only, int sea_x, int sea_y, float* window, float* shift_host,
+                  void* stream) {
+  if (!group || !sum || cmp_x < 3 || cmp_y < 4 || sea_x < 3 || sea_y < 3) return MC3_EINVAL;
+  if (sea_x > (cmp_x - 1) * 2 || sea_y > cmp_y) return MC3_EINVAL;
+  cudaStream_t st = as_stream(stream);
+  // Treat `group` as a one-frame stack whose single group is that frame;
+  // corr_cols computes conj(G) (S - G) with S = `sum`.
+  const size_t nel = (size_t)cmp_x * cmp_y;
+  float2 *sh = nullptr, *ex = nullptr, *ey = nullptr, *T = nullptr, *pk = nullptr;
+  int *act = nullptr, *gs = nullptr, *gz = nullptr;
+  float* win = nullptr;
+  int s = MC3_OK;
+  if (cudaMalloc(&sh, sizeof(float2)) != cudaSuccess || cudaMalloc(&ex, sizeof(float2) * cmp_x) != cudaSuccess ||
+      cudaMalloc(&ey, sizeof(float2) * cmp_y) != cudaSuccess || cudaMalloc(&act, sizeof(int) * 3) != cudaSuccess ||
+      cudaMalloc(&T, sizeof(float2) * (size_t)sea_y * cmp_x) != cudaSuccess ||
+      cudaMalloc(&win, sizeof(float) * (size_t)sea_x * sea_y) != cudaSuccess ||
+      cudaMalloc(&pk, sizeof(float2)) != cudaSuccess) {
+    s = MC3_ENOMEM;
+  }
+  gs = act + 1;
+  gz = act + 2;
+  if (s == MC3_OK) {
+    float2 h;
+    h.x = 0.f;
+    h.y = 0.f;
+    int hi[3] = {0, 0, 1};
+    cudaMemcpyAsync(sh, &h, sizeof(float2), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(act, hi, sizeof(int) * 3, cudaMemcpyHostToDevice, st);
+    s = phase_tables(sh, 1, cmp_x, cmp_y, ex, ey, false, st);
+    AlignDims d{};
+    d.cmpX = cmp_x;
+    d.cmpY = cmp_y;
+    d.N = 1;
+    d.stack_stride = (long)nel;
+    d.G = 1;
+    d.seaX = sea_x;
+    d.seaY = sea_y;
+    d.A = 1;
+    if (s == MC3_OK)
+      s = corr_cols(reinterpret_cast<const float2*>(group), act, ex, ey,
+                    reinterpret_cast<const float2*>(sum), gs, gz, bfactor, phase_only, T, d, st);
+    if (s == MC3_OK) s = corr_rows(T, win, d, st);
+    if (s == MC3_OK) s = peak_search(win, pk, d, st);
+    if (s == MC3_OK && window)
+      cudaMemcpyAsync(window, win, sizeof(float) * sea_x * sea_y, cudaMemcpyDeviceToDevice, st);
+    float2 r;
+    if (s == MC3_OK) {
+      cudaMemcpyAsync(&r, pk, sizeof(float2), cudaMemcpyDeviceToHost, st);
+      if (cudaStreamSynchronize(st) != cudaSuccess) s = MC3_ECUDA;
+      if (s == MC3_OK && shift_host) {
+        shift_host[0] = r.x;
+        shift_host[1] = r.y;
+      }
+    }
+  }
+  cudaFree(sh);
+  cudaFree(ex);
+  cudaFree(ey);
+  cudaFree(act);
+  cudaFree(T);
+  cudaFree(win);
+  cudaFree(pk);
+  return s;
+}
+
+int mc3_iterative_align(mc3_ctx* ctx, const float* stack, int cmp_x, int cmp_y, int n, int group,
+                        int max_iter, float tol, float bfactor, int phase_only, float* shifts_host,
+                        int* iters) {
+  if (!ctx || !stack || !shifts_host || n < 3 || group < 1 || max_iter < 1) return MC3_EINVAL;
+  Engine* e = ctx->eng;
+  const int saved_iter = e->prm.iter, saved_po = e->prm.phase_only;
+  e->prm.iter = max_iter;
+  e->prm.phase_only = phase_only;
+  host::FrameGroups g;
+  g.setup(n, group);
+  std::vector<host::StackShift> sh;
+  std::vector<int> it;
+  std::vector<std::vector<float>> err;
+  int s = e->align_stacks(reinterpret_cast<const float2*>(stack), (long)cmp_x * cmp_y * n, 1, cmp_x,
+                          cmp_y, n, g, bfactor, tol, sh, it, err);
+  e->prm.iter = saved_iter;
+  e->prm.phase_only = saved_po;
+  if (s != kOk) return s;
+  for (int f = 0; f < n; ++f) {
+    shifts_host[2 * f] = sh[0].x(f);
+    shifts_host[2 * f + 1] = sh[0].y(f);
+  }
+  if (iters) *iters = it[0];
+  return MC3_OK;
+}
+
+int mc3_dose_weighted_sums(mc3_ctx* ctx, const float* spectra, int nx, int ny, int nz,
+                           const float* shifts_host, float* sums, int* n_sums) {
+  if (!ctx || !spectra || !sums || !shifts_host) return MC3_EINVAL;
+  Engine* e = ctx->eng;
+  Geometry g;
+  int s = g.compute(nx, ny, nz, e->prm);
+  if (s) return s;
+  host::StackShift fs;
+  fs.setup(nz);
+  for (int f = 0; f < nz; ++f) {
+    fs.x(f) = shifts_host[2 * f];
+    fs.y(f) = shifts_host[2 * f + 1];
+  }
+  const size_t ncmp = (size_t)g.cmpX * g.cmpY;
+  cudaStream_t st = e->stream;
+  if ((s = e->d_acc.ensure(sizeof(float) * nz)) || (s = e->d_Wn.ensure(sizeof(float) * ncmp))) return s;
+  std::vector<float> acc(nz);
+  for (int i = 0; i < nz; ++i) acc[i] = e->prm.fm_dose * (i + 1);
+  if (cudaMemcpyAsync(e->d_acc.p, acc.data(), sizeof(float) * nz, cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return MC3_ECUDA;
+  DoseParams dp{};
+  dp.enabled = g.dw ? 1 : 0;
+  dp.dws = g.dws ? 1 : 0;
+  dp.pix_size = e->prm.pix_size;
+  dp.kv_factor = host::kv_factor(e->prm.kv);
+  dp.sum_range[0] = e->prm.sum_range[0];
+  dp.sum_range[1] = e->prm.sum_range[1];
+  if (g.dw && (s = dose_norm(e->d_acc.as<float>(), nz, g.cmpX, g.cmpY, dp.pix_size, dp.kv_factor,
+                             e->d_Wn.as<float>(), st)))
+    return s;
+  if ((s = e->global_sums(reinterpret_cast<const float2*>(spectra), nz, fs, g))) return s;
+  s = frame_sums(reinterpret_cast<const float2*>(spectra), (long)ncmp, nz, g.cmpX, g.cmpY,
+                 e->d_fex.as<float2>(), e->d_fey.as<float2>(), e->d_acc.as<float>(), e->d_Wn.as<float>(),
+                 dp, reinterpret_cast<float2*>(sums), g.nSums, st);
+  if (s) return s;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return MC3_ECUDA;
+  if (n_sums) *n_sums = g.nSums;
+  return MC3_OK;
+}
+
+// ---- host bookkeeping ----
+void mc3_peak2d(const float* window, int sea_x, int sea_y, float* shift) {
+  host::peak2d(window, sea_x, sea_y, shift);
+}
+
+void mc3_remove_spikes(float* sx, float* sy, int n) { host::remove_spikes(sx, sy, n); }
+
+int mc3_lin_eqs(float* coeff, float* vals, int dim) { return host::lin_eqs(coeff, vals, dim) ? 1 : 0; }
+
+void mc3_smooth_shifts(float* sx, float* sy, int n, float weight) {
+  host::StackShift s;
+  s.setup(n);
+  std::memcpy(s.v.data(), sx, sizeof(float) * n);
+  std::memcpy(s.v.data() + n, sy, sizeof(float) * n);
+  s.smooth(weight);
+  std::memcpy(sx, s.v.data(), sizeof(float) * n);
+  std::memcpy(sy, s.v.data() + n, sizeof(float) * n);
+}
+
+void mc3_patch_make_relative(float* shifts, int nz, int n_patches) {
+  std::vector<float> v(shifts, shifts + (size_t)nz * n_patches * 2);
+  host::patch_make_relative(v, nz, n_patches);
+  std::memcpy(shifts, v.data(), sizeof(float) * v.size());
+}
+
+void mc3_patch_detect_bads(const float* shifts, const float* centers, int nz, int n_patches,
+                           int nx, int ny, unsigned char* bad) {
+  host::patch_detect_bads(shifts, centers, nz, n_patches, nx, ny, bad);
+}
+
+}  // extern "C"

@@ -1,0 +1,301 @@
+// MotionCor3-compatible command line over libmc3 (single-movie MRC mode).
+//
+// Tags, defaults and value parsing follow CInput::Parse (CInput.cpp:425-677)
+// and Util::CParseArgs (Util/CParseArgs.cpp); output naming follows
+// sGenOutputName (CSaveSerialCryoEM.cpp:13-31) and CAlnSums::Setup
+// (DataUtil/CAlnSums.cpp:18-43); log files follow CFullAlign::LogShift
+// (Align/CFullAlign.cpp:173-194) and CPatchShifts::Log* (Align/CPatchShifts.cpp:155-249);
+// exit codes follow ERetCode (CMotionCor3.cpp:20-28).  Tags outside the
+// implemented path are accepted and ignored with a warning.
+#include <cctype>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <strings.h>
+#include <vector>
+
+#include "../../include/mc3.h"
+#include "mrc.h"
+
+namespace {
+
+enum RetCode { eSuccess = 0, eNoFreeGPUs = 1, eInputOutputSame = 2, eFailLoad = 3, eFailSave = 4,
+               eNoValidGPUs = 5, eFailProcess = 6 };
+
+struct Args {
+  int argc;
+  char** argv;
+  // CParseArgs::FindVals: values follow the tag until a token "-<alpha>...".
+  bool find(const char* tag, int* first, int* count) const {
+    *first = -1;
+    *count = 0;
+    for (int i = 1; i < argc; ++i)
+      if (strcasecmp(argv[i], tag) == 0) {
+        *first = i + 1;
+        break;
+      }
+    if (*first < 0) return false;
+    for (int i = *first; i < argc; ++i) {
+      const char* a = argv[i];
+      if (a[0] == '-' && std::strlen(a) >= 2 && std::isalpha((unsigned char)a[1])) break;
+      char buf[256];
+      std::snprintf(buf, sizeof(buf), "%s", a);
+      for (char* t = std::strtok(buf, ", "); t; t = std::strtok(nullptr, ", ")) *count += 1;
+    }
+    return *count > 0;
+  }
+  std::string str(const char* tag) const {
+    int f, n;
+    if (!find(tag, &f, &n) || f >= argc) return std::string();
+    return argv[f];
+  }
+  int ints(const char* tag, int* v, int maxn) const {
+    int f, n;
+    if (!find(tag, &f, &n)) return 0;
+    if (n > maxn) n = maxn;
+    int c = 0;
+    for (int i = 0; i < n && f + i < argc && c < n; ++i) {
+      char buf[256];
+      std::snprintf(buf, sizeof(buf), "%s", argv[f + i]);
+      for (char* t = std::strtok(buf, ", "); t && c < n; t = std::strtok(nullptr, ", "))
+        std::sscanf(t, "%d", v + c++);
+    }
+    return c;
+  }
+  int floats(const char* tag, float* v, int maxn) const {
+    int f, n;
+    if (!find(tag, &f, &n)) return 0;
+    if (n > maxn) n = maxn;
+    int c = 0;
+    for (int i = 0; i < n && f + i < argc; ++i) std::sscanf(argv[f + i], "%f", v + c++);
+    return c;
+  }
+};
+
+std::string out_name(const std::string& out_mrc, const char* suffix, const char* ext) {
+  std::string s = out_mrc;
+  auto cut = [&](const char* pat) {
+    const char* p = strcasestr(s.c_str(), pat);
+    if (p) s.resize(p - s.c_str());
+  };
+  cut(".mrc");
+  cut(".st");
+  return s + suffix + ext;
+}
+
+std::string log_stem(const std::string& log_dir, const std::string& in_file) {
+  if (log_dir.empty()) return std::string();
+  const char* base = std::strrchr(in_file.c_str(), '/');
+  base = base ? base + 1 : in_file.c_str();
+  std::string s = log_dir + base;
+  const char* p = strcasestr(s.c_str(), ".mrc");
+  if (!p) return std::string();
+  s.resize(p - s.c_str());
+  return s;
+}
+
+void stats(const float* img, size_t n, float* mn, float* mx, float* mean) {
+  double s = 0;
+  float a = img[0], b = img[0];
+  for (size_t i = 0; i < n; ++i) {
+    a = img[i] < a ? img[i] : a;
+    b = img[i] > b ? img[i] : b;
+    s += img[i];
+  }
+  *mn = a;
+  *mx = b;
+  *mean = (float)(s / n);
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  if (argc == 2 && strcasecmp(argv[1], "--version") == 0) {
+    std::printf("MotionCor3 (mc3-b200) %s\n", mc3_version());
+    return eSuccess;
+  }
+  if (argc <= 1 || (argc == 2 && strcasecmp(argv[1], "--help") == 0)) {
+    std::printf("Usage: MotionCor3 -InMrc movie.mrc -OutMrc sum.mrc [-Gain gain.mrc] "
+                "[-Patch x y] [-Iter n] [-Tol px] [-Bft g p] [-FmDose d] [-PixSize a] "
+                "[-kV kv] [-Group g p] [-FmRef f] [-SumRange lo hi] [-PhaseOnly 0|1] "
+                "[-LogDir dir] [-Gpu id]\n");
+    return eSuccess;
+  }
+  Args A{argc, argv};
+  mc3_params p;
+  mc3_params_default(&p);
+  const std::string in_mrc = A.str("-InMrc");
+  const std::string out_mrc = A.str("-OutMrc");
+  const std::string gain_mrc = A.str("-Gain");
+  std::string log_dir = A.str("-LogDir");
+  if (!log_dir.empty() && log_dir.back() != '/') log_dir += "/";
+  int pt[3] = {0, 0, 0};
+  A.ints("-Patch", pt, 3);
+  p.patch[0] = pt[0] <= 1 ? 0 : pt[0];
+  p.patch[1] = pt[1] <= 1 ? 0 : pt[1];
+  A.ints("-Iter", &p.iter, 1);
+  A.floats("-Tol", &p.tol, 1);
+  A.floats("-Bft", p.bft, 2);
+  A.ints("-PhaseOnly", &p.phase_only, 1);
+  A.floats("-FtBin", &p.ft_bin, 1);
+  A.floats("-InitDose", &p.init_dose, 1);
+  A.floats("-FmDose", &p.fm_dose, 1);
+  A.floats("-PixSize", &p.pix_size, 1);
+  A.ints("-kV", &p.kv, 1);
+  A.ints("-Align", &p.align, 1);
+  if (A.floats("-SumRange", p.sum_range, 2) && p.sum_range[0] < 0) p.sum_range[0] = 0;
+  A.ints("-Group", p.group, 2);
+  if (p.group[0] < 1) p.group[0] = 1;
+  if (p.group[1] < 1) p.group[1] = 1;
+  A.ints("-FmRef", &p.fm_ref, 1);
+  int gpu[8];
+  if (A.ints("-Gpu", gpu, 8) > 0) p.gpu = gpu[0];
+  const char* ignored[] = {"-InTiff", "-InEer", "-InSuffix", "-InSkips", "-ArcDir", "-Dark",
+                           "-DefectFile", "-InAln", "-OutAln", "-DefectMap", "-FullSum", "-TmpFile",
+                           "-StackZ", "-Cs", "-AmpCont", "-ExtPhase", "-Throw", "-Trunc", "-Serial",
+                           "-Tilt", "-Crop", "-OutStack", "-RotGain", "-FlipGain", "-InvGain", "-Mag",
+                           "-InFmMotion", "-GpuMemUsage", "-UseGpus", "-SplitSum", "-FmIntFile",
+                           "-EerSampling", "-OutStar", "-TiffOrder", "-CorrInterp"};
+  for (const char* t : ignored) {
+    int f, n;
+    A.find(t, &f, &n);
+    if (f > 0) std::fprintf(stderr, "Warning: %s is outside the implemented path and is ignored.\n", t);
+  }
+  if (in_mrc.empty() || out_mrc.empty()) return eFailLoad;
+  if (in_mrc == out_mrc) return eInputOutputSame;
+
+  mc3::mrc::Header h;
+  if (!mc3::mrc::read_header(in_mrc, &h) || mc3::mrc::bytes_per_pixel(h.mode) == 0) {
+    std::fprintf(stderr, "Error: cannot load %s\n", in_mrc.c_str());
+    return eFailLoad;
+  }
+  std::printf("MRC file size mode: %d  %d  %d  %d\n", h.nx, h.ny, h.nz, h.mode);
+  const size_t frame_bytes = (size_t)h.nx * h.ny * mc3::mrc::bytes_per_pixel(h.mode);
+  std::vector<unsigned char> frames(frame_bytes * h.nz);
+  if (!mc3::mrc::read_frames(in_mrc, h, 0, h.nz, frames.data())) return eFailLoad;
+
+  mc3_ctx* ctx = nullptr;
+  int s = mc3_create(&p, &ctx);
+  if (s != MC3_OK) {
+    std::fprintf(stderr, "Error: %s\n", mc3_strerror(s));
+    return eNoValidGPUs;
+  }
+  if (!gain_mrc.empty()) {
+    std::vector<float> gain;
+    int gx = 0, gy = 0;
+    if (!mc3::mrc::read_image_float(gain_mrc, &gain, &gx, &gy)) {
+      std::printf("Warning: Gain ref not found.\n......   Gain correction will be skipped.\n\n");
+    } else if (gx != h.nx || gy != h.ny) {
+      std::fprintf(stderr, "Error: Gain and frame dimensions mismatch!\n"
+                           "...... Gain size:  %d  %d\n...... Frame size: %d  %d\n"
+                           "Motion correction skipped.\n\n", gx, gy, h.nx, h.ny);
+      mc3_destroy(ctx);
+      return eFailProcess;
+    } else {
+      mc3_set_gain(ctx, gain.data(), gx, gy, 0);
+    }
+  }
+  mc3_plan_info info;
+  if ((s = mc3_plan(ctx, h.nx, h.ny, h.nz, &info)) != MC3_OK) {
+    std::fprintf(stderr, "Error: %s\n", mc3_strerror(s));
+    mc3_destroy(ctx);
+    return eFailProcess;
+  }
+  const int N = h.nz, P = info.n_patches;
+  std::vector<float> sums((size_t)info.n_sums * h.nx * h.ny);
+  std::vector<float> gsh(2 * (size_t)N), psh(2 * (size_t)N * (P > 0 ? P : 1)), pc(2 * (P > 0 ? P : 1));
+  std::vector<unsigned char> pb((size_t)N * (P > 0 ? P : 1));
+  std::vector<int> iters(1 + P);
+  std::vector<float> errs((size_t)p.iter * (1 + P));
+  mc3_movie mv{frames.data(), h.mode, h.nx, h.ny, h.nz, 0};
+  mc3_result r{};
+  r.sums = sums.data();
+  r.global_shifts = gsh.data();
+  r.patch_shifts = P ? psh.data() : nullptr;
+  r.patch_centers = P ? pc.data() : nullptr;
+  r.patch_bad = P ? pb.data() : nullptr;
+  r.iterations = iters.data();
+  r.errors = errs.data();
+  auto t0 = std::chrono::steady_clock::now();
+  s = mc3_process_movie(ctx, &mv, &r);
+  auto t1 = std::chrono::steady_clock::now();
+  if (s != MC3_OK) {
+    std::fprintf(stderr, "Error: processing failed: %s\n", mc3_strerror(s));
+    mc3_destroy(ctx);
+    return eFailProcess;
+  }
+  for (int i = 0; i < iters[0]; ++i)
+    std::printf("Iteration %2d  Error: %9.3f\n", i + 1, errs[i]);
+  std::printf("Computation time: %f sec\n\n", std::chrono::duration<double>(t1 - t0).count());
+  // ---- sums ----
+  const char* ext_dw[3] = {"", "_DW", "_DWS"};
+  const float pix = p.pix_size * p.ft_bin;
+  bool saved = true;
+  for (int i = 0; i < r.n_sums; ++i) {
+    const float* img = sums.data() + (size_t)i * h.nx * h.ny;
+    float mn, mx, me;
+    stats(img, (size_t)h.nx * h.ny, &mn, &mx, &me);
+    const std::string name = out_name(out_mrc, ext_dw[i], ".mrc");
+    saved = mc3::mrc::write_float_image(name, img, h.nx, h.ny, pix, mn, mx, me) && saved;
+    std::printf("Corrected sum has been saved in:\n   %s\n\n", name.c_str());
+  }
+  // ---- logs ----
+  const std::string stem = log_stem(log_dir, in_mrc);
+  if (!stem.empty()) {
+    const char* fmt = "%4d  %8.2f  %8.2f\n";
+    if (P == 0) {
+      FILE* f = std::fopen((stem + "-Full.log").c_str(), "wt");
+      if (f) {
+        std::fprintf(f, "# full frame alignment\n");
+        for (int i = 0; i < N; ++i) std::fprintf(f, fmt, i + 1, gsh[2 * i], gsh[2 * i + 1]);
+        std::fclose(f);
+      }
+    } else {
+      FILE* f = std::fopen((stem + "-Patch-Full.log").c_str(), "wt");
+      if (f) {
+        std::fprintf(f, "# Patch based alignment\n");
+        std::fprintf(f, "# Initial alignment based upon full frames\n\n");
+        for (int i = 0; i < N; ++i) std::fprintf(f, fmt, i + 1, gsh[2 * i], gsh[2 * i + 1]);
+        std::fclose(f);
+      }
+      f = std::fopen((stem + "-Patch-Patch.log").c_str(), "wt");
+      if (f) {
+        std::fprintf(f, "# Patch based alignment\n");
+        std::fprintf(f, "# Number of patches: %d\n", P);
+        std::fprintf(f, "# Shifts are listed per patch.\n");
+        std::fprintf(f, "# Movie size: %d  %d  %d\n\n", h.nx, h.ny, N);
+        for (int i = 0; i < P; ++i) {
+          std::fprintf(f, "#Patch %03d raw and fit shifts\n", i + 1);
+          for (int j = 0; j < N; ++j) {
+            const size_t k = (size_t)j * P + i;
+            std::fprintf(f, "%4d %8.2f %8.2f ", j + 1, pc[2 * i], pc[2 * i + 1]);
+            std::fprintf(f, "%8.2f %8.2f %4d\n", psh[2 * k], psh[2 * k + 1], (int)pb[k]);
+          }
+          std::fprintf(f, "\n");
+        }
+        std::fclose(f);
+      }
+      f = std::fopen((stem + "-Patch-Frame.log").c_str(), "wt");
+      if (f) {
+        std::fprintf(f, "# Patch based alignment\n");
+        std::fprintf(f, "# Number of patches: %d\n", P);
+        std::fprintf(f, "# Shifts are listed per frame.\n");
+        std::fprintf(f, "# Movie size: %d  %d  %d\n\n", h.nx, h.ny, N);
+        for (int i = 0; i < N; ++i) {
+          for (int j = 0; j < P; ++j) {
+            const size_t k = (size_t)i * P + j;
+            std::fprintf(f, "%4d %8.2f %8.2f ", i + 1, pc[2 * j], pc[2 * j + 1]);
+            std::fprintf(f, "%8.2f %8.2f %4d\n", psh[2 * k], psh[2 * k + 1], (int)pb[k]);
+          }
+          std::fprintf(f, "\n");
+        }
+        std::fclose(f);
+      }
+    }
+  }
+  mc3_destroy(ctx);
+  return saved ? eSuccess : eFailSave;
+}

@@ -1,0 +1,170 @@
+// Correction kernels: dose-weight normalisation, fused shift + dose weight
+// + summation over all frames, local-motion gather, output unpadding.
+// Restates Correct/GWeightFrame.cu, Correct/CCorrectFullShift.cpp:271-334,
+// Correct/GCorrectPatchShift.cu:17-66 and the positivity/unpad steps of
+// CCorrectFullShift::mUnpadSums (:146-185).
+#include "kernels.cuh"
+
+namespace mc3 {
+
+// GWeightFrame mGCalcWeight (Correct/GWeightFrame.cu:19-30)
+__device__ __forceinline__ float dose_weight(int x, int y, int cmpX, int cmpY, float fDose,
+                                             float kvf, float pix) {
+  float fX = (float)x * 0.5f / (float)(unsigned)(cmpX - 1);
+  float fY = y / (float)cmpY;
+  if (fY >= 0.5f) fY -= 1.0f;
+  fX = sqrtf(fX * fX + fY * fY) / pix;
+  float fCritDose = 0.24499f * powf(fX, -1.6649f) + 2.8141f;
+  fCritDose *= kvf;
+  return expf(-0.5f * fDose / fCritDose);
+}
+
+// GWeightFrame::BuildWeight: per-frame accumulation of w^2 in frame order,
+// then the square root; DC excluded (stays 0).
+__global__ void k_dose_norm(const float* acc, int N, int cmpX, int cmpY, float pix, float kvf,
+                            float* Wn) {
+  const long n = (long)cmpX * cmpY;
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (i == 0) {
+    Wn[0] = 0.0f;
+    return;
+  }
+  const int x = (int)(i % cmpX), y = (int)(i / cmpX);
+  float s = 0.0f;
+  for (int f = 0; f < N; ++f) {
+    const float w = dose_weight(x, y, cmpX, cmpY, acc[f], kvf, pix);
+    s += (w * w);
+  }
+  Wn[i] = sqrtf(s);
+}
+
+int dose_norm(const float* acc_dose, int N, int cmpX, int cmpY, float pix, float kvf, float* Wn,
+              cudaStream_t st) {
+  const long n = (long)cmpX * cmpY;
+  k_dose_norm<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(acc_dose, N, cmpX, cmpY, pix, kvf, Wn);
+  MC3_CHECK_LAUNCH("k_dose_norm");
+  return kOk;
+}
+
+// All sums in one pass over the frames (CCorrectFullShift::mGenSums):
+// sum0 += X; X *= w_f/Wn (DC untouched); sum1 += X; sum2 += X when the
+// frame's accumulated dose lies in the selected range.
+__global__ void k_frame_sums(const float2* __restrict__ spec, long fr_stride, int N, int cmpX,
+                             int cmpY, const float2* __restrict__ ex, const float2* __restrict__ ey,
+                             const float* acc, const float* Wn, DoseParams dp, float2* sums,
+                             int n_sums) {
+  const long n = (long)cmpX * cmpY;
+  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int x = (int)(k % cmpX), y = (int)(k / cmpX);
+  float2 s0 = c2(0.f, 0.f), s1 = c2(0.f, 0.f), s2 = c2(0.f, 0.f);
+  const float wn = dp.enabled && k > 0 ? Wn[k] : 1.0f;
+  for (int f = 0; f < N; ++f) {
+    float2 X = spec[(long)f * fr_stride + k];
+    if (ex) {
+      const float2 e = cmul(ex[(long)f * cmpX + x], ey[(long)f * cmpY + y]);
+      X = c2(e.x * X.x - e.y * X.y, e.x * X.y + e.y * X.x);
+    }
+    s0 = cadd(X, s0);
+    if (dp.enabled) {
+      if (k > 0) {
+        float fW = dose_weight(x, y, cmpX, cmpY, acc[f], dp.kv_factor, dp.pix_size);
+        fW = fW / wn;
+        X.x *= fW;
+        X.y *= fW;
+      }
+      s1 = cadd(X, s1);
+      if (dp.dws && acc[f] >= dp.sum_range[0] && acc[f] <= dp.sum_range[1]) s2 = cadd(X, s2);
+    }
+  }
+  sums[k] = s0;
+  if (n_sums > 1) sums[n + k] = s1;
+  if (n_sums > 2) sums[2 * n + k] = s2;
+}
+
+int frame_sums(const float2* spec, long fr_stride, int N, int cmpX, int cmpY, const float2* ex,
+               const float2* ey, const float* acc_dose, const float* Wn, const DoseParams& dp,
+               float2* sums, int n_sums, cudaStream_t st) {
+  const long n = (long)cmpX * cmpY;
+  k_frame_sums<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(spec, fr_stride, N, cmpX, cmpY, ex, ey,
+                                                           acc_dose, Wn, dp, sums, n_sums);
+  MC3_CHECK_LAUNCH("k_frame_sums");
+  return kOk;
+}
+
+// mGCorrect3D (Correct/GCorrectPatchShift.cu:17-66) with upsampling 1:
+// per-pixel local shift = sum_p w_p s_p / sum_p w_p, w_p = exp(-100 r_p)
+// over good patches with normalised distance r_p <= 0.6, then a
+// nearest-neighbour (int-truncated) gather; out-of-range sources fold to
+// (811*|v|) mod size.
+__global__ void k_local_gather(const float* __restrict__ in, long in_stride, float* out,
+                               long out_stride, int W, int H, const float* __restrict__ cent,
+                               const float2* __restrict__ sh, const uint8_t* __restrict__ bad,
+                               int P, int f0) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= W) return;
+  const int b = blockIdx.z;
+  const int f = f0 + b;
+  const float2* s = sh + (long)f * P;
+  const uint8_t* bd = bad ? bad + (long)f * P : nullptr;
+  const float fB = 100.0f;
+  float fSx = 0.0f, fSy = 0.0f, fW = 0.0f;
+  for (int p = 0; p < P; ++p) {
+    if (bd != 0 && bd[p]) continue;
+    float ax = ((float)(unsigned)x - cent[2 * p]) / (float)(unsigned)W;
+    float ay = (y - cent[2 * p + 1]) / H;
+    ax = sqrtf(ax * ax + ay * ay);
+    if (ax > 0.6f) continue;
+    ax = expf(-fB * ax);
+    fW += ax;
+    fSx += s[p].x * ax;
+    fSy += s[p].y * ax;
+  }
+  if (fW > 0) {
+    fSx = fSx / fW;
+    fSy = fSy / fW;
+  }
+  int ix = (int)(((float)(unsigned)x - fSx) * 1);
+  int iy = (int)((y - fSy) * 1);
+  if (ix < 0 || iy < 0 || ix >= W || iy >= H) {
+    ix = (ix < 0) ? -ix : ix;
+    iy = (iy < 0) ? -iy : iy;
+    ix = (811 * ix) % W;
+    iy = (811 * iy) % H;
+  }
+  const int padX = (W / 2 + 1) * 2;
+  out[(long)b * out_stride + (long)y * padX + x] = in[(long)b * in_stride + (long)iy * padX + ix];
+}
+
+int local_gather(const float* in, long in_stride, float* out, long out_stride, int nb, int W,
+                 int H, const float* centers, const float2* shifts, const uint8_t* bad, int P,
+                 cudaStream_t st) {
+  // `shifts`/`bad` point at the first frame of the batch.
+  dim3 grid(ceil_div(W, 256), H, nb);
+  k_local_gather<<<grid, 256, 0, st>>>(in, in_stride, out, out_stride, W, H, centers, shifts, bad,
+                                       P, 0);
+  MC3_CHECK_LAUNCH("k_local_gather");
+  return kOk;
+}
+
+__global__ void k_unpad_positive(const float* in, long pitch, float* out, int W, int H,
+                                 long in_stride) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= W) return;
+  const int s = blockIdx.z;
+  const float v = in[(long)s * in_stride + (long)y * pitch + x];
+  out[(long)s * W * H + (long)y * W + x] = fmaxf(0.0f, v);
+}
+
+int unpad_positive(const float* in, long pitch, float* out, int W, int H, int n, long in_stride,
+                   cudaStream_t st) {
+  dim3 grid(ceil_div(W, 256), H, n);
+  k_unpad_positive<<<grid, 256, 0, st>>>(in, pitch, out, W, H, in_stride);
+  MC3_CHECK_LAUNCH("k_unpad_positive");
+  return kOk;
+}
+
+}  // namespace mc3

@@ -1,0 +1,541 @@
+// Processing engine: the single-movie path of CProcessThread::mProcess
+// (CProcessThread.cpp:82-107) on one GPU stream.
+#include "engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <math.h>
+
+namespace mc3 {
+
+int cuda_status(cudaError_t e, const char* where) {
+  (void)where;
+  if (e == cudaSuccess) return kOk;
+  if (e == cudaErrorMemoryAllocation) return kENoMem;
+  return kECuda;
+}
+
+int last_cuda_status(const char* where) { return cuda_status(cudaGetLastError(), where); }
+
+int DevBuf::ensure(size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  if (bytes <= cap) return kOk;
+  release();
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    cudaGetLastError();
+    return kENoMem;
+  }
+  cap = bytes;
+  return kOk;
+}
+
+void DevBuf::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  cap = 0;
+}
+
+// ---------------------------------------------------------------------------
+int Geometry::compute(int w, int h, int n, const mc3_params& p) {
+  if (w < 16 || h < 16 || n < 3 || (w & 1) || (h & 1)) return kEInval;
+  W = w;
+  H = h;
+  N = n;
+  cmpX = W / 2 + 1;
+  cmpY = H;
+  padX = 2 * cmpX;
+  // CBufferPool::mCreateXcfBuffer (CBufferPool.cpp:220-242)
+  const float fBinX = W / 2048.0f;
+  const float fBinY = H / 2048.0f;
+  float fBin = (float)fmin(fBinX, fBinY);
+  if (fBin < 1) fBin = 1.0f;
+  const int iXcfX = (int)(W / fBin + 0.5f);
+  const int iXcfY = (int)(H / fBin + 0.5f);
+  xcfCmpX = iXcfX / 2 + 1;
+  xcfCmpY = iXcfY / 2 * 2;
+  xcfBin[0] = (cmpX - 1.0f) / (xcfCmpX - 1.0f);
+  xcfBin[1] = cmpY * 1.0f / xcfCmpY;
+  // CBufferPool::mCreatePatBuffer (CBufferPool.cpp:244-262),
+  // CPatchCenters::Calculate patch size (Align/CPatchCenters.cpp:48-51)
+  Px = p.patch[0] > 1 ? p.patch[0] : 0;
+  Py = p.patch[1] > 1 ? p.patch[1] : 0;
+  patch = false;
+  P = 0;
+  if (Px > 1 && Py > 1) {
+    const int ix = (xcfCmpX - 1) * 2, iy = xcfCmpY;
+    const int ipx = ix / Px, ipy = iy / Py;
+    if (ipx <= ix / 2 && ipy <= iy / 2) {
+      patch = true;
+      P = Px * Py;
+      patCmpX = ipx / 2 + 1;
+      patCmpY = ipy / 2 * 2;
+      patSizeX = ix / Px / 2 * 2;
+      patSizeY = iy / Py / 2 * 2;
+    }
+  }
+  // CFmIntParam::bDoseWeight / bDWSelectedSum (DataUtil/CFmIntParam.cpp:222-247)
+  dw = !(p.kv < 80 || p.kv > 300) && p.pix_size > 0 && p.fm_dose > 0;
+  dws = dw && p.sum_range[0] >= 0 && p.sum_range[1] > 0 &&
+        (p.sum_range[1] - p.sum_range[0]) > 1.0f;
+  nSums = 1 + (dw ? 1 : 0) + (dws ? 1 : 0);
+  return kOk;
+}
+
+// ---------------------------------------------------------------------------
+Engine::Engine(const mc3_params& p) : prm(p) { device = p.gpu; }
+
+Engine::~Engine() {
+  if (device >= 0) cudaSetDevice(device);
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+  if (own_stream) cudaStreamDestroy(own_stream);
+}
+
+int Engine::init() {
+  MC3_CUDA(cudaSetDevice(device));
+  MC3_CUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
+  stream = own_stream;
+  MC3_CUDA(cudaEventCreate(&ev0));
+  MC3_CUDA(cudaEventCreate(&ev1));
+  return kOk;
+}
+
+int Engine::set_stream(cudaStream_t s) {
+  stream = s ? s : own_stream;
+  return kOk;
+}
+
+int Engine::set_gain(const float* gain, int w, int h, bool on_device) {
+  MC3_CUDA(cudaSetDevice(device));
+  if (!gain) {
+    has_gain = false;
+    return kOk;
+  }
+  if (w <= 0 || h <= 0) return kEInval;
+  MC3_TRY(d_gain.ensure(sizeof(float) * (size_t)w * h));
+  MC3_CUDA(cudaMemcpyAsync(d_gain.p, gain, sizeof(float) * (size_t)w * h,
+                           on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream));
+  MC3_CUDA(cudaStreamSynchronize(stream));
+  has_gain = true;
+  gain_w = w;
+  gain_h = h;
+  return kOk;
+}
+
+int Engine::plan(int w, int h, int n, mc3_plan_info* info) {
+  Geometry g;
+  MC3_TRY(g.compute(w, h, n, prm));
+  info->n_sums = g.nSums;
+  info->n_patches = g.P;
+  info->xcf_size[0] = (g.xcfCmpX - 1) * 2;
+  info->xcf_size[1] = g.xcfCmpY;
+  info->patch_size[0] = g.patch ? (g.patCmpX - 1) * 2 : 0;
+  info->patch_size[1] = g.patch ? g.patCmpY : 0;
+  info->xcf_bin[0] = g.xcfBin[0];
+  info->xcf_bin[1] = g.xcfBin[1];
+  size_t cmp = (size_t)g.cmpX * g.cmpY * sizeof(float2);
+  size_t xcf = (size_t)g.xcfCmpX * g.xcfCmpY * sizeof(float2);
+  size_t bytes = cmp * g.N + xcf * g.N + cmp * (g.nSums + 2) + (size_t)g.W * g.H * 4 * g.N;
+  if (g.patch) bytes += (size_t)g.P * g.N * g.patCmpX * g.patCmpY * sizeof(float2) + 2 * cmp * 32;
+  info->device_bytes = bytes;
+  return kOk;
+}
+
+// ---------------------------------------------------------------------------
+// Batched CIterativeAlign::mAlignStack (Align/CIterativeAlign.cpp:99-156).
+int Engine::align_stacks(const float2* spec, long stack_stride, int nstack, int cmpX, int cmpY,
+                         int N, const host::FrameGroups& grp, float bf0, float tol,
+                         std::vector<host::StackShift>& shifts, std::vector<int>& iters,
+                         std::vector<std::vector<float>>& errors) {
+  const int G = grp.count();
+  const int imgX = (cmpX - 1) * 2;
+  AlignDims d;
+  d.cmpX = cmpX;
+  d.cmpY = cmpY;
+  d.N = N;
+  d.stack_stride = stack_stride;
+  d.G = G;
+  d.seaX = 64 < imgX ? 64 : imgX;   // CAlignStack::Set2 (Align/CAlignStack.cpp:58-61)
+  d.seaY = 64 < cmpY ? 64 : cmpY;
+  const size_t nel = (size_t)cmpX * cmpY;
+  MC3_TRY(d_sh.ensure(sizeof(float2) * (size_t)nstack * N));
+  MC3_TRY(d_ex.ensure(sizeof(float2) * (size_t)nstack * N * cmpX));
+  MC3_TRY(d_ey.ensure(sizeof(float2) * (size_t)nstack * N * cmpY));
+  MC3_TRY(d_S.ensure(sizeof(float2) * (size_t)nstack * nel));
+  MC3_TRY(d_T.ensure(sizeof(float2) * (size_t)nstack * G * d.seaY * cmpX));
+  MC3_TRY(d_win.ensure(sizeof(float) * (size_t)nstack * G * d.seaY * d.seaX));
+  MC3_TRY(d_gsh.ensure(sizeof(float2) * (size_t)nstack * G));
+  MC3_TRY(d_act.ensure(sizeof(int) * (size_t)nstack));
+  MC3_TRY(d_gstart.ensure(sizeof(int) * (size_t)G));
+  MC3_TRY(d_gsize.ensure(sizeof(int) * (size_t)G));
+  MC3_CUDA(cudaMemcpyAsync(d_gstart.p, grp.start.data(), sizeof(int) * G, cudaMemcpyHostToDevice, stream));
+  MC3_CUDA(cudaMemcpyAsync(d_gsize.p, grp.size.data(), sizeof(int) * G, cudaMemcpyHostToDevice, stream));
+
+  std::vector<host::IterState> st(nstack);
+  for (auto& s : st) s.start(N, G, bf0);
+  std::vector<int> active(nstack);
+  for (int i = 0; i < nstack; ++i) active[i] = i;
+  std::vector<float2> hsh((size_t)nstack * N);
+  std::vector<float2> hg((size_t)nstack * G);
+  for (int it = 0; it < prm.iter && !active.empty(); ++it) {
+    const int A = (int)active.size();
+    d.A = A;
+    for (int a = 0; a < A; ++a) {
+      const host::StackShift& t = st[active[a]].tmp;
+      for (int f = 0; f < N; ++f) {
+        // CAlignedSum / CAlignStack apply GetShift(f, -1): the negated shift
+        hsh[(size_t)a * N + f].x = t.x(f) * -1.0f;
+        hsh[(size_t)a * N + f].y = t.y(f) * -1.0f;
+      }
+    }
+    MC3_CUDA(cudaMemcpyAsync(d_act.p, active.data(), sizeof(int) * A, cudaMemcpyHostToDevice, stream));
+    MC3_CUDA(cudaMemcpyAsync(d_sh.p, hsh.data(), sizeof(float2) * (size_t)A * N, cudaMemcpyHostToDevice, stream));
+    MC3_TRY(phase_tables(d_sh.as<float2>(), A * N, cmpX, cmpY, d_ex.as<float2>(), d_ey.as<float2>(), false, stream));
+    MC3_TRY(aligned_sum(spec, d_act.as<int>(), d_ex.as<float2>(), d_ey.as<float2>(), d_S.as<float2>(), d, stream));
+    const float bf = st[active[0]].bfactor;
+    MC3_TRY(corr_cols(spec, d_act.as<int>(), d_ex.as<float2>(), d_ey.as<float2>(), d_S.as<float2>(),
+                      d_gstart.as<int>(), d_gsize.as<int>(), bf, prm.phase_only, d_T.as<float2>(), d, stream));
+    MC3_TRY(corr_rows(d_T.as<float2>(), d_win.as<float>(), d, stream));
+    MC3_TRY(peak_search(d_win.as<float>(), d_gsh.as<float2>(), d, stream));
+    MC3_CUDA(cudaMemcpyAsync(hg.data(), d_gsh.p, sizeof(float2) * (size_t)A * G, cudaMemcpyDeviceToHost, stream));
+    MC3_CUDA(cudaStreamSynchronize(stream));
+    std::vector<int> next;
+    for (int a = 0; a < A; ++a) {
+      host::IterState& s = st[active[a]];
+      const bool fin = s.step(reinterpret_cast<const float*>(&hg[(size_t)a * G]), grp, it, prm.iter, tol);
+      if (!fin) next.push_back(active[a]);
+    }
+    active.swap(next);
+  }
+  shifts.resize(nstack);
+  iters.resize(nstack);
+  errors.resize(nstack);
+  for (int s = 0; s < nstack; ++s) {
+    shifts[s] = st[s].finish(grp, N);
+    iters[s] = st[s].iterations;
+    errors[s] = st[s].errors;
+  }
+  return kOk;
+}
+
+// ---------------------------------------------------------------------------
+int Engine::global_sums(const float2* spec, int N, const host::StackShift& fs, const Geometry& g) {
+  MC3_TRY(d_sh.ensure(sizeof(float2) * (size_t)N));
+  MC3_TRY(d_fex.ensure(sizeof(float2) * (size_t)N * g.cmpX));
+  MC3_TRY(d_fey.ensure(sizeof(float2) * (size_t)N * g.cmpY));
+  std::vector<float2> hsh(N);
+  for (int f = 0; f < N; ++f) {
+    hsh[f].x = fs.x(f) * -1.0f;
+    hsh[f].y = fs.y(f) * -1.0f;
+  }
+  MC3_CUDA(cudaMemcpyAsync(d_sh.p, hsh.data(), sizeof(float2) * N, cudaMemcpyHostToDevice, stream));
+  // in-place GPhaseShift2D::DoIt skips |s| < 0.1 px (Util/GPhaseShift2D.cu:68-79)
+  MC3_TRY(phase_tables(d_sh.as<float2>(), N, g.cmpX, g.cmpY, d_fex.as<float2>(), d_fey.as<float2>(), true, stream));
+  return kOk;
+}
+
+// ---------------------------------------------------------------------------
+int Engine::process(const mc3_movie& mv, mc3_result* out) {
+  MC3_CUDA(cudaSetDevice(device));
+  if (prm.align == 0) return kEUnsupported;
+  if (prm.ft_bin != 1.0f) return kEUnsupported;
+  if (!mv.frames) return kEInval;
+  int bpp = 0;
+  switch (mv.mode) {
+    case 0: bpp = 1; break;
+    case 1: case 6: bpp = 2; break;
+    case 2: bpp = 4; break;
+    default: return kEUnsupported;
+  }
+  Geometry g;
+  MC3_TRY(g.compute(mv.nx, mv.ny, mv.nz, prm));
+  if (has_gain && (gain_w != g.W || gain_h != g.H)) return kEInval;  // CProcessThread::mCheckGain
+  const int W = g.W, H = g.H, N = g.N;
+  const size_t npx = (size_t)W * H;
+  const size_t ncmp = (size_t)g.cmpX * g.cmpY;
+  const size_t nxcf = (size_t)g.xcfCmpX * g.xcfCmpY;
+  cudaStream_t st = stream;
+
+  MC3_CUDA(cudaEventRecord(ev0, st));
+  // ---- 1. raw frames on the device ----
+  const void* raw = mv.frames;
+  if (!mv.on_device) {
+    MC3_TRY(d_raw.ensure((size_t)bpp * npx * N));
+    MC3_CUDA(cudaMemcpyAsync(d_raw.p, mv.frames, (size_t)bpp * npx * N, cudaMemcpyHostToDevice, st));
+    raw = d_raw.p;
+  }
+  // ---- 2. gain + frame sum (MrcUtil/CApplyRefs.cpp:36-212, CSumFFTStack) ----
+  MC3_TRY(d_frames.ensure(sizeof(float2) * ncmp * N));
+  MC3_TRY(d_sum.ensure(sizeof(float) * (size_t)g.padX * H));
+  float* frames = d_frames.as<float>();
+  const long fr_stride_f = (long)g.padX * H;
+  MC3_TRY(gain_and_sum(raw, mv.mode, (long)npx, has_gain ? d_gain.as<float>() : nullptr, frames,
+                       fr_stride_f, prm.correct_bad ? d_sum.as<float>() : nullptr, W, H, N, st));
+  // ---- 3. hot pixels and defects (BadPixel/CDetectMain.cpp, CCorrectMain.cpp) ----
+  if (prm.correct_bad) {
+    MC3_TRY(d_cc.ensure(sizeof(float) * (size_t)g.padX * H));
+    MC3_TRY(d_bad.ensure(npx));
+    MC3_TRY(d_part.ensure(sizeof(float) * 1024));
+    MC3_TRY(d_mom.ensure(sizeof(float) * 16));
+    float tpl[36];
+    host::defect_template(6, tpl);
+    MC3_TRY(detect_bad_pixels(d_sum.as<float>(), W, H, d_cc.as<float>(), d_part.as<float>(),
+                              d_mom.as<float>(), d_bad.as<uint8_t>(), tpl, 6, st));
+    MC3_TRY(correct_bad_pixels(frames, fr_stride_f, N, d_bad.as<uint8_t>(), W, H, st));
+  }
+  // ---- 4. forward FFT, normalised, + xcf crop (CTransformStack, CGenXcfStack) ----
+  MC3_TRY(d_xcf.ensure(sizeof(float2) * nxcf * N));
+  float2* spec = d_frames.as<float2>();
+  {
+    Batch b{N, N, fr_stride_f, nullptr, (long)ncmp};
+    MC3_TRY(row_r2c(frames, g.padX, spec, g.cmpX, W, H, b, 1.0f, st));
+    Batch bc{N, N, (long)ncmp, nullptr, (long)ncmp};
+    ColOps ops{};
+    ops.dir = -1;
+    ops.scale = (float)(1.0 / W / H);
+    ops.crop = d_xcf.as<float2>();
+    ops.crop_x = g.xcfCmpX;
+    ops.crop_y = g.xcfCmpY;
+    MC3_TRY(col_fft(spec, spec, g.cmpX, g.cmpX, H, bc, ops, st));
+  }
+  // ---- 5. full-frame alignment (Align/CFullAlign.cpp:127-164) ----
+  const float bin = fmaxf(g.xcfBin[0], g.xcfBin[1]);
+  const float tol = prm.tol / bin;
+  host::FrameGroups G0, G1;
+  G0.setup(N, prm.group[0]);
+  std::vector<host::StackShift> xs;
+  std::vector<int> it0;
+  std::vector<std::vector<float>> err0;
+  MC3_TRY(align_stacks(d_xcf.as<float2>(), (long)nxcf * N, 1, g.xcfCmpX, g.xcfCmpY, N, G0,
+                       prm.bft[0], tol, xs, it0, err0));
+  host::StackShift xsh = xs[0];  // xcf pixels
+
+  std::vector<float> patShift, patCent;
+  std::vector<unsigned char> patBad;
+  std::vector<int> patIters;
+  std::vector<std::vector<float>> patErr;
+  if (g.patch) {
+    const int xcfX = (g.xcfCmpX - 1) * 2, xcfY = g.xcfCmpY;
+    // ---- 6a. features on the aligned xcf sum (Align/CDetectFeatures.cpp:58-181) ----
+    {
+      MC3_TRY(d_sh.ensure(sizeof(float2) * N));
+      MC3_TRY(d_ex.ensure(sizeof(float2) * (size_t)N * g.xcfCmpX));
+      MC3_TRY(d_ey.ensure(sizeof(float2) * (size_t)N * g.xcfCmpY));
+      MC3_TRY(d_S.ensure(sizeof(float2) * nxcf));
+      MC3_TRY(d_act.ensure(sizeof(int)));
+      std::vector<float2> hsh(N);
+      for (int f = 0; f < N; ++f) {
+        hsh[f].x = xsh.x(f) * -1.0f;
+        hsh[f].y = xsh.y(f) * -1.0f;
+      }
+      int zero = 0;
+      MC3_CUDA(cudaMemcpyAsync(d_act.p, &zero, sizeof(int), cudaMemcpyHostToDevice, st));
+      MC3_CUDA(cudaMemcpyAsync(d_sh.p, hsh.data(), sizeof(float2) * N, cudaMemcpyHostToDevice, st));
+      MC3_TRY(phase_tables(d_sh.as<float2>(), N, g.xcfCmpX, g.xcfCmpY, d_ex.as<float2>(), d_ey.as<float2>(), false, st));
+      AlignDims d{};
+      d.cmpX = g.xcfCmpX;
+      d.cmpY = g.xcfCmpY;
+      d.N = N;
+      d.stack_stride = (long)nxcf * N;
+      d.A = 1;
+      MC3_TRY(aligned_sum(d_xcf.as<float2>(), d_act.as<int>(), d_ex.as<float2>(), d_ey.as<float2>(), d_S.as<float2>(), d, st));
+      const int bx = 128, by = 128, bcx = bx / 2 + 1;
+      MC3_TRY(d_bsum.ensure(sizeof(float2) * bcx * by));
+      MC3_TRY(d_btmp.ensure(sizeof(float2) * bcx * by));
+      MC3_TRY(d_bmap.ensure(sizeof(float) * bx * by));
+      MC3_TRY(d_scal.ensure(sizeof(float) * 8));
+      MC3_TRY(d_part.ensure(sizeof(float) * 1024));
+      MC3_TRY(fourier_crop(d_S.as<float2>(), g.xcfCmpX, g.xcfCmpY, d_bsum.as<float2>(), bcx, by, st));
+      Batch b1{1, 1, 0, nullptr, 0};
+      ColOps ops{};
+      ops.dir = 1;
+      ops.scale = 1.0f;
+      MC3_TRY(col_fft(d_bsum.as<float2>(), d_bsum.as<float2>(), bcx, bcx, by, b1, ops, st));
+      MC3_TRY(row_c2r(d_bsum.as<float2>(), bcx, d_bsum.as<float>(), 2 * bcx, bx, by, b1, st));
+      MC3_TRY(feature_map(d_bsum.as<float>(), bx, by, d_btmp.as<float>(), d_part.as<float>(), d_scal.as<float>(), d_bmap.as<float>(), st));
+      std::vector<float> map((size_t)bx * by);
+      float scal[3];
+      MC3_CUDA(cudaMemcpyAsync(map.data(), d_bmap.p, sizeof(float) * bx * by, cudaMemcpyDeviceToHost, st));
+      MC3_CUDA(cudaMemcpyAsync(scal, d_scal.p, sizeof(float) * 3, cudaMemcpyDeviceToHost, st));
+      MC3_CUDA(cudaStreamSynchronize(st));
+      std::vector<int> starts;
+      host::patch_starts(map.data(), bx, by, scal[1], scal[2], g.Px, g.Py, xcfX, xcfY,
+                         g.patSizeX, g.patSizeY, starts);
+      // ---- 6b. xcf frames to real space (Correct/CGenRealStack.cpp) ----
+      MC3_TRY(phase_tables(d_sh.as<float2>(), N, g.xcfCmpX, g.xcfCmpY, d_ex.as<float2>(), d_ey.as<float2>(), true, st));
+      Batch bn{N, N, (long)nxcf, nullptr, (long)nxcf};
+      ColOps inv{};
+      inv.dir = 1;
+      inv.scale = 1.0f;
+      inv.ex = d_ex.as<float2>();
+      inv.ey = d_ey.as<float2>();
+      MC3_TRY(col_fft(d_xcf.as<float2>(), d_xcf.as<float2>(), g.xcfCmpX, g.xcfCmpX, xcfY, bn, inv, st));
+      Batch br{N, N, (long)nxcf, nullptr, (long)nxcf * 2};
+      MC3_TRY(row_c2r(d_xcf.as<float2>(), g.xcfCmpX, d_xcf.as<float>(), 2 * g.xcfCmpX, xcfX, xcfY, br, st));
+      // ---- 6c. patch extraction + unnormalised R2C (CExtractPatch, CTransformStack) ----
+      const int P = g.P;
+      const size_t npat = (size_t)g.patCmpX * g.patCmpY;
+      MC3_TRY(d_pat.ensure(sizeof(float2) * npat * N * P));
+      MC3_TRY(d_patoff.ensure(sizeof(long) * P));
+      std::vector<long> off(P);
+      for (int p = 0; p < P; ++p) off[p] = (long)starts[2 * p + 1] * (2 * g.xcfCmpX) + starts[2 * p];
+      MC3_CUDA(cudaMemcpyAsync(d_patoff.p, off.data(), sizeof(long) * P, cudaMemcpyHostToDevice, st));
+      const int pw = (g.patCmpX - 1) * 2, ph = g.patCmpY;
+      Batch bp{P * N, N, (long)nxcf * 2, d_patoff.as<long>(), (long)npat};
+      MC3_TRY(row_r2c(d_xcf.as<float>(), 2 * g.xcfCmpX, d_pat.as<float2>(), g.patCmpX, pw, ph, bp, 1.0f, st));
+      Batch bpc{P * N, P * N, (long)npat, nullptr, (long)npat};
+      ColOps fwd{};
+      fwd.dir = -1;
+      fwd.scale = 1.0f;
+      MC3_TRY(col_fft(d_pat.as<float2>(), d_pat.as<float2>(), g.patCmpX, g.patCmpX, ph, bpc, fwd, st));
+      // ---- 6d. all patch stacks aligned together (Align/CMeasurePatches.cpp:22-84) ----
+      G1.setup(N, prm.group[1]);
+      std::vector<host::StackShift> ps;
+      MC3_TRY(align_stacks(d_pat.as<float2>(), (long)npat * N, P, g.patCmpX, g.patCmpY, N, G1,
+                           prm.bft[1], tol, ps, patIters, patErr));
+      patShift.assign((size_t)N * P * 2, 0.0f);
+      patCent.assign((size_t)P * 2, 0.0f);
+      for (int p = 0; p < P; ++p) {
+        const int cx = starts[2 * p] + g.patSizeX / 2, cy = starts[2 * p + 1] + g.patSizeY / 2;
+        patCent[2 * p] = cx * g.xcfBin[0];
+        patCent[2 * p + 1] = cy * g.xcfBin[1];
+        host::StackShift s = ps[p];
+        s.multiply(g.xcfBin[0], g.xcfBin[1]);
+        for (int f = 0; f < N; ++f) {
+          patShift[((size_t)f * P + p) * 2] = s.x(f);
+          patShift[((size_t)f * P + p) * 2 + 1] = s.y(f);
+        }
+      }
+      host::patch_make_relative(patShift, N, P);
+      patBad.assign((size_t)N * P, 0);
+      host::patch_detect_bads(patShift.data(), patCent.data(), N, P, W, H, patBad.data());
+    }
+  }
+  // full-frame pixels + 0.01 px truncation (CFullAlign.cpp:96, 163)
+  host::StackShift fs = xsh;
+  fs.multiply(g.xcfBin[0], g.xcfBin[1]);
+  fs.truncate_decimal();
+  if (g.patch) {
+    // CPatchAlign::mCorrectFullShift (Align/CPatchAlign.cpp:47-65)
+    int ref = N / 2;
+    if (prm.fm_ref >= 0) {
+      ref = prm.fm_ref - 1;
+      if (ref < 0) ref = 0;
+      else if (ref >= N) ref = N - 1;
+    }
+    fs.make_relative(ref);
+  }
+
+  // ---- 7. correction + sums ----
+  MC3_TRY(d_sums.ensure(sizeof(float2) * ncmp * g.nSums));
+  MC3_TRY(d_acc.ensure(sizeof(float) * N));
+  MC3_TRY(d_Wn.ensure(sizeof(float) * ncmp));
+  std::vector<float> acc(N);
+  for (int i = 0; i < N; ++i) acc[i] = prm.fm_dose * (i + 1);  // CFmIntParam::mSetup
+  MC3_CUDA(cudaMemcpyAsync(d_acc.p, acc.data(), sizeof(float) * N, cudaMemcpyHostToDevice, st));
+  DoseParams dp{};
+  dp.enabled = g.dw ? 1 : 0;
+  dp.dws = g.dws ? 1 : 0;
+  dp.pix_size = prm.pix_size;
+  dp.kv_factor = host::kv_factor(prm.kv);
+  dp.sum_range[0] = prm.sum_range[0];
+  dp.sum_range[1] = prm.sum_range[1];
+  if (g.dw) MC3_TRY(dose_norm(d_acc.as<float>(), N, g.cmpX, g.cmpY, dp.pix_size, dp.kv_factor, d_Wn.as<float>(), st));
+  MC3_TRY(global_sums(spec, N, fs, g));
+  if (!g.patch) {
+    MC3_TRY(frame_sums(spec, (long)ncmp, N, g.cmpX, g.cmpY, d_fex.as<float2>(), d_fey.as<float2>(),
+                       d_acc.as<float>(), d_Wn.as<float>(), dp, d_sums.as<float2>(), g.nSums, st));
+  } else {
+    // Correct/GCorrectPatchShift.cu:97-285: per frame C2R -> gather -> R2C
+    const int P = g.P;
+    MC3_TRY(d_pcent.ensure(sizeof(float) * 2 * P));
+    MC3_TRY(d_pshift.ensure(sizeof(float) * 2 * (size_t)P * N));
+    MC3_TRY(d_pbad.ensure((size_t)P * N));
+    MC3_CUDA(cudaMemcpyAsync(d_pcent.p, patCent.data(), sizeof(float) * 2 * P, cudaMemcpyHostToDevice, st));
+    MC3_CUDA(cudaMemcpyAsync(d_pshift.p, patShift.data(), sizeof(float) * 2 * (size_t)P * N, cudaMemcpyHostToDevice, st));
+    MC3_CUDA(cudaMemcpyAsync(d_pbad.p, patBad.data(), (size_t)P * N, cudaMemcpyHostToDevice, st));
+    const int B = std::min(N, 16);
+    MC3_TRY(d_real.ensure(sizeof(float2) * ncmp * B));
+    MC3_TRY(d_gath.ensure(sizeof(float2) * ncmp * B));
+    for (int f0 = 0; f0 < N; f0 += B) {
+      const int nb = std::min(B, N - f0);
+      Batch bi{nb, nb, (long)ncmp, nullptr, (long)ncmp};
+      ColOps inv{};
+      inv.dir = 1;
+      inv.scale = 1.0f;
+      inv.ex = d_fex.as<float2>() + (size_t)f0 * g.cmpX;
+      inv.ey = d_fey.as<float2>() + (size_t)f0 * g.cmpY;
+      MC3_TRY(col_fft(spec + (size_t)f0 * ncmp, d_real.as<float2>(), g.cmpX, g.cmpX, H, bi, inv, st));
+      Batch br{nb, nb, (long)ncmp, nullptr, (long)ncmp * 2};
+      MC3_TRY(row_c2r(d_real.as<float2>(), g.cmpX, d_real.as<float>(), g.padX, W, H, br, st));
+      MC3_TRY(local_gather(d_real.as<float>(), (long)ncmp * 2, d_gath.as<float>(), (long)ncmp * 2, nb, W, H,
+                           d_pcent.as<float>(), d_pshift.as<float2>() + (size_t)f0 * P,
+                           d_pbad.as<uint8_t>() + (size_t)f0 * P, P, st));
+      Batch bf{nb, nb, (long)ncmp * 2, nullptr, (long)ncmp};
+      MC3_TRY(row_r2c(d_gath.as<float>(), g.padX, spec + (size_t)f0 * ncmp, g.cmpX, W, H, bf, 1.0f, st));
+      ColOps fwd{};
+      fwd.dir = -1;
+      fwd.scale = (float)(1.0 / W / H);
+      MC3_TRY(col_fft(spec + (size_t)f0 * ncmp, spec + (size_t)f0 * ncmp, g.cmpX, g.cmpX, H, bi, fwd, st));
+    }
+    MC3_TRY(frame_sums(spec, (long)ncmp, N, g.cmpX, g.cmpY, nullptr, nullptr, d_acc.as<float>(),
+                       d_Wn.as<float>(), dp, d_sums.as<float2>(), g.nSums, st));
+  }
+  // ---- 8. sums to real space (CCorrectFullShift::mUnpadSums) ----
+  {
+    Batch bs{g.nSums, g.nSums, (long)ncmp, nullptr, (long)ncmp};
+    ColOps inv{};
+    inv.dir = 1;
+    inv.scale = 1.0f;
+    MC3_TRY(col_fft(d_sums.as<float2>(), d_sums.as<float2>(), g.cmpX, g.cmpX, H, bs, inv, st));
+    Batch br{g.nSums, g.nSums, (long)ncmp, nullptr, (long)ncmp * 2};
+    MC3_TRY(row_c2r(d_sums.as<float2>(), g.cmpX, d_sums.as<float>(), g.padX, W, H, br, st));
+    float* dst = nullptr;
+    if (out && out->sums && out->sums_on_device) {
+      dst = out->sums;
+    } else {
+      MC3_TRY(d_out.ensure(sizeof(float) * npx * g.nSums));
+      dst = d_out.as<float>();
+    }
+    MC3_TRY(unpad_positive(d_sums.as<float>(), g.padX, dst, W, H, g.nSums, (long)ncmp * 2, st));
+    if (out && out->sums && !out->sums_on_device)
+      MC3_CUDA(cudaMemcpyAsync(out->sums, dst, sizeof(float) * npx * g.nSums, cudaMemcpyDeviceToHost, st));
+  }
+  MC3_CUDA(cudaEventRecord(ev1, st));
+  MC3_CUDA(cudaStreamSynchronize(st));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ev0, ev1);
+  // ---- 9. result tables ----
+  if (out) {
+    out->n_sums = g.nSums;
+    out->n_patches = g.P;
+    out->time_ms = ms;
+    if (out->global_shifts)
+      for (int f = 0; f < N; ++f) {
+        out->global_shifts[2 * f] = fs.x(f);
+        out->global_shifts[2 * f + 1] = fs.y(f);
+      }
+    if (g.patch) {
+      if (out->patch_shifts) std::memcpy(out->patch_shifts, patShift.data(), sizeof(float) * patShift.size());
+      if (out->patch_centers) std::memcpy(out->patch_centers, patCent.data(), sizeof(float) * patCent.size());
+      if (out->patch_bad) std::memcpy(out->patch_bad, patBad.data(), patBad.size());
+    }
+    if (out->iterations) {
+      out->iterations[0] = it0[0];
+      for (int p = 0; p < g.P; ++p) out->iterations[1 + p] = patIters[p];
+    }
+    if (out->errors) {
+      const int I = prm.iter;
+      for (int s = 0; s < 1 + g.P; ++s) {
+        const std::vector<float>& e = s == 0 ? err0[0] : patErr[s - 1];
+        for (int i = 0; i < I; ++i) out->errors[(size_t)s * I + i] = i < (int)e.size() ? e[i] * bin : 0.0f;
+      }
+    }
+  }
+  return kOk;
+}
+
+}  // namespace mc3

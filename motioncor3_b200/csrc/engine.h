@@ -1,0 +1,76 @@
+// The per-context processing engine behind the C ABI: owns device buffers
+// sized for the current movie geometry and runs the whole path on one
+// stream.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/mc3.h"
+#include "host_align.h"
+#include "kernels.cuh"
+
+namespace mc3 {
+
+// Grows-only device allocation reused across movies.
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  int ensure(size_t bytes);
+  void release();
+  template <typename T>
+  T* as() const { return reinterpret_cast<T*>(p); }
+  ~DevBuf() { release(); }
+};
+
+// Buffer geometry of one movie (CBufferPool.cpp:185-270).
+struct Geometry {
+  int W = 0, H = 0, N = 0;
+  int cmpX = 0, cmpY = 0, padX = 0;
+  int xcfCmpX = 0, xcfCmpY = 0;
+  float xcfBin[2] = {1.f, 1.f};
+  bool patch = false;
+  int Px = 0, Py = 0, P = 0;
+  int patCmpX = 0, patCmpY = 0;
+  int patSizeX = 0, patSizeY = 0;
+  bool dw = false, dws = false;
+  int nSums = 1;
+  int compute(int w, int h, int n, const mc3_params& p);
+};
+
+class Engine {
+ public:
+  explicit Engine(const mc3_params& p);
+  ~Engine();
+  int init();
+  int set_stream(cudaStream_t s);
+  int set_gain(const float* gain, int w, int h, bool on_device);
+  int plan(int w, int h, int n, mc3_plan_info* info);
+  int process(const mc3_movie& mv, mc3_result* out);
+
+  // Batched CIterativeAlign over `nstack` stacks of N spectra each.
+  int align_stacks(const float2* spec, long stack_stride, int nstack, int cmpX, int cmpY, int N,
+                   const host::FrameGroups& grp, float bf0, float tol,
+                   std::vector<host::StackShift>& shifts, std::vector<int>& iters,
+                   std::vector<std::vector<float>>& errors);
+  // Sums of spectra shifted by -shifts (global correction) into d_sums_.
+  int global_sums(const float2* spec, int N, const host::StackShift& fs, const Geometry& g);
+
+  mc3_params prm;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaStream_t own_stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string last_error;
+
+  // device buffers
+  DevBuf d_gain, d_raw, d_frames, d_sum, d_cc, d_bad, d_part, d_mom;
+  DevBuf d_xcf, d_sh, d_ex, d_ey, d_S, d_T, d_win, d_gsh, d_act, d_gstart, d_gsize;
+  DevBuf d_pat, d_patoff, d_bsum, d_bimg, d_btmp, d_bmap, d_scal;
+  DevBuf d_fex, d_fey, d_Wn, d_acc, d_sums, d_real, d_gath, d_pcent, d_pshift, d_pbad, d_out;
+  bool has_gain = false;
+  int gain_w = 0, gain_h = 0;
+};
+
+}  // namespace mc3

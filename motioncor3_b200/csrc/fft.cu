@@ -1,0 +1,225 @@
+// Shared-memory 2D FFT passes (see fft.cuh).
+#include <cmath>
+#include <map>
+#include <mutex>
+#include <vector>
+
+#include "fft.cuh"
+
+namespace mc3 {
+
+namespace {
+std::mutex g_tw_mu;
+std::map<std::pair<int, int>, float2*> g_tw;  // (device, n) -> table
+constexpr int kSmemBudget = 100 * 1024;
+}  // namespace
+
+const float2* twiddles(int n) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_tw_mu);
+  auto key = std::make_pair(dev, n);
+  auto it = g_tw.find(key);
+  if (it != g_tw.end()) return it->second;
+  std::vector<float2> h(n);
+  for (int k = 0; k < n; ++k) {
+    const double a = -2.0 * M_PI * (double)k / (double)n;
+    h[k].x = (float)std::cos(a);
+    h[k].y = (float)std::sin(a);
+  }
+  float2* d = nullptr;
+  if (cudaMalloc(&d, sizeof(float2) * n) != cudaSuccess) return nullptr;
+  if (cudaMemcpy(d, h.data(), sizeof(float2) * n, cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(d);
+    return nullptr;
+  }
+  g_tw[key] = d;
+  return d;
+}
+
+int make_desc(int n, int table_n, FftDesc* d) {
+  d->n = n;
+  d->nstages = fft_factorize(n, d->radix);
+  if (d->nstages < 0 || table_n % n) return kEInval;
+  d->tw = twiddles(table_n);
+  if (!d->tw) return kENoMem;
+  d->tws = table_n / n;
+  return kOk;
+}
+
+__device__ __forceinline__ long batch_in_off(const Batch& b, int item) {
+  long off = (long)(item % b.nf) * b.in_stride;
+  if (b.patch_off) off += b.patch_off[item / b.nf];
+  return off;
+}
+
+// ---------------------------------------------------------------------
+// Row real FFT (R2C): each CTA transforms `rows` rows of one batch item.
+// ---------------------------------------------------------------------
+__global__ void k_row_r2c(const float* __restrict__ in, long in_pitch, float2* out, long out_pitch,
+                          int W, int H, int rows, Batch bt, FftDesc dM, float scale) {
+  extern __shared__ float2 sm[];
+  const int M = W / 2;
+  const int ld = M + 1;
+  float2* A = sm;
+  float2* B = sm + rows * ld;
+  const int item = blockIdx.y;
+  const int r0 = blockIdx.x * rows;
+  const int nr = min(rows, H - r0);
+  const float* src = in + batch_in_off(bt, item) + (long)r0 * in_pitch;
+  for (int t = threadIdx.x; t < nr * M; t += blockDim.x) {
+    const int r = t / M, m = t - r * M;
+    const float* p = src + (long)r * in_pitch + 2 * m;
+    A[r * ld + m] = c2(p[0], p[1]);
+  }
+  __syncthreads();
+  float2* R = cta_fft<-1>(A, B, dM, nr, 1, ld);
+  float2* dst = out + (long)item * bt.out_stride + (long)r0 * out_pitch;
+  for (int t = threadIdx.x; t < nr * (M + 1); t += blockDim.x) {
+    const int r = t / (M + 1), k = t - r * (M + 1);
+    float2 v = r2c_post(R + r * ld, M, k, dM.tw, 1);
+    dst[(long)r * out_pitch + k] = cscale(v, scale);
+  }
+}
+
+// ---------------------------------------------------------------------
+// Row real inverse (C2R), unnormalised.
+// ---------------------------------------------------------------------
+__global__ void k_row_c2r(const float2* in, long in_pitch, float* out, long out_pitch, int W,
+                          int H, int rows, Batch bt, FftDesc dM) {
+  extern __shared__ float2 sm[];
+  const int M = W / 2;
+  const int ld = M + 1;
+  float2* A = sm;
+  float2* B = sm + rows * ld;
+  const int item = blockIdx.y;
+  const int r0 = blockIdx.x * rows;
+  const int nr = min(rows, H - r0);
+  const float2* src = in + batch_in_off(bt, item) + (long)r0 * in_pitch;
+  for (int t = threadIdx.x; t < nr * (M + 1); t += blockDim.x) {
+    const int r = t / (M + 1), k = t - r * (M + 1);
+    B[r * ld + k] = src[(long)r * in_pitch + k];
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < nr * M; t += blockDim.x) {
+    const int r = t / M, k = t - r * M;
+    A[r * ld + k] = c2r_pre(B + r * ld, M, k, dM.tw, 1);
+  }
+  __syncthreads();
+  float2* R = cta_fft<1>(A, B, dM, nr, 1, ld);
+  float* dst = out + (long)item * bt.out_stride + (long)r0 * out_pitch;
+  for (int t = threadIdx.x; t < nr * M; t += blockDim.x) {
+    const int r = t / M, m = t - r * M;
+    const float2 v = R[r * ld + m];
+    float* p = dst + (long)r * out_pitch + 2 * m;
+    p[0] = v.x;
+    p[1] = v.y;
+  }
+}
+
+// ---------------------------------------------------------------------
+// Column complex FFT with optional phase-shift prologue and crop epilogue.
+// ---------------------------------------------------------------------
+__global__ void k_col_fft(const float2* in, float2* out, long pitch, int cmpX, int H, int TX,
+                          Batch bt, FftDesc dH, ColOps ops) {
+  extern __shared__ float2 sm[];
+  const int ld = H + 1;
+  float2* A = sm;
+  float2* B = sm + TX * ld;
+  const int item = blockIdx.y;
+  const int x0 = blockIdx.x * TX;
+  const float2* src = in + batch_in_off(bt, item);
+  const float2* ex = ops.ex ? ops.ex + (long)item * cmpX : nullptr;
+  const float2* ey = ops.ey ? ops.ey + (long)item * H : nullptr;
+  for (int t = threadIdx.x; t < TX * H; t += blockDim.x) {
+    const int y = t / TX, c = t - y * TX;
+    const int x = x0 + c;
+    float2 v = c2(0.f, 0.f);
+    if (x < cmpX) {
+      v = src[(long)y * pitch + x];
+      if (ex) v = cmul(v, cmul(ex[x], ey[y]));
+    }
+    A[c * ld + y] = v;
+  }
+  __syncthreads();
+  float2* R = ops.dir < 0 ? cta_fft<-1>(A, B, dH, TX, 1, ld) : cta_fft<1>(A, B, dH, TX, 1, ld);
+  float2* dst = out + (long)item * bt.out_stride;
+  float2* crop = ops.crop ? ops.crop + (long)item * ops.crop_x * ops.crop_y : nullptr;
+  for (int t = threadIdx.x; t < TX * H; t += blockDim.x) {
+    const int y = t / TX, c = t - y * TX;
+    const int x = x0 + c;
+    if (x >= cmpX) continue;
+    const float2 v = cscale(R[c * ld + y], ops.scale);
+    dst[(long)y * pitch + x] = v;
+    if (crop && x < ops.crop_x) {
+      // GFourierResize2D::mGResize row mapping (Util/GFourierResize2D.cu:7-37)
+      int yo = -1;
+      if (y <= ops.crop_y / 2) yo = y;
+      else if (y > H - ops.crop_y / 2) yo = y - H + ops.crop_y;
+      if (yo >= 0) crop[(long)yo * ops.crop_x + x] = v;
+    }
+  }
+}
+
+int row_tile(int M) {
+  int rows = kSmemBudget / (2 * (M + 1) * (int)sizeof(float2));
+  if (rows < 1) rows = 1;
+  if (rows > 16) rows = 16;
+  return rows;
+}
+int col_tile(int H) {
+  int tx = kSmemBudget / (2 * (H + 1) * (int)sizeof(float2));
+  int p = 1;
+  while (p * 2 <= tx && p < 16) p *= 2;
+  return p;
+}
+
+int row_r2c(const float* in, long in_pitch, float2* out, long out_pitch, int W, int H,
+            const Batch& b, float scale, cudaStream_t st) {
+  if (W < 2 || (W & 1) || H < 1 || b.items < 1) return kEInval;
+  const int M = W / 2;
+  FftDesc d;
+  MC3_TRY(make_desc(M, W, &d));
+  const int rows = row_tile(M);
+  const size_t smem = 2 * (size_t)rows * (M + 1) * sizeof(float2);
+  if (smem > 200 * 1024) return kEUnsupported;
+  MC3_TRY(set_smem_attr(k_row_r2c, smem));
+  dim3 grid(ceil_div(H, rows), b.items);
+  k_row_r2c<<<grid, 256, smem, st>>>(in, in_pitch, out, out_pitch, W, H, rows, b, d, scale);
+  MC3_CHECK_LAUNCH("k_row_r2c");
+  return kOk;
+}
+
+int row_c2r(const float2* in, long in_pitch, float* out, long out_pitch, int W, int H,
+            const Batch& b, cudaStream_t st) {
+  if (W < 2 || (W & 1) || H < 1 || b.items < 1) return kEInval;
+  const int M = W / 2;
+  FftDesc d;
+  MC3_TRY(make_desc(M, W, &d));
+  const int rows = row_tile(M);
+  const size_t smem = 2 * (size_t)rows * (M + 1) * sizeof(float2);
+  if (smem > 200 * 1024) return kEUnsupported;
+  MC3_TRY(set_smem_attr(k_row_c2r, smem));
+  dim3 grid(ceil_div(H, rows), b.items);
+  k_row_c2r<<<grid, 256, smem, st>>>(in, in_pitch, out, out_pitch, W, H, rows, b, d);
+  MC3_CHECK_LAUNCH("k_row_c2r");
+  return kOk;
+}
+
+int col_fft(const float2* in, float2* out, long pitch, int cmpX, int H, const Batch& b,
+            const ColOps& ops, cudaStream_t st) {
+  if (cmpX < 1 || H < 1 || b.items < 1) return kEInval;
+  if (ops.crop && (ops.crop_x > cmpX || ops.crop_y > H)) return kEInval;
+  FftDesc d;
+  MC3_TRY(make_desc(H, H, &d));
+  const int tx = col_tile(H);
+  const size_t smem = 2 * (size_t)tx * (H + 1) * sizeof(float2);
+  if (smem > 200 * 1024) return kEUnsupported;
+  MC3_TRY(set_smem_attr(k_col_fft, smem));
+  dim3 grid(ceil_div(cmpX, tx), b.items);
+  k_col_fft<<<grid, 256, smem, st>>>(in, out, pitch, cmpX, H, tx, b, d, ops);
+  MC3_CHECK_LAUNCH("k_col_fft");
+  return kOk;
+}
+
+}  // namespace mc3

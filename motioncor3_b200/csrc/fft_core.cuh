@@ -1,0 +1,289 @@
+// Mixed-radix Stockham FFT core shared by every transform in libmc3.
+//
+// The reference delegates all transforms to cuFFT through Util::CCufft2D
+// (Util/CCufft2D.cpp:23-120: R2C forward with optional 1/(Nx*Ny) scaling,
+// unnormalised C2R inverse).  libmc3 does not link cuFFT: every 2D
+// transform is split into a row pass and a column pass that each run a
+// batch of 1D transforms inside one CTA's shared memory, using the
+// functions below.
+//
+// Algorithm: out-of-place Stockham auto-sort (no bit reversal), one stage
+// per factor of n.  For a stage of radix R with Ns = product of the
+// earlier radices, butterfly j (0 <= j < n/R) reads x[j + r*n/R],
+// multiplies input r by w_n^(r*(j%Ns)*n/(Ns*R)), applies a length-R DFT
+// and writes y[(j/Ns)*Ns*R + j%Ns + r*Ns].  Radices 2, 3, 4 and 8 have
+// dedicated butterflies; any other factor (5, 7, 11, 17, 41, ...) uses a
+// per-output direct DFT that reads its inputs from shared memory.
+//
+// Every index computation lives in __host__ __device__ functions so the
+// exact same code is exercised by a sequential host driver in the CPU
+// tests (fft_host_reference below) and by the CTA driver in the kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <vector_types.h>
+
+#ifndef MC3_HD
+#define MC3_HD __host__ __device__ __forceinline__
+#endif
+
+namespace mc3 {
+
+constexpr int kMaxStages = 24;
+
+MC3_HD float2 c2(float x, float y) { float2 r; r.x = x; r.y = y; return r; }
+MC3_HD float2 cadd(float2 a, float2 b) { return c2(a.x + b.x, a.y + b.y); }
+MC3_HD float2 csub(float2 a, float2 b) { return c2(a.x - b.x, a.y - b.y); }
+MC3_HD float2 cscale(float2 a, float s) { return c2(a.x * s, a.y * s); }
+MC3_HD float2 cconj(float2 a) { return c2(a.x, -a.y); }
+MC3_HD float2 cmul(float2 a, float2 b) {
+  return c2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// Multiply by -i for the forward direction (DIR = -1, kernel e^{-i...})
+// and by +i for the inverse direction (DIR = +1).
+template <int DIR>
+MC3_HD float2 crot(float2 a) {
+  return DIR < 0 ? c2(a.y, -a.x) : c2(-a.y, a.x);
+}
+// Twiddle lookup: table holds e^{-2 pi i k / n}; the inverse uses the
+// conjugate.
+template <int DIR>
+MC3_HD float2 twid(const float2* tw, int tws, int k) {
+  float2 w = tw[k * tws];
+  return DIR < 0 ? w : cconj(w);
+}
+
+// Description of one complex transform length.  `tw` points at a table of
+// e^{-2 pi i k / n} values sampled every `tws` entries (a length-2n table
+// with tws = 2 serves an n-point transform, which is how the real-data
+// transforms share one table).
+struct FftDesc {
+  int n;
+  int nstages;
+  int radix[kMaxStages];
+  const float2* tw;
+  int tws;
+};
+
+// Factor n into stage radices: as many 8s as possible, then 4, then 2,
+// then 3 (as 3), then the remaining primes in increasing order.
+// Returns the number of stages, or -1 if n < 1 or too many stages.
+inline int fft_factorize(int n, int* radix) {
+  if (n < 1) return -1;
+  int ns = 0;
+  int m = n;
+  int p2 = 0;
+  while (m % 2 == 0) { m /= 2; ++p2; }
+  while (p2 >= 3) { radix[ns++] = 8; p2 -= 3; }
+  if (p2 == 2) radix[ns++] = 4;
+  if (p2 == 1) radix[ns++] = 2;
+  for (int p = 3; m > 1; p += 2) {
+    while (m % p == 0) {
+      if (ns >= kMaxStages) return -1;
+      radix[ns++] = p;
+      m /= p;
+    }
+    if (p * p > m && m > 1) {
+      if (ns >= kMaxStages) return -1;
+      radix[ns++] = m;
+      m = 1;
+    }
+  }
+  return ns;
+}
+
+// ---- length-R DFT kernels on register arrays ---------------------------
+template <int R, int DIR>
+struct Dft;
+
+template <int DIR>
+struct Dft<2, DIR> {
+  MC3_HD static void run(float2* v) {
+    float2 a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  }
+};
+
+template <int DIR>
+struct Dft<4, DIR> {
+  MC3_HD static void run(float2* v) {
+    float2 a = cadd(v[0], v[2]);
+    float2 b = csub(v[0], v[2]);
+    float2 c = cadd(v[1], v[3]);
+    float2 d = crot<DIR>(csub(v[1], v[3]));
+    v[0] = cadd(a, c);
+    v[2] = csub(a, c);
+    v[1] = cadd(b, d);
+    v[3] = csub(b, d);
+  }
+};
+
+template <int DIR>
+struct Dft<3, DIR> {
+  MC3_HD static void run(float2* v) {
+    // e^{-2 pi i / 3} = -1/2 - i*sqrt(3)/2 (forward)
+    const float kS = 0.86602540378443864676f;
+    float2 t = cadd(v[1], v[2]);
+    float2 u = csub(v[1], v[2]);
+    float2 m = c2(v[0].x - 0.5f * t.x, v[0].y - 0.5f * t.y);
+    float2 r = crot<DIR>(cscale(u, kS));
+    v[0] = cadd(v[0], t);
+    v[1] = cadd(m, r);
+    v[2] = csub(m, r);
+  }
+};
+
+template <int DIR>
+struct Dft<8, DIR> {
+  MC3_HD static void run(float2* v) {
+    const float kH = 0.70710678118654752440f;
+    float2 e[4] = {v[0], v[2], v[4], v[6]};
+    float2 o[4] = {v[1], v[3], v[5], v[7]};
+    Dft<4, DIR>::run(e);
+    Dft<4, DIR>::run(o);
+    // o[k] *= w8^k ; w8 = e^{DIR * i pi / 4}
+    float2 o1 = o[1];
+    o[1] = DIR < 0 ? c2(kH * (o1.x + o1.y), kH * (o1.y - o1.x))
+                   : c2(kH * (o1.x - o1.y), kH * (o1.y + o1.x));
+    o[2] = crot<DIR>(o[2]);
+    float2 o3 = o[3];
+    o[3] = DIR < 0 ? c2(kH * (o3.y - o3.x), -kH * (o3.x + o3.y))
+                   : c2(-kH * (o3.x + o3.y), kH * (o3.x - o3.y));
+    for (int k = 0; k < 4; ++k) {
+      v[k] = cadd(e[k], o[k]);
+      v[k + 4] = csub(e[k], o[k]);
+    }
+  }
+};
+
+// One butterfly of a dedicated-radix stage.  A/B: sequence base pointers,
+// es: element stride.
+template <int R, int DIR>
+MC3_HD void stage_bfly(const float2* A, float2* B, int n, int Ns, int j,
+                       const float2* tw, int tws, int es) {
+  const int nR = n / R;
+  const int k = j % Ns;
+  float2 v[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) v[r] = A[(j + r * nR) * es];
+  if (Ns > 1) {
+    const int step = (n / (Ns * R)) * k;
+#pragma unroll
+    for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twid<DIR>(tw, tws, step * r));
+  }
+  Dft<R, DIR>::run(v);
+  const int idxD = (j / Ns) * Ns * R + k;
+#pragma unroll
+  for (int r = 0; r < R; ++r) B[(idxD + r * Ns) * es] = v[r];
+}
+
+// One output of a direct-DFT stage (any radix R dividing n).
+// o in [0, n): j = o / R, q = o % R.
+template <int DIR>
+MC3_HD void stage_direct(const float2* A, float2* B, int n, int R, int Ns, int o,
+                         const float2* tw, int tws, int es) {
+  const int nR = n / R;
+  const int j = o / R;
+  const int q = o - j * R;
+  const int k = j % Ns;
+  const int step = (n / (Ns * R)) * k;
+  float2 acc = c2(0.f, 0.f);
+  for (int r = 0; r < R; ++r) {
+    float2 x = A[(j + r * nR) * es];
+    if (Ns > 1 && r > 0) x = cmul(x, twid<DIR>(tw, tws, step * r));
+    const int m = (r * q) % R;
+    if (m) x = cmul(x, twid<DIR>(tw, tws, m * nR));
+    acc = cadd(acc, x);
+  }
+  const int idxD = (j / Ns) * Ns * R + k;
+  B[(idxD + q * Ns) * es] = acc;
+}
+
+MC3_HD bool radix_is_dedicated(int R) { return R == 2 || R == 3 || R == 4 || R == 8; }
+
+template <int DIR>
+MC3_HD void stage_item(const float2* A, float2* B, int n, int R, int Ns, int item,
+                       const float2* tw, int tws, int es) {
+  switch (R) {
+    case 2: stage_bfly<2, DIR>(A, B, n, Ns, item, tw, tws, es); break;
+    case 3: stage_bfly<3, DIR>(A, B, n, Ns, item, tw, tws, es); break;
+    case 4: stage_bfly<4, DIR>(A, B, n, Ns, item, tw, tws, es); break;
+    case 8: stage_bfly<8, DIR>(A, B, n, Ns, item, tw, tws, es); break;
+    default: stage_direct<DIR>(A, B, n, R, Ns, item, tw, tws, es); break;
+  }
+}
+
+MC3_HD int stage_items(int n, int R) { return radix_is_dedicated(R) ? n / R : n; }
+
+#ifdef __CUDACC__
+// CTA driver: nb sequences; sequence b, element i at A[b*bs + i*es].
+// B is scratch of the same layout.  Returns the buffer holding the result.
+// Must be called by all threads of the CTA; ends with __syncthreads().
+template <int DIR>
+__device__ float2* cta_fft(float2* A, float2* B, const FftDesc& d, int nb, int es, int bs) {
+  int Ns = 1;
+  for (int s = 0; s < d.nstages; ++s) {
+    const int R = d.radix[s];
+    const int per = stage_items(d.n, R);
+    const int items = nb * per;
+    for (int it = threadIdx.x; it < items; it += blockDim.x) {
+      const int b = it / per;
+      const int j = it - b * per;
+      stage_item<DIR>(A + b * bs, B + b * bs, d.n, R, Ns, j, d.tw, d.tws, es);
+    }
+    __syncthreads();
+    float2* t = A; A = B; B = t;
+    Ns *= R;
+  }
+  return A;
+}
+#endif
+
+// Sequential host driver running the identical stage code (CPU tests).
+template <int DIR>
+inline float2* fft_host_reference(float2* A, float2* B, const FftDesc& d) {
+  int Ns = 1;
+  for (int s = 0; s < d.nstages; ++s) {
+    const int R = d.radix[s];
+    const int per = stage_items(d.n, R);
+    for (int j = 0; j < per; ++j) stage_item<DIR>(A, B, d.n, R, Ns, j, d.tw, d.tws, 1);
+    float2* t = A; A = B; B = t;
+    Ns *= R;
+  }
+  return A;
+}
+
+// ---- real-data helpers (length W = 2M real <-> M+1 complex) -----------
+// Forward: Z = FFT_M(x[2m] + i x[2m+1]); X[k] for k in [0, M].
+// twW: table e^{-2 pi i k / W} (stride twWs).
+MC3_HD float2 r2c_post(const float2* Z, int M, int k, const float2* twW, int twWs) {
+  const float2 zk = Z[k == M ? 0 : k];
+  const float2 zm = cconj(Z[k == 0 ? 0 : M - k]);
+  const float2 fe = c2(0.5f * (zk.x + zm.x), 0.5f * (zk.y + zm.y));
+  // fo = (zk - zm) * (-i/2)
+  const float2 dd = csub(zk, zm);
+  const float2 fo = c2(0.5f * dd.y, -0.5f * dd.x);
+  const float2 w = twW[k * twWs];
+  return cadd(fe, cmul(w, fo));
+}
+
+// Inverse pre-processing: X[0..M] (row of a half spectrum) -> Z[k], k<M.
+// The imaginary parts of X[0] and X[M] are ignored, i.e. the result is the
+// real part of the inverse of the Hermitian extension of the row.
+MC3_HD float2 c2r_pre(const float2* X, int M, int k, const float2* twW, int twWs) {
+  float2 xa, xb;
+  if (k == 0) {
+    xa = c2(X[0].x, 0.f);
+    xb = c2(X[M].x, 0.f);
+  } else {
+    xa = X[k];
+    xb = cconj(X[M - k]);
+  }
+  const float2 e = cadd(xa, xb);
+  float2 o = csub(xa, xb);
+  if (k) o = cmul(o, cconj(twW[k * twWs]));
+  // Z = e + i*o
+  return c2(e.x - o.y, e.y + o.x);
+}
+
+}  // namespace mc3

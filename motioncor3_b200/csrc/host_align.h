@@ -1,0 +1,82 @@
+// Host-side shift bookkeeping of the alignment path, in FP32 with the same
+// operation order as the reference's host code, so that its discontinuous
+// steps (0.01 px truncation, the 5/10 px spike tests, bad-patch tests)
+// take the same branches.
+#pragma once
+#include <vector>
+
+namespace mc3 {
+namespace host {
+
+// Frame groups of -Group binZ (DataUtil/CFmGroupParam.cpp:26-78) for movies
+// without a frame-integration file: consecutive runs of binZ frames.
+struct FrameGroups {
+  int binZ = 1;
+  std::vector<int> start, size;
+  std::vector<float> center;
+  void setup(int n_frames, int bin_z);
+  int count() const { return (int)start.size(); }
+};
+
+// Per-frame shift pairs stored as [x0..xn-1][y0..yn-1] (Align/CStackShift.cpp).
+struct StackShift {
+  int n = 0;
+  std::vector<float> v;
+  void setup(int n_frames) { n = n_frames; v.assign(2 * (size_t)n_frames, 0.0f); }
+  float& x(int i) { return v[i]; }
+  float& y(int i) { return v[n + i]; }
+  float x(int i) const { return v[i]; }
+  float y(int i) const { return v[n + i]; }
+  void add(const StackShift& d);
+  void multiply(float fx, float fy);
+  void truncate_decimal();          // CStackShift::TruncateDecimal
+  void make_relative(int ref);      // CStackShift::MakeRelative
+  void smooth(float w);             // CStackShift::Smooth
+  void remove_spikes();             // CStackShift::RemoveSpikes(false)
+};
+
+// CInterpolateShift::DoIt: group shifts -> frame shifts.
+StackShift interpolate(const StackShift& grp, const FrameGroups& g, int n_frames, bool nearest);
+
+// Util_LinEqs::DoIt (Gauss-Jordan, full pivoting).  Returns false when
+// singular.
+bool lin_eqs(float* coeff, float* vals, int dim);
+// CRemoveSpikes1D::DoIt(pfX, pfY, bSingle=false)
+void remove_spikes(float* sx, float* sy, int n);
+// CPeak2D::DoIt on a float window.
+void peak2d(const float* win, int sx, int sy, float* shift);
+
+// Iteration driver state of CIterativeAlign::mAlignStack for one stack.
+struct IterState {
+  StackShift tmp, grp, total;
+  float bfactor = 0;
+  float max_err = 0;
+  int iterations = 0;
+  bool done = false;
+  std::vector<float> errors;
+  void start(int n_frames, int n_groups, float bf);
+  // Consumes the group shifts measured in iteration `it`; returns true when
+  // the stack has finished iterating.
+  bool step(const float* grp_xy, const FrameGroups& g, int it, int max_iter, float tol);
+  // Final trajectory (linear interpolation, spike removal, two smoothings).
+  StackShift finish(const FrameGroups& g, int n_frames) const;
+};
+
+// Patch bookkeeping (Align/CPatchShifts.cpp).  shifts: [N][P][2].
+void patch_make_relative(std::vector<float>& shifts, int n_frames, int n_patches);
+void patch_detect_bads(const float* shifts, const float* centers, int n_frames, int n_patches,
+                       int W, int H, unsigned char* bad);
+
+// CDetectFeatures + CPatchCenters: patch start pixels in the alignment
+// (xcf) image from the normalised 128x128 feature map and its moments.
+void patch_starts(const float* map, int bx, int by, float mean, float m2, int px, int py,
+                  int xcf_x, int xcf_y, int pat_x, int pat_y, std::vector<int>& starts);
+
+// Ring template of the defect detector (BadPixel/CTemplate.cpp:20-57).
+void defect_template(int ms, float* tpl);
+
+// kV factor of the critical-dose curve (Correct/GWeightFrame.cu:101-109).
+float kv_factor(int kv);
+
+}  // namespace host
+}  // namespace mc3

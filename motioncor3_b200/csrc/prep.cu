@@ -1,0 +1,226 @@
+// Frame preparation: gain application, frame sum, hot-pixel and defect
+// detection, defect fill, image moments.  Restates MrcUtil/GApplyRefsToFrame.cu,
+// MrcUtil/CSumFFTStack.cpp, BadPixel/GDetectHot.cu, BadPixel/GLocalCC.cu,
+// BadPixel/GDetectPatch.cu, BadPixel/GCorrectBad.cu and Util/GCalcMoment2D.cu.
+#include "kernels.cuh"
+
+namespace mc3 {
+
+// ---- gain + running frame sum --------------------------------------------
+// One thread per pixel walks all frames: frame_f = raw_f * gain is written
+// to the padded frame stack and accumulated (in frame order, as the
+// reference's CSumFFTStack does) into the padded sum image.
+template <typename T>
+__global__ void k_gain_sum(const T* __restrict__ raw, long raw_stride, const float* __restrict__ gain,
+                           float* frames, long fr_stride, float* sum, int W, int H, int N, int padX) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= W) return;
+  const float g = gain ? gain[(long)y * W + x] : 1.0f;
+  float s = 0.0f;
+  for (int f = 0; f < N; ++f) {
+    float v = (float)raw[(long)f * raw_stride + (long)y * W + x];
+    if (gain) v *= g;
+    frames[(long)f * fr_stride + (long)y * padX + x] = v;
+    s += v;
+  }
+  if (sum) sum[(long)y * padX + x] = s;
+}
+
+int gain_and_sum(const void* raw, int mode, long raw_stride, const float* gain, float* frames,
+                 long fr_stride, float* sum, int W, int H, int N, cudaStream_t st) {
+  const int padX = 2 * (W / 2 + 1);
+  dim3 grid(ceil_div(W, 256), H);
+  switch (mode) {
+    case 0: k_gain_sum<uint8_t><<<grid, 256, 0, st>>>((const uint8_t*)raw, raw_stride, gain, frames, fr_stride, sum, W, H, N, padX); break;
+    case 1: k_gain_sum<int16_t><<<grid, 256, 0, st>>>((const int16_t*)raw, raw_stride, gain, frames, fr_stride, sum, W, H, N, padX); break;
+    case 2: k_gain_sum<float><<<grid, 256, 0, st>>>((const float*)raw, raw_stride, gain, frames, fr_stride, sum, W, H, N, padX); break;
+    case 6: k_gain_sum<uint16_t><<<grid, 256, 0, st>>>((const uint16_t*)raw, raw_stride, gain, frames, fr_stride, sum, W, H, N, padX); break;
+    default: return kEUnsupported;
+  }
+  MC3_CHECK_LAUNCH("k_gain_sum");
+  return kOk;
+}
+
+// ---- moments with the reference's reduction order ------------------------
+// GCalcMoment2D::DoIt (Util/GCalcMoment2D.cu:10-60, 96-114): grid-stride
+// per-thread FP32 sums, shared-memory tree, per-block division by W*H, then
+// a one-block tree over the block partials.  The same order gives the same
+// FP32 result, so thresholds derived from it match the reference.
+__global__ void k_moment_partial(const float* img, int W, int H, long pitch, int iExp, float* part) {
+  extern __shared__ float sh[];
+  float sum = 0.0f;
+  for (int y = blockIdx.x; y < H; y += gridDim.x) {
+    const float* ptr = img + (long)y * pitch;
+    for (int ix = threadIdx.x; ix < W; ix += blockDim.x) {
+      float val = ptr[ix];
+      float expval = val;
+      for (int i = 1; i < iExp; i++) expval *= val;
+      sum += expval;
+    }
+  }
+  sh[threadIdx.x] = sum;
+  __syncthreads();
+  for (int off = blockDim.x / 2; off > 0; off = off / 2) {
+    if (threadIdx.x < off) sh[threadIdx.x] += sh[threadIdx.x + off];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = sh[0] / (W * H);
+}
+
+__global__ void k_moment_final(float* part, float* out) {
+  extern __shared__ float sh[];
+  sh[threadIdx.x] = part[threadIdx.x];
+  __syncthreads();
+  for (int off = blockDim.x / 2; off > 0; off = off / 2) {
+    if (threadIdx.x < off) sh[threadIdx.x] += sh[threadIdx.x + off];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sh[0];
+}
+
+int moment_grid(int W, int H) {
+  const long px = (long)W * H;
+  const long nb = (px + 511) / 512;
+  if (nb >= 512) return 512;
+  if (nb >= 128) return 128;
+  if (nb >= 64) return 64;
+  return 32;
+}
+
+int image_moment(const float* img, int W, int H, long pitch, int iExp, float* d_part,
+                 float* d_out, cudaStream_t st) {
+  const int g = moment_grid(W, H);
+  k_moment_partial<<<g, 512, 512 * sizeof(float), st>>>(img, W, H, pitch, iExp, d_part);
+  MC3_CHECK_LAUNCH("k_moment_partial");
+  k_moment_final<<<1, g, g * sizeof(float), st>>>(d_part, d_out);
+  MC3_CHECK_LAUNCH("k_moment_final");
+  return kOk;
+}
+
+// ---- hot pixels (BadPixel/GDetectHot.cu:10-57) ----------------------------
+// mean/std come from two image_moment() results already on the device.
+__global__ void k_detect_hot(const float* sum, long pitch, int W, int H, const float* mom,
+                             float thr_sigma, uint8_t* bad) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= W) return;
+  const float fMean = mom[0];
+  float fStd = mom[1] - fMean * fMean;
+  fStd = (float)sqrtf(fmaxf(fStd, 0));
+  float fDelta = thr_sigma * fStd;
+  if (fDelta < 10) fDelta = 10;
+  const float fMax = fMean + fDelta;
+  bad[(long)y * W + x] = sum[(long)y * pitch + x] <= fMax ? 0 : 1;
+}
+
+// ---- local CC against the ring template (BadPixel/GLocalCC.cu:20-61) -----
+__constant__ float c_tpl[64];
+
+__global__ void k_local_cc(const float* img, long pitch, int W, int H, int ms, float* cc) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= W) return;
+  const long o = (long)y * pitch + x;
+  cc[o] = 0.0f;
+  if ((x + ms) >= W) return;
+  if ((y + ms) >= H) return;
+  const float* src = img + o;
+  float fMean = 0.0f, fStd = 0.0f, fCC = 0.0f;
+  for (int j = 0; j < ms; j++) {
+    for (int i = 0; i < ms; i++) {
+      float fImg = src[j * pitch + i];
+      float fRef = c_tpl[j * ms + i];
+      fMean += fImg;
+      fStd += (fImg * fImg);
+      fCC += (fRef * fImg);
+    }
+  }
+  int n = ms * ms;
+  fCC /= n;
+  fMean /= n;
+  fStd = fStd / n - fMean * fMean;
+  if (fStd < 0) fStd = 0.0f;
+  else fStd = sqrtf(fStd);
+  if (fStd == 0) cc[o] = 0.0f;
+  else cc[o] = fabsf(fCC) / fStd;
+}
+
+// GDetectPatch::mUpdateBadMap (BadPixel/GDetectPatch.cu:10-46, 56-104)
+__global__ void k_mark_defects(const float* cc, long pitch, int W, int H, const float* mom,
+                               float thr_sigma, int ms, uint8_t* bad) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if ((x + ms) >= W) return;
+  if ((y + ms) >= H) return;
+  const float fMean = mom[0];
+  const float fStd = (float)sqrtf(fmaxf(0, mom[1] - fMean * fMean));
+  const float thr = fMean + thr_sigma * fStd;
+  if (cc[(long)y * pitch + x] <= thr) return;
+  for (int j = 0; j < ms; ++j)
+    for (int i = 0; i < ms; ++i) bad[(long)(y + j) * W + x + i] = 1;
+}
+
+int detect_bad_pixels(const float* sum, int W, int H, float* cc_buf, float* d_part,
+                      float* d_mom /*4 floats*/, uint8_t* bad, const float* tpl, int ms,
+                      cudaStream_t st) {
+  const long pitch = 2 * (W / 2 + 1);
+  MC3_TRY(image_moment(sum, W, H, pitch, 1, d_part, d_mom + 0, st));
+  MC3_TRY(image_moment(sum, W, H, pitch, 2, d_part, d_mom + 1, st));
+  dim3 grid(ceil_div(W, 256), H);
+  k_detect_hot<<<grid, 256, 0, st>>>(sum, pitch, W, H, d_mom, 6.0f, bad);
+  MC3_CHECK_LAUNCH("k_detect_hot");
+  MC3_CUDA(cudaMemcpyToSymbolAsync(c_tpl, tpl, sizeof(float) * ms * ms, 0, cudaMemcpyHostToDevice, st));
+  k_local_cc<<<grid, 256, 0, st>>>(sum, pitch, W, H, ms, cc_buf);
+  MC3_CHECK_LAUNCH("k_local_cc");
+  MC3_TRY(image_moment(cc_buf, W, H, pitch, 1, d_part, d_mom + 2, st));
+  MC3_TRY(image_moment(cc_buf, W, H, pitch, 2, d_part, d_mom + 3, st));
+  k_mark_defects<<<grid, 256, 0, st>>>(cc_buf, pitch, W, H, d_mom + 2, 6.0f, ms, bad);
+  MC3_CHECK_LAUNCH("k_mark_defects");
+  return kOk;
+}
+
+// ---- defect fill (BadPixel/GCorrectBad.cu:44-69, 96-150) ------------------
+__global__ void k_correct_bad(float* frames, long fr_stride, const uint8_t* bad, int W, int H,
+                              int padX, int win0) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= W) return;
+  if (bad[(long)y * W + x] == 0) return;
+  float* fr = frames + (long)blockIdx.z * fr_stride;
+  const int i = y * padX + x;
+  unsigned int next = i * 109 + 619;
+  int win = win0;
+  for (int j = 0; j < 10; j++) {
+    unsigned int nl = next;
+    const int w2 = win * win, half = win / 2;
+    for (int k = 0; k < 500; k++) {
+      nl *= 997;
+      int iX = nl % w2;
+      int iY = iX / win - half + y;
+      if (iY < 0 || iY >= H) continue;
+      iX = iX % win - half + x;
+      if (iX < 0 || iX >= W) continue;
+      if (bad[(long)iY * W + iX] == 1) continue;
+      fr[i] = fr[(long)iY * padX + iX];
+      return;
+    }
+    win += 50;
+    next *= 997;
+  }
+  int iX = next % (unsigned int)(W * H);
+  int iY = iX / W;
+  iX = iX % W;
+  fr[i] = fr[(long)iY * padX + iX];
+}
+
+int correct_bad_pixels(float* frames, long fr_stride, int N, const uint8_t* bad, int W, int H,
+                       cudaStream_t st) {
+  const int padX = 2 * (W / 2 + 1);
+  dim3 grid(ceil_div(W, 256), H, N);
+  k_correct_bad<<<grid, 256, 0, st>>>(frames, fr_stride, bad, W, H, padX, 31);
+  MC3_CHECK_LAUNCH("k_correct_bad");
+  return kOk;
+}
+
+}  // namespace mc3

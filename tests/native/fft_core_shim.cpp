@@ -1,0 +1,74 @@
+// Host-side shim exposing the libmc3 FFT core (fft_core.cuh) to the CPU
+// tests: runs the exact Stockham stage code sequentially so the index
+// arithmetic of the device kernels is checked against numpy without a GPU.
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include "../../motioncor3_b200/csrc/fft_core.cuh"
+
+using namespace mc3;
+
+static std::vector<float2> make_table(int n) {
+  std::vector<float2> t(n);
+  for (int k = 0; k < n; ++k) {
+    double a = -2.0 * M_PI * (double)k / (double)n;
+    t[k].x = (float)std::cos(a);
+    t[k].y = (float)std::sin(a);
+  }
+  return t;
+}
+
+extern "C" int shim_factorize(int n, int* radix) { return fft_factorize(n, radix); }
+
+// Complex FFT of length n, dir = -1 forward, +1 inverse (unnormalised).
+extern "C" int shim_cfft(const float* in, float* out, int n, int dir) {
+  FftDesc d;
+  d.n = n;
+  d.nstages = fft_factorize(n, d.radix);
+  if (d.nstages < 0) return -1;
+  std::vector<float2> tw = make_table(n);
+  d.tw = tw.data();
+  d.tws = 1;
+  std::vector<float2> A(n), B(n);
+  std::memcpy(A.data(), in, sizeof(float2) * n);
+  float2* r = dir < 0 ? fft_host_reference<-1>(A.data(), B.data(), d)
+                      : fft_host_reference<1>(A.data(), B.data(), d);
+  std::memcpy(out, r, sizeof(float2) * n);
+  return 0;
+}
+
+// Real forward transform of length W (even): out has W/2+1 complex values.
+extern "C" int shim_rfft(const float* in, float* out, int W) {
+  const int M = W / 2;
+  FftDesc d;
+  d.n = M;
+  d.nstages = fft_factorize(M, d.radix);
+  if (d.nstages < 0) return -1;
+  std::vector<float2> tw = make_table(W);
+  d.tw = tw.data();
+  d.tws = 2;
+  std::vector<float2> A(M), B(M);
+  for (int m = 0; m < M; ++m) { A[m].x = in[2 * m]; A[m].y = in[2 * m + 1]; }
+  float2* Z = fft_host_reference<-1>(A.data(), B.data(), d);
+  float2* o = reinterpret_cast<float2*>(out);
+  for (int k = 0; k <= M; ++k) o[k] = r2c_post(Z, M, k, tw.data(), 1);
+  return 0;
+}
+
+// Real inverse (unnormalised) of length W from W/2+1 complex values.
+extern "C" int shim_irfft(const float* in, float* out, int W) {
+  const int M = W / 2;
+  FftDesc d;
+  d.n = M;
+  d.nstages = fft_factorize(M, d.radix);
+  if (d.nstages < 0) return -1;
+  std::vector<float2> tw = make_table(W);
+  d.tw = tw.data();
+  d.tws = 2;
+  const float2* X = reinterpret_cast<const float2*>(in);
+  std::vector<float2> A(M), B(M);
+  for (int k = 0; k < M; ++k) A[k] = c2r_pre(X, M, k, tw.data(), 1);
+  float2* z = fft_host_reference<1>(A.data(), B.data(), d);
+  for (int m = 0; m < M; ++m) { out[2 * m] = z[m].x; out[2 * m + 1] = z[m].y; }
+  return 0;
+}
