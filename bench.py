@@ -1,0 +1,327 @@
+#!/usr/bin/env python
+"""Benchmark: frames/s aligned + corrected at 4096^2.
+
+Workload (one step = one movie): 60 synthetic float32 frames of 4096x4096,
+5x5 patches, -Iter 10 -Bft 500 150 -Tol 0.1, 0.8 e/px/frame (FmDose 1.161
+e/A^2 at 0.83 A/px, 300 kV, dose weighting on), gain uniform in [0.9, 1.1],
+global random-walk drift plus a smooth local field of up to 2 px.  The data
+are generated on the GPU from a fixed seed (no dataset is needed).
+
+`value`: frames/s with the raw frames already in HBM (device timing with
+CUDA events on the work stream, max over ranks).  `e2e`: the same through
+the C ABI with pinned host buffers (H2D of the raw frames and D2H of the
+sums inside the timed region).  Inputs (4 GB per movie) exceed L2, so no
+flush is needed between steps.  Multi-GPU runs are independent replicas
+(one movie per GPU, no collective on the data path).
+
+`--impl reference` times the FP64 CPU restatement of the reference path (the
+reference has no CPU implementation of its own) on all host cores, on a
+bounded sample of the same workload (3 frames of 4096x4096 per step).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "frames/s aligned+corrected at 4096^2 vs plain GPU path; shift err <=0.05 px"
+CPU_SAMPLE_FRAMES = 3
+
+
+def workload(cfg: str):
+    if cfg == "cfg1":
+        return dict(nx=1024, ny=1024, nz=40, dose=1.0, gain=False, local=False,
+                    params=dict(patch=(0, 0), iter=7, tol=0.5, bft=(150, 100), pix_size=1.0),
+                    name="40x1024^2 global only, -Iter 7 -Tol 0.5 -Bft 150, 1 e/px/frame")
+    return dict(nx=4096, ny=4096, nz=60, dose=0.8, gain=True, local=True,
+                params=dict(patch=(5, 5), iter=10, tol=0.1, bft=(500, 150), fm_dose=1.161,
+                            pix_size=0.83, kv=300),
+                name="60x4096^2 float32, -Patch 5 5 -Iter 10 -Bft 500 150, dose-weighted (DW+DWS), gain")
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for i, n in enumerate(names):
+                if s[5 + i].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.samples)}
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_run(frames, gain, params, steps=1):
+    """Oracle (FP64 restatement) on the sample; returns seconds per step."""
+    from oracle import oracle as O
+    kw = dict(params)
+    O.lib()
+    ts = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        O.process_movie(frames, gain=gain, **kw)
+        ts.append(time.perf_counter() - t0)
+    return ts
+
+
+def run_reference(args, wl, world, rank):
+    """CPU arm: the FP64 restatement of the reference path on all host cores."""
+    if rank != 0:
+        return 0
+    import numpy as np
+    from motioncor3_b200 import synthetic as S
+    n = CPU_SAMPLE_FRAMES
+    try:
+        import torch
+        if torch.cuda.is_available():
+            mv = S.make_movie(wl["nx"], wl["ny"], n, dose=wl["dose"], seed=7, gain=wl["gain"],
+                              local=wl["local"], backend="torch")
+            frames = mv.frames.cpu().numpy()
+            gain = mv.gain.cpu().numpy() if mv.gain is not None else None
+        else:
+            raise RuntimeError
+    except Exception:
+        mv = S.make_movie(wl["nx"], wl["ny"], n, dose=wl["dose"], seed=7, gain=wl["gain"],
+                          local=False)
+        frames, gain = mv.frames, mv.gain
+    params = dict(wl["params"])
+    for _ in range(args.warmup):
+        cpu_run(frames, gain, params)
+    ts = cpu_run(frames, gain, params, steps=args.steps)
+    total = sum(ts)
+    value = n * args.steps / total
+    cores = os.cpu_count() or 1
+    sample = f"{n} frames of {wl['nx']}x{wl['ny']} per step, same options"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "frames/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": wl["name"], "sample": sample, "l2_flush": "inputs > L2"},
+        "cpu_baseline": {"value": value, "unit": "frames/s", "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "frames/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, wl, world, rank, local):
+    import numpy as np
+    import torch
+    from motioncor3_b200 import api
+    from motioncor3_b200 import synthetic as S
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    nx, ny, nz = wl["nx"], wl["ny"], wl["nz"]
+    mv = S.make_movie(nx, ny, nz, dose=wl["dose"], seed=1000 + rank, gain=wl["gain"],
+                      local=wl["local"], backend="torch", device=f"cuda:{local}")
+    params = api.Params(gpu=local, **wl["params"])
+    mc = api.MotionCor3(params)
+    stream = torch.cuda.current_stream()
+    mc.set_stream(stream.cuda_stream)
+    if mv.gain is not None:
+        mc.set_gain(mv.gain)
+    frames = mv.frames
+    info = mc.plan(nx, ny, nz)
+    sums = torch.empty((info["n_sums"], ny, nx), dtype=torch.float32, device="cuda")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # ---- device-resident timing ----
+    for _ in range(args.warmup):
+        mc.process(frames, sums_out=sums)
+    api.profile_enable(True)
+    api.profile_read(reset=True)
+    launches0 = api.kernel_launches()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    last = None
+    for _ in range(args.steps):
+        last = mc.process(frames, sums_out=sums)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    launches = (api.kernel_launches() - launches0) // max(args.steps, 1)
+    prof = api.profile_read(reset=True)
+    api.profile_enable(False)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * nz * args.steps / (ms / 1000.0)
+
+    # ---- end to end through the C ABI with pinned host buffers ----
+    host_frames = frames.cpu().pin_memory()
+    host_sums = torch.empty((info["n_sums"], ny, nx), dtype=torch.float32).pin_memory()
+    hf, hs = host_frames.numpy(), host_sums.numpy()
+    mc.process(hf, sums_out=hs)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.steps):
+        mc.process(hf, sums_out=hs)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    e2e_ms = max(f0.elapsed_time(f1), wall * 1000.0)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = world * nz * args.steps / (e2e_ms / 1000.0)
+    h2d = hf.nbytes
+    d2h = hs.nbytes
+
+    # ---- roofline of the dominant kernel ----
+    peak, peak_kind = measured_peak_hbm()
+    top = max(prof.items(), key=lambda kv: kv[1][1]) if prof else None
+    roof = None
+    if top:
+        name, (n_launch, tot_ms, tot_bytes) = top
+        achieved = (tot_bytes / n_launch) / ((tot_ms / n_launch) / 1000.0) / 1e9
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tp):
+            traffic = json.load(open(tp)).get(name)
+        roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "launches_per_step": n_launch / args.steps,
+                "share_of_step": tot_ms / ms if ms else None,
+                "algorithmic_bytes_per_launch": tot_bytes / n_launch}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        n = CPU_SAMPLE_FRAMES
+        sf = host_frames[:n].numpy().copy()
+        g = mv.gain.cpu().numpy() if mv.gain is not None else None
+        ts = cpu_run(sf, g, dict(wl["params"]))
+        cpu = {"value": n / ts[0], "unit": "frames/s", "cores": os.cpu_count() or 1,
+               "kind": "port",
+               "sample": f"{n} frames of {nx}x{ny} with the same options (FP64 oracle, all cores)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": wl["name"], "frames_per_step": nz,
+                       "parallelism": f"replicas x{world}", "l2_flush": "inputs 4 GB > L2",
+                       "iterations_global": int(last.iterations[0]),
+                       "iterations_patch_max": int(last.iterations[1:].max()) if last.n_patches else 0},
+            "e2e": {"value": e2e, "unit": "frames/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "kernels": {k: {"launches_per_step": v[0] / args.steps, "ms_per_step": v[1] / args.steps,
+                            "GBps": (v[2] / v[1] / 1e6) if v[1] else None}
+                        for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
+        }
+        print(json.dumps(line), flush=True)
+    mc.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=["cfg2", "cfg1"], default="cfg2")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    args = ap.parse_args(argv)
+    world, rank, local = dist_setup()
+    wl = workload(args.config)
+    if args.impl == "reference":
+        return run_reference(args, wl, world, rank)
+    return run_ours(args, wl, world, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

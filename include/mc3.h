@@ -159,6 +159,15 @@ int mc3_local_gather(const float* in, float* out, int nx, int ny, const float* c
 int mc3_dose_weighted_sums(mc3_ctx* ctx, const float* spectra, int nx, int ny, int nz,
                            const float* shifts_host, float* sums, int* n_sums);
 
+/* ---- diagnostics (no counterpart in the reference, which reports NVTX
+ * ranges and wall-clock prints instead, e.g. CProcessThread.cpp:103-104) ---- */
+/* Per-kernel timing with CUDA events around every launch (process-wide). */
+void mc3_profile_enable(int on);
+/* Writes {"kernel": [launches, total_ms, algorithmic_bytes], ...} as JSON. */
+int mc3_profile_read(char* buf, size_t len, int reset);
+/* Kernel launches issued by this library since it was loaded. */
+unsigned long long mc3_kernel_launches(void);
+
 /* ---- host-side bookkeeping (host pointers) ---- */
 /* Align::CPeak2D::DoIt (Align/CPeak2D.cpp:39-109). */
 void mc3_peak2d(const float* window, int sea_x, int sea_y, float* shift);

@@ -1,0 +1,459 @@
+"""ctypes binding of libmc3 (include/mc3.h).
+
+`MotionCor3` mirrors the reference program's single-movie flow
+(CMain::mDoSingleCryoEM, CMain.cpp:93): options as in CInput (CInput.cpp:82-127),
+one call from raw frames to the unweighted / dose-weighted sums and the
+global and patch shift tables.  Component functions expose the individual
+replaced interfaces (FFT, phase shift, correlation + peak, bad pixels, local
+gather, dose-weighted sums, host bookkeeping) for integrators and tests.
+
+Device arrays are passed as torch CUDA tensors (their data_ptr); host arrays
+as numpy arrays.  Errors raise MC3Error carrying the library status code.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import os
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+lib_path = os.path.join(_HERE, "libmc3.so")
+
+MC3_OK, MC3_EINVAL, MC3_ENOMEM, MC3_ECUDA, MC3_ETIMEOUT, MC3_EIO, MC3_EUNSUPPORTED = range(7)
+
+
+class MC3Error(RuntimeError):
+    def __init__(self, code: int, what: str = ""):
+        self.code = code
+        msg = _lib().mc3_strerror(code).decode() if _LIB is not None else f"status {code}"
+        super().__init__(f"{what}: {msg} (status {code})" if what else f"{msg} (status {code})")
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [
+        ("patch", ctypes.c_int * 3),
+        ("iter", ctypes.c_int),
+        ("tol", ctypes.c_float),
+        ("bft", ctypes.c_float * 2),
+        ("phase_only", ctypes.c_int),
+        ("ft_bin", ctypes.c_float),
+        ("init_dose", ctypes.c_float),
+        ("fm_dose", ctypes.c_float),
+        ("pix_size", ctypes.c_float),
+        ("kv", ctypes.c_int),
+        ("group", ctypes.c_int * 2),
+        ("fm_ref", ctypes.c_int),
+        ("sum_range", ctypes.c_float * 2),
+        ("align", ctypes.c_int),
+        ("correct_bad", ctypes.c_int),
+        ("gpu", ctypes.c_int),
+    ]
+
+
+class _PlanInfo(ctypes.Structure):
+    _fields_ = [
+        ("n_sums", ctypes.c_int),
+        ("n_patches", ctypes.c_int),
+        ("xcf_size", ctypes.c_int * 2),
+        ("patch_size", ctypes.c_int * 2),
+        ("xcf_bin", ctypes.c_float * 2),
+        ("device_bytes", ctypes.c_size_t),
+    ]
+
+
+class _Movie(ctypes.Structure):
+    _fields_ = [
+        ("frames", ctypes.c_void_p),
+        ("mode", ctypes.c_int),
+        ("nx", ctypes.c_int),
+        ("ny", ctypes.c_int),
+        ("nz", ctypes.c_int),
+        ("on_device", ctypes.c_int),
+    ]
+
+
+class _Result(ctypes.Structure):
+    _fields_ = [
+        ("sums", ctypes.c_void_p),
+        ("sums_on_device", ctypes.c_int),
+        ("global_shifts", ctypes.c_void_p),
+        ("patch_shifts", ctypes.c_void_p),
+        ("patch_centers", ctypes.c_void_p),
+        ("patch_bad", ctypes.c_void_p),
+        ("iterations", ctypes.c_void_p),
+        ("errors", ctypes.c_void_p),
+        ("n_sums", ctypes.c_int),
+        ("n_patches", ctypes.c_int),
+        ("time_ms", ctypes.c_double),
+    ]
+
+
+_LIB: Optional[ctypes.CDLL] = None
+_VP = ctypes.c_void_p
+_I = ctypes.c_int
+_F = ctypes.c_float
+
+_SIGS = {
+    "mc3_version": ([], ctypes.c_char_p),
+    "mc3_strerror": ([_I], ctypes.c_char_p),
+    "mc3_params_default": ([ctypes.POINTER(_Params)], None),
+    "mc3_create": ([ctypes.POINTER(_Params), ctypes.POINTER(_VP)], _I),
+    "mc3_destroy": ([_VP], _I),
+    "mc3_set_stream": ([_VP, _VP], _I),
+    "mc3_plan": ([_VP, _I, _I, _I, ctypes.POINTER(_PlanInfo)], _I),
+    "mc3_set_gain": ([_VP, _VP, _I, _I, _I], _I),
+    "mc3_process_movie": ([_VP, ctypes.POINTER(_Movie), ctypes.POINTER(_Result)], _I),
+    "mc3_fft_forward": ([_VP, _I, _I, _I, _I, _VP], _I),
+    "mc3_fft_inverse": ([_VP, _I, _I, _I, _VP], _I),
+    "mc3_phase_shift": ([_VP, _VP, _I, _I, _F, _F, _I, _VP], _I),
+    "mc3_fourier_crop": ([_VP, _I, _I, _VP, _I, _I, _VP], _I),
+    "mc3_correlate": ([_VP, _VP, _I, _I, _F, _I, _I, _I, _VP, _VP, _VP], _I),
+    "mc3_iterative_align": ([_VP, _VP, _I, _I, _I, _I, _I, _F, _F, _I, _VP, _VP], _I),
+    "mc3_detect_bad_pixels": ([_VP, _I, _I, _VP, _VP], _I),
+    "mc3_correct_bad_pixels": ([_VP, _I, _I, _I, _VP, _VP], _I),
+    "mc3_local_gather": ([_VP, _VP, _I, _I, _VP, _VP, _VP, _I, _VP], _I),
+    "mc3_dose_weighted_sums": ([_VP, _VP, _I, _I, _I, _VP, _VP, _VP], _I),
+    "mc3_profile_enable": ([_I], None),
+    "mc3_profile_read": ([ctypes.c_char_p, ctypes.c_size_t, _I], _I),
+    "mc3_kernel_launches": ([], ctypes.c_ulonglong),
+    "mc3_peak2d": ([_VP, _I, _I, _VP], None),
+    "mc3_remove_spikes": ([_VP, _VP, _I], None),
+    "mc3_lin_eqs": ([_VP, _VP, _I], _I),
+    "mc3_smooth_shifts": ([_VP, _VP, _I, _F], None),
+    "mc3_patch_make_relative": ([_VP, _I, _I], None),
+    "mc3_patch_detect_bads": ([_VP, _VP, _I, _I, _I, _I, _VP], None),
+}
+
+
+def _lib() -> ctypes.CDLL:
+    """Loads libmc3.so (built in place by motioncor3_b200.build); raises if absent."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(lib_path):
+            raise RuntimeError(
+                f"libmc3.so not found at {lib_path}; build it with "
+                "`python -m motioncor3_b200.build` (there is no fallback path)")
+        L = ctypes.CDLL(lib_path)
+        for name, (args, res) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _LIB = L
+    return _LIB
+
+
+lib = _lib
+
+
+def _check(code: int, what: str) -> None:
+    if code != MC3_OK:
+        raise MC3Error(code, what)
+
+
+def _hp(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(_VP)
+
+
+def _stream():
+    import torch
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _dp(t) -> ctypes.c_void_p:
+    return ctypes.c_void_p(t.data_ptr())
+
+
+@dataclasses.dataclass
+class Params:
+    """In-scope MotionCor3 options; defaults of CInput::CInput (CInput.cpp:82-127)."""
+    patch: tuple = (0, 0)
+    iter: int = 15
+    tol: float = 0.1
+    bft: tuple = (500.0, 100.0)
+    phase_only: int = 0
+    ft_bin: float = 1.0
+    init_dose: float = 0.0
+    fm_dose: float = 0.0
+    pix_size: float = 0.0
+    kv: int = 300
+    group: tuple = (1, 4)
+    fm_ref: int = -1
+    sum_range: tuple = (3.0, 25.0)
+    align: int = 1
+    correct_bad: int = 1
+    gpu: int = 0
+
+    def to_c(self) -> _Params:
+        p = _Params()
+        _lib().mc3_params_default(ctypes.byref(p))
+        px = list(self.patch) + [0] * (3 - len(self.patch))
+        for i in range(3):
+            p.patch[i] = int(px[i])
+        p.iter = int(self.iter)
+        p.tol = float(self.tol)
+        p.bft[0], p.bft[1] = float(self.bft[0]), float(self.bft[1])
+        p.phase_only = int(self.phase_only)
+        p.ft_bin = float(self.ft_bin)
+        p.init_dose = float(self.init_dose)
+        p.fm_dose = float(self.fm_dose)
+        p.pix_size = float(self.pix_size)
+        p.kv = int(self.kv)
+        p.group[0], p.group[1] = int(self.group[0]), int(self.group[1])
+        p.fm_ref = int(self.fm_ref)
+        p.sum_range[0], p.sum_range[1] = float(self.sum_range[0]), float(self.sum_range[1])
+        p.align = int(self.align)
+        p.correct_bad = int(self.correct_bad)
+        p.gpu = int(self.gpu)
+        return p
+
+
+@dataclasses.dataclass
+class Result:
+    sums: object                 # [n_sums][ny][nx] numpy (host) or torch tensor (device)
+    global_shifts: np.ndarray    # [nz][2]
+    patch_shifts: Optional[np.ndarray]
+    patch_centers: Optional[np.ndarray]
+    patch_bad: Optional[np.ndarray]
+    iterations: np.ndarray       # [1 + n_patches]
+    errors: np.ndarray           # [1 + n_patches][iter]
+    n_sums: int
+    n_patches: int
+    time_ms: float
+
+
+_MODES = {np.dtype(np.uint8): 0, np.dtype(np.int16): 1, np.dtype(np.float32): 2, np.dtype(np.uint16): 6}
+
+
+class MotionCor3:
+    """One processing context on one GPU (mc3_create / mc3_process_movie)."""
+
+    def __init__(self, params: Optional[Params] = None):
+        self.params = params or Params()
+        self._p = self.params.to_c()
+        h = _VP()
+        _check(_lib().mc3_create(ctypes.byref(self._p), ctypes.byref(h)), "mc3_create")
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _lib().mc3_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_stream(self, stream) -> None:
+        _check(_lib().mc3_set_stream(self._h, stream), "mc3_set_stream")
+
+    def plan(self, nx: int, ny: int, nz: int) -> dict:
+        info = _PlanInfo()
+        _check(_lib().mc3_plan(self._h, nx, ny, nz, ctypes.byref(info)), "mc3_plan")
+        return dict(n_sums=info.n_sums, n_patches=info.n_patches, xcf_size=tuple(info.xcf_size),
+                    patch_size=tuple(info.patch_size), xcf_bin=tuple(info.xcf_bin),
+                    device_bytes=info.device_bytes)
+
+    def set_gain(self, gain) -> None:
+        if gain is None:
+            _check(_lib().mc3_set_gain(self._h, None, 0, 0, 0), "mc3_set_gain")
+            return
+        if hasattr(gain, "data_ptr"):
+            _check(_lib().mc3_set_gain(self._h, _dp(gain), gain.shape[1], gain.shape[0], 1),
+                   "mc3_set_gain")
+        else:
+            g = np.ascontiguousarray(gain, dtype=np.float32)
+            _check(_lib().mc3_set_gain(self._h, _hp(g), g.shape[1], g.shape[0], 0), "mc3_set_gain")
+
+    def process(self, frames, sums_out=None) -> Result:
+        """frames: [nz][ny][nx] numpy array (host) or torch CUDA tensor."""
+        on_dev = hasattr(frames, "data_ptr")
+        if on_dev:
+            import torch
+            dt = {torch.uint8: 0, torch.int16: 1, torch.float32: 2}.get(frames.dtype)
+            if dt is None:
+                raise MC3Error(MC3_EUNSUPPORTED, "frame dtype")
+            nz, ny, nx = frames.shape
+            fptr = _dp(frames)
+            keep = frames
+        else:
+            keep = np.ascontiguousarray(frames)
+            dt = _MODES.get(keep.dtype)
+            if dt is None:
+                raise MC3Error(MC3_EUNSUPPORTED, "frame dtype")
+            nz, ny, nx = keep.shape
+            fptr = keep.ctypes.data_as(_VP)
+        info = self.plan(nx, ny, nz)
+        ns, P = info["n_sums"], info["n_patches"]
+        it = int(self.params.iter)
+        gsh = np.zeros((nz, 2), np.float32)
+        psh = np.zeros((nz, max(P, 1), 2), np.float32)
+        pc = np.zeros((max(P, 1), 2), np.float32)
+        pb = np.zeros((nz, max(P, 1)), np.uint8)
+        iters = np.zeros(1 + P, np.int32)
+        errs = np.zeros((1 + P, it), np.float32)
+        r = _Result()
+        if sums_out is not None and hasattr(sums_out, "data_ptr"):
+            r.sums = sums_out.data_ptr()
+            r.sums_on_device = 1
+            sums = sums_out
+        elif sums_out is not None:
+            sums = sums_out
+            r.sums = sums.ctypes.data
+            r.sums_on_device = 0
+        else:
+            sums = np.zeros((ns, ny, nx), np.float32)
+            r.sums = sums.ctypes.data
+            r.sums_on_device = 0
+        r.global_shifts = gsh.ctypes.data
+        r.patch_shifts = psh.ctypes.data if P else None
+        r.patch_centers = pc.ctypes.data if P else None
+        r.patch_bad = pb.ctypes.data if P else None
+        r.iterations = iters.ctypes.data
+        r.errors = errs.ctypes.data
+        mv = _Movie(fptr, dt, nx, ny, nz, 1 if on_dev else 0)
+        _check(_lib().mc3_process_movie(self._h, ctypes.byref(mv), ctypes.byref(r)),
+               "mc3_process_movie")
+        del keep
+        return Result(sums=sums, global_shifts=gsh, patch_shifts=psh if P else None,
+                      patch_centers=pc if P else None, patch_bad=pb if P else None,
+                      iterations=iters, errors=errs, n_sums=r.n_sums, n_patches=r.n_patches,
+                      time_ms=r.time_ms)
+
+    # ---- component entry points needing the context ----
+    def iterative_align(self, stack, group: int, max_iter: int, tol: float, bfactor: float,
+                        phase_only: int = 0):
+        """stack: torch complex64 CUDA tensor [n][cmp_y][cmp_x]."""
+        n, cy, cx = stack.shape
+        sh = np.zeros((n, 2), np.float32)
+        its = ctypes.c_int(0)
+        _check(_lib().mc3_iterative_align(self._h, _dp(stack), cx, cy, n, group, max_iter, tol,
+                                          bfactor, phase_only, _hp(sh), ctypes.byref(its)),
+               "mc3_iterative_align")
+        return sh, its.value
+
+    def dose_weighted_sums(self, spectra, nx: int, ny: int, shifts: np.ndarray, sums):
+        nz = spectra.shape[0]
+        s = np.ascontiguousarray(shifts, np.float32)
+        ns = ctypes.c_int(0)
+        _check(_lib().mc3_dose_weighted_sums(self._h, _dp(spectra), nx, ny, nz, _hp(s), _dp(sums),
+                                             ctypes.byref(ns)), "mc3_dose_weighted_sums")
+        return ns.value
+
+
+# ---- stateless components (device tensors) ----
+def fft_forward(frames, nx: int, ny: int, normalise: bool = True) -> None:
+    """In place on a float32 CUDA tensor [nz][ny][2*(nx//2+1)]."""
+    nz = frames.shape[0]
+    _check(_lib().mc3_fft_forward(_dp(frames), nx, ny, nz, int(normalise), _stream()), "mc3_fft_forward")
+
+
+def fft_inverse(frames, nx: int, ny: int) -> None:
+    nz = frames.shape[0]
+    _check(_lib().mc3_fft_inverse(_dp(frames), nx, ny, nz, _stream()), "mc3_fft_inverse")
+
+
+def phase_shift(src, dst, sx: float, sy: float, accumulate: bool = False) -> None:
+    cy, cx = src.shape[-2], src.shape[-1]
+    _check(_lib().mc3_phase_shift(_dp(src), _dp(dst), cx, cy, sx, sy, int(accumulate), _stream()),
+           "mc3_phase_shift")
+
+
+def fourier_crop(src, dst) -> None:
+    _check(_lib().mc3_fourier_crop(_dp(src), src.shape[-1], src.shape[-2], _dp(dst), dst.shape[-1],
+                                   dst.shape[-2], _stream()), "mc3_fourier_crop")
+
+
+def correlate(group, sum_, bfactor: float, phase_only: int = 0, sea=(64, 64), window=None):
+    cy, cx = group.shape[-2], group.shape[-1]
+    sh = np.zeros(2, np.float32)
+    _check(_lib().mc3_correlate(_dp(group), _dp(sum_), cx, cy, bfactor, phase_only, sea[0], sea[1],
+                                _dp(window) if window is not None else None, _hp(sh), _stream()),
+           "mc3_correlate")
+    return sh
+
+
+def detect_bad_pixels(sum_padded, nx: int, ny: int, bad) -> None:
+    _check(_lib().mc3_detect_bad_pixels(_dp(sum_padded), nx, ny, _dp(bad), _stream()),
+           "mc3_detect_bad_pixels")
+
+
+def correct_bad_pixels(frames, nx: int, ny: int, bad) -> None:
+    _check(_lib().mc3_correct_bad_pixels(_dp(frames), nx, ny, frames.shape[0], _dp(bad), _stream()),
+           "mc3_correct_bad_pixels")
+
+
+def local_gather(src, dst, nx: int, ny: int, centers, shifts, bad=None) -> None:
+    P = centers.shape[0]
+    _check(_lib().mc3_local_gather(_dp(src), _dp(dst), nx, ny, _dp(centers), _dp(shifts),
+                                   _dp(bad) if bad is not None else None, P, _stream()),
+           "mc3_local_gather")
+
+
+# ---- diagnostics ----
+def profile_enable(on: bool) -> None:
+    _lib().mc3_profile_enable(int(on))
+
+
+def profile_read(reset: bool = False) -> dict:
+    import json
+    buf = ctypes.create_string_buffer(1 << 16)
+    _check(_lib().mc3_profile_read(buf, len(buf), int(reset)), "mc3_profile_read")
+    return json.loads(buf.value.decode())
+
+
+def kernel_launches() -> int:
+    return int(_lib().mc3_kernel_launches())
+
+
+# ---- host bookkeeping ----
+def peak2d(window: np.ndarray) -> np.ndarray:
+    w = np.ascontiguousarray(window, np.float32)
+    out = np.zeros(2, np.float32)
+    _lib().mc3_peak2d(_hp(w), w.shape[1], w.shape[0], _hp(out))
+    return out
+
+
+def remove_spikes(sx: np.ndarray, sy: np.ndarray):
+    x = np.ascontiguousarray(sx, np.float32).copy()
+    y = np.ascontiguousarray(sy, np.float32).copy()
+    _lib().mc3_remove_spikes(_hp(x), _hp(y), len(x))
+    return x, y
+
+
+def lin_eqs(coeff: np.ndarray, vals: np.ndarray):
+    a = np.ascontiguousarray(coeff, np.float32).copy()
+    b = np.ascontiguousarray(vals, np.float32).copy()
+    ok = _lib().mc3_lin_eqs(_hp(a), _hp(b), len(b))
+    return bool(ok), b
+
+
+def smooth_shifts(sx: np.ndarray, sy: np.ndarray, weight: float):
+    x = np.ascontiguousarray(sx, np.float32).copy()
+    y = np.ascontiguousarray(sy, np.float32).copy()
+    _lib().mc3_smooth_shifts(_hp(x), _hp(y), len(x), weight)
+    return x, y
+
+
+def patch_make_relative(shifts: np.ndarray) -> np.ndarray:
+    s = np.ascontiguousarray(shifts, np.float32).copy()
+    _lib().mc3_patch_make_relative(_hp(s), s.shape[0], s.shape[1])
+    return s
+
+
+def patch_detect_bads(shifts: np.ndarray, centers: np.ndarray, nx: int, ny: int) -> np.ndarray:
+    s = np.ascontiguousarray(shifts, np.float32)
+    c = np.ascontiguousarray(centers, np.float32)
+    bad = np.zeros(s.shape[:2], np.uint8)
+    _lib().mc3_patch_detect_bads(_hp(s), _hp(c), s.shape[0], s.shape[1], nx, ny, _hp(bad))
+    return bad

@@ -84,8 +84,13 @@ def build(force: bool = False, jobs: int = 8, verbose: bool = False) -> str:
 
     with cf.ThreadPoolExecutor(max_workers=max(1, jobs)) as ex:
         list(ex.map(run, cmds))
+    vscript = os.path.join(OBJ, "exports.map")
+    with open(vscript, "w") as fh:
+        fh.write("{ global: mc3_*; local: *; };\n")
     if force or cmds or _stale(LIB, objs):
-        run([nvcc, *ARCH, "-shared", "-ccbin", cxx, "-o", LIB, *objs, "-lpthread"])
+        # only the C ABI is exported; the static CUDA runtime stays private
+        run([nvcc, *ARCH, "-shared", "-ccbin", cxx, "-o", LIB, *objs, "-lpthread",
+             "-Xlinker", f"--version-script={vscript}"])
     cli_src = [os.path.join(SRC, "cli.cpp"), os.path.join(SRC, "mrc.cpp")]
     if force or _stale(CLI, [*cli_src, LIB, *hdrs]):
         run([cxx, "-O2", "-std=c++17", "-I", cuda_inc, *cli_src, "-o", CLI, LIB,

@@ -46,6 +46,7 @@ int phase_tables(const float2* sh, int items, int cmpX, int cmpY, float2* ex, fl
                  bool skip_small, cudaStream_t st) {
   const int n = cmpX > cmpY ? cmpX : cmpY;
   dim3 grid(ceil_div(n, 256), items);
+  prof::Scope ps("k_phase_tables", (double)items * (cmpX + cmpY) * 8.0, st);
   k_phase_tables<<<grid, 256, 0, st>>>(sh, cmpX, cmpY, ex, ey, skip_small ? 1 : 0);
   MC3_CHECK_LAUNCH("k_phase_tables");
   return kOk;
@@ -72,6 +73,7 @@ __global__ void k_phase_apply(const float2* in, float2* out, int cmpX, int cmpY,
 int phase_apply(const float2* in, float2* out, int cmpX, int cmpY, const float2* ex,
                 const float2* ey, bool accumulate, cudaStream_t st) {
   const long n = (long)cmpX * cmpY;
+  prof::Scope ps("k_phase_apply", (double)n * (accumulate ? 24.0 : 16.0), st);
   k_phase_apply<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(in, out, cmpX, cmpY, ex, ey,
                                                             accumulate ? 1 : 0);
   MC3_CHECK_LAUNCH("k_phase_apply");
@@ -106,6 +108,7 @@ int aligned_sum(const float2* spec, const int* act, const float2* ex, const floa
                 const AlignDims& d, cudaStream_t st) {
   const long nel = (long)d.cmpX * d.cmpY;
   dim3 grid((unsigned)((nel + 255) / 256), d.A);
+  prof::Scope ps("k_aligned_sum", (double)d.A * nel * 8.0 * (d.N + 1), st);
   k_aligned_sum<<<grid, 256, 0, st>>>(spec, act, ex, ey, S, d.cmpX, d.cmpY, d.N, d.stack_stride);
   MC3_CHECK_LAUNCH("k_aligned_sum");
   return kOk;
@@ -192,6 +195,7 @@ int corr_cols(const float2* spec, const int* act, const float2* ex, const float2
   if (smem > 200 * 1024) return kEUnsupported;
   MC3_TRY(set_smem_attr(k_corr_cols, smem));
   dim3 grid(ceil_div(d.cmpX, tx), d.G, d.A);
+  prof::Scope ps("k_corr_cols", (double)d.A * ((double)d.cmpX * d.cmpY * 8.0 * (d.N + 1) + (double)d.G * d.seaY * d.cmpX * 8.0), st);
   k_corr_cols<<<grid, 256, smem, st>>>(spec, act, ex, ey, S, gstart, gsize, bfactor, phase_only,
                                        T, d.cmpX, d.cmpY, d.N, d.stack_stride, d.G, d.seaY, tx, dH);
   MC3_CHECK_LAUNCH("k_corr_cols");
@@ -245,6 +249,7 @@ int corr_rows(const float2* T, float* win, const AlignDims& d, cudaStream_t st) 
   if (smem > 200 * 1024) return kEUnsupported;
   MC3_TRY(set_smem_attr(k_corr_rows, smem));
   dim3 grid(ceil_div(d.seaY, rows), d.G, d.A);
+  prof::Scope ps("k_corr_rows", (double)d.A * d.G * d.seaY * (d.cmpX * 8.0 + d.seaX * 4.0), st);
   k_corr_rows<<<grid, 256, smem, st>>>(T, win, d.cmpX, d.seaX, d.seaY, d.G, rows, dM);
   MC3_CHECK_LAUNCH("k_corr_rows");
   return kOk;
@@ -307,6 +312,7 @@ __global__ void k_peak(const float* win, float2* out, int seaX, int seaY, int G)
 
 int peak_search(const float* win, float2* out, const AlignDims& d, cudaStream_t st) {
   dim3 grid(d.G, d.A);
+  prof::Scope ps("k_peak", (double)d.A * d.G * d.seaX * d.seaY * 4.0, st);
   k_peak<<<grid, 256, 0, st>>>(win, out, d.seaX, d.seaY, d.G);
   MC3_CHECK_LAUNCH("k_peak");
   return kOk;

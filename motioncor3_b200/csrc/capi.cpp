@@ -5,7 +5,10 @@
 #include <new>
 #include <vector>
 
+#include <string>
+
 #include "engine.h"
+#include "profile.h"
 
 struct mc3_ctx {
   mc3::Engine* eng;
@@ -344,6 +347,20 @@ int mc3_dose_weighted_sums(mc3_ctx* ctx, const float* spectra, int nx, int ny, i
   if (n_sums) *n_sums = g.nSums;
   return MC3_OK;
 }
+
+// ---- diagnostics ----
+void mc3_profile_enable(int on) { prof::enable(on != 0); }
+
+int mc3_profile_read(char* buf, size_t len, int reset) {
+  if (!buf || len == 0) return MC3_EINVAL;
+  std::string s = prof::json();
+  if (reset) prof::reset();
+  if (s.size() + 1 > len) return MC3_EINVAL;
+  std::memcpy(buf, s.c_str(), s.size() + 1);
+  return MC3_OK;
+}
+
+unsigned long long mc3_kernel_launches(void) { return prof::launches(); }
 
 // ---- host bookkeeping ----
 void mc3_peak2d(const float* window, int sea_x, int sea_y, float* shift) {

@@ -5,6 +5,7 @@
 #include <cstdio>
 
 #include "fft_core.cuh"
+#include "profile.h"
 
 namespace mc3 {
 

@@ -42,6 +42,7 @@ __global__ void k_dose_norm(const float* acc, int N, int cmpX, int cmpY, float p
 int dose_norm(const float* acc_dose, int N, int cmpX, int cmpY, float pix, float kvf, float* Wn,
               cudaStream_t st) {
   const long n = (long)cmpX * cmpY;
+  prof::Scope ps("k_dose_norm", (double)n * 4.0, st);
   k_dose_norm<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(acc_dose, N, cmpX, cmpY, pix, kvf, Wn);
   MC3_CHECK_LAUNCH("k_dose_norm");
   return kOk;
@@ -87,6 +88,7 @@ int frame_sums(const float2* spec, long fr_stride, int N, int cmpX, int cmpY, co
                const float2* ey, const float* acc_dose, const float* Wn, const DoseParams& dp,
                float2* sums, int n_sums, cudaStream_t st) {
   const long n = (long)cmpX * cmpY;
+  prof::Scope ps("k_frame_sums", (double)n * (8.0 * (N + n_sums) + (dp.enabled ? 4.0 : 0.0)), st);
   k_frame_sums<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(spec, fr_stride, N, cmpX, cmpY, ex, ey,
                                                            acc_dose, Wn, dp, sums, n_sums);
   MC3_CHECK_LAUNCH("k_frame_sums");
@@ -133,6 +135,10 @@ __global__ void k_local_gather(const float* __restrict__ in, long in_stride, flo
     iy = (iy < 0) ? -iy : iy;
     ix = (811 * ix) % W;
     iy = (811 * iy) % H;
+    // Only non-finite shifts reach here out of range (the int conversion of
+    // NaN/inf); keep the read inside the frame.
+    if (ix < 0 || ix >= W) ix = 0;
+    if (iy < 0 || iy >= H) iy = 0;
   }
   const int padX = (W / 2 + 1) * 2;
   out[(long)b * out_stride + (long)y * padX + x] = in[(long)b * in_stride + (long)iy * padX + ix];
@@ -143,6 +149,7 @@ int local_gather(const float* in, long in_stride, float* out, long out_stride, i
                  cudaStream_t st) {
   // `shifts`/`bad` point at the first frame of the batch.
   dim3 grid(ceil_div(W, 256), H, nb);
+  prof::Scope ps("k_local_gather", (double)nb * W * H * 8.0, st);
   k_local_gather<<<grid, 256, 0, st>>>(in, in_stride, out, out_stride, W, H, centers, shifts, bad,
                                        P, 0);
   MC3_CHECK_LAUNCH("k_local_gather");
@@ -162,6 +169,7 @@ __global__ void k_unpad_positive(const float* in, long pitch, float* out, int W,
 int unpad_positive(const float* in, long pitch, float* out, int W, int H, int n, long in_stride,
                    cudaStream_t st) {
   dim3 grid(ceil_div(W, 256), H, n);
+  prof::Scope ps("k_unpad_positive", (double)n * W * H * 8.0, st);
   k_unpad_positive<<<grid, 256, 0, st>>>(in, pitch, out, W, H, in_stride);
   MC3_CHECK_LAUNCH("k_unpad_positive");
   return kOk;

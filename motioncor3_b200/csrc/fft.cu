@@ -185,6 +185,7 @@ int row_r2c(const float* in, long in_pitch, float2* out, long out_pitch, int W, 
   if (smem > 200 * 1024) return kEUnsupported;
   MC3_TRY(set_smem_attr(k_row_r2c, smem));
   dim3 grid(ceil_div(H, rows), b.items);
+  prof::Scope ps("k_row_r2c", (double)b.items * H * (W * 4.0 + (W / 2 + 1) * 8.0), st);
   k_row_r2c<<<grid, 256, smem, st>>>(in, in_pitch, out, out_pitch, W, H, rows, b, d, scale);
   MC3_CHECK_LAUNCH("k_row_r2c");
   return kOk;
@@ -201,6 +202,7 @@ int row_c2r(const float2* in, long in_pitch, float* out, long out_pitch, int W, 
   if (smem > 200 * 1024) return kEUnsupported;
   MC3_TRY(set_smem_attr(k_row_c2r, smem));
   dim3 grid(ceil_div(H, rows), b.items);
+  prof::Scope ps("k_row_c2r", (double)b.items * H * (W * 4.0 + (W / 2 + 1) * 8.0), st);
   k_row_c2r<<<grid, 256, smem, st>>>(in, in_pitch, out, out_pitch, W, H, rows, b, d);
   MC3_CHECK_LAUNCH("k_row_c2r");
   return kOk;
@@ -217,6 +219,7 @@ int col_fft(const float2* in, float2* out, long pitch, int cmpX, int H, const Ba
   if (smem > 200 * 1024) return kEUnsupported;
   MC3_TRY(set_smem_attr(k_col_fft, smem));
   dim3 grid(ceil_div(cmpX, tx), b.items);
+  prof::Scope ps("k_col_fft", (double)b.items * ((double)cmpX * H * 16.0 + (ops.crop ? (double)ops.crop_x * ops.crop_y * 8.0 : 0.0)), st);
   k_col_fft<<<grid, 256, smem, st>>>(in, out, pitch, cmpX, H, tx, b, d, ops);
   MC3_CHECK_LAUNCH("k_col_fft");
   return kOk;

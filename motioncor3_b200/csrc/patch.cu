@@ -25,6 +25,7 @@ __global__ void k_fourier_crop(const float2* in, int inX, int inY, float2* out, 
 int fourier_crop(const float2* in, int inX, int inY, float2* out, int outX, int outY,
                  cudaStream_t st) {
   dim3 grid(ceil_div(outX, 128), outY);
+  prof::Scope ps("k_fourier_crop", (double)outX * outY * 16.0, st);
   k_fourier_crop<<<grid, 128, 0, st>>>(in, inX, inY, out, outX, outY);
   MC3_CHECK_LAUNCH("k_fourier_crop");
   return kOk;
@@ -93,13 +94,20 @@ __global__ void k_copy_unpad(const float* in, long pitch, float* out, int bx, in
 int feature_map(float* img, int bx, int by, float* tmp, float* d_part, float* d_scal,
                 float* map_out, cudaStream_t st) {
   const long pitch = 2 * (bx / 2 + 1);
+  {
+  prof::Scope ps("k_min_add", (double)pitch * by * 8.0, st);
   k_min_add<<<1, 256, 0, st>>>(img, bx, by, pitch, d_scal);
   MC3_CHECK_LAUNCH("k_min_add");
+  }
   dim3 grid(ceil_div(bx, 128), by);
+  {
+  prof::Scope ps("k_norm_by_std", (double)pitch * by * 8.0, st);
   k_norm_by_std<<<grid, 128, 0, st>>>(img, tmp, bx, by, pitch, 5, 5);
   MC3_CHECK_LAUNCH("k_norm_by_std");
+  }
   MC3_TRY(image_moment(tmp, bx, by, pitch, 1, d_part, d_scal + 1, st));
   MC3_TRY(image_moment(tmp, bx, by, pitch, 2, d_part, d_scal + 2, st));
+  prof::Scope ps("k_copy_unpad", (double)bx * by * 8.0, st);
   k_copy_unpad<<<ceil_div(bx * by, 256), 256, 0, st>>>(tmp, pitch, map_out, bx, by);
   MC3_CHECK_LAUNCH("k_copy_unpad");
   return kOk;

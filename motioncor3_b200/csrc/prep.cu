@@ -31,6 +31,8 @@ int gain_and_sum(const void* raw, int mode, long raw_stride, const float* gain, 
                  long fr_stride, float* sum, int W, int H, int N, cudaStream_t st) {
   const int padX = 2 * (W / 2 + 1);
   dim3 grid(ceil_div(W, 256), H);
+  const int bpp = mode == 0 ? 1 : (mode == 2 ? 4 : 2);
+  prof::Scope ps("k_gain_sum", (double)W * H * (N * (bpp + 4.0) + (gain ? 4.0 : 0.0) + (sum ? 4.0 : 0.0)), st);
   switch (mode) {
     case 0: k_gain_sum<uint8_t><<<grid, 256, 0, st>>>((const uint8_t*)raw, raw_stride, gain, frames, fr_stride, sum, W, H, N, padX); break;
     case 1: k_gain_sum<int16_t><<<grid, 256, 0, st>>>((const int16_t*)raw, raw_stride, gain, frames, fr_stride, sum, W, H, N, padX); break;
@@ -91,8 +93,12 @@ int moment_grid(int W, int H) {
 int image_moment(const float* img, int W, int H, long pitch, int iExp, float* d_part,
                  float* d_out, cudaStream_t st) {
   const int g = moment_grid(W, H);
+  {
+  prof::Scope ps("k_moment_partial", (double)W * H * 4.0, st);
   k_moment_partial<<<g, 512, 512 * sizeof(float), st>>>(img, W, H, pitch, iExp, d_part);
   MC3_CHECK_LAUNCH("k_moment_partial");
+  }
+  prof::Scope ps2("k_moment_final", g * 4.0, st);
   k_moment_final<<<1, g, g * sizeof(float), st>>>(d_part, d_out);
   MC3_CHECK_LAUNCH("k_moment_final");
   return kOk;
@@ -168,13 +174,20 @@ int detect_bad_pixels(const float* sum, int W, int H, float* cc_buf, float* d_pa
   MC3_TRY(image_moment(sum, W, H, pitch, 1, d_part, d_mom + 0, st));
   MC3_TRY(image_moment(sum, W, H, pitch, 2, d_part, d_mom + 1, st));
   dim3 grid(ceil_div(W, 256), H);
+  {
+  prof::Scope ps("k_detect_hot", (double)W * H * 5.0, st);
   k_detect_hot<<<grid, 256, 0, st>>>(sum, pitch, W, H, d_mom, 6.0f, bad);
   MC3_CHECK_LAUNCH("k_detect_hot");
+  }
   MC3_CUDA(cudaMemcpyToSymbolAsync(c_tpl, tpl, sizeof(float) * ms * ms, 0, cudaMemcpyHostToDevice, st));
+  {
+  prof::Scope ps("k_local_cc", (double)W * H * 8.0, st);
   k_local_cc<<<grid, 256, 0, st>>>(sum, pitch, W, H, ms, cc_buf);
   MC3_CHECK_LAUNCH("k_local_cc");
+  }
   MC3_TRY(image_moment(cc_buf, W, H, pitch, 1, d_part, d_mom + 2, st));
   MC3_TRY(image_moment(cc_buf, W, H, pitch, 2, d_part, d_mom + 3, st));
+  prof::Scope ps("k_mark_defects", (double)W * H * 4.0, st);
   k_mark_defects<<<grid, 256, 0, st>>>(cc_buf, pitch, W, H, d_mom + 2, 6.0f, ms, bad);
   MC3_CHECK_LAUNCH("k_mark_defects");
   return kOk;
@@ -218,6 +231,7 @@ int correct_bad_pixels(float* frames, long fr_stride, int N, const uint8_t* bad,
                        cudaStream_t st) {
   const int padX = 2 * (W / 2 + 1);
   dim3 grid(ceil_div(W, 256), H, N);
+  prof::Scope ps("k_correct_bad", (double)W * H, st);
   k_correct_bad<<<grid, 256, 0, st>>>(frames, fr_stride, bad, W, H, padX, 31);
   MC3_CHECK_LAUNCH("k_correct_bad");
   return kOk;

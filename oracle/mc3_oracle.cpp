@@ -975,6 +975,8 @@ void local_gather(const double* in, double* out, int W, int H, const float* cent
         iy = iy < 0 ? -iy : iy;
         ix = (811 * ix) % W;
         iy = (811 * iy) % H;
+        if (ix < 0 || ix >= W) ix = 0;  // non-finite shifts only
+        if (iy < 0 || iy >= H) iy = 0;
       }
       out[(long)y * W + x] = in[(long)iy * W + ix];
     }
@@ -1152,13 +1154,17 @@ int oracle_process_movie(const oracle_params* p, const float* frames, int W, int
   for (int f = 0; f < N; ++f)
     fourier_resize(&spec[(long)f * ncmp], g.cmpX, g.cmpY, &xcf[(long)f * nx], g.xcfCmpX, g.xcfCmpY);
   // ---- global alignment (Align/CFullAlign.cpp:70-164) ----
+  const bool forced = out->use_global_shifts != nullptr;
   const float bin = std::fmax(g.xcfBin[0], g.xcfBin[1]);
   const float tol = p->tol / bin;
   Groups G0 = make_groups(N, p->group[0]);
-  AlignResult ga = iterative_align(xcf.data(), g.xcfCmpX, g.xcfCmpY, N, G0, p->iter, tol,
-                                   p->bft[0], p->phase_only != 0);
-  Shifts xs = ga.shifts;  // xcf units
-  if (out->iterations) out->iterations[0] = ga.iterations;
+  Shifts xs(N);  // xcf units
+  if (!forced) {
+    AlignResult ga = iterative_align(xcf.data(), g.xcfCmpX, g.xcfCmpY, N, G0, p->iter, tol,
+                                     p->bft[0], p->phase_only != 0);
+    xs = ga.shifts;
+    if (out->iterations) out->iterations[0] = ga.iterations;
+  }
 
   const bool patchMode = g.patch;
   std::vector<float> patCent, patShift;
@@ -1166,7 +1172,7 @@ int oracle_process_movie(const oracle_params* p, const float* frames, int W, int
   const int P = patchMode ? g.Px * g.Py : 0;
   std::vector<double> xreal;
   std::vector<int> patStart;
-  if (patchMode) {
+  if (patchMode && !forced) {
     // CDetectFeatures::DoIt on the aligned xcf sum (CFullAlign.cpp:147-159)
     std::vector<cd> xsum(nx, cd(0.0));
     for (int f = 0; f < N; ++f)
@@ -1206,7 +1212,17 @@ int oracle_process_movie(const oracle_params* p, const float* frames, int W, int
   }
   for (int i = 0; i < 2 * N; ++i) fs.v[i] = 0.01f * (int)(fs.v[i] * 100);
 
-  if (patchMode) {
+  if (forced) {
+    for (int i = 0; i < N; ++i) {
+      fs.x(i) = out->use_global_shifts[2 * i];
+      fs.y(i) = out->use_global_shifts[2 * i + 1];
+    }
+    if (patchMode) {
+      patShift.assign(out->use_patch_shifts, out->use_patch_shifts + (size_t)N * P * 2);
+      patCent.assign(out->use_patch_centers, out->use_patch_centers + (size_t)P * 2);
+      patBad.assign(out->use_patch_bad, out->use_patch_bad + (size_t)N * P);
+    }
+  } else if (patchMode) {
     // CPatchAlign::mCorrectFullShift (Align/CPatchAlign.cpp:47-65)
     int ref = p->fm_ref < 0 ? N / 2 : std::min(std::max(p->fm_ref - 1, 0), N - 1);
     float rx = fs.x(ref), ry = fs.y(ref);

@@ -49,6 +49,14 @@ typedef struct {
   unsigned char* patch_bad; /* [N][P]                                     */
   int* iterations;        /* [1 + P] iterations run (global, each patch)  */
   unsigned char* bad_map; /* [H][W] detected bad pixels, may be NULL      */
+  /* Optional inputs: when use_global_shifts is set, alignment is skipped and
+   * the movie is corrected with these shifts (as logged: absolute in global
+   * mode, relative to the reference frame in patch mode) and, in patch
+   * mode, with the given local shifts, centres and bad flags. */
+  const float* use_global_shifts;     /* [N][2]    */
+  const float* use_patch_shifts;      /* [N][P][2] */
+  const float* use_patch_centers;     /* [P][2]    */
+  const unsigned char* use_patch_bad; /* [N][P]    */
 } oracle_result;
 
 void oracle_default_params(oracle_params* p);

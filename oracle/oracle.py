@@ -1,0 +1,263 @@
+"""ctypes binding of the FP64 CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Imported only by tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline / reference arm.  Builds oracle/_build/libmc3_oracle.so with the
+Makefile beside this file when it is missing or stale, and the reference
+host-code checker oracle/_ref/libmc3ref_host.so when the reference tree is
+present (the prebuilt .so is used otherwise).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "libmc3_oracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libmc3ref_host.so")
+REF_TREE = "/root/reference"
+_VP = ctypes.c_void_p
+
+
+def _cxx_env():
+    env = dict(os.environ)
+    if os.path.exists("/usr/bin/g++"):
+        env["CXX"] = "/usr/bin/g++"
+    return env
+
+
+def build() -> str:
+    srcs = [os.path.join(HERE, f) for f in ("mc3_oracle.cpp", "mc3_oracle.h", "Makefile")]
+    if not os.path.exists(LIB) or any(os.path.getmtime(s) > os.path.getmtime(LIB) for s in srcs):
+        subprocess.run(["make", "-C", HERE], check=True, env=_cxx_env(), capture_output=True)
+    return LIB
+
+
+def build_ref_host() -> str | None:
+    """Compiles the reference's own host classes when the reference tree exists."""
+    if os.path.isdir(REF_TREE):
+        d = os.path.join(HERE, "ref_host")
+        subprocess.run(["make", "-C", d, f"REF={REF_TREE}"], check=True, capture_output=True)
+    return REF_LIB if os.path.exists(REF_LIB) else None
+
+
+class OracleParams(ctypes.Structure):
+    _fields_ = [
+        ("patch", ctypes.c_int * 2),
+        ("iter", ctypes.c_int),
+        ("tol", ctypes.c_float),
+        ("bft", ctypes.c_float * 2),
+        ("phase_only", ctypes.c_int),
+        ("fm_dose", ctypes.c_float),
+        ("pix_size", ctypes.c_float),
+        ("kv", ctypes.c_int),
+        ("group", ctypes.c_int * 2),
+        ("fm_ref", ctypes.c_int),
+        ("sum_range", ctypes.c_float * 2),
+        ("correct_bad", ctypes.c_int),
+    ]
+
+
+class OracleResult(ctypes.Structure):
+    _fields_ = [
+        ("n_sums", ctypes.c_int),
+        ("sums", _VP),
+        ("global_shifts", _VP),
+        ("n_patches", ctypes.c_int),
+        ("patch_shifts", _VP),
+        ("patch_centers", _VP),
+        ("patch_bad", _VP),
+        ("iterations", _VP),
+        ("bad_map", _VP),
+        ("use_global_shifts", _VP),
+        ("use_patch_shifts", _VP),
+        ("use_patch_centers", _VP),
+        ("use_patch_bad", _VP),
+    ]
+
+
+_L = None
+
+
+def lib() -> ctypes.CDLL:
+    global _L
+    if _L is None:
+        _L = ctypes.CDLL(build())
+    return _L
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_VP)
+
+
+def params(**kw) -> OracleParams:
+    p = OracleParams()
+    lib().oracle_default_params(ctypes.byref(p))
+    for k, v in kw.items():
+        if k in ("patch", "bft", "group", "sum_range"):
+            arr = getattr(p, k)
+            for i, x in enumerate(v[:2]):
+                arr[i] = x
+        else:
+            setattr(p, k, v)
+    return p
+
+
+def process_movie(frames: np.ndarray, gain=None, force=None, **kw) -> dict:
+    """Runs the whole oracle path.  `force` may hold global_shifts (and
+    patch_shifts / patch_centers / patch_bad) to correct with given shifts."""
+    p = params(**kw)
+    nz, ny, nx = frames.shape
+    fr = np.ascontiguousarray(frames, np.float32)
+    g = None if gain is None else np.ascontiguousarray(gain, np.float32)
+    P = (p.patch[0] * p.patch[1]) if (p.patch[0] > 1 and p.patch[1] > 1) else 0
+    sums = np.zeros((3, ny, nx), np.float32)
+    gsh = np.zeros((nz, 2), np.float32)
+    psh = np.zeros((nz, max(P, 1), 2), np.float32)
+    pc = np.zeros((max(P, 1), 2), np.float32)
+    pb = np.zeros((nz, max(P, 1)), np.uint8)
+    its = np.zeros(1 + P, np.int32)
+    bad = np.zeros((ny, nx), np.uint8)
+    r = OracleResult()
+    r.sums = sums.ctypes.data
+    r.global_shifts = gsh.ctypes.data
+    r.patch_shifts = psh.ctypes.data
+    r.patch_centers = pc.ctypes.data
+    r.patch_bad = pb.ctypes.data
+    r.iterations = its.ctypes.data
+    r.bad_map = bad.ctypes.data
+    keep = []
+    if force:
+        for key in ("global_shifts", "patch_shifts", "patch_centers", "patch_bad"):
+            if force.get(key) is not None:
+                dt = np.uint8 if key == "patch_bad" else np.float32
+                a = np.ascontiguousarray(force[key], dt)
+                keep.append(a)
+                setattr(r, "use_" + key, a.ctypes.data)
+    rc = lib().oracle_process_movie(ctypes.byref(p), _p(fr), nx, ny, nz, _p(g), ctypes.byref(r))
+    if rc != 0:
+        raise RuntimeError(f"oracle_process_movie failed ({rc})")
+    return dict(sums=sums[: r.n_sums], global_shifts=gsh, patch_shifts=psh if P else None,
+                patch_centers=pc if P else None, patch_bad=pb if P else None, iterations=its,
+                bad_map=bad, n_sums=r.n_sums)
+
+
+def rfft2(img: np.ndarray, normalise: bool = True) -> np.ndarray:
+    ny, nx = img.shape
+    a = np.ascontiguousarray(img, np.float64)
+    out = np.zeros((ny, nx // 2 + 1), np.complex128)
+    lib().oracle_rfft2(_p(a), _p(out), nx, ny, int(normalise))
+    return out
+
+
+def irfft2(spec: np.ndarray, nx: int) -> np.ndarray:
+    ny = spec.shape[0]
+    a = np.ascontiguousarray(spec, np.complex128)
+    out = np.zeros((ny, nx), np.float64)
+    lib().oracle_irfft2(_p(a), _p(out), nx, ny)
+    return out
+
+
+def cfft(x: np.ndarray, direction: int) -> np.ndarray:
+    a = np.ascontiguousarray(x, np.complex128)
+    out = np.zeros_like(a)
+    lib().oracle_cfft(_p(a), _p(out), len(a), direction)
+    return out
+
+
+def detect_bad(sum_img: np.ndarray) -> np.ndarray:
+    ny, nx = sum_img.shape
+    a = np.ascontiguousarray(sum_img, np.float64)
+    bad = np.zeros((ny, nx), np.uint8)
+    lib().oracle_detect_bad(_p(a), nx, ny, _p(bad))
+    return bad
+
+
+def correct_bad(frame: np.ndarray, bad: np.ndarray) -> np.ndarray:
+    ny, nx = frame.shape
+    a = np.ascontiguousarray(frame, np.float64).copy()
+    b = np.ascontiguousarray(bad, np.uint8)
+    lib().oracle_correct_bad(_p(a), _p(b), nx, ny)
+    return a
+
+
+def correlate_window(grp: np.ndarray, sum_: np.ndarray, bfactor: float, phase_only=0, sea=(64, 64)):
+    cy, cx = grp.shape
+    g = np.ascontiguousarray(grp, np.complex128)
+    s = np.ascontiguousarray(sum_, np.complex128)
+    win = np.zeros((sea[1], sea[0]), np.float32)
+    lib().oracle_correlate_window(_p(g), _p(s), cx, cy, ctypes.c_float(bfactor), phase_only, sea[0],
+                                  sea[1], _p(win))
+    return win
+
+
+def peak2d(win: np.ndarray) -> np.ndarray:
+    w = np.ascontiguousarray(win, np.float32)
+    out = np.zeros(2, np.float32)
+    lib().oracle_peak2d(_p(w), w.shape[1], w.shape[0], _p(out))
+    return out
+
+
+def iterative_align(spec: np.ndarray, group: int, max_iter: int, tol: float, bfactor: float,
+                    phase_only: int = 0):
+    n, cy, cx = spec.shape
+    s = np.ascontiguousarray(spec, np.complex128)
+    out = np.zeros((n, 2), np.float32)
+    it = lib().oracle_iterative_align(_p(s), cx, cy, n, group, max_iter, ctypes.c_float(tol),
+                                      ctypes.c_float(bfactor), phase_only, _p(out))
+    return out, it
+
+
+def local_gather(img: np.ndarray, centers, shifts, bad=None) -> np.ndarray:
+    ny, nx = img.shape
+    a = np.ascontiguousarray(img, np.float64)
+    out = np.zeros_like(a)
+    c = np.ascontiguousarray(centers, np.float32)
+    s = np.ascontiguousarray(shifts, np.float32)
+    b = None if bad is None else np.ascontiguousarray(bad, np.uint8)
+    lib().oracle_local_gather(_p(a), _p(out), nx, ny, _p(c), _p(s), _p(b), len(c))
+    return out
+
+
+def dose_weights(acc_dose, frame: int, cmpx: int, cmpy: int, pix: float, kv: int) -> np.ndarray:
+    acc = np.ascontiguousarray(acc_dose, np.float32)
+    out = np.zeros((cmpy, cmpx), np.float64)
+    lib().oracle_dose_weights(_p(acc), len(acc), frame, cmpx, cmpy, ctypes.c_float(pix), kv, _p(out))
+    return out
+
+
+def remove_spikes(sx, sy):
+    x = np.ascontiguousarray(sx, np.float32).copy()
+    y = np.ascontiguousarray(sy, np.float32).copy()
+    lib().oracle_remove_spikes(_p(x), _p(y), len(x))
+    return x, y
+
+
+def lin_eqs(a, b):
+    A = np.ascontiguousarray(a, np.float32).copy()
+    B = np.ascontiguousarray(b, np.float32).copy()
+    ok = lib().oracle_lin_eqs(_p(A), _p(B), len(B))
+    return bool(ok), B
+
+
+def patch_make_relative(shifts):
+    s = np.ascontiguousarray(shifts, np.float32).copy()
+    lib().oracle_patch_make_relative(_p(s), s.shape[0], s.shape[1])
+    return s
+
+
+def patch_detect_bads(shifts, centers, nx, ny):
+    s = np.ascontiguousarray(shifts, np.float32)
+    c = np.ascontiguousarray(centers, np.float32)
+    bad = np.zeros(s.shape[:2], np.uint8)
+    lib().oracle_patch_detect_bads(_p(s), _p(c), s.shape[0], s.shape[1], nx, ny, _p(bad))
+    return bad
+
+
+def ref_host():
+    """The reference's own host classes (None when neither the tree nor the
+    prebuilt checker is available)."""
+    path = build_ref_host()
+    return ctypes.CDLL(path) if path else None

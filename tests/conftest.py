@@ -1,0 +1,76 @@
+"""Shared fixtures.  `gpu` marks tests that need a CUDA device; everything
+else runs on the CPU (oracle, reference-host checker, host bookkeeping,
+symbol checks)."""
+import ctypes
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (runs on the B200 box)")
+
+
+@pytest.fixture(scope="session")
+def mc3lib():
+    from motioncor3_b200 import build
+    build.build()
+    from motioncor3_b200 import api
+    return api._lib()
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    from oracle import oracle as O
+    O.lib()
+    return O
+
+
+@pytest.fixture(scope="session")
+def ref_host():
+    from oracle import oracle as O
+    L = O.ref_host()
+    if L is None:
+        pytest.skip("reference host checker not available")
+    P = ctypes.c_void_p
+    L.ref_interpolate.restype = ctypes.c_int
+    L.ref_lin_eqs.restype = ctypes.c_int
+    return L
+
+
+@pytest.fixture(scope="session")
+def shim():
+    out_dir = os.path.join(ROOT, "tests", "_build")
+    os.makedirs(out_dir, exist_ok=True)
+    so = os.path.join(out_dir, "fft_core_shim.so")
+    src = os.path.join(ROOT, "tests", "native", "fft_core_shim.cpp")
+    hdr = os.path.join(ROOT, "motioncor3_b200", "csrc", "fft_core.cuh")
+    if not os.path.exists(so) or os.path.getmtime(so) < max(os.path.getmtime(src), os.path.getmtime(hdr)):
+        cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+        subprocess.run([cxx, "-O2", "-shared", "-fPIC", "-I/usr/local/cuda/include", src, "-o", so],
+                       check=True)
+    return ctypes.CDLL(so)
+
+
+@pytest.fixture(scope="session")
+def torch_cuda():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def fp(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+@pytest.fixture
+def rng():
+    return np.random.default_rng(1234)

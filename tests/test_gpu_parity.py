@@ -1,0 +1,215 @@
+"""GPU parity: every libmc3 kernel and the whole path against the FP64
+oracle (and numpy / cuFFT for the transforms).  Tolerances: FFTs 2e-6
+relative to the spectrum maximum; correlation windows 1e-4 relative; shifts
+within 0.05 px; sums within 1e-4 relative RMS; integer / gather work exact."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel_rms(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.sqrt(np.mean((a - b) ** 2)) / np.sqrt(np.mean(b ** 2)))
+
+
+@pytest.fixture(scope="module")
+def api(mc3lib, torch_cuda):
+    from motioncor3_b200 import api as A
+    return A
+
+
+@pytest.mark.parametrize("ny,nx", [(64, 64), (256, 256), (408, 408), (408, 410), (1024, 1024),
+                                   (2048, 2048), (4096, 4096), (4092, 5760)])
+def test_fft_forward_inverse(api, torch_cuda, ny, nx):
+    torch = torch_cuda
+    rng = np.random.default_rng(nx + ny)
+    nz = 2
+    img = rng.standard_normal((nz, ny, nx)).astype(np.float32)
+    cx = nx // 2 + 1
+    buf = torch.zeros((nz, ny, 2 * cx), dtype=torch.float32, device="cuda")
+    buf[:, :, :nx] = torch.from_numpy(img).cuda()
+    api.fft_forward(buf, nx, ny, normalise=True)
+    torch.cuda.synchronize()
+    spec = torch.view_as_complex(buf.view(nz, ny, cx, 2)).cpu().numpy()
+    ref = np.fft.rfft2(img.astype(np.float64)) / (nx * ny)
+    assert np.abs(spec - ref).max() / np.abs(ref).max() < 2e-6
+    # non-Hermitian input to the inverse: cuFFT (torch) and numpy agree on it
+    half = (rng.standard_normal((nz, ny, cx)) + 1j * rng.standard_normal((nz, ny, cx))).astype(np.complex64)
+    hb = torch.view_as_real(torch.from_numpy(half).cuda()).reshape(nz, ny, 2 * cx).contiguous()
+    api.fft_inverse(hb, nx, ny)
+    torch.cuda.synchronize()
+    out = hb[:, :, :nx].cpu().numpy()
+    refb = np.fft.irfft2(half.astype(np.complex128), s=(ny, nx)) * nx * ny
+    assert np.abs(out - refb).max() / np.abs(refb).max() < 2e-6
+    cu = torch.fft.irfft2(torch.from_numpy(half).cuda(), s=(ny, nx), norm="forward").cpu().numpy()
+    assert np.abs(out - cu).max() / np.abs(cu).max() < 2e-6
+
+
+def test_phase_shift(api, torch_cuda):
+    torch = torch_cuda
+    rng = np.random.default_rng(2)
+    cy, cx = 128, 65
+    X = (rng.standard_normal((cy, cx)) + 1j * rng.standard_normal((cy, cx))).astype(np.complex64)
+    src = torch.from_numpy(X).cuda()
+    dst = torch.zeros_like(src)
+    sx, sy = 3.37, -7.81
+    api.phase_shift(src, dst, sx, sy)
+    torch.cuda.synchronize()
+    kx = np.arange(cx)[None, :]
+    ky = np.fft.fftfreq(cy, 1.0 / cy)[:, None]
+    ky = np.where(np.arange(cy)[:, None] > cy // 2, np.arange(cy)[:, None] - cy, np.arange(cy)[:, None])
+    ref = X * np.exp(2j * np.pi * (kx * sx / ((cx - 1) * 2) + ky * sy / cy))
+    assert np.abs(dst.cpu().numpy() - ref).max() < 1e-5 * np.abs(ref).max()
+    api.phase_shift(src, dst, sx, sy, accumulate=True)
+    torch.cuda.synchronize()
+    assert np.abs(dst.cpu().numpy() - 2 * ref).max() < 2e-5 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("cy,cx,phase_only", [(256, 129, 0), (408, 205, 0), (512, 257, 1)])
+def test_correlate_window_and_peak(api, oracle, torch_cuda, cy, cx, phase_only):
+    torch = torch_cuda
+    from motioncor3_b200 import synthetic as S
+    rng = np.random.default_rng(cy)
+    nx = (cx - 1) * 2
+    truth = S.truth_image(nx, cy, rng, n_blobs=60)
+    a = rng.poisson(4 * truth).astype(np.float64)
+    b = rng.poisson(4 * np.roll(truth, (3, -5), (0, 1))).astype(np.float64)
+    G = oracle.rfft2(a) * 1.0
+    Sm = oracle.rfft2(a) + oracle.rfft2(b)
+    win_o = oracle.correlate_window(G, Sm, 150.0, phase_only)
+    sh_o = oracle.peak2d(win_o)
+    g = torch.from_numpy(G.astype(np.complex64)).cuda()
+    s = torch.from_numpy(Sm.astype(np.complex64)).cuda()
+    win = torch.zeros((64, 64), dtype=torch.float32, device="cuda")
+    sh = api.correlate(g, s, 150.0, phase_only, (64, 64), win)
+    w = win.cpu().numpy()
+    assert np.abs(w - win_o).max() < 1e-4 * np.abs(win_o).max()
+    assert np.abs(sh - sh_o).max() < 0.01
+    assert np.allclose(np.abs(sh_o), [5, 3], atol=0.6)
+
+
+def test_bad_pixel_detection_and_fill(api, oracle, torch_cuda):
+    torch = torch_cuda
+    rng = np.random.default_rng(9)
+    ny, nx, nz = 200, 256, 3
+    frames = rng.poisson(20.0, (nz, ny, nx)).astype(np.float32)
+    frames[:, 50, 60] = 400.0            # hot pixel
+    frames[:, 120:126, 30:36] = 2.0      # dark defect block
+    frames[:, 128:130, 31:33] = 90.0
+    total = frames.astype(np.float64).sum(0)
+    bad_o = oracle.detect_bad(total)
+    cx = nx // 2 + 1
+    pad = torch.zeros((nz, ny, 2 * cx), dtype=torch.float32, device="cuda")
+    pad[:, :, :nx] = torch.from_numpy(frames).cuda()
+    ssum = torch.zeros((ny, 2 * cx), dtype=torch.float32, device="cuda")
+    ssum[:, :nx] = torch.from_numpy(frames.sum(0)).cuda()
+    bad = torch.zeros((ny, nx), dtype=torch.uint8, device="cuda")
+    api.detect_bad_pixels(ssum, nx, ny, bad)
+    bad_g = bad.cpu().numpy()
+    assert bad_o[50, 60] == 1 and bad_o.sum() > 1
+    assert np.array_equal(bad_g, bad_o)
+    api.correct_bad_pixels(pad, nx, ny, bad)
+    torch.cuda.synchronize()
+    got = pad[:, :, :nx].cpu().numpy()
+    for f in range(nz):
+        ref = oracle.correct_bad(frames[f], bad_o)
+        assert np.array_equal(got[f], ref.astype(np.float32))
+
+
+def test_local_gather_exact(api, oracle, torch_cuda):
+    torch = torch_cuda
+    rng = np.random.default_rng(4)
+    ny, nx, P = 384, 512, 9
+    img = rng.standard_normal((ny, nx)).astype(np.float32)
+    cen = np.array([[(i % 3 + 0.5) * nx / 3 + rng.normal(0, 9), (i // 3 + 0.5) * ny / 3 + rng.normal(0, 9)]
+                    for i in range(P)], np.float32)
+    sh = rng.normal(0, 2.5, (P, 2)).astype(np.float32)
+    bad = np.zeros(P, np.uint8)
+    bad[4] = 1
+    ref = oracle.local_gather(img, cen, sh, bad)
+    cx = nx // 2 + 1
+    src = torch.zeros((ny, 2 * cx), dtype=torch.float32, device="cuda")
+    src[:, :nx] = torch.from_numpy(img).cuda()
+    dst = torch.zeros_like(src)
+    api.local_gather(src, dst, nx, ny, torch.from_numpy(cen).cuda(), torch.from_numpy(sh).cuda(),
+                     torch.from_numpy(bad).cuda())
+    torch.cuda.synchronize()
+    got = dst[:, :nx].cpu().numpy()
+    mism = np.mean(got != ref.astype(np.float32))
+    assert mism < 1e-4, mism
+
+
+def test_iterative_align_component(api, oracle, torch_cuda):
+    torch = torch_cuda
+    from motioncor3_b200 import synthetic as S
+    m = S.make_movie(256, 256, 14, dose=5.0, seed=21)
+    spec = np.stack([oracle.rfft2(f.astype(np.float64)) for f in m.frames])
+    ref, it_o = oracle.iterative_align(spec, 1, 8, 0.05, 150.0)
+    with api.MotionCor3(api.Params()) as mc:
+        t = torch.from_numpy(spec.astype(np.complex64)).cuda()
+        got, it_g = mc.iterative_align(t, 1, 8, 0.05, 150.0)
+    assert it_g == it_o
+    assert np.abs(got - ref).max() <= 0.05
+
+
+def _compare_movie(api, oracle, movie, params, forced_sum_tol=1e-4):
+    """Runs the GPU path and the oracle on the same raw frames: shifts within
+    0.05 px and sums (oracle corrected with the GPU's shifts) within 1e-4."""
+    kw = dict(patch=params.patch[:2], iter=params.iter, tol=params.tol, bft=params.bft,
+              fm_dose=params.fm_dose, pix_size=params.pix_size, kv=params.kv, group=params.group)
+    with api.MotionCor3(params) as mc:
+        if movie.gain is not None:
+            mc.set_gain(np.asarray(movie.gain))
+        res = mc.process(np.asarray(movie.frames))
+    orc = oracle.process_movie(np.asarray(movie.frames),
+                               gain=None if movie.gain is None else np.asarray(movie.gain), **kw)
+    assert res.n_sums == orc["n_sums"]
+    dg = np.abs(res.global_shifts - orc["global_shifts"]).max()
+    assert dg <= 0.05, dg
+    force = dict(global_shifts=res.global_shifts)
+    if res.n_patches:
+        assert np.abs(res.patch_shifts - orc["patch_shifts"]).max() <= 0.05
+        assert np.array_equal(res.patch_centers, orc["patch_centers"])
+        force.update(patch_shifts=res.patch_shifts, patch_centers=res.patch_centers,
+                     patch_bad=res.patch_bad)
+    same = oracle.process_movie(np.asarray(movie.frames),
+                                gain=None if movie.gain is None else np.asarray(movie.gain),
+                                force=force, **kw)
+    for s in range(res.n_sums):
+        e = _rel_rms(res.sums[s], same["sums"][s])
+        assert e <= forced_sum_tol, (s, e)
+    return res, orc
+
+
+def test_pipeline_global_small(api, oracle, torch_cuda):
+    from motioncor3_b200 import synthetic as S
+    m = S.make_movie(256, 256, 16, dose=4.0, seed=31)
+    p = api.Params(iter=7, tol=0.5, bft=(150, 100), pix_size=1.0)
+    _compare_movie(api, oracle, m, p)
+
+
+def test_pipeline_global_dose_weighted_gain(api, oracle, torch_cuda):
+    from motioncor3_b200 import synthetic as S
+    m = S.make_movie(384, 320, 12, dose=3.0, seed=32, gain=True)
+    p = api.Params(iter=6, tol=0.2, bft=(300, 100), fm_dose=1.2, pix_size=0.9, kv=300)
+    res, _ = _compare_movie(api, oracle, m, p)
+    assert res.n_sums == 3
+
+
+def test_pipeline_patch_small(api, oracle, torch_cuda):
+    from motioncor3_b200 import synthetic as S
+    m = S.make_movie(512, 512, 12, dose=4.0, seed=33, gain=True, local=True)
+    p = api.Params(patch=(3, 3), iter=5, tol=0.2, bft=(500, 150), fm_dose=1.0, pix_size=1.0, kv=300)
+    res, _ = _compare_movie(api, oracle, m, p)
+    assert res.n_patches == 9
+
+
+def test_pipeline_config1_full_size(api, oracle, torch_cuda):
+    """40 frames of 1024x1024, global alignment only (-Patch 0 0 -Iter 7
+    -Tol 0.5 -Bft 150 -PixSize 1.0), dose 1 e/px/frame, unit gain."""
+    from motioncor3_b200 import synthetic as S
+    m = S.make_movie(1024, 1024, 40, dose=1.0, seed=101)
+    p = api.Params(iter=7, tol=0.5, bft=(150, 100), pix_size=1.0)
+    _compare_movie(api, oracle, m, p)

@@ -1,0 +1,103 @@
+"""libmc3's host-side shift bookkeeping (C ABI, no GPU needed) against the
+reference's own host classes compiled from its sources: bit-exact."""
+import ctypes
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import fp
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_peak2d_bit_exact(mc3lib, ref_host):
+    from motioncor3_b200 import api
+    rng = np.random.default_rng(7)
+    for t in range(500):
+        w = rng.standard_normal((64, 64)).astype(np.float32)
+        if t % 2:
+            w[rng.integers(0, 64), rng.integers(0, 64)] += 6
+        if t % 7 == 0:
+            w[0, 0] = 50  # border peak gets pulled inside
+        ref = np.zeros(2, np.float32)
+        ref_host.ref_peak2d(fp(w), 64, 64, fp(ref))
+        assert np.array_equal(api.peak2d(w), ref)
+
+
+@pytest.mark.parametrize("n", [3, 8, 29, 30, 31, 45, 60, 61, 90, 120])
+def test_remove_spikes_bit_exact(mc3lib, ref_host, n):
+    from motioncor3_b200 import api
+    rng = np.random.default_rng(n)
+    for t in range(20):
+        x = np.cumsum(rng.normal(0, 1.0, n)).astype(np.float32)
+        y = np.cumsum(rng.normal(0, 1.0, n)).astype(np.float32)
+        if t % 2:
+            x[rng.integers(0, n)] += 25
+            y[rng.integers(0, n)] -= 14
+        xr, yr = x.copy(), y.copy()
+        ref_host.ref_remove_spikes(fp(xr), fp(yr), n)
+        xm, ym = api.remove_spikes(x, y)
+        assert np.array_equal(xm, xr) and np.array_equal(ym, yr)
+
+
+def test_smooth_and_lin_eqs(mc3lib, ref_host):
+    from motioncor3_b200 import api
+    rng = np.random.default_rng(3)
+    for w in (0.4, 0.5, 0.7, 0.9):
+        x = rng.normal(0, 3, 50).astype(np.float32)
+        y = rng.normal(0, 3, 50).astype(np.float32)
+        xr, yr = x.copy(), y.copy()
+        ref_host.ref_smooth(fp(xr), fp(yr), 50, ctypes.c_float(w))
+        xm, ym = api.smooth_shifts(x, y, w)
+        assert np.array_equal(xm, xr) and np.array_equal(ym, yr)
+    for dim in (3, 4, 6, 9):
+        A = rng.normal(0, 1, (dim, dim)).astype(np.float32) + np.eye(dim, dtype=np.float32) * 3
+        b = rng.normal(0, 1, dim).astype(np.float32)
+        Ar, br = A.copy(), b.copy()
+        ref_host.ref_lin_eqs(fp(Ar), fp(br), dim)
+        ok, bm = api.lin_eqs(A, b)
+        assert ok and np.array_equal(bm, br)
+
+
+def test_lin_eqs_reference_kat(mc3lib):
+    from motioncor3_b200 import api
+    kat = json.load(open(os.path.join(GOLD, "lin_eqs_kat.json")))
+    ok, sol = api.lin_eqs(np.array(kat["coeff"]), np.array(kat["vals"]))
+    assert ok and np.allclose(sol, kat["solution"], atol=1e-4)
+
+
+def test_patch_bookkeeping_bit_exact(mc3lib, ref_host):
+    from motioncor3_b200 import api
+    rng = np.random.default_rng(11)
+    for (N, Px, Py) in ((10, 2, 2), (30, 5, 5), (41, 7, 5), (60, 5, 5)):
+        P = Px * Py
+        raw = rng.normal(0, 2.0, (P, N, 2)).astype(np.float32)
+        raw[rng.integers(0, P), rng.integers(0, N)] += 15
+        cen = np.array([[(i % Px + 0.5) * 4096 / Px + rng.normal(0, 40),
+                         (i // Px + 0.5) * 4096 / Py + rng.normal(0, 40)] for i in range(P)], np.float32)
+        sh = np.zeros((N, P, 2), np.float32)
+        bad = np.zeros((N, P), np.uint8)
+        ref_host.ref_patch_shifts(fp(raw), fp(cen), N, P, 4096, 4096, fp(sh), fp(bad))
+        tab = np.ascontiguousarray(raw.transpose(1, 0, 2))
+        rel = api.patch_make_relative(tab)
+        assert np.array_equal(rel, sh)
+        assert np.array_equal(api.patch_detect_bads(rel, cen, 4096, 4096), bad)
+
+
+def test_golden_vectors(mc3lib):
+    """Same checks from the committed fixtures (no reference tree needed)."""
+    from motioncor3_b200 import api
+    g = json.load(open(os.path.join(GOLD, "host_bookkeeping.json")))
+    for c in g["peak2d"]:
+        w = np.array(c["window"], np.float32).reshape(64, 64)
+        assert np.array_equal(api.peak2d(w), np.array(c["shift"], np.float32))
+    for c in g["remove_spikes"]:
+        x, y = api.remove_spikes(np.array(c["x"]), np.array(c["y"]))
+        assert np.array_equal(x, np.array(c["x_out"], np.float32))
+        assert np.array_equal(y, np.array(c["y_out"], np.float32))
+    for c in g["smooth"]:
+        x, y = api.smooth_shifts(np.array(c["x"]), np.array(c["y"]), c["w"])
+        assert np.array_equal(x, np.array(c["x_out"], np.float32))
+        assert np.array_equal(y, np.array(c["y_out"], np.float32))

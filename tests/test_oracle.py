@@ -1,0 +1,89 @@
+"""The FP64 oracle pinned before it is trusted: its FFT against numpy, its
+solver against the reference's own known-answer test, its host bookkeeping
+against golden vectors produced by the reference's own host code, and its
+whole path on small synthetic movies."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.mark.parametrize("shape", [(64, 64), (96, 128), (408, 408), (410, 408), (256, 512)])
+def test_oracle_fft2_matches_numpy(oracle, shape):
+    ny, nx = shape
+    rng = np.random.default_rng(nx * ny)
+    img = rng.standard_normal((ny, nx))
+    spec = oracle.rfft2(img, normalise=True)
+    ref = np.fft.rfft2(img) / (nx * ny)
+    assert np.abs(spec - ref).max() < 1e-12 * np.abs(ref).max() * nx
+    half = rng.standard_normal((ny, nx // 2 + 1)) + 1j * rng.standard_normal((ny, nx // 2 + 1))
+    back = oracle.irfft2(half, nx)
+    refb = np.fft.irfft2(half, s=(ny, nx)) * nx * ny
+    assert np.abs(back - refb).max() < 1e-10 * np.abs(refb).max()
+
+
+def test_oracle_cfft_prime_lengths(oracle):
+    for n in (17, 31, 41, 131, 2882):
+        x = np.random.default_rng(n).standard_normal(n) + 0j
+        assert np.allclose(oracle.cfft(x, -1), np.fft.fft(x), atol=1e-9 * n)
+
+
+def test_lin_eqs_reference_kat(oracle):
+    kat = json.load(open(os.path.join(GOLD, "lin_eqs_kat.json")))
+    ok, sol = oracle.lin_eqs(np.array(kat["coeff"]), np.array(kat["vals"]))
+    assert ok
+    assert np.allclose(sol, kat["solution"], atol=0.5 * 10 ** -kat["solution_decimals"] + 1e-4)
+
+
+def test_oracle_host_bookkeeping_golden(oracle):
+    g = json.load(open(os.path.join(GOLD, "host_bookkeeping.json")))
+    for c in g["peak2d"]:
+        w = np.array(c["window"], np.float32).reshape(64, 64)
+        assert np.array_equal(oracle.peak2d(w), np.array(c["shift"], np.float32))
+    for c in g["remove_spikes"]:
+        x, y = oracle.remove_spikes(np.array(c["x"]), np.array(c["y"]))
+        assert np.array_equal(x, np.array(c["x_out"], np.float32))
+        assert np.array_equal(y, np.array(c["y_out"], np.float32))
+    for c in g["patch_shifts"]:
+        N, P = c["N"], c["P"]
+        raw = np.array(c["raw"], np.float32).reshape(P, N, 2)
+        cen = np.array(c["centers"], np.float32).reshape(P, 2)
+        tab = np.ascontiguousarray(raw.transpose(1, 0, 2))
+        rel = oracle.patch_make_relative(tab)
+        assert np.array_equal(rel, np.array(c["shifts"], np.float32).reshape(N, P, 2))
+        bad = oracle.patch_detect_bads(rel, cen, 4096, 4096)
+        assert np.array_equal(bad, np.array(c["bad"], np.uint8).reshape(N, P))
+
+
+def test_oracle_recovers_drift(oracle):
+    from motioncor3_b200 import synthetic as S
+    m = S.make_movie(256, 256, 20, dose=6.0, seed=11)
+    r = oracle.process_movie(m.frames, iter=10, tol=0.05, bft=(150, 100), pix_size=1.0)
+    est = r["global_shifts"] - r["global_shifts"][10]
+    true = -(m.drift - m.drift[10])
+    # the reference smooths the trajectory twice, so a jittery random walk is
+    # followed only to about a pixel
+    assert np.abs(est - true).max() < 1.5
+    assert np.corrcoef(est[:, 0], true[:, 0])[0, 1] > 0.9
+    assert r["n_sums"] == 1 and r["sums"][0].min() >= 0
+
+
+def test_oracle_patch_and_dose_paths_run(oracle):
+    from motioncor3_b200 import synthetic as S
+    m = S.make_movie(256, 256, 12, dose=4.0, seed=5, gain=True, local=True)
+    r = oracle.process_movie(m.frames, gain=m.gain, patch=(3, 3), iter=4, tol=0.2,
+                             bft=(150, 100), fm_dose=1.0, pix_size=1.0, kv=300)
+    assert r["n_sums"] == 3
+    assert r["patch_shifts"].shape == (12, 9, 2)
+    assert np.isfinite(r["sums"]).all()
+    # with forced shifts the oracle reproduces its own sums
+    f = oracle.process_movie(m.frames, gain=m.gain, patch=(3, 3), iter=4, tol=0.2,
+                             bft=(150, 100), fm_dose=1.0, pix_size=1.0, kv=300,
+                             force=dict(global_shifts=r["global_shifts"],
+                                        patch_shifts=r["patch_shifts"],
+                                        patch_centers=r["patch_centers"],
+                                        patch_bad=r["patch_bad"]))
+    assert np.array_equal(f["sums"], r["sums"])
