@@ -7,15 +7,19 @@
 
 namespace mc3 {
 
-// GWeightFrame mGCalcWeight (Correct/GWeightFrame.cu:19-30)
-__device__ __forceinline__ float dose_weight(int x, int y, int cmpX, int cmpY, float fDose,
-                                             float kvf, float pix) {
+// GWeightFrame mGCalcWeight (Correct/GWeightFrame.cu:19-30), split into the
+// frame-independent critical dose and the per-frame exponential (the same
+// FP32 operations as the reference, with powf evaluated once per frequency).
+__device__ __forceinline__ float crit_dose(int x, int y, int cmpX, int cmpY, float kvf, float pix) {
   float fX = (float)x * 0.5f / (float)(unsigned)(cmpX - 1);
   float fY = y / (float)cmpY;
   if (fY >= 0.5f) fY -= 1.0f;
   fX = sqrtf(fX * fX + fY * fY) / pix;
   float fCritDose = 0.24499f * powf(fX, -1.6649f) + 2.8141f;
   fCritDose *= kvf;
+  return fCritDose;
+}
+__device__ __forceinline__ float dose_weight_c(float fCritDose, float fDose) {
   return expf(-0.5f * fDose / fCritDose);
 }
 
@@ -31,9 +35,10 @@ __global__ void k_dose_norm(const float* acc, int N, int cmpX, int cmpY, float p
     return;
   }
   const int x = (int)(i % cmpX), y = (int)(i / cmpX);
+  const float cd = crit_dose(x, y, cmpX, cmpY, kvf, pix);
   float s = 0.0f;
   for (int f = 0; f < N; ++f) {
-    const float w = dose_weight(x, y, cmpX, cmpY, acc[f], kvf, pix);
+    const float w = dose_weight_c(cd, acc[f]);
     s += (w * w);
   }
   Wn[i] = sqrtf(s);
@@ -61,6 +66,7 @@ __global__ void k_frame_sums(const float2* __restrict__ spec, long fr_stride, in
   const int x = (int)(k % cmpX), y = (int)(k / cmpX);
   float2 s0 = c2(0.f, 0.f), s1 = c2(0.f, 0.f), s2 = c2(0.f, 0.f);
   const float wn = dp.enabled && k > 0 ? Wn[k] : 1.0f;
+  const float cd = dp.enabled && k > 0 ? crit_dose(x, y, cmpX, cmpY, dp.kv_factor, dp.pix_size) : 1.0f;
   for (int f = 0; f < N; ++f) {
     float2 X = spec[(long)f * fr_stride + k];
     if (ex) {
@@ -70,7 +76,7 @@ __global__ void k_frame_sums(const float2* __restrict__ spec, long fr_stride, in
     s0 = cadd(X, s0);
     if (dp.enabled) {
       if (k > 0) {
-        float fW = dose_weight(x, y, cmpX, cmpY, acc[f], dp.kv_factor, dp.pix_size);
+        float fW = dose_weight_c(cd, acc[f]);
         fW = fW / wn;
         X.x *= fW;
         X.y *= fW;

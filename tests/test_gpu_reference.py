@@ -1,0 +1,105 @@
+"""End-to-end parity with the reference program itself.
+
+The reference (MotionCor3 1.2.1) is compiled from its own sources for
+sm_100 into oracle/_ref/MotionCor3 by oracle/ref_full/Makefile.  Each case
+writes a seeded synthetic movie (and gain) as MRC, runs the reference and
+the mc3-b200 command line with the same tags, and compares the shift logs
+(within 0.05 px) and the sums (within 1e-4 relative RMS).  Skipped when the
+reference binary is not present."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "MotionCor3")
+OUR_BIN = os.path.join(ROOT, "motioncor3_b200", "MotionCor3")
+
+
+def _env():
+    env = dict(os.environ)
+    env["LD_LIBRARY_PATH"] = "/usr/local/cuda/lib64:" + env.get("LD_LIBRARY_PATH", "")
+    return env
+
+
+def _read_log(path):
+    rows = []
+    for line in open(path):
+        if line.startswith("#") or not line.strip():
+            continue
+        rows.append([float(v) for v in line.split()])
+    return np.array(rows)
+
+
+def run_program(binary, workdir, movie, gain, tags):
+    from motioncor3_b200 import mrcio
+    os.makedirs(workdir, exist_ok=True)
+    mv = os.path.join(workdir, "movie.mrc")
+    mrcio.write(mv, movie)
+    args = [binary, "-InMrc", mv, "-OutMrc", os.path.join(workdir, "sum.mrc"), "-LogDir",
+            workdir + "/", "-Gpu", "0", "-Cs", "0"] + tags
+    if gain is not None:
+        gp = os.path.join(workdir, "gain.mrc")
+        mrcio.write(gp, gain.astype(np.float32))
+        args += ["-Gain", gp]
+    p = subprocess.run(args, capture_output=True, text=True, env=_env(), timeout=900, cwd=workdir)
+    out = p.stdout + p.stderr
+    assert p.returncode == 0, out[-3000:]
+    m = re.search(r"Computation time:\s*([0-9.]+)", out)
+    secs = float(m.group(1)) if m else None
+    sums = {}
+    for suf in ("", "_DW", "_DWS"):
+        f = os.path.join(workdir, f"sum{suf}.mrc")
+        if os.path.exists(f):
+            sums[suf] = mrcio.read(f)[0].astype(np.float64)
+    logs = {}
+    for suf in ("-Full.log", "-Patch-Full.log", "-Patch-Patch.log", "-Patch-Frame.log"):
+        f = os.path.join(workdir, "movie" + suf)
+        if os.path.exists(f):
+            logs[suf] = f
+    return dict(sums=sums, logs=logs, secs=secs, stdout=out)
+
+
+CASES = {
+    "global_256": dict(shape=(16, 256, 256), dose=4.0, seed=31, gain=False, local=False,
+                       tags="-Patch 0 0 -Iter 7 -Tol 0.5 -Bft 150 -PixSize 1"),
+    "global_dw_gain": dict(shape=(12, 320, 384), dose=3.0, seed=32, gain=True, local=False,
+                           tags="-Iter 6 -Tol 0.2 -Bft 300 -FmDose 1.2 -PixSize 0.9 -kV 300"),
+    "patch_3x3": dict(shape=(12, 512, 512), dose=4.0, seed=33, gain=True, local=True,
+                      tags="-Patch 3 3 -Iter 5 -Tol 0.2 -Bft 500 150 -FmDose 1 -PixSize 1 -kV 300"),
+    "config1_1024x40": dict(shape=(40, 1024, 1024), dose=1.0, seed=101, gain=False, local=False,
+                            tags="-Patch 0 0 -Iter 7 -Tol 0.5 -Bft 150 -PixSize 1.0"),
+}
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_cli_matches_reference_program(name, tmp_path, mc3lib):
+    if not os.path.exists(REF_BIN):
+        pytest.skip("reference program not built (oracle/ref_full)")
+    from motioncor3_b200 import build, synthetic as S
+    build.build()
+    c = CASES[name]
+    nz, ny, nx = c["shape"]
+    m = S.make_movie(nx, ny, nz, dose=c["dose"], seed=c["seed"], gain=c["gain"], local=c["local"])
+    tags = c["tags"].split()
+    ref = run_program(REF_BIN, str(tmp_path / "ref"), m.frames, m.gain, tags)
+    ours = run_program(OUR_BIN, str(tmp_path / "ours"), m.frames, m.gain, tags)
+    assert sorted(ref["sums"]) == sorted(ours["sums"])
+    assert sorted(ref["logs"]) == sorted(ours["logs"])
+    same_shifts = True
+    for key in ref["logs"]:
+        a, b = _read_log(ref["logs"][key]), _read_log(ours["logs"][key])
+        assert a.shape == b.shape, key
+        d = np.abs(a - b).max()
+        assert d <= 0.05 + 1e-6, (key, d)
+        same_shifts &= d == 0
+    for suf in ref["sums"]:
+        r, o = ref["sums"][suf], ours["sums"][suf]
+        rel = np.sqrt(np.mean((r - o) ** 2) / np.mean(r ** 2))
+        print(f"{name} sum{suf}: rel RMS {rel:.2e}; reference {ref['secs']} s, ours {ours['secs']} s")
+        if same_shifts:
+            assert rel <= 1e-4, (suf, rel)
