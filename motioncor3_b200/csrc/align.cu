@@ -185,11 +185,102 @@ __global__ void k_corr_cols(const float2* __restrict__ spec, const int* act,
   }
 }
 
+// Same computation with the in-place padded FFT (power-of-two cmpY).
+__device__ __forceinline__ float2 corr_value(const float2* __restrict__ X,
+                                             const float2* __restrict__ ex,
+                                             const float2* __restrict__ ey, const float2* Sa,
+                                             int a, int N, int f0, int gs, int x, int y, int cmpX,
+                                             int H, long nel, float fFilt0, int phase_only) {
+  const long k = (long)y * cmpX + x;
+  float2 Gs = c2(0.f, 0.f);
+  for (int i = 0; i < gs; ++i) {
+    const long tf = (long)a * N + f0 + i;
+    const float2 e = cmul(ex[tf * cmpX + x], ey[tf * H + y]);
+    const float2 v = rot(X[(long)(f0 + i) * nel + k], e);
+    Gs = i ? cadd(Gs, v) : v;
+  }
+  float2 cs = Sa[k];
+  cs.x -= Gs.x;
+  cs.y -= Gs.y;
+  float2 C;
+  C.x = Gs.x * cs.x + Gs.y * cs.y;
+  C.y = Gs.x * cs.y - Gs.y * cs.x;
+  const int yy = wrap_half(y, H);
+  float fFilt = expf(fFilt0 * (float)((unsigned)(x * x) + (unsigned)(yy * yy)));
+  if (phase_only) {
+    float fAmp = sqrtf(C.x * C.x + C.y * C.y);
+    fFilt = fFilt / (fAmp + (float)1e-20);
+  }
+  if (k > 0) {
+    C.x *= fFilt;
+    C.y *= fFilt;
+  } else {
+    C = c2(0.f, 0.f);
+  }
+  const int sgn = ((x + y) % 2 == 0) ? 1 : -1;
+  C.x *= sgn;
+  C.y *= sgn;
+  return C;
+}
+
+template <int MAXB>
+__global__ void __launch_bounds__(512, 2) k_corr_cols_ip(
+    const float2* __restrict__ spec, const int* act, const float2* __restrict__ ex,
+    const float2* __restrict__ ey, const float2* __restrict__ S, const int* gstart,
+    const int* gsize, float bf, int phase_only, float2* T, int cmpX, int H, int N, long sstride,
+    int G, int seaY, int TX, FftDesc dH) {
+  extern __shared__ float2 sm[];
+  const int ld = spad_len(H);
+  const int a = blockIdx.z;
+  const int g = blockIdx.y;
+  const int x0 = blockIdx.x * TX;
+  const long nel = (long)cmpX * H;
+  const float2* X = spec + (long)act[a] * sstride;
+  const float2* Sa = S + (long)a * nel;
+  const int f0 = gstart[g], gs = gsize[g];
+  const float fFilt0 = -0.25f * bf / ((unsigned)(cmpX - 1) * (unsigned)H);
+  for (int t = threadIdx.x; t < TX * H; t += blockDim.x) {
+    const int y = t / TX, c = t - y * TX;
+    const int x = x0 + c;
+    float2 C = c2(0.f, 0.f);
+    if (x < cmpX) C = corr_value(X, ex, ey, Sa, a, N, f0, gs, x, y, cmpX, H, nel, fFilt0, phase_only);
+    sm[c * ld + spad(y)] = C;
+  }
+  __syncthreads();
+  cta_fft_inplace<1, MAXB>(sm, dH, TX, ld);
+  const int y0 = (H - seaY) / 2;
+  float2* Tg = T + ((long)a * G + g) * seaY * cmpX;
+  for (int t = threadIdx.x; t < TX * seaY; t += blockDim.x) {
+    const int yi = t / TX, c = t - yi * TX;
+    const int x = x0 + c;
+    if (x < cmpX) Tg[(long)yi * cmpX + x] = sm[c * ld + spad(y0 + yi)];
+  }
+}
+
 int corr_cols(const float2* spec, const int* act, const float2* ex, const float2* ey,
               const float2* S, const int* gstart, const int* gsize, float bfactor,
               int phase_only, float2* T, const AlignDims& d, cudaStream_t st) {
   FftDesc dH;
   MC3_TRY(make_desc(d.cmpY, d.cmpY, &dH));
+  if (all_dedicated(dH) && !getenv("MC3_FFT_PINGPONG")) {
+    const int ld = spad_len(d.cmpY);
+    int rmin = 8;
+    for (int s = 0; s < dH.nstages; ++s) rmin = dH.radix[s] < rmin ? dH.radix[s] : rmin;
+    int tx = (2 * 512) / (d.cmpY / rmin);
+    const int by_smem = (72 * 1024) / (ld * (int)sizeof(float2));
+    if (by_smem < tx) tx = by_smem;
+    if (tx > 16) tx = 16;
+    if (tx >= 1) {
+      const size_t smem = (size_t)tx * ld * sizeof(float2);
+      MC3_TRY(set_smem_attr(k_corr_cols_ip<2>, smem));
+      dim3 grid(ceil_div(d.cmpX, tx), d.G, d.A);
+      prof::Scope ps("k_corr_cols", (double)d.A * ((double)d.cmpX * d.cmpY * 8.0 * (d.N + 1) + (double)d.G * d.seaY * d.cmpX * 8.0), st);
+      k_corr_cols_ip<2><<<grid, 512, smem, st>>>(spec, act, ex, ey, S, gstart, gsize, bfactor, phase_only,
+                                                 T, d.cmpX, d.cmpY, d.N, d.stack_stride, d.G, d.seaY, tx, dH);
+      MC3_CHECK_LAUNCH("k_corr_cols_ip");
+      return kOk;
+    }
+  }
   const int tx = col_tile(d.cmpY);
   const size_t smem = 2 * (size_t)tx * (d.cmpY + 1) * sizeof(float2);
   if (smem > 200 * 1024) return kEUnsupported;

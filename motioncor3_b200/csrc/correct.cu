@@ -106,58 +106,79 @@ int frame_sums(const float2* spec, long fr_stride, int N, int cmpX, int cmpY, co
 // over good patches with normalised distance r_p <= 0.6, then a
 // nearest-neighbour (int-truncated) gather; out-of-range sources fold to
 // (811*|v|) mod size.
-__global__ void k_local_gather(const float* __restrict__ in, long in_stride, float* out,
-                               long out_stride, int W, int H, const float* __restrict__ cent,
-                               const float2* __restrict__ sh, const uint8_t* __restrict__ bad,
-                               int P, int f0) {
+//
+// The distance weights do not depend on the frame, so each thread evaluates
+// them once for its pixel (held in registers, PMAX >= P) and then walks all
+// nb frames, accumulating in patch order exactly as the reference does per
+// frame; the result is bit-identical to evaluating them per frame.
+template <int PMAX>
+__global__ void __launch_bounds__(128) k_local_gather(
+    const float* __restrict__ in, long in_stride, float* out, long out_stride, int W, int H,
+    const float* __restrict__ cent, const float2* __restrict__ sh,
+    const uint8_t* __restrict__ bad, int P, int nb) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y;
   if (x >= W) return;
-  const int b = blockIdx.z;
-  const int f = f0 + b;
-  const float2* s = sh + (long)f * P;
-  const uint8_t* bd = bad ? bad + (long)f * P : nullptr;
   const float fB = 100.0f;
-  float fSx = 0.0f, fSy = 0.0f, fW = 0.0f;
-  for (int p = 0; p < P; ++p) {
-    if (bd != 0 && bd[p]) continue;
-    float ax = ((float)(unsigned)x - cent[2 * p]) / (float)(unsigned)W;
-    float ay = (y - cent[2 * p + 1]) / H;
-    ax = sqrtf(ax * ax + ay * ay);
-    if (ax > 0.6f) continue;
-    ax = expf(-fB * ax);
-    fW += ax;
-    fSx += s[p].x * ax;
-    fSy += s[p].y * ax;
-  }
-  if (fW > 0) {
-    fSx = fSx / fW;
-    fSy = fSy / fW;
-  }
-  int ix = (int)(((float)(unsigned)x - fSx) * 1);
-  int iy = (int)((y - fSy) * 1);
-  if (ix < 0 || iy < 0 || ix >= W || iy >= H) {
-    ix = (ix < 0) ? -ix : ix;
-    iy = (iy < 0) ? -iy : iy;
-    ix = (811 * ix) % W;
-    iy = (811 * iy) % H;
-    // Only non-finite shifts reach here out of range (the int conversion of
-    // NaN/inf); keep the read inside the frame.
-    if (ix < 0 || ix >= W) ix = 0;
-    if (iy < 0 || iy >= H) iy = 0;
+  float w[PMAX];
+#pragma unroll
+  for (int p = 0; p < PMAX; ++p) {
+    w[p] = -1.0f;  // -1: patch farther than r = 0.6 (never a valid weight)
+    if (p < P) {
+      float ax = ((float)(unsigned)x - cent[2 * p]) / (float)(unsigned)W;
+      float ay = (y - cent[2 * p + 1]) / H;
+      ax = sqrtf(ax * ax + ay * ay);
+      if (!(ax > 0.6f)) w[p] = expf(-fB * ax);
+    }
   }
   const int padX = (W / 2 + 1) * 2;
-  out[(long)b * out_stride + (long)y * padX + x] = in[(long)b * in_stride + (long)iy * padX + ix];
+  const long o = (long)y * padX + x;
+  for (int f = 0; f < nb; ++f) {
+    const float2* s = sh + (long)f * P;
+    const uint8_t* bd = bad ? bad + (long)f * P : nullptr;
+    float fSx = 0.0f, fSy = 0.0f, fW = 0.0f;
+#pragma unroll
+    for (int p = 0; p < PMAX; ++p) {
+      if (p >= P) break;
+      if (bd != 0 && bd[p]) continue;
+      if (w[p] < 0.0f) continue;
+      fW += w[p];
+      fSx += s[p].x * w[p];
+      fSy += s[p].y * w[p];
+    }
+    if (fW > 0) {
+      fSx = fSx / fW;
+      fSy = fSy / fW;
+    }
+    int ix = (int)(((float)(unsigned)x - fSx) * 1);
+    int iy = (int)((y - fSy) * 1);
+    if (ix < 0 || iy < 0 || ix >= W || iy >= H) {
+      ix = (ix < 0) ? -ix : ix;
+      iy = (iy < 0) ? -iy : iy;
+      ix = (811 * ix) % W;
+      iy = (811 * iy) % H;
+      // Only non-finite shifts reach here out of range (the int conversion
+      // of NaN/inf); keep the read inside the frame.
+      if (ix < 0 || ix >= W) ix = 0;
+      if (iy < 0 || iy >= H) iy = 0;
+    }
+    out[(long)f * out_stride + o] = in[(long)f * in_stride + (long)iy * padX + ix];
+  }
 }
 
 int local_gather(const float* in, long in_stride, float* out, long out_stride, int nb, int W,
                  int H, const float* centers, const float2* shifts, const uint8_t* bad, int P,
                  cudaStream_t st) {
   // `shifts`/`bad` point at the first frame of the batch.
-  dim3 grid(ceil_div(W, 256), H, nb);
+  if (P < 1 || P > 64) return kEUnsupported;
+  dim3 grid(ceil_div(W, 128), H);
   prof::Scope ps("k_local_gather", (double)nb * W * H * 8.0, st);
-  k_local_gather<<<grid, 256, 0, st>>>(in, in_stride, out, out_stride, W, H, centers, shifts, bad,
-                                       P, 0);
+  if (P <= 16)
+    k_local_gather<16><<<grid, 128, 0, st>>>(in, in_stride, out, out_stride, W, H, centers, shifts, bad, P, nb);
+  else if (P <= 36)
+    k_local_gather<36><<<grid, 128, 0, st>>>(in, in_stride, out, out_stride, W, H, centers, shifts, bad, P, nb);
+  else
+    k_local_gather<64><<<grid, 128, 0, st>>>(in, in_stride, out, out_stride, W, H, centers, shifts, bad, P, nb);
   MC3_CHECK_LAUNCH("k_local_gather");
   return kOk;
 }

@@ -457,29 +457,29 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
     MC3_CUDA(cudaMemcpyAsync(d_pcent.p, patCent.data(), sizeof(float) * 2 * P, cudaMemcpyHostToDevice, st));
     MC3_CUDA(cudaMemcpyAsync(d_pshift.p, patShift.data(), sizeof(float) * 2 * (size_t)P * N, cudaMemcpyHostToDevice, st));
     MC3_CUDA(cudaMemcpyAsync(d_pbad.p, patBad.data(), (size_t)P * N, cudaMemcpyHostToDevice, st));
-    const int B = std::min(N, 16);
-    MC3_TRY(d_real.ensure(sizeof(float2) * ncmp * B));
-    MC3_TRY(d_gath.ensure(sizeof(float2) * ncmp * B));
-    for (int f0 = 0; f0 < N; f0 += B) {
-      const int nb = std::min(B, N - f0);
-      Batch bi{nb, nb, (long)ncmp, nullptr, (long)ncmp};
+    // All frames at once: the spectra are shifted and inverted in place, the
+    // gather writes a second frame stack, and the forward transform of the
+    // gathered frames lands back in the spectrum buffer.  Patch weights are
+    // then evaluated once per pixel for the whole movie.
+    MC3_TRY(d_gath.ensure(sizeof(float2) * ncmp * N));
+    {
+      Batch bi{N, N, (long)ncmp, nullptr, (long)ncmp};
       ColOps inv{};
       inv.dir = 1;
       inv.scale = 1.0f;
-      inv.ex = d_fex.as<float2>() + (size_t)f0 * g.cmpX;
-      inv.ey = d_fey.as<float2>() + (size_t)f0 * g.cmpY;
-      MC3_TRY(col_fft(spec + (size_t)f0 * ncmp, d_real.as<float2>(), g.cmpX, g.cmpX, H, bi, inv, st));
-      Batch br{nb, nb, (long)ncmp, nullptr, (long)ncmp * 2};
-      MC3_TRY(row_c2r(d_real.as<float2>(), g.cmpX, d_real.as<float>(), g.padX, W, H, br, st));
-      MC3_TRY(local_gather(d_real.as<float>(), (long)ncmp * 2, d_gath.as<float>(), (long)ncmp * 2, nb, W, H,
-                           d_pcent.as<float>(), d_pshift.as<float2>() + (size_t)f0 * P,
-                           d_pbad.as<uint8_t>() + (size_t)f0 * P, P, st));
-      Batch bf{nb, nb, (long)ncmp * 2, nullptr, (long)ncmp};
-      MC3_TRY(row_r2c(d_gath.as<float>(), g.padX, spec + (size_t)f0 * ncmp, g.cmpX, W, H, bf, 1.0f, st));
+      inv.ex = d_fex.as<float2>();
+      inv.ey = d_fey.as<float2>();
+      MC3_TRY(col_fft(spec, spec, g.cmpX, g.cmpX, H, bi, inv, st));
+      Batch br{N, N, (long)ncmp, nullptr, (long)ncmp * 2};
+      MC3_TRY(row_c2r(spec, g.cmpX, frames, g.padX, W, H, br, st));
+      MC3_TRY(local_gather(frames, (long)ncmp * 2, d_gath.as<float>(), (long)ncmp * 2, N, W, H,
+                           d_pcent.as<float>(), d_pshift.as<float2>(), d_pbad.as<uint8_t>(), P, st));
+      Batch bf{N, N, (long)ncmp * 2, nullptr, (long)ncmp};
+      MC3_TRY(row_r2c(d_gath.as<float>(), g.padX, spec, g.cmpX, W, H, bf, 1.0f, st));
       ColOps fwd{};
       fwd.dir = -1;
       fwd.scale = (float)(1.0 / W / H);
-      MC3_TRY(col_fft(spec + (size_t)f0 * ncmp, spec + (size_t)f0 * ncmp, g.cmpX, g.cmpX, H, bi, fwd, st));
+      MC3_TRY(col_fft(spec, spec, g.cmpX, g.cmpX, H, bi, fwd, st));
     }
     MC3_TRY(frame_sums(spec, (long)ncmp, N, g.cmpX, g.cmpY, nullptr, nullptr, d_acc.as<float>(),
                        d_Wn.as<float>(), dp, d_sums.as<float2>(), g.nSums, st));

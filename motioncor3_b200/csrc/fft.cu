@@ -161,6 +161,144 @@ __global__ void k_col_fft(const float2* in, float2* out, long pitch, int cmpX, i
   }
 }
 
+// ---------------------------------------------------------------------
+// In-place variants (plans made only of radices 2, 3, 4, 8): one padded
+// buffer per sequence, register-staged stages.  Used whenever the plan
+// allows; the ping-pong kernels above cover every other length.
+// ---------------------------------------------------------------------
+template <int MAXB>
+__global__ void __launch_bounds__(512, 2) k_row_r2c_ip(const float* __restrict__ in, long in_pitch,
+                                                    float2* out, long out_pitch, int W, int H,
+                                                    int rows, Batch bt, FftDesc dM, float scale) {
+  extern __shared__ float2 sm[];
+  const int M = W / 2;
+  const int ld = spad_len(M + 1);
+  const int item = blockIdx.y;
+  const int r0 = blockIdx.x * rows;
+  const int nr = min(rows, H - r0);
+  const float* src = in + batch_in_off(bt, item) + (long)r0 * in_pitch;
+  for (int t = threadIdx.x; t < nr * M; t += blockDim.x) {
+    const int r = t / M, m = t - r * M;
+    const float* p = src + (long)r * in_pitch + 2 * m;
+    sm[r * ld + spad(m)] = c2(p[0], p[1]);
+  }
+  __syncthreads();
+  cta_fft_inplace<-1, MAXB>(sm, dM, nr, ld);
+  const int np = M / 2 + 1;
+  for (int t = threadIdx.x; t < nr * np; t += blockDim.x) {
+    const int r = t / np, p = t - r * np;
+    r2c_post_pair(sm + r * ld, M, p, dM.tw, scale);
+  }
+  __syncthreads();
+  float2* dst = out + (long)item * bt.out_stride + (long)r0 * out_pitch;
+  for (int t = threadIdx.x; t < nr * (M + 1); t += blockDim.x) {
+    const int r = t / (M + 1), k = t - r * (M + 1);
+    dst[(long)r * out_pitch + k] = sm[r * ld + spad(k)];
+  }
+}
+
+template <int MAXB>
+__global__ void __launch_bounds__(512, 2) k_row_c2r_ip(const float2* in, long in_pitch, float* out,
+                                                    long out_pitch, int W, int H, int rows,
+                                                    Batch bt, FftDesc dM) {
+  extern __shared__ float2 sm[];
+  const int M = W / 2;
+  const int ld = spad_len(M + 1);
+  const int item = blockIdx.y;
+  const int r0 = blockIdx.x * rows;
+  const int nr = min(rows, H - r0);
+  const float2* src = in + batch_in_off(bt, item) + (long)r0 * in_pitch;
+  for (int t = threadIdx.x; t < nr * (M + 1); t += blockDim.x) {
+    const int r = t / (M + 1), k = t - r * (M + 1);
+    sm[r * ld + spad(k)] = src[(long)r * in_pitch + k];
+  }
+  __syncthreads();
+  const int np = M / 2 + 1;
+  for (int t = threadIdx.x; t < nr * np; t += blockDim.x) {
+    const int r = t / np, p = t - r * np;
+    c2r_pre_pair(sm + r * ld, M, p, dM.tw);
+  }
+  __syncthreads();
+  cta_fft_inplace<1, MAXB>(sm, dM, nr, ld);
+  float* dst = out + (long)item * bt.out_stride + (long)r0 * out_pitch;
+  for (int t = threadIdx.x; t < nr * M; t += blockDim.x) {
+    const int r = t / M, m = t - r * M;
+    const float2 v = sm[r * ld + spad(m)];
+    float* p = dst + (long)r * out_pitch + 2 * m;
+    p[0] = v.x;
+    p[1] = v.y;
+  }
+}
+
+template <int MAXB>
+__global__ void __launch_bounds__(512, 2) k_col_fft_ip(const float2* in, float2* out, long pitch,
+                                                    int cmpX, int H, int TX, Batch bt, FftDesc dH,
+                                                    ColOps ops) {
+  extern __shared__ float2 sm[];
+  const int ld = spad_len(H);
+  const int item = blockIdx.y;
+  const int x0 = blockIdx.x * TX;
+  const float2* src = in + batch_in_off(bt, item);
+  const float2* ex = ops.ex ? ops.ex + (long)item * cmpX : nullptr;
+  const float2* ey = ops.ey ? ops.ey + (long)item * H : nullptr;
+  for (int t = threadIdx.x; t < TX * H; t += blockDim.x) {
+    const int y = t / TX, c = t - y * TX;
+    const int x = x0 + c;
+    float2 v = c2(0.f, 0.f);
+    if (x < cmpX) {
+      v = src[(long)y * pitch + x];
+      if (ex) v = cmul(v, cmul(ex[x], ey[y]));
+    }
+    sm[c * ld + spad(y)] = v;
+  }
+  __syncthreads();
+  if (ops.dir < 0) cta_fft_inplace<-1, MAXB>(sm, dH, TX, ld);
+  else cta_fft_inplace<1, MAXB>(sm, dH, TX, ld);
+  float2* dst = out + (long)item * bt.out_stride;
+  float2* crop = ops.crop ? ops.crop + (long)item * ops.crop_x * ops.crop_y : nullptr;
+  for (int t = threadIdx.x; t < TX * H; t += blockDim.x) {
+    const int y = t / TX, c = t - y * TX;
+    const int x = x0 + c;
+    if (x >= cmpX) continue;
+    const float2 v = cscale(sm[c * ld + spad(y)], ops.scale);
+    dst[(long)y * pitch + x] = v;
+    if (crop && x < ops.crop_x) {
+      int yo = -1;
+      if (y <= ops.crop_y / 2) yo = y;
+      else if (y > H - ops.crop_y / 2) yo = y - H + ops.crop_y;
+      if (yo >= 0) crop[(long)yo * ops.crop_x + x] = v;
+    }
+  }
+}
+
+namespace {
+constexpr int kIpThreads = 512;
+constexpr int kIpBudget = 72 * 1024;   // shared memory per CTA, in-place kernels
+int min_radix(const FftDesc& d) {
+  int r = 64;
+  for (int s = 0; s < d.nstages; ++s) r = d.radix[s] < r ? d.radix[s] : r;
+  return r;
+}
+// Sequences per CTA for an in-place pass: bounded by the register staging
+// capacity (MAXB butterflies per thread) and the shared-memory budget.
+// MC3_FFT_PINGPONG=1 forces the generic kernels (A/B comparisons).
+bool use_inplace(const FftDesc& d) {
+  static const bool off = [] {
+    const char* e = getenv("MC3_FFT_PINGPONG");
+    return e && e[0] == '1';
+  }();
+  return !off && all_dedicated(d);
+}
+int ip_batch(const FftDesc& d, int ld, int maxb) {
+  const int per = d.n / min_radix(d);
+  int nb = (maxb * kIpThreads) / per;
+  const int by_smem = kIpBudget / (ld * (int)sizeof(float2));
+  if (by_smem < nb) nb = by_smem;
+  if (nb > 16) nb = 16;
+  return nb;
+}
+}  // namespace
+
 int row_tile(int M) {
   int rows = kSmemBudget / (2 * (M + 1) * (int)sizeof(float2));
   if (rows < 1) rows = 1;
@@ -180,6 +318,19 @@ int row_r2c(const float* in, long in_pitch, float2* out, long out_pitch, int W, 
   const int M = W / 2;
   FftDesc d;
   MC3_TRY(make_desc(M, W, &d));
+  if (use_inplace(d)) {
+    const int ld = spad_len(M + 1);
+    const int rows = ip_batch(d, ld, 2);
+    if (rows >= 1) {
+      const size_t smem = (size_t)rows * ld * sizeof(float2);
+      MC3_TRY(set_smem_attr(k_row_r2c_ip<2>, smem));
+      dim3 grid(ceil_div(H, rows), b.items);
+      prof::Scope ps("k_row_r2c", (double)b.items * H * (W * 4.0 + (W / 2 + 1) * 8.0), st);
+      k_row_r2c_ip<2><<<grid, kIpThreads, smem, st>>>(in, in_pitch, out, out_pitch, W, H, rows, b, d, scale);
+      MC3_CHECK_LAUNCH("k_row_r2c_ip");
+      return kOk;
+    }
+  }
   const int rows = row_tile(M);
   const size_t smem = 2 * (size_t)rows * (M + 1) * sizeof(float2);
   if (smem > 200 * 1024) return kEUnsupported;
@@ -197,6 +348,19 @@ int row_c2r(const float2* in, long in_pitch, float* out, long out_pitch, int W, 
   const int M = W / 2;
   FftDesc d;
   MC3_TRY(make_desc(M, W, &d));
+  if (use_inplace(d)) {
+    const int ld = spad_len(M + 1);
+    const int rows = ip_batch(d, ld, 2);
+    if (rows >= 1) {
+      const size_t smem = (size_t)rows * ld * sizeof(float2);
+      MC3_TRY(set_smem_attr(k_row_c2r_ip<2>, smem));
+      dim3 grid(ceil_div(H, rows), b.items);
+      prof::Scope ps("k_row_c2r", (double)b.items * H * (W * 4.0 + (W / 2 + 1) * 8.0), st);
+      k_row_c2r_ip<2><<<grid, kIpThreads, smem, st>>>(in, in_pitch, out, out_pitch, W, H, rows, b, d);
+      MC3_CHECK_LAUNCH("k_row_c2r_ip");
+      return kOk;
+    }
+  }
   const int rows = row_tile(M);
   const size_t smem = 2 * (size_t)rows * (M + 1) * sizeof(float2);
   if (smem > 200 * 1024) return kEUnsupported;
@@ -214,6 +378,19 @@ int col_fft(const float2* in, float2* out, long pitch, int cmpX, int H, const Ba
   if (ops.crop && (ops.crop_x > cmpX || ops.crop_y > H)) return kEInval;
   FftDesc d;
   MC3_TRY(make_desc(H, H, &d));
+  if (use_inplace(d)) {
+    const int ld = spad_len(H);
+    const int tx = ip_batch(d, ld, 2);
+    if (tx >= 1) {
+      const size_t smem = (size_t)tx * ld * sizeof(float2);
+      MC3_TRY(set_smem_attr(k_col_fft_ip<2>, smem));
+      dim3 grid(ceil_div(cmpX, tx), b.items);
+      prof::Scope ps("k_col_fft", (double)b.items * ((double)cmpX * H * 16.0 + (ops.crop ? (double)ops.crop_x * ops.crop_y * 8.0 : 0.0)), st);
+      k_col_fft_ip<2><<<grid, kIpThreads, smem, st>>>(in, out, pitch, cmpX, H, tx, b, d, ops);
+      MC3_CHECK_LAUNCH("k_col_fft_ip");
+      return kOk;
+    }
+  }
   const int tx = col_tile(H);
   const size_t smem = 2 * (size_t)tx * (H + 1) * sizeof(float2);
   if (smem > 200 * 1024) return kEUnsupported;

@@ -73,6 +73,12 @@ inline int fft_factorize(int n, int* radix) {
   int m = n;
   int p2 = 0;
   while (m % 2 == 0) { m /= 2; ++p2; }
+  // powers of two as 8s and 4s (a lone 2 only for a single factor 2)
+  if (p2 >= 4 && p2 % 3 == 1) {
+    radix[ns++] = 4;
+    radix[ns++] = 4;
+    p2 -= 4;
+  }
   while (p2 >= 3) { radix[ns++] = 8; p2 -= 3; }
   if (p2 == 2) radix[ns++] = 4;
   if (p2 == 1) radix[ns++] = 2;
@@ -238,6 +244,131 @@ __device__ float2* cta_fft(float2* A, float2* B, const FftDesc& d, int nb, int e
   return A;
 }
 #endif
+
+// ---- in-place variant (dedicated radices only) -----------------------
+// Shared-memory index with one padding slot per 32 elements: the strided
+// butterfly writes of the first stages then spread over all banks.
+MC3_HD int spad(int i) { return i + (i >> 5); }
+// Padded length of a sequence of n elements.
+MC3_HD int spad_len(int n) { return n + (n >> 5) + 1; }
+
+// True when every stage radix is 4 or 8 (the in-place path).
+inline bool all_dedicated(const FftDesc& d) {
+  for (int s = 0; s < d.nstages; ++s)
+    if (d.radix[s] != 4 && d.radix[s] != 8) return false;
+  return true;
+}
+
+#ifdef __CUDACC__
+// One stage in place: every thread first loads the inputs of up to MAXB
+// butterflies into registers, the CTA synchronises, then all outputs are
+// written back to the same buffer.  Sequence b, element i lives at
+// buf[b*ld + spad(i)].
+template <int R, int DIR, int MAXB>
+__device__ __forceinline__ void stage_inplace(float2* buf, int n, int Ns, int nb, int ld,
+                                              const float2* __restrict__ tw, int tws) {
+  const int per = n / R;
+  const int items = nb * per;
+  float2 v[MAXB][R];
+  int bj[MAXB];
+#pragma unroll
+  for (int m = 0; m < MAXB; ++m) {
+    const int it = threadIdx.x + m * blockDim.x;
+    bj[m] = -1;
+    if (it < items) {
+      const int b = it / per;
+      const int j = it - b * per;
+      bj[m] = it;
+      const float2* A = buf + b * ld;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[m][r] = A[spad(j + r * per)];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int m = 0; m < MAXB; ++m) {
+    if (bj[m] < 0) continue;
+    const int b = bj[m] / per;
+    const int j = bj[m] - b * per;
+    const int k = j % Ns;
+    if (Ns > 1) {
+      const int step = (n / (Ns * R)) * k;
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[m][r] = cmul(v[m][r], twid<DIR>(tw, tws, step * r));
+    }
+    Dft<R, DIR>::run(v[m]);
+    const int idxD = (j / Ns) * Ns * R + k;
+    float2* A = buf + b * ld;
+#pragma unroll
+    for (int r = 0; r < R; ++r) A[spad(idxD + r * Ns)] = v[m][r];
+  }
+  __syncthreads();
+}
+
+// In-place CTA transform of nb sequences (buf[b*ld + spad(i)]); requires
+// all_dedicated(d) (radices 4 and 8 only) and nb*n/R <= MAXB*blockDim.x for every stage radix R.
+template <int DIR, int MAXB>
+__device__ void cta_fft_inplace(float2* buf, const FftDesc& d, int nb, int ld) {
+  int Ns = 1;
+  for (int s = 0; s < d.nstages; ++s) {
+    const int R = d.radix[s];
+    if (R == 8) stage_inplace<8, DIR, MAXB>(buf, d.n, Ns, nb, ld, d.tw, d.tws);
+    else stage_inplace<4, DIR, MAXB>(buf, d.n, Ns, nb, ld, d.tw, d.tws);
+    Ns *= R;
+  }
+}
+#endif
+
+// Paired real-transform helpers working in place on one row held at
+// buf[spad(i)]: pair p (0 <= p <= M/2) owns elements p and M-p.
+// Forward post-processing: Z[0..M) -> X[0..M].
+MC3_HD void r2c_post_pair(float2* buf, int M, int p, const float2* twW, float scale) {
+  if (p == 0) {
+    const float2 z = buf[spad(0)];
+    buf[spad(0)] = c2((z.x + z.y) * scale, 0.0f);
+    buf[spad(M)] = c2((z.x - z.y) * scale, 0.0f);
+    return;
+  }
+  const int q = M - p;
+  const float2 zp = buf[spad(p)];
+  const float2 zq = buf[spad(q)];
+  // X[k] = (Z[k] + conj Z[M-k])/2 + w_k (Z[k] - conj Z[M-k]) (-i/2)
+  auto one = [&](float2 a, float2 b, int k) {
+    const float2 bm = cconj(b);
+    const float2 fe = c2(0.5f * (a.x + bm.x), 0.5f * (a.y + bm.y));
+    const float2 dd = csub(a, bm);
+    const float2 fo = c2(0.5f * dd.y, -0.5f * dd.x);
+    return cscale(cadd(fe, cmul(twW[k], fo)), scale);
+  };
+  const float2 xp = one(zp, zq, p);
+  if (q != p) {
+    const float2 xq = one(zq, zp, q);
+    buf[spad(q)] = xq;
+  }
+  buf[spad(p)] = xp;
+}
+
+// Inverse pre-processing: X[0..M] -> Z[0..M) (imaginary parts of X[0] and
+// X[M] ignored, see c2r_pre).
+MC3_HD void c2r_pre_pair(float2* buf, int M, int p, const float2* twW) {
+  if (p == 0) {
+    const float a = buf[spad(0)].x, b = buf[spad(M)].x;
+    buf[spad(0)] = c2(a + b, a - b);
+    return;
+  }
+  const int q = M - p;
+  const float2 xp = buf[spad(p)];
+  const float2 xq = buf[spad(q)];
+  auto one = [&](float2 a, float2 b, int k) {
+    const float2 bm = cconj(b);
+    const float2 e = cadd(a, bm);
+    const float2 o = cmul(csub(a, bm), cconj(twW[k]));
+    return c2(e.x - o.y, e.y + o.x);
+  };
+  const float2 zp = one(xp, xq, p);
+  if (q != p) buf[spad(q)] = one(xq, xp, q);
+  buf[spad(p)] = zp;
+}
 
 // Sequential host driver running the identical stage code (CPU tests).
 template <int DIR>

@@ -72,3 +72,43 @@ extern "C" int shim_irfft(const float* in, float* out, int W) {
   for (int m = 0; m < M; ++m) { out[2 * m] = z[m].x; out[2 * m + 1] = z[m].y; }
   return 0;
 }
+
+// Real transforms through the padded in-place pair helpers used by the
+// in-place row kernels (same layout: element i at buf[spad(i)]).
+extern "C" int shim_rfft_pairs(const float* in, float* out, int W) {
+  const int M = W / 2;
+  FftDesc d;
+  d.n = M;
+  d.nstages = fft_factorize(M, d.radix);
+  std::vector<float2> tw = make_table(W);
+  d.tw = tw.data();
+  d.tws = 2;
+  std::vector<float2> A(M), B(M);
+  for (int m = 0; m < M; ++m) { A[m].x = in[2 * m]; A[m].y = in[2 * m + 1]; }
+  float2* Z = fft_host_reference<-1>(A.data(), B.data(), d);
+  std::vector<float2> buf(spad_len(M + 1));
+  for (int m = 0; m < M; ++m) buf[spad(m)] = Z[m];
+  for (int p = 0; p <= M / 2; ++p) r2c_post_pair(buf.data(), M, p, tw.data(), 1.0f);
+  float2* o = reinterpret_cast<float2*>(out);
+  for (int k = 0; k <= M; ++k) o[k] = buf[spad(k)];
+  return 0;
+}
+
+extern "C" int shim_irfft_pairs(const float* in, float* out, int W) {
+  const int M = W / 2;
+  FftDesc d;
+  d.n = M;
+  d.nstages = fft_factorize(M, d.radix);
+  std::vector<float2> tw = make_table(W);
+  d.tw = tw.data();
+  d.tws = 2;
+  const float2* X = reinterpret_cast<const float2*>(in);
+  std::vector<float2> buf(spad_len(M + 1));
+  for (int k = 0; k <= M; ++k) buf[spad(k)] = X[k];
+  for (int p = 0; p <= M / 2; ++p) c2r_pre_pair(buf.data(), M, p, tw.data());
+  std::vector<float2> A(M), B(M);
+  for (int k = 0; k < M; ++k) A[k] = buf[spad(k)];
+  float2* z = fft_host_reference<1>(A.data(), B.data(), d);
+  for (int m = 0; m < M; ++m) { out[2 * m] = z[m].x; out[2 * m + 1] = z[m].y; }
+  return 0;
+}

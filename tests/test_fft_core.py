@@ -49,3 +49,19 @@ def test_factorisation_covers_lengths(shim):
         k = shim.shim_factorize(n, radix)
         assert k >= 0
         assert int(np.prod([radix[i] for i in range(k)])) == n
+
+
+@pytest.mark.parametrize("w", [2, 4, 6, 16, 128, 408, 1024, 4096])
+def test_real_fft_pair_helpers(shim, w):
+    """The in-place paired pre/post-processing of the row kernels."""
+    rng = np.random.default_rng(w + 1)
+    x = rng.standard_normal(w).astype(np.float32)
+    X = np.empty(w // 2 + 1, np.complex64)
+    assert shim.shim_rfft_pairs(fp(x), fp(X), w) == 0
+    ref = np.fft.rfft(x.astype(np.float64))
+    assert np.abs(X - ref).max() / np.abs(ref).max() < 2e-6
+    Y = (rng.standard_normal(w // 2 + 1) + 1j * rng.standard_normal(w // 2 + 1)).astype(np.complex64)
+    y = np.empty(w, np.float32)
+    assert shim.shim_irfft_pairs(fp(Y), fp(y), w) == 0
+    refy = np.fft.irfft(Y.astype(np.complex128), w) * w
+    assert np.abs(y - refy).max() / np.abs(refy).max() < 2e-6
