@@ -315,9 +315,14 @@ def main(argv=None):
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=["cfg2", "cfg1"], default="cfg2")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--frames", type=int, default=0,
+                    help="override the frame count (small cases for profiling; not a bench line)")
     args = ap.parse_args(argv)
     world, rank, local = dist_setup()
     wl = workload(args.config)
+    if args.frames > 0:
+        wl["nz"] = args.frames
+        wl["name"] = wl["name"].replace(f"{workload(args.config)['nz']}x", f"{args.frames}x", 1)
     if args.impl == "reference":
         return run_reference(args, wl, world, rank)
     return run_ours(args, wl, world, rank, local)

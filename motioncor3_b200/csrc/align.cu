@@ -94,6 +94,7 @@ __global__ void k_aligned_sum(const float2* __restrict__ spec, const int* act,
   const int kx = (int)(k % cmpX), ky = (int)(k / cmpX);
   const float2* X = spec + (long)act[a] * sstride + k;
   float2 e0 = c2(0.f, 0.f), e1 = c2(0.f, 0.f);
+#pragma unroll 4
   for (int f = 0; f < N; ++f) {
     const long t = (long)a * N + f;
     const float2 e = cmul(ex[t * cmpX + kx], ey[t * cmpY + ky]);

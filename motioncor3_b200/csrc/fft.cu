@@ -47,6 +47,28 @@ int make_desc(int n, int table_n, FftDesc* d) {
   return kOk;
 }
 
+// Global -> shared staging with kStage independent global loads in flight
+// per thread before their shared-memory stores: element t of `total` is
+// produced by load(t) and consumed by store(t, v).
+template <int kStage, class LoadF, class StoreF>
+__device__ __forceinline__ void staged_copy(int total, LoadF load, StoreF store) {
+  const int step = blockDim.x;
+  for (int t0 = threadIdx.x; t0 < total; t0 += step * kStage) {
+    float2 v[kStage];
+#pragma unroll
+    for (int j = 0; j < kStage; ++j) {
+      const int t = t0 + j * step;
+      if (t < total) v[j] = load(t);
+    }
+#pragma unroll
+    for (int j = 0; j < kStage; ++j) {
+      const int t = t0 + j * step;
+      if (t < total) store(t, v[j]);
+    }
+  }
+}
+constexpr int kStageLoads = 8;
+
 __device__ __forceinline__ long batch_in_off(const Batch& b, int item) {
   long off = (long)(item % b.nf) * b.in_stride;
   if (b.patch_off) off += b.patch_off[item / b.nf];
@@ -67,11 +89,18 @@ __global__ void k_row_r2c(const float* __restrict__ in, long in_pitch, float2* o
   const int r0 = blockIdx.x * rows;
   const int nr = min(rows, H - r0);
   const float* src = in + batch_in_off(bt, item) + (long)r0 * in_pitch;
-  for (int t = threadIdx.x; t < nr * M; t += blockDim.x) {
-    const int r = t / M, m = t - r * M;
-    const float* p = src + (long)r * in_pitch + 2 * m;
-    A[r * ld + m] = c2(p[0], p[1]);
-  }
+  const bool pair = ((reinterpret_cast<uintptr_t>(src) & 7) == 0) && !(in_pitch & 1);
+  staged_copy<kStageLoads>(
+      nr * M,
+      [&](int t) {
+        const int r = t / M, m = t - r * M;
+        const float* p = src + (long)r * in_pitch + 2 * m;
+        return pair ? *reinterpret_cast<const float2*>(p) : c2(p[0], p[1]);
+      },
+      [&](int t, float2 v) {
+        const int r = t / M, m = t - r * M;
+        A[r * ld + m] = v;
+      });
   __syncthreads();
   float2* R = cta_fft<-1>(A, B, dM, nr, 1, ld);
   float2* dst = out + (long)item * bt.out_stride + (long)r0 * out_pitch;
@@ -96,10 +125,16 @@ __global__ void k_row_c2r(const float2* in, long in_pitch, float* out, long out_
   const int r0 = blockIdx.x * rows;
   const int nr = min(rows, H - r0);
   const float2* src = in + batch_in_off(bt, item) + (long)r0 * in_pitch;
-  for (int t = threadIdx.x; t < nr * (M + 1); t += blockDim.x) {
-    const int r = t / (M + 1), k = t - r * (M + 1);
-    B[r * ld + k] = src[(long)r * in_pitch + k];
-  }
+  staged_copy<kStageLoads>(
+      nr * (M + 1),
+      [&](int t) {
+        const int r = t / (M + 1), k = t - r * (M + 1);
+        return src[(long)r * in_pitch + k];
+      },
+      [&](int t, float2 v) {
+        const int r = t / (M + 1), k = t - r * (M + 1);
+        B[r * ld + k] = v;
+      });
   __syncthreads();
   for (int t = threadIdx.x; t < nr * M; t += blockDim.x) {
     const int r = t / M, k = t - r * M;
@@ -131,16 +166,22 @@ __global__ void k_col_fft(const float2* in, float2* out, long pitch, int cmpX, i
   const float2* src = in + batch_in_off(bt, item);
   const float2* ex = ops.ex ? ops.ex + (long)item * cmpX : nullptr;
   const float2* ey = ops.ey ? ops.ey + (long)item * H : nullptr;
-  for (int t = threadIdx.x; t < TX * H; t += blockDim.x) {
-    const int y = t / TX, c = t - y * TX;
-    const int x = x0 + c;
-    float2 v = c2(0.f, 0.f);
-    if (x < cmpX) {
-      v = src[(long)y * pitch + x];
-      if (ex) v = cmul(v, cmul(ex[x], ey[y]));
-    }
-    A[c * ld + y] = v;
-  }
+  staged_copy<kStageLoads>(
+      TX * H,
+      [&](int t) {
+        const int y = t / TX, c = t - y * TX;
+        const int x = x0 + c;
+        float2 v = c2(0.f, 0.f);
+        if (x < cmpX) {
+          v = src[(long)y * pitch + x];
+          if (ex) v = cmul(v, cmul(ex[x], ey[y]));
+        }
+        return v;
+      },
+      [&](int t, float2 v) {
+        const int y = t / TX, c = t - y * TX;
+        A[c * ld + y] = v;
+      });
   __syncthreads();
   float2* R = ops.dir < 0 ? cta_fft<-1>(A, B, dH, TX, 1, ld) : cta_fft<1>(A, B, dH, TX, 1, ld);
   float2* dst = out + (long)item * bt.out_stride;
@@ -177,11 +218,20 @@ __global__ void __launch_bounds__(512, 2) k_row_r2c_ip(const float* __restrict__
   const int r0 = blockIdx.x * rows;
   const int nr = min(rows, H - r0);
   const float* src = in + batch_in_off(bt, item) + (long)r0 * in_pitch;
-  for (int t = threadIdx.x; t < nr * M; t += blockDim.x) {
-    const int r = t / M, m = t - r * M;
-    const float* p = src + (long)r * in_pitch + 2 * m;
-    sm[r * ld + spad(m)] = c2(p[0], p[1]);
-  }
+  // 8-byte loads when every row start is 8-byte aligned (patch extraction
+  // offsets can be odd).
+  const bool pair = ((reinterpret_cast<uintptr_t>(src) & 7) == 0) && !(in_pitch & 1);
+  staged_copy<kStageLoads>(
+      nr * M,
+      [&](int t) {
+        const int r = t / M, m = t - r * M;
+        const float* p = src + (long)r * in_pitch + 2 * m;
+        return pair ? *reinterpret_cast<const float2*>(p) : c2(p[0], p[1]);
+      },
+      [&](int t, float2 v) {
+        const int r = t / M, m = t - r * M;
+        sm[r * ld + spad(m)] = v;
+      });
   __syncthreads();
   cta_fft_inplace<-1, MAXB>(sm, dM, nr, ld);
   const int np = M / 2 + 1;
@@ -208,10 +258,16 @@ __global__ void __launch_bounds__(512, 2) k_row_c2r_ip(const float2* in, long in
   const int r0 = blockIdx.x * rows;
   const int nr = min(rows, H - r0);
   const float2* src = in + batch_in_off(bt, item) + (long)r0 * in_pitch;
-  for (int t = threadIdx.x; t < nr * (M + 1); t += blockDim.x) {
-    const int r = t / (M + 1), k = t - r * (M + 1);
-    sm[r * ld + spad(k)] = src[(long)r * in_pitch + k];
-  }
+  staged_copy<kStageLoads>(
+      nr * (M + 1),
+      [&](int t) {
+        const int r = t / (M + 1), k = t - r * (M + 1);
+        return src[(long)r * in_pitch + k];
+      },
+      [&](int t, float2 v) {
+        const int r = t / (M + 1), k = t - r * (M + 1);
+        sm[r * ld + spad(k)] = v;
+      });
   __syncthreads();
   const int np = M / 2 + 1;
   for (int t = threadIdx.x; t < nr * np; t += blockDim.x) {
@@ -221,12 +277,17 @@ __global__ void __launch_bounds__(512, 2) k_row_c2r_ip(const float2* in, long in
   __syncthreads();
   cta_fft_inplace<1, MAXB>(sm, dM, nr, ld);
   float* dst = out + (long)item * bt.out_stride + (long)r0 * out_pitch;
+  const bool pair = ((reinterpret_cast<uintptr_t>(dst) & 7) == 0) && !(out_pitch & 1);
   for (int t = threadIdx.x; t < nr * M; t += blockDim.x) {
     const int r = t / M, m = t - r * M;
     const float2 v = sm[r * ld + spad(m)];
     float* p = dst + (long)r * out_pitch + 2 * m;
-    p[0] = v.x;
-    p[1] = v.y;
+    if (pair) {
+      *reinterpret_cast<float2*>(p) = v;
+    } else {
+      p[0] = v.x;
+      p[1] = v.y;
+    }
   }
 }
 
@@ -241,16 +302,22 @@ __global__ void __launch_bounds__(512, 2) k_col_fft_ip(const float2* in, float2*
   const float2* src = in + batch_in_off(bt, item);
   const float2* ex = ops.ex ? ops.ex + (long)item * cmpX : nullptr;
   const float2* ey = ops.ey ? ops.ey + (long)item * H : nullptr;
-  for (int t = threadIdx.x; t < TX * H; t += blockDim.x) {
-    const int y = t / TX, c = t - y * TX;
-    const int x = x0 + c;
-    float2 v = c2(0.f, 0.f);
-    if (x < cmpX) {
-      v = src[(long)y * pitch + x];
-      if (ex) v = cmul(v, cmul(ex[x], ey[y]));
-    }
-    sm[c * ld + spad(y)] = v;
-  }
+  staged_copy<kStageLoads>(
+      TX * H,
+      [&](int t) {
+        const int y = t / TX, c = t - y * TX;
+        const int x = x0 + c;
+        float2 v = c2(0.f, 0.f);
+        if (x < cmpX) {
+          v = src[(long)y * pitch + x];
+          if (ex) v = cmul(v, cmul(ex[x], ey[y]));
+        }
+        return v;
+      },
+      [&](int t, float2 v) {
+        const int y = t / TX, c = t - y * TX;
+        sm[c * ld + spad(y)] = v;
+      });
   __syncthreads();
   if (ops.dir < 0) cta_fft_inplace<-1, MAXB>(sm, dH, TX, ld);
   else cta_fft_inplace<1, MAXB>(sm, dH, TX, ld);

