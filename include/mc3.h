@@ -30,6 +30,7 @@ extern "C" {
 #define MC3_ETIMEOUT 4    /* a bounded device wait gave up */
 #define MC3_EIO 5         /* file could not be read or written */
 #define MC3_EUNSUPPORTED 6 /* option or size outside the implemented path */
+#define MC3_ETOOBIG 7     /* size above the fixed scratch of a no-allocation entry point */
 
 typedef struct mc3_ctx mc3_ctx;
 
@@ -125,6 +126,23 @@ int mc3_fft_inverse(float* frames, int nx, int ny, int nz, void* stream);
  * e^{i 2pi (kx sx/Nx + ky sy/Ny)} on a [cmp_y][cmp_x] half spectrum. */
 int mc3_phase_shift(const float* in, float* out, int cmp_x, int cmp_y, float sx, float sy,
                     int accumulate, void* stream);
+/* No counterpart in the reference.  The same phase shift as mc3_phase_shift,
+ * for callers that cannot allocate device memory while they run (an
+ * application that owns a fixed memory pool or budget, or a latency-bound
+ * path where cudaMalloc/cudaFree would stall the device): it calls no
+ * cudaMalloc, cudaFree or allocating library routine.  Its scratch is a
+ * fixed device array of 197,120 bytes inside libmc3, so cmp_x may be at most
+ * MC3_NOALLOC_MAX_CMP_X and cmp_y at most MC3_NOALLOC_MAX_CMP_Y; larger sizes
+ * return MC3_ETOOBIG.  The first call on a device looks up that array's
+ * address (once per device, the device current); make that first call before
+ * any stream capture.  Every call on a device shares the one array, so calls
+ * that overlap on the GPU (other streams, other host threads) race; calls in
+ * one stream are ordered.  Asynchronous: unlike mc3_phase_shift it does not
+ * synchronise `stream` before returning. */
+#define MC3_NOALLOC_MAX_CMP_X 8193
+#define MC3_NOALLOC_MAX_CMP_Y 16384
+int mc3_phase_shift_noalloc(const float* in, float* out, int cmp_x, int cmp_y, float sx,
+                            float sy, int accumulate, void* stream);
 /* Util::GFourierResize2D::DoIt (Util/GFourierResize2D.cu:110-126), copy mode. */
 int mc3_fourier_crop(const float* in, int in_cmp_x, int in_cmp_y, float* out, int out_cmp_x,
                      int out_cmp_y, void* stream);

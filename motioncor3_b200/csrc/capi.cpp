@@ -33,6 +33,7 @@ const char* mc3_strerror(int code) {
     case MC3_ETIMEOUT: return "device wait timed out";
     case MC3_EIO: return "file I/O error";
     case MC3_EUNSUPPORTED: return "unsupported option or size";
+    case MC3_ETOOBIG: return "size exceeds the fixed scratch of the no-allocation entry point";
     default: return "unknown error";
   }
 }
