@@ -232,6 +232,7 @@ def run_ours(args, wl, world, rank, local):
     host_frames = frames.cpu().pin_memory()
     host_sums = torch.empty((info["n_sums"], ny, nx), dtype=torch.float32).pin_memory()
     hf, hs = host_frames.numpy(), host_sums.numpy()
+    mc.prefetch(hf)
     mc.process(hf, sums_out=hs)
     barrier()
     torch.cuda.synchronize()
@@ -239,7 +240,12 @@ def run_ours(args, wl, world, rank, local):
     f0 = torch.cuda.Event(enable_timing=True)
     f1 = torch.cuda.Event(enable_timing=True)
     f0.record(stream)
-    for _ in range(args.steps):
+    # every step copies its movie host->device and its sums back; the copy of
+    # movie k+1 runs on the copy stream while movie k is processed
+    mc.prefetch(hf)
+    for i in range(args.steps):
+        if i + 1 < args.steps:
+            mc.prefetch(hf)
         mc.process(hf, sums_out=hs)
     f1.record(stream)
     torch.cuda.synchronize()

@@ -101,8 +101,18 @@ int mc3_create(const mc3_params* p, mc3_ctx** out);
 int mc3_destroy(mc3_ctx* ctx);
 /* Work stream (cudaStream_t); NULL = the context's own stream. */
 int mc3_set_stream(mc3_ctx* ctx, void* stream);
-/* Buffer geometry for a movie size (CBufferPool.cpp:185-270). */
+/* Buffer geometry for a movie size (CBufferPool.cpp:185-270); also reserves
+ * the context's device buffers for that size (CBufferPool::CreateBuffers,
+ * CBufferPool.cpp:95-183), so the first mc3_process_movie does not pay for
+ * the allocation. */
 int mc3_plan(mc3_ctx* ctx, int nx, int ny, int nz, mc3_plan_info* info);
+/* Page-locked host memory for movies and sums (the reference keeps frames
+ * that do not fit on the GPU in cudaMallocHost buffers,
+ * CGpuBuffer.cpp:156-175, and reads raw frames over the link from pinned
+ * memory, MrcUtil/GApplyRefsToFrame.cu:129): copies from it run at full link
+ * speed and can overlap kernels. */
+int mc3_host_alloc(size_t bytes, void** ptr);
+int mc3_host_free(void* ptr);
 /* Gain reference [ny][nx] float (CLoadRefs::LoadGain, CLoadRefs.cpp:82-95);
  * NULL clears it. */
 int mc3_set_gain(mc3_ctx* ctx, const float* gain, int nx, int ny, int on_device);
@@ -114,6 +124,17 @@ int mc3_set_gain(mc3_ctx* ctx, const float* gain, int nx, int ny, int on_device)
  * BadPixel::CDetectMain::DoIt, BadPixel::CCorrectMain::DoIt and
  * Align::CAlignMain::DoIt (Align/CAlignMain.cpp:39-75). */
 int mc3_process_movie(mc3_ctx* ctx, const mc3_movie* movie, mc3_result* out);
+/* Loading the next movie while the current one is processed, as the
+ * reference's loader thread does (MrcUtil/CLoadCryoEMStack.cpp:130-180):
+ * starts the host->device copy of `movie`'s raw frames on the context's
+ * copy stream and returns.  The following mc3_process_movie calls must
+ * pass the prefetched movies in the same order (same frames pointer and
+ * size; MC3_EINVAL otherwise); at most two may be outstanding.  The host
+ * frames must stay valid and unchanged until their mc3_process_movie
+ * returns, and must be pinned (mc3_host_alloc, cudaHostAlloc or
+ * cudaHostRegister) for the copy to overlap.  Device-resident movies need
+ * no prefetch (no-op). */
+int mc3_prefetch_movie(mc3_ctx* ctx, const mc3_movie* movie);
 
 /* ---- components (device pointers unless stated) ---- */
 /* Util::CCufft2D::Forward (Util/CCufft2D.cpp:65-87): in-place R2C of nz

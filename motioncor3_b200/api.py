@@ -104,8 +104,11 @@ _SIGS = {
     "mc3_destroy": ([_VP], _I),
     "mc3_set_stream": ([_VP, _VP], _I),
     "mc3_plan": ([_VP, _I, _I, _I, ctypes.POINTER(_PlanInfo)], _I),
+    "mc3_host_alloc": ([ctypes.c_size_t, ctypes.POINTER(_VP)], _I),
+    "mc3_host_free": ([_VP], _I),
     "mc3_set_gain": ([_VP, _VP, _I, _I, _I], _I),
     "mc3_process_movie": ([_VP, ctypes.POINTER(_Movie), ctypes.POINTER(_Result)], _I),
+    "mc3_prefetch_movie": ([_VP, ctypes.POINTER(_Movie)], _I),
     "mc3_fft_forward": ([_VP, _I, _I, _I, _I, _VP], _I),
     "mc3_fft_inverse": ([_VP, _I, _I, _I, _VP], _I),
     "mc3_phase_shift": ([_VP, _VP, _I, _I, _F, _F, _I, _VP], _I),
@@ -236,6 +239,7 @@ class MotionCor3:
         h = _VP()
         _check(_lib().mc3_create(ctypes.byref(self._p), ctypes.byref(h)), "mc3_create")
         self._h = h
+        self._prefetched = []  # host arrays whose copies are in flight
 
     def close(self) -> None:
         if getattr(self, "_h", None):
@@ -275,8 +279,8 @@ class MotionCor3:
             g = np.ascontiguousarray(gain, dtype=np.float32)
             _check(_lib().mc3_set_gain(self._h, _hp(g), g.shape[1], g.shape[0], 0), "mc3_set_gain")
 
-    def process(self, frames, sums_out=None) -> Result:
-        """frames: [nz][ny][nx] numpy array (host) or torch CUDA tensor."""
+    @staticmethod
+    def _movie(frames):
         on_dev = hasattr(frames, "data_ptr")
         if on_dev:
             import torch
@@ -293,6 +297,20 @@ class MotionCor3:
                 raise MC3Error(MC3_EUNSUPPORTED, "frame dtype")
             nz, ny, nx = keep.shape
             fptr = keep.ctypes.data_as(_VP)
+        return _Movie(fptr, dt, nx, ny, nz, 1 if on_dev else 0), keep
+
+    def prefetch(self, frames) -> None:
+        """Starts copying a later movie's host frames to the device
+        (mc3_prefetch_movie); pass the same array to a later process()."""
+        mv, keep = self._movie(frames)
+        _check(_lib().mc3_prefetch_movie(self._h, ctypes.byref(mv)), "mc3_prefetch_movie")
+        if not mv.on_device:
+            self._prefetched.append(keep)
+
+    def process(self, frames, sums_out=None) -> Result:
+        """frames: [nz][ny][nx] numpy array (host) or torch CUDA tensor."""
+        mv, keep = self._movie(frames)
+        nx, ny, nz = mv.nx, mv.ny, mv.nz
         info = self.plan(nx, ny, nz)
         ns, P = info["n_sums"], info["n_patches"]
         it = int(self.params.iter)
@@ -321,9 +339,10 @@ class MotionCor3:
         r.patch_bad = pb.ctypes.data if P else None
         r.iterations = iters.ctypes.data
         r.errors = errs.ctypes.data
-        mv = _Movie(fptr, dt, nx, ny, nz, 1 if on_dev else 0)
         _check(_lib().mc3_process_movie(self._h, ctypes.byref(mv), ctypes.byref(r)),
                "mc3_process_movie")
+        if not mv.on_device and self._prefetched:
+            self._prefetched.pop(0)
         del keep
         return Result(sums=sums, global_shifts=gsh, patch_shifts=psh if P else None,
                       patch_centers=pc if P else None, patch_bad=pb if P else None,

@@ -107,6 +107,22 @@ int mc3_plan(mc3_ctx* ctx, int nx, int ny, int nz, mc3_plan_info* info) {
   return ctx->eng->plan(nx, ny, nz, info);
 }
 
+int mc3_host_alloc(size_t bytes, void** ptr) {
+  if (!ptr || bytes == 0) return MC3_EINVAL;
+  *ptr = nullptr;
+  if (cudaHostAlloc(ptr, bytes, cudaHostAllocPortable) != cudaSuccess) {
+    cudaGetLastError();
+    *ptr = nullptr;
+    return MC3_ENOMEM;
+  }
+  return MC3_OK;
+}
+
+int mc3_host_free(void* ptr) {
+  if (!ptr) return MC3_OK;
+  return cudaFreeHost(ptr) == cudaSuccess ? MC3_OK : MC3_ECUDA;
+}
+
 int mc3_set_gain(mc3_ctx* ctx, const float* gain, int nx, int ny, int on_device) {
   if (!ctx) return MC3_EINVAL;
   return ctx->eng->set_gain(gain, nx, ny, on_device != 0);
@@ -115,6 +131,11 @@ int mc3_set_gain(mc3_ctx* ctx, const float* gain, int nx, int ny, int on_device)
 int mc3_process_movie(mc3_ctx* ctx, const mc3_movie* movie, mc3_result* out) {
   if (!ctx || !movie) return MC3_EINVAL;
   return ctx->eng->process(*movie, out);
+}
+
+int mc3_prefetch_movie(mc3_ctx* ctx, const mc3_movie* movie) {
+  if (!ctx || !movie) return MC3_EINVAL;
+  return ctx->eng->prefetch(*movie);
 }
 
 // ---- components ----

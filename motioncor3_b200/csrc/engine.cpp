@@ -89,17 +89,69 @@ Engine::Engine(const mc3_params& p) : prm(p) { device = p.gpu; }
 
 Engine::~Engine() {
   if (device >= 0) cudaSetDevice(device);
+  if (copy_stream) cudaStreamSynchronize(copy_stream);
+  for (int i = 0; i < 2; ++i) {
+    if (slot_loaded[i]) cudaEventDestroy(slot_loaded[i]);
+    if (slot_free[i]) cudaEventDestroy(slot_free[i]);
+  }
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
+  if (copy_stream) cudaStreamDestroy(copy_stream);
   if (own_stream) cudaStreamDestroy(own_stream);
 }
 
 int Engine::init() {
   MC3_CUDA(cudaSetDevice(device));
   MC3_CUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
+  MC3_CUDA(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
   stream = own_stream;
   MC3_CUDA(cudaEventCreate(&ev0));
   MC3_CUDA(cudaEventCreate(&ev1));
+  for (int i = 0; i < 2; ++i) {
+    MC3_CUDA(cudaEventCreateWithFlags(&slot_loaded[i], cudaEventDisableTiming));
+    MC3_CUDA(cudaEventCreateWithFlags(&slot_free[i], cudaEventDisableTiming));
+  }
+  return kOk;
+}
+
+namespace {
+int mode_bytes(int mode) {
+  switch (mode) {
+    case 0: return 1;
+    case 1: case 6: return 2;
+    case 2: return 4;
+    default: return 0;
+  }
+}
+}  // namespace
+
+// The reference overlaps loading the next movie with processing the
+// current one through its loader thread and pinned frame buffers
+// (MrcUtil/CLoadCryoEMStack.cpp:130-180, CGpuBuffer.cpp:156-175).  Here the
+// raw frames of a later movie are copied on a second stream into one of two
+// device slots while the caller's stream works on the current movie.
+int Engine::prefetch(const mc3_movie& mv) {
+  MC3_CUDA(cudaSetDevice(device));
+  if (!mv.frames || mv.nx < 1 || mv.ny < 1 || mv.nz < 1) return kEInval;
+  const int bpp = mode_bytes(mv.mode);
+  if (!bpp) return kEUnsupported;
+  if (mv.on_device) return kOk;  // nothing to copy
+  if (n_pending >= 2) {
+    last_error = "two movies are already prefetched; process one first";
+    return kEInval;
+  }
+  const size_t bytes = (size_t)bpp * mv.nx * mv.ny * mv.nz;
+  const int slot = next_slot;
+  if (d_rawslot[slot].cap < bytes) {
+    // growing the slot frees it: wait for its last reader first
+    MC3_CUDA(cudaEventSynchronize(slot_free[slot]));
+    MC3_TRY(d_rawslot[slot].ensure(bytes));
+  }
+  MC3_CUDA(cudaStreamWaitEvent(copy_stream, slot_free[slot], 0));
+  MC3_CUDA(cudaMemcpyAsync(d_rawslot[slot].p, mv.frames, bytes, cudaMemcpyHostToDevice, copy_stream));
+  MC3_CUDA(cudaEventRecord(slot_loaded[slot], copy_stream));
+  pending[n_pending++] = Pending{mv.frames, bytes, slot};
+  next_slot ^= 1;
   return kOk;
 }
 
@@ -141,6 +193,25 @@ int Engine::plan(int w, int h, int n, mc3_plan_info* info) {
   size_t bytes = cmp * g.N + xcf * g.N + cmp * (g.nSums + 2) + (size_t)g.W * g.H * 4 * g.N;
   if (g.patch) bytes += (size_t)g.P * g.N * g.patCmpX * g.patCmpY * sizeof(float2) + 2 * cmp * 32;
   info->device_bytes = bytes;
+  // Reserve the large per-movie buffers now, as the reference creates its
+  // buffer pool before processing (CMain::mCreateBufferPool, CMain.cpp:400-427);
+  // process() reuses them (grow-only, same sizes).
+  MC3_CUDA(cudaSetDevice(device));
+  const size_t ncmp = (size_t)g.cmpX * g.cmpY;
+  const size_t nxcf = (size_t)g.xcfCmpX * g.xcfCmpY;
+  MC3_TRY(d_frames.ensure(sizeof(float2) * ncmp * g.N));
+  MC3_TRY(d_sum.ensure(sizeof(float) * (size_t)g.padX * g.H));
+  if (prm.correct_bad) {
+    MC3_TRY(d_cc.ensure(sizeof(float) * (size_t)g.padX * g.H));
+    MC3_TRY(d_bad.ensure((size_t)g.W * g.H));
+  }
+  MC3_TRY(d_xcf.ensure(sizeof(float2) * nxcf * g.N));
+  MC3_TRY(d_sums.ensure(sizeof(float2) * ncmp * g.nSums));
+  MC3_TRY(d_Wn.ensure(sizeof(float) * ncmp));
+  if (g.patch) {
+    MC3_TRY(d_pat.ensure(sizeof(float2) * (size_t)g.patCmpX * g.patCmpY * g.N * g.P));
+    MC3_TRY(d_gath.ensure(sizeof(float2) * ncmp * g.N));
+  }
   return kOk;
 }
 
@@ -262,7 +333,20 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
   MC3_CUDA(cudaEventRecord(ev0, st));
   // ---- 1. raw frames on the device ----
   const void* raw = mv.frames;
-  if (!mv.on_device) {
+  int used_slot = -1;
+  if (!mv.on_device && n_pending > 0) {
+    // the oldest prefetched movie must be this one
+    const Pending pf = pending[0];
+    if (pf.host != mv.frames || pf.bytes != (size_t)bpp * npx * N) {
+      last_error = "movie differs from the oldest prefetched movie";
+      return kEInval;
+    }
+    pending[0] = pending[1];
+    --n_pending;
+    MC3_CUDA(cudaStreamWaitEvent(st, slot_loaded[pf.slot], 0));
+    raw = d_rawslot[pf.slot].p;
+    used_slot = pf.slot;
+  } else if (!mv.on_device) {
     MC3_TRY(d_raw.ensure((size_t)bpp * npx * N));
     MC3_CUDA(cudaMemcpyAsync(d_raw.p, mv.frames, (size_t)bpp * npx * N, cudaMemcpyHostToDevice, st));
     raw = d_raw.p;
@@ -274,6 +358,7 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
   const long fr_stride_f = (long)g.padX * H;
   MC3_TRY(gain_and_sum(raw, mv.mode, (long)npx, has_gain ? d_gain.as<float>() : nullptr, frames,
                        fr_stride_f, prm.correct_bad ? d_sum.as<float>() : nullptr, W, H, N, st));
+  if (used_slot >= 0) MC3_CUDA(cudaEventRecord(slot_free[used_slot], st));  // raw is read only above
   // ---- 3. hot pixels and defects (BadPixel/CDetectMain.cpp, CCorrectMain.cpp) ----
   if (prm.correct_bad) {
     MC3_TRY(d_cc.ensure(sizeof(float) * (size_t)g.padX * H));

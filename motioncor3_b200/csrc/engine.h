@@ -48,6 +48,9 @@ class Engine {
   int set_gain(const float* gain, int w, int h, bool on_device);
   int plan(int w, int h, int n, mc3_plan_info* info);
   int process(const mc3_movie& mv, mc3_result* out);
+  // Starts the host->device copy of a later movie's raw frames on the copy
+  // stream (at most two outstanding); process() consumes them in order.
+  int prefetch(const mc3_movie& mv);
 
   // Batched CIterativeAlign over `nstack` stacks of N spectra each.
   int align_stacks(const float2* spec, long stack_stride, int nstack, int cmpX, int cmpY, int N,
@@ -62,6 +65,20 @@ class Engine {
   cudaStream_t stream = nullptr;
   cudaStream_t own_stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  // Movie prefetch: two raw-frame slots filled on copy_stream.
+  struct Pending {
+    const void* host;
+    size_t bytes;
+    int slot;
+  };
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t slot_loaded[2] = {nullptr, nullptr};  // copy into the slot finished
+  cudaEvent_t slot_free[2] = {nullptr, nullptr};    // last read of the slot finished
+  DevBuf d_rawslot[2];
+  Pending pending[2];
+  int n_pending = 0;
+  int next_slot = 0;
   std::string last_error;
 
   // device buffers
