@@ -258,11 +258,76 @@ __global__ void __launch_bounds__(512, 2) k_corr_cols_ip(
   }
 }
 
+// Compile-time variant for power-of-two cmpY (H).
+template <int H>
+__global__ void __launch_bounds__(kCtThreads, 2) k_corr_cols_ct(
+    const float2* __restrict__ spec, const int* act, const float2* __restrict__ ex,
+    const float2* __restrict__ ey, const float2* __restrict__ S, const int* gstart,
+    const int* gsize, float bf, int phase_only, float2* T, int cmpX, int N, long sstride, int G,
+    int seaY, const float2* __restrict__ tw) {
+  constexpr int LD = ct_spad_len(H);
+  constexpr int TX = ct_batch(LD);
+  extern __shared__ float2 sm[];
+  const int a = blockIdx.z;
+  const int g = blockIdx.y;
+  const int x0 = blockIdx.x * TX;
+  const long nel = (long)cmpX * H;
+  const float2* X = spec + (long)act[a] * sstride;
+  const float2* Sa = S + (long)a * nel;
+  const int f0 = gstart[g], gs = gsize[g];
+  const float fFilt0 = -0.25f * bf / ((unsigned)(cmpX - 1) * (unsigned)H);
+#pragma unroll 4
+  for (int t = threadIdx.x; t < TX * H; t += kCtThreads) {
+    const int y = t / TX, c = t % TX;
+    const int x = x0 + c;
+    float2 C = c2(0.f, 0.f);
+    if (x < cmpX) C = corr_value(X, ex, ey, Sa, a, N, f0, gs, x, y, cmpX, H, nel, fFilt0, phase_only);
+    sm[c * LD + spad(y)] = C;
+  }
+  __syncthreads();
+  cta_fft_ct<1, H, TX, kCtThreads, LD>(sm, tw, 1);
+  const int y0 = (H - seaY) / 2;
+  float2* Tg = T + ((long)a * G + g) * seaY * cmpX;
+  for (int t = threadIdx.x; t < TX * seaY; t += kCtThreads) {
+    const int yi = t / TX, c = t % TX;
+    const int x = x0 + c;
+    if (x < cmpX) Tg[(long)yi * cmpX + x] = sm[c * LD + spad(y0 + yi)];
+  }
+}
+
+template <int H>
+int launch_corr_cols_ct(const float2* spec, const int* act, const float2* ex, const float2* ey,
+                        const float2* S, const int* gstart, const int* gsize, float bfactor,
+                        int phase_only, float2* T, const AlignDims& d, const float2* tw,
+                        cudaStream_t st) {
+  constexpr int LD = ct_spad_len(H);
+  constexpr int TX = ct_batch(LD);
+  const size_t smem = (size_t)TX * LD * sizeof(float2);
+  MC3_TRY(set_smem_attr(k_corr_cols_ct<H>, smem));
+  dim3 grid(ceil_div(d.cmpX, TX), d.G, d.A);
+  k_corr_cols_ct<H><<<grid, kCtThreads, smem, st>>>(spec, act, ex, ey, S, gstart, gsize, bfactor,
+                                                    phase_only, T, d.cmpX, d.N, d.stack_stride,
+                                                    d.G, d.seaY, tw);
+  MC3_CHECK_LAUNCH("k_corr_cols_ct");
+  return kOk;
+}
+
 int corr_cols(const float2* spec, const int* act, const float2* ex, const float2* ey,
               const float2* S, const int* gstart, const int* gsize, float bfactor,
               int phase_only, float2* T, const AlignDims& d, cudaStream_t st) {
   FftDesc dH;
   MC3_TRY(make_desc(d.cmpY, d.cmpY, &dH));
+  if (all_dedicated(dH) && !getenv("MC3_FFT_PINGPONG") && !getenv("MC3_FFT_RUNTIME_PLAN")) {
+    prof::Scope ps("k_corr_cols", (double)d.A * ((double)d.cmpX * d.cmpY * 8.0 * (d.N + 1) + (double)d.G * d.seaY * d.cmpX * 8.0), st);
+    switch (d.cmpY) {
+      case 256: return launch_corr_cols_ct<256>(spec, act, ex, ey, S, gstart, gsize, bfactor, phase_only, T, d, dH.tw, st);
+      case 512: return launch_corr_cols_ct<512>(spec, act, ex, ey, S, gstart, gsize, bfactor, phase_only, T, d, dH.tw, st);
+      case 1024: return launch_corr_cols_ct<1024>(spec, act, ex, ey, S, gstart, gsize, bfactor, phase_only, T, d, dH.tw, st);
+      case 2048: return launch_corr_cols_ct<2048>(spec, act, ex, ey, S, gstart, gsize, bfactor, phase_only, T, d, dH.tw, st);
+      case 4096: return launch_corr_cols_ct<4096>(spec, act, ex, ey, S, gstart, gsize, bfactor, phase_only, T, d, dH.tw, st);
+      default: break;
+    }
+  }
   if (all_dedicated(dH) && !getenv("MC3_FFT_PINGPONG")) {
     const int ld = spad_len(d.cmpY);
     int rmin = 8;

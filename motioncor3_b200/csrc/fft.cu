@@ -338,6 +338,193 @@ __global__ void __launch_bounds__(512, 2) k_col_fft_ip(const float2* in, float2*
   }
 }
 
+// ---------------------------------------------------------------------
+// Compile-time variants of the in-place kernels for power-of-two lengths
+// (M complex per row, H per column): the sequence length, the sequences
+// per CTA and the padded stride are template constants.
+// ---------------------------------------------------------------------
+template <int M>
+__global__ void __launch_bounds__(kCtThreads, 2) k_row_r2c_ct(const float* __restrict__ in,
+                                                              long in_pitch, float2* out,
+                                                              long out_pitch, int H, Batch bt,
+                                                              const float2* __restrict__ tw,
+                                                              float scale) {
+  constexpr int LD = ct_spad_len(M + 1);
+  constexpr int ROWS = ct_batch(LD);
+  extern __shared__ float2 sm[];
+  const int item = blockIdx.y;
+  const int r0 = blockIdx.x * ROWS;
+  const int nr = min(ROWS, H - r0);
+  const float* src = in + batch_in_off(bt, item) + (long)r0 * in_pitch;
+  const bool pair = ((reinterpret_cast<uintptr_t>(src) & 7) == 0) && !(in_pitch & 1);
+  staged_copy<kStageLoads>(
+      nr * M,
+      [&](int t) {
+        const int r = t / M, m = t % M;
+        const float* p = src + (long)r * in_pitch + 2 * m;
+        return pair ? *reinterpret_cast<const float2*>(p) : c2(p[0], p[1]);
+      },
+      [&](int t, float2 v) {
+        const int r = t / M, m = t % M;
+        sm[r * LD + spad(m)] = v;
+      });
+  __syncthreads();
+  // tw: the 2M-point table, read every second entry by the M-point stages
+  cta_fft_ct<-1, M, ROWS, kCtThreads, LD>(sm, tw, 2);
+  constexpr int NP = M / 2 + 1;
+  for (int t = threadIdx.x; t < nr * NP; t += kCtThreads) {
+    const int r = t / NP, p = t % NP;
+    r2c_post_pair(sm + r * LD, M, p, tw, scale);
+  }
+  __syncthreads();
+  float2* dst = out + (long)item * bt.out_stride + (long)r0 * out_pitch;
+  for (int t = threadIdx.x; t < nr * (M + 1); t += kCtThreads) {
+    const int r = t / (M + 1), k = t % (M + 1);
+    dst[(long)r * out_pitch + k] = sm[r * LD + spad(k)];
+  }
+}
+
+template <int M>
+__global__ void __launch_bounds__(kCtThreads, 2) k_row_c2r_ct(const float2* in, long in_pitch,
+                                                              float* out, long out_pitch, int H,
+                                                              Batch bt,
+                                                              const float2* __restrict__ tw) {
+  constexpr int LD = ct_spad_len(M + 1);
+  constexpr int ROWS = ct_batch(LD);
+  extern __shared__ float2 sm[];
+  const int item = blockIdx.y;
+  const int r0 = blockIdx.x * ROWS;
+  const int nr = min(ROWS, H - r0);
+  const float2* src = in + batch_in_off(bt, item) + (long)r0 * in_pitch;
+  staged_copy<kStageLoads>(
+      nr * (M + 1),
+      [&](int t) {
+        const int r = t / (M + 1), k = t % (M + 1);
+        return src[(long)r * in_pitch + k];
+      },
+      [&](int t, float2 v) {
+        const int r = t / (M + 1), k = t % (M + 1);
+        sm[r * LD + spad(k)] = v;
+      });
+  __syncthreads();
+  constexpr int NP = M / 2 + 1;
+  for (int t = threadIdx.x; t < nr * NP; t += kCtThreads) {
+    const int r = t / NP, p = t % NP;
+    c2r_pre_pair(sm + r * LD, M, p, tw);
+  }
+  __syncthreads();
+  cta_fft_ct<1, M, ROWS, kCtThreads, LD>(sm, tw, 2);
+  float* dst = out + (long)item * bt.out_stride + (long)r0 * out_pitch;
+  const bool pair = ((reinterpret_cast<uintptr_t>(dst) & 7) == 0) && !(out_pitch & 1);
+  for (int t = threadIdx.x; t < nr * M; t += kCtThreads) {
+    const int r = t / M, m = t % M;
+    const float2 v = sm[r * LD + spad(m)];
+    float* p = dst + (long)r * out_pitch + 2 * m;
+    if (pair) {
+      *reinterpret_cast<float2*>(p) = v;
+    } else {
+      p[0] = v.x;
+      p[1] = v.y;
+    }
+  }
+}
+
+template <int H>
+__global__ void __launch_bounds__(kCtThreads, 2) k_col_fft_ct(const float2* in, float2* out,
+                                                              long pitch, int cmpX, Batch bt,
+                                                              const float2* __restrict__ tw,
+                                                              ColOps ops) {
+  constexpr int LD = ct_spad_len(H);
+  constexpr int TX = ct_batch(LD);
+  extern __shared__ float2 sm[];
+  const int item = blockIdx.y;
+  const int x0 = blockIdx.x * TX;
+  const float2* src = in + batch_in_off(bt, item);
+  const float2* ex = ops.ex ? ops.ex + (long)item * cmpX : nullptr;
+  const float2* ey = ops.ey ? ops.ey + (long)item * H : nullptr;
+  staged_copy<kStageLoads>(
+      TX * H,
+      [&](int t) {
+        const int y = t / TX, c = t % TX;
+        const int x = x0 + c;
+        float2 v = c2(0.f, 0.f);
+        if (x < cmpX) {
+          v = src[(long)y * pitch + x];
+          if (ex) v = cmul(v, cmul(ex[x], ey[y]));
+        }
+        return v;
+      },
+      [&](int t, float2 v) {
+        const int y = t / TX, c = t % TX;
+        sm[c * LD + spad(y)] = v;
+      });
+  __syncthreads();
+  if (ops.dir < 0) cta_fft_ct<-1, H, TX, kCtThreads, LD>(sm, tw, 1);
+  else cta_fft_ct<1, H, TX, kCtThreads, LD>(sm, tw, 1);
+  float2* dst = out + (long)item * bt.out_stride;
+  float2* crop = ops.crop ? ops.crop + (long)item * ops.crop_x * ops.crop_y : nullptr;
+  for (int t = threadIdx.x; t < TX * H; t += kCtThreads) {
+    const int y = t / TX, c = t % TX;
+    const int x = x0 + c;
+    if (x >= cmpX) continue;
+    const float2 v = cscale(sm[c * LD + spad(y)], ops.scale);
+    dst[(long)y * pitch + x] = v;
+    if (crop && x < ops.crop_x) {
+      int yo = -1;
+      if (y <= ops.crop_y / 2) yo = y;
+      else if (y > H - ops.crop_y / 2) yo = y - H + ops.crop_y;
+      if (yo >= 0) crop[(long)yo * ops.crop_x + x] = v;
+    }
+  }
+}
+
+namespace {
+template <int M>
+int launch_row_r2c_ct(const float* in, long in_pitch, float2* out, long out_pitch, int H,
+                      const Batch& b, const float2* tw, float scale, cudaStream_t st) {
+  constexpr int LD = ct_spad_len(M + 1);
+  constexpr int ROWS = ct_batch(LD);
+  const size_t smem = (size_t)ROWS * LD * sizeof(float2);
+  MC3_TRY(set_smem_attr(k_row_r2c_ct<M>, smem));
+  dim3 grid(ceil_div(H, ROWS), b.items);
+  k_row_r2c_ct<M><<<grid, kCtThreads, smem, st>>>(in, in_pitch, out, out_pitch, H, b, tw, scale);
+  MC3_CHECK_LAUNCH("k_row_r2c_ct");
+  return kOk;
+}
+template <int M>
+int launch_row_c2r_ct(const float2* in, long in_pitch, float* out, long out_pitch, int H,
+                      const Batch& b, const float2* tw, cudaStream_t st) {
+  constexpr int LD = ct_spad_len(M + 1);
+  constexpr int ROWS = ct_batch(LD);
+  const size_t smem = (size_t)ROWS * LD * sizeof(float2);
+  MC3_TRY(set_smem_attr(k_row_c2r_ct<M>, smem));
+  dim3 grid(ceil_div(H, ROWS), b.items);
+  k_row_c2r_ct<M><<<grid, kCtThreads, smem, st>>>(in, in_pitch, out, out_pitch, H, b, tw);
+  MC3_CHECK_LAUNCH("k_row_c2r_ct");
+  return kOk;
+}
+template <int H>
+int launch_col_fft_ct(const float2* in, float2* out, long pitch, int cmpX, const Batch& b,
+                      const float2* tw, const ColOps& ops, cudaStream_t st) {
+  constexpr int LD = ct_spad_len(H);
+  constexpr int TX = ct_batch(LD);
+  const size_t smem = (size_t)TX * LD * sizeof(float2);
+  MC3_TRY(set_smem_attr(k_col_fft_ct<H>, smem));
+  dim3 grid(ceil_div(cmpX, TX), b.items);
+  k_col_fft_ct<H><<<grid, kCtThreads, smem, st>>>(in, out, pitch, cmpX, b, tw, ops);
+  MC3_CHECK_LAUNCH("k_col_fft_ct");
+  return kOk;
+}
+// MC3_FFT_RUNTIME_PLAN=1 keeps the runtime-plan in-place kernels (A/B runs).
+bool ct_off() {
+  static const bool off = [] {
+    const char* e = getenv("MC3_FFT_RUNTIME_PLAN");
+    return e && e[0] == '1';
+  }();
+  return off;
+}
+}  // namespace
+
 namespace {
 constexpr int kIpThreads = 512;
 constexpr int kIpBudget = 72 * 1024;   // shared memory per CTA, in-place kernels
@@ -385,6 +572,17 @@ int row_r2c(const float* in, long in_pitch, float2* out, long out_pitch, int W, 
   const int M = W / 2;
   FftDesc d;
   MC3_TRY(make_desc(M, W, &d));
+  if (use_inplace(d) && !ct_off()) {
+    prof::Scope ps("k_row_r2c", (double)b.items * H * (W * 4.0 + (W / 2 + 1) * 8.0), st);
+    switch (M) {
+      case 128: return launch_row_r2c_ct<128>(in, in_pitch, out, out_pitch, H, b, d.tw, scale, st);
+      case 256: return launch_row_r2c_ct<256>(in, in_pitch, out, out_pitch, H, b, d.tw, scale, st);
+      case 512: return launch_row_r2c_ct<512>(in, in_pitch, out, out_pitch, H, b, d.tw, scale, st);
+      case 1024: return launch_row_r2c_ct<1024>(in, in_pitch, out, out_pitch, H, b, d.tw, scale, st);
+      case 2048: return launch_row_r2c_ct<2048>(in, in_pitch, out, out_pitch, H, b, d.tw, scale, st);
+      default: break;
+    }
+  }
   if (use_inplace(d)) {
     const int ld = spad_len(M + 1);
     const int rows = ip_batch(d, ld, 2);
@@ -415,6 +613,17 @@ int row_c2r(const float2* in, long in_pitch, float* out, long out_pitch, int W, 
   const int M = W / 2;
   FftDesc d;
   MC3_TRY(make_desc(M, W, &d));
+  if (use_inplace(d) && !ct_off()) {
+    prof::Scope ps("k_row_c2r", (double)b.items * H * (W * 4.0 + (W / 2 + 1) * 8.0), st);
+    switch (M) {
+      case 128: return launch_row_c2r_ct<128>(in, in_pitch, out, out_pitch, H, b, d.tw, st);
+      case 256: return launch_row_c2r_ct<256>(in, in_pitch, out, out_pitch, H, b, d.tw, st);
+      case 512: return launch_row_c2r_ct<512>(in, in_pitch, out, out_pitch, H, b, d.tw, st);
+      case 1024: return launch_row_c2r_ct<1024>(in, in_pitch, out, out_pitch, H, b, d.tw, st);
+      case 2048: return launch_row_c2r_ct<2048>(in, in_pitch, out, out_pitch, H, b, d.tw, st);
+      default: break;
+    }
+  }
   if (use_inplace(d)) {
     const int ld = spad_len(M + 1);
     const int rows = ip_batch(d, ld, 2);
@@ -445,6 +654,17 @@ int col_fft(const float2* in, float2* out, long pitch, int cmpX, int H, const Ba
   if (ops.crop && (ops.crop_x > cmpX || ops.crop_y > H)) return kEInval;
   FftDesc d;
   MC3_TRY(make_desc(H, H, &d));
+  if (use_inplace(d) && !ct_off()) {
+    prof::Scope ps("k_col_fft", (double)b.items * ((double)cmpX * H * 16.0 + (ops.crop ? (double)ops.crop_x * ops.crop_y * 8.0 : 0.0)), st);
+    switch (H) {
+      case 256: return launch_col_fft_ct<256>(in, out, pitch, cmpX, b, d.tw, ops, st);
+      case 512: return launch_col_fft_ct<512>(in, out, pitch, cmpX, b, d.tw, ops, st);
+      case 1024: return launch_col_fft_ct<1024>(in, out, pitch, cmpX, b, d.tw, ops, st);
+      case 2048: return launch_col_fft_ct<2048>(in, out, pitch, cmpX, b, d.tw, ops, st);
+      case 4096: return launch_col_fft_ct<4096>(in, out, pitch, cmpX, b, d.tw, ops, st);
+      default: break;
+    }
+  }
   if (use_inplace(d)) {
     const int ld = spad_len(H);
     const int tx = ip_batch(d, ld, 2);

@@ -27,6 +27,18 @@ int make_desc(int n, int table_n, FftDesc* d);
 int col_tile(int H);      // columns per CTA for a length-H column pass
 int row_tile(int M);      // rows per CTA for a row pass of M complex values
 
+// Compile-time in-place passes (power-of-two lengths): threads per CTA,
+// shared memory per CTA (two CTAs per SM) and the number of padded
+// sequences of length n_padded that one CTA holds (a power of two <= 16).
+constexpr int kCtThreads = 512;
+constexpr int kCtBudget = 72 * 1024;
+__host__ __device__ constexpr int ct_batch(int n_padded) {
+  int nb = kCtBudget / (n_padded * (int)sizeof(float2));
+  int p = 1;
+  while (p * 2 <= nb && p < 16) p *= 2;
+  return p;
+}
+
 template <typename K>
 int set_smem_attr(K kernel, size_t bytes) {
   if (bytes > 48 * 1024) {

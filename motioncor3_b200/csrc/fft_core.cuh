@@ -319,6 +319,93 @@ __device__ void cta_fft_inplace(float2* buf, const FftDesc& d, int nb, int ld) {
 }
 #endif
 
+// ---- compile-time plans for power-of-two lengths -----------------------
+// The same factorisation as fft_factorize (so results are identical to the
+// runtime in-place path), evaluated at compile time: all index arithmetic
+// of a stage becomes shifts and masks and every loop unrolls.
+MC3_HD constexpr int ct_log2(int n) {
+  int l = 0;
+  while ((1 << l) < n) ++l;
+  return l;
+}
+MC3_HD constexpr int ct_nstages(int n) {
+  int p2 = ct_log2(n), ns = 0;
+  if (p2 >= 4 && p2 % 3 == 1) {
+    ns += 2;
+    p2 -= 4;
+  }
+  ns += p2 / 3;
+  if (p2 % 3) ++ns;
+  return ns;
+}
+MC3_HD constexpr int ct_radix(int n, int s) {
+  int p2 = ct_log2(n), first = 0;
+  if (p2 >= 4 && p2 % 3 == 1) {
+    if (s < 2) return 4;
+    first = 2;
+    p2 -= 4;
+  }
+  if (s < first + p2 / 3) return 8;
+  if (s == first + p2 / 3 && p2 % 3) return 1 << (p2 % 3);
+  return 1;
+}
+// Shared-memory words of a padded sequence of n elements (spad_len).
+MC3_HD constexpr int ct_spad_len(int n) { return n + (n >> 5) + 1; }
+
+#ifdef __CUDACC__
+// One in-place stage over NB sequences of N elements (sequence b at
+// buf[b*LD + spad(i)]) by a CTA of T threads; same arithmetic as
+// stage_inplace.
+template <int R, int DIR, int N, int NS, int NB, int T, int LD>
+__device__ __forceinline__ void stage_ct(float2* buf, const float2* __restrict__ tw, int tws) {
+  constexpr int per = N / R;
+  constexpr int items = NB * per;
+  constexpr int MB = (items + T - 1) / T;
+  float2 v[MB][R];
+  const unsigned tid = threadIdx.x;
+#pragma unroll
+  for (int m = 0; m < MB; ++m) {
+    const unsigned it = tid + m * T;
+    if (items % T == 0 || it < (unsigned)items) {
+      const unsigned b = it / per, j = it % per;
+      const float2* A = buf + b * LD;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[m][r] = A[spad(j + r * per)];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int m = 0; m < MB; ++m) {
+    const unsigned it = tid + m * T;
+    if (items % T == 0 || it < (unsigned)items) {
+      const unsigned b = it / per, j = it % per;
+      const unsigned k = j % NS;
+      if (NS > 1) {
+        const int step = (N / (NS * R)) * k;
+#pragma unroll
+        for (int r = 1; r < R; ++r) v[m][r] = cmul(v[m][r], twid<DIR>(tw, tws, step * r));
+      }
+      Dft<R, DIR>::run(v[m]);
+      const unsigned idxD = (j / NS) * NS * R + k;
+      float2* A = buf + b * LD;
+#pragma unroll
+      for (int r = 0; r < R; ++r) A[spad(idxD + r * NS)] = v[m][r];
+    }
+  }
+  __syncthreads();
+}
+
+// In-place CTA transform of NB sequences of power-of-two length N.
+template <int DIR, int N, int NB, int T, int LD, int S = 0, int NS = 1>
+__device__ __forceinline__ void cta_fft_ct(float2* buf, const float2* __restrict__ tw, int tws) {
+  if constexpr (S < ct_nstages(N)) {
+    constexpr int R = ct_radix(N, S);
+    stage_ct<R, DIR, N, NS, NB, T, LD>(buf, tw, tws);
+    cta_fft_ct<DIR, N, NB, T, LD, S + 1, NS * R>(buf, tw, tws);
+  }
+}
+#endif
+
 // Paired real-transform helpers working in place on one row held at
 // buf[spad(i)]: pair p (0 <= p <= M/2) owns elements p and M-p.
 // Forward post-processing: Z[0..M) -> X[0..M].
