@@ -200,7 +200,19 @@ int mc3_correct_bad_pixels(float* frames, int nx, int ny, int nz, const unsigned
                            void* stream) {
   if (!frames || !bad || nx < 2 || (nx & 1) || ny < 1 || nz < 1) return MC3_EINVAL;
   const long pad = 2 * (nx / 2 + 1);
-  return correct_bad_pixels(frames, pad * ny, nz, bad, nx, ny, as_stream(stream));
+  int* cnt = nullptr;
+  int2* list = nullptr;
+  if (cudaMalloc(&cnt, sizeof(int)) != cudaSuccess) return MC3_ENOMEM;
+  if (cudaMalloc(&list, sizeof(int2) * (size_t)nx * ny) != cudaSuccess) {
+    cudaFree(cnt);
+    return MC3_ENOMEM;
+  }
+  cudaStream_t st = as_stream(stream);
+  int s = correct_bad_pixels(frames, pad * ny, nz, bad, nx, ny, cnt, list, st);
+  if (s == kOk && cudaStreamSynchronize(st) != cudaSuccess) s = MC3_ECUDA;
+  cudaFree(cnt);
+  cudaFree(list);
+  return s;
 }
 
 int mc3_local_gather(const float* in, float* out, int nx, int ny, const float* centers,
@@ -208,7 +220,8 @@ int mc3_local_gather(const float* in, float* out, int nx, int ny, const float* c
   if (!in || !out || !centers || !shifts || n_patches < 1) return MC3_EINVAL;
   const long pad = 2 * (nx / 2 + 1);
   return local_gather(in, pad * ny, out, pad * ny, 1, nx, ny, centers,
-                      reinterpret_cast<const float2*>(shifts), bad, n_patches, as_stream(stream));
+                      reinterpret_cast<const float2*>(shifts), nullptr, bad, n_patches,
+                      as_stream(stream));
 }
 
 int mc3_phase_shift(const float* in, float* out, int cmp_x, int cmp_y, float sx, float sy,

@@ -109,43 +109,56 @@ int frame_sums(const float2* spec, long fr_stride, int N, int cmpX, int cmpY, co
 // (811*|v|) mod size.
 //
 // The distance weights do not depend on the frame, so each thread evaluates
-// them once for its pixel (held in registers, PMAX >= P) and then walks all
-// nb frames, accumulating in patch order exactly as the reference does per
-// frame; the result is bit-identical to evaluating them per frame.
-template <int PMAX>
+// them once for its pixel (held in registers, with a bit mask of the
+// patches within 0.6) and then walks all nb frames.  The patches used in a
+// frame are that mask minus the frame's bad-patch mask (one 64-bit mask per
+// frame); the accumulation runs in patch order exactly as the reference's,
+// as predicated adds rather than branches.
+// EXACT: P == PMAX; otherwise P < PMAX and reads are clamped to patch P-1.
+template <int PMAX, bool EXACT>
 __global__ void __launch_bounds__(128) k_local_gather(
     const float* __restrict__ in, long in_stride, float* out, long out_stride, int W, int H,
     const float* __restrict__ cent, const float2* __restrict__ sh,
-    const uint8_t* __restrict__ bad, int P, int nb) {
+    const unsigned long long* __restrict__ masks, const uint8_t* __restrict__ bad, int P, int nb) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y;
   if (x >= W) return;
   const float fB = 100.0f;
   float w[PMAX];
+  unsigned long long inc = 0ull;  // patches within r <= 0.6 of this pixel
 #pragma unroll
   for (int p = 0; p < PMAX; ++p) {
-    w[p] = -1.0f;  // -1: patch farther than r = 0.6 (never a valid weight)
-    if (p < P) {
+    w[p] = 0.0f;
+    if (EXACT || p < P) {
       float ax = ((float)(unsigned)x - cent[2 * p]) / (float)(unsigned)W;
       float ay = (y - cent[2 * p + 1]) / H;
       ax = sqrtf(ax * ax + ay * ay);
-      if (!(ax > 0.6f)) w[p] = expf(-fB * ax);
+      if (!(ax > 0.6f)) {
+        w[p] = expf(-fB * ax);
+        inc |= 1ull << p;
+      }
     }
   }
   const int padX = (W / 2 + 1) * 2;
   const long o = (long)y * padX + x;
   for (int f = 0; f < nb; ++f) {
     const float2* s = sh + (long)f * P;
-    const uint8_t* bd = bad ? bad + (long)f * P : nullptr;
+    unsigned long long m = 0ull;
+    if (masks) {
+      m = masks[f];
+    } else if (bad) {
+      for (int p = 0; p < P; ++p) m |= (unsigned long long)(bad[(long)f * P + p] != 0) << p;
+    }
+    const unsigned long long use = inc & ~m;
     float fSx = 0.0f, fSy = 0.0f, fW = 0.0f;
 #pragma unroll
     for (int p = 0; p < PMAX; ++p) {
-      if (p >= P) break;
-      if (bd != 0 && bd[p]) continue;
-      if (w[p] < 0.0f) continue;
-      fW += w[p];
-      fSx += s[p].x * w[p];
-      fSy += s[p].y * w[p];
+      const float2 sp = s[EXACT ? p : (p < P ? p : P - 1)];
+      if ((use >> p) & 1ull) {
+        fW += w[p];
+        fSx += sp.x * w[p];
+        fSy += sp.y * w[p];
+      }
     }
     if (fW > 0) {
       fSx = fSx / fW;
@@ -167,20 +180,56 @@ __global__ void __launch_bounds__(128) k_local_gather(
   }
 }
 
+template <int PMAX, bool EXACT>
+static void launch_gather(dim3 grid, cudaStream_t st, const float* in, long in_stride, float* out,
+                          long out_stride, int W, int H, const float* centers,
+                          const float2* shifts, const unsigned long long* masks,
+                          const uint8_t* bad, int P, int nb) {
+  k_local_gather<PMAX, EXACT><<<grid, 128, 0, st>>>(in, in_stride, out, out_stride, W, H, centers,
+                                                    shifts, masks, bad, P, nb);
+}
+
 int local_gather(const float* in, long in_stride, float* out, long out_stride, int nb, int W,
-                 int H, const float* centers, const float2* shifts, const uint8_t* bad, int P,
-                 cudaStream_t st) {
-  // `shifts`/`bad` point at the first frame of the batch.
+                 int H, const float* centers, const float2* shifts,
+                 const unsigned long long* masks, const uint8_t* bad, int P, cudaStream_t st) {
+  // `shifts`/`masks`/`bad` point at the first frame of the batch.
   if (P < 1 || P > 64) return kEUnsupported;
   dim3 grid(ceil_div(W, 128), H);
   prof::Scope ps("k_local_gather", (double)nb * W * H * 8.0, st);
-  if (P <= 16)
-    k_local_gather<16><<<grid, 128, 0, st>>>(in, in_stride, out, out_stride, W, H, centers, shifts, bad, P, nb);
-  else if (P <= 36)
-    k_local_gather<36><<<grid, 128, 0, st>>>(in, in_stride, out, out_stride, W, H, centers, shifts, bad, P, nb);
-  else
-    k_local_gather<64><<<grid, 128, 0, st>>>(in, in_stride, out, out_stride, W, H, centers, shifts, bad, P, nb);
+#define MC3_GATHER(PM, EX) \
+  launch_gather<PM, EX>(grid, st, in, in_stride, out, out_stride, W, H, centers, shifts, masks, bad, P, nb)
+  switch (P) {
+    case 4: MC3_GATHER(4, true); break;
+    case 9: MC3_GATHER(9, true); break;
+    case 16: MC3_GATHER(16, true); break;
+    case 25: MC3_GATHER(25, true); break;
+    case 35: MC3_GATHER(35, true); break;
+    case 36: MC3_GATHER(36, true); break;
+    case 49: MC3_GATHER(49, true); break;
+    case 64: MC3_GATHER(64, true); break;
+    default:
+      if (P <= 16) MC3_GATHER(16, false);
+      else if (P <= 36) MC3_GATHER(36, false);
+      else MC3_GATHER(64, false);
+  }
+#undef MC3_GATHER
   MC3_CHECK_LAUNCH("k_local_gather");
+  return kOk;
+}
+
+// Per-frame 64-bit masks of the bad-patch flags [nb][P] (bit p = patch p).
+__global__ void k_patch_masks(const uint8_t* bad, int P, int nb, unsigned long long* masks) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= nb) return;
+  unsigned long long m = 0ull;
+  for (int p = 0; p < P; ++p) m |= (unsigned long long)(bad[(long)f * P + p] != 0) << p;
+  masks[f] = m;
+}
+
+int patch_masks(const uint8_t* bad, int P, int nb, unsigned long long* masks, cudaStream_t st) {
+  if (P < 1 || P > 64) return kEUnsupported;
+  k_patch_masks<<<ceil_div(nb, 128), 128, 0, st>>>(bad, P, nb, masks);
+  MC3_CHECK_LAUNCH("k_patch_masks");
   return kOk;
 }
 

@@ -206,6 +206,10 @@ int Engine::plan(int w, int h, int n, mc3_plan_info* info) {
     MC3_TRY(d_bad.ensure((size_t)g.W * g.H));
   }
   MC3_TRY(d_xcf.ensure(sizeof(float2) * nxcf * g.N));
+  if (prm.correct_bad) {
+    MC3_TRY(d_badn.ensure(sizeof(int)));
+    MC3_TRY(d_badlist.ensure(sizeof(int2) * (size_t)g.W * g.H));
+  }
   MC3_TRY(d_sums.ensure(sizeof(float2) * ncmp * g.nSums));
   MC3_TRY(d_Wn.ensure(sizeof(float) * ncmp));
   if (g.patch) {
@@ -369,7 +373,10 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
     host::defect_template(6, tpl);
     MC3_TRY(detect_bad_pixels(d_sum.as<float>(), W, H, d_cc.as<float>(), d_part.as<float>(),
                               d_mom.as<float>(), d_bad.as<uint8_t>(), tpl, 6, st));
-    MC3_TRY(correct_bad_pixels(frames, fr_stride_f, N, d_bad.as<uint8_t>(), W, H, st));
+    MC3_TRY(d_badn.ensure(sizeof(int)));
+    MC3_TRY(d_badlist.ensure(sizeof(int2) * npx));
+    MC3_TRY(correct_bad_pixels(frames, fr_stride_f, N, d_bad.as<uint8_t>(), W, H, d_badn.as<int>(),
+                               d_badlist.as<int2>(), st));
   }
   // ---- 4. forward FFT, normalised, + xcf crop (CTransformStack, CGenXcfStack) ----
   MC3_TRY(d_xcf.ensure(sizeof(float2) * nxcf * N));
@@ -557,8 +564,11 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
       MC3_TRY(col_fft(spec, spec, g.cmpX, g.cmpX, H, bi, inv, st));
       Batch br{N, N, (long)ncmp, nullptr, (long)ncmp * 2};
       MC3_TRY(row_c2r(spec, g.cmpX, frames, g.padX, W, H, br, st));
+      MC3_TRY(d_pmask.ensure(sizeof(unsigned long long) * N));
+      MC3_TRY(patch_masks(d_pbad.as<uint8_t>(), P, N, d_pmask.as<unsigned long long>(), st));
       MC3_TRY(local_gather(frames, (long)ncmp * 2, d_gath.as<float>(), (long)ncmp * 2, N, W, H,
-                           d_pcent.as<float>(), d_pshift.as<float2>(), d_pbad.as<uint8_t>(), P, st));
+                           d_pcent.as<float>(), d_pshift.as<float2>(),
+                           d_pmask.as<unsigned long long>(), nullptr, P, st));
       Batch bf{N, N, (long)ncmp * 2, nullptr, (long)ncmp};
       MC3_TRY(row_r2c(d_gath.as<float>(), g.padX, spec, g.cmpX, W, H, bf, 1.0f, st));
       ColOps fwd{};

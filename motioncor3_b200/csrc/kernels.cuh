@@ -15,8 +15,9 @@ int image_moment(const float* img, int W, int H, long pitch, int iExp, float* d_
                  float* d_out, cudaStream_t st);
 int detect_bad_pixels(const float* sum, int W, int H, float* cc_buf, float* d_part,
                       float* d_mom, uint8_t* bad, const float* tpl, int ms, cudaStream_t st);
+// d_count: 1 int, d_list: W*H int2 of device scratch (bad-pixel list).
 int correct_bad_pixels(float* frames, long fr_stride, int N, const uint8_t* bad, int W, int H,
-                       cudaStream_t st);
+                       int* d_count, int2* d_list, cudaStream_t st);
 
 // ---- align.cu ----
 // Separable phase tables for shifts sh[item] = (sx, sy) in pixels of an
@@ -68,10 +69,12 @@ int dose_norm(const float* acc_dose, int N, int cmpX, int cmpY, float pix, float
 int frame_sums(const float2* spec, long fr_stride, int N, int cmpX, int cmpY, const float2* ex,
                const float2* ey, const float* acc_dose, const float* Wn, const DoseParams& dp,
                float2* sums, int n_sums, cudaStream_t st);
-// mGCorrect3D per frame of a batch.
+// mGCorrect3D per frame of a batch.  Bad patches come as per-frame 64-bit
+// masks (patch_masks) or, when masks is null, as [nb][P] flags.
 int local_gather(const float* in, long in_stride, float* out, long out_stride, int nb, int W,
-                 int H, const float* centers, const float2* shifts, const uint8_t* bad,
-                 int P, cudaStream_t st);
+                 int H, const float* centers, const float2* shifts,
+                 const unsigned long long* masks, const uint8_t* bad, int P, cudaStream_t st);
+int patch_masks(const uint8_t* bad, int P, int nb, unsigned long long* masks, cudaStream_t st);
 // out[y*W+x] = max(0, in[y*pitch+x])
 int unpad_positive(const float* in, long pitch, float* out, int W, int H, int n,
                    long in_stride, cudaStream_t st);

@@ -194,13 +194,14 @@ int detect_bad_pixels(const float* sum, int W, int H, float* cc_buf, float* d_pa
 }
 
 // ---- defect fill (BadPixel/GCorrectBad.cu:44-69, 96-150) ------------------
-__global__ void k_correct_bad(float* frames, long fr_stride, const uint8_t* bad, int W, int H,
-                              int padX, int win0) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y;
-  if (x >= W) return;
-  if (bad[(long)y * W + x] == 0) return;
-  float* fr = frames + (long)blockIdx.z * fr_stride;
+// The replacement pixel of a bad pixel depends only on its position and on
+// the bad-pixel map (the pseudo-random walk below), not on the frame, and
+// it is never itself bad.  So the fill is split into: list the bad pixels
+// (one pass over the map), pick each one's source once, then copy source
+// to destination in every frame.  Fills do not interact, so the list order
+// (atomics) does not matter.
+__device__ __forceinline__ int bad_source(const uint8_t* bad, int x, int y, int W, int H,
+                                          int padX, int win0) {
   const int i = y * padX + x;
   unsigned int next = i * 109 + 619;
   int win = win0;
@@ -215,8 +216,7 @@ __global__ void k_correct_bad(float* frames, long fr_stride, const uint8_t* bad,
       iX = iX % win - half + x;
       if (iX < 0 || iX >= W) continue;
       if (bad[(long)iY * W + iX] == 1) continue;
-      fr[i] = fr[(long)iY * padX + iX];
-      return;
+      return iY * padX + iX;
     }
     win += 50;
     next *= 997;
@@ -224,16 +224,47 @@ __global__ void k_correct_bad(float* frames, long fr_stride, const uint8_t* bad,
   int iX = next % (unsigned int)(W * H);
   int iY = iX / W;
   iX = iX % W;
-  fr[i] = fr[(long)iY * padX + iX];
+  return iY * padX + iX;
+}
+
+// list[k] = (destination, source) padded offsets of the k-th bad pixel.
+__global__ void k_bad_list(const uint8_t* __restrict__ bad, int W, int H, int padX, int win0,
+                           int* count, int2* list) {
+  const long npx = (long)W * H;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < npx;
+       i += (long)gridDim.x * blockDim.x) {
+    if (bad[i] == 0) continue;
+    const int y = (int)(i / W), x = (int)(i % W);
+    const int k = atomicAdd(count, 1);
+    list[k] = make_int2(y * padX + x, bad_source(bad, x, y, W, H, padX, win0));
+  }
+}
+
+__global__ void k_fill_bad(float* frames, long fr_stride, int N, const int* count,
+                           const int2* __restrict__ list) {
+  const int n = *count;
+  const long total = (long)n * N;
+  for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long)gridDim.x * blockDim.x) {
+    const int f = (int)(t / n);
+    const int2 e = list[t - (long)f * n];
+    float* fr = frames + (long)f * fr_stride;
+    fr[e.x] = fr[e.y];
+  }
 }
 
 int correct_bad_pixels(float* frames, long fr_stride, int N, const uint8_t* bad, int W, int H,
-                       cudaStream_t st) {
+                       int* d_count, int2* d_list, cudaStream_t st) {
   const int padX = 2 * (W / 2 + 1);
-  dim3 grid(ceil_div(W, 256), H, N);
-  prof::Scope ps("k_correct_bad", (double)W * H, st);
-  k_correct_bad<<<grid, 256, 0, st>>>(frames, fr_stride, bad, W, H, padX, 31);
-  MC3_CHECK_LAUNCH("k_correct_bad");
+  MC3_CUDA(cudaMemsetAsync(d_count, 0, sizeof(int), st));
+  {
+    prof::Scope ps("k_bad_list", (double)W * H, st);
+    k_bad_list<<<148 * 8, 256, 0, st>>>(bad, W, H, padX, 31, d_count, d_list);
+    MC3_CHECK_LAUNCH("k_bad_list");
+  }
+  prof::Scope ps("k_fill_bad", 0.0, st);
+  k_fill_bad<<<148 * 4, 256, 0, st>>>(frames, fr_stride, N, d_count, d_list);
+  MC3_CHECK_LAUNCH("k_fill_bad");
   return kOk;
 }
 
