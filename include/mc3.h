@@ -42,7 +42,7 @@ typedef struct {
   float tol;           /* -Tol (0.1 px)                                        */
   float bft[2];        /* -Bft global, patch (500, 100)                        */
   int phase_only;      /* -PhaseOnly (0)                                       */
-  float ft_bin;        /* -FtBin (1; only 1 is implemented)                    */
+  float ft_bin;        /* -FtBin (1): Fourier binning of the output sums       */
   float init_dose;     /* -InitDose (accepted, unused by the reference path)  */
   float fm_dose;       /* -FmDose e/A^2 per frame (0 = no dose weighting)      */
   float pix_size;      /* -PixSize A (0)                                       */
@@ -54,16 +54,18 @@ typedef struct {
   int correct_bad;     /* hot-pixel / defect detection + fill (1, as the
                           reference's CProcessThread.cpp:94-99 always runs)    */
   int gpu;             /* CUDA device ordinal (-Gpu first entry)               */
+  int split_sum;       /* -SplitSum (0): also sum odd and even frames           */
 } mc3_params;
 
 /* Sizes a movie will use (CBufferPool::CreateBuffers, CBufferPool.cpp:95-270). */
 typedef struct {
-  int n_sums;          /* 1 + DW + DWS                                        */
+  int n_sums;          /* 1 + DW + DWS + 2*SplitSum                           */
   int n_patches;       /* px*py in patch mode, else 0                         */
   int xcf_size[2];     /* alignment (Fourier-binned) image size               */
   int patch_size[2];   /* patch image size (0 in global mode)                 */
   float xcf_bin[2];    /* binning factors of the alignment image             */
   size_t device_bytes; /* device memory the context holds for this movie     */
+  int out_size[2];     /* size of each output sum (binned by -FtBin)          */
 } mc3_plan_info;
 
 typedef struct {
@@ -75,7 +77,8 @@ typedef struct {
 
 /* Caller-allocated outputs; any pointer may be NULL to skip it. */
 typedef struct {
-  float* sums;             /* [n_sums][ny][nx]: plain, DW, DWS               */
+  float* sums;             /* [n_sums][out_size[1]][out_size[0]]: plain, DW, DWS,
+                              ODD, EVN as enabled (out_size from mc3_plan) */
   int sums_on_device;      /* 1: `sums` is a device pointer                   */
   float* global_shifts;    /* [nz][2]: full-frame shifts as logged            */
   float* patch_shifts;     /* [nz][n_patches][2]                              */

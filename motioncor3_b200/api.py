@@ -50,6 +50,7 @@ class _Params(ctypes.Structure):
         ("align", ctypes.c_int),
         ("correct_bad", ctypes.c_int),
         ("gpu", ctypes.c_int),
+        ("split_sum", ctypes.c_int),
     ]
 
 
@@ -61,6 +62,7 @@ class _PlanInfo(ctypes.Structure):
         ("patch_size", ctypes.c_int * 2),
         ("xcf_bin", ctypes.c_float * 2),
         ("device_bytes", ctypes.c_size_t),
+        ("out_size", ctypes.c_int * 2),
     ]
 
 
@@ -188,6 +190,7 @@ class Params:
     align: int = 1
     correct_bad: int = 1
     gpu: int = 0
+    split_sum: int = 0
 
     def to_c(self) -> _Params:
         p = _Params()
@@ -210,6 +213,7 @@ class Params:
         p.align = int(self.align)
         p.correct_bad = int(self.correct_bad)
         p.gpu = int(self.gpu)
+        p.split_sum = int(self.split_sum)
         return p
 
 
@@ -266,7 +270,7 @@ class MotionCor3:
         _check(_lib().mc3_plan(self._h, nx, ny, nz, ctypes.byref(info)), "mc3_plan")
         return dict(n_sums=info.n_sums, n_patches=info.n_patches, xcf_size=tuple(info.xcf_size),
                     patch_size=tuple(info.patch_size), xcf_bin=tuple(info.xcf_bin),
-                    device_bytes=info.device_bytes)
+                    device_bytes=info.device_bytes, out_size=tuple(info.out_size))
 
     def set_gain(self, gain) -> None:
         if gain is None:
@@ -330,7 +334,8 @@ class MotionCor3:
             r.sums = sums.ctypes.data
             r.sums_on_device = 0
         else:
-            sums = np.zeros((ns, ny, nx), np.float32)
+            ox, oy = info["out_size"]
+            sums = np.zeros((ns, oy, ox), np.float32)
             r.sums = sums.ctypes.data
             r.sums_on_device = 0
         r.global_shifts = gsh.ctypes.data

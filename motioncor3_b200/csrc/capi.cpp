@@ -61,6 +61,7 @@ void mc3_params_default(mc3_params* p) {
   p->align = 1;
   p->correct_bad = 1;
   p->gpu = 0;
+  p->split_sum = 0;
 }
 
 int mc3_create(const mc3_params* p, mc3_ctx** out) {
@@ -370,6 +371,7 @@ int mc3_dose_weighted_sums(mc3_ctx* ctx, const float* spectra, int nx, int ny, i
   dp.kv_factor = host::kv_factor(e->prm.kv);
   dp.sum_range[0] = e->prm.sum_range[0];
   dp.sum_range[1] = e->prm.sum_range[1];
+  dp.split = e->prm.split_sum ? 1 : 0;
   if (g.dw && (s = dose_norm(e->d_acc.as<float>(), nz, g.cmpX, g.cmpY, dp.pix_size, dp.kv_factor,
                              e->d_Wn.as<float>(), st)))
     return s;

@@ -144,7 +144,8 @@ int main(int argc, char** argv) {
   if (argc <= 1 || (argc == 2 && strcasecmp(argv[1], "--help") == 0)) {
     std::printf("Usage: MotionCor3 -InMrc movie.mrc -OutMrc sum.mrc [-Gain gain.mrc] "
                 "[-Patch x y] [-Iter n] [-Tol px] [-Bft g p] [-FmDose d] [-PixSize a] "
-                "[-kV kv] [-Group g p] [-FmRef f] [-SumRange lo hi] [-PhaseOnly 0|1] "
+                "[-kV kv] [-Group g p] [-FmRef f] [-SumRange lo hi] [-PhaseOnly 0|1] [-SplitSum 0|1] "
+                "[-FtBin b] [-OutAln dir] "
                 "[-LogDir dir] [-Gpu id]\n");
     return eSuccess;
   }
@@ -160,6 +161,8 @@ int main(int argc, char** argv) {
   A.ints("-Patch", pt, 3);
   p.patch[0] = pt[0] <= 1 ? 0 : pt[0];
   p.patch[1] = pt[1] <= 1 ? 0 : pt[1];
+  p.patch[2] = pt[2] < 0 ? 0 : (pt[2] > 100 ? 100 : pt[2]);  // CInput.cpp:507-511
+  const std::string out_aln = A.str("-OutAln");
   A.ints("-Iter", &p.iter, 1);
   A.floats("-Tol", &p.tol, 1);
   A.floats("-Bft", p.bft, 2);
@@ -175,13 +178,14 @@ int main(int argc, char** argv) {
   if (p.group[0] < 1) p.group[0] = 1;
   if (p.group[1] < 1) p.group[1] = 1;
   A.ints("-FmRef", &p.fm_ref, 1);
+  A.ints("-SplitSum", &p.split_sum, 1);  // CInput.cpp:657-663
   int gpu[8];
   if (A.ints("-Gpu", gpu, 8) > 0) p.gpu = gpu[0];
   const char* ignored[] = {"-InTiff", "-InEer", "-InSuffix", "-InSkips", "-ArcDir", "-Dark",
-                           "-DefectFile", "-InAln", "-OutAln", "-DefectMap", "-FullSum", "-TmpFile",
+                           "-DefectFile", "-InAln", "-DefectMap", "-FullSum", "-TmpFile",
                            "-StackZ", "-Cs", "-AmpCont", "-ExtPhase", "-Throw", "-Trunc", "-Serial",
                            "-Tilt", "-Crop", "-OutStack", "-RotGain", "-FlipGain", "-InvGain", "-Mag",
-                           "-InFmMotion", "-GpuMemUsage", "-UseGpus", "-SplitSum", "-FmIntFile",
+                           "-InFmMotion", "-GpuMemUsage", "-UseGpus", "-FmIntFile",
                            "-EerSampling", "-OutStar", "-TiffOrder", "-CorrInterp"};
   for (const char* t : ignored) {
     int f, n;
@@ -229,7 +233,8 @@ int main(int argc, char** argv) {
     return eFailProcess;
   }
   const int N = h.nz, P = info.n_patches;
-  HostBuf sums_buf(sizeof(float) * (size_t)info.n_sums * h.nx * h.ny);
+  const int ox = info.out_size[0], oy = info.out_size[1];  // -FtBin output size
+  HostBuf sums_buf(sizeof(float) * (size_t)info.n_sums * ox * oy);
   float* sums = sums_buf.as<float>();
   std::vector<float> gsh(2 * (size_t)N), psh(2 * (size_t)N * (P > 0 ? P : 1)), pc(2 * (P > 0 ? P : 1));
   std::vector<unsigned char> pb((size_t)N * (P > 0 ? P : 1));
@@ -256,15 +261,21 @@ int main(int argc, char** argv) {
     std::printf("Iteration %2d  Error: %9.3f\n", i + 1, errs[i]);
   std::printf("Computation time: %f sec\n\n", std::chrono::duration<double>(t1 - t0).count());
   // ---- sums ----
-  const char* ext_dw[3] = {"", "_DW", "_DWS"};
+  // file name extensions in the order of CAlnSums::Setup (DataUtil/CAlnSums.cpp:18-43)
+  std::vector<const char*> exts = {"", "_DW", "_DWS"};
+  exts.resize(r.n_sums - (p.split_sum ? 2 : 0));
+  if (p.split_sum) {
+    exts.push_back("_ODD");
+    exts.push_back("_EVN");
+  }
   const float pix = p.pix_size * p.ft_bin;
   bool saved = true;
   for (int i = 0; i < r.n_sums; ++i) {
-    const float* img = sums + (size_t)i * h.nx * h.ny;
+    const float* img = sums + (size_t)i * ox * oy;
     float mn, mx, me;
-    stats(img, (size_t)h.nx * h.ny, &mn, &mx, &me);
-    const std::string name = out_name(out_mrc, ext_dw[i], ".mrc");
-    saved = mc3::mrc::write_float_image(name, img, h.nx, h.ny, pix, mn, mx, me) && saved;
+    stats(img, (size_t)ox * oy, &mn, &mx, &me);
+    const std::string name = out_name(out_mrc, exts[i], ".mrc");
+    saved = mc3::mrc::write_float_image(name, img, ox, oy, pix, mn, mx, me) && saved;
     std::printf("Corrected sum has been saved in:\n   %s\n\n", name.c_str());
   }
   // ---- logs ----
@@ -319,6 +330,49 @@ int main(int argc, char** argv) {
         }
         std::fclose(f);
       }
+    }
+  }
+  // ---- alignment file (-OutAln; Align/CSaveAlign.cpp:61-151, opened by
+  //      CMain::mOpenOutAlnFile, CMain.cpp:367-380) ----
+  if (!out_aln.empty()) {
+    std::string name = out_aln;
+    if (name.back() != '/') name += "/";
+    const size_t slash = in_mrc.rfind('/');
+    name += slash == std::string::npos ? in_mrc : in_mrc.substr(slash + 1);
+    const size_t dot = name.rfind('.');
+    if (dot == std::string::npos) name += ".aln";
+    else name = name.substr(0, dot) + ".aln";
+    FILE* f = std::fopen(name.c_str(), "wt");
+    if (!f) {
+      std::printf("Info: %s\n%s\n\n", "      cannot be opened. Alignment wiil not be saved.",
+                  name.c_str());
+    } else {
+      std::fprintf(f, "setting\n");
+      std::fprintf(f, "   stackSize: %d %d %d %d\n", h.nx, h.ny, N, 1);
+      std::fprintf(f, "   patches: %d %d %d\n", p.patch[0], p.patch[1], p.patch[2]);
+      std::fprintf(f, "   throw: %d %d\n", 0, 0);
+      std::fprintf(f, "#    Global Shift\n");
+      std::fprintf(f, "#---------------------\n");
+      std::fprintf(f, "globalShift\n");
+      std::fprintf(f, "   stackID %d\n", 0);
+      for (int i = 0; i < N; ++i)
+        std::fprintf(f, "%6d  %+8.3f  %+8.3f\n", i, gsh[2 * i], gsh[2 * i + 1]);
+      if (P > 0) {
+        std::fprintf(f, "#    Local Shift\n");
+        std::fprintf(f, "#---------------------\n");
+        std::fprintf(f, "localShift\n");
+        for (int i = 0; i < P; ++i) {
+          std::fprintf(f, "   patchID: %d\n", i);
+          std::fprintf(f, "   Converge: %d\n", 1);
+          for (int j = 0; j < N; ++j) {
+            const size_t k = (size_t)j * P + i;
+            std::fprintf(f, "%6d  %8.2f  %8.2f  %+8.3f  %+8.3f\n", j, pc[2 * i], pc[2 * i + 1],
+                         psh[2 * k], psh[2 * k + 1]);
+          }
+          if (i < P - 1) std::fprintf(f, "\n");
+        }
+      }
+      std::fclose(f);
     }
   }
   mc3_destroy(ctx);

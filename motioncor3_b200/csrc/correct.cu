@@ -53,9 +53,11 @@ int dose_norm(const float* acc_dose, int N, int cmpX, int cmpY, float pix, float
   return kOk;
 }
 
-// All sums in one pass over the frames (CCorrectFullShift::mGenSums):
-// sum0 += X; X *= w_f/Wn (DC untouched); sum1 += X; sum2 += X when the
-// frame's accumulated dose lies in the selected range.
+// All sums in one pass over the frames (CCorrectFullShift::mGenSums,
+// Correct/CCorrectFullShift.cpp:271-300): sum0 += X; X *= w_f/Wn (DC
+// untouched); sum1 += X; sum2 += X when the frame's accumulated dose lies in
+// the selected range; with -SplitSum the (weighted) X also goes to the
+// "_ODD" sum for even frame indices and to "_EVN" for odd ones.
 __global__ void k_frame_sums(const float2* __restrict__ spec, long fr_stride, int N, int cmpX,
                              int cmpY, const float2* __restrict__ ex, const float2* __restrict__ ey,
                              const float* acc, const float* Wn, DoseParams dp, float2* sums,
@@ -65,6 +67,7 @@ __global__ void k_frame_sums(const float2* __restrict__ spec, long fr_stride, in
   if (k >= n) return;
   const int x = (int)(k % cmpX), y = (int)(k / cmpX);
   float2 s0 = c2(0.f, 0.f), s1 = c2(0.f, 0.f), s2 = c2(0.f, 0.f);
+  float2 so = c2(0.f, 0.f), se = c2(0.f, 0.f);
   const float wn = dp.enabled && k > 0 ? Wn[k] : 1.0f;
   const float cd = dp.enabled && k > 0 ? crit_dose(x, y, cmpX, cmpY, dp.kv_factor, dp.pix_size) : 1.0f;
 #pragma unroll 4
@@ -85,16 +88,32 @@ __global__ void k_frame_sums(const float2* __restrict__ spec, long fr_stride, in
       s1 = cadd(X, s1);
       if (dp.dws && acc[f] >= dp.sum_range[0] && acc[f] <= dp.sum_range[1]) s2 = cadd(X, s2);
     }
+    if (dp.split) {
+      if (f % 2 == 0) so = cadd(X, so);
+      else se = cadd(X, se);
+    }
   }
   sums[k] = s0;
-  if (n_sums > 1) sums[n + k] = s1;
-  if (n_sums > 2) sums[2 * n + k] = s2;
+  int next = 1;
+  if (dp.enabled) {
+    sums[n + k] = s1;
+    next = 2;
+    if (dp.dws) {
+      sums[2 * n + k] = s2;
+      next = 3;
+    }
+  }
+  if (dp.split) {
+    sums[(long)next * n + k] = so;
+    sums[(long)(next + 1) * n + k] = se;
+  }
 }
 
 int frame_sums(const float2* spec, long fr_stride, int N, int cmpX, int cmpY, const float2* ex,
                const float2* ey, const float* acc_dose, const float* Wn, const DoseParams& dp,
                float2* sums, int n_sums, cudaStream_t st) {
   const long n = (long)cmpX * cmpY;
+  if (n_sums != 1 + (dp.enabled ? 1 + (dp.dws ? 1 : 0) : 0) + (dp.split ? 2 : 0)) return kEInval;
   prof::Scope ps("k_frame_sums", (double)n * (8.0 * (N + n_sums) + (dp.enabled ? 4.0 : 0.0)), st);
   k_frame_sums<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(spec, fr_stride, N, cmpX, cmpY, ex, ey,
                                                            acc_dose, Wn, dp, sums, n_sums);

@@ -80,7 +80,15 @@ int Geometry::compute(int w, int h, int n, const mc3_params& p) {
   dw = !(p.kv < 80 || p.kv > 300) && p.pix_size > 0 && p.fm_dose > 0;
   dws = dw && p.sum_range[0] >= 0 && p.sum_range[1] > 0 &&
         (p.sum_range[1] - p.sum_range[0]) > 1.0f;
-  nSums = 1 + (dw ? 1 : 0) + (dws ? 1 : 0);
+  nSums = 1 + (dw ? 1 : 0) + (dws ? 1 : 0) + (p.split_sum ? 2 : 0);
+  // CInput::GetBinnedSize (CInput.cpp:678-688): output sums binned by -FtBin
+  outW = W;
+  outH = H;
+  if (p.ft_bin > 0) {
+    outW = (int)(W / p.ft_bin + 0.5f) / 2 * 2;
+    outH = (int)(H / p.ft_bin + 0.5f) / 2 * 2;
+  }
+  if (outW < 2 || outH < 2 || outW > W || outH > H) return kEUnsupported;
   return kOk;
 }
 
@@ -188,6 +196,8 @@ int Engine::plan(int w, int h, int n, mc3_plan_info* info) {
   info->patch_size[1] = g.patch ? g.patCmpY : 0;
   info->xcf_bin[0] = g.xcfBin[0];
   info->xcf_bin[1] = g.xcfBin[1];
+  info->out_size[0] = g.outW;
+  info->out_size[1] = g.outH;
   size_t cmp = (size_t)g.cmpX * g.cmpY * sizeof(float2);
   size_t xcf = (size_t)g.xcfCmpX * g.xcfCmpY * sizeof(float2);
   size_t bytes = cmp * g.N + xcf * g.N + cmp * (g.nSums + 2) + (size_t)g.W * g.H * 4 * g.N;
@@ -316,7 +326,6 @@ int Engine::global_sums(const float2* spec, int N, const host::StackShift& fs, c
 int Engine::process(const mc3_movie& mv, mc3_result* out) {
   MC3_CUDA(cudaSetDevice(device));
   if (prm.align == 0) return kEUnsupported;
-  if (prm.ft_bin != 1.0f) return kEUnsupported;
   if (!mv.frames) return kEInval;
   int bpp = 0;
   switch (mv.mode) {
@@ -531,6 +540,7 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
   DoseParams dp{};
   dp.enabled = g.dw ? 1 : 0;
   dp.dws = g.dws ? 1 : 0;
+  dp.split = prm.split_sum ? 1 : 0;
   dp.pix_size = prm.pix_size;
   dp.kv_factor = host::kv_factor(prm.kv);
   dp.sum_range[0] = prm.sum_range[0];
@@ -579,25 +589,40 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
     MC3_TRY(frame_sums(spec, (long)ncmp, N, g.cmpX, g.cmpY, nullptr, nullptr, d_acc.as<float>(),
                        d_Wn.as<float>(), dp, d_sums.as<float2>(), g.nSums, st));
   }
-  // ---- 8. sums to real space (CCorrectFullShift::mUnpadSums) ----
+  // ---- 8. sums to real space (CCorrectFullShift::mUnpadSums,
+  //      Correct/CCorrectFullShift.cpp:146-185): Fourier crop to the -FtBin
+  //      output size, C2R, positivity, unpad ----
   {
-    Batch bs{g.nSums, g.nSums, (long)ncmp, nullptr, (long)ncmp};
+    const int oW = g.outW, oH = g.outH;
+    const int ocX = oW / 2 + 1;
+    const size_t ocmp = (size_t)ocX * oH;
+    float2* osum = d_sums.as<float2>();
+    if (oW != W || oH != H) {
+      MC3_TRY(d_bsums.ensure(sizeof(float2) * ocmp * g.nSums));
+      osum = d_bsums.as<float2>();
+      for (int sidx = 0; sidx < g.nSums; ++sidx)
+        MC3_TRY(fourier_crop(d_sums.as<float2>() + ncmp * sidx, g.cmpX, g.cmpY, osum + ocmp * sidx,
+                             ocX, oH, st));
+    }
+    Batch bs{g.nSums, g.nSums, (long)ocmp, nullptr, (long)ocmp};
     ColOps inv{};
     inv.dir = 1;
     inv.scale = 1.0f;
-    MC3_TRY(col_fft(d_sums.as<float2>(), d_sums.as<float2>(), g.cmpX, g.cmpX, H, bs, inv, st));
-    Batch br{g.nSums, g.nSums, (long)ncmp, nullptr, (long)ncmp * 2};
-    MC3_TRY(row_c2r(d_sums.as<float2>(), g.cmpX, d_sums.as<float>(), g.padX, W, H, br, st));
+    MC3_TRY(col_fft(osum, osum, ocX, ocX, oH, bs, inv, st));
+    Batch br{g.nSums, g.nSums, (long)ocmp, nullptr, (long)ocmp * 2};
+    MC3_TRY(row_c2r(osum, ocX, reinterpret_cast<float*>(osum), 2 * ocX, oW, oH, br, st));
+    const size_t opx = (size_t)oW * oH;
     float* dst = nullptr;
     if (out && out->sums && out->sums_on_device) {
       dst = out->sums;
     } else {
-      MC3_TRY(d_out.ensure(sizeof(float) * npx * g.nSums));
+      MC3_TRY(d_out.ensure(sizeof(float) * opx * g.nSums));
       dst = d_out.as<float>();
     }
-    MC3_TRY(unpad_positive(d_sums.as<float>(), g.padX, dst, W, H, g.nSums, (long)ncmp * 2, st));
+    MC3_TRY(unpad_positive(reinterpret_cast<float*>(osum), 2 * ocX, dst, oW, oH, g.nSums,
+                           (long)ocmp * 2, st));
     if (out && out->sums && !out->sums_on_device)
-      MC3_CUDA(cudaMemcpyAsync(out->sums, dst, sizeof(float) * npx * g.nSums, cudaMemcpyDeviceToHost, st));
+      MC3_CUDA(cudaMemcpyAsync(out->sums, dst, sizeof(float) * opx * g.nSums, cudaMemcpyDeviceToHost, st));
   }
   MC3_CUDA(cudaEventRecord(ev1, st));
   MC3_CUDA(cudaStreamSynchronize(st));

@@ -36,6 +36,7 @@ struct Geometry {
   int patSizeX = 0, patSizeY = 0;
   bool dw = false, dws = false;
   int nSums = 1;
+  int outW = 0, outH = 0;  // output sum size after -FtBin
   int compute(int w, int h, int n, const mc3_params& p);
 };
 
@@ -85,7 +86,7 @@ class Engine {
   DevBuf d_gain, d_raw, d_frames, d_sum, d_cc, d_bad, d_part, d_mom, d_badn, d_badlist;
   DevBuf d_xcf, d_sh, d_ex, d_ey, d_S, d_T, d_win, d_gsh, d_act, d_gstart, d_gsize;
   DevBuf d_pat, d_patoff, d_bsum, d_bimg, d_btmp, d_bmap, d_scal;
-  DevBuf d_fex, d_fey, d_Wn, d_acc, d_sums, d_real, d_gath, d_pcent, d_pshift, d_pbad, d_pmask, d_out;
+  DevBuf d_fex, d_fey, d_Wn, d_acc, d_sums, d_real, d_gath, d_pcent, d_pshift, d_pbad, d_pmask, d_out, d_bsums;
   bool has_gain = false;
   int gain_w = 0, gain_h = 0;
 };

@@ -61,6 +61,7 @@ struct DoseParams {
   float pix_size;
   float kv_factor;
   float sum_range[2];
+  int split;  // odd/even sums of the (weighted) frames after the others
 };
 // Wn[k] = sqrt(sum_f w_f(k)^2) (GWeightFrame::BuildWeight)
 int dose_norm(const float* acc_dose, int N, int cmpX, int cmpY, float pix, float kvf, float* Wn,

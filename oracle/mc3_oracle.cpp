@@ -1043,6 +1043,8 @@ void oracle_default_params(oracle_params* p) {
   p->sum_range[0] = 3.0f;
   p->sum_range[1] = 25.0f;
   p->correct_bad = 1;
+  p->split_sum = 0;
+  p->ft_bin = 1.0f;
 }
 
 void oracle_rfft2(const double* img, double* spec, int W, int H, int normalise) {
@@ -1268,7 +1270,8 @@ int oracle_process_movie(const oracle_params* p, const float* frames, int W, int
   const bool dw = !(p->kv < 80 || p->kv > 300) && p->pix_size > 0 && p->fm_dose > 0;
   const bool dws = dw && p->sum_range[0] >= 0 && p->sum_range[1] > 0 &&
                    (p->sum_range[1] - p->sum_range[0]) > 1.0f;
-  const int nSums = 1 + (dw ? 1 : 0) + (dws ? 1 : 0);
+  const int nBase = 1 + (dw ? 1 : 0) + (dws ? 1 : 0);
+  const int nSums = nBase + (p->split_sum ? 2 : 0);
   std::vector<float> acc(N);
   for (int i = 0; i < N; ++i) acc[i] = p->fm_dose * (i + 1);
   std::vector<double> wsum;
@@ -1303,6 +1306,9 @@ int oracle_process_movie(const oracle_params* p, const float* frames, int W, int
     }
     cd* s0 = &sums[0];
     for (long i = 0; i < ncmp; ++i) s0[i] += X[i];
+    // CCorrectFullShift::mGenSums (Correct/CCorrectFullShift.cpp:271-300):
+    // the odd/even split sums take the frame after dose weighting
+    cd* split = p->split_sum ? &sums[(long)(nBase + (f % 2)) * ncmp] : nullptr;
     if (dw) {
       const bool inRange = acc[f] >= p->sum_range[0] && acc[f] <= p->sum_range[1];
       for (int y = 0; y < g.cmpY; ++y)
@@ -1312,14 +1318,32 @@ int oracle_process_movie(const oracle_params* p, const float* frames, int W, int
           if (i > 0) v *= dose_weight(x, y, g.cmpX, g.cmpY, acc[f], p->pix_size, kvf) / wsum[i];
           sums[ncmp + i] += v;
           if (dws && inRange) sums[2 * ncmp + i] += v;
+          if (split) split[i] += v;
         }
+    } else if (split) {
+      for (long i = 0; i < ncmp; ++i) split[i] += X[i];
     }
   }
-  // mUnpadSums (CCorrectFullShift.cpp:146-185): C2R, positivity
-  std::vector<double> img(npx);
+  // mUnpadSums (CCorrectFullShift.cpp:146-185): Fourier crop to the -FtBin
+  // size (CInput::GetBinnedSize, CInput.cpp:678-688; GFourierResize2D copy
+  // mode, Util/GFourierResize2D.cu:7-37), C2R, positivity
+  int oW = W, oH = H;
+  if (p->ft_bin > 0) {
+    oW = (int)(W / p->ft_bin + 0.5f) / 2 * 2;
+    oH = (int)(H / p->ft_bin + 0.5f) / 2 * 2;
+  }
+  const int ocX = oW / 2 + 1;
+  const long opx = (long)oW * oH;
+  std::vector<double> img(opx);
+  std::vector<cd> crop((long)ocX * oH);
   for (int s = 0; s < nSums; ++s) {
-    irfft2(&sums[(long)s * ncmp], img.data(), W, H);
-    for (long i = 0; i < npx; ++i) out->sums[(long)s * npx + i] = (float)std::max(0.0, img[i]);
+    const cd* S = &sums[(long)s * ncmp];
+    for (int yo = 0; yo < oH; ++yo) {
+      const int yi = yo > oH / 2 ? yo - oH + H : yo;
+      for (int x = 0; x < ocX; ++x) crop[(long)yo * ocX + x] = S[(long)yi * g.cmpX + x];
+    }
+    irfft2(crop.data(), img.data(), oW, oH);
+    for (long i = 0; i < opx; ++i) out->sums[(long)s * opx + i] = (float)std::max(0.0, img[i]);
   }
   out->n_sums = nSums;
   // logged full-frame shifts: absolute (global mode) or relative (patch mode)

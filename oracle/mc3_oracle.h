@@ -37,11 +37,13 @@ typedef struct {
   int fm_ref;         /* -FmRef (<0: central frame)                       */
   float sum_range[2]; /* -SumRange (e/A^2)                                */
   int correct_bad;    /* run hot-pixel/defect detection and correction     */
+  int split_sum;      /* -SplitSum: odd and even frame sums after the others */
+  float ft_bin;       /* -FtBin: Fourier binning of the output sums        */
 } oracle_params;
 
 typedef struct {
-  int n_sums;             /* 1 (plain), 2 (+DW) or 3 (+DW +DWS)           */
-  float* sums;            /* [n_sums][H][W] caller-allocated              */
+  int n_sums;             /* 1 (plain), +1 DW, +1 DWS, +2 odd/even         */
+  float* sums;            /* [n_sums][Hb][Wb] caller-allocated (-FtBin size) */
   float* global_shifts;   /* [N][2] final full-frame shifts (log values)  */
   int n_patches;          /* P (0 in global mode)                         */
   float* patch_shifts;    /* [N][P][2] relative local shifts              */

@@ -57,6 +57,8 @@ class OracleParams(ctypes.Structure):
         ("fm_ref", ctypes.c_int),
         ("sum_range", ctypes.c_float * 2),
         ("correct_bad", ctypes.c_int),
+        ("split_sum", ctypes.c_int),
+        ("ft_bin", ctypes.c_float),
     ]
 
 
@@ -113,7 +115,11 @@ def process_movie(frames: np.ndarray, gain=None, force=None, **kw) -> dict:
     fr = np.ascontiguousarray(frames, np.float32)
     g = None if gain is None else np.ascontiguousarray(gain, np.float32)
     P = (p.patch[0] * p.patch[1]) if (p.patch[0] > 1 and p.patch[1] > 1) else 0
-    sums = np.zeros((3, ny, nx), np.float32)
+    ob, oh = nx, ny
+    if p.ft_bin > 0:  # CInput::GetBinnedSize (CInput.cpp:678-688)
+        ob = int(np.float32(nx) / np.float32(p.ft_bin) + np.float32(0.5)) // 2 * 2
+        oh = int(np.float32(ny) / np.float32(p.ft_bin) + np.float32(0.5)) // 2 * 2
+    sums = np.zeros((5, oh, ob), np.float32)
     gsh = np.zeros((nz, 2), np.float32)
     psh = np.zeros((nz, max(P, 1), 2), np.float32)
     pc = np.zeros((max(P, 1), 2), np.float32)

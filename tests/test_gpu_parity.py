@@ -162,7 +162,8 @@ def _compare_movie(api, oracle, movie, params, forced_sum_tol=1e-4):
     """Runs the GPU path and the oracle on the same raw frames: shifts within
     0.05 px and sums (oracle corrected with the GPU's shifts) within 1e-4."""
     kw = dict(patch=params.patch[:2], iter=params.iter, tol=params.tol, bft=params.bft,
-              fm_dose=params.fm_dose, pix_size=params.pix_size, kv=params.kv, group=params.group)
+              fm_dose=params.fm_dose, pix_size=params.pix_size, kv=params.kv, group=params.group,
+              split_sum=params.split_sum, ft_bin=params.ft_bin)
     with api.MotionCor3(params) as mc:
         if movie.gain is not None:
             mc.set_gain(np.asarray(movie.gain))
@@ -200,6 +201,30 @@ def test_pipeline_global_dose_weighted_gain(api, oracle, torch_cuda):
     p = api.Params(iter=6, tol=0.2, bft=(300, 100), fm_dose=1.2, pix_size=0.9, kv=300)
     res, _ = _compare_movie(api, oracle, m, p)
     assert res.n_sums == 3
+
+
+@pytest.mark.parametrize("dose", [0.0, 1.2])
+def test_pipeline_split_sums(api, oracle, torch_cuda, dose):
+    """-SplitSum 1: odd/even frame sums after the plain (and DW, DWS) sums."""
+    from motioncor3_b200 import synthetic as S
+    m = S.make_movie(320, 256, 11, dose=3.0, seed=36, gain=False)
+    p = api.Params(iter=6, tol=0.2, bft=(300, 100), fm_dose=dose, pix_size=0.9, kv=300,
+                   split_sum=1)
+    res, _ = _compare_movie(api, oracle, m, p)
+    assert res.n_sums == (5 if dose > 0 else 3)
+
+
+@pytest.mark.parametrize("ft_bin", [2.0, 1.5])
+def test_pipeline_fourier_binned_sums(api, oracle, torch_cuda, ft_bin):
+    """-FtBin: sums Fourier-cropped to the binned size before the inverse."""
+    from motioncor3_b200 import synthetic as S
+    m = S.make_movie(384, 320, 10, dose=3.0, seed=37, gain=False)
+    p = api.Params(iter=6, tol=0.2, bft=(300, 100), fm_dose=1.2, pix_size=0.9, kv=300,
+                   ft_bin=ft_bin)
+    res, _ = _compare_movie(api, oracle, m, p)
+    ob = int(np.float32(384) / np.float32(ft_bin) + np.float32(0.5)) // 2 * 2
+    oh = int(np.float32(320) / np.float32(ft_bin) + np.float32(0.5)) // 2 * 2
+    assert res.sums.shape == (3, oh, ob)
 
 
 def test_pipeline_patch_small(api, oracle, torch_cuda):

@@ -42,7 +42,7 @@ def run_program(binary, workdir, movie, gain, tags):
     mv = os.path.join(workdir, "movie.mrc")
     mrcio.write(mv, movie)
     args = [binary, "-InMrc", mv, "-OutMrc", os.path.join(workdir, "sum.mrc"), "-LogDir",
-            workdir + "/", "-Gpu", "0", "-Cs", "0"] + tags
+            workdir + "/", "-OutAln", workdir, "-Gpu", "0", "-Cs", "0"] + tags
     if gain is not None:
         gp = os.path.join(workdir, "gain.mrc")
         mrcio.write(gp, gain.astype(np.float32))
@@ -53,7 +53,7 @@ def run_program(binary, workdir, movie, gain, tags):
     m = re.search(r"Computation time:\s*([0-9.]+)", out)
     secs = float(m.group(1)) if m else None
     sums = {}
-    for suf in ("", "_DW", "_DWS"):
+    for suf in ("", "_DW", "_DWS", "_ODD", "_EVN"):
         f = os.path.join(workdir, f"sum{suf}.mrc")
         if os.path.exists(f):
             sums[suf] = mrcio.read(f)[0].astype(np.float64)
@@ -62,7 +62,17 @@ def run_program(binary, workdir, movie, gain, tags):
         f = os.path.join(workdir, "movie" + suf)
         if os.path.exists(f):
             logs[suf] = f
-    return dict(sums=sums, logs=logs, secs=secs, stdout=out)
+    aln = os.path.join(workdir, "movie.aln")
+    return dict(sums=sums, logs=logs, secs=secs, stdout=out,
+                aln=open(aln).read() if os.path.exists(aln) else None)
+
+
+def _aln_parts(text):
+    """(non-numeric skeleton, numbers) of an -OutAln file."""
+    toks = text.split()
+    nums = [float(t) for t in toks if re.fullmatch(r"[+-]?\d+(\.\d+)?", t)]
+    skel = [t for t in toks if not re.fullmatch(r"[+-]?\d+(\.\d+)?", t)]
+    return skel, np.array(nums)
 
 
 CASES = {
@@ -70,6 +80,10 @@ CASES = {
                        tags="-Patch 0 0 -Iter 7 -Tol 0.5 -Bft 150 -PixSize 1"),
     "global_dw_gain": dict(shape=(12, 320, 384), dose=3.0, seed=32, gain=True, local=False,
                            tags="-Iter 6 -Tol 0.2 -Bft 300 -FmDose 1.2 -PixSize 0.9 -kV 300"),
+    "global_split_dw": dict(shape=(11, 320, 256), dose=3.0, seed=36, gain=False, local=False,
+                            tags="-Iter 6 -Tol 0.2 -Bft 300 -FmDose 1.2 -PixSize 0.9 -SplitSum 1"),
+    "global_ftbin2": dict(shape=(10, 384, 320), dose=3.0, seed=37, gain=False, local=False,
+                          tags="-Iter 6 -Tol 0.2 -Bft 300 -FmDose 1.2 -PixSize 0.9 -FtBin 2"),
     "patch_3x3": dict(shape=(12, 512, 512), dose=4.0, seed=33, gain=True, local=True,
                       tags="-Patch 3 3 -Iter 5 -Tol 0.2 -Bft 500 150 -FmDose 1 -PixSize 1 -kV 300"),
     "config1_1024x40": dict(shape=(40, 1024, 1024), dose=1.0, seed=101, gain=False, local=False,
@@ -98,6 +112,11 @@ def test_cli_matches_reference_program(name, tmp_path, mc3lib):
         d = np.abs(a - b).max()
         assert d <= 0.05 + 1e-6, (key, d)
         same_shifts &= d == 0
+    # alignment files (-OutAln): same layout, values within the shift tolerance
+    assert ref["aln"] is not None and ours["aln"] is not None
+    (sr, nr), (so, no) = _aln_parts(ref["aln"]), _aln_parts(ours["aln"])
+    assert sr == so
+    assert nr.shape == no.shape and np.abs(nr - no).max() <= 0.05 + 1e-6
     # Patch mode: the local correction gathers the nearest pixel of
     # (x - s(x, y)) with s interpolated from UNtruncated patch shifts
     # (Align/CMeasurePatches.cpp:79-81 keeps full float precision), so a

@@ -112,3 +112,41 @@ def test_patch_sum_sensitivity_to_shift_rounding(oracle):
         rels[eps] = np.sqrt(np.mean((a - b) ** 2) / np.mean(a ** 2))
     assert rels[1e-7] < 1e-5
     assert rels[1e-5] > 1e-4
+
+
+def test_oracle_split_sums_partition_the_weighted_sum(oracle):
+    """-SplitSum: the _ODD (even frame indices) and _EVN sums of the dose-
+    weighted frames add up to the _DW sum (before positivity clamping, which
+    a positive movie does not reach), as CCorrectFullShift::mGenSums builds
+    them (Correct/CCorrectFullShift.cpp:271-300)."""
+    from motioncor3_b200 import synthetic as S
+    m = S.make_movie(128, 96, 7, dose=20.0, seed=8)
+    kw = dict(iter=4, tol=0.2, bft=(300, 100), fm_dose=1.2, pix_size=0.9, kv=300)
+    r = oracle.process_movie(m.frames, split_sum=1, **kw)
+    assert r["n_sums"] == 5
+    plain = oracle.process_movie(m.frames, **kw)
+    assert plain["n_sums"] == 3
+    for i in range(3):
+        assert np.array_equal(r["sums"][i], plain["sums"][i])
+    dw, odd, evn = (r["sums"][i].astype(np.float64) for i in (1, 3, 4))
+    assert np.abs(odd + evn - dw).max() <= 1e-4 * np.abs(dw).max()
+    assert np.abs(odd - evn).max() > 1e-3 * np.abs(dw).max()
+
+
+def test_oracle_fourier_binned_sums(oracle):
+    """-FtBin 2: the output sum is the Fourier crop of the full-size sum to
+    the binned size (CInput::GetBinnedSize rounding), inverted unnormalised,
+    i.e. the band-limited half-size image with the same mean."""
+    from motioncor3_b200 import synthetic as S
+    m = S.make_movie(200, 150, 6, dose=20.0, seed=9)
+    kw = dict(iter=4, tol=0.2, bft=(300, 100), pix_size=1.0)
+    full = oracle.process_movie(m.frames, **kw)["sums"][0].astype(np.float64)
+    binned = oracle.process_movie(m.frames, ft_bin=2.0, **kw)["sums"][0].astype(np.float64)
+    oh, ow = 74, 100                   # (int)(150/2 + 0.5) = 75, made even
+    assert binned.shape == (oh, ow)
+    F = np.fft.rfft2(full) / full.size
+    rows = [yo if yo <= oh // 2 else yo - oh + 150 for yo in range(oh)]
+    crop = F[rows, : ow // 2 + 1]
+    ref = np.fft.irfft2(crop, s=(oh, ow)) * (oh * ow)
+    assert np.abs(binned - np.maximum(ref, 0)).max() <= 1e-3 * np.abs(ref).max()
+    assert abs(binned.mean() - full.mean()) <= 1e-3 * full.mean()
