@@ -122,7 +122,7 @@ int aligned_sum(const float2* spec, const int* act, const float2* ex, const floa
 // then the inverse FFT along ky; only the seaY rows that the 64x64 search
 // window reads are written.
 // ---------------------------------------------------------------------
-__global__ void k_corr_cols(const float2* __restrict__ spec, const int* act,
+__global__ void __launch_bounds__(256, 2) k_corr_cols(const float2* __restrict__ spec, const int* act,
                             const float2* __restrict__ ex, const float2* __restrict__ ey,
                             const float2* __restrict__ S, const int* gstart, const int* gsize,
                             float bf, int phase_only, float2* T, int cmpX, int H, int N,
@@ -363,7 +363,7 @@ int corr_cols(const float2* spec, const int* act, const float2* ex, const float2
 // Row pass of the correlation: real inverse of each kept row, keeping the
 // seaX central columns (the window GCorrelateSum2D.cu:130-139 copies).
 // ---------------------------------------------------------------------
-__global__ void k_corr_rows(const float2* __restrict__ T, float* win, int cmpX, int seaX, int seaY,
+__global__ void __launch_bounds__(256, 2) k_corr_rows(const float2* __restrict__ T, float* win, int cmpX, int seaX, int seaY,
                             int G, int rows, FftDesc dM) {
   extern __shared__ float2 sm[];
   const int M = cmpX - 1;

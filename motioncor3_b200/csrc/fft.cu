@@ -78,7 +78,7 @@ __device__ __forceinline__ long batch_in_off(const Batch& b, int item) {
 // ---------------------------------------------------------------------
 // Row real FFT (R2C): each CTA transforms `rows` rows of one batch item.
 // ---------------------------------------------------------------------
-__global__ void k_row_r2c(const float* __restrict__ in, long in_pitch, float2* out, long out_pitch,
+__global__ void __launch_bounds__(256, 2) k_row_r2c(const float* __restrict__ in, long in_pitch, float2* out, long out_pitch,
                           int W, int H, int rows, Batch bt, FftDesc dM, float scale) {
   extern __shared__ float2 sm[];
   const int M = W / 2;
@@ -114,7 +114,7 @@ __global__ void k_row_r2c(const float* __restrict__ in, long in_pitch, float2* o
 // ---------------------------------------------------------------------
 // Row real inverse (C2R), unnormalised.
 // ---------------------------------------------------------------------
-__global__ void k_row_c2r(const float2* in, long in_pitch, float* out, long out_pitch, int W,
+__global__ void __launch_bounds__(256, 2) k_row_c2r(const float2* in, long in_pitch, float* out, long out_pitch, int W,
                           int H, int rows, Batch bt, FftDesc dM) {
   extern __shared__ float2 sm[];
   const int M = W / 2;
@@ -155,7 +155,7 @@ __global__ void k_row_c2r(const float2* in, long in_pitch, float* out, long out_
 // ---------------------------------------------------------------------
 // Column complex FFT with optional phase-shift prologue and crop epilogue.
 // ---------------------------------------------------------------------
-__global__ void k_col_fft(const float2* in, float2* out, long pitch, int cmpX, int H, int TX,
+__global__ void __launch_bounds__(256, 2) k_col_fft(const float2* in, float2* out, long pitch, int cmpX, int H, int TX,
                           Batch bt, FftDesc dH, ColOps ops) {
   extern __shared__ float2 sm[];
   const int ld = H + 1;

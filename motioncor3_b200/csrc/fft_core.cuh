@@ -12,7 +12,8 @@
 // earlier radices, butterfly j (0 <= j < n/R) reads x[j + r*n/R],
 // multiplies input r by w_n^(r*(j%Ns)*n/(Ns*R)), applies a length-R DFT
 // and writes y[(j/Ns)*Ns*R + j%Ns + r*Ns].  Radices 2, 3, 4 and 8 have
-// dedicated butterflies; any other factor (5, 7, 11, 17, 41, ...) uses a
+// dedicated butterflies, odd primes 5..31 a register butterfly built on
+// input pairs (dft_prime); any other factor (41, 131, ...) uses a
 // per-output direct DFT that reads its inputs from shared memory.
 //
 // Every index computation lives in __host__ __device__ functions so the
@@ -162,6 +163,81 @@ struct Dft<8, DIR> {
   }
 };
 
+// Odd prime radices 5..31 in registers: with H = (R-1)/2 and the input
+// pairs a_j = x_j + x_{R-j}, b_j = x_j - x_{R-j} (j = 1..H),
+//   y_k     = x_0 + sum_j a_j cos(2 pi jk/R) + DIR i sum_j b_j sin(2 pi jk/R)
+//   y_{R-k} = the same with the sine term negated,
+// which needs H^2 complex-by-real products per sum instead of R^2 complex
+// ones.  cos/sin of 2 pi m/R come from the stage's twiddle table
+// (entry m*nR*tws holds e^{-2 pi i m / R}).
+MC3_HD constexpr bool is_prime_radix(int R) {
+  return R == 5 || R == 7 || R == 11 || R == 13 || R == 17 || R == 19 || R == 23 || R == 29 ||
+         R == 31;
+}
+template <int R, int DIR>
+MC3_HD void dft_prime(float2* v, const float2* tw, int tws, int nR) {
+  constexpr int H = (R - 1) / 2;
+  float cs[H + 1], sn[H + 1];
+#pragma unroll
+  for (int m = 1; m <= H; ++m) {
+    const float2 w = tw[m * nR * tws];
+    cs[m] = w.x;
+    sn[m] = -w.y;
+  }
+  float2 a[H + 1], b[H + 1];
+  const float2 x0 = v[0];
+  float2 y0 = x0;
+#pragma unroll
+  for (int j = 1; j <= H; ++j) {
+    a[j] = cadd(v[j], v[R - j]);
+    b[j] = csub(v[j], v[R - j]);
+    y0 = cadd(y0, a[j]);
+  }
+  v[0] = y0;  // the inputs now live in x0, a and b; outputs overwrite v
+#pragma unroll
+  for (int k = 1; k <= H; ++k) {
+    float2 A = x0, B = c2(0.f, 0.f);
+#pragma unroll
+    for (int j = 1; j <= H; ++j) {
+      const int m = (j * k) % R;
+      const float cm = m <= H ? cs[m] : cs[R - m];
+      const float sm = m <= H ? sn[m] : -sn[R - m];
+      A.x += a[j].x * cm;
+      A.y += a[j].y * cm;
+      B.x += b[j].x * sm;
+      B.y += b[j].y * sm;
+    }
+    // i*B = (-B.y, B.x)
+    if (DIR < 0) {
+      v[k] = c2(A.x + B.y, A.y - B.x);
+      v[R - k] = c2(A.x - B.y, A.y + B.x);
+    } else {
+      v[k] = c2(A.x - B.y, A.y + B.x);
+      v[R - k] = c2(A.x + B.y, A.y - B.x);
+    }
+  }
+}
+
+// One butterfly of a prime-radix stage (register DFT above).
+template <int R, int DIR>
+MC3_HD void stage_bfly_prime(const float2* A, float2* B, int n, int Ns, int j,
+                             const float2* tw, int tws, int es) {
+  const int nR = n / R;
+  const int k = j % Ns;
+  float2 v[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) v[r] = A[(j + r * nR) * es];
+  if (Ns > 1) {
+    const int step = (n / (Ns * R)) * k;
+#pragma unroll
+    for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twid<DIR>(tw, tws, step * r));
+  }
+  dft_prime<R, DIR>(v, tw, tws, nR);
+  const int idxD = (j / Ns) * Ns * R + k;
+#pragma unroll
+  for (int r = 0; r < R; ++r) B[(idxD + r * Ns) * es] = v[r];
+}
+
 // One butterfly of a dedicated-radix stage.  A/B: sequence base pointers,
 // es: element stride.
 template <int R, int DIR>
@@ -205,7 +281,9 @@ MC3_HD void stage_direct(const float2* A, float2* B, int n, int R, int Ns, int o
   B[(idxD + q * Ns) * es] = acc;
 }
 
-MC3_HD bool radix_is_dedicated(int R) { return R == 2 || R == 3 || R == 4 || R == 8; }
+MC3_HD bool radix_is_dedicated(int R) {
+  return R == 2 || R == 3 || R == 4 || R == 8 || is_prime_radix(R);
+}
 
 template <int DIR>
 MC3_HD void stage_item(const float2* A, float2* B, int n, int R, int Ns, int item,
@@ -215,6 +293,15 @@ MC3_HD void stage_item(const float2* A, float2* B, int n, int R, int Ns, int ite
     case 3: stage_bfly<3, DIR>(A, B, n, Ns, item, tw, tws, es); break;
     case 4: stage_bfly<4, DIR>(A, B, n, Ns, item, tw, tws, es); break;
     case 8: stage_bfly<8, DIR>(A, B, n, Ns, item, tw, tws, es); break;
+    case 5: stage_bfly_prime<5, DIR>(A, B, n, Ns, item, tw, tws, es); break;
+    case 7: stage_bfly_prime<7, DIR>(A, B, n, Ns, item, tw, tws, es); break;
+    case 11: stage_bfly_prime<11, DIR>(A, B, n, Ns, item, tw, tws, es); break;
+    case 13: stage_bfly_prime<13, DIR>(A, B, n, Ns, item, tw, tws, es); break;
+    case 17: stage_bfly_prime<17, DIR>(A, B, n, Ns, item, tw, tws, es); break;
+    case 19: stage_bfly_prime<19, DIR>(A, B, n, Ns, item, tw, tws, es); break;
+    case 23: stage_bfly_prime<23, DIR>(A, B, n, Ns, item, tw, tws, es); break;
+    case 29: stage_bfly_prime<29, DIR>(A, B, n, Ns, item, tw, tws, es); break;
+    case 31: stage_bfly_prime<31, DIR>(A, B, n, Ns, item, tw, tws, es); break;
     default: stage_direct<DIR>(A, B, n, R, Ns, item, tw, tws, es); break;
   }
 }
