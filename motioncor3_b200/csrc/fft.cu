@@ -429,13 +429,15 @@ __global__ void __launch_bounds__(kCtThreads, 2) k_row_c2r_ct(const float2* in, 
   }
 }
 
-template <int H>
-__global__ void __launch_bounds__(kCtThreads, 2) k_col_fft_ct(const float2* in, float2* out,
-                                                              long pitch, int cmpX, Batch bt,
-                                                              const float2* __restrict__ tw,
-                                                              ColOps ops) {
+// TX columns per CTA (default: two CTAs of kCtThreads per SM); the wide
+// form (TX doubled, 2*kCtThreads threads, one CTA per SM) reads full 32-byte
+// sectors at H = 4096.
+template <int H, int TX, int T>
+__global__ void __launch_bounds__(T, 1024 / T) k_col_fft_ct(const float2* in, float2* out,
+                                                           long pitch, int cmpX, Batch bt,
+                                                           const float2* __restrict__ tw,
+                                                           ColOps ops) {
   constexpr int LD = ct_spad_len(H);
-  constexpr int TX = ct_batch(LD);
   extern __shared__ float2 sm[];
   const int item = blockIdx.y;
   const int x0 = blockIdx.x * TX;
@@ -459,11 +461,11 @@ __global__ void __launch_bounds__(kCtThreads, 2) k_col_fft_ct(const float2* in, 
         sm[c * LD + spad(y)] = v;
       });
   __syncthreads();
-  if (ops.dir < 0) cta_fft_ct<-1, H, TX, kCtThreads, LD>(sm, tw, 1);
-  else cta_fft_ct<1, H, TX, kCtThreads, LD>(sm, tw, 1);
+  if (ops.dir < 0) cta_fft_ct<-1, H, TX, T, LD>(sm, tw, 1);
+  else cta_fft_ct<1, H, TX, T, LD>(sm, tw, 1);
   float2* dst = out + (long)item * bt.out_stride;
   float2* crop = ops.crop ? ops.crop + (long)item * ops.crop_x * ops.crop_y : nullptr;
-  for (int t = threadIdx.x; t < TX * H; t += kCtThreads) {
+  for (int t = threadIdx.x; t < TX * H; t += T) {
     const int y = t / TX, c = t % TX;
     const int x = x0 + c;
     if (x >= cmpX) continue;
@@ -503,17 +505,26 @@ int launch_row_c2r_ct(const float2* in, long in_pitch, float* out, long out_pitc
   MC3_CHECK_LAUNCH("k_row_c2r_ct");
   return kOk;
 }
-template <int H>
+template <int H, bool WIDE = false>
 int launch_col_fft_ct(const float2* in, float2* out, long pitch, int cmpX, const Batch& b,
                       const float2* tw, const ColOps& ops, cudaStream_t st) {
   constexpr int LD = ct_spad_len(H);
-  constexpr int TX = ct_batch(LD);
+  constexpr int TX = ct_batch(LD) * (WIDE ? 2 : 1);
+  constexpr int T = kCtThreads * (WIDE ? 2 : 1);
   const size_t smem = (size_t)TX * LD * sizeof(float2);
-  MC3_TRY(set_smem_attr(k_col_fft_ct<H>, smem));
+  MC3_TRY(set_smem_attr(k_col_fft_ct<H, TX, T>, smem));
   dim3 grid(ceil_div(cmpX, TX), b.items);
-  k_col_fft_ct<H><<<grid, kCtThreads, smem, st>>>(in, out, pitch, cmpX, b, tw, ops);
+  k_col_fft_ct<H, TX, T><<<grid, T, smem, st>>>(in, out, pitch, cmpX, b, tw, ops);
   MC3_CHECK_LAUNCH("k_col_fft_ct");
   return kOk;
+}
+// MC3_FFT_COL_WIDE=1 selects the wide 4096-point column form (A/B runs).
+bool col_wide() {
+  static const bool on = [] {
+    const char* e = getenv("MC3_FFT_COL_WIDE");
+    return e && e[0] == '1';
+  }();
+  return on;
 }
 // MC3_FFT_RUNTIME_PLAN=1 keeps the runtime-plan in-place kernels (A/B runs).
 bool ct_off() {
@@ -661,7 +672,9 @@ int col_fft(const float2* in, float2* out, long pitch, int cmpX, int H, const Ba
       case 512: return launch_col_fft_ct<512>(in, out, pitch, cmpX, b, d.tw, ops, st);
       case 1024: return launch_col_fft_ct<1024>(in, out, pitch, cmpX, b, d.tw, ops, st);
       case 2048: return launch_col_fft_ct<2048>(in, out, pitch, cmpX, b, d.tw, ops, st);
-      case 4096: return launch_col_fft_ct<4096>(in, out, pitch, cmpX, b, d.tw, ops, st);
+      case 4096:
+        if (col_wide()) return launch_col_fft_ct<4096, true>(in, out, pitch, cmpX, b, d.tw, ops, st);
+        return launch_col_fft_ct<4096>(in, out, pitch, cmpX, b, d.tw, ops, st);
       default: break;
     }
   }
