@@ -43,6 +43,16 @@ def build_ref_host() -> str | None:
     return REF_LIB if os.path.exists(REF_LIB) else None
 
 
+def build_ref_program() -> str | None:
+    """Compiles the reference program itself (checker for the command line)
+    from the reference tree when it exists; make keeps it incremental."""
+    exe = os.path.join(HERE, "_ref", "MotionCor3")
+    if os.path.isdir(REF_TREE):
+        d = os.path.join(HERE, "ref_full")
+        subprocess.run(["make", "-C", d, f"REF={REF_TREE}", "-j8"], check=True, capture_output=True)
+    return exe if os.path.exists(exe) else None
+
+
 class OracleParams(ctypes.Structure):
     _fields_ = [
         ("patch", ctypes.c_int * 2),
