@@ -407,9 +407,9 @@ __device__ void cta_fft_inplace(float2* buf, const FftDesc& d, int nb, int ld) {
 #endif
 
 // ---- compile-time plans for power-of-two lengths -----------------------
-// The same factorisation as fft_factorize (so results are identical to the
-// runtime in-place path), evaluated at compile time: all index arithmetic
-// of a stage becomes shifts and masks and every loop unrolls.
+// The same factorisation as fft_factorize, evaluated at compile time: all
+// index arithmetic of a stage becomes shifts and masks and every loop
+// unrolls.
 MC3_HD constexpr int ct_log2(int n) {
   int l = 0;
   while ((1 << l) < n) ++l;
@@ -441,8 +441,8 @@ MC3_HD constexpr int ct_spad_len(int n) { return n + (n >> 5) + 1; }
 
 #ifdef __CUDACC__
 // One in-place stage over NB sequences of N elements (sequence b at
-// buf[b*LD + spad(i)]) by a CTA of T threads; same arithmetic as
-// stage_inplace.
+// buf[b*LD + spad(i)]) by a CTA of T threads; the arithmetic of
+// stage_inplace except for the twiddle powers (see below).
 template <int R, int DIR, int N, int NS, int NB, int T, int LD>
 __device__ __forceinline__ void stage_ct(float2* buf, const float2* __restrict__ tw, int tws) {
   constexpr int per = N / R;
@@ -468,9 +468,24 @@ __device__ __forceinline__ void stage_ct(float2* buf, const float2* __restrict__
       const unsigned b = it / per, j = it % per;
       const unsigned k = j % NS;
       if (NS > 1) {
+        // One table read per butterfly; the other powers of the twiddle by
+        // a product tree of depth <= 3 (a few FP32 ulp), which keeps the
+        // shared L1/shared-memory pipe free of six more loads.
         const int step = (N / (NS * R)) * k;
+        float2 w[R];
+        w[1] = twid<DIR>(tw, tws, step);
+        if constexpr (R >= 4) {
+          w[2] = cmul(w[1], w[1]);
+          w[3] = cmul(w[2], w[1]);
+        }
+        if constexpr (R == 8) {
+          w[4] = cmul(w[2], w[2]);
+          w[5] = cmul(w[4], w[1]);
+          w[6] = cmul(w[3], w[3]);
+          w[7] = cmul(w[4], w[3]);
+        }
 #pragma unroll
-        for (int r = 1; r < R; ++r) v[m][r] = cmul(v[m][r], twid<DIR>(tw, tws, step * r));
+        for (int r = 1; r < R; ++r) v[m][r] = cmul(v[m][r], w[r]);
       }
       Dft<R, DIR>::run(v[m]);
       const unsigned idxD = (j / NS) * NS * R + k;
