@@ -266,13 +266,20 @@ def run_ours(args, wl, world, rank, local):
     if top:
         name, (n_launch, tot_ms, tot_bytes) = top
         achieved = (tot_bytes / n_launch) / ((tot_ms / n_launch) / 1000.0) / 1e9
-        traffic = None
+        # DRAM traffic per launch: the ncu-measured ratio of DRAM bytes to
+        # algorithmic bytes for this kernel (profiles/traffic.json, captured
+        # on a smaller case of the same launch shape), scaled to this launch
+        traffic, traffic_src = None, None
         tp = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tp):
-            traffic = json.load(open(tp)).get(name)
+            ent = json.load(open(tp)).get(name)
+            if ent:
+                traffic = ent["dram_over_algorithmic"] * tot_bytes / n_launch
+                traffic_src = ent["capture"]
         roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
                 "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "launches_per_step": n_launch / args.steps,
+                "traffic": traffic, "traffic_source": traffic_src,
+                "launches_per_step": n_launch / args.steps,
                 "share_of_step": tot_ms / ms if ms else None,
                 "algorithmic_bytes_per_launch": tot_bytes / n_launch}
 

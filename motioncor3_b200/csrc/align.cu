@@ -318,7 +318,7 @@ int corr_cols(const float2* spec, const int* act, const float2* ex, const float2
   FftDesc dH;
   MC3_TRY(make_desc(d.cmpY, d.cmpY, &dH));
   if (all_dedicated(dH) && !getenv("MC3_FFT_PINGPONG") && !getenv("MC3_FFT_RUNTIME_PLAN")) {
-    prof::Scope ps("k_corr_cols", (double)d.A * ((double)d.cmpX * d.cmpY * 8.0 * (d.N + 1) + (double)d.G * d.seaY * d.cmpX * 8.0), st);
+    prof::Scope ps("k_corr_cols_ct", (double)d.A * ((double)d.cmpX * d.cmpY * 8.0 * (d.N + 1) + (double)d.G * d.seaY * d.cmpX * 8.0), st);
     switch (d.cmpY) {
       case 256: return launch_corr_cols_ct<256>(spec, act, ex, ey, S, gstart, gsize, bfactor, phase_only, T, d, dH.tw, st);
       case 512: return launch_corr_cols_ct<512>(spec, act, ex, ey, S, gstart, gsize, bfactor, phase_only, T, d, dH.tw, st);

@@ -584,15 +584,21 @@ int row_r2c(const float* in, long in_pitch, float2* out, long out_pitch, int W, 
   FftDesc d;
   MC3_TRY(make_desc(M, W, &d));
   if (use_inplace(d) && !ct_off()) {
-    prof::Scope ps("k_row_r2c", (double)b.items * H * (W * 4.0 + (W / 2 + 1) * 8.0), st);
+    const double bytes = (double)b.items * H * (W * 4.0 + (W / 2 + 1) * 8.0);
+#define MC3_CT(NAME, MM)                                                                   \
+  case MM: {                                                                               \
+    prof::Scope ps(NAME, bytes, st);                                                       \
+    return launch_row_r2c_ct<MM>(in, in_pitch, out, out_pitch, H, b, d.tw, scale, st);    \
+  }
     switch (M) {
-      case 128: return launch_row_r2c_ct<128>(in, in_pitch, out, out_pitch, H, b, d.tw, scale, st);
-      case 256: return launch_row_r2c_ct<256>(in, in_pitch, out, out_pitch, H, b, d.tw, scale, st);
-      case 512: return launch_row_r2c_ct<512>(in, in_pitch, out, out_pitch, H, b, d.tw, scale, st);
-      case 1024: return launch_row_r2c_ct<1024>(in, in_pitch, out, out_pitch, H, b, d.tw, scale, st);
-      case 2048: return launch_row_r2c_ct<2048>(in, in_pitch, out, out_pitch, H, b, d.tw, scale, st);
+      MC3_CT("k_row_r2c_ct<128>", 128)
+      MC3_CT("k_row_r2c_ct<256>", 256)
+      MC3_CT("k_row_r2c_ct<512>", 512)
+      MC3_CT("k_row_r2c_ct<1024>", 1024)
+      MC3_CT("k_row_r2c_ct<2048>", 2048)
       default: break;
     }
+#undef MC3_CT
   }
   if (use_inplace(d)) {
     const int ld = spad_len(M + 1);
@@ -625,15 +631,21 @@ int row_c2r(const float2* in, long in_pitch, float* out, long out_pitch, int W, 
   FftDesc d;
   MC3_TRY(make_desc(M, W, &d));
   if (use_inplace(d) && !ct_off()) {
-    prof::Scope ps("k_row_c2r", (double)b.items * H * (W * 4.0 + (W / 2 + 1) * 8.0), st);
+    const double bytes = (double)b.items * H * (W * 4.0 + (W / 2 + 1) * 8.0);
+#define MC3_CT(NAME, MM)                                                              \
+  case MM: {                                                                          \
+    prof::Scope ps(NAME, bytes, st);                                                  \
+    return launch_row_c2r_ct<MM>(in, in_pitch, out, out_pitch, H, b, d.tw, st);       \
+  }
     switch (M) {
-      case 128: return launch_row_c2r_ct<128>(in, in_pitch, out, out_pitch, H, b, d.tw, st);
-      case 256: return launch_row_c2r_ct<256>(in, in_pitch, out, out_pitch, H, b, d.tw, st);
-      case 512: return launch_row_c2r_ct<512>(in, in_pitch, out, out_pitch, H, b, d.tw, st);
-      case 1024: return launch_row_c2r_ct<1024>(in, in_pitch, out, out_pitch, H, b, d.tw, st);
-      case 2048: return launch_row_c2r_ct<2048>(in, in_pitch, out, out_pitch, H, b, d.tw, st);
+      MC3_CT("k_row_c2r_ct<128>", 128)
+      MC3_CT("k_row_c2r_ct<256>", 256)
+      MC3_CT("k_row_c2r_ct<512>", 512)
+      MC3_CT("k_row_c2r_ct<1024>", 1024)
+      MC3_CT("k_row_c2r_ct<2048>", 2048)
       default: break;
     }
+#undef MC3_CT
   }
   if (use_inplace(d)) {
     const int ld = spad_len(M + 1);
@@ -666,17 +678,25 @@ int col_fft(const float2* in, float2* out, long pitch, int cmpX, int H, const Ba
   FftDesc d;
   MC3_TRY(make_desc(H, H, &d));
   if (use_inplace(d) && !ct_off()) {
-    prof::Scope ps("k_col_fft", (double)b.items * ((double)cmpX * H * 16.0 + (ops.crop ? (double)ops.crop_x * ops.crop_y * 8.0 : 0.0)), st);
+    const double bytes = (double)b.items * ((double)cmpX * H * 16.0 + (ops.crop ? (double)ops.crop_x * ops.crop_y * 8.0 : 0.0));
+#define MC3_CT(NAME, HH)                                                              \
+  case HH: {                                                                          \
+    prof::Scope ps(NAME, bytes, st);                                                  \
+    if constexpr (HH == 4096) {                                                       \
+      if (col_wide())                                                                 \
+        return launch_col_fft_ct<HH, true>(in, out, pitch, cmpX, b, d.tw, ops, st);   \
+    }                                                                                 \
+    return launch_col_fft_ct<HH>(in, out, pitch, cmpX, b, d.tw, ops, st);             \
+  }
     switch (H) {
-      case 256: return launch_col_fft_ct<256>(in, out, pitch, cmpX, b, d.tw, ops, st);
-      case 512: return launch_col_fft_ct<512>(in, out, pitch, cmpX, b, d.tw, ops, st);
-      case 1024: return launch_col_fft_ct<1024>(in, out, pitch, cmpX, b, d.tw, ops, st);
-      case 2048: return launch_col_fft_ct<2048>(in, out, pitch, cmpX, b, d.tw, ops, st);
-      case 4096:
-        if (col_wide()) return launch_col_fft_ct<4096, true>(in, out, pitch, cmpX, b, d.tw, ops, st);
-        return launch_col_fft_ct<4096>(in, out, pitch, cmpX, b, d.tw, ops, st);
+      MC3_CT("k_col_fft_ct<256>", 256)
+      MC3_CT("k_col_fft_ct<512>", 512)
+      MC3_CT("k_col_fft_ct<1024>", 1024)
+      MC3_CT("k_col_fft_ct<2048>", 2048)
+      MC3_CT("k_col_fft_ct<4096>", 4096)
       default: break;
     }
+#undef MC3_CT
   }
   if (use_inplace(d)) {
     const int ld = spad_len(H);
