@@ -134,32 +134,38 @@ int frame_sums(const float2* spec, long fr_stride, int N, int cmpX, int cmpY, co
 // frame); the accumulation runs in patch order exactly as the reference's,
 // as predicated adds rather than branches.
 // EXACT: P == PMAX; otherwise P < PMAX and reads are clamped to patch P-1.
-template <int PMAX, bool EXACT>
+template <int PMAX, bool EXACT, int PX>
 __global__ void __launch_bounds__(128) k_local_gather(
     const float* __restrict__ in, long in_stride, float* out, long out_stride, int W, int H,
     const float* __restrict__ cent, const float2* __restrict__ sh,
     const unsigned long long* __restrict__ masks, const uint8_t* __restrict__ bad, int P, int nb) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  // PX pixels per thread, 128 apart in the row: each patch shift read
+  // (uniform over the warp) serves PX pixels.
   const int y = blockIdx.y;
-  if (x >= W) return;
+  const int xb = blockIdx.x * (128 * PX) + threadIdx.x;
   const float fB = 100.0f;
-  float w[PMAX];
-  unsigned long long inc = 0ull;  // patches within r <= 0.6 of this pixel
+  float w[PX][PMAX];
+  unsigned long long inc[PX];  // patches within r <= 0.6 of each pixel
 #pragma unroll
-  for (int p = 0; p < PMAX; ++p) {
-    w[p] = 0.0f;
-    if (EXACT || p < P) {
-      float ax = ((float)(unsigned)x - cent[2 * p]) / (float)(unsigned)W;
-      float ay = (y - cent[2 * p + 1]) / H;
-      ax = sqrtf(ax * ax + ay * ay);
-      if (!(ax > 0.6f)) {
-        w[p] = expf(-fB * ax);
-        inc |= 1ull << p;
+  for (int q = 0; q < PX; ++q) {
+    const int x = xb + 128 * q;
+    inc[q] = 0ull;
+#pragma unroll
+    for (int p = 0; p < PMAX; ++p) {
+      w[q][p] = 0.0f;
+      if (x < W && (EXACT || p < P)) {
+        float ax = ((float)(unsigned)x - cent[2 * p]) / (float)(unsigned)W;
+        float ay = (y - cent[2 * p + 1]) / H;
+        ax = sqrtf(ax * ax + ay * ay);
+        if (!(ax > 0.6f)) {
+          w[q][p] = expf(-fB * ax);
+          inc[q] |= 1ull << p;
+        }
       }
     }
   }
+  if (xb >= W) return;
   const int padX = (W / 2 + 1) * 2;
-  const long o = (long)y * padX + x;
   for (int f = 0; f < nb; ++f) {
     const float2* s = sh + (long)f * P;
     unsigned long long m = 0ull;
@@ -168,44 +174,60 @@ __global__ void __launch_bounds__(128) k_local_gather(
     } else if (bad) {
       for (int p = 0; p < P; ++p) m |= (unsigned long long)(bad[(long)f * P + p] != 0) << p;
     }
-    const unsigned long long use = inc & ~m;
-    float fSx = 0.0f, fSy = 0.0f, fW = 0.0f;
+    float fSx[PX], fSy[PX], fW[PX];
+    unsigned long long use[PX];
+#pragma unroll
+    for (int q = 0; q < PX; ++q) {
+      fSx[q] = fSy[q] = fW[q] = 0.0f;
+      use[q] = inc[q] & ~m;
+    }
 #pragma unroll
     for (int p = 0; p < PMAX; ++p) {
       const float2 sp = s[EXACT ? p : (p < P ? p : P - 1)];
-      if ((use >> p) & 1ull) {
-        fW += w[p];
-        fSx += sp.x * w[p];
-        fSy += sp.y * w[p];
+#pragma unroll
+      for (int q = 0; q < PX; ++q) {
+        if ((use[q] >> p) & 1ull) {
+          fW[q] += w[q][p];
+          fSx[q] += sp.x * w[q][p];
+          fSy[q] += sp.y * w[q][p];
+        }
       }
     }
-    if (fW > 0) {
-      fSx = fSx / fW;
-      fSy = fSy / fW;
+#pragma unroll
+    for (int q = 0; q < PX; ++q) {
+      const int x = xb + 128 * q;
+      if (x >= W) continue;
+      float sx = fSx[q], sy = fSy[q];
+      if (fW[q] > 0) {
+        sx = sx / fW[q];
+        sy = sy / fW[q];
+      }
+      int ix = (int)(((float)(unsigned)x - sx) * 1);
+      int iy = (int)((y - sy) * 1);
+      if (ix < 0 || iy < 0 || ix >= W || iy >= H) {
+        ix = (ix < 0) ? -ix : ix;
+        iy = (iy < 0) ? -iy : iy;
+        ix = (811 * ix) % W;
+        iy = (811 * iy) % H;
+        // Only non-finite shifts reach here out of range (the int conversion
+        // of NaN/inf); keep the read inside the frame.
+        if (ix < 0 || ix >= W) ix = 0;
+        if (iy < 0 || iy >= H) iy = 0;
+      }
+      out[(long)f * out_stride + (long)y * padX + x] = in[(long)f * in_stride + (long)iy * padX + ix];
     }
-    int ix = (int)(((float)(unsigned)x - fSx) * 1);
-    int iy = (int)((y - fSy) * 1);
-    if (ix < 0 || iy < 0 || ix >= W || iy >= H) {
-      ix = (ix < 0) ? -ix : ix;
-      iy = (iy < 0) ? -iy : iy;
-      ix = (811 * ix) % W;
-      iy = (811 * iy) % H;
-      // Only non-finite shifts reach here out of range (the int conversion
-      // of NaN/inf); keep the read inside the frame.
-      if (ix < 0 || ix >= W) ix = 0;
-      if (iy < 0 || iy >= H) iy = 0;
-    }
-    out[(long)f * out_stride + o] = in[(long)f * in_stride + (long)iy * padX + ix];
   }
 }
 
 template <int PMAX, bool EXACT>
-static void launch_gather(dim3 grid, cudaStream_t st, const float* in, long in_stride, float* out,
-                          long out_stride, int W, int H, const float* centers,
+static void launch_gather(int W, int H, cudaStream_t st, const float* in, long in_stride,
+                          float* out, long out_stride, const float* centers,
                           const float2* shifts, const unsigned long long* masks,
                           const uint8_t* bad, int P, int nb) {
-  k_local_gather<PMAX, EXACT><<<grid, 128, 0, st>>>(in, in_stride, out, out_stride, W, H, centers,
-                                                    shifts, masks, bad, P, nb);
+  constexpr int PX = PMAX <= 36 ? 2 : 1;
+  dim3 grid(ceil_div(W, 128 * PX), H);
+  k_local_gather<PMAX, EXACT, PX><<<grid, 128, 0, st>>>(in, in_stride, out, out_stride, W, H,
+                                                        centers, shifts, masks, bad, P, nb);
 }
 
 int local_gather(const float* in, long in_stride, float* out, long out_stride, int nb, int W,
@@ -213,10 +235,9 @@ int local_gather(const float* in, long in_stride, float* out, long out_stride, i
                  const unsigned long long* masks, const uint8_t* bad, int P, cudaStream_t st) {
   // `shifts`/`masks`/`bad` point at the first frame of the batch.
   if (P < 1 || P > 64) return kEUnsupported;
-  dim3 grid(ceil_div(W, 128), H);
   prof::Scope ps("k_local_gather", (double)nb * W * H * 8.0, st);
 #define MC3_GATHER(PM, EX) \
-  launch_gather<PM, EX>(grid, st, in, in_stride, out, out_stride, W, H, centers, shifts, masks, bad, P, nb)
+  launch_gather<PM, EX>(W, H, st, in, in_stride, out, out_stride, centers, shifts, masks, bad, P, nb)
   switch (P) {
     case 4: MC3_GATHER(4, true); break;
     case 9: MC3_GATHER(9, true); break;
