@@ -69,11 +69,6 @@ __device__ __forceinline__ void staged_copy(int total, LoadF load, StoreF store)
 }
 constexpr int kStageLoads = 8;
 
-__device__ __forceinline__ long batch_in_off(const Batch& b, int item) {
-  long off = (long)(item % b.nf) * b.in_stride;
-  if (b.patch_off) off += b.patch_off[item / b.nf];
-  return off;
-}
 
 // ---------------------------------------------------------------------
 // Row real FFT (R2C): each CTA transforms `rows` rows of one batch item.
@@ -580,6 +575,10 @@ int col_tile(int H) {
 int row_r2c(const float* in, long in_pitch, float2* out, long out_pitch, int W, int H,
             const Batch& b, float scale, cudaStream_t st) {
   if (W < 2 || (W & 1) || H < 1 || b.items < 1) return kEInval;
+  {
+    const int s = row_r2c_r16(in, in_pitch, out, out_pitch, W, H, b, scale, st);
+    if (s != kEUnsupported) return s;
+  }
   const int M = W / 2;
   FftDesc d;
   MC3_TRY(make_desc(M, W, &d));
@@ -627,6 +626,10 @@ int row_r2c(const float* in, long in_pitch, float2* out, long out_pitch, int W, 
 int row_c2r(const float2* in, long in_pitch, float* out, long out_pitch, int W, int H,
             const Batch& b, cudaStream_t st) {
   if (W < 2 || (W & 1) || H < 1 || b.items < 1) return kEInval;
+  {
+    const int s = row_c2r_r16(in, in_pitch, out, out_pitch, W, H, b, st);
+    if (s != kEUnsupported) return s;
+  }
   const int M = W / 2;
   FftDesc d;
   MC3_TRY(make_desc(M, W, &d));
@@ -675,6 +678,10 @@ int col_fft(const float2* in, float2* out, long pitch, int cmpX, int H, const Ba
             const ColOps& ops, cudaStream_t st) {
   if (cmpX < 1 || H < 1 || b.items < 1) return kEInval;
   if (ops.crop && (ops.crop_x > cmpX || ops.crop_y > H)) return kEInval;
+  {
+    const int s = col_fft_r16(in, out, pitch, cmpX, H, b, ops, st);
+    if (s != kEUnsupported) return s;
+  }
   FftDesc d;
   MC3_TRY(make_desc(H, H, &d));
   if (use_inplace(d) && !ct_off()) {

@@ -60,6 +60,26 @@ struct Batch {
   long out_stride;        // elements between consecutive items
 };
 
+#ifdef __CUDACC__
+__device__ __forceinline__ long batch_in_off(const Batch& b, int item) {
+  long off = (long)(item % b.nf) * b.in_stride;
+  if (b.patch_off) off += b.patch_off[item / b.nf];
+  return off;
+}
+#endif
+
+// Radix-16 register passes (fft_r16.cu) for power-of-two lengths: return
+// kEUnsupported for other lengths (the caller then uses another kernel).
+struct ColOps;
+int row_r2c_r16(const float* in, long in_pitch, float2* out, long out_pitch, int W, int H,
+                const Batch& b, float scale, cudaStream_t st);
+int row_c2r_r16(const float2* in, long in_pitch, float* out, long out_pitch, int W, int H,
+                const Batch& b, cudaStream_t st);
+int col_fft_r16(const float2* in, float2* out, long pitch, int cmpX, int H, const Batch& b,
+                const ColOps& ops, cudaStream_t st);
+// MC3_FFT_R16=0 disables them (A/B runs).
+bool r16_enabled();
+
 // Row real FFT: rows of W reals (row pitch in_pitch floats) -> W/2+1
 // complex (row pitch out_pitch complex), multiplied by `scale`.  In-place
 // use (out aliases in with in_pitch = 2*out_pitch) is allowed.

@@ -509,9 +509,12 @@ __device__ __forceinline__ void cta_fft_ct(float2* buf, const float2* __restrict
 #endif
 
 // Paired real-transform helpers working in place on one row held at
-// buf[spad(i)]: pair p (0 <= p <= M/2) owns elements p and M-p.
+// buf[i + (i >> SH)] (SH = 5: spad, SH = 4: spad16): pair p (0 <= p <= M/2)
+// owns elements p and M-p.
 // Forward post-processing: Z[0..M) -> X[0..M].
+template <int SH = 5>
 MC3_HD void r2c_post_pair(float2* buf, int M, int p, const float2* twW, float scale) {
+  auto spad = [](int i) { return i + (i >> SH); };
   if (p == 0) {
     const float2 z = buf[spad(0)];
     buf[spad(0)] = c2((z.x + z.y) * scale, 0.0f);
@@ -539,7 +542,9 @@ MC3_HD void r2c_post_pair(float2* buf, int M, int p, const float2* twW, float sc
 
 // Inverse pre-processing: X[0..M] -> Z[0..M) (imaginary parts of X[0] and
 // X[M] ignored, see c2r_pre).
+template <int SH = 5>
 MC3_HD void c2r_pre_pair(float2* buf, int M, int p, const float2* twW) {
+  auto spad = [](int i) { return i + (i >> SH); };
   if (p == 0) {
     const float a = buf[spad(0)].x, b = buf[spad(M)].x;
     buf[spad(0)] = c2(a + b, a - b);

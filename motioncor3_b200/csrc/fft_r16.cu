@@ -1,0 +1,265 @@
+// Row and column passes built on the radix-16 register FFT (fft_r16.cuh):
+// the first stage reads global memory directly, the last stage writes it
+// directly, and shared memory only carries the exchanges between stages.
+// 512 threads per CTA, up to 72 KB of shared memory, two CTAs per SM.
+#include <cstdlib>
+
+#include "fft.cuh"
+#include "fft_r16.cuh"
+
+namespace mc3 {
+
+namespace {
+constexpr int kR16Threads = 512;
+constexpr int kR16Budget = 72 * 1024;
+// Sequences per CTA: one per N/16 threads.
+__host__ __device__ constexpr int r16_batch(int n) { return kR16Threads / (n / 16); }
+}  // namespace
+
+bool r16_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("MC3_FFT_R16");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+// ---------------------------------------------------------------------
+// Column pass: NB adjacent columns per CTA; thread t -> column t % NB,
+// slot t / NB, so a warp's loads cover NB adjacent columns of 32/NB rows.
+// ---------------------------------------------------------------------
+template <int H>
+__global__ void __launch_bounds__(kR16Threads, 2) k_col_fft_r16(const float2* in, float2* out,
+                                                                long pitch, int cmpX, Batch bt,
+                                                                const float2* __restrict__ tw,
+                                                                ColOps ops) {
+  constexpr int NB = r16_batch(H);
+  constexpr int LD = spad16_len(H);
+  static_assert(NB * LD * (int)sizeof(float2) <= kR16Budget, "shared memory budget");
+  extern __shared__ float2 sm[];
+  const int item = blockIdx.y;
+  const int c = threadIdx.x % NB;
+  const int j = threadIdx.x / NB;
+  const int x = blockIdx.x * NB + c;
+  const bool live = x < cmpX;
+  const float2* src = in + batch_in_off(bt, item) + x;
+  const float2* ex = ops.ex ? ops.ex + (long)item * cmpX : nullptr;
+  const float2* ey = ops.ey ? ops.ey + (long)item * H : nullptr;
+  const float2 exx = (ex && live) ? ex[x] : c2(1.f, 0.f);
+  float2* dst = out + (long)item * bt.out_stride + x;
+  float2* crop = ops.crop ? ops.crop + (long)item * ops.crop_x * ops.crop_y + x : nullptr;
+  const bool in_crop = crop && x < ops.crop_x;
+  auto load = [&](int y) {
+    if (!live) return c2(0.f, 0.f);
+    float2 v = src[(long)y * pitch];
+    if (ey) v = cmul(v, cmul(exx, ey[y]));
+    return v;
+  };
+  auto store = [&](int y, float2 v) {
+    if (!live) return;
+    v = cscale(v, ops.scale);
+    dst[(long)y * pitch] = v;
+    if (in_crop) {
+      int yo = -1;
+      if (y <= ops.crop_y / 2) yo = y;
+      else if (y > H - ops.crop_y / 2) yo = y - H + ops.crop_y;
+      if (yo >= 0) crop[(long)yo * ops.crop_x] = v;
+    }
+  };
+  float2* buf = sm + c * LD;
+  if (ops.dir < 0) fft_r16<-1, H, false, false>(buf, j, tw, 1, load, store);
+  else fft_r16<1, H, false, false>(buf, j, tw, 1, load, store);
+}
+
+// ---------------------------------------------------------------------
+// Row R2C: ROWS rows per CTA, M = W/2 complex points per row (the real row
+// read as complex pairs), thread t -> row t / (M/16), slot t % (M/16).  The
+// transform ends in shared memory for the paired post-processing, then the
+// W/2+1 outputs of each row are stored.
+// ---------------------------------------------------------------------
+template <int M>
+__global__ void __launch_bounds__(kR16Threads, 2) k_row_r2c_r16(const float* __restrict__ in,
+                                                                long in_pitch, float2* out,
+                                                                long out_pitch, int H, Batch bt,
+                                                                const float2* __restrict__ tw,
+                                                                float scale) {
+  constexpr int ROWS = r16_batch(M);
+  constexpr int LD = spad16_len(M + 1);
+  static_assert(ROWS * LD * (int)sizeof(float2) <= kR16Budget, "shared memory budget");
+  extern __shared__ float2 sm[];
+  const int item = blockIdx.y;
+  const int rr = threadIdx.x / (M / 16);
+  const int j = threadIdx.x % (M / 16);
+  const int r0 = blockIdx.x * ROWS;
+  const int nr = min(ROWS, H - r0);
+  const bool live = rr < nr;
+  const float* src = in + batch_in_off(bt, item) + (long)(r0 + rr) * in_pitch;
+  const bool pair = ((reinterpret_cast<uintptr_t>(in + batch_in_off(bt, item)) & 7) == 0) &&
+                    !(in_pitch & 1);
+  auto load = [&](int m) {
+    if (!live) return c2(0.f, 0.f);
+    const float* p = src + 2 * m;
+    return pair ? *reinterpret_cast<const float2*>(p) : c2(p[0], p[1]);
+  };
+  auto none = [](int, float2) {};
+  // tw: the W-point table; the M-point stages read every second entry
+  fft_r16<-1, M, false, true>(sm + rr * LD, j, tw, 2, load, none);
+  constexpr int NP = M / 2 + 1;
+  for (int t = threadIdx.x; t < nr * NP; t += kR16Threads) {
+    const int r = t / NP, p = t % NP;
+    r2c_post_pair<4>(sm + r * LD, M, p, tw, scale);
+  }
+  __syncthreads();
+  float2* dst = out + (long)item * bt.out_stride + (long)r0 * out_pitch;
+  for (int t = threadIdx.x; t < nr * (M + 1); t += kR16Threads) {
+    const int r = t / (M + 1), k = t % (M + 1);
+    dst[(long)r * out_pitch + k] = sm[r * LD + spad16(k)];
+  }
+}
+
+// ---------------------------------------------------------------------
+// Row C2R (unnormalised): rows loaded to shared memory, paired
+// pre-processing in place, then the transform from shared memory with the
+// last stage storing real pairs straight to global memory.
+// ---------------------------------------------------------------------
+template <int M>
+__global__ void __launch_bounds__(kR16Threads, 2) k_row_c2r_r16(const float2* in, long in_pitch,
+                                                                float* out, long out_pitch, int H,
+                                                                Batch bt,
+                                                                const float2* __restrict__ tw) {
+  constexpr int ROWS = r16_batch(M);
+  constexpr int LD = spad16_len(M + 1);
+  static_assert(ROWS * LD * (int)sizeof(float2) <= kR16Budget, "shared memory budget");
+  extern __shared__ float2 sm[];
+  const int item = blockIdx.y;
+  const int r0 = blockIdx.x * ROWS;
+  const int nr = min(ROWS, H - r0);
+  const float2* src = in + batch_in_off(bt, item) + (long)r0 * in_pitch;
+  for (int t = threadIdx.x; t < nr * (M + 1); t += kR16Threads) {
+    const int r = t / (M + 1), k = t % (M + 1);
+    sm[r * LD + spad16(k)] = src[(long)r * in_pitch + k];
+  }
+  __syncthreads();
+  constexpr int NP = M / 2 + 1;
+  for (int t = threadIdx.x; t < nr * NP; t += kR16Threads) {
+    const int r = t / NP, p = t % NP;
+    c2r_pre_pair<4>(sm + r * LD, M, p, tw);
+  }
+  __syncthreads();
+  const int rr = threadIdx.x / (M / 16);
+  const int j = threadIdx.x % (M / 16);
+  const bool live = rr < nr;
+  float* dst = out + (long)item * bt.out_stride + (long)(r0 + rr) * out_pitch;
+  const bool pair = ((reinterpret_cast<uintptr_t>(out + (long)item * bt.out_stride) & 7) == 0) &&
+                    !(out_pitch & 1);
+  auto none = [](int) { return c2(0.f, 0.f); };
+  auto store = [&](int m, float2 v) {
+    if (!live) return;
+    float* p = dst + 2 * m;
+    if (pair) {
+      *reinterpret_cast<float2*>(p) = v;
+    } else {
+      p[0] = v.x;
+      p[1] = v.y;
+    }
+  };
+  fft_r16<1, M, true, false>(sm + rr * LD, j, tw, 2, none, store);
+}
+
+// ---------------------------------------------------------------------
+// Launchers (compile-time lengths 256..4096 columns, 128..2048 row pairs).
+// ---------------------------------------------------------------------
+namespace {
+template <int H>
+int launch_col(const float2* in, float2* out, long pitch, int cmpX, const Batch& b,
+               const float2* tw, const ColOps& ops, const char* name, cudaStream_t st) {
+  constexpr int NB = r16_batch(H);
+  const size_t smem = (size_t)NB * spad16_len(H) * sizeof(float2);
+  MC3_TRY(set_smem_attr(k_col_fft_r16<H>, smem));
+  dim3 grid(ceil_div(cmpX, NB), b.items);
+  prof::Scope ps(name, (double)b.items * ((double)cmpX * H * 16.0 + (ops.crop ? (double)ops.crop_x * ops.crop_y * 8.0 : 0.0)), st);
+  k_col_fft_r16<H><<<grid, kR16Threads, smem, st>>>(in, out, pitch, cmpX, b, tw, ops);
+  MC3_CHECK_LAUNCH(name);
+  return kOk;
+}
+template <int M>
+int launch_r2c(const float* in, long in_pitch, float2* out, long out_pitch, int H, const Batch& b,
+               const float2* tw, float scale, const char* name, cudaStream_t st) {
+  constexpr int ROWS = r16_batch(M);
+  const size_t smem = (size_t)ROWS * spad16_len(M + 1) * sizeof(float2);
+  MC3_TRY(set_smem_attr(k_row_r2c_r16<M>, smem));
+  dim3 grid(ceil_div(H, ROWS), b.items);
+  prof::Scope ps(name, (double)b.items * H * (2 * M * 4.0 + (M + 1) * 8.0), st);
+  k_row_r2c_r16<M><<<grid, kR16Threads, smem, st>>>(in, in_pitch, out, out_pitch, H, b, tw, scale);
+  MC3_CHECK_LAUNCH(name);
+  return kOk;
+}
+template <int M>
+int launch_c2r(const float2* in, long in_pitch, float* out, long out_pitch, int H, const Batch& b,
+               const float2* tw, const char* name, cudaStream_t st) {
+  constexpr int ROWS = r16_batch(M);
+  const size_t smem = (size_t)ROWS * spad16_len(M + 1) * sizeof(float2);
+  MC3_TRY(set_smem_attr(k_row_c2r_r16<M>, smem));
+  dim3 grid(ceil_div(H, ROWS), b.items);
+  prof::Scope ps(name, (double)b.items * H * (2 * M * 4.0 + (M + 1) * 8.0), st);
+  k_row_c2r_r16<M><<<grid, kR16Threads, smem, st>>>(in, in_pitch, out, out_pitch, H, b, tw);
+  MC3_CHECK_LAUNCH(name);
+  return kOk;
+}
+}  // namespace
+
+int col_fft_r16(const float2* in, float2* out, long pitch, int cmpX, int H, const Batch& b,
+                const ColOps& ops, cudaStream_t st) {
+  if (!r16_enabled()) return kEUnsupported;
+  FftDesc d;
+  switch (H) {
+    case 256: case 512: case 1024: case 2048: case 4096: break;
+    default: return kEUnsupported;
+  }
+  MC3_TRY(make_desc(H, H, &d));
+  switch (H) {
+    case 256: return launch_col<256>(in, out, pitch, cmpX, b, d.tw, ops, "k_col_fft_r16<256>", st);
+    case 512: return launch_col<512>(in, out, pitch, cmpX, b, d.tw, ops, "k_col_fft_r16<512>", st);
+    case 1024: return launch_col<1024>(in, out, pitch, cmpX, b, d.tw, ops, "k_col_fft_r16<1024>", st);
+    case 2048: return launch_col<2048>(in, out, pitch, cmpX, b, d.tw, ops, "k_col_fft_r16<2048>", st);
+    default: return launch_col<4096>(in, out, pitch, cmpX, b, d.tw, ops, "k_col_fft_r16<4096>", st);
+  }
+}
+
+int row_r2c_r16(const float* in, long in_pitch, float2* out, long out_pitch, int W, int H,
+                const Batch& b, float scale, cudaStream_t st) {
+  if (!r16_enabled()) return kEUnsupported;
+  const int M = W / 2;
+  switch (M) {
+    case 256: case 512: case 1024: case 2048: break;
+    default: return kEUnsupported;
+  }
+  FftDesc d;
+  MC3_TRY(make_desc(M, W, &d));
+  switch (M) {
+    case 256: return launch_r2c<256>(in, in_pitch, out, out_pitch, H, b, d.tw, scale, "k_row_r2c_r16<256>", st);
+    case 512: return launch_r2c<512>(in, in_pitch, out, out_pitch, H, b, d.tw, scale, "k_row_r2c_r16<512>", st);
+    case 1024: return launch_r2c<1024>(in, in_pitch, out, out_pitch, H, b, d.tw, scale, "k_row_r2c_r16<1024>", st);
+    default: return launch_r2c<2048>(in, in_pitch, out, out_pitch, H, b, d.tw, scale, "k_row_r2c_r16<2048>", st);
+  }
+}
+
+int row_c2r_r16(const float2* in, long in_pitch, float* out, long out_pitch, int W, int H,
+                const Batch& b, cudaStream_t st) {
+  if (!r16_enabled()) return kEUnsupported;
+  const int M = W / 2;
+  switch (M) {
+    case 256: case 512: case 1024: case 2048: break;
+    default: return kEUnsupported;
+  }
+  FftDesc d;
+  MC3_TRY(make_desc(M, W, &d));
+  switch (M) {
+    case 256: return launch_c2r<256>(in, in_pitch, out, out_pitch, H, b, d.tw, "k_row_c2r_r16<256>", st);
+    case 512: return launch_c2r<512>(in, in_pitch, out, out_pitch, H, b, d.tw, "k_row_c2r_r16<512>", st);
+    case 1024: return launch_c2r<1024>(in, in_pitch, out, out_pitch, H, b, d.tw, "k_row_c2r_r16<1024>", st);
+    default: return launch_c2r<2048>(in, in_pitch, out, out_pitch, H, b, d.tw, "k_row_c2r_r16<2048>", st);
+  }
+}
+
+}  // namespace mc3

@@ -52,7 +52,8 @@ def shim():
     so = os.path.join(out_dir, "fft_core_shim.so")
     src = os.path.join(ROOT, "tests", "native", "fft_core_shim.cpp")
     hdr = os.path.join(ROOT, "motioncor3_b200", "csrc", "fft_core.cuh")
-    if not os.path.exists(so) or os.path.getmtime(so) < max(os.path.getmtime(src), os.path.getmtime(hdr)):
+    hdr16 = os.path.join(ROOT, "motioncor3_b200", "csrc", "fft_r16.cuh")
+    if not os.path.exists(so) or os.path.getmtime(so) < max(os.path.getmtime(src), os.path.getmtime(hdr), os.path.getmtime(hdr16)):
         cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
         subprocess.run([cxx, "-O2", "-shared", "-fPIC", "-I/usr/local/cuda/include", src, "-o", so],
                        check=True)

@@ -112,3 +112,59 @@ extern "C" int shim_irfft_pairs(const float* in, float* out, int W) {
   for (int m = 0; m < M; ++m) { out[2 * m] = z[m].x; out[2 * m + 1] = z[m].y; }
   return 0;
 }
+
+// ---- radix-16 register FFT (fft_r16.cuh), emulated thread by thread: each
+// stage runs the read phase of every slot, then the compute/write phase of
+// every slot, the order the device driver's barriers enforce.
+#include "../../motioncor3_b200/csrc/fft_r16.cuh"
+#include <array>
+
+template <int DIR, int N, int S>
+static void r16_host_stage(std::vector<float2>& buf, const float* in, float* out,
+                           const float2* tw) {
+  if constexpr (S < r16_nstages(N)) {
+    using St = R16Stage<N, S>;
+    const int slots = N / 16;
+    std::vector<std::array<float2, 16>> v(slots);
+    for (int j = 0; j < slots; ++j)
+      for (int i = 0; i < St::NB; ++i)
+        for (int r = 0; r < St::R; ++r) {
+          const int idx = r16_in_index<N, S>(j, i, r);
+          v[j][i * St::R + r] = S == 0 ? c2(in[2 * idx], in[2 * idx + 1]) : buf[spad16(idx)];
+        }
+    for (int j = 0; j < slots; ++j) {
+      float2 u[16];
+      for (int q = 0; q < 16; ++q) u[q] = v[j][q];
+      if (St::LAST) {
+        r16_compute<DIR, N, S>(u, j, tw, 1, [&](int idx, float2 x) {
+          out[2 * idx] = x.x;
+          out[2 * idx + 1] = x.y;
+        });
+      } else {
+        r16_compute<DIR, N, S>(u, j, tw, 1, [&](int idx, float2 x) { buf[spad16(idx)] = x; });
+      }
+    }
+    r16_host_stage<DIR, N, S + 1>(buf, in, out, tw);
+  }
+}
+
+template <int N>
+static int r16_host(const float* in, float* out, int dir) {
+  std::vector<float2> tw = make_table(N);
+  std::vector<float2> buf(spad16_len(N));
+  if (dir < 0) r16_host_stage<-1, N, 0>(buf, in, out, tw.data());
+  else r16_host_stage<1, N, 0>(buf, in, out, tw.data());
+  return 0;
+}
+
+extern "C" int shim_cfft_r16(const float* in, float* out, int n, int dir) {
+  switch (n) {
+    case 128: return r16_host<128>(in, out, dir);
+    case 256: return r16_host<256>(in, out, dir);
+    case 512: return r16_host<512>(in, out, dir);
+    case 1024: return r16_host<1024>(in, out, dir);
+    case 2048: return r16_host<2048>(in, out, dir);
+    case 4096: return r16_host<4096>(in, out, dir);
+    default: return -1;
+  }
+}

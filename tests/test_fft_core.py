@@ -65,3 +65,17 @@ def test_real_fft_pair_helpers(shim, w):
     assert shim.shim_irfft_pairs(fp(Y), fp(y), w) == 0
     refy = np.fft.irfft(Y.astype(np.complex128), w) * w
     assert np.abs(y - refy).max() / np.abs(refy).max() < 2e-6
+
+
+@pytest.mark.parametrize("n", [128, 256, 512, 1024, 2048, 4096])
+@pytest.mark.parametrize("direction", [-1, 1])
+def test_radix16_register_fft(shim, n, direction):
+    """The radix-16 register FFT (fft_r16.cuh: 16,16,..,RL plan, spad16
+    layout, product-tree twiddles), run thread by thread in barrier order,
+    against numpy."""
+    rng = np.random.default_rng(n)
+    x = (rng.standard_normal(n) + 1j * rng.standard_normal(n)).astype(np.complex64)
+    out = np.zeros(n, np.complex64)
+    assert shim.shim_cfft_r16(fp(x), fp(out), n, direction) == 0
+    ref = np.fft.fft(x.astype(np.complex128)) if direction < 0 else np.fft.ifft(x.astype(np.complex128)) * n
+    assert np.abs(out - ref).max() < 2e-6 * np.abs(ref).max()
