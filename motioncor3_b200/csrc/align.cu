@@ -7,6 +7,7 @@
 // (Align/CAlignStack.cpp:118-192, Align/GCorrelateSum2D.cu:108-140,
 // Align/CPeak2D.cpp:39-109).
 #include "kernels.cuh"
+#include "fft_r16.cuh"
 
 namespace mc3 {
 
@@ -295,6 +296,57 @@ __global__ void __launch_bounds__(kCtThreads, 2) k_corr_cols_ct(
   }
 }
 
+// Radix-16 register variant (fft_r16.cuh): corr_value feeds the first
+// stage directly and the last stage stores only the kept window rows.
+template <int H>
+__global__ void __launch_bounds__(512, 2) k_corr_cols_r16(
+    const float2* __restrict__ spec, const int* act, const float2* __restrict__ ex,
+    const float2* __restrict__ ey, const float2* __restrict__ S, const int* gstart,
+    const int* gsize, float bf, int phase_only, float2* T, int cmpX, int N, long sstride, int G,
+    int seaY, const float2* __restrict__ tw) {
+  constexpr int NB = 512 / (H / 16);
+  constexpr int LD = spad16_len(H);
+  extern __shared__ float2 sm[];
+  const int a = blockIdx.z;
+  const int g = blockIdx.y;
+  const int c = threadIdx.x % NB;
+  const int j = threadIdx.x / NB;
+  const int x = blockIdx.x * NB + c;
+  const bool live = x < cmpX;
+  const long nel = (long)cmpX * H;
+  const float2* X = spec + (long)act[a] * sstride;
+  const float2* Sa = S + (long)a * nel;
+  const int f0 = gstart[g], gs = gsize[g];
+  const float fFilt0 = -0.25f * bf / ((unsigned)(cmpX - 1) * (unsigned)H);
+  const int y0 = (H - seaY) / 2;
+  float2* Tg = T + ((long)a * G + g) * seaY * cmpX + x;
+  auto load = [&](int y) {
+    return live ? corr_value(X, ex, ey, Sa, a, N, f0, gs, x, y, cmpX, H, nel, fFilt0, phase_only)
+                : c2(0.f, 0.f);
+  };
+  auto store = [&](int y, float2 v) {
+    const int yi = y - y0;
+    if (live && yi >= 0 && yi < seaY) Tg[(long)yi * cmpX] = v;
+  };
+  fft_r16<1, H, false, false>(sm + c * LD, j, tw, 1, load, store);
+}
+
+template <int H>
+int launch_corr_cols_r16(const float2* spec, const int* act, const float2* ex, const float2* ey,
+                         const float2* S, const int* gstart, const int* gsize, float bfactor,
+                         int phase_only, float2* T, const AlignDims& d, const float2* tw,
+                         cudaStream_t st) {
+  constexpr int NB = 512 / (H / 16);
+  const size_t smem = (size_t)NB * spad16_len(H) * sizeof(float2);
+  MC3_TRY(set_smem_attr(k_corr_cols_r16<H>, smem));
+  dim3 grid(ceil_div(d.cmpX, NB), d.G, d.A);
+  k_corr_cols_r16<H><<<grid, 512, smem, st>>>(spec, act, ex, ey, S, gstart, gsize, bfactor,
+                                              phase_only, T, d.cmpX, d.N, d.stack_stride, d.G,
+                                              d.seaY, tw);
+  MC3_CHECK_LAUNCH("k_corr_cols_r16");
+  return kOk;
+}
+
 template <int H>
 int launch_corr_cols_ct(const float2* spec, const int* act, const float2* ex, const float2* ey,
                         const float2* S, const int* gstart, const int* gsize, float bfactor,
@@ -317,6 +369,24 @@ int corr_cols(const float2* spec, const int* act, const float2* ex, const float2
               int phase_only, float2* T, const AlignDims& d, cudaStream_t st) {
   FftDesc dH;
   MC3_TRY(make_desc(d.cmpY, d.cmpY, &dH));
+  if (r16_enabled() && !getenv("MC3_FFT_PINGPONG") && !getenv("MC3_FFT_RUNTIME_PLAN")) {
+    const double bytes = (double)d.A * ((double)d.cmpX * d.cmpY * 8.0 * (d.N + 1) + (double)d.G * d.seaY * d.cmpX * 8.0);
+    switch (d.cmpY) {
+      case 1024: {
+        prof::Scope ps("k_corr_cols_r16<1024>", bytes, st);
+        return launch_corr_cols_r16<1024>(spec, act, ex, ey, S, gstart, gsize, bfactor, phase_only, T, d, dH.tw, st);
+      }
+      case 2048: {
+        prof::Scope ps("k_corr_cols_r16<2048>", bytes, st);
+        return launch_corr_cols_r16<2048>(spec, act, ex, ey, S, gstart, gsize, bfactor, phase_only, T, d, dH.tw, st);
+      }
+      case 4096: {
+        prof::Scope ps("k_corr_cols_r16<4096>", bytes, st);
+        return launch_corr_cols_r16<4096>(spec, act, ex, ey, S, gstart, gsize, bfactor, phase_only, T, d, dH.tw, st);
+      }
+      default: break;
+    }
+  }
   if (all_dedicated(dH) && !getenv("MC3_FFT_PINGPONG") && !getenv("MC3_FFT_RUNTIME_PLAN")) {
     prof::Scope ps("k_corr_cols_ct", (double)d.A * ((double)d.cmpX * d.cmpY * 8.0 * (d.N + 1) + (double)d.G * d.seaY * d.cmpX * 8.0), st);
     switch (d.cmpY) {
