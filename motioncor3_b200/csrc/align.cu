@@ -85,33 +85,50 @@ int phase_apply(const float2* in, float2* out, int cmpX, int cmpY, const float2*
 // Aligned sum (Align/CAlignedSum.cpp:69-126): frames alternate between two
 // partial sums (even and odd frame index) that are added at the end.
 // ---------------------------------------------------------------------
-__global__ void k_aligned_sum(const float2* __restrict__ spec, const int* act,
-                              const float2* __restrict__ ex, const float2* __restrict__ ey,
-                              float2* S, int cmpX, int cmpY, int N, long sstride) {
+// Thread (kx, 4 consecutive rows): each frame's x phase factor is read once
+// for the 4 rows; the y factors are uniform over the warp (one row).
+constexpr int kAsRows = 4;
+__global__ void __launch_bounds__(128) k_aligned_sum(const float2* __restrict__ spec,
+                                                     const int* act,
+                                                     const float2* __restrict__ ex,
+                                                     const float2* __restrict__ ey, float2* S,
+                                                     int cmpX, int cmpY, int N, long sstride) {
   const long nel = (long)cmpX * cmpY;
-  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nel) return;
-  const int a = blockIdx.y;
-  const int kx = (int)(k % cmpX), ky = (int)(k / cmpX);
-  const float2* X = spec + (long)act[a] * sstride + k;
-  float2 e0 = c2(0.f, 0.f), e1 = c2(0.f, 0.f);
-#pragma unroll 4
+  const int kx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (kx >= cmpX) return;
+  const int ky0 = blockIdx.y * kAsRows;
+  const int a = blockIdx.z;
+  const float2* X = spec + (long)act[a] * sstride;
+  float2 e0[kAsRows], e1[kAsRows];
+#pragma unroll
+  for (int i = 0; i < kAsRows; ++i) e0[i] = e1[i] = c2(0.f, 0.f);
+#pragma unroll 2
   for (int f = 0; f < N; ++f) {
     const long t = (long)a * N + f;
-    const float2 e = cmul(ex[t * cmpX + kx], ey[t * cmpY + ky]);
-    const float2 v = rot(X[(long)f * nel], e);
-    if (f & 1) e1 = cadd(e1, v);
-    else e0 = cadd(e0, v);
+    const float2 exf = ex[t * cmpX + kx];
+#pragma unroll
+    for (int i = 0; i < kAsRows; ++i) {
+      const int ky = ky0 + i;
+      if (ky >= cmpY) break;
+      const float2 e = cmul(exf, ey[t * cmpY + ky]);
+      const float2 v = rot(X[(long)f * nel + (long)ky * cmpX + kx], e);
+      if (f & 1) e1[i] = cadd(e1[i], v);
+      else e0[i] = cadd(e0[i], v);
+    }
   }
-  S[(long)a * nel + k] = cadd(e0, e1);
+#pragma unroll
+  for (int i = 0; i < kAsRows; ++i) {
+    const int ky = ky0 + i;
+    if (ky < cmpY) S[(long)a * nel + (long)ky * cmpX + kx] = cadd(e0[i], e1[i]);
+  }
 }
 
 int aligned_sum(const float2* spec, const int* act, const float2* ex, const float2* ey, float2* S,
                 const AlignDims& d, cudaStream_t st) {
   const long nel = (long)d.cmpX * d.cmpY;
-  dim3 grid((unsigned)((nel + 255) / 256), d.A);
+  dim3 grid(ceil_div(d.cmpX, 128), ceil_div(d.cmpY, kAsRows), d.A);
   prof::Scope ps("k_aligned_sum", (double)d.A * nel * 8.0 * (d.N + 1), st);
-  k_aligned_sum<<<grid, 256, 0, st>>>(spec, act, ex, ey, S, d.cmpX, d.cmpY, d.N, d.stack_stride);
+  k_aligned_sum<<<grid, 128, 0, st>>>(spec, act, ex, ey, S, d.cmpX, d.cmpY, d.N, d.stack_stride);
   MC3_CHECK_LAUNCH("k_aligned_sum");
   return kOk;
 }
