@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <math.h>
 
@@ -98,6 +99,9 @@ Engine::Engine(const mc3_params& p) : prm(p) { device = p.gpu; }
 Engine::~Engine() {
   if (device >= 0) cudaSetDevice(device);
   if (copy_stream) cudaStreamSynchronize(copy_stream);
+  if (copy_stream2) cudaStreamSynchronize(copy_stream2);
+  if (half_done) cudaEventDestroy(half_done);
+  if (copy_stream2) cudaStreamDestroy(copy_stream2);
   for (int i = 0; i < 2; ++i) {
     if (slot_loaded[i]) cudaEventDestroy(slot_loaded[i]);
     if (slot_free[i]) cudaEventDestroy(slot_free[i]);
@@ -112,6 +116,8 @@ int Engine::init() {
   MC3_CUDA(cudaSetDevice(device));
   MC3_CUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
   MC3_CUDA(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
+  MC3_CUDA(cudaStreamCreateWithFlags(&copy_stream2, cudaStreamNonBlocking));
+  MC3_CUDA(cudaEventCreateWithFlags(&half_done, cudaEventDisableTiming));
   stream = own_stream;
   MC3_CUDA(cudaEventCreate(&ev0));
   MC3_CUDA(cudaEventCreate(&ev1));
@@ -156,7 +162,24 @@ int Engine::prefetch(const mc3_movie& mv) {
     MC3_TRY(d_rawslot[slot].ensure(bytes));
   }
   MC3_CUDA(cudaStreamWaitEvent(copy_stream, slot_free[slot], 0));
-  MC3_CUDA(cudaMemcpyAsync(d_rawslot[slot].p, mv.frames, bytes, cudaMemcpyHostToDevice, copy_stream));
+  // MC3_H2D_SPLIT=1 copies in two halves on two streams (A/B runs: whether
+  // two copy engines move more than one over the host link).
+  static const bool split = [] {
+    const char* e = getenv("MC3_H2D_SPLIT");
+    return e && e[0] == '1';
+  }();
+  if (split && bytes >= (size_t)1 << 24) {
+    const size_t h = bytes / 2 / 256 * 256;
+    MC3_CUDA(cudaStreamWaitEvent(copy_stream2, slot_free[slot], 0));
+    MC3_CUDA(cudaMemcpyAsync(d_rawslot[slot].p, mv.frames, h, cudaMemcpyHostToDevice, copy_stream));
+    MC3_CUDA(cudaMemcpyAsync(static_cast<char*>(d_rawslot[slot].p) + h,
+                             static_cast<const char*>(mv.frames) + h, bytes - h,
+                             cudaMemcpyHostToDevice, copy_stream2));
+    MC3_CUDA(cudaEventRecord(half_done, copy_stream2));
+    MC3_CUDA(cudaStreamWaitEvent(copy_stream, half_done, 0));
+  } else {
+    MC3_CUDA(cudaMemcpyAsync(d_rawslot[slot].p, mv.frames, bytes, cudaMemcpyHostToDevice, copy_stream));
+  }
   MC3_CUDA(cudaEventRecord(slot_loaded[slot], copy_stream));
   pending[n_pending++] = Pending{mv.frames, bytes, slot};
   next_slot ^= 1;

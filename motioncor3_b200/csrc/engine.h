@@ -74,6 +74,8 @@ class Engine {
     int slot;
   };
   cudaStream_t copy_stream = nullptr;
+  cudaStream_t copy_stream2 = nullptr;  // second half of a split copy
+  cudaEvent_t half_done = nullptr;
   cudaEvent_t slot_loaded[2] = {nullptr, nullptr};  // copy into the slot finished
   cudaEvent_t slot_free[2] = {nullptr, nullptr};    // last read of the slot finished
   DevBuf d_rawslot[2];
