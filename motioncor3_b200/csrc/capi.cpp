@@ -221,7 +221,7 @@ int mc3_local_gather(const float* in, float* out, int nx, int ny, const float* c
   if (!in || !out || !centers || !shifts || n_patches < 1) return MC3_EINVAL;
   const long pad = 2 * (nx / 2 + 1);
   return local_gather(in, pad * ny, out, pad * ny, 1, nx, ny, centers,
-                      reinterpret_cast<const float2*>(shifts), nullptr, bad, n_patches,
+                      reinterpret_cast<const float2*>(shifts), nullptr, bad, nullptr, n_patches,
                       as_stream(stream));
 }
 

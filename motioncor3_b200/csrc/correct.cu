@@ -134,11 +134,37 @@ int frame_sums(const float2* spec, long fr_stride, int N, int cmpX, int cmpY, co
 // frame); the accumulation runs in patch order exactly as the reference's,
 // as predicated adds rather than branches.
 // EXACT: P == PMAX; otherwise P < PMAX and reads are clamped to patch P-1.
+// Shift = weighted sums / weight total, int-truncated source, fold of
+// out-of-range sources, copy (the tail of mGCorrect3D).
+__device__ __forceinline__ void gather_store(const float* __restrict__ in, long in_stride,
+                                             float* out, long out_stride, int W, int H, int padX,
+                                             int f, int x, int y, float sx, float sy, float fW) {
+  if (x >= W) return;
+  if (fW > 0) {
+    sx = sx / fW;
+    sy = sy / fW;
+  }
+  int ix = (int)(((float)(unsigned)x - sx) * 1);
+  int iy = (int)((y - sy) * 1);
+  if (ix < 0 || iy < 0 || ix >= W || iy >= H) {
+    ix = (ix < 0) ? -ix : ix;
+    iy = (iy < 0) ? -iy : iy;
+    ix = (811 * ix) % W;
+    iy = (811 * iy) % H;
+    // Only non-finite shifts reach here out of range (the int conversion
+    // of NaN/inf); keep the read inside the frame.
+    if (ix < 0 || ix >= W) ix = 0;
+    if (iy < 0 || iy >= H) iy = 0;
+  }
+  out[(long)f * out_stride + (long)y * padX + x] = in[(long)f * in_stride + (long)iy * padX + ix];
+}
+
 template <int PMAX, bool EXACT, int PX>
 __global__ void __launch_bounds__(128) k_local_gather(
     const float* __restrict__ in, long in_stride, float* out, long out_stride, int W, int H,
     const float* __restrict__ cent, const float2* __restrict__ sh,
-    const unsigned long long* __restrict__ masks, const uint8_t* __restrict__ bad, int P, int nb) {
+    const unsigned long long* __restrict__ masks, const uint8_t* __restrict__ bad,
+    const uint8_t* __restrict__ clean, int P, int nb) {
   // PX pixels per thread, 128 apart in the row: each patch shift read
   // (uniform over the warp) serves PX pixels.
   const int y = blockIdx.y;
@@ -164,10 +190,42 @@ __global__ void __launch_bounds__(128) k_local_gather(
       }
     }
   }
+  // Sum of the included weights in patch order: the weight total of every
+  // frame without bad patches (same additions, same order, same bits).
+  float wsum[PX];
+#pragma unroll
+  for (int q = 0; q < PX; ++q) {
+    wsum[q] = 0.0f;
+#pragma unroll
+    for (int p = 0; p < PMAX; ++p)
+      if ((inc[q] >> p) & 1ull) wsum[q] += w[q][p];
+  }
   if (xb >= W) return;
   const int padX = (W / 2 + 1) * 2;
   for (int f = 0; f < nb; ++f) {
     const float2* s = sh + (long)f * P;
+    if (clean && clean[f]) {
+      // Frame without bad patches and with finite shifts: the excluded
+      // patches carry weight 0, and adding 0 * s (s finite) leaves the sums
+      // unchanged, so every patch is accumulated without a test.
+      float fSx[PX], fSy[PX];
+#pragma unroll
+      for (int q = 0; q < PX; ++q) fSx[q] = fSy[q] = 0.0f;
+#pragma unroll
+      for (int p = 0; p < PMAX; ++p) {
+        const float2 sp = s[EXACT ? p : (p < P ? p : P - 1)];
+#pragma unroll
+        for (int q = 0; q < PX; ++q) {
+          fSx[q] += sp.x * w[q][p];
+          fSy[q] += sp.y * w[q][p];
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < PX; ++q)
+        gather_store(in, in_stride, out, out_stride, W, H, padX, f, xb + 128 * q, y, fSx[q],
+                     fSy[q], wsum[q]);
+      continue;
+    }
     unsigned long long m = 0ull;
     if (masks) {
       m = masks[f];
@@ -194,28 +252,9 @@ __global__ void __launch_bounds__(128) k_local_gather(
       }
     }
 #pragma unroll
-    for (int q = 0; q < PX; ++q) {
-      const int x = xb + 128 * q;
-      if (x >= W) continue;
-      float sx = fSx[q], sy = fSy[q];
-      if (fW[q] > 0) {
-        sx = sx / fW[q];
-        sy = sy / fW[q];
-      }
-      int ix = (int)(((float)(unsigned)x - sx) * 1);
-      int iy = (int)((y - sy) * 1);
-      if (ix < 0 || iy < 0 || ix >= W || iy >= H) {
-        ix = (ix < 0) ? -ix : ix;
-        iy = (iy < 0) ? -iy : iy;
-        ix = (811 * ix) % W;
-        iy = (811 * iy) % H;
-        // Only non-finite shifts reach here out of range (the int conversion
-        // of NaN/inf); keep the read inside the frame.
-        if (ix < 0 || ix >= W) ix = 0;
-        if (iy < 0 || iy >= H) iy = 0;
-      }
-      out[(long)f * out_stride + (long)y * padX + x] = in[(long)f * in_stride + (long)iy * padX + ix];
-    }
+    for (int q = 0; q < PX; ++q)
+      gather_store(in, in_stride, out, out_stride, W, H, padX, f, xb + 128 * q, y, fSx[q], fSy[q],
+                   fW[q]);
   }
 }
 
@@ -223,21 +262,22 @@ template <int PMAX, bool EXACT>
 static void launch_gather(int W, int H, cudaStream_t st, const float* in, long in_stride,
                           float* out, long out_stride, const float* centers,
                           const float2* shifts, const unsigned long long* masks,
-                          const uint8_t* bad, int P, int nb) {
+                          const uint8_t* bad, const uint8_t* clean, int P, int nb) {
   constexpr int PX = PMAX <= 36 ? 2 : 1;
   dim3 grid(ceil_div(W, 128 * PX), H);
   k_local_gather<PMAX, EXACT, PX><<<grid, 128, 0, st>>>(in, in_stride, out, out_stride, W, H,
-                                                        centers, shifts, masks, bad, P, nb);
+                                                        centers, shifts, masks, bad, clean, P, nb);
 }
 
 int local_gather(const float* in, long in_stride, float* out, long out_stride, int nb, int W,
                  int H, const float* centers, const float2* shifts,
-                 const unsigned long long* masks, const uint8_t* bad, int P, cudaStream_t st) {
-  // `shifts`/`masks`/`bad` point at the first frame of the batch.
+                 const unsigned long long* masks, const uint8_t* bad, const uint8_t* clean,
+                 int P, cudaStream_t st) {
+  // `shifts`/`masks`/`bad`/`clean` point at the first frame of the batch.
   if (P < 1 || P > 64) return kEUnsupported;
   prof::Scope ps("k_local_gather", (double)nb * W * H * 8.0, st);
 #define MC3_GATHER(PM, EX) \
-  launch_gather<PM, EX>(W, H, st, in, in_stride, out, out_stride, centers, shifts, masks, bad, P, nb)
+  launch_gather<PM, EX>(W, H, st, in, in_stride, out, out_stride, centers, shifts, masks, bad, clean, P, nb)
   switch (P) {
     case 4: MC3_GATHER(4, true); break;
     case 9: MC3_GATHER(9, true); break;
@@ -257,18 +297,27 @@ int local_gather(const float* in, long in_stride, float* out, long out_stride, i
   return kOk;
 }
 
-// Per-frame 64-bit masks of the bad-patch flags [nb][P] (bit p = patch p).
-__global__ void k_patch_masks(const uint8_t* bad, int P, int nb, unsigned long long* masks) {
+// Per-frame 64-bit masks of the bad-patch flags [nb][P] (bit p = patch p),
+// and clean[f] = 1 when frame f has no bad patch and only finite shifts.
+__global__ void k_patch_masks(const uint8_t* bad, const float2* sh, int P, int nb,
+                              unsigned long long* masks, uint8_t* clean) {
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= nb) return;
   unsigned long long m = 0ull;
-  for (int p = 0; p < P; ++p) m |= (unsigned long long)(bad[(long)f * P + p] != 0) << p;
+  bool finite = true;
+  for (int p = 0; p < P; ++p) {
+    m |= (unsigned long long)(bad[(long)f * P + p] != 0) << p;
+    const float2 s = sh[(long)f * P + p];
+    finite = finite && isfinite(s.x) && isfinite(s.y);
+  }
   masks[f] = m;
+  clean[f] = (m == 0ull && finite) ? 1 : 0;
 }
 
-int patch_masks(const uint8_t* bad, int P, int nb, unsigned long long* masks, cudaStream_t st) {
+int patch_masks(const uint8_t* bad, const float2* shifts, int P, int nb,
+                unsigned long long* masks, uint8_t* clean, cudaStream_t st) {
   if (P < 1 || P > 64) return kEUnsupported;
-  k_patch_masks<<<ceil_div(nb, 128), 128, 0, st>>>(bad, P, nb, masks);
+  k_patch_masks<<<ceil_div(nb, 128), 128, 0, st>>>(bad, shifts, P, nb, masks, clean);
   MC3_CHECK_LAUNCH("k_patch_masks");
   return kOk;
 }

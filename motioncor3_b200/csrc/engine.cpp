@@ -597,11 +597,13 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
       MC3_TRY(col_fft(spec, spec, g.cmpX, g.cmpX, H, bi, inv, st));
       Batch br{N, N, (long)ncmp, nullptr, (long)ncmp * 2};
       MC3_TRY(row_c2r(spec, g.cmpX, frames, g.padX, W, H, br, st));
-      MC3_TRY(d_pmask.ensure(sizeof(unsigned long long) * N));
-      MC3_TRY(patch_masks(d_pbad.as<uint8_t>(), P, N, d_pmask.as<unsigned long long>(), st));
+      MC3_TRY(d_pmask.ensure(sizeof(unsigned long long) * N + N));
+      unsigned long long* masks = d_pmask.as<unsigned long long>();
+      uint8_t* clean = reinterpret_cast<uint8_t*>(masks + N);
+      MC3_TRY(patch_masks(d_pbad.as<uint8_t>(), d_pshift.as<float2>(), P, N, masks, clean, st));
       MC3_TRY(local_gather(frames, (long)ncmp * 2, d_gath.as<float>(), (long)ncmp * 2, N, W, H,
-                           d_pcent.as<float>(), d_pshift.as<float2>(),
-                           d_pmask.as<unsigned long long>(), nullptr, P, st));
+                           d_pcent.as<float>(), d_pshift.as<float2>(), masks, nullptr, clean, P,
+                           st));
       Batch bf{N, N, (long)ncmp * 2, nullptr, (long)ncmp};
       MC3_TRY(row_r2c(d_gath.as<float>(), g.padX, spec, g.cmpX, W, H, bf, 1.0f, st));
       ColOps fwd{};

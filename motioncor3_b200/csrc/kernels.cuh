@@ -71,11 +71,14 @@ int frame_sums(const float2* spec, long fr_stride, int N, int cmpX, int cmpY, co
                const float2* ey, const float* acc_dose, const float* Wn, const DoseParams& dp,
                float2* sums, int n_sums, cudaStream_t st);
 // mGCorrect3D per frame of a batch.  Bad patches come as per-frame 64-bit
-// masks (patch_masks) or, when masks is null, as [nb][P] flags.
+// masks (patch_masks) or, when masks is null, as [nb][P] flags; clean[f]
+// (optional) marks frames without bad patches and with finite shifts.
 int local_gather(const float* in, long in_stride, float* out, long out_stride, int nb, int W,
                  int H, const float* centers, const float2* shifts,
-                 const unsigned long long* masks, const uint8_t* bad, int P, cudaStream_t st);
-int patch_masks(const uint8_t* bad, int P, int nb, unsigned long long* masks, cudaStream_t st);
+                 const unsigned long long* masks, const uint8_t* bad, const uint8_t* clean,
+                 int P, cudaStream_t st);
+int patch_masks(const uint8_t* bad, const float2* shifts, int P, int nb,
+                unsigned long long* masks, uint8_t* clean, cudaStream_t st);
 // out[y*W+x] = max(0, in[y*pitch+x])
 int unpad_positive(const float* in, long pitch, float* out, int W, int H, int n,
                    long in_stride, cudaStream_t st);
