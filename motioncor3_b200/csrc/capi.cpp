@@ -372,6 +372,7 @@ int mc3_dose_weighted_sums(mc3_ctx* ctx, const float* spectra, int nx, int ny, i
   dp.sum_range[0] = e->prm.sum_range[0];
   dp.sum_range[1] = e->prm.sum_range[1];
   dp.split = e->prm.split_sum ? 1 : 0;
+  e->wn_valid = false;  // d_Wn is rebuilt here for this call's geometry
   if (g.dw && (s = dose_norm(e->d_acc.as<float>(), nz, g.cmpX, g.cmpY, dp.pix_size, dp.kv_factor,
                              e->d_Wn.as<float>(), st)))
     return s;

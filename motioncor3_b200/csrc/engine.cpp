@@ -568,7 +568,18 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
   dp.kv_factor = host::kv_factor(prm.kv);
   dp.sum_range[0] = prm.sum_range[0];
   dp.sum_range[1] = prm.sum_range[1];
-  if (g.dw) MC3_TRY(dose_norm(d_acc.as<float>(), N, g.cmpX, g.cmpY, dp.pix_size, dp.kv_factor, d_Wn.as<float>(), st));
+  if (g.dw) {
+    // The normalisation depends only on the geometry and the dose options,
+    // so it is rebuilt only when they change between movies.
+    const double key[6] = {(double)g.cmpX, (double)g.cmpY, (double)N, prm.fm_dose, dp.pix_size,
+                           dp.kv_factor};
+    if (!wn_valid || std::memcmp(key, wn_key, sizeof(key)) != 0 || d_Wn.cap < sizeof(float) * ncmp) {
+      MC3_TRY(dose_norm(d_acc.as<float>(), N, g.cmpX, g.cmpY, dp.pix_size, dp.kv_factor,
+                        d_Wn.as<float>(), st));
+      std::memcpy(wn_key, key, sizeof(key));
+      wn_valid = true;
+    }
+  }
   MC3_TRY(global_sums(spec, N, fs, g));
   if (!g.patch) {
     MC3_TRY(frame_sums(spec, (long)ncmp, N, g.cmpX, g.cmpY, d_fex.as<float2>(), d_fey.as<float2>(),

@@ -90,6 +90,8 @@ class Engine {
   DevBuf d_pat, d_patoff, d_bsum, d_bimg, d_btmp, d_bmap, d_scal;
   DevBuf d_fex, d_fey, d_Wn, d_acc, d_sums, d_real, d_gath, d_pcent, d_pshift, d_pbad, d_pmask, d_out, d_bsums;
   bool has_gain = false;
+  double wn_key[6] = {0, 0, 0, 0, 0, 0};  // geometry and dose options of d_Wn
+  bool wn_valid = false;
   int gain_w = 0, gain_h = 0;
 };
 
