@@ -322,7 +322,7 @@ __global__ void __launch_bounds__(512, 2) k_corr_cols_r16(
     const int* gsize, float bf, int phase_only, float2* T, int cmpX, int N, long sstride, int G,
     int seaY, const float2* __restrict__ tw) {
   constexpr int NB = 512 / (H / 16);
-  constexpr int LD = spad16_len(H);
+  constexpr int LD = spad16_col_stride(H, NB);
   extern __shared__ float2 sm[];
   const int a = blockIdx.z;
   const int g = blockIdx.y;
@@ -354,7 +354,7 @@ int launch_corr_cols_r16(const float2* spec, const int* act, const float2* ex, c
                          int phase_only, float2* T, const AlignDims& d, const float2* tw,
                          cudaStream_t st) {
   constexpr int NB = 512 / (H / 16);
-  const size_t smem = (size_t)NB * spad16_len(H) * sizeof(float2);
+  const size_t smem = (size_t)NB * spad16_col_stride(H, NB) * sizeof(float2);
   MC3_TRY(set_smem_attr(k_corr_cols_r16<H>, smem));
   dim3 grid(ceil_div(d.cmpX, NB), d.G, d.A);
   k_corr_cols_r16<H><<<grid, 512, smem, st>>>(spec, act, ex, ey, S, gstart, gsize, bfactor,

@@ -34,7 +34,7 @@ __global__ void __launch_bounds__(kR16Threads, 2) k_col_fft_r16(const float2* in
                                                                 const float2* __restrict__ tw,
                                                                 ColOps ops) {
   constexpr int NB = r16_batch(H);
-  constexpr int LD = spad16_len(H);
+  constexpr int LD = spad16_col_stride(H, NB);
   static_assert(NB * LD * (int)sizeof(float2) <= kR16Budget, "shared memory budget");
   extern __shared__ float2 sm[];
   const int item = blockIdx.y;
@@ -174,7 +174,7 @@ template <int H>
 int launch_col(const float2* in, float2* out, long pitch, int cmpX, const Batch& b,
                const float2* tw, const ColOps& ops, const char* name, cudaStream_t st) {
   constexpr int NB = r16_batch(H);
-  const size_t smem = (size_t)NB * spad16_len(H) * sizeof(float2);
+  const size_t smem = (size_t)NB * spad16_col_stride(H, NB) * sizeof(float2);
   MC3_TRY(set_smem_attr(k_col_fft_r16<H>, smem));
   dim3 grid(ceil_div(cmpX, NB), b.items);
   prof::Scope ps(name, (double)b.items * ((double)cmpX * H * 16.0 + (ops.crop ? (double)ops.crop_x * ops.crop_y * 8.0 : 0.0)), st);

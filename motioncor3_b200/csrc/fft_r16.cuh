@@ -26,6 +26,17 @@ namespace mc3 {
 
 MC3_HD int spad16(int i) { return i + (i >> 4); }
 MC3_HD constexpr int spad16_len(int n) { return n + (n >> 4) + 1; }
+// Stride between the NB column sequences of a column CTA (thread t ->
+// column t % NB): 64-bit shared accesses are served per half-warp, which
+// holds 16/NB slots of each of NB columns, so column c must start 16/NB
+// word pairs after column c-1 modulo the 16 bank pairs: stride = 16/NB
+// (mod 16), at least spad16_len(n).
+MC3_HD constexpr int spad16_col_stride(int n, int nb) {
+  const int want = nb >= 16 ? 1 : 16 / nb;
+  int ld = spad16_len(n);
+  while (ld % 16 != want % 16) ++ld;
+  return ld;
+}
 
 // Plan of N = 2^p: p/4 radix-16 stages, then one stage of radix 2^(p%4).
 MC3_HD constexpr int r16_nstages(int n) {
