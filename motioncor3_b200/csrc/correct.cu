@@ -3,6 +3,8 @@
 // Restates Correct/GWeightFrame.cu, Correct/CCorrectFullShift.cpp:271-334,
 // Correct/GCorrectPatchShift.cu:17-66 and the positivity/unpad steps of
 // CCorrectFullShift::mUnpadSums (:146-185).
+#include <cstdlib>
+
 #include "kernels.cuh"
 
 namespace mc3 {
@@ -263,10 +265,20 @@ static void launch_gather(int W, int H, cudaStream_t st, const float* in, long i
                           float* out, long out_stride, const float* centers,
                           const float2* shifts, const unsigned long long* masks,
                           const uint8_t* bad, const uint8_t* clean, int P, int nb) {
-  constexpr int PX = PMAX <= 36 ? 2 : 1;
-  dim3 grid(ceil_div(W, 128 * PX), H);
-  k_local_gather<PMAX, EXACT, PX><<<grid, 128, 0, st>>>(in, in_stride, out, out_stride, W, H,
-                                                        centers, shifts, masks, bad, clean, P, nb);
+  // two pixels per thread up to 36 patches; MC3_GATHER_PX=1 forces one (A/B runs)
+  static const bool one = [] {
+    const char* e = getenv("MC3_GATHER_PX");
+    return e && e[0] == '1';
+  }();
+  if (PMAX <= 36 && !one) {
+    dim3 grid(ceil_div(W, 256), H);
+    k_local_gather<PMAX, EXACT, 2><<<grid, 128, 0, st>>>(in, in_stride, out, out_stride, W, H,
+                                                         centers, shifts, masks, bad, clean, P, nb);
+  } else {
+    dim3 grid(ceil_div(W, 128), H);
+    k_local_gather<PMAX, EXACT, 1><<<grid, 128, 0, st>>>(in, in_stride, out, out_stride, W, H,
+                                                         centers, shifts, masks, bad, clean, P, nb);
+  }
 }
 
 int local_gather(const float* in, long in_stride, float* out, long out_stride, int nb, int W,
