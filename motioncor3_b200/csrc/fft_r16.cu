@@ -28,7 +28,9 @@ bool r16_enabled() {
 // Column pass: NB adjacent columns per CTA; thread t -> column t % NB,
 // slot t / NB, so a warp's loads cover NB adjacent columns of 32/NB rows.
 // ---------------------------------------------------------------------
-template <int H>
+// PHASE / CROP: the phase-shift prologue and the crop epilogue are compiled
+// in only where used.
+template <int H, bool PHASE, bool CROP>
 __global__ void __launch_bounds__(kR16Threads, 2) k_col_fft_r16(const float2* in, float2* out,
                                                                 long pitch, int cmpX, Batch bt,
                                                                 const float2* __restrict__ tw,
@@ -43,23 +45,22 @@ __global__ void __launch_bounds__(kR16Threads, 2) k_col_fft_r16(const float2* in
   const int x = blockIdx.x * NB + c;
   const bool live = x < cmpX;
   const float2* src = in + batch_in_off(bt, item) + x;
-  const float2* ex = ops.ex ? ops.ex + (long)item * cmpX : nullptr;
-  const float2* ey = ops.ey ? ops.ey + (long)item * H : nullptr;
-  const float2 exx = (ex && live) ? ex[x] : c2(1.f, 0.f);
+  const float2* ey = PHASE ? ops.ey + (long)item * H : nullptr;
+  const float2 exx = (PHASE && live) ? ops.ex[(long)item * cmpX + x] : c2(1.f, 0.f);
   float2* dst = out + (long)item * bt.out_stride + x;
-  float2* crop = ops.crop ? ops.crop + (long)item * ops.crop_x * ops.crop_y + x : nullptr;
-  const bool in_crop = crop && x < ops.crop_x;
+  float2* crop = CROP ? ops.crop + (long)item * ops.crop_x * ops.crop_y + x : nullptr;
+  const bool in_crop = CROP && x < ops.crop_x;
   auto load = [&](int y) {
     if (!live) return c2(0.f, 0.f);
     float2 v = src[(long)y * pitch];
-    if (ey) v = cmul(v, cmul(exx, ey[y]));
+    if constexpr (PHASE) v = cmul(v, cmul(exx, ey[y]));
     return v;
   };
   auto store = [&](int y, float2 v) {
     if (!live) return;
     v = cscale(v, ops.scale);
     dst[(long)y * pitch] = v;
-    if (in_crop) {
+    if (CROP && in_crop) {
       int yo = -1;
       if (y <= ops.crop_y / 2) yo = y;
       else if (y > H - ops.crop_y / 2) yo = y - H + ops.crop_y;
@@ -175,10 +176,19 @@ int launch_col(const float2* in, float2* out, long pitch, int cmpX, const Batch&
                const float2* tw, const ColOps& ops, const char* name, cudaStream_t st) {
   constexpr int NB = r16_batch(H);
   const size_t smem = (size_t)NB * spad16_col_stride(H, NB) * sizeof(float2);
-  MC3_TRY(set_smem_attr(k_col_fft_r16<H>, smem));
   dim3 grid(ceil_div(cmpX, NB), b.items);
   prof::Scope ps(name, (double)b.items * ((double)cmpX * H * 16.0 + (ops.crop ? (double)ops.crop_x * ops.crop_y * 8.0 : 0.0)), st);
-  k_col_fft_r16<H><<<grid, kR16Threads, smem, st>>>(in, out, pitch, cmpX, b, tw, ops);
+  const bool phase = ops.ex && ops.ey, crop = ops.crop != nullptr;
+#define MC3_COLK(P, C)                                                                   \
+  {                                                                                      \
+    MC3_TRY(set_smem_attr(k_col_fft_r16<H, P, C>, smem));                                \
+    k_col_fft_r16<H, P, C><<<grid, kR16Threads, smem, st>>>(in, out, pitch, cmpX, b, tw, ops); \
+  }
+  if (phase && crop) MC3_COLK(true, true)
+  else if (phase) MC3_COLK(true, false)
+  else if (crop) MC3_COLK(false, true)
+  else MC3_COLK(false, false)
+#undef MC3_COLK
   MC3_CHECK_LAUNCH(name);
   return kOk;
 }
