@@ -137,11 +137,10 @@ int frame_sums(const float2* spec, long fr_stride, int N, int cmpX, int cmpY, co
 // as predicated adds rather than branches.
 // EXACT: P == PMAX; otherwise P < PMAX and reads are clamped to patch P-1.
 // Shift = weighted sums / weight total, int-truncated source, fold of
-// out-of-range sources, copy (the tail of mGCorrect3D).
-__device__ __forceinline__ void gather_store(const float* __restrict__ in, long in_stride,
-                                             float* out, long out_stride, int W, int H, int padX,
-                                             int f, int x, int y, float sx, float sy, float fW) {
-  if (x >= W) return;
+// out-of-range sources (the tail of mGCorrect3D); returns the source offset
+// within the padded frame.
+__device__ __forceinline__ int gather_src(int W, int H, int padX, int x, int y, float sx, float sy,
+                                          float fW) {
   if (fW > 0) {
     sx = sx / fW;
     sy = sy / fW;
@@ -158,7 +157,7 @@ __device__ __forceinline__ void gather_store(const float* __restrict__ in, long 
     if (ix < 0 || ix >= W) ix = 0;
     if (iy < 0 || iy >= H) iy = 0;
   }
-  out[(long)f * out_stride + (long)y * padX + x] = in[(long)f * in_stride + (long)iy * padX + ix];
+  return iy * padX + ix;
 }
 
 template <int PMAX, bool EXACT, int PX>
@@ -204,59 +203,77 @@ __global__ void __launch_bounds__(128) k_local_gather(
   }
   if (xb >= W) return;
   const int padX = (W / 2 + 1) * 2;
-  for (int f = 0; f < nb; ++f) {
-    const float2* s = sh + (long)f * P;
-    if (clean && clean[f]) {
-      // Frame without bad patches and with finite shifts: the excluded
-      // patches carry weight 0, and adding 0 * s (s finite) leaves the sums
-      // unchanged, so every patch is accumulated without a test.
-      float fSx[PX], fSy[PX];
+  // Frames in groups of FB: the source offsets of the whole group are
+  // computed first, then its loads are issued together, then the stores.
+  constexpr int FB = 4;
+  for (int f0 = 0; f0 < nb; f0 += FB) {
+    int src[FB][PX];
 #pragma unroll
-      for (int q = 0; q < PX; ++q) fSx[q] = fSy[q] = 0.0f;
-#pragma unroll
-      for (int p = 0; p < PMAX; ++p) {
-        const float2 sp = s[EXACT ? p : (p < P ? p : P - 1)];
+    for (int b = 0; b < FB; ++b) {
+      const int f = f0 + b;
+      if (f >= nb) break;
+      const float2* s = sh + (long)f * P;
+      float fSx[PX], fSy[PX], fW[PX];
+      if (clean && clean[f]) {
+        // Frame without bad patches and with finite shifts: the excluded
+        // patches carry weight 0, and adding 0 * s (s finite) leaves the
+        // sums unchanged, so every patch is accumulated without a test.
 #pragma unroll
         for (int q = 0; q < PX; ++q) {
-          fSx[q] += sp.x * w[q][p];
-          fSy[q] += sp.y * w[q][p];
+          fSx[q] = fSy[q] = 0.0f;
+          fW[q] = wsum[q];
+        }
+#pragma unroll
+        for (int p = 0; p < PMAX; ++p) {
+          const float2 sp = s[EXACT ? p : (p < P ? p : P - 1)];
+#pragma unroll
+          for (int q = 0; q < PX; ++q) {
+            fSx[q] += sp.x * w[q][p];
+            fSy[q] += sp.y * w[q][p];
+          }
+        }
+      } else {
+        unsigned long long m = 0ull;
+        if (masks) {
+          m = masks[f];
+        } else if (bad) {
+          for (int p = 0; p < P; ++p) m |= (unsigned long long)(bad[(long)f * P + p] != 0) << p;
+        }
+        unsigned long long use[PX];
+#pragma unroll
+        for (int q = 0; q < PX; ++q) {
+          fSx[q] = fSy[q] = fW[q] = 0.0f;
+          use[q] = inc[q] & ~m;
+        }
+#pragma unroll
+        for (int p = 0; p < PMAX; ++p) {
+          const float2 sp = s[EXACT ? p : (p < P ? p : P - 1)];
+#pragma unroll
+          for (int q = 0; q < PX; ++q) {
+            if ((use[q] >> p) & 1ull) {
+              fW[q] += w[q][p];
+              fSx[q] += sp.x * w[q][p];
+              fSy[q] += sp.y * w[q][p];
+            }
+          }
         }
       }
 #pragma unroll
       for (int q = 0; q < PX; ++q)
-        gather_store(in, in_stride, out, out_stride, W, H, padX, f, xb + 128 * q, y, fSx[q],
-                     fSy[q], wsum[q]);
-      continue;
+        src[b][q] = gather_src(W, H, padX, xb + 128 * q, y, fSx[q], fSy[q], fW[q]);
     }
-    unsigned long long m = 0ull;
-    if (masks) {
-      m = masks[f];
-    } else if (bad) {
-      for (int p = 0; p < P; ++p) m |= (unsigned long long)(bad[(long)f * P + p] != 0) << p;
-    }
-    float fSx[PX], fSy[PX], fW[PX];
-    unsigned long long use[PX];
+    float v[FB][PX];
 #pragma unroll
-    for (int q = 0; q < PX; ++q) {
-      fSx[q] = fSy[q] = fW[q] = 0.0f;
-      use[q] = inc[q] & ~m;
-    }
+    for (int b = 0; b < FB; ++b)
 #pragma unroll
-    for (int p = 0; p < PMAX; ++p) {
-      const float2 sp = s[EXACT ? p : (p < P ? p : P - 1)];
+      for (int q = 0; q < PX; ++q)
+        if (f0 + b < nb && xb + 128 * q < W) v[b][q] = in[(long)(f0 + b) * in_stride + src[b][q]];
 #pragma unroll
-      for (int q = 0; q < PX; ++q) {
-        if ((use[q] >> p) & 1ull) {
-          fW[q] += w[q][p];
-          fSx[q] += sp.x * w[q][p];
-          fSy[q] += sp.y * w[q][p];
-        }
-      }
-    }
+    for (int b = 0; b < FB; ++b)
 #pragma unroll
-    for (int q = 0; q < PX; ++q)
-      gather_store(in, in_stride, out, out_stride, W, H, padX, f, xb + 128 * q, y, fSx[q], fSy[q],
-                   fW[q]);
+      for (int q = 0; q < PX; ++q)
+        if (f0 + b < nb && xb + 128 * q < W)
+          out[(long)(f0 + b) * out_stride + (long)y * padX + xb + 128 * q] = v[b][q];
   }
 }
 
@@ -265,12 +282,12 @@ static void launch_gather(int W, int H, cudaStream_t st, const float* in, long i
                           float* out, long out_stride, const float* centers,
                           const float2* shifts, const unsigned long long* masks,
                           const uint8_t* bad, const uint8_t* clean, int P, int nb) {
-  // two pixels per thread up to 36 patches; MC3_GATHER_PX=1 forces one (A/B runs)
-  static const bool one = [] {
+  // one pixel per thread; MC3_GATHER_PX=2 gives two (up to 36 patches, A/B runs)
+  static const bool two = [] {
     const char* e = getenv("MC3_GATHER_PX");
-    return e && e[0] == '1';
+    return e && e[0] == '2';
   }();
-  if (PMAX <= 36 && !one) {
+  if (PMAX <= 36 && two) {
     dim3 grid(ceil_div(W, 256), H);
     k_local_gather<PMAX, EXACT, 2><<<grid, 128, 0, st>>>(in, in_stride, out, out_stride, W, H,
                                                          centers, shifts, masks, bad, clean, P, nb);
