@@ -72,7 +72,7 @@ __global__ void k_frame_sums(const float2* __restrict__ spec, long fr_stride, in
   float2 so = c2(0.f, 0.f), se = c2(0.f, 0.f);
   const float wn = dp.enabled && k > 0 ? Wn[k] : 1.0f;
   const float cd = dp.enabled && k > 0 ? crit_dose(x, y, cmpX, cmpY, dp.kv_factor, dp.pix_size) : 1.0f;
-#pragma unroll 8
+#pragma unroll 4
   for (int f = 0; f < N; ++f) {
     float2 X = spec[(long)f * fr_stride + k];
     if (ex) {
