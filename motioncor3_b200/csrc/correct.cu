@@ -60,54 +60,95 @@ int dose_norm(const float* acc_dose, int N, int cmpX, int cmpY, float pix, float
 // untouched); sum1 += X; sum2 += X when the frame's accumulated dose lies in
 // the selected range; with -SplitSum the (weighted) X also goes to the
 // "_ODD" sum for even frame indices and to "_EVN" for odd ones.
+// Two neighbouring frequencies per thread (one 16-byte load per frame when
+// the layout allows it); the arithmetic of each frequency is unchanged.
+__device__ __forceinline__ void frame_sum_step(float2 X, int f, int k, int x, int y, int cmpX,
+                                               int cmpY, const float2* __restrict__ ex,
+                                               const float2* __restrict__ ey, const float* acc,
+                                               const DoseParams& dp, float cd, float wn,
+                                               float2& s0, float2& s1, float2& s2, float2& so,
+                                               float2& se) {
+  if (ex) {
+    const float2 e = cmul(ex[(long)f * cmpX + x], ey[(long)f * cmpY + y]);
+    X = c2(e.x * X.x - e.y * X.y, e.x * X.y + e.y * X.x);
+  }
+  s0 = cadd(X, s0);
+  if (dp.enabled) {
+    if (k > 0) {
+      float fW = dose_weight_c(cd, acc[f]);
+      fW = fW / wn;
+      X.x *= fW;
+      X.y *= fW;
+    }
+    s1 = cadd(X, s1);
+    if (dp.dws && acc[f] >= dp.sum_range[0] && acc[f] <= dp.sum_range[1]) s2 = cadd(X, s2);
+  }
+  if (dp.split) {
+    if (f % 2 == 0) so = cadd(X, so);
+    else se = cadd(X, se);
+  }
+}
+
 __global__ void k_frame_sums(const float2* __restrict__ spec, long fr_stride, int N, int cmpX,
                              int cmpY, const float2* __restrict__ ex, const float2* __restrict__ ey,
                              const float* acc, const float* Wn, DoseParams dp, float2* sums,
                              int n_sums) {
   const long n = (long)cmpX * cmpY;
-  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  const int x = (int)(k % cmpX), y = (int)(k / cmpX);
-  float2 s0 = c2(0.f, 0.f), s1 = c2(0.f, 0.f), s2 = c2(0.f, 0.f);
-  float2 so = c2(0.f, 0.f), se = c2(0.f, 0.f);
-  const float wn = dp.enabled && k > 0 ? Wn[k] : 1.0f;
-  const float cd = dp.enabled && k > 0 ? crit_dose(x, y, cmpX, cmpY, dp.kv_factor, dp.pix_size) : 1.0f;
+  const long k0 = 2 * ((long)blockIdx.x * blockDim.x + threadIdx.x);
+  if (k0 >= n) return;
+  const bool two = k0 + 1 < n;
+  const bool vec = two && !(fr_stride & 1) &&
+                   ((reinterpret_cast<uintptr_t>(spec) & 15) == 0);
+  int x[2], y[2];
+  float cd[2], wn[2];
+  float2 s0[2], s1[2], s2[2], so[2], se[2];
+#pragma unroll
+  for (int e = 0; e < 2; ++e) {
+    const long k = k0 + e;
+    x[e] = (int)(k % cmpX);
+    y[e] = (int)(k / cmpX);
+    const bool ok = k < n;
+    wn[e] = dp.enabled && k > 0 && ok ? Wn[k] : 1.0f;
+    cd[e] = dp.enabled && k > 0 && ok ? crit_dose(x[e], y[e], cmpX, cmpY, dp.kv_factor, dp.pix_size)
+                                      : 1.0f;
+    s0[e] = s1[e] = s2[e] = so[e] = se[e] = c2(0.f, 0.f);
+  }
 #pragma unroll 4
   for (int f = 0; f < N; ++f) {
-    float2 X = spec[(long)f * fr_stride + k];
-    if (ex) {
-      const float2 e = cmul(ex[(long)f * cmpX + x], ey[(long)f * cmpY + y]);
-      X = c2(e.x * X.x - e.y * X.y, e.x * X.y + e.y * X.x);
+    const float2* fr = spec + (long)f * fr_stride + k0;
+    float2 X0, X1 = c2(0.f, 0.f);
+    if (vec) {
+      const float4 q = *reinterpret_cast<const float4*>(fr);
+      X0 = c2(q.x, q.y);
+      X1 = c2(q.z, q.w);
+    } else {
+      X0 = fr[0];
+      if (two) X1 = fr[1];
     }
-    s0 = cadd(X, s0);
+    frame_sum_step(X0, f, (int)k0, x[0], y[0], cmpX, cmpY, ex, ey, acc, dp, cd[0], wn[0], s0[0],
+                   s1[0], s2[0], so[0], se[0]);
+    if (two)
+      frame_sum_step(X1, f, (int)k0 + 1, x[1], y[1], cmpX, cmpY, ex, ey, acc, dp, cd[1], wn[1],
+                     s0[1], s1[1], s2[1], so[1], se[1]);
+  }
+#pragma unroll
+  for (int e = 0; e < 2; ++e) {
+    const long k = k0 + e;
+    if (k >= n) break;
+    sums[k] = s0[e];
+    int next = 1;
     if (dp.enabled) {
-      if (k > 0) {
-        float fW = dose_weight_c(cd, acc[f]);
-        fW = fW / wn;
-        X.x *= fW;
-        X.y *= fW;
+      sums[n + k] = s1[e];
+      next = 2;
+      if (dp.dws) {
+        sums[2 * n + k] = s2[e];
+        next = 3;
       }
-      s1 = cadd(X, s1);
-      if (dp.dws && acc[f] >= dp.sum_range[0] && acc[f] <= dp.sum_range[1]) s2 = cadd(X, s2);
     }
     if (dp.split) {
-      if (f % 2 == 0) so = cadd(X, so);
-      else se = cadd(X, se);
+      sums[(long)next * n + k] = so[e];
+      sums[(long)(next + 1) * n + k] = se[e];
     }
-  }
-  sums[k] = s0;
-  int next = 1;
-  if (dp.enabled) {
-    sums[n + k] = s1;
-    next = 2;
-    if (dp.dws) {
-      sums[2 * n + k] = s2;
-      next = 3;
-    }
-  }
-  if (dp.split) {
-    sums[(long)next * n + k] = so;
-    sums[(long)(next + 1) * n + k] = se;
   }
 }
 
@@ -117,7 +158,7 @@ int frame_sums(const float2* spec, long fr_stride, int N, int cmpX, int cmpY, co
   const long n = (long)cmpX * cmpY;
   if (n_sums != 1 + (dp.enabled ? 1 + (dp.dws ? 1 : 0) : 0) + (dp.split ? 2 : 0)) return kEInval;
   prof::Scope ps("k_frame_sums", (double)n * (8.0 * (N + n_sums) + (dp.enabled ? 4.0 : 0.0)), st);
-  k_frame_sums<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(spec, fr_stride, N, cmpX, cmpY, ex, ey,
+  k_frame_sums<<<(unsigned)((n + 511) / 512), 256, 0, st>>>(spec, fr_stride, N, cmpX, cmpY, ex, ey,
                                                            acc_dose, Wn, dp, sums, n_sums);
   MC3_CHECK_LAUNCH("k_frame_sums");
   return kOk;
@@ -160,120 +201,171 @@ __device__ __forceinline__ int gather_src(int W, int H, int padX, int x, int y, 
   return iy * padX + ix;
 }
 
+// Two IEEE fp32 FMAs in one instruction (Blackwell packed f32x2): lane i
+// is fmaf(a_i, b_i, c_i), the same rounding as the scalar form.
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
+  unsigned long long ra, rb, rc, rd;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(ra) : "f"(a.x), "f"(a.y));
+  asm("mov.b64 %0, {%1, %2};" : "=l"(rb) : "f"(b.x), "f"(b.y));
+  asm("mov.b64 %0, {%1, %2};" : "=l"(rc) : "f"(c.x), "f"(c.y));
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(rd) : "l"(ra), "l"(rb), "l"(rc));
+  float2 d;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(d.x), "=f"(d.y) : "l"(rd));
+  return d;
+}
+
+// Per-pixel patch weights of mGCorrect3D: w = exp(-100 r) for patches with
+// r <= 0.6 (r = distance to the patch centre in units of the frame size),
+// bit p of the returned mask set for those patches; the others weigh 0.
+template <int PMAX, bool EXACT>
+__device__ __forceinline__ unsigned long long gather_weights(int x, int y, int W, int H,
+                                                             const float* __restrict__ cent, int P,
+                                                             float (&w)[PMAX]) {
+  const float fB = 100.0f;
+  unsigned long long inc = 0ull;
+#pragma unroll
+  for (int p = 0; p < PMAX; ++p) {
+    w[p] = 0.0f;
+    if (x < W && (EXACT || p < P)) {
+      float ax = ((float)(unsigned)x - cent[2 * p]) / (float)(unsigned)W;
+      float ay = (y - cent[2 * p + 1]) / H;
+      ax = sqrtf(ax * ax + ay * ay);
+      if (!(ax > 0.6f)) {
+        w[p] = expf(-fB * ax);
+        inc |= 1ull << p;
+      }
+    }
+  }
+  return inc;
+}
+
+// Local-motion gather (mGCorrect3D): every output pixel of every frame is
+// read from the frame at the pixel minus the weighted mean of the patch
+// shifts.  One CTA = one row segment; the patch shifts of a chunk of frames
+// are staged in shared memory as (sx, sx, sy, sy) so that one 16-byte read
+// serves a patch for both pixels of a thread.  PX = 2: the thread's pixels
+// are 128 apart in the row and their sums are carried as f32x2 pairs
+// (lane q = pixel q), so one packed FMA does the work of two.  PX = 1: one
+// pixel, scalar FMAs.  Frames whose patches are all good and whose shifts
+// are finite take the branch-free path (excluded patches weigh 0 and the
+// weight total is the precomputed sum of the included weights, added in
+// patch order); the others test every patch.
 template <int PMAX, bool EXACT, int PX>
 __global__ void __launch_bounds__(128) k_local_gather(
     const float* __restrict__ in, long in_stride, float* out, long out_stride, int W, int H,
     const float* __restrict__ cent, const float2* __restrict__ sh,
     const unsigned long long* __restrict__ masks, const uint8_t* __restrict__ bad,
     const uint8_t* __restrict__ clean, int P, int nb) {
-  // PX pixels per thread, 128 apart in the row: each patch shift read
-  // (uniform over the warp) serves PX pixels.
+  static_assert(PX == 1 || PX == 2, "one or two pixels per thread");
+  constexpr int FCH = 16;  // frames per shared-memory chunk
+  __shared__ float4 s_sh[FCH * PMAX];
+  __shared__ int s_clean[FCH];
   const int y = blockIdx.y;
   const int xb = blockIdx.x * (128 * PX) + threadIdx.x;
-  const float fB = 100.0f;
   float w[PX][PMAX];
-  unsigned long long inc[PX];  // patches within r <= 0.6 of each pixel
-#pragma unroll
-  for (int q = 0; q < PX; ++q) {
-    const int x = xb + 128 * q;
-    inc[q] = 0ull;
-#pragma unroll
-    for (int p = 0; p < PMAX; ++p) {
-      w[q][p] = 0.0f;
-      if (x < W && (EXACT || p < P)) {
-        float ax = ((float)(unsigned)x - cent[2 * p]) / (float)(unsigned)W;
-        float ay = (y - cent[2 * p + 1]) / H;
-        ax = sqrtf(ax * ax + ay * ay);
-        if (!(ax > 0.6f)) {
-          w[q][p] = expf(-fB * ax);
-          inc[q] |= 1ull << p;
-        }
-      }
-    }
-  }
-  // Sum of the included weights in patch order: the weight total of every
-  // frame without bad patches (same additions, same order, same bits).
+  unsigned long long inc[PX];
   float wsum[PX];
 #pragma unroll
   for (int q = 0; q < PX; ++q) {
+    inc[q] = gather_weights<PMAX, EXACT>(xb + 128 * q, y, W, H, cent, P, w[q]);
+    // weight total of a frame without bad patches (same additions, same order)
     wsum[q] = 0.0f;
 #pragma unroll
     for (int p = 0; p < PMAX; ++p)
       if ((inc[q] >> p) & 1ull) wsum[q] += w[q][p];
   }
-  if (xb >= W) return;
+  float2 wp[PMAX];  // (w of pixel 0, w of pixel 1) for the packed FMAs
+  if constexpr (PX == 2) {
+#pragma unroll
+    for (int p = 0; p < PMAX; ++p) wp[p] = make_float2(w[0][p], w[1][p]);
+  }
+  const bool act0 = xb < W;
   const int padX = (W / 2 + 1) * 2;
-  // Frames in groups of FB: the source offsets of the whole group are
-  // computed first, then its loads are issued together, then the stores.
-  constexpr int FB = 4;
-  for (int f0 = 0; f0 < nb; f0 += FB) {
-    int src[FB][PX];
+  for (int c0 = 0; c0 < nb; c0 += FCH) {
+    const int nc = min(FCH, nb - c0);
+    __syncthreads();  // the previous chunk's readers are done
+    for (int i = threadIdx.x; i < nc * PMAX; i += 128) {
+      const int f = i / PMAX, p = i - f * PMAX;
+      float2 v = make_float2(0.0f, 0.0f);  // patches p >= P weigh 0
+      if (EXACT || p < P) v = sh[(long)(c0 + f) * P + p];
+      s_sh[i] = make_float4(v.x, v.x, v.y, v.y);
+    }
+    if (threadIdx.x < nc) s_clean[threadIdx.x] = clean ? clean[c0 + threadIdx.x] : 0;
+    __syncthreads();
+    if (!act0) continue;
+    // Frames in groups of FB: source offsets, then loads, then stores.
+    constexpr int FB = 4;
+    for (int f0 = 0; f0 < nc; f0 += FB) {
+      int src[FB][PX];
 #pragma unroll
-    for (int b = 0; b < FB; ++b) {
-      const int f = f0 + b;
-      if (f >= nb) break;
-      const float2* s = sh + (long)f * P;
-      float fSx[PX], fSy[PX], fW[PX];
-      if (clean && clean[f]) {
-        // Frame without bad patches and with finite shifts: the excluded
-        // patches carry weight 0, and adding 0 * s (s finite) leaves the
-        // sums unchanged, so every patch is accumulated without a test.
+      for (int b = 0; b < FB; ++b) {
+        const int fl = f0 + b;
+        if (fl >= nc) break;
+        const float4* s = s_sh + fl * PMAX;
+        float fSx[PX], fSy[PX], fW[PX];
+        if (s_clean[fl]) {
+          if constexpr (PX == 2) {
+            float2 Sx = make_float2(0.0f, 0.0f), Sy = Sx;
 #pragma unroll
-        for (int q = 0; q < PX; ++q) {
-          fSx[q] = fSy[q] = 0.0f;
-          fW[q] = wsum[q];
-        }
+            for (int p = 0; p < PMAX; ++p) {
+              const float4 sp = s[p];
+              Sx = ffma2(make_float2(sp.x, sp.y), wp[p], Sx);
+              Sy = ffma2(make_float2(sp.z, sp.w), wp[p], Sy);
+            }
+            fSx[0] = Sx.x, fSx[1] = Sx.y, fSy[0] = Sy.x, fSy[1] = Sy.y;
+          } else {
+            fSx[0] = fSy[0] = 0.0f;
 #pragma unroll
-        for (int p = 0; p < PMAX; ++p) {
-          const float2 sp = s[EXACT ? p : (p < P ? p : P - 1)];
-#pragma unroll
-          for (int q = 0; q < PX; ++q) {
-            fSx[q] += sp.x * w[q][p];
-            fSy[q] += sp.y * w[q][p];
+            for (int p = 0; p < PMAX; ++p) {
+              const float4 sp = s[p];
+              fSx[0] += sp.x * w[0][p];
+              fSy[0] += sp.z * w[0][p];
+            }
           }
-        }
-      } else {
-        unsigned long long m = 0ull;
-        if (masks) {
-          m = masks[f];
-        } else if (bad) {
-          for (int p = 0; p < P; ++p) m |= (unsigned long long)(bad[(long)f * P + p] != 0) << p;
-        }
-        unsigned long long use[PX];
 #pragma unroll
-        for (int q = 0; q < PX; ++q) {
-          fSx[q] = fSy[q] = fW[q] = 0.0f;
-          use[q] = inc[q] & ~m;
-        }
-#pragma unroll
-        for (int p = 0; p < PMAX; ++p) {
-          const float2 sp = s[EXACT ? p : (p < P ? p : P - 1)];
+          for (int q = 0; q < PX; ++q) fW[q] = wsum[q];
+        } else {
+          const int f = c0 + fl;
+          unsigned long long m = 0ull;
+          if (masks) {
+            m = masks[f];
+          } else if (bad) {
+            for (int p = 0; p < P; ++p) m |= (unsigned long long)(bad[(long)f * P + p] != 0) << p;
+          }
 #pragma unroll
           for (int q = 0; q < PX; ++q) {
-            if ((use[q] >> p) & 1ull) {
-              fW[q] += w[q][p];
-              fSx[q] += sp.x * w[q][p];
-              fSy[q] += sp.y * w[q][p];
+            const unsigned long long use = inc[q] & ~m;
+            fSx[q] = fSy[q] = fW[q] = 0.0f;
+#pragma unroll
+            for (int p = 0; p < PMAX; ++p) {
+              if ((use >> p) & 1ull) {
+                const float4 sp = s[p];
+                const float wq = PX == 2 ? (q ? wp[p].y : wp[p].x) : w[0][p];
+                fW[q] += wq;
+                fSx[q] += sp.x * wq;
+                fSy[q] += sp.z * wq;
+              }
             }
           }
         }
+#pragma unroll
+        for (int q = 0; q < PX; ++q)
+          src[b][q] = gather_src(W, H, padX, xb + 128 * q, y, fSx[q], fSy[q], fW[q]);
       }
+      float v[FB][PX];
 #pragma unroll
-      for (int q = 0; q < PX; ++q)
-        src[b][q] = gather_src(W, H, padX, xb + 128 * q, y, fSx[q], fSy[q], fW[q]);
+      for (int b = 0; b < FB; ++b)
+#pragma unroll
+        for (int q = 0; q < PX; ++q)
+          if (f0 + b < nc && xb + 128 * q < W)
+            v[b][q] = in[(long)(c0 + f0 + b) * in_stride + src[b][q]];
+#pragma unroll
+      for (int b = 0; b < FB; ++b)
+#pragma unroll
+        for (int q = 0; q < PX; ++q)
+          if (f0 + b < nc && xb + 128 * q < W)
+            out[(long)(c0 + f0 + b) * out_stride + (long)y * padX + xb + 128 * q] = v[b][q];
     }
-    float v[FB][PX];
-#pragma unroll
-    for (int b = 0; b < FB; ++b)
-#pragma unroll
-      for (int q = 0; q < PX; ++q)
-        if (f0 + b < nb && xb + 128 * q < W) v[b][q] = in[(long)(f0 + b) * in_stride + src[b][q]];
-#pragma unroll
-    for (int b = 0; b < FB; ++b)
-#pragma unroll
-      for (int q = 0; q < PX; ++q)
-        if (f0 + b < nb && xb + 128 * q < W)
-          out[(long)(f0 + b) * out_stride + (long)y * padX + xb + 128 * q] = v[b][q];
   }
 }
 
@@ -282,12 +374,13 @@ static void launch_gather(int W, int H, cudaStream_t st, const float* in, long i
                           float* out, long out_stride, const float* centers,
                           const float2* shifts, const unsigned long long* masks,
                           const uint8_t* bad, const uint8_t* clean, int P, int nb) {
-  // one pixel per thread; MC3_GATHER_PX=2 gives two (up to 36 patches, A/B runs)
-  static const bool two = [] {
+  // two pixels per thread up to 36 patches (MC3_GATHER_PX=1 forces one,
+  // for A/B runs); one above (register budget of the weights)
+  static const bool one = [] {
     const char* e = getenv("MC3_GATHER_PX");
-    return e && e[0] == '2';
+    return e && e[0] == '1';
   }();
-  if (PMAX <= 36 && two) {
+  if (PMAX <= 36 && !one) {
     dim3 grid(ceil_div(W, 256), H);
     k_local_gather<PMAX, EXACT, 2><<<grid, 128, 0, st>>>(in, in_stride, out, out_stride, W, H,
                                                          centers, shifts, masks, bad, clean, P, nb);

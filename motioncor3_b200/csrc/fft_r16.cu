@@ -73,86 +73,6 @@ __global__ void __launch_bounds__(kR16Threads, 2) k_col_fft_r16(const float2* in
 }
 
 // ---------------------------------------------------------------------
-// Pipelined persistent column pass: one CTA per SM walks the column tiles
-// (NB columns x H rows of one item); while a tile is transformed, the next
-// tile is copied into the other half of a double buffer with cp.async
-// (8-byte copies: the complex rows of an odd-width spectrum are only 8-byte
-// aligned), so the DRAM traffic of a tile overlaps the compute of the
-// previous one instead of stalling the two resident CTAs.
-// ---------------------------------------------------------------------
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
-
-template <int H, bool PHASE, bool CROP>
-__global__ void __launch_bounds__(kR16Threads, 1) k_col_fft_r16p(const float2* in, float2* out,
-                                                                 long pitch, int cmpX, Batch bt,
-                                                                 const float2* __restrict__ tw,
-                                                                 ColOps ops, int tiles_x,
-                                                                 int ntiles) {
-  constexpr int NB = r16_batch(H);
-  constexpr int LD = spad16_col_stride(H, NB);
-  constexpr int TILE = NB * H;  // complex values of a raw tile, [y][c]
-  extern __shared__ float2 sm[];
-  float2* raw = sm;                // [2][TILE]
-  float2* xb = sm + 2 * TILE;      // [NB][LD] exchange buffer
-  const int c = threadIdx.x % NB;
-  const int j = threadIdx.x / NB;
-  auto prefetch = [&](int tile, int half) {
-    const int item = tile / tiles_x;
-    const int x0 = (tile - item * tiles_x) * NB;
-    const float2* src = in + batch_in_off(bt, item) + x0;
-    float2* dstb = raw + half * TILE;
-    for (int e = threadIdx.x; e < TILE; e += kR16Threads) {
-      const int y = e / NB, cc = e % NB;
-      if (x0 + cc < cmpX) cp_async8(dstb + e, src + (long)y * pitch + cc);
-      else dstb[e] = c2(0.f, 0.f);
-    }
-  };
-  int tile = blockIdx.x;
-  if (tile < ntiles) prefetch(tile, 0);
-  cp_async_commit();
-  for (int half = 0; tile < ntiles; tile += gridDim.x, half ^= 1) {
-    const int next = tile + gridDim.x;
-    if (next < ntiles) prefetch(next, half ^ 1);
-    cp_async_commit();
-    cp_async_wait1();   // this thread's copies of `tile` have landed
-    __syncthreads();    // everyone's have, and the previous tile is done
-    const int item = tile / tiles_x;
-    const int x = (tile - item * tiles_x) * NB + c;
-    const bool live = x < cmpX;
-    const float2* rb = raw + half * TILE;
-    const float2* ey = PHASE ? ops.ey + (long)item * H : nullptr;
-    const float2 exx = (PHASE && live) ? ops.ex[(long)item * cmpX + x] : c2(1.f, 0.f);
-    float2* dst = out + (long)item * bt.out_stride + x;
-    float2* crop = CROP ? ops.crop + (long)item * ops.crop_x * ops.crop_y + x : nullptr;
-    const bool in_crop = CROP && x < ops.crop_x;
-    auto load = [&](int y) {
-      float2 v = rb[y * NB + c];
-      if constexpr (PHASE) v = cmul(v, cmul(exx, ey[y]));
-      return v;
-    };
-    auto store = [&](int y, float2 v) {
-      if (!live) return;
-      v = cscale(v, ops.scale);
-      dst[(long)y * pitch] = v;
-      if (CROP && in_crop) {
-        int yo = -1;
-        if (y <= ops.crop_y / 2) yo = y;
-        else if (y > H - ops.crop_y / 2) yo = y - H + ops.crop_y;
-        if (yo >= 0) crop[(long)yo * ops.crop_x] = v;
-      }
-    };
-    if (ops.dir < 0) fft_r16<-1, H, false, false>(xb + c * LD, j, tw, 1, load, store);
-    else fft_r16<1, H, false, false>(xb + c * LD, j, tw, 1, load, store);
-    __syncthreads();    // xb and this raw half are free again
-  }
-}
-
-// ---------------------------------------------------------------------
 // Row R2C: ROWS rows per CTA, M = W/2 complex points per row (the real row
 // read as complex pairs), thread t -> row t / (M/16), slot t % (M/16).  The
 // transform ends in shared memory for the paired post-processing, then the
@@ -298,44 +218,6 @@ int launch_c2r(const float2* in, long in_pitch, float* out, long out_pitch, int 
 }
 }  // namespace
 
-namespace {
-// MC3_COL_PIPE=1 selects the pipelined persistent column pass (A/B runs).
-bool col_pipe() {
-  static const bool on = [] {
-    const char* e = getenv("MC3_COL_PIPE");
-    return e && e[0] == '1';
-  }();
-  return on;
-}
-template <int H>
-int launch_col_pipe(const float2* in, float2* out, long pitch, int cmpX, const Batch& b,
-                    const float2* tw, const ColOps& ops, const char* name, cudaStream_t st) {
-  constexpr int NB = r16_batch(H);
-  const size_t smem = (2 * (size_t)NB * H + (size_t)NB * spad16_col_stride(H, NB)) * sizeof(float2);
-  const int tiles_x = ceil_div(cmpX, NB);
-  const int ntiles = tiles_x * b.items;
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int grid = ntiles < sms ? ntiles : sms;
-  prof::Scope ps(name, (double)b.items * ((double)cmpX * H * 16.0 + (ops.crop ? (double)ops.crop_x * ops.crop_y * 8.0 : 0.0)), st);
-  const bool phase = ops.ex && ops.ey, crop = ops.crop != nullptr;
-#define MC3_COLP(P, C)                                                                        \
-  {                                                                                           \
-    MC3_TRY(set_smem_attr(k_col_fft_r16p<H, P, C>, smem));                                    \
-    k_col_fft_r16p<H, P, C><<<grid, kR16Threads, smem, st>>>(in, out, pitch, cmpX, b, tw, ops, \
-                                                             tiles_x, ntiles);                \
-  }
-  if (phase && crop) MC3_COLP(true, true)
-  else if (phase) MC3_COLP(true, false)
-  else if (crop) MC3_COLP(false, true)
-  else MC3_COLP(false, false)
-#undef MC3_COLP
-  MC3_CHECK_LAUNCH(name);
-  return kOk;
-}
-}  // namespace
-
 int col_fft_r16(const float2* in, float2* out, long pitch, int cmpX, int H, const Batch& b,
                 const ColOps& ops, cudaStream_t st) {
   if (!r16_enabled()) return kEUnsupported;
@@ -345,10 +227,6 @@ int col_fft_r16(const float2* in, float2* out, long pitch, int cmpX, int H, cons
     default: return kEUnsupported;
   }
   MC3_TRY(make_desc(H, H, &d));
-  if (col_pipe() && H == 4096)
-    return launch_col_pipe<4096>(in, out, pitch, cmpX, b, d.tw, ops, "k_col_fft_r16p<4096>", st);
-  if (col_pipe() && H == 2048)
-    return launch_col_pipe<2048>(in, out, pitch, cmpX, b, d.tw, ops, "k_col_fft_r16p<2048>", st);
   switch (H) {
     case 256: return launch_col<256>(in, out, pitch, cmpX, b, d.tw, ops, "k_col_fft_r16<256>", st);
     case 512: return launch_col<512>(in, out, pitch, cmpX, b, d.tw, ops, "k_col_fft_r16<512>", st);
