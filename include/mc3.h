@@ -55,6 +55,9 @@ typedef struct {
                           reference's CProcessThread.cpp:94-99 always runs)    */
   int gpu;             /* CUDA device ordinal (-Gpu first entry)               */
   int split_sum;       /* -SplitSum (0): also sum odd and even frames           */
+  int out_stack[2];    /* -OutStack (0 1): 1 = also return the aligned frames;
+                          second value: sum them in groups of this many frames
+                          (CZbinStack, Align/CZbinStack.cpp:27-71)              */
 } mc3_params;
 
 /* Sizes a movie will use (CBufferPool::CreateBuffers, CBufferPool.cpp:95-270). */
@@ -89,7 +92,26 @@ typedef struct {
   int n_sums;              /* out                                             */
   int n_patches;           /* out                                             */
   double time_ms;          /* out: device time of the call                    */
+  float* stack;            /* -OutStack: [nz][out_size[1]][out_size[0]] aligned
+                              (and locally corrected) frames before dose
+                              weighting, -FtBin-binned, unclamped
+                              (CCorrectFullShift::mCropFrame,
+                              Correct/CCorrectFullShift.cpp:336-356); with
+                              out_stack[1] > 1 the group sums fill the first
+                              stack_frames slots                               */
+  int stack_on_device;     /* 1: `stack` is a device pointer                   */
+  int stack_frames;        /* out: frames written to `stack`                   */
 } mc3_result;
+
+/* A known alignment (the -InAln file of Align/CLoadAlign.cpp:118-250): the
+ * movie is corrected with these shifts and not aligned. */
+typedef struct {
+  int nz;                     /* frames the tables cover (must equal the movie's) */
+  const float* global_shifts; /* [nz][2] full-frame shifts as in the file     */
+  int n_patches;              /* 0: full-frame correction only                */
+  const float* patch_shifts;  /* [nz][n_patches][2] local shifts              */
+  const float* patch_centers; /* [n_patches][2]                               */
+} mc3_alignment;
 
 /* ---- library ---- */
 const char* mc3_version(void);
@@ -138,6 +160,15 @@ int mc3_process_movie(mc3_ctx* ctx, const mc3_movie* movie, mc3_result* out);
  * cudaHostRegister) for the copy to overlap.  Device-resident movies need
  * no prefetch (no-op). */
 int mc3_prefetch_movie(mc3_ctx* ctx, const mc3_movie* movie);
+/* Align::CLoadAlign (Align/CLoadAlign.cpp:52-250; used by
+ * CFullAlign::Align, Align/CFullAlign.cpp:85-89, and
+ * CPatchAlign::mCalcPatchShifts, Align/CPatchAlign.cpp:67-96): the tables
+ * are copied and used, instead of measuring, by every following
+ * mc3_process_movie until cleared with NULL.  As in the reference, patch
+ * mode makes the full-frame shifts relative to the reference frame
+ * (-FmRef) and treats every loaded patch shift as good.  n_patches must
+ * match the context's -Patch grid (MC3_EINVAL otherwise). */
+int mc3_set_alignment(mc3_ctx* ctx, const mc3_alignment* aln);
 
 /* ---- components (device pointers unless stated) ---- */
 /* Util::CCufft2D::Forward (Util/CCufft2D.cpp:65-87): in-place R2C of nz

@@ -51,6 +51,7 @@ class _Params(ctypes.Structure):
         ("correct_bad", ctypes.c_int),
         ("gpu", ctypes.c_int),
         ("split_sum", ctypes.c_int),
+        ("out_stack", ctypes.c_int * 2),
     ]
 
 
@@ -90,6 +91,19 @@ class _Result(ctypes.Structure):
         ("n_sums", ctypes.c_int),
         ("n_patches", ctypes.c_int),
         ("time_ms", ctypes.c_double),
+        ("stack", ctypes.c_void_p),
+        ("stack_on_device", ctypes.c_int),
+        ("stack_frames", ctypes.c_int),
+    ]
+
+
+class _Alignment(ctypes.Structure):
+    _fields_ = [
+        ("nz", ctypes.c_int),
+        ("global_shifts", ctypes.c_void_p),
+        ("n_patches", ctypes.c_int),
+        ("patch_shifts", ctypes.c_void_p),
+        ("patch_centers", ctypes.c_void_p),
     ]
 
 
@@ -111,6 +125,7 @@ _SIGS = {
     "mc3_set_gain": ([_VP, _VP, _I, _I, _I], _I),
     "mc3_process_movie": ([_VP, ctypes.POINTER(_Movie), ctypes.POINTER(_Result)], _I),
     "mc3_prefetch_movie": ([_VP, ctypes.POINTER(_Movie)], _I),
+    "mc3_set_alignment": ([_VP, ctypes.POINTER(_Alignment)], _I),
     "mc3_fft_forward": ([_VP, _I, _I, _I, _I, _VP], _I),
     "mc3_fft_inverse": ([_VP, _I, _I, _I, _VP], _I),
     "mc3_phase_shift": ([_VP, _VP, _I, _I, _F, _F, _I, _VP], _I),
@@ -191,6 +206,7 @@ class Params:
     correct_bad: int = 1
     gpu: int = 0
     split_sum: int = 0
+    out_stack: tuple = (0, 1)
 
     def to_c(self) -> _Params:
         p = _Params()
@@ -214,6 +230,7 @@ class Params:
         p.correct_bad = int(self.correct_bad)
         p.gpu = int(self.gpu)
         p.split_sum = int(self.split_sum)
+        p.out_stack[0], p.out_stack[1] = int(self.out_stack[0]), int(self.out_stack[1])
         return p
 
 
@@ -229,6 +246,7 @@ class Result:
     n_sums: int
     n_patches: int
     time_ms: float
+    stack: Optional[np.ndarray] = None  # [stack_frames][ny][nx] aligned frames (-OutStack)
 
 
 _MODES = {np.dtype(np.uint8): 0, np.dtype(np.int16): 1, np.dtype(np.float32): 2, np.dtype(np.uint16): 6}
@@ -311,6 +329,28 @@ class MotionCor3:
         if not mv.on_device:
             self._prefetched.append(keep)
 
+    def set_alignment(self, global_shifts=None, patch_shifts=None, patch_centers=None) -> None:
+        """Known alignment for the following movies (mc3_set_alignment, the
+        -InAln path); global_shifts None clears it.  global_shifts [nz][2],
+        patch_shifts [nz][P][2], patch_centers [P][2]."""
+        if global_shifts is None:
+            _check(_lib().mc3_set_alignment(self._h, None), "mc3_set_alignment")
+            return
+        g = np.ascontiguousarray(global_shifts, np.float32)
+        a = _Alignment()
+        a.nz = g.shape[0]
+        a.global_shifts = g.ctypes.data
+        keep = [g]
+        if patch_shifts is not None:
+            ps = np.ascontiguousarray(patch_shifts, np.float32)
+            pc = np.ascontiguousarray(patch_centers, np.float32)
+            a.n_patches = ps.shape[1]
+            a.patch_shifts = ps.ctypes.data
+            a.patch_centers = pc.ctypes.data
+            keep += [ps, pc]
+        _check(_lib().mc3_set_alignment(self._h, ctypes.byref(a)), "mc3_set_alignment")
+        del keep  # the library copies the tables
+
     def process(self, frames, sums_out=None) -> Result:
         """frames: [nz][ny][nx] numpy array (host) or torch CUDA tensor."""
         mv, keep = self._movie(frames)
@@ -344,15 +384,22 @@ class MotionCor3:
         r.patch_bad = pb.ctypes.data if P else None
         r.iterations = iters.ctypes.data
         r.errors = errs.ctypes.data
+        stack = None
+        if int(self.params.out_stack[0]):
+            ox, oy = info["out_size"]
+            stack = np.zeros((nz, oy, ox), np.float32)
+            r.stack = stack.ctypes.data
         _check(_lib().mc3_process_movie(self._h, ctypes.byref(mv), ctypes.byref(r)),
                "mc3_process_movie")
+        if stack is not None:
+            stack = stack[:r.stack_frames]
         if not mv.on_device and self._prefetched:
             self._prefetched.pop(0)
         del keep
         return Result(sums=sums, global_shifts=gsh, patch_shifts=psh if P else None,
                       patch_centers=pc if P else None, patch_bad=pb if P else None,
                       iterations=iters, errors=errs, n_sums=r.n_sums, n_patches=r.n_patches,
-                      time_ms=r.time_ms)
+                      time_ms=r.time_ms, stack=stack)
 
     # ---- component entry points needing the context ----
     def iterative_align(self, stack, group: int, max_iter: int, tol: float, bfactor: float,

@@ -62,6 +62,8 @@ void mc3_params_default(mc3_params* p) {
   p->correct_bad = 1;
   p->gpu = 0;
   p->split_sum = 0;
+  p->out_stack[0] = 0;
+  p->out_stack[1] = 1;
 }
 
 int mc3_create(const mc3_params* p, mc3_ctx** out) {
@@ -137,6 +139,11 @@ int mc3_process_movie(mc3_ctx* ctx, const mc3_movie* movie, mc3_result* out) {
 int mc3_prefetch_movie(mc3_ctx* ctx, const mc3_movie* movie) {
   if (!ctx || !movie) return MC3_EINVAL;
   return ctx->eng->prefetch(*movie);
+}
+
+int mc3_set_alignment(mc3_ctx* ctx, const mc3_alignment* aln) {
+  if (!ctx) return MC3_EINVAL;
+  return ctx->eng->set_alignment(aln);
 }
 
 // ---- components ----

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <strings.h>
 #include <vector>
@@ -134,6 +135,85 @@ struct HostBuf {
   T* as() { return static_cast<T*>(p); }
 };
 
+// Align/CLoadAlign.cpp:52-250: an -InAln alignment file, as -OutAln (and
+// the reference) write it.  Keywords are searched in order ("setting",
+// "stackSize", "patches", "throw"); the first nz lines that scan as
+// "%d %f %f" are the full-frame shifts; in patch mode every later line
+// that scans as "%d %f %f %f %f" is (frame, centre x, y, shift x, y), nz of
+// them per patch.
+struct LoadedAln {
+  int stk[4] = {0, 0, 0, 0};
+  int patches[3] = {0, 0, 0};
+  int thr[2] = {0, 0};
+  std::vector<float> global, patch, centers;  // [nz][2], [nz][P][2], [P][2]
+};
+
+bool load_aln(const std::string& path, LoadedAln* a) {
+  FILE* f = std::fopen(path.c_str(), "rt");
+  if (!f) return false;
+  char line[256], buf[64];
+  auto find = [&](const char* key) {
+    while (std::fgets(line, sizeof(line), f))
+      if (std::strstr(line, key)) return true;
+    return false;
+  };
+  bool ok = find("setting") && find("stackSize") &&
+            std::sscanf(line, "%63s %d %d %d %d", buf, a->stk, a->stk + 1, a->stk + 2, a->stk + 3) >= 4;
+  ok = ok && find("patches") &&
+       std::sscanf(line, "%63s %d %d %d", buf, a->patches, a->patches + 1, a->patches + 2) >= 4;
+  ok = ok && find("throw") && std::sscanf(line, "%63s %d %d", buf, a->thr, a->thr + 1) >= 3;
+  const int nz = a->stk[2] - a->thr[0] - a->thr[1];
+  ok = ok && nz > 0;
+  if (ok) {
+    a->global.assign(2 * (size_t)nz, 0.0f);
+    int n = 0, fr;
+    float sx, sy;
+    while (n < nz && std::fgets(line, sizeof(line), f))
+      if (std::sscanf(line, "%d  %f  %f", &fr, &sx, &sy) == 3) {
+        a->global[2 * n] = sx;
+        a->global[2 * n + 1] = sy;
+        ++n;
+      }
+    ok = n == nz;
+  }
+  const int P = a->patches[0] * a->patches[1];
+  if (ok && P > 0) {
+    a->patch.assign(2 * (size_t)nz * P, 0.0f);
+    a->centers.assign(2 * (size_t)P, 0.0f);
+    int fm = 0, pc = 0, fr;
+    float cx, cy, sx, sy;
+    while (pc < P && std::fgets(line, sizeof(line), f)) {
+      if (line[0] == '#') continue;
+      if (std::sscanf(line, "%d %f %f %f %f", &fr, &cx, &cy, &sx, &sy) != 5) continue;
+      a->patch[((size_t)fm * P + pc) * 2] = sx;
+      a->patch[((size_t)fm * P + pc) * 2 + 1] = sy;
+      a->centers[2 * pc] = cx;
+      a->centers[2 * pc + 1] = cy;
+      if (++fm == nz) {
+        fm = 0;
+        ++pc;
+      }
+    }
+    ok = pc == P;
+  }
+  std::fclose(f);
+  return ok;
+}
+
+// CLoadAlign::Open(dir, stack) (Align/CLoadAlign.cpp:66-86) and
+// CMain::mOpenOutAlnFile: <dir>/<movie file name> with its last extension
+// replaced by .aln.
+std::string aln_name(const std::string& dir_in, const std::string& movie) {
+  std::string name = dir_in;
+  if (name.empty() || name.back() != '/') name += "/";
+  const size_t slash = movie.rfind('/');
+  name += slash == std::string::npos ? movie : movie.substr(slash + 1);
+  const size_t dot = name.rfind('.');
+  if (dot == std::string::npos) name += ".aln";
+  else name = name.substr(0, dot) + ".aln";
+  return name;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -145,7 +225,7 @@ int main(int argc, char** argv) {
     std::printf("Usage: MotionCor3 -InMrc movie.mrc -OutMrc sum.mrc [-Gain gain.mrc] "
                 "[-Patch x y] [-Iter n] [-Tol px] [-Bft g p] [-FmDose d] [-PixSize a] "
                 "[-kV kv] [-Group g p] [-FmRef f] [-SumRange lo hi] [-PhaseOnly 0|1] [-SplitSum 0|1] "
-                "[-FtBin b] [-OutAln dir] "
+                "[-FtBin b] [-OutAln dir] [-InAln dir] [-OutStack 0|1 zbin] "
                 "[-LogDir dir] [-Gpu id]\n");
     return eSuccess;
   }
@@ -179,12 +259,14 @@ int main(int argc, char** argv) {
   if (p.group[1] < 1) p.group[1] = 1;
   A.ints("-FmRef", &p.fm_ref, 1);
   A.ints("-SplitSum", &p.split_sum, 1);  // CInput.cpp:657-663
+  A.ints("-OutStack", p.out_stack, 2);    // CInput.cpp:590-592
+  const std::string in_aln = A.str("-InAln");
   int gpu[8];
   if (A.ints("-Gpu", gpu, 8) > 0) p.gpu = gpu[0];
   const char* ignored[] = {"-InTiff", "-InEer", "-InSuffix", "-InSkips", "-ArcDir", "-Dark",
-                           "-DefectFile", "-InAln", "-DefectMap", "-FullSum", "-TmpFile",
+                           "-DefectFile", "-DefectMap", "-FullSum", "-TmpFile",
                            "-StackZ", "-Cs", "-AmpCont", "-ExtPhase", "-Throw", "-Trunc", "-Serial",
-                           "-Tilt", "-Crop", "-OutStack", "-RotGain", "-FlipGain", "-InvGain", "-Mag",
+                           "-Tilt", "-Crop", "-RotGain", "-FlipGain", "-InvGain", "-Mag",
                            "-InFmMotion", "-GpuMemUsage", "-UseGpus", "-FmIntFile",
                            "-EerSampling", "-OutStar", "-TiffOrder", "-CorrInterp"};
   for (const char* t : ignored) {
@@ -201,6 +283,30 @@ int main(int argc, char** argv) {
     return eFailLoad;
   }
   std::printf("MRC file size mode: %d  %d  %d  %d\n", h.nx, h.ny, h.nz, h.mode);
+  // -InAln (CMain::mOpenInAlnFile, CMain.cpp:382-398): the file's patch
+  // grid and throws replace the command line's.
+  LoadedAln la;
+  bool aln_ok = false;
+  if (!in_aln.empty()) {
+    aln_ok = load_aln(aln_name(in_aln, in_mrc), &la);
+    if (aln_ok && (la.thr[0] != 0 || la.thr[1] != 0)) {
+      std::printf("Info: alignment files with thrown frames are not supported; "
+                  "the movie is aligned.\n\n");
+      aln_ok = false;
+    } else if (aln_ok && la.stk[2] != h.nz) {
+      std::printf("Info: alignment file covers %d frames, the movie has %d; "
+                  "the movie is aligned.\n\n", la.stk[2], h.nz);
+      aln_ok = false;
+    } else if (!aln_ok) {
+      std::printf("Info: Alignment file cannot be read.\n\n");
+    }
+    if (aln_ok) {
+      p.patch[0] = la.patches[0] <= 1 ? 0 : la.patches[0];
+      p.patch[1] = la.patches[1] <= 1 ? 0 : la.patches[1];
+      p.patch[2] = la.patches[2];
+      if (p.patch[0] == 0 || p.patch[1] == 0) la.patch.clear();
+    }
+  }
   const size_t frame_bytes = (size_t)h.nx * h.ny * mc3::mrc::bytes_per_pixel(h.mode);
   HostBuf frames(frame_bytes * h.nz);
   if (!mc3::mrc::read_frames(in_mrc, h, 0, h.nz, frames.as<unsigned char>())) return eFailLoad;
@@ -233,6 +339,19 @@ int main(int argc, char** argv) {
     return eFailProcess;
   }
   const int N = h.nz, P = info.n_patches;
+  if (aln_ok) {
+    mc3_alignment al{};
+    al.nz = N;
+    al.global_shifts = la.global.data();
+    al.n_patches = la.patch.empty() ? 0 : P;
+    al.patch_shifts = la.patch.empty() ? nullptr : la.patch.data();
+    al.patch_centers = la.patch.empty() ? nullptr : la.centers.data();
+    if ((s = mc3_set_alignment(ctx, &al)) != MC3_OK) {
+      std::fprintf(stderr, "Error: %s\n", mc3_strerror(s));
+      mc3_destroy(ctx);
+      return eFailProcess;
+    }
+  }
   const int ox = info.out_size[0], oy = info.out_size[1];  // -FtBin output size
   HostBuf sums_buf(sizeof(float) * (size_t)info.n_sums * ox * oy);
   float* sums = sums_buf.as<float>();
@@ -249,6 +368,11 @@ int main(int argc, char** argv) {
   r.patch_bad = P ? pb.data() : nullptr;
   r.iterations = iters.data();
   r.errors = errs.data();
+  std::unique_ptr<HostBuf> stack_buf;
+  if (p.out_stack[0] != 0) {
+    stack_buf.reset(new HostBuf(sizeof(float) * (size_t)N * ox * oy));
+    r.stack = stack_buf->as<float>();
+  }
   auto t0 = std::chrono::steady_clock::now();
   s = mc3_process_movie(ctx, &mv, &r);
   auto t1 = std::chrono::steady_clock::now();
@@ -277,6 +401,26 @@ int main(int argc, char** argv) {
     const std::string name = out_name(out_mrc, exts[i], ".mrc");
     saved = mc3::mrc::write_float_image(name, img, ox, oy, pix, mn, mx, me) && saved;
     std::printf("Corrected sum has been saved in:\n   %s\n\n", name.c_str());
+  }
+  // ---- aligned stack (CSaveSerialCryoEM::mSaveStack, CSaveSerialCryoEM.cpp:146-211):
+  //      min/max over frames, mean of the frame means, 32 ext-header floats ----
+  if (stack_buf && r.stack_frames > 0) {
+    const size_t fpx = (size_t)ox * oy;
+    float mn = 1e20f, mx = -1e20f;
+    double mean = 0.0;
+    for (int i = 0; i < r.stack_frames; ++i) {
+      float a, b, m;
+      stats(r.stack + i * fpx, fpx, &a, &b, &m);
+      mn = a < mn ? a : mn;
+      mx = b > mx ? b : mx;
+      mean += m;
+    }
+    mean /= r.stack_frames;
+    const std::string name = out_name(out_mrc, "_Stk", ".mrc");
+    std::printf("Saving motion corrected stack ......\n");
+    saved = mc3::mrc::write_float_stack(name, r.stack, ox, oy, r.stack_frames, pix, mn, mx,
+                                        (float)mean, 32) && saved;
+    std::printf("Motion corrected stack done.\n\n");
   }
   // ---- logs ----
   const std::string stem = log_stem(log_dir, in_mrc);
@@ -335,13 +479,7 @@ int main(int argc, char** argv) {
   // ---- alignment file (-OutAln; Align/CSaveAlign.cpp:61-151, opened by
   //      CMain::mOpenOutAlnFile, CMain.cpp:367-380) ----
   if (!out_aln.empty()) {
-    std::string name = out_aln;
-    if (name.back() != '/') name += "/";
-    const size_t slash = in_mrc.rfind('/');
-    name += slash == std::string::npos ? in_mrc : in_mrc.substr(slash + 1);
-    const size_t dot = name.rfind('.');
-    if (dot == std::string::npos) name += ".aln";
-    else name = name.substr(0, dot) + ".aln";
+    const std::string name = aln_name(out_aln, in_mrc);
     FILE* f = std::fopen(name.c_str(), "wt");
     if (!f) {
       std::printf("Info: %s\n%s\n\n", "      cannot be opened. Alignment wiil not be saved.",

@@ -444,6 +444,62 @@ int patch_masks(const uint8_t* bad, const float2* shifts, int P, int nb,
   return kOk;
 }
 
+// -OutStack frames: GFourierResize2D copy-mode crop (Util/GFourierResize2D.cu:7-37)
+// of every frame spectrum, with the frame's phase shift (tables ex [N][inX],
+// ey [N][inY], as the column passes apply them) when ex is given.
+__global__ void k_crop_frames(const float2* __restrict__ in, int inX, int inY, long in_stride,
+                              const float2* __restrict__ ex, const float2* __restrict__ ey,
+                              float2* __restrict__ out, int outX, int outY, long out_stride) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int yo = blockIdx.y;
+  const int f = blockIdx.z;
+  if (x >= outX) return;
+  const int yi = yo > outY / 2 ? yo - outY + inY : yo;
+  float2 v = in[(long)f * in_stride + (long)yi * inX + x];
+  if (ex) v = cmul(v, cmul(ex[(long)f * inX + x], ey[(long)f * inY + yi]));
+  out[(long)f * out_stride + (long)yo * outX + x] = v;
+}
+
+int crop_frames(const float2* in, int inX, int inY, long in_stride, const float2* ex,
+                const float2* ey, float2* out, int outX, int outY, long out_stride, int N,
+                cudaStream_t st) {
+  if (outX > inX || outY > inY || N < 1 || N > 65535) return kEUnsupported;
+  dim3 grid(ceil_div(outX, 128), outY, N);
+  prof::Scope ps("k_crop_frames", (double)N * outX * outY * 16.0, st);
+  k_crop_frames<<<grid, 128, 0, st>>>(in, inX, inY, in_stride, ex, ey, out, outX, outY,
+                                      out_stride);
+  MC3_CHECK_LAUNCH("k_crop_frames");
+  return kOk;
+}
+
+// CZbinStack::mGroup (Align/CZbinStack.cpp:57-71) in place: group g of zbin
+// frames (the last one shorter) is summed in frame order into slot g.  One
+// thread owns one pixel of every frame, and group g reads only slots >= g*zbin
+// >= g, so the in-place update is race-free.
+__global__ void k_zbin_frames(float* frames, long fr_stride, int pitch, int W, int H, int N,
+                              int zbin) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= W) return;
+  float* p = frames + (long)y * pitch + x;
+  for (int g = 0, f0 = 0; f0 < N; ++g, f0 += zbin) {
+    const int n = min(zbin, N - f0);
+    float s = p[(long)f0 * fr_stride];
+    for (int i = 1; i < n; ++i) s += p[(long)(f0 + i) * fr_stride];
+    p[(long)g * fr_stride] = s;
+  }
+}
+
+int zbin_frames(float* frames, long fr_stride, int pitch, int W, int H, int N, int zbin,
+                cudaStream_t st) {
+  if (zbin < 1 || N < 1) return kEInval;
+  dim3 grid(ceil_div(W, 128), H);
+  prof::Scope ps("k_zbin_frames", (double)N * W * H * 4.0 + (double)W * H * 4.0 * ((N + zbin - 1) / zbin), st);
+  k_zbin_frames<<<grid, 128, 0, st>>>(frames, fr_stride, pitch, W, H, N, zbin);
+  MC3_CHECK_LAUNCH("k_zbin_frames");
+  return kOk;
+}
+
 __global__ void k_unpad_positive(const float* in, long pitch, float* out, int W, int H,
                                  long in_stride) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;

@@ -346,6 +346,79 @@ int Engine::global_sums(const float2* spec, int N, const host::StackShift& fs, c
 }
 
 // ---------------------------------------------------------------------------
+// Align/CLoadAlign.cpp:52-250: the loaded tables replace the measured ones.
+int Engine::set_alignment(const mc3_alignment* aln) {
+  if (!aln) {
+    aln_loaded = false;
+    aln_global.clear();
+    aln_patch.clear();
+    aln_centers.clear();
+    return kOk;
+  }
+  if (aln->nz < 1 || !aln->global_shifts || aln->n_patches < 0 || aln->n_patches > 64)
+    return kEInval;
+  if (aln->n_patches > 0 && (!aln->patch_shifts || !aln->patch_centers)) return kEInval;
+  aln_nz = aln->nz;
+  aln_P = aln->n_patches;
+  aln_global.assign(aln->global_shifts, aln->global_shifts + 2 * (size_t)aln->nz);
+  if (aln_P > 0) {
+    aln_patch.assign(aln->patch_shifts, aln->patch_shifts + 2 * (size_t)aln->nz * aln_P);
+    aln_centers.assign(aln->patch_centers, aln->patch_centers + 2 * (size_t)aln_P);
+  } else {
+    aln_patch.clear();
+    aln_centers.clear();
+  }
+  aln_loaded = true;
+  return kOk;
+}
+
+// CCorrectFullShift::mCropFrame (Correct/CCorrectFullShift.cpp:336-356) for
+// all frames at once, then CZbinStack::DoIt (Align/CZbinStack.cpp:27-71):
+// the (shifted) normalised spectra are cropped to the output size, brought
+// to real space by an unnormalised C2R and, with a z-bin above 1, summed in
+// groups of out_stack[1] frames (the last group takes what is left).
+int Engine::write_stack(float2* spec, bool phase, const Geometry& g, mc3_result* out) {
+  const int N = g.N, oW = g.outW, oH = g.outH, ocX = oW / 2 + 1;
+  const size_t ncmp = (size_t)g.cmpX * g.cmpY, ocmp = (size_t)ocX * oH;
+  cudaStream_t st = stream;
+  float2* s = spec;
+  const bool crop = oW != g.W || oH != g.H;
+  if (crop) {
+    MC3_TRY(d_stk.ensure(sizeof(float2) * ocmp * N));
+    s = d_stk.as<float2>();
+    MC3_TRY(crop_frames(spec, g.cmpX, g.cmpY, (long)ncmp, phase ? d_fex.as<float2>() : nullptr,
+                        phase ? d_fey.as<float2>() : nullptr, s, ocX, oH, (long)ocmp, N, st));
+  }
+  Batch bi{N, N, (long)ocmp, nullptr, (long)ocmp};
+  ColOps inv{};
+  inv.dir = 1;
+  inv.scale = 1.0f;
+  if (phase && !crop) {
+    inv.ex = d_fex.as<float2>();
+    inv.ey = d_fey.as<float2>();
+  }
+  MC3_TRY(col_fft(s, s, ocX, ocX, oH, bi, inv, st));
+  Batch br{N, N, (long)ocmp, nullptr, (long)ocmp * 2};
+  float* real = reinterpret_cast<float*>(s);
+  MC3_TRY(row_c2r(s, ocX, real, 2 * ocX, oW, oH, br, st));
+  int nf = N;
+  if (prm.out_stack[1] > 1) {
+    host::FrameGroups G;
+    G.setup(N, prm.out_stack[1]);
+    nf = G.count();
+    MC3_TRY(zbin_frames(real, (long)ocmp * 2, 2 * ocX, oW, oH, N, prm.out_stack[1], st));
+  }
+  // every row of every frame lies 2*ocX floats after the previous one
+  MC3_CUDA(cudaMemcpy2DAsync(out->stack, sizeof(float) * oW, real, sizeof(float) * 2 * ocX,
+                             sizeof(float) * oW, (size_t)nf * oH,
+                             out->stack_on_device ? cudaMemcpyDeviceToDevice
+                                                  : cudaMemcpyDeviceToHost,
+                             st));
+  out->stack_frames = nf;
+  return kOk;
+}
+
+// ---------------------------------------------------------------------------
 int Engine::process(const mc3_movie& mv, mc3_result* out) {
   MC3_CUDA(cudaSetDevice(device));
   if (prm.align == 0) return kEUnsupported;
@@ -360,6 +433,12 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
   Geometry g;
   MC3_TRY(g.compute(mv.nx, mv.ny, mv.nz, prm));
   if (has_gain && (gain_w != g.W || gain_h != g.H)) return kEInval;  // CProcessThread::mCheckGain
+  const bool loaded = aln_loaded;
+  if (loaded && (aln_nz != g.N || aln_P != g.P)) {
+    last_error = "loaded alignment does not match the movie (frames or patches)";
+    return kEInval;
+  }
+  const bool want_stack = prm.out_stack[0] != 0 && out && out->stack;
   const int W = g.W, H = g.H, N = g.N;
   const size_t npx = (size_t)W * H;
   const size_t ncmp = (size_t)g.cmpX * g.cmpY;
@@ -420,9 +499,11 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
     ColOps ops{};
     ops.dir = -1;
     ops.scale = (float)(1.0 / W / H);
-    ops.crop = d_xcf.as<float2>();
-    ops.crop_x = g.xcfCmpX;
-    ops.crop_y = g.xcfCmpY;
+    if (!loaded) {  // a loaded alignment needs no alignment stack
+      ops.crop = d_xcf.as<float2>();
+      ops.crop_x = g.xcfCmpX;
+      ops.crop_y = g.xcfCmpY;
+    }
     MC3_TRY(col_fft(spec, spec, g.cmpX, g.cmpX, H, bc, ops, st));
   }
   // ---- 5. full-frame alignment (Align/CFullAlign.cpp:127-164) ----
@@ -433,15 +514,30 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
   std::vector<host::StackShift> xs;
   std::vector<int> it0;
   std::vector<std::vector<float>> err0;
-  MC3_TRY(align_stacks(d_xcf.as<float2>(), (long)nxcf * N, 1, g.xcfCmpX, g.xcfCmpY, N, G0,
-                       prm.bft[0], tol, xs, it0, err0));
+  if (loaded) {  // CFullAlign::Align with CLoadAlign loaded (Align/CFullAlign.cpp:85-89)
+    xs.resize(1);
+    xs[0].setup(N);
+    it0.assign(1, 0);
+    err0.assign(1, std::vector<float>());
+  } else {
+    MC3_TRY(align_stacks(d_xcf.as<float2>(), (long)nxcf * N, 1, g.xcfCmpX, g.xcfCmpY, N, G0,
+                         prm.bft[0], tol, xs, it0, err0));
+  }
   host::StackShift xsh = xs[0];  // xcf pixels
 
   std::vector<float> patShift, patCent;
   std::vector<unsigned char> patBad;
   std::vector<int> patIters;
   std::vector<std::vector<float>> patErr;
-  if (g.patch) {
+  if (g.patch && loaded) {
+    // CPatchAlign::mCalcPatchShifts with CLoadAlign loaded
+    // (Align/CPatchAlign.cpp:67-96): tables as read, no bad flags
+    patShift = aln_patch;
+    patCent = aln_centers;
+    patBad.assign((size_t)N * g.P, 0);
+    patIters.assign(g.P, 0);
+    patErr.assign(g.P, std::vector<float>());
+  } else if (g.patch) {
     const int xcfX = (g.xcfCmpX - 1) * 2, xcfY = g.xcfCmpY;
     // ---- 6a. features on the aligned xcf sum (Align/CDetectFeatures.cpp:58-181) ----
     {
@@ -542,6 +638,11 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
   host::StackShift fs = xsh;
   fs.multiply(g.xcfBin[0], g.xcfBin[1]);
   fs.truncate_decimal();
+  if (loaded)
+    for (int f = 0; f < N; ++f) {
+      fs.x(f) = aln_global[2 * f];
+      fs.y(f) = aln_global[2 * f + 1];
+    }
   if (g.patch) {
     // CPatchAlign::mCorrectFullShift (Align/CPatchAlign.cpp:47-65)
     int ref = N / 2;
@@ -584,6 +685,7 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
   if (!g.patch) {
     MC3_TRY(frame_sums(spec, (long)ncmp, N, g.cmpX, g.cmpY, d_fex.as<float2>(), d_fey.as<float2>(),
                        d_acc.as<float>(), d_Wn.as<float>(), dp, d_sums.as<float2>(), g.nSums, st));
+    if (want_stack) MC3_TRY(write_stack(spec, true, g, out));  // spectra are not needed after
   } else {
     // Correct/GCorrectPatchShift.cu:97-285: per frame C2R -> gather -> R2C
     const int P = g.P;
@@ -624,7 +726,9 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
     }
     MC3_TRY(frame_sums(spec, (long)ncmp, N, g.cmpX, g.cmpY, nullptr, nullptr, d_acc.as<float>(),
                        d_Wn.as<float>(), dp, d_sums.as<float2>(), g.nSums, st));
+    if (want_stack) MC3_TRY(write_stack(spec, false, g, out));
   }
+  if (out && !want_stack) out->stack_frames = 0;
   // ---- 8. sums to real space (CCorrectFullShift::mUnpadSums,
   //      Correct/CCorrectFullShift.cpp:146-185): Fourier crop to the -FtBin
   //      output size, C2R, positivity, unpad ----

@@ -52,6 +52,12 @@ class Engine {
   // Starts the host->device copy of a later movie's raw frames on the copy
   // stream (at most two outstanding); process() consumes them in order.
   int prefetch(const mc3_movie& mv);
+  // Known alignment used instead of measuring (NULL clears it).
+  int set_alignment(const mc3_alignment* aln);
+  // -OutStack: the corrected frames (spectra `spec`, phase tables when
+  // `phase`) cropped to the output size, to real space, z-binned, copied to
+  // out->stack.
+  int write_stack(float2* spec, bool phase, const Geometry& g, mc3_result* out);
 
   // Batched CIterativeAlign over `nstack` stacks of N spectra each.
   int align_stacks(const float2* spec, long stack_stride, int nstack, int cmpX, int cmpY, int N,
@@ -89,6 +95,11 @@ class Engine {
   DevBuf d_xcf, d_sh, d_ex, d_ey, d_S, d_T, d_win, d_gsh, d_act, d_gstart, d_gsize;
   DevBuf d_pat, d_patoff, d_bsum, d_bimg, d_btmp, d_bmap, d_scal;
   DevBuf d_fex, d_fey, d_Wn, d_acc, d_sums, d_real, d_gath, d_pcent, d_pshift, d_pbad, d_pmask, d_out, d_bsums;
+  DevBuf d_stk;
+  // loaded alignment (mc3_set_alignment)
+  bool aln_loaded = false;
+  int aln_nz = 0, aln_P = 0;
+  std::vector<float> aln_global, aln_patch, aln_centers;
   bool has_gain = false;
   double wn_key[6] = {0, 0, 0, 0, 0, 0};  // geometry and dose options of d_Wn
   bool wn_valid = false;

@@ -79,6 +79,14 @@ int local_gather(const float* in, long in_stride, float* out, long out_stride, i
                  int P, cudaStream_t st);
 int patch_masks(const uint8_t* bad, const float2* shifts, int P, int nb,
                 unsigned long long* masks, uint8_t* clean, cudaStream_t st);
+// Fourier crop of N frame spectra, with their phase shift when ex/ey are given.
+int crop_frames(const float2* in, int inX, int inY, long in_stride, const float2* ex,
+                const float2* ey, float2* out, int outX, int outY, long out_stride, int N,
+                cudaStream_t st);
+// In-place group sums of N real frames (groups of zbin, last shorter) into
+// the first ceil(N/zbin) frames.
+int zbin_frames(float* frames, long fr_stride, int pitch, int W, int H, int N, int zbin,
+                cudaStream_t st);
 // out[y*W+x] = max(0, in[y*pitch+x])
 int unpad_positive(const float* in, long pitch, float* out, int W, int H, int n,
                    long in_stride, cudaStream_t st);

@@ -106,6 +106,11 @@ bool read_image_float(const std::string& path, std::vector<float>* img, int* nx,
 // SetExtHeader(0, 0, 0) + SetMinMaxMean).
 bool write_float_image(const std::string& path, const float* img, int nx, int ny, float pix,
                        float amin, float amax, float amean) {
+  return write_float_stack(path, img, nx, ny, 1, pix, amin, amax, amean, 0);
+}
+
+bool write_float_stack(const std::string& path, const float* img, int nx, int ny, int nz,
+                       float pix, float amin, float amax, float amean, int ext_floats) {
   unsigned char hd[1024];
   std::memset(hd, 0, sizeof(hd));
   auto put_i = [&](int off, int32_t v) { std::memcpy(hd + off, &v, 4); };
@@ -113,17 +118,17 @@ bool write_float_image(const std::string& path, const float* img, int nx, int ny
   auto put_s = [&](int off, int16_t v) { std::memcpy(hd + off, &v, 2); };
   put_i(0, nx);
   put_i(4, ny);
-  put_i(8, 1);
+  put_i(8, nz);
   put_i(12, 2);
   put_i(16, 0);
   put_i(20, 0);
   put_i(24, 0);
   put_i(28, nx);
   put_i(32, ny);
-  put_i(36, 1);
+  put_i(36, nz);
   put_f(40, nx * pix);
   put_f(44, ny * pix);
-  put_f(48, 1 * pix);
+  put_f(48, nz * pix);
   put_f(52, 90.f);
   put_f(56, 90.f);
   put_f(60, 90.f);
@@ -134,12 +139,13 @@ bool write_float_image(const std::string& path, const float* img, int nx, int ny
   put_f(80, amax);
   put_f(84, amean);
   put_i(88, 0);
-  put_i(92, 0);
+  const int nsymbt = ext_floats * 4 * nz;
+  put_i(92, nsymbt);
   put_s(96, -16224);
   std::memcpy(hd + 104, "AGAR", 5);
   put_i(108, 2014 * 10);
   put_s(128, 0);
-  put_s(130, 0);
+  put_s(130, (int16_t)ext_floats);
   put_s(132, 1);
   put_s(160, 5);
   put_f(184, 90.f);
@@ -151,7 +157,15 @@ bool write_float_image(const std::string& path, const float* img, int nx, int ny
   FILE* f = std::fopen(path.c_str(), "wb");
   if (!f) return false;
   bool ok = std::fwrite(hd, 1, 1024, f) == 1024;
-  const size_t n = (size_t)nx * ny;
+  if (ok && nsymbt > 0) {
+    // CSaveExtHeader: ext_floats per section, float 11 = pixel size
+    // (LibSrc/Mrcfile/Header/CSaveExtHeader.cpp:28-46, 102-123)
+    std::vector<float> ext((size_t)ext_floats * nz, 0.0f);
+    if (ext_floats > 11)
+      for (int z = 0; z < nz; ++z) ext[(size_t)z * ext_floats + 11] = pix;
+    ok = std::fwrite(ext.data(), sizeof(float), ext.size(), f) == ext.size();
+  }
+  const size_t n = (size_t)nx * ny * nz;
   if (ok) ok = std::fwrite(img, sizeof(float), n, f) == n;
   ok = (std::fclose(f) == 0) && ok;
   return ok;

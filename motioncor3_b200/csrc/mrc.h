@@ -28,6 +28,11 @@ bool read_image_float(const std::string& path, std::vector<float>* img, int* nx,
 // Writes a single float image (mode 2) with min/max/mean in the header.
 bool write_float_image(const std::string& path, const float* img, int nx, int ny, float pix,
                        float amin, float amax, float amean);
+// Writes nz float images (mode 2) with `ext_floats` extended-header floats
+// per section holding the pixel size at float 11 (the aligned stack of
+// CSaveSerialCryoEM::mSaveStack, CSaveSerialCryoEM.cpp:146-211).
+bool write_float_stack(const std::string& path, const float* img, int nx, int ny, int nz,
+                       float pix, float amin, float amax, float amean, int ext_floats);
 
 }  // namespace mrc
 }  // namespace mc3

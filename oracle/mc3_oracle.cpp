@@ -1045,6 +1045,8 @@ void oracle_default_params(oracle_params* p) {
   p->correct_bad = 1;
   p->split_sum = 0;
   p->ft_bin = 1.0f;
+  p->out_stack[0] = 0;
+  p->out_stack[1] = 1;
 }
 
 void oracle_rfft2(const double* img, double* spec, int W, int H, int normalise) {
@@ -1220,6 +1222,11 @@ int oracle_process_movie(const oracle_params* p, const float* frames, int W, int
       fs.y(i) = out->use_global_shifts[2 * i + 1];
     }
     if (patchMode) {
+      // CPatchAlign::mCorrectFullShift makes loaded shifts relative too
+      // (Align/CPatchAlign.cpp:47-52); shifts already relative are unchanged
+      int ref = p->fm_ref < 0 ? N / 2 : std::min(std::max(p->fm_ref - 1, 0), N - 1);
+      float rx = fs.x(ref), ry = fs.y(ref);
+      for (int i = 0; i < N; ++i) { fs.x(i) -= rx; fs.y(i) -= ry; }
       patShift.assign(out->use_patch_shifts, out->use_patch_shifts + (size_t)N * P * 2);
       patCent.assign(out->use_patch_centers, out->use_patch_centers + (size_t)P * 2);
       patBad.assign(out->use_patch_bad, out->use_patch_bad + (size_t)N * P);
@@ -1290,6 +1297,24 @@ int oracle_process_movie(const oracle_params* p, const float* frames, int W, int
         wsum[i] = std::sqrt(s);
       }
   }
+  // output size of -FtBin (CInput::GetBinnedSize, CInput.cpp:678-688)
+  int oW = W, oH = H;
+  if (p->ft_bin > 0) {
+    oW = (int)(W / p->ft_bin + 0.5f) / 2 * 2;
+    oH = (int)(H / p->ft_bin + 0.5f) / 2 * 2;
+  }
+  const int ocX = oW / 2 + 1;
+  const long opx = (long)oW * oH;
+  // GFourierResize2D copy-mode crop (Util/GFourierResize2D.cu:7-37)
+  auto crop_to_out = [&](const cd* S, cd* dst) {
+    for (int yo = 0; yo < oH; ++yo) {
+      const int yi = yo > oH / 2 ? yo - oH + H : yo;
+      for (int x = 0; x < ocX; ++x) dst[(long)yo * ocX + x] = S[(long)yi * g.cmpX + x];
+    }
+  };
+  const bool want_stack = p->out_stack[0] != 0 && out->stack != nullptr;
+  std::vector<cd> stk_crop(want_stack ? (long)ocX * oH : 0);
+  std::vector<double> stk_img(want_stack ? opx : 0);
   std::vector<cd> sums((long)nSums * ncmp, cd(0.0));
   std::vector<double> realf, gath;
   if (patchMode) { realf.resize(npx); gath.resize(npx); }
@@ -1306,6 +1331,12 @@ int oracle_process_movie(const oracle_params* p, const float* frames, int W, int
     }
     cd* s0 = &sums[0];
     for (long i = 0; i < ncmp; ++i) s0[i] += X[i];
+    if (want_stack) {
+      // CCorrectFullShift::mCropFrame (Correct/CCorrectFullShift.cpp:336-356)
+      crop_to_out(X, stk_crop.data());
+      irfft2(stk_crop.data(), stk_img.data(), oW, oH);
+      for (long i = 0; i < opx; ++i) out->stack[(long)f * opx + i] = (float)stk_img[i];
+    }
     // CCorrectFullShift::mGenSums (Correct/CCorrectFullShift.cpp:271-300):
     // the odd/even split sums take the frame after dose weighting
     cd* split = p->split_sum ? &sums[(long)(nBase + (f % 2)) * ncmp] : nullptr;
@@ -1327,25 +1358,31 @@ int oracle_process_movie(const oracle_params* p, const float* frames, int W, int
   // mUnpadSums (CCorrectFullShift.cpp:146-185): Fourier crop to the -FtBin
   // size (CInput::GetBinnedSize, CInput.cpp:678-688; GFourierResize2D copy
   // mode, Util/GFourierResize2D.cu:7-37), C2R, positivity
-  int oW = W, oH = H;
-  if (p->ft_bin > 0) {
-    oW = (int)(W / p->ft_bin + 0.5f) / 2 * 2;
-    oH = (int)(H / p->ft_bin + 0.5f) / 2 * 2;
-  }
-  const int ocX = oW / 2 + 1;
-  const long opx = (long)oW * oH;
   std::vector<double> img(opx);
   std::vector<cd> crop((long)ocX * oH);
   for (int s = 0; s < nSums; ++s) {
-    const cd* S = &sums[(long)s * ncmp];
-    for (int yo = 0; yo < oH; ++yo) {
-      const int yi = yo > oH / 2 ? yo - oH + H : yo;
-      for (int x = 0; x < ocX; ++x) crop[(long)yo * ocX + x] = S[(long)yi * g.cmpX + x];
-    }
+    crop_to_out(&sums[(long)s * ncmp], crop.data());
     irfft2(crop.data(), img.data(), oW, oH);
     for (long i = 0; i < opx; ++i) out->sums[(long)s * opx + i] = (float)std::max(0.0, img[i]);
   }
   out->n_sums = nSums;
+  out->stack_frames = 0;
+  if (want_stack) {
+    // CZbinStack::DoIt (Align/CZbinStack.cpp:27-71): FP32 sums in frame
+    // order, groups of out_stack[1] frames, the last one shorter
+    const int zb = p->out_stack[1] > 1 ? p->out_stack[1] : 1;
+    int ng = 0;
+    for (int f0 = 0; f0 < N; f0 += zb, ++ng) {
+      const int n = std::min(zb, N - f0);
+      float* dst = out->stack + (long)ng * opx;
+      for (long i = 0; i < opx; ++i) {
+        float v = out->stack[(long)f0 * opx + i];
+        for (int k = 1; k < n; ++k) v += out->stack[(long)(f0 + k) * opx + i];
+        dst[i] = v;
+      }
+    }
+    out->stack_frames = ng;
+  }
   // logged full-frame shifts: absolute (global mode) or relative (patch mode)
   for (int i = 0; i < N; ++i) {
     out->global_shifts[2 * i] = fs.x(i);

@@ -39,6 +39,7 @@ typedef struct {
   int correct_bad;    /* run hot-pixel/defect detection and correction     */
   int split_sum;      /* -SplitSum: odd and even frame sums after the others */
   float ft_bin;       /* -FtBin: Fourier binning of the output sums        */
+  int out_stack[2];   /* -OutStack: aligned frames wanted, z-bin            */
 } oracle_params;
 
 typedef struct {
@@ -59,6 +60,11 @@ typedef struct {
   const float* use_patch_shifts;      /* [N][P][2] */
   const float* use_patch_centers;     /* [P][2]    */
   const unsigned char* use_patch_bad; /* [N][P]    */
+  /* -OutStack output (when out_stack[0] and stack are set): the corrected
+   * frames before dose weighting, -FtBin-cropped, C2R, unclamped, z-binned
+   * into the first stack_frames slots; [N][Hb][Wb] caller-allocated. */
+  float* stack;
+  int stack_frames;       /* out */
 } oracle_result;
 
 void oracle_default_params(oracle_params* p);

@@ -69,6 +69,7 @@ class OracleParams(ctypes.Structure):
         ("correct_bad", ctypes.c_int),
         ("split_sum", ctypes.c_int),
         ("ft_bin", ctypes.c_float),
+        ("out_stack", ctypes.c_int * 2),
     ]
 
 
@@ -87,6 +88,8 @@ class OracleResult(ctypes.Structure):
         ("use_patch_shifts", _VP),
         ("use_patch_centers", _VP),
         ("use_patch_bad", _VP),
+        ("stack", _VP),
+        ("stack_frames", ctypes.c_int),
     ]
 
 
@@ -108,7 +111,7 @@ def params(**kw) -> OracleParams:
     p = OracleParams()
     lib().oracle_default_params(ctypes.byref(p))
     for k, v in kw.items():
-        if k in ("patch", "bft", "group", "sum_range"):
+        if k in ("patch", "bft", "group", "sum_range", "out_stack"):
             arr = getattr(p, k)
             for i, x in enumerate(v[:2]):
                 arr[i] = x
@@ -144,6 +147,10 @@ def process_movie(frames: np.ndarray, gain=None, force=None, **kw) -> dict:
     r.patch_bad = pb.ctypes.data
     r.iterations = its.ctypes.data
     r.bad_map = bad.ctypes.data
+    stack = None
+    if p.out_stack[0]:
+        stack = np.zeros((nz, oh, ob), np.float32)
+        r.stack = stack.ctypes.data
     keep = []
     if force:
         for key in ("global_shifts", "patch_shifts", "patch_centers", "patch_bad"):
@@ -157,7 +164,8 @@ def process_movie(frames: np.ndarray, gain=None, force=None, **kw) -> dict:
         raise RuntimeError(f"oracle_process_movie failed ({rc})")
     return dict(sums=sums[: r.n_sums], global_shifts=gsh, patch_shifts=psh if P else None,
                 patch_centers=pc if P else None, patch_bad=pb if P else None, iterations=its,
-                bad_map=bad, n_sums=r.n_sums)
+                bad_map=bad, n_sums=r.n_sums,
+                stack=None if stack is None else stack[: r.stack_frames])
 
 
 def rfft2(img: np.ndarray, normalise: bool = True) -> np.ndarray:

@@ -36,6 +36,7 @@ def test_defaults_match_reference_cinput(mc3lib):
     assert (p.group[0], p.group[1]) == (1, 4)
     assert p.kv == 300 and p.fm_ref == -1
     assert (p.sum_range[0], p.sum_range[1]) == (3.0, 25.0)
+    assert (p.out_stack[0], p.out_stack[1]) == (0, 1)  # m_aiOutStack (CInput.cpp:107-108)
 
 
 def test_strerror_and_version(mc3lib):

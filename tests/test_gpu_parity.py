@@ -235,6 +235,95 @@ def test_pipeline_patch_small(api, oracle, torch_cuda):
     assert res.n_patches == 9
 
 
+def _oracle_kw(params):
+    return dict(patch=params.patch[:2], iter=params.iter, tol=params.tol, bft=params.bft,
+                fm_dose=params.fm_dose, pix_size=params.pix_size, kv=params.kv,
+                group=params.group, split_sum=params.split_sum, ft_bin=params.ft_bin,
+                out_stack=params.out_stack)
+
+
+@pytest.mark.parametrize("ft_bin,zbin", [(1.0, 1), (1.5, 3)])
+def test_pipeline_aligned_stack(api, oracle, torch_cuda, ft_bin, zbin):
+    """-OutStack 1 zbin: the aligned frames (phase-shifted spectra, Fourier
+    crop, C2R, no clamp) and their group sums against the oracle corrected
+    with the GPU's shifts; the sums are unchanged by the stack."""
+    from motioncor3_b200 import synthetic as S
+    m = S.make_movie(384, 320, 10, dose=3.0, seed=38, gain=False)
+    p = api.Params(iter=6, tol=0.2, bft=(300, 100), fm_dose=1.2, pix_size=0.9, kv=300,
+                   ft_bin=ft_bin, out_stack=(1, zbin))
+    with api.MotionCor3(p) as mc:
+        res = mc.process(np.asarray(m.frames))
+    with api.MotionCor3(api.Params(iter=6, tol=0.2, bft=(300, 100), fm_dose=1.2, pix_size=0.9,
+                                   kv=300, ft_bin=ft_bin)) as mc:
+        plain = mc.process(np.asarray(m.frames))
+    for i in range(res.n_sums):
+        assert np.array_equal(res.sums[i], plain.sums[i])
+    same = oracle.process_movie(np.asarray(m.frames), force=dict(global_shifts=res.global_shifts),
+                                **_oracle_kw(p))
+    assert res.stack.shape == same["stack"].shape == ((10 + zbin - 1) // zbin,) + res.sums[0].shape
+    for f in range(res.stack.shape[0]):
+        e = _rel_rms(res.stack[f], same["stack"][f])
+        assert e <= 1e-5, (f, e)
+
+
+def test_pipeline_aligned_stack_patch(api, oracle, torch_cuda):
+    """-OutStack in patch mode: the locally corrected frames."""
+    from motioncor3_b200 import synthetic as S
+    m = S.make_movie(512, 512, 12, dose=4.0, seed=33, gain=True, local=True)
+    p = api.Params(patch=(3, 3), iter=5, tol=0.2, bft=(500, 150), fm_dose=1.0, pix_size=1.0,
+                   kv=300, out_stack=(1, 1))
+    with api.MotionCor3(p) as mc:
+        mc.set_gain(np.asarray(m.gain))
+        res = mc.process(np.asarray(m.frames))
+    force = dict(global_shifts=res.global_shifts, patch_shifts=res.patch_shifts,
+                 patch_centers=res.patch_centers, patch_bad=res.patch_bad)
+    same = oracle.process_movie(np.asarray(m.frames), gain=np.asarray(m.gain), force=force,
+                                **_oracle_kw(p))
+    assert res.stack.shape == same["stack"].shape == (12, 512, 512)
+    for f in range(12):
+        e = _rel_rms(res.stack[f], same["stack"][f])
+        assert e <= 1e-4, (f, e)
+
+
+@pytest.mark.parametrize("patch", [False, True])
+def test_pipeline_loaded_alignment(api, oracle, torch_cuda, patch):
+    """mc3_set_alignment (-InAln): the movie is corrected with the given
+    shifts, nothing is measured (0 iterations), and the sums match the
+    oracle corrected with the same tables (all patches good)."""
+    from motioncor3_b200 import synthetic as S
+    if patch:
+        m = S.make_movie(512, 512, 12, dose=4.0, seed=33, gain=False, local=True)
+        p = api.Params(patch=(3, 3), iter=5, tol=0.2, bft=(500, 150), fm_dose=1.0, pix_size=1.0)
+    else:
+        m = S.make_movie(384, 320, 12, dose=3.0, seed=32, gain=False)
+        p = api.Params(iter=6, tol=0.2, bft=(300, 100), fm_dose=1.2, pix_size=0.9)
+    with api.MotionCor3(p) as mc:
+        first = mc.process(np.asarray(m.frames))
+        g = first.global_shifts + np.float32(0.5)  # patch mode makes them relative again
+        mc.set_alignment(g if patch else first.global_shifts,
+                         first.patch_shifts if patch else None,
+                         first.patch_centers if patch else None)
+        res = mc.process(np.asarray(m.frames))
+        mc.set_alignment(None)
+        again = mc.process(np.asarray(m.frames))
+    assert res.iterations.max() == 0 and first.iterations[0] > 0
+    assert np.array_equal(again.global_shifts, first.global_shifts)
+    if not patch:
+        assert np.array_equal(res.global_shifts, first.global_shifts)
+        for i in range(res.n_sums):  # same shifts, same kernels: same bits
+            assert np.array_equal(res.sums[i], first.sums[i])
+        return
+    assert np.abs(res.global_shifts - first.global_shifts).max() <= 1e-6
+    assert np.array_equal(res.patch_shifts, first.patch_shifts)
+    assert not res.patch_bad.any()
+    force = dict(global_shifts=res.global_shifts, patch_shifts=res.patch_shifts,
+                 patch_centers=res.patch_centers, patch_bad=res.patch_bad)
+    same = oracle.process_movie(np.asarray(m.frames), force=force, **_oracle_kw(p))
+    for i in range(res.n_sums):
+        e = _rel_rms(res.sums[i], same["sums"][i])
+        assert e <= 1e-4, (i, e)
+
+
 def test_pipeline_config1_full_size(api, oracle, torch_cuda):
     """40 frames of 1024x1024, global alignment only (-Patch 0 0 -Iter 7
     -Tol 0.5 -Bft 150 -PixSize 1.0), dose 1 e/px/frame, unit gain."""

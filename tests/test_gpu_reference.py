@@ -36,13 +36,13 @@ def _read_log(path):
     return np.array(rows)
 
 
-def run_program(binary, workdir, movie, gain, tags):
+def run_program(binary, workdir, movie, gain, tags, extra=()):
     from motioncor3_b200 import mrcio
     os.makedirs(workdir, exist_ok=True)
     mv = os.path.join(workdir, "movie.mrc")
     mrcio.write(mv, movie)
     args = [binary, "-InMrc", mv, "-OutMrc", os.path.join(workdir, "sum.mrc"), "-LogDir",
-            workdir + "/", "-OutAln", workdir, "-Gpu", "0", "-Cs", "0"] + tags
+            workdir + "/", "-OutAln", workdir, "-Gpu", "0", "-Cs", "0"] + tags + list(extra)
     if gain is not None:
         gp = os.path.join(workdir, "gain.mrc")
         mrcio.write(gp, gain.astype(np.float32))
@@ -63,8 +63,11 @@ def run_program(binary, workdir, movie, gain, tags):
         if os.path.exists(f):
             logs[suf] = f
     aln = os.path.join(workdir, "movie.aln")
+    stk = os.path.join(workdir, "sum_Stk.mrc")
     return dict(sums=sums, logs=logs, secs=secs, stdout=out,
-                aln=open(aln).read() if os.path.exists(aln) else None)
+                aln=open(aln).read() if os.path.exists(aln) else None,
+                stack=mrcio.read(stk).astype(np.float64) if os.path.exists(stk) else None,
+                stack_header=mrcio.read_header(stk) if os.path.exists(stk) else None)
 
 
 def _aln_parts(text):
@@ -132,3 +135,71 @@ def test_cli_matches_reference_program(name, tmp_path, mc3lib):
         print(f"{name} sum{suf}: rel RMS {rel:.2e}; reference {ref['secs']} s, ours {ours['secs']} s")
         if same_shifts:
             assert rel <= tol, (suf, rel)
+
+
+def _rel(r, o):
+    return float(np.sqrt(np.mean((r - o) ** 2) / np.mean(r ** 2)))
+
+
+@pytest.mark.parametrize("tags", ["-Iter 6 -Tol 0.2 -Bft 300 -FmDose 1.2 -PixSize 0.9 -OutStack 1",
+                                  "-Iter 6 -Tol 0.2 -Bft 300 -FmDose 1.2 -PixSize 0.9 -FtBin 2 "
+                                  "-OutStack 1 3"])
+def test_cli_aligned_stack_matches_reference_program(tags, tmp_path, mc3lib):
+    """-OutStack: <OutMrc>_Stk.mrc (CSaveSerialCryoEM::mSaveStack) with the
+    same frames (z-binned by CZbinStack), size, pixel size and 32-float
+    extended header per section as the reference program's."""
+    if not os.path.exists(REF_BIN):
+        pytest.skip("reference program not built (oracle/ref_full)")
+    from motioncor3_b200 import build, synthetic as S
+    build.build()
+    m = S.make_movie(384, 320, 10, dose=3.0, seed=39, gain=False)
+    ref = run_program(REF_BIN, str(tmp_path / "ref"), m.frames, None, tags.split())
+    ours = run_program(OUR_BIN, str(tmp_path / "ours"), m.frames, None, tags.split())
+    assert ref["stack"] is not None and ours["stack"] is not None
+    assert ref["stack"].shape == ours["stack"].shape
+    hr, ho = ref["stack_header"], ours["stack_header"]
+    assert (hr["nx"], hr["ny"], hr["nz"], hr["mode"], hr["nsymbt"], hr["mx"]) == \
+        (ho["nx"], ho["ny"], ho["nz"], ho["mode"], ho["nsymbt"], ho["mx"])
+    assert abs(hr["xlen"] - ho["xlen"]) <= 1e-4 * abs(hr["xlen"])
+    ext = lambda path: np.fromfile(path, np.float32, count=hr["nsymbt"] // 4, offset=1024)
+    er = ext(str(tmp_path / "ref" / "sum_Stk.mrc"))
+    eo = ext(str(tmp_path / "ours" / "sum_Stk.mrc"))
+    assert np.array_equal(er, eo)
+    a, b = _read_log(ref["logs"]["-Full.log"]), _read_log(ours["logs"]["-Full.log"])
+    if np.array_equal(a, b):
+        for f in range(ref["stack"].shape[0]):
+            assert _rel(ref["stack"][f], ours["stack"][f]) <= 1e-4, f
+        for key in ("amin", "amax", "amean"):
+            assert abs(hr[key] - ho[key]) <= 1e-3 * max(abs(hr[key]), 1.0), key
+
+
+@pytest.mark.parametrize("name", ["global_dw_gain", "patch_3x3"])
+def test_cli_loaded_alignment_matches_reference_program(name, tmp_path, mc3lib):
+    """-InAln: both programs read the reference's own -OutAln file for the
+    movie and correct with it, without aligning; their sums agree as closely
+    as with identical measured shifts."""
+    if not os.path.exists(REF_BIN):
+        pytest.skip("reference program not built (oracle/ref_full)")
+    from motioncor3_b200 import build, synthetic as S
+    build.build()
+    c = CASES[name]
+    nz, ny, nx = c["shape"]
+    m = S.make_movie(nx, ny, nz, dose=c["dose"], seed=c["seed"], gain=c["gain"], local=c["local"])
+    tags = c["tags"].split()
+    src = run_program(REF_BIN, str(tmp_path / "src"), m.frames, m.gain, tags)
+    assert src["aln"] is not None
+    extra = ["-InAln", str(tmp_path / "src")]
+    ref = run_program(REF_BIN, str(tmp_path / "ref"), m.frames, m.gain, tags, extra)
+    ours = run_program(OUR_BIN, str(tmp_path / "ours"), m.frames, m.gain, tags, extra)
+    assert "Iteration  1" not in ours["stdout"]
+    assert sorted(ref["sums"]) == sorted(ours["sums"])
+    for key in ref["logs"]:
+        if key == "-Patch-Patch.log" or key == "-Patch-Frame.log":
+            continue  # bad-patch flags of a loaded file are unset in the reference
+        a, b = _read_log(ref["logs"][key]), _read_log(ours["logs"][key])
+        assert np.abs(a - b).max() <= 1e-6, key
+    tol = 1e-3 if c["local"] else 1e-4
+    for suf in ref["sums"]:
+        e = _rel(ref["sums"][suf], ours["sums"][suf])
+        print(f"{name} -InAln sum{suf}: rel RMS {e:.2e}")
+        assert e <= tol, (suf, e)

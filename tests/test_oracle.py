@@ -150,3 +150,49 @@ def test_oracle_fourier_binned_sums(oracle):
     ref = np.fft.irfft2(crop, s=(oh, ow)) * (oh * ow)
     assert np.abs(binned - np.maximum(ref, 0)).max() <= 1e-3 * np.abs(ref).max()
     assert abs(binned.mean() - full.mean()) <= 1e-3 * full.mean()
+
+
+def test_oracle_aligned_stack_and_zbin(oracle):
+    """-OutStack: the aligned frames add up to the plain sum (before its
+    positivity clamp, which a positive movie does not reach), and -OutStack
+    1 3 holds the FP32 group sums of three consecutive frames, the last
+    group shorter (CZbinStack::DoIt, Align/CZbinStack.cpp:27-71)."""
+    from motioncor3_b200 import synthetic as S
+    m = S.make_movie(128, 96, 7, dose=20.0, seed=10)
+    kw = dict(iter=4, tol=0.2, bft=(300, 100), fm_dose=1.2, pix_size=0.9, kv=300, ft_bin=1.5)
+    one = oracle.process_movie(m.frames, out_stack=(1, 1), **kw)
+    st = one["stack"]
+    assert st.shape == (7,) + one["sums"][0].shape
+    tot = st.astype(np.float64).sum(axis=0)
+    plain = one["sums"][0].astype(np.float64)
+    assert np.abs(tot - plain).max() <= 1e-5 * np.abs(plain).max()
+    three = oracle.process_movie(m.frames, out_stack=(1, 3), **kw)
+    assert three["stack"].shape[0] == 3
+    for g, (a, b) in enumerate([(0, 3), (3, 6), (6, 7)]):
+        ref = st[a].copy()
+        for k in range(a + 1, b):
+            ref = (ref + st[k]).astype(np.float32)
+        assert np.array_equal(three["stack"][g], ref), g
+    for i in range(one["n_sums"]):  # the stack leaves the sums alone
+        assert np.array_equal(three["sums"][i], one["sums"][i])
+
+
+def test_oracle_loaded_patch_alignment_is_made_relative(oracle):
+    """-InAln in patch mode: CPatchAlign::mCorrectFullShift makes the loaded
+    full-frame shifts relative to the reference frame (Align/CPatchAlign.cpp:47-52),
+    so an offset added to every loaded shift changes nothing."""
+    from motioncor3_b200 import synthetic as S
+    m = S.make_movie(192, 192, 6, dose=20.0, seed=11)
+    kw = dict(patch=(2, 2), iter=3, tol=0.2, bft=(300, 100), pix_size=1.0, group=(1, 2))
+    r = oracle.process_movie(m.frames, **kw)
+    force = dict(global_shifts=r["global_shifts"], patch_shifts=r["patch_shifts"],
+                 patch_centers=r["patch_centers"], patch_bad=np.zeros_like(r["patch_bad"]))
+    a = oracle.process_movie(m.frames, force=force, **kw)
+    force["global_shifts"] = r["global_shifts"] + np.float32(1.25)
+    b = oracle.process_movie(m.frames, force=force, **kw)
+    assert np.array_equal(a["global_shifts"], r["global_shifts"])
+    # (s + c) - (s_ref + c) rounds differently from s - s_ref by ~1e-7 px
+    assert np.abs(b["global_shifts"] - a["global_shifts"]).max() <= 1e-6
+    for i in range(a["n_sums"]):
+        d = a["sums"][i].astype(np.float64) - b["sums"][i]
+        assert np.sqrt(np.mean(d ** 2) / np.mean(a["sums"][i].astype(np.float64) ** 2)) <= 1e-3
