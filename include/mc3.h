@@ -73,7 +73,9 @@ typedef struct {
 
 typedef struct {
   const void* frames;  /* [nz][ny][nx] pixels, MRC mode `mode`               */
-  int mode;            /* 0 uint8, 1 int16, 2 float32, 6 uint16               */
+  int mode;            /* 0 and 5 uint8, 1 int16, 2 float32, 6 uint16, 101
+                          4-bit packed (rows of (nx+1)/2 bytes, even pixel in
+                          the low nibble; MrcUtil/GApplyRefsToFrame.cu:30-53) */
   int nx, ny, nz;
   int on_device;       /* 1: frames is a device pointer                       */
 } mc3_movie;

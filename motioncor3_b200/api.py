@@ -302,7 +302,15 @@ class MotionCor3:
             _check(_lib().mc3_set_gain(self._h, _hp(g), g.shape[1], g.shape[0], 0), "mc3_set_gain")
 
     @staticmethod
-    def _movie(frames):
+    def _movie(frames, nx4=None):
+        if nx4 is not None:  # packed 4-bit frames [nz][ny][(nx4+1)//2] (MRC mode 101)
+            on_dev = hasattr(frames, "data_ptr")
+            keep = frames if on_dev else np.ascontiguousarray(frames, np.uint8)
+            nz, ny, pk = keep.shape
+            if pk != (nx4 + 1) // 2:
+                raise MC3Error(MC3_EINVAL, "packed row length")
+            fptr = _dp(keep) if on_dev else keep.ctypes.data_as(_VP)
+            return _Movie(fptr, 101, nx4, ny, nz, 1 if on_dev else 0), keep
         on_dev = hasattr(frames, "data_ptr")
         if on_dev:
             import torch
@@ -321,10 +329,10 @@ class MotionCor3:
             fptr = keep.ctypes.data_as(_VP)
         return _Movie(fptr, dt, nx, ny, nz, 1 if on_dev else 0), keep
 
-    def prefetch(self, frames) -> None:
+    def prefetch(self, frames, nx4=None) -> None:
         """Starts copying a later movie's host frames to the device
         (mc3_prefetch_movie); pass the same array to a later process()."""
-        mv, keep = self._movie(frames)
+        mv, keep = self._movie(frames, nx4)
         _check(_lib().mc3_prefetch_movie(self._h, ctypes.byref(mv)), "mc3_prefetch_movie")
         if not mv.on_device:
             self._prefetched.append(keep)
@@ -351,9 +359,10 @@ class MotionCor3:
         _check(_lib().mc3_set_alignment(self._h, ctypes.byref(a)), "mc3_set_alignment")
         del keep  # the library copies the tables
 
-    def process(self, frames, sums_out=None) -> Result:
-        """frames: [nz][ny][nx] numpy array (host) or torch CUDA tensor."""
-        mv, keep = self._movie(frames)
+    def process(self, frames, sums_out=None, nx4=None) -> Result:
+        """frames: [nz][ny][nx] numpy array (host) or torch CUDA tensor; with
+        nx4, packed 4-bit frames [nz][ny][(nx4+1)//2] of width nx4."""
+        mv, keep = self._movie(frames, nx4)
         nx, ny, nz = mv.nx, mv.ny, mv.nz
         info = self.plan(nx, ny, nz)
         ns, P = info["n_sums"], info["n_patches"]

@@ -278,7 +278,7 @@ int main(int argc, char** argv) {
   if (in_mrc == out_mrc) return eInputOutputSame;
 
   mc3::mrc::Header h;
-  if (!mc3::mrc::read_header(in_mrc, &h) || mc3::mrc::bytes_per_pixel(h.mode) == 0) {
+  if (!mc3::mrc::read_header(in_mrc, &h) || mc3::mrc::frame_bytes(h.mode, h.nx, h.ny) == 0) {
     std::fprintf(stderr, "Error: cannot load %s\n", in_mrc.c_str());
     return eFailLoad;
   }
@@ -307,7 +307,7 @@ int main(int argc, char** argv) {
       if (p.patch[0] == 0 || p.patch[1] == 0) la.patch.clear();
     }
   }
-  const size_t frame_bytes = (size_t)h.nx * h.ny * mc3::mrc::bytes_per_pixel(h.mode);
+  const size_t frame_bytes = (size_t)mc3::mrc::frame_bytes(h.mode, h.nx, h.ny);
   HostBuf frames(frame_bytes * h.nz);
   if (!mc3::mrc::read_frames(in_mrc, h, 0, h.nz, frames.as<unsigned char>())) return eFailLoad;
 

@@ -129,11 +129,15 @@ int Engine::init() {
 }
 
 namespace {
-int mode_bytes(int mode) {
+// Bytes of one raw frame in MRC mode `mode` (0 when unsupported); mode 101
+// packs two 4-bit pixels per byte in rows of (nx+1)/2 bytes
+// (LibSrc/Mrcfile/Image/C4BitImage.cpp:15-40).
+size_t raw_frame_bytes(int mode, int nx, int ny) {
   switch (mode) {
-    case 0: return 1;
-    case 1: case 6: return 2;
-    case 2: return 4;
+    case 0: case 5: return (size_t)nx * ny;
+    case 1: case 6: return (size_t)nx * ny * 2;
+    case 2: return (size_t)nx * ny * 4;
+    case 101: return (size_t)((nx + 1) / 2) * ny;
     default: return 0;
   }
 }
@@ -147,14 +151,14 @@ int mode_bytes(int mode) {
 int Engine::prefetch(const mc3_movie& mv) {
   MC3_CUDA(cudaSetDevice(device));
   if (!mv.frames || mv.nx < 1 || mv.ny < 1 || mv.nz < 1) return kEInval;
-  const int bpp = mode_bytes(mv.mode);
-  if (!bpp) return kEUnsupported;
+  const size_t fbytes = raw_frame_bytes(mv.mode, mv.nx, mv.ny);
+  if (!fbytes) return kEUnsupported;
   if (mv.on_device) return kOk;  // nothing to copy
   if (n_pending >= 2) {
     last_error = "two movies are already prefetched; process one first";
     return kEInval;
   }
-  const size_t bytes = (size_t)bpp * mv.nx * mv.ny * mv.nz;
+  const size_t bytes = fbytes * mv.nz;
   const int slot = next_slot;
   if (d_rawslot[slot].cap < bytes) {
     // growing the slot frees it: wait for its last reader first
@@ -423,13 +427,8 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
   MC3_CUDA(cudaSetDevice(device));
   if (prm.align == 0) return kEUnsupported;
   if (!mv.frames) return kEInval;
-  int bpp = 0;
-  switch (mv.mode) {
-    case 0: bpp = 1; break;
-    case 1: case 6: bpp = 2; break;
-    case 2: bpp = 4; break;
-    default: return kEUnsupported;
-  }
+  const size_t fbytes = raw_frame_bytes(mv.mode, mv.nx, mv.ny);
+  if (!fbytes) return kEUnsupported;
   Geometry g;
   MC3_TRY(g.compute(mv.nx, mv.ny, mv.nz, prm));
   if (has_gain && (gain_w != g.W || gain_h != g.H)) return kEInval;  // CProcessThread::mCheckGain
@@ -452,7 +451,7 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
   if (!mv.on_device && n_pending > 0) {
     // the oldest prefetched movie must be this one
     const Pending pf = pending[0];
-    if (pf.host != mv.frames || pf.bytes != (size_t)bpp * npx * N) {
+    if (pf.host != mv.frames || pf.bytes != fbytes * N) {
       last_error = "movie differs from the oldest prefetched movie";
       return kEInval;
     }
@@ -462,8 +461,8 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
     raw = d_rawslot[pf.slot].p;
     used_slot = pf.slot;
   } else if (!mv.on_device) {
-    MC3_TRY(d_raw.ensure((size_t)bpp * npx * N));
-    MC3_CUDA(cudaMemcpyAsync(d_raw.p, mv.frames, (size_t)bpp * npx * N, cudaMemcpyHostToDevice, st));
+    MC3_TRY(d_raw.ensure(fbytes * N));
+    MC3_CUDA(cudaMemcpyAsync(d_raw.p, mv.frames, fbytes * N, cudaMemcpyHostToDevice, st));
     raw = d_raw.p;
   }
   // ---- 2. gain + frame sum (MrcUtil/CApplyRefs.cpp:36-212, CSumFFTStack) ----
@@ -471,7 +470,9 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
   MC3_TRY(d_sum.ensure(sizeof(float) * (size_t)g.padX * H));
   float* frames = d_frames.as<float>();
   const long fr_stride_f = (long)g.padX * H;
-  MC3_TRY(gain_and_sum(raw, mv.mode, (long)npx, has_gain ? d_gain.as<float>() : nullptr, frames,
+  // raw frame stride in elements of the mode's type (bytes for packed 4-bit)
+  const long raw_stride = mv.mode == 101 ? (long)fbytes : (long)npx;
+  MC3_TRY(gain_and_sum(raw, mv.mode, raw_stride, has_gain ? d_gain.as<float>() : nullptr, frames,
                        fr_stride_f, prm.correct_bad ? d_sum.as<float>() : nullptr, W, H, N, st));
   if (used_slot >= 0) MC3_CUDA(cudaEventRecord(slot_free[used_slot], st));  // raw is read only above
   // ---- 3. hot pixels and defects (BadPixel/CDetectMain.cpp, CCorrectMain.cpp) ----

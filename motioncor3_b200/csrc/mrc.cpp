@@ -17,11 +17,16 @@ bool valid_mode(int m) { return m == 0 || m == 1 || m == 2 || m == 6; }
 
 int bytes_per_pixel(int mode) {
   switch (mode) {
-    case 0: return 1;
+    case 0: case 5: return 1;
     case 1: case 6: return 2;
     case 2: return 4;
     default: return 0;
   }
+}
+
+long long frame_bytes(int mode, int nx, int ny) {
+  if (mode == 101) return (long long)((nx + 1) / 2) * ny;  // C4BitImage::GetImgBytes
+  return (long long)nx * ny * bytes_per_pixel(mode);
 }
 
 bool read_header(const std::string& path, Header* h) {
@@ -60,10 +65,10 @@ bool read_header(const std::string& path, Header* h) {
 
 bool read_frames(const std::string& path, const Header& h, int z0, int nz, void* dst) {
   const int bpp = bytes_per_pixel(h.mode);
-  if (!bpp || z0 < 0 || z0 + nz > h.nz) return false;
+  const long long frame = frame_bytes(h.mode, h.nx, h.ny);
+  if (!frame || z0 < 0 || z0 + nz > h.nz) return false;
   FILE* f = std::fopen(path.c_str(), "rb");
   if (!f) return false;
-  const long long frame = (long long)h.nx * h.ny * bpp;
   const long long off = 1024LL + h.nsymbt + frame * z0;
   bool ok = fseeko(f, (off_t)off, SEEK_SET) == 0;
   if (ok) ok = std::fread(dst, 1, (size_t)(frame * nz), f) == (size_t)(frame * nz);
@@ -85,12 +90,13 @@ bool read_image_float(const std::string& path, std::vector<float>* img, int* nx,
   Header h;
   if (!read_header(path, &h)) return false;
   const int bpp = bytes_per_pixel(h.mode);
+  if (!bpp) return false;  // images (gain) in packed modes are not read
   std::vector<unsigned char> raw((size_t)h.nx * h.ny * bpp);
   if (!read_frames(path, h, 0, 1, raw.data())) return false;
   img->resize((size_t)h.nx * h.ny);
   for (size_t i = 0; i < img->size(); ++i) {
     switch (h.mode) {
-      case 0: (*img)[i] = raw[i]; break;
+      case 0: case 5: (*img)[i] = raw[i]; break;
       case 1: (*img)[i] = ((const int16_t*)raw.data())[i]; break;
       case 2: (*img)[i] = ((const float*)raw.data())[i]; break;
       case 6: (*img)[i] = ((const uint16_t*)raw.data())[i]; break;

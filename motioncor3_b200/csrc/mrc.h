@@ -17,7 +17,8 @@ struct Header {
   bool swapped = false;
 };
 
-int bytes_per_pixel(int mode);  // 0 when unsupported
+int bytes_per_pixel(int mode);  // 0 when unsupported (and for packed mode 101)
+long long frame_bytes(int mode, int nx, int ny);  // 0 when unsupported
 // Reads the header; returns false on failure.
 bool read_header(const std::string& path, Header* h);
 // Reads frames [z0, z0+nz) as raw bytes in the file's mode (byte-swapped

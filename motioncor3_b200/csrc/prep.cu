@@ -27,14 +27,38 @@ __global__ void k_gain_sum(const T* __restrict__ raw, long raw_stride, const flo
   if (sum) sum[(long)y * padX + x] = s;
 }
 
+// Mode 101 (4-bit, two pixels per byte, rows of (W+1)/2 bytes): pixel x is
+// the low nibble of byte x/2 for even x, the high nibble for odd x
+// (GApplyRefsToFrame mGDoPkd, MrcUtil/GApplyRefsToFrame.cu:30-53).
+__global__ void k_gain_sum_pkd(const uint8_t* __restrict__ raw, long raw_stride,
+                               const float* __restrict__ gain, float* frames, long fr_stride,
+                               float* sum, int W, int H, int N, int padX) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= W) return;
+  const int pkX = (W + 1) / 2;
+  const float g = gain ? gain[(long)y * W + x] : 1.0f;
+  float s = 0.0f;
+  for (int f = 0; f < N; ++f) {
+    int b = raw[(long)f * raw_stride + (long)y * pkX + x / 2];
+    if (x & 1) b >>= 4;
+    float v = (float)(b & 0xf);
+    if (gain) v *= g;
+    frames[(long)f * fr_stride + (long)y * padX + x] = v;
+    s += v;
+  }
+  if (sum) sum[(long)y * padX + x] = s;
+}
+
 int gain_and_sum(const void* raw, int mode, long raw_stride, const float* gain, float* frames,
                  long fr_stride, float* sum, int W, int H, int N, cudaStream_t st) {
   const int padX = 2 * (W / 2 + 1);
   dim3 grid(ceil_div(W, 256), H);
-  const int bpp = mode == 0 ? 1 : (mode == 2 ? 4 : 2);
+  const double bpp = mode == 101 ? 0.5 : (mode == 0 || mode == 5) ? 1 : (mode == 2 ? 4 : 2);
   prof::Scope ps("k_gain_sum", (double)W * H * (N * (bpp + 4.0) + (gain ? 4.0 : 0.0) + (sum ? 4.0 : 0.0)), st);
   switch (mode) {
-    case 0: k_gain_sum<uint8_t><<<grid, 256, 0, st>>>((const uint8_t*)raw, raw_stride, gain, frames, fr_stride, sum, W, H, N, padX); break;
+    case 101: k_gain_sum_pkd<<<grid, 256, 0, st>>>((const uint8_t*)raw, raw_stride, gain, frames, fr_stride, sum, W, H, N, padX); break;
+    case 0: case 5: k_gain_sum<uint8_t><<<grid, 256, 0, st>>>((const uint8_t*)raw, raw_stride, gain, frames, fr_stride, sum, W, H, N, padX); break;
     case 1: k_gain_sum<int16_t><<<grid, 256, 0, st>>>((const int16_t*)raw, raw_stride, gain, frames, fr_stride, sum, W, H, N, padX); break;
     case 2: k_gain_sum<float><<<grid, 256, 0, st>>>((const float*)raw, raw_stride, gain, frames, fr_stride, sum, W, H, N, padX); break;
     case 6: k_gain_sum<uint16_t><<<grid, 256, 0, st>>>((const uint16_t*)raw, raw_stride, gain, frames, fr_stride, sum, W, H, N, padX); break;

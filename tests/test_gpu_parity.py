@@ -324,6 +324,26 @@ def test_pipeline_loaded_alignment(api, oracle, torch_cuda, patch):
         assert e <= 1e-4, (i, e)
 
 
+@pytest.mark.parametrize("nx", [320, 321])
+def test_pipeline_four_bit_frames(api, torch_cuda, nx):
+    """MRC mode 101 (two 4-bit pixels per byte, GApplyRefsToFrame mGDoPkd):
+    the packed movie gives the same sums, bit for bit, as its uint8
+    unpacking, for even and odd widths."""
+    from motioncor3_b200 import mrcio, synthetic as S
+    m = S.make_movie(nx, 256, 8, dose=2.0, seed=41, gain=True)
+    u8 = np.minimum(np.asarray(m.frames), 15).astype(np.uint8)
+    pk = mrcio.pack4(u8)
+    assert np.array_equal(mrcio.unpack4(pk, nx), u8)
+    p = api.Params(iter=5, tol=0.2, bft=(300, 100), fm_dose=1.0, pix_size=1.0)
+    with api.MotionCor3(p) as mc:
+        mc.set_gain(np.asarray(m.gain))
+        a = mc.process(u8)
+        b = mc.process(pk, nx4=nx)
+    assert np.array_equal(a.global_shifts, b.global_shifts)
+    for i in range(a.n_sums):
+        assert np.array_equal(a.sums[i], b.sums[i])
+
+
 def test_pipeline_config1_full_size(api, oracle, torch_cuda):
     """40 frames of 1024x1024, global alignment only (-Patch 0 0 -Iter 7
     -Tol 0.5 -Bft 150 -PixSize 1.0), dose 1 e/px/frame, unit gain."""

@@ -36,11 +36,11 @@ def _read_log(path):
     return np.array(rows)
 
 
-def run_program(binary, workdir, movie, gain, tags, extra=()):
+def run_program(binary, workdir, movie, gain, tags, extra=(), four_bit=False):
     from motioncor3_b200 import mrcio
     os.makedirs(workdir, exist_ok=True)
     mv = os.path.join(workdir, "movie.mrc")
-    mrcio.write(mv, movie)
+    mrcio.write(mv, movie, four_bit=four_bit)
     args = [binary, "-InMrc", mv, "-OutMrc", os.path.join(workdir, "sum.mrc"), "-LogDir",
             workdir + "/", "-OutAln", workdir, "-Gpu", "0", "-Cs", "0"] + tags + list(extra)
     if gain is not None:
@@ -203,3 +203,24 @@ def test_cli_loaded_alignment_matches_reference_program(name, tmp_path, mc3lib):
         e = _rel(ref["sums"][suf], ours["sums"][suf])
         print(f"{name} -InAln sum{suf}: rel RMS {e:.2e}")
         assert e <= tol, (suf, e)
+
+
+def test_cli_four_bit_movie_matches_reference_program(tmp_path, mc3lib):
+    """A mode-101 (4-bit packed) movie with an odd width, read and unpacked
+    as the reference does (CLoadCryoEMStack::mLoadSingle + GApplyRefsToFrame
+    mGDoPkd)."""
+    if not os.path.exists(REF_BIN):
+        pytest.skip("reference program not built (oracle/ref_full)")
+    from motioncor3_b200 import build, synthetic as S
+    build.build()
+    m = S.make_movie(321, 256, 10, dose=2.0, seed=42, gain=True)
+    u8 = np.minimum(m.frames, 15).astype(np.uint8)
+    tags = "-Iter 6 -Tol 0.2 -Bft 300 -FmDose 1.0 -PixSize 1.0".split()
+    ref = run_program(REF_BIN, str(tmp_path / "ref"), u8, m.gain, tags, four_bit=True)
+    ours = run_program(OUR_BIN, str(tmp_path / "ours"), u8, m.gain, tags, four_bit=True)
+    assert sorted(ref["sums"]) == sorted(ours["sums"])
+    a, b = _read_log(ref["logs"]["-Full.log"]), _read_log(ours["logs"]["-Full.log"])
+    assert np.abs(a - b).max() <= 0.05 + 1e-6
+    if np.array_equal(a, b):
+        for suf in ref["sums"]:
+            assert _rel(ref["sums"][suf], ours["sums"][suf]) <= 1e-4, suf

@@ -196,3 +196,20 @@ def test_oracle_loaded_patch_alignment_is_made_relative(oracle):
     for i in range(a["n_sums"]):
         d = a["sums"][i].astype(np.float64) - b["sums"][i]
         assert np.sqrt(np.mean(d ** 2) / np.mean(a["sums"][i].astype(np.float64) ** 2)) <= 1e-3
+
+
+def test_mrc_four_bit_round_trip(tmp_path):
+    """Mode 101 files: packed rows of (nx+1)//2 bytes, even pixel in the low
+    nibble (LibSrc/Mrcfile/Image/C4BitImage.cpp), odd widths included."""
+    from motioncor3_b200 import mrcio
+    rng = np.random.default_rng(5)
+    for nx in (6, 7):
+        a = rng.integers(0, 16, size=(3, 5, nx)).astype(np.uint8)
+        pk = mrcio.pack4(a)
+        assert pk.shape == (3, 5, (nx + 1) // 2)
+        assert pk[0, 0, 0] == (a[0, 0, 0] | (a[0, 0, 1] << 4))
+        f = str(tmp_path / f"m{nx}.mrc")
+        mrcio.write(f, a, four_bit=True)
+        h = mrcio.read_header(f)
+        assert (h["nx"], h["mode"]) == (nx, 101)
+        assert np.array_equal(mrcio.read(f), a)
