@@ -115,6 +115,22 @@ typedef struct {
   const float* patch_centers; /* [n_patches][2]                               */
 } mc3_alignment;
 
+/* Frame integration (-FmIntFile; DataUtil/CFmIntParam.cpp:29-283 and
+ * MrcUtil/CLoadCryoEMStack.cpp:184-262): the movie's n_raw raw frames are
+ * rendered into n_int frames, frame i the sum of raw frames start[i] ..
+ * start[i]+size[i]-1 taken modulo 256 as the reference's 8-bit rendered
+ * stack holds it (modes 0, 5 and 101 only).  acc_dose[i] is the dose
+ * accumulated at the end of rendered frame i; dose_weight asks for dose
+ * weighting even when -FmDose is 0 (the file gave a dose). */
+typedef struct {
+  int n_raw;              /* raw frames (mc3_movie.nz)                         */
+  int n_int;              /* rendered frames                                   */
+  const int* start;       /* [n_int]                                           */
+  const int* size;        /* [n_int]                                           */
+  const float* acc_dose;  /* [n_int] e/A^2                                     */
+  int dose_weight;
+} mc3_frame_integration;
+
 /* ---- library ---- */
 const char* mc3_version(void);
 const char* mc3_strerror(int code);
@@ -171,6 +187,11 @@ int mc3_prefetch_movie(mc3_ctx* ctx, const mc3_movie* movie);
  * (-FmRef) and treats every loaded patch shift as good.  n_patches must
  * match the context's -Patch grid (MC3_EINVAL otherwise). */
 int mc3_set_alignment(mc3_ctx* ctx, const mc3_alignment* aln);
+/* CFmIntParam / CFmGroupParam set up from a frame-integration table: the
+ * following movies (nz = n_raw) are rendered, dose-weighted with acc_dose
+ * and grouped by raw-frame counts (CFmGroupParam::mGroupByRawSize,
+ * DataUtil/CFmGroupParam.cpp:60-78); NULL clears it. */
+int mc3_set_frame_integration(mc3_ctx* ctx, const mc3_frame_integration* fi);
 
 /* ---- components (device pointers unless stated) ---- */
 /* Util::CCufft2D::Forward (Util/CCufft2D.cpp:65-87): in-place R2C of nz
@@ -244,6 +265,19 @@ int mc3_profile_read(char* buf, size_t len, int reset);
 unsigned long long mc3_kernel_launches(void);
 
 /* ---- host-side bookkeeping (host pointers) ---- */
+/* CReadFmIntFile::DoIt (DataUtil/CReadFmIntFile.cpp:104-170): up to
+ * max_entries (group size, integration size, raw-frame dose) rows of a
+ * frame-integration file; two-column files take fm_dose.  MC3_EIO when the
+ * file cannot be opened; *n_entries = 0 when it holds mixed doses. */
+int mc3_read_fmint_file(const char* path, float fm_dose, int max_entries, int* group_size,
+                        int* int_size, float* dose, int* n_entries);
+/* CFmIntParam::Setup (DataUtil/CFmIntParam.cpp:29-136): rendered-frame
+ * tables for n_raw raw frames from n_entries file rows (n_entries = 0: no
+ * file); fills up to max_int entries of start/size/acc_dose and returns
+ * their count in *n_int, *dose_weight = the file has a dose. */
+int mc3_frame_integration_tables(const int* group_size, const int* int_size, const float* dose,
+                                 int n_entries, int n_raw, float fm_dose, int max_int, int* n_int,
+                                 int* start, int* size, float* acc_dose, int* dose_weight);
 /* Align::CPeak2D::DoIt (Align/CPeak2D.cpp:39-109). */
 void mc3_peak2d(const float* window, int sea_x, int sea_y, float* shift);
 /* Util::CRemoveSpikes1D::DoIt(x, y, false) (Util/CRemoveSpikes1D.cpp:59-105). */

@@ -97,6 +97,17 @@ class _Result(ctypes.Structure):
     ]
 
 
+class _FrameIntegration(ctypes.Structure):
+    _fields_ = [
+        ("n_raw", ctypes.c_int),
+        ("n_int", ctypes.c_int),
+        ("start", ctypes.c_void_p),
+        ("size", ctypes.c_void_p),
+        ("acc_dose", ctypes.c_void_p),
+        ("dose_weight", ctypes.c_int),
+    ]
+
+
 class _Alignment(ctypes.Structure):
     _fields_ = [
         ("nz", ctypes.c_int),
@@ -126,6 +137,9 @@ _SIGS = {
     "mc3_process_movie": ([_VP, ctypes.POINTER(_Movie), ctypes.POINTER(_Result)], _I),
     "mc3_prefetch_movie": ([_VP, ctypes.POINTER(_Movie)], _I),
     "mc3_set_alignment": ([_VP, ctypes.POINTER(_Alignment)], _I),
+    "mc3_set_frame_integration": ([_VP, ctypes.POINTER(_FrameIntegration)], _I),
+    "mc3_read_fmint_file": ([ctypes.c_char_p, _F, _I, _VP, _VP, _VP, _VP], _I),
+    "mc3_frame_integration_tables": ([_VP, _VP, _VP, _I, _I, _F, _I, _VP, _VP, _VP, _VP, _VP], _I),
     "mc3_fft_forward": ([_VP, _I, _I, _I, _I, _VP], _I),
     "mc3_fft_inverse": ([_VP, _I, _I, _I, _VP], _I),
     "mc3_phase_shift": ([_VP, _VP, _I, _I, _F, _F, _I, _VP], _I),
@@ -359,6 +373,21 @@ class MotionCor3:
         _check(_lib().mc3_set_alignment(self._h, ctypes.byref(a)), "mc3_set_alignment")
         del keep  # the library copies the tables
 
+    def set_frame_integration(self, tables: Optional[dict], n_raw: int = 0) -> None:
+        """Rendered frames for the following movies of n_raw raw frames
+        (mc3_set_frame_integration); tables as frame_integration_tables()
+        returns them; None clears."""
+        if tables is None:
+            _check(_lib().mc3_set_frame_integration(self._h, None), "mc3_set_frame_integration")
+            return
+        st = np.ascontiguousarray(tables["start"], np.int32)
+        sz = np.ascontiguousarray(tables["size"], np.int32)
+        acc = np.ascontiguousarray(tables["acc_dose"], np.float32)
+        fi = _FrameIntegration(n_raw, len(st), st.ctypes.data, sz.ctypes.data, acc.ctypes.data,
+                               int(tables.get("dose_weight", 0)))
+        _check(_lib().mc3_set_frame_integration(self._h, ctypes.byref(fi)),
+               "mc3_set_frame_integration")
+
     def process(self, frames, sums_out=None, nx4=None) -> Result:
         """frames: [nz][ny][nx] numpy array (host) or torch CUDA tensor; with
         nx4, packed 4-bit frames [nz][ny][(nx4+1)//2] of width nx4."""
@@ -478,6 +507,43 @@ def local_gather(src, dst, nx: int, ny: int, centers, shifts, bad=None) -> None:
     _check(_lib().mc3_local_gather(_dp(src), _dp(dst), nx, ny, _dp(centers), _dp(shifts),
                                    _dp(bad) if bad is not None else None, P, _stream()),
            "mc3_local_gather")
+
+
+# ---- frame integration (host) ----
+def read_fmint_file(path: str, fm_dose: float = 0.0, max_entries: int = 4096):
+    """CReadFmIntFile::DoIt: (group_size, int_size, dose) arrays of a
+    frame-integration file (empty when it mixes doses)."""
+    g = np.zeros(max_entries, np.int32)
+    n = np.zeros(max_entries, np.int32)
+    d = np.zeros(max_entries, np.float32)
+    ne = ctypes.c_int(0)
+    _check(_lib().mc3_read_fmint_file(path.encode(), fm_dose, max_entries, _hp(g), _hp(n), _hp(d),
+                                      ctypes.byref(ne)), "mc3_read_fmint_file")
+    k = min(ne.value, max_entries)
+    return g[:k], n[:k], d[:k]
+
+
+def frame_integration_tables(entries, n_raw: int, fm_dose: float = 0.0) -> dict:
+    """CFmIntParam::Setup: rendered-frame tables for n_raw raw frames from
+    (group_size, int_size, dose) entries (None or empty: no file)."""
+    if entries is None or len(entries[0]) == 0:
+        g = n = d = None
+        ne = 0
+    else:
+        g = np.ascontiguousarray(entries[0], np.int32)
+        n = np.ascontiguousarray(entries[1], np.int32)
+        d = np.ascontiguousarray(entries[2], np.float32)
+        ne = len(g)
+    start = np.zeros(n_raw, np.int32)
+    size = np.zeros(n_raw, np.int32)
+    acc = np.zeros(n_raw, np.float32)
+    nint = ctypes.c_int(0)
+    dwt = ctypes.c_int(0)
+    _check(_lib().mc3_frame_integration_tables(_hp(g), _hp(n), _hp(d), ne, n_raw, fm_dose, n_raw,
+                                               ctypes.byref(nint), _hp(start), _hp(size), _hp(acc),
+                                               ctypes.byref(dwt)), "mc3_frame_integration_tables")
+    k = nint.value
+    return dict(start=start[:k], size=size[:k], acc_dose=acc[:k], dose_weight=dwt.value)
 
 
 # ---- diagnostics ----

@@ -1,6 +1,7 @@
 // extern "C" entry points declared in include/mc3.h.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -144,6 +145,53 @@ int mc3_prefetch_movie(mc3_ctx* ctx, const mc3_movie* movie) {
 int mc3_set_alignment(mc3_ctx* ctx, const mc3_alignment* aln) {
   if (!ctx) return MC3_EINVAL;
   return ctx->eng->set_alignment(aln);
+}
+
+int mc3_set_frame_integration(mc3_ctx* ctx, const mc3_frame_integration* fi) {
+  if (!ctx) return MC3_EINVAL;
+  return ctx->eng->set_frame_integration(fi);
+}
+
+int mc3_read_fmint_file(const char* path, float fm_dose, int max_entries, int* group_size,
+                        int* int_size, float* dose, int* n_entries) {
+  if (!path || !n_entries || max_entries < 0) return MC3_EINVAL;
+  std::vector<int> g, n;
+  std::vector<float> d;
+  if (!host::read_fmint_file(path, fm_dose, g, n, d)) return MC3_EIO;
+  *n_entries = (int)g.size();
+  for (int i = 0; i < (int)g.size() && i < max_entries; ++i) {
+    if (group_size) group_size[i] = g[i];
+    if (int_size) int_size[i] = n[i];
+    if (dose) dose[i] = d[i];
+  }
+  return MC3_OK;
+}
+
+int mc3_frame_integration_tables(const int* group_size, const int* int_size, const float* dose,
+                                 int n_entries, int n_raw, float fm_dose, int max_int, int* n_int,
+                                 int* start, int* size, float* acc_dose, int* dose_weight) {
+  if (n_raw < 1 || n_entries < 0 || !n_int) return MC3_EINVAL;
+  if (n_entries > 0 && (!group_size || !int_size || !dose)) return MC3_EINVAL;
+  for (int i = 0; i < n_entries; ++i)
+    if (int_size[i] < 1 || group_size[i] < 0) return MC3_EINVAL;
+  // CReadFmIntFile::NeedIntegrate (DataUtil/CReadFmIntFile.cpp:73-89)
+  bool integrate = false;
+  if (n_entries > 0 && std::fabs(dose[0] - dose[n_entries - 1]) < 0.0001f)
+    for (int i = 0; i < n_entries; ++i) integrate = integrate || int_size[i] > 1;
+  host::FmInt t;
+  if (integrate)
+    t.integrate(std::vector<int>(group_size, group_size + n_entries),
+                std::vector<int>(int_size, int_size + n_entries), dose[0], n_raw);
+  else
+    t.plain(n_raw, fm_dose);
+  *n_int = t.count();
+  for (int i = 0; i < t.count() && i < max_int; ++i) {
+    if (start) start[i] = t.start[i];
+    if (size) size[i] = t.size[i];
+    if (acc_dose) acc_dose[i] = t.acc[i];
+  }
+  if (dose_weight) *dose_weight = (n_entries > 0 && dose[0] > 0) ? 1 : 0;  // HasDose
+  return MC3_OK;
 }
 
 // ---- components ----

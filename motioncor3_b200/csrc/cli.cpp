@@ -225,7 +225,7 @@ int main(int argc, char** argv) {
     std::printf("Usage: MotionCor3 -InMrc movie.mrc -OutMrc sum.mrc [-Gain gain.mrc] "
                 "[-Patch x y] [-Iter n] [-Tol px] [-Bft g p] [-FmDose d] [-PixSize a] "
                 "[-kV kv] [-Group g p] [-FmRef f] [-SumRange lo hi] [-PhaseOnly 0|1] [-SplitSum 0|1] "
-                "[-FtBin b] [-OutAln dir] [-InAln dir] [-OutStack 0|1 zbin] "
+                "[-FtBin b] [-OutAln dir] [-InAln dir] [-OutStack 0|1 zbin] [-FmIntFile file] "
                 "[-LogDir dir] [-Gpu id]\n");
     return eSuccess;
   }
@@ -261,13 +261,14 @@ int main(int argc, char** argv) {
   A.ints("-SplitSum", &p.split_sum, 1);  // CInput.cpp:657-663
   A.ints("-OutStack", p.out_stack, 2);    // CInput.cpp:590-592
   const std::string in_aln = A.str("-InAln");
+  const std::string fmint_file = A.str("-FmIntFile");
   int gpu[8];
   if (A.ints("-Gpu", gpu, 8) > 0) p.gpu = gpu[0];
   const char* ignored[] = {"-InTiff", "-InEer", "-InSuffix", "-InSkips", "-ArcDir", "-Dark",
                            "-DefectFile", "-DefectMap", "-FullSum", "-TmpFile",
                            "-StackZ", "-Cs", "-AmpCont", "-ExtPhase", "-Throw", "-Trunc", "-Serial",
                            "-Tilt", "-Crop", "-RotGain", "-FlipGain", "-InvGain", "-Mag",
-                           "-InFmMotion", "-GpuMemUsage", "-UseGpus", "-FmIntFile",
+                           "-InFmMotion", "-GpuMemUsage", "-UseGpus",
                            "-EerSampling", "-OutStar", "-TiffOrder", "-CorrInterp"};
   for (const char* t : ignored) {
     int f, n;
@@ -283,6 +284,37 @@ int main(int argc, char** argv) {
     return eFailLoad;
   }
   std::printf("MRC file size mode: %d  %d  %d  %d\n", h.nx, h.ny, h.nz, h.mode);
+  // -FmIntFile (CReadFmIntFile::DoIt, CFmIntParam::Setup): rendered-frame
+  // tables for this movie's raw frames
+  std::vector<int> fi_start, fi_size;
+  std::vector<float> fi_acc;
+  int fi_dose = 0;
+  bool fi_on = false;
+  if (!fmint_file.empty()) {
+    const int maxe = 4096;
+    std::vector<int> eg(maxe), en(maxe);
+    std::vector<float> ed(maxe);
+    int ne = 0;
+    if (mc3_read_fmint_file(fmint_file.c_str(), p.fm_dose, maxe, eg.data(), en.data(), ed.data(),
+                            &ne) == MC3_OK && ne > 0) {
+      ne = ne < maxe ? ne : maxe;
+      fi_start.resize(h.nz);
+      fi_size.resize(h.nz);
+      fi_acc.resize(h.nz);
+      int nint = 0;
+      if (mc3_frame_integration_tables(eg.data(), en.data(), ed.data(), ne, h.nz, p.fm_dose, h.nz,
+                                       &nint, fi_start.data(), fi_size.data(), fi_acc.data(),
+                                       &fi_dose) == MC3_OK && nint > 0) {
+        fi_start.resize(nint);
+        fi_size.resize(nint);
+        fi_acc.resize(nint);
+        fi_on = true;
+        std::printf("Rendered size mode: %d  %d  %d  %d\n", h.nx, h.ny, nint,
+                    (nint != h.nz) ? 0 : h.mode);
+      }
+    }
+  }
+  const int n_render = fi_on ? (int)fi_start.size() : h.nz;
   // -InAln (CMain::mOpenInAlnFile, CMain.cpp:382-398): the file's patch
   // grid and throws replace the command line's.
   LoadedAln la;
@@ -293,9 +325,9 @@ int main(int argc, char** argv) {
       std::printf("Info: alignment files with thrown frames are not supported; "
                   "the movie is aligned.\n\n");
       aln_ok = false;
-    } else if (aln_ok && la.stk[2] != h.nz) {
+    } else if (aln_ok && la.stk[2] != n_render) {
       std::printf("Info: alignment file covers %d frames, the movie has %d; "
-                  "the movie is aligned.\n\n", la.stk[2], h.nz);
+                  "the movie is aligned.\n\n", la.stk[2], n_render);
       aln_ok = false;
     } else if (!aln_ok) {
       std::printf("Info: Alignment file cannot be read.\n\n");
@@ -333,12 +365,21 @@ int main(int argc, char** argv) {
     }
   }
   mc3_plan_info info;
+  if (fi_on) {
+    mc3_frame_integration fi{h.nz, (int)fi_start.size(), fi_start.data(), fi_size.data(),
+                             fi_acc.data(), fi_dose};
+    if ((s = mc3_set_frame_integration(ctx, &fi)) != MC3_OK) {
+      std::fprintf(stderr, "Error: %s\n", mc3_strerror(s));
+      mc3_destroy(ctx);
+      return eFailProcess;
+    }
+  }
   if ((s = mc3_plan(ctx, h.nx, h.ny, h.nz, &info)) != MC3_OK) {
     std::fprintf(stderr, "Error: %s\n", mc3_strerror(s));
     mc3_destroy(ctx);
     return eFailProcess;
   }
-  const int N = h.nz, P = info.n_patches;
+  const int N = n_render, P = info.n_patches;
   if (aln_ok) {
     mc3_alignment al{};
     al.nz = N;

@@ -60,95 +60,54 @@ int dose_norm(const float* acc_dose, int N, int cmpX, int cmpY, float pix, float
 // untouched); sum1 += X; sum2 += X when the frame's accumulated dose lies in
 // the selected range; with -SplitSum the (weighted) X also goes to the
 // "_ODD" sum for even frame indices and to "_EVN" for odd ones.
-// Two neighbouring frequencies per thread (one 16-byte load per frame when
-// the layout allows it); the arithmetic of each frequency is unchanged.
-__device__ __forceinline__ void frame_sum_step(float2 X, int f, int k, int x, int y, int cmpX,
-                                               int cmpY, const float2* __restrict__ ex,
-                                               const float2* __restrict__ ey, const float* acc,
-                                               const DoseParams& dp, float cd, float wn,
-                                               float2& s0, float2& s1, float2& s2, float2& so,
-                                               float2& se) {
-  if (ex) {
-    const float2 e = cmul(ex[(long)f * cmpX + x], ey[(long)f * cmpY + y]);
-    X = c2(e.x * X.x - e.y * X.y, e.x * X.y + e.y * X.x);
-  }
-  s0 = cadd(X, s0);
-  if (dp.enabled) {
-    if (k > 0) {
-      float fW = dose_weight_c(cd, acc[f]);
-      fW = fW / wn;
-      X.x *= fW;
-      X.y *= fW;
-    }
-    s1 = cadd(X, s1);
-    if (dp.dws && acc[f] >= dp.sum_range[0] && acc[f] <= dp.sum_range[1]) s2 = cadd(X, s2);
-  }
-  if (dp.split) {
-    if (f % 2 == 0) so = cadd(X, so);
-    else se = cadd(X, se);
-  }
-}
-
 __global__ void k_frame_sums(const float2* __restrict__ spec, long fr_stride, int N, int cmpX,
                              int cmpY, const float2* __restrict__ ex, const float2* __restrict__ ey,
                              const float* acc, const float* Wn, DoseParams dp, float2* sums,
                              int n_sums) {
   const long n = (long)cmpX * cmpY;
-  const long k0 = 2 * ((long)blockIdx.x * blockDim.x + threadIdx.x);
-  if (k0 >= n) return;
-  const bool two = k0 + 1 < n;
-  const bool vec = two && !(fr_stride & 1) &&
-                   ((reinterpret_cast<uintptr_t>(spec) & 15) == 0);
-  int x[2], y[2];
-  float cd[2], wn[2];
-  float2 s0[2], s1[2], s2[2], so[2], se[2];
-#pragma unroll
-  for (int e = 0; e < 2; ++e) {
-    const long k = k0 + e;
-    x[e] = (int)(k % cmpX);
-    y[e] = (int)(k / cmpX);
-    const bool ok = k < n;
-    wn[e] = dp.enabled && k > 0 && ok ? Wn[k] : 1.0f;
-    cd[e] = dp.enabled && k > 0 && ok ? crit_dose(x[e], y[e], cmpX, cmpY, dp.kv_factor, dp.pix_size)
-                                      : 1.0f;
-    s0[e] = s1[e] = s2[e] = so[e] = se[e] = c2(0.f, 0.f);
-  }
+  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int x = (int)(k % cmpX), y = (int)(k / cmpX);
+  float2 s0 = c2(0.f, 0.f), s1 = c2(0.f, 0.f), s2 = c2(0.f, 0.f);
+  float2 so = c2(0.f, 0.f), se = c2(0.f, 0.f);
+  const float wn = dp.enabled && k > 0 ? Wn[k] : 1.0f;
+  const float cd = dp.enabled && k > 0 ? crit_dose(x, y, cmpX, cmpY, dp.kv_factor, dp.pix_size) : 1.0f;
 #pragma unroll 4
   for (int f = 0; f < N; ++f) {
-    const float2* fr = spec + (long)f * fr_stride + k0;
-    float2 X0, X1 = c2(0.f, 0.f);
-    if (vec) {
-      const float4 q = *reinterpret_cast<const float4*>(fr);
-      X0 = c2(q.x, q.y);
-      X1 = c2(q.z, q.w);
-    } else {
-      X0 = fr[0];
-      if (two) X1 = fr[1];
+    float2 X = spec[(long)f * fr_stride + k];
+    if (ex) {
+      const float2 e = cmul(ex[(long)f * cmpX + x], ey[(long)f * cmpY + y]);
+      X = c2(e.x * X.x - e.y * X.y, e.x * X.y + e.y * X.x);
     }
-    frame_sum_step(X0, f, (int)k0, x[0], y[0], cmpX, cmpY, ex, ey, acc, dp, cd[0], wn[0], s0[0],
-                   s1[0], s2[0], so[0], se[0]);
-    if (two)
-      frame_sum_step(X1, f, (int)k0 + 1, x[1], y[1], cmpX, cmpY, ex, ey, acc, dp, cd[1], wn[1],
-                     s0[1], s1[1], s2[1], so[1], se[1]);
-  }
-#pragma unroll
-  for (int e = 0; e < 2; ++e) {
-    const long k = k0 + e;
-    if (k >= n) break;
-    sums[k] = s0[e];
-    int next = 1;
+    s0 = cadd(X, s0);
     if (dp.enabled) {
-      sums[n + k] = s1[e];
-      next = 2;
-      if (dp.dws) {
-        sums[2 * n + k] = s2[e];
-        next = 3;
+      if (k > 0) {
+        float fW = dose_weight_c(cd, acc[f]);
+        fW = fW / wn;
+        X.x *= fW;
+        X.y *= fW;
       }
+      s1 = cadd(X, s1);
+      if (dp.dws && acc[f] >= dp.sum_range[0] && acc[f] <= dp.sum_range[1]) s2 = cadd(X, s2);
     }
     if (dp.split) {
-      sums[(long)next * n + k] = so[e];
-      sums[(long)(next + 1) * n + k] = se[e];
+      if (f % 2 == 0) so = cadd(X, so);
+      else se = cadd(X, se);
     }
+  }
+  sums[k] = s0;
+  int next = 1;
+  if (dp.enabled) {
+    sums[n + k] = s1;
+    next = 2;
+    if (dp.dws) {
+      sums[2 * n + k] = s2;
+      next = 3;
+    }
+  }
+  if (dp.split) {
+    sums[(long)next * n + k] = so;
+    sums[(long)(next + 1) * n + k] = se;
   }
 }
 
@@ -158,7 +117,7 @@ int frame_sums(const float2* spec, long fr_stride, int N, int cmpX, int cmpY, co
   const long n = (long)cmpX * cmpY;
   if (n_sums != 1 + (dp.enabled ? 1 + (dp.dws ? 1 : 0) : 0) + (dp.split ? 2 : 0)) return kEInval;
   prof::Scope ps("k_frame_sums", (double)n * (8.0 * (N + n_sums) + (dp.enabled ? 4.0 : 0.0)), st);
-  k_frame_sums<<<(unsigned)((n + 511) / 512), 256, 0, st>>>(spec, fr_stride, N, cmpX, cmpY, ex, ey,
+  k_frame_sums<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(spec, fr_stride, N, cmpX, cmpY, ex, ey,
                                                            acc_dose, Wn, dp, sums, n_sums);
   MC3_CHECK_LAUNCH("k_frame_sums");
   return kOk;
@@ -472,30 +431,30 @@ int crop_frames(const float2* in, int inX, int inY, long in_stride, const float2
   return kOk;
 }
 
-// CZbinStack::mGroup (Align/CZbinStack.cpp:57-71) in place: group g of zbin
-// frames (the last one shorter) is summed in frame order into slot g.  One
-// thread owns one pixel of every frame, and group g reads only slots >= g*zbin
-// >= g, so the in-place update is race-free.
-__global__ void k_zbin_frames(float* frames, long fr_stride, int pitch, int W, int H, int N,
-                              int zbin) {
+// CZbinStack::mGroup (Align/CZbinStack.cpp:57-71) in place: group g (frames
+// grp[g] .. grp[g]+grp[ng+g]-1, consecutive groups) is summed in frame
+// order into slot g.  One thread owns one pixel of every frame, and group g
+// reads only slots >= its start >= g, so the in-place update is race-free.
+__global__ void k_zbin_frames(float* frames, long fr_stride, int pitch, int W, int H,
+                              const int* __restrict__ grp, int ng) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y;
   if (x >= W) return;
   float* p = frames + (long)y * pitch + x;
-  for (int g = 0, f0 = 0; f0 < N; ++g, f0 += zbin) {
-    const int n = min(zbin, N - f0);
+  for (int g = 0; g < ng; ++g) {
+    const int f0 = grp[g], n = grp[ng + g];
     float s = p[(long)f0 * fr_stride];
     for (int i = 1; i < n; ++i) s += p[(long)(f0 + i) * fr_stride];
     p[(long)g * fr_stride] = s;
   }
 }
 
-int zbin_frames(float* frames, long fr_stride, int pitch, int W, int H, int N, int zbin,
-                cudaStream_t st) {
-  if (zbin < 1 || N < 1) return kEInval;
+int zbin_frames(float* frames, long fr_stride, int pitch, int W, int H, const int* groups,
+                int n_groups, cudaStream_t st) {
+  if (n_groups < 1) return kEInval;
   dim3 grid(ceil_div(W, 128), H);
-  prof::Scope ps("k_zbin_frames", (double)N * W * H * 4.0 + (double)W * H * 4.0 * ((N + zbin - 1) / zbin), st);
-  k_zbin_frames<<<grid, 128, 0, st>>>(frames, fr_stride, pitch, W, H, N, zbin);
+  prof::Scope ps("k_zbin_frames", (double)W * H * 8.0 * n_groups, st);
+  k_zbin_frames<<<grid, 128, 0, st>>>(frames, fr_stride, pitch, W, H, groups, n_groups);
   MC3_CHECK_LAUNCH("k_zbin_frames");
   return kOk;
 }

@@ -40,7 +40,7 @@ void DevBuf::release() {
 }
 
 // ---------------------------------------------------------------------------
-int Geometry::compute(int w, int h, int n, const mc3_params& p) {
+int Geometry::compute(int w, int h, int n, const mc3_params& p, bool file_dose) {
   if (w < 16 || h < 16 || n < 3 || (w & 1) || (h & 1)) return kEInval;
   W = w;
   H = h;
@@ -78,7 +78,7 @@ int Geometry::compute(int w, int h, int n, const mc3_params& p) {
     }
   }
   // CFmIntParam::bDoseWeight / bDWSelectedSum (DataUtil/CFmIntParam.cpp:222-247)
-  dw = !(p.kv < 80 || p.kv > 300) && p.pix_size > 0 && p.fm_dose > 0;
+  dw = !(p.kv < 80 || p.kv > 300) && p.pix_size > 0 && (p.fm_dose > 0 || file_dose);
   dws = dw && p.sum_range[0] >= 0 && p.sum_range[1] > 0 &&
         (p.sum_range[1] - p.sum_range[0]) > 1.0f;
   nSums = 1 + (dw ? 1 : 0) + (dws ? 1 : 0) + (p.split_sum ? 2 : 0);
@@ -214,7 +214,8 @@ int Engine::set_gain(const float* gain, int w, int h, bool on_device) {
 
 int Engine::plan(int w, int h, int n, mc3_plan_info* info) {
   Geometry g;
-  MC3_TRY(g.compute(w, h, n, prm));
+  if (fmint && n != fmint_raw) return kEInval;
+  MC3_TRY(g.compute(w, h, fmint ? fmint_tab.count() : n, prm, fmint && fmint_dose));
   info->n_sums = g.nSums;
   info->n_patches = g.P;
   info->xcf_size[0] = (g.xcfCmpX - 1) * 2;
@@ -376,12 +377,42 @@ int Engine::set_alignment(const mc3_alignment* aln) {
   return kOk;
 }
 
+int Engine::set_frame_integration(const mc3_frame_integration* fi) {
+  if (!fi) {
+    fmint = false;
+    fmint_tab = host::FmInt();
+    return kOk;
+  }
+  if (fi->n_raw < 1 || fi->n_int < 1 || !fi->start || !fi->size || !fi->acc_dose) return kEInval;
+  host::FmInt t;
+  t.start.assign(fi->start, fi->start + fi->n_int);
+  t.size.assign(fi->size, fi->size + fi->n_int);
+  t.acc.assign(fi->acc_dose, fi->acc_dose + fi->n_int);
+  t.dose.assign(fi->n_int, 0.0f);
+  for (int i = 0; i < fi->n_int; ++i)
+    if (t.size[i] < 1 || t.start[i] < 0 || t.start[i] + t.size[i] > fi->n_raw) return kEInval;
+  t.centers();
+  fmint_tab = t;
+  fmint_raw = fi->n_raw;
+  fmint_dose = fi->dose_weight != 0;
+  fmint = true;
+  return kOk;
+}
+
+host::FmInt Engine::frame_tables(int n_raw) const {
+  if (fmint) return fmint_tab;
+  host::FmInt t;
+  t.plain(n_raw, prm.fm_dose);  // CFmIntParam::mSetup
+  return t;
+}
+
 // CCorrectFullShift::mCropFrame (Correct/CCorrectFullShift.cpp:336-356) for
 // all frames at once, then CZbinStack::DoIt (Align/CZbinStack.cpp:27-71):
 // the (shifted) normalised spectra are cropped to the output size, brought
 // to real space by an unnormalised C2R and, with a z-bin above 1, summed in
 // groups of out_stack[1] frames (the last group takes what is left).
-int Engine::write_stack(float2* spec, bool phase, const Geometry& g, mc3_result* out) {
+int Engine::write_stack(float2* spec, bool phase, const Geometry& g, const host::FmInt& fi,
+                        mc3_result* out) {
   const int N = g.N, oW = g.outW, oH = g.outH, ocX = oW / 2 + 1;
   const size_t ncmp = (size_t)g.cmpX * g.cmpY, ocmp = (size_t)ocX * oH;
   cudaStream_t st = stream;
@@ -407,10 +438,14 @@ int Engine::write_stack(float2* spec, bool phase, const Geometry& g, mc3_result*
   MC3_TRY(row_c2r(s, ocX, real, 2 * ocX, oW, oH, br, st));
   int nf = N;
   if (prm.out_stack[1] > 1) {
-    host::FrameGroups G;
-    G.setup(N, prm.out_stack[1]);
+    host::FrameGroups G;  // CFmGroupParam::Setup(OutStack[1], FmIntParam)
+    G.setup(fi, prm.out_stack[1]);
     nf = G.count();
-    MC3_TRY(zbin_frames(real, (long)ocmp * 2, 2 * ocX, oW, oH, N, prm.out_stack[1], st));
+    MC3_TRY(d_zgrp.ensure(sizeof(int) * 2 * nf));
+    std::vector<int> tab(G.start);
+    tab.insert(tab.end(), G.size.begin(), G.size.end());
+    MC3_CUDA(cudaMemcpyAsync(d_zgrp.p, tab.data(), sizeof(int) * 2 * nf, cudaMemcpyHostToDevice, st));
+    MC3_TRY(zbin_frames(real, (long)ocmp * 2, 2 * ocX, oW, oH, d_zgrp.as<int>(), nf, st));
   }
   // every row of every frame lies 2*ocX floats after the previous one
   MC3_CUDA(cudaMemcpy2DAsync(out->stack, sizeof(float) * oW, real, sizeof(float) * 2 * ocX,
@@ -430,7 +465,20 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
   const size_t fbytes = raw_frame_bytes(mv.mode, mv.nx, mv.ny);
   if (!fbytes) return kEUnsupported;
   Geometry g;
-  MC3_TRY(g.compute(mv.nx, mv.ny, mv.nz, prm));
+  if (fmint && mv.nz != fmint_raw) {
+    last_error = "movie frame count differs from the frame-integration table";
+    return kEInval;
+  }
+  const host::FmInt fi = frame_tables(mv.nz);
+  MC3_TRY(g.compute(mv.nx, mv.ny, fi.count(), prm, fmint && fmint_dose));
+  const int Nraw = mv.nz;
+  bool render = false;  // some rendered frame sums several raw frames
+  for (int i = 0; fmint && i < fi.count(); ++i) render = render || fi.size[i] != 1 || fi.start[i] != i;
+  if (render && !(mv.mode == 0 || mv.mode == 5 || mv.mode == 101)) {
+    // the reference renders integrated frames as 8-bit (CLoadCryoEMStack::OpenFile)
+    last_error = "frame integration needs an 8-bit or 4-bit movie";
+    return kEUnsupported;
+  }
   if (has_gain && (gain_w != g.W || gain_h != g.H)) return kEInval;  // CProcessThread::mCheckGain
   const bool loaded = aln_loaded;
   if (loaded && (aln_nz != g.N || aln_P != g.P)) {
@@ -451,7 +499,7 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
   if (!mv.on_device && n_pending > 0) {
     // the oldest prefetched movie must be this one
     const Pending pf = pending[0];
-    if (pf.host != mv.frames || pf.bytes != fbytes * N) {
+    if (pf.host != mv.frames || pf.bytes != fbytes * Nraw) {
       last_error = "movie differs from the oldest prefetched movie";
       return kEInval;
     }
@@ -461,8 +509,8 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
     raw = d_rawslot[pf.slot].p;
     used_slot = pf.slot;
   } else if (!mv.on_device) {
-    MC3_TRY(d_raw.ensure(fbytes * N));
-    MC3_CUDA(cudaMemcpyAsync(d_raw.p, mv.frames, fbytes * N, cudaMemcpyHostToDevice, st));
+    MC3_TRY(d_raw.ensure(fbytes * Nraw));
+    MC3_CUDA(cudaMemcpyAsync(d_raw.p, mv.frames, fbytes * Nraw, cudaMemcpyHostToDevice, st));
     raw = d_raw.p;
   }
   // ---- 2. gain + frame sum (MrcUtil/CApplyRefs.cpp:36-212, CSumFFTStack) ----
@@ -472,8 +520,20 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
   const long fr_stride_f = (long)g.padX * H;
   // raw frame stride in elements of the mode's type (bytes for packed 4-bit)
   const long raw_stride = mv.mode == 101 ? (long)fbytes : (long)npx;
-  MC3_TRY(gain_and_sum(raw, mv.mode, raw_stride, has_gain ? d_gain.as<float>() : nullptr, frames,
-                       fr_stride_f, prm.correct_bad ? d_sum.as<float>() : nullptr, W, H, N, st));
+  if (render) {
+    // CLoadCryoEMStack::mLoadInt / mLoadInt4Bits (MrcUtil/CLoadCryoEMStack.cpp:184-262)
+    // fused with the gain pass
+    MC3_TRY(d_istart.ensure(sizeof(int) * N));
+    MC3_TRY(d_isize.ensure(sizeof(int) * N));
+    MC3_CUDA(cudaMemcpyAsync(d_istart.p, fi.start.data(), sizeof(int) * N, cudaMemcpyHostToDevice, st));
+    MC3_CUDA(cudaMemcpyAsync(d_isize.p, fi.size.data(), sizeof(int) * N, cudaMemcpyHostToDevice, st));
+    MC3_TRY(gain_and_sum_int(raw, mv.mode, raw_stride, d_istart.as<int>(), d_isize.as<int>(),
+                             has_gain ? d_gain.as<float>() : nullptr, frames, fr_stride_f,
+                             prm.correct_bad ? d_sum.as<float>() : nullptr, W, H, N, st));
+  } else {
+    MC3_TRY(gain_and_sum(raw, mv.mode, raw_stride, has_gain ? d_gain.as<float>() : nullptr, frames,
+                         fr_stride_f, prm.correct_bad ? d_sum.as<float>() : nullptr, W, H, N, st));
+  }
   if (used_slot >= 0) MC3_CUDA(cudaEventRecord(slot_free[used_slot], st));  // raw is read only above
   // ---- 3. hot pixels and defects (BadPixel/CDetectMain.cpp, CCorrectMain.cpp) ----
   if (prm.correct_bad) {
@@ -511,7 +571,7 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
   const float bin = fmaxf(g.xcfBin[0], g.xcfBin[1]);
   const float tol = prm.tol / bin;
   host::FrameGroups G0, G1;
-  G0.setup(N, prm.group[0]);
+  G0.setup(fi, prm.group[0]);
   std::vector<host::StackShift> xs;
   std::vector<int> it0;
   std::vector<std::vector<float>> err0;
@@ -613,7 +673,7 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
       fwd.scale = 1.0f;
       MC3_TRY(col_fft(d_pat.as<float2>(), d_pat.as<float2>(), g.patCmpX, g.patCmpX, ph, bpc, fwd, st));
       // ---- 6d. all patch stacks aligned together (Align/CMeasurePatches.cpp:22-84) ----
-      G1.setup(N, prm.group[1]);
+      G1.setup(fi, prm.group[1]);
       std::vector<host::StackShift> ps;
       MC3_TRY(align_stacks(d_pat.as<float2>(), (long)npat * N, P, g.patCmpX, g.patCmpY, N, G1,
                            prm.bft[1], tol, ps, patIters, patErr));
@@ -660,7 +720,7 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
   MC3_TRY(d_acc.ensure(sizeof(float) * N));
   MC3_TRY(d_Wn.ensure(sizeof(float) * ncmp));
   std::vector<float> acc(N);
-  for (int i = 0; i < N; ++i) acc[i] = prm.fm_dose * (i + 1);  // CFmIntParam::mSetup
+  for (int i = 0; i < N; ++i) acc[i] = fi.acc[i];  // CFmIntParam::m_pfAccFmDose
   MC3_CUDA(cudaMemcpyAsync(d_acc.p, acc.data(), sizeof(float) * N, cudaMemcpyHostToDevice, st));
   DoseParams dp{};
   dp.enabled = g.dw ? 1 : 0;
@@ -673,7 +733,9 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
   if (g.dw) {
     // The normalisation depends only on the geometry and the dose options,
     // so it is rebuilt only when they change between movies.
-    const double key[6] = {(double)g.cmpX, (double)g.cmpY, (double)N, prm.fm_dose, dp.pix_size,
+    double acc_key = 0.0;  // the dose table enters through the accumulated doses
+    for (int i = 0; i < N; ++i) acc_key += (double)acc[i] * (i + 1);
+    const double key[6] = {(double)g.cmpX, (double)g.cmpY, (double)N, acc_key, dp.pix_size,
                            dp.kv_factor};
     if (!wn_valid || std::memcmp(key, wn_key, sizeof(key)) != 0 || d_Wn.cap < sizeof(float) * ncmp) {
       MC3_TRY(dose_norm(d_acc.as<float>(), N, g.cmpX, g.cmpY, dp.pix_size, dp.kv_factor,
@@ -686,7 +748,7 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
   if (!g.patch) {
     MC3_TRY(frame_sums(spec, (long)ncmp, N, g.cmpX, g.cmpY, d_fex.as<float2>(), d_fey.as<float2>(),
                        d_acc.as<float>(), d_Wn.as<float>(), dp, d_sums.as<float2>(), g.nSums, st));
-    if (want_stack) MC3_TRY(write_stack(spec, true, g, out));  // spectra are not needed after
+    if (want_stack) MC3_TRY(write_stack(spec, true, g, fi, out));  // spectra are not needed after
   } else {
     // Correct/GCorrectPatchShift.cu:97-285: per frame C2R -> gather -> R2C
     const int P = g.P;
@@ -727,7 +789,7 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
     }
     MC3_TRY(frame_sums(spec, (long)ncmp, N, g.cmpX, g.cmpY, nullptr, nullptr, d_acc.as<float>(),
                        d_Wn.as<float>(), dp, d_sums.as<float2>(), g.nSums, st));
-    if (want_stack) MC3_TRY(write_stack(spec, false, g, out));
+    if (want_stack) MC3_TRY(write_stack(spec, false, g, fi, out));
   }
   if (out && !want_stack) out->stack_frames = 0;
   // ---- 8. sums to real space (CCorrectFullShift::mUnpadSums,

@@ -37,7 +37,8 @@ struct Geometry {
   bool dw = false, dws = false;
   int nSums = 1;
   int outW = 0, outH = 0;  // output sum size after -FtBin
-  int compute(int w, int h, int n, const mc3_params& p);
+  // n: rendered frames; file_dose: a frame-integration file gave a dose
+  int compute(int w, int h, int n, const mc3_params& p, bool file_dose = false);
 };
 
 class Engine {
@@ -54,10 +55,14 @@ class Engine {
   int prefetch(const mc3_movie& mv);
   // Known alignment used instead of measuring (NULL clears it).
   int set_alignment(const mc3_alignment* aln);
+  int set_frame_integration(const mc3_frame_integration* fi);
+  // Rendered-frame tables of a movie of n_raw raw frames.
+  host::FmInt frame_tables(int n_raw) const;
   // -OutStack: the corrected frames (spectra `spec`, phase tables when
   // `phase`) cropped to the output size, to real space, z-binned, copied to
   // out->stack.
-  int write_stack(float2* spec, bool phase, const Geometry& g, mc3_result* out);
+  int write_stack(float2* spec, bool phase, const Geometry& g, const host::FmInt& fi,
+                  mc3_result* out);
 
   // Batched CIterativeAlign over `nstack` stacks of N spectra each.
   int align_stacks(const float2* spec, long stack_stride, int nstack, int cmpX, int cmpY, int N,
@@ -95,11 +100,17 @@ class Engine {
   DevBuf d_xcf, d_sh, d_ex, d_ey, d_S, d_T, d_win, d_gsh, d_act, d_gstart, d_gsize;
   DevBuf d_pat, d_patoff, d_bsum, d_bimg, d_btmp, d_bmap, d_scal;
   DevBuf d_fex, d_fey, d_Wn, d_acc, d_sums, d_real, d_gath, d_pcent, d_pshift, d_pbad, d_pmask, d_out, d_bsums;
-  DevBuf d_stk;
+  DevBuf d_stk, d_zgrp;
   // loaded alignment (mc3_set_alignment)
   bool aln_loaded = false;
   int aln_nz = 0, aln_P = 0;
   std::vector<float> aln_global, aln_patch, aln_centers;
+  // frame integration (mc3_set_frame_integration)
+  bool fmint = false;
+  int fmint_raw = 0;
+  bool fmint_dose = false;
+  host::FmInt fmint_tab;
+  DevBuf d_istart, d_isize;
   bool has_gain = false;
   double wn_key[6] = {0, 0, 0, 0, 0, 0};  // geometry and dose options of d_Wn
   bool wn_valid = false;

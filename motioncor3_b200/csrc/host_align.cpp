@@ -2,37 +2,150 @@
 #include "host_align.h"
 
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <math.h>
 
 namespace mc3 {
 namespace host {
 
-// ---- DataUtil/CFmGroupParam.cpp:26-78 (one raw frame per frame) ----------
+// ---- DataUtil/CFmIntParam.cpp ------------------------------------------------
+void FmInt::plain(int n_raw, float fm_dose) {
+  start.resize(n_raw);
+  size.assign(n_raw, 1);
+  dose.assign(n_raw, fm_dose);
+  acc.resize(n_raw);
+  for (int i = 0; i < n_raw; ++i) {
+    start[i] = i;
+    acc[i] = fm_dose * (i + 1);
+  }
+  centers();
+}
+
+void FmInt::integrate(const std::vector<int>& gsz_in, const std::vector<int>& isz, float raw_dose,
+                      int n_raw) {
+  const int ne = (int)gsz_in.size();
+  std::vector<int> gsz(gsz_in), nint(ne, 0);
+  int count = 0;
+  for (int i = 0; i < ne; ++i) count += gsz[i];
+  // more frames in the file than in the movie: take them off the last
+  // entries first; fewer: the last entry gets the rest (:150-161)
+  int extra = count - n_raw;
+  const int last = ne - 1;
+  if (extra > 0) {
+    for (int i = last; i >= 0; --i) {
+      const int g = gsz[i];
+      gsz[i] -= extra;
+      if (gsz[i] <= 0) gsz[i] = 0;
+      else extra = extra - g;
+      if (extra <= 0) break;
+    }
+  } else if (extra < 0) {
+    gsz[last] -= extra;
+  }
+  // leftovers of an entry move to the next one (:165-173)
+  for (int i = 0; i < last; ++i) {
+    nint[i] = gsz[i] / isz[i];
+    gsz[i + 1] += gsz[i] % isz[i];
+  }
+  extra = gsz[last] % isz[last];
+  nint[last] = gsz[last] / isz[last];
+  int n = 0;
+  for (int i = 0; i < ne; ++i) n += nint[i];
+  size.assign(n, 0);
+  start.assign(n, 0);
+  int c = 0;
+  for (int i = 0; i < ne; ++i)
+    for (int k = 0; k < nint[i]; ++k) size[c++] = isz[i];
+  // the last rendered frames take one leftover raw frame each (:189-193)
+  for (int i = 0; i < extra; ++i) size[n - 1 - i] += 1;
+  for (int i = 1; i < n; ++i) start[i] = start[i - 1] + size[i - 1];
+  dose.resize(n);
+  acc.resize(n);
+  for (int i = 0; i < n; ++i) dose[i] = size[i] * raw_dose;
+  if (n > 0) acc[0] = dose[0];
+  for (int i = 1; i < n; ++i) acc[i] = acc[i - 1] + dose[i];
+  centers();
+}
+
+void FmInt::centers() {
+  center.resize(start.size());
+  for (size_t i = 0; i < start.size(); ++i) center[i] = start[i] + 0.5f * (size[i] - 1.0f);
+}
+
+bool read_fmint_file(const char* path, float cli_fm_dose, std::vector<int>& gs,
+                     std::vector<int>& is, std::vector<float>& ds) {
+  gs.clear();
+  is.clear();
+  ds.clear();
+  FILE* f = std::fopen(path, "rt");
+  if (!f) return false;
+  char buf[256] = {0};
+  int g = 0, n = 0;
+  float d = 0.0f;
+  if (!std::fgets(buf, sizeof(buf), f)) buf[0] = 0;
+  int items = std::sscanf(buf, "%d  %d  %f", &g, &n, &d);
+  bool ok = items >= 2;
+  const bool two = items == 2;
+  if (two) d = cli_fm_dose;
+  while (ok) {
+    gs.push_back(g);
+    is.push_back(n);
+    ds.push_back(d);
+    if (std::feof(f)) break;
+    if (!std::fgets(buf, sizeof(buf), f)) break;
+    if (two) {
+      if (std::sscanf(buf, "%d  %d", &g, &n) != 2) continue;
+    } else {
+      // the reference compares (==) instead of assigning here, so a line
+      // that does not scan leaves the previous values, which are pushed again
+      std::sscanf(buf, "%d  %d  %f", &g, &n, &d);
+      if (d < 0) ok = false;
+    }
+  }
+  std::fclose(f);
+  for (size_t i = 1; i < ds.size(); ++i)
+    if (ds[i] != ds[0]) {  // various frame doses: no integration (:160-169)
+      gs.clear();
+      is.clear();
+      ds.clear();
+      break;
+    }
+  return true;
+}
+
+// ---- DataUtil/CFmGroupParam.cpp:26-78 ----------------------------------------
 void FrameGroups::setup(int n_frames, int bin_z) {
+  FmInt fi;
+  fi.plain(n_frames, 0.0f);
+  setup(fi, bin_z);
+}
+
+void FrameGroups::setup(const FmInt& fi, int bin_z) {
   binZ = bin_z;
   start.clear();
   size.clear();
   center.clear();
-  const int max_raw = bin_z;  // binZ * smallest integrated-frame size (1)
+  fm_center = fi.center;
+  const int n = fi.count();
+  int min_raw = 2147483647;  // (int)1e20 in the reference, which g++ folds to INT_MAX
+  for (int i = 0; i < n; ++i) min_raw = fi.size[i] < min_raw ? fi.size[i] : min_raw;
+  const int max_raw = bin_z * min_raw;  // mFindMaxGroupRawFms
   int f = 0;
-  while (f < n_frames) {
+  while (f < n) {  // mGroupByRawSize
     start.push_back(f);
     int sz = 0, raw = 0;
     for (;;) {
-      raw += 1;
+      raw += fi.size[f];
       sz += 1;
       f += 1;
-      if (f >= n_frames || raw >= max_raw) break;
+      if (f >= n || raw >= max_raw) break;
     }
     size.push_back(sz);
   }
   for (size_t g = 0; g < start.size(); ++g) {
     float acc = 0.0f;
-    for (int i = 0; i < size[g]; ++i) {
-      // frame centre = start + 0.5*(size-1) with size 1 (CFmIntParam.cpp:423-429)
-      acc += (float)(start[g] + i) + 0.5f * (1 - 1.0f);
-    }
+    for (int i = 0; i < size[g]; ++i) acc += fi.center[start[g] + i];
     center.push_back(acc / size[g]);
   }
 }
@@ -95,7 +208,7 @@ StackShift interpolate(const StackShift& grp, const FrameGroups& g, int n_frames
     return out;
   }
   for (int i = 0; i < n_frames; ++i) {
-    const float fc = (float)i;
+    const float fc = g.fm_center[i];  // CFmIntParam::m_pfIntFmCents
     int k = ng - 1;
     if (fc <= g.center[0]) {
       k = 1;

@@ -8,13 +8,40 @@
 namespace mc3 {
 namespace host {
 
-// Frame groups of -Group binZ (DataUtil/CFmGroupParam.cpp:26-78) for movies
-// without a frame-integration file: consecutive runs of binZ frames.
+// Rendered (integrated) frames of a movie (DataUtil/CFmIntParam.cpp): raw
+// frames start[i] .. start[i]+size[i]-1 are summed into frame i, which
+// carries dose[i] and the accumulated dose acc[i]; its time stamp is
+// center[i] = start + (size - 1)/2 in raw frames.
+struct FmInt {
+  std::vector<int> start, size;
+  std::vector<float> dose, acc, center;
+  int count() const { return (int)start.size(); }
+  // CFmIntParam::mSetup (:118-136): one raw frame per rendered frame.
+  void plain(int n_raw, float fm_dose);
+  // CFmIntParam::mCalcIntFms (:138-229) from frame-integration entries
+  // (raw frames, raw frames per rendered frame, raw-frame dose).
+  void integrate(const std::vector<int>& group_size, const std::vector<int>& int_size,
+                 float raw_dose, int n_raw);
+  void centers();  // CFmIntParam::mCalcIntFmCenters (:276-283)
+};
+
+// CReadFmIntFile::DoIt (DataUtil/CReadFmIntFile.cpp:104-170): the entries
+// of a frame-integration file, with the reference's parsing (a line that
+// does not scan repeats the previous entry in the three-column form; mixed
+// doses discard the file).  Returns false when the file cannot be opened.
+bool read_fmint_file(const char* path, float cli_fm_dose, std::vector<int>& group_size,
+                     std::vector<int>& int_size, std::vector<float>& dose);
+
+// Frame groups of -Group binZ (DataUtil/CFmGroupParam.cpp:26-78): runs of
+// rendered frames holding binZ x (smallest rendered-frame size) raw frames;
+// group centres are the mean time stamps of their frames.
 struct FrameGroups {
   int binZ = 1;
   std::vector<int> start, size;
   std::vector<float> center;
-  void setup(int n_frames, int bin_z);
+  std::vector<float> fm_center;  // time stamp of every rendered frame
+  void setup(int n_frames, int bin_z);  // one raw frame per rendered frame
+  void setup(const FmInt& fi, int bin_z);
   int count() const { return (int)start.size(); }
 };
 

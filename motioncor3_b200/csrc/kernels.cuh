@@ -10,6 +10,11 @@ namespace mc3 {
 // mode: MRC pixel mode (0 u8, 1 i16, 2 f32, 6 u16).  frames: padded stack.
 int gain_and_sum(const void* raw, int mode, long raw_stride, const float* gain, float* frames,
                  long fr_stride, float* sum, int W, int H, int N, cudaStream_t st);
+// The same with frame integration (modes 0, 5, 101): rendered frame f sums
+// raw frames start[f] .. start[f]+size[f]-1 modulo 256 (device tables).
+int gain_and_sum_int(const void* raw, int mode, long raw_stride, const int* start,
+                     const int* size, const float* gain, float* frames, long fr_stride, float* sum,
+                     int W, int H, int N, cudaStream_t st);
 int moment_grid(int W, int H);
 int image_moment(const float* img, int W, int H, long pitch, int iExp, float* d_part,
                  float* d_out, cudaStream_t st);
@@ -83,10 +88,10 @@ int patch_masks(const uint8_t* bad, const float2* shifts, int P, int nb,
 int crop_frames(const float2* in, int inX, int inY, long in_stride, const float2* ex,
                 const float2* ey, float2* out, int outX, int outY, long out_stride, int N,
                 cudaStream_t st);
-// In-place group sums of N real frames (groups of zbin, last shorter) into
-// the first ceil(N/zbin) frames.
-int zbin_frames(float* frames, long fr_stride, int pitch, int W, int H, int N, int zbin,
-                cudaStream_t st);
+// In-place group sums of real frames into the first n_groups frames;
+// groups: device [2][n_groups] (starts, then sizes) of consecutive groups.
+int zbin_frames(float* frames, long fr_stride, int pitch, int W, int H, const int* groups,
+                int n_groups, cudaStream_t st);
 // out[y*W+x] = max(0, in[y*pitch+x])
 int unpad_positive(const float* in, long pitch, float* out, int W, int H, int n,
                    long in_stride, cudaStream_t st);

@@ -68,6 +68,60 @@ int gain_and_sum(const void* raw, int mode, long raw_stride, const float* gain, 
   return kOk;
 }
 
+// Frame integration fused with the gain pass: rendered frame i is the sum of
+// raw frames start[i] .. start[i]+size[i]-1 in 8-bit arithmetic (the
+// reference adds raw frames into an unsigned-char rendered frame,
+// Util/GAddFrames.cu mGAddUChar, so the sum wraps modulo 256;
+// MrcUtil/CLoadCryoEMStack.cpp:184-262), then converted and gain-multiplied
+// as an 8-bit frame.  PACKED: 4-bit raw frames (mode 101) unpacked first.
+template <bool PACKED>
+__global__ void k_gain_sum_int(const uint8_t* __restrict__ raw, long raw_stride,
+                               const int* __restrict__ start, const int* __restrict__ size,
+                               const float* __restrict__ gain, float* frames, long fr_stride,
+                               float* sum, int W, int H, int N, int padX) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= W) return;
+  const long off = PACKED ? (long)y * ((W + 1) / 2) + x / 2 : (long)y * W + x;
+  const float g = gain ? gain[(long)y * W + x] : 1.0f;
+  float s = 0.0f;
+  for (int f = 0; f < N; ++f) {
+    const int r0 = start[f], nr = size[f];
+    unsigned acc = 0;
+    for (int k = 0; k < nr; ++k) {
+      unsigned b = raw[(long)(r0 + k) * raw_stride + off];
+      if (PACKED) b = ((x & 1) ? (b >> 4) : b) & 0xfu;
+      acc += b;
+    }
+    float v = (float)(acc & 0xffu);
+    if (gain) v *= g;
+    frames[(long)f * fr_stride + (long)y * padX + x] = v;
+    s += v;
+  }
+  if (sum) sum[(long)y * padX + x] = s;
+}
+
+int gain_and_sum_int(const void* raw, int mode, long raw_stride, const int* start,
+                     const int* size, const float* gain, float* frames, long fr_stride, float* sum,
+                     int W, int H, int N, cudaStream_t st) {
+  const int padX = 2 * (W / 2 + 1);
+  dim3 grid(ceil_div(W, 256), H);
+  prof::Scope ps("k_gain_sum_int", (double)W * H * N * 4.0, st);  // rendered-frame writes
+  switch (mode) {
+    case 101:
+      k_gain_sum_int<true><<<grid, 256, 0, st>>>((const uint8_t*)raw, raw_stride, start, size, gain,
+                                                 frames, fr_stride, sum, W, H, N, padX);
+      break;
+    case 0: case 5:
+      k_gain_sum_int<false><<<grid, 256, 0, st>>>((const uint8_t*)raw, raw_stride, start, size,
+                                                  gain, frames, fr_stride, sum, W, H, N, padX);
+      break;
+    default: return kEUnsupported;
+  }
+  MC3_CHECK_LAUNCH("k_gain_sum_int");
+  return kOk;
+}
+
 // ---- moments with the reference's reduction order ------------------------
 // GCalcMoment2D::DoIt (Util/GCalcMoment2D.cu:10-60, 96-114): grid-stride
 // per-thread FP32 sums, shared-memory tree, per-block division by W*H, then

@@ -223,34 +223,43 @@ Geo make_geo(int W, int H, int N, const oracle_params* p) {
 // ======================================================================
 struct Groups {
   std::vector<int> start, size;
-  std::vector<float> center;
+  std::vector<float> center;     // group centres
+  std::vector<float> fm_center;  // rendered-frame time stamps
   int binZ;
 };
 
-Groups make_groups(int N, int binZ) {
+// CFmGroupParam::Setup (DataUtil/CFmGroupParam.cpp:26-78) over rendered
+// frames of int_size raw frames each (all 1 when int_size is NULL), whose
+// time stamps are start + 0.5*(size-1) (CFmIntParam.cpp:276-283).
+Groups make_groups(int N, int binZ, const int* int_size = nullptr) {
   Groups G;
   G.binZ = binZ;
-  const int maxRaw = binZ * 1;  // every integrated frame holds one raw frame
+  std::vector<int> sz(N, 1);
+  if (int_size) sz.assign(int_size, int_size + N);
+  G.fm_center.resize(N);
+  int raw0 = 0, minRaw = sz.empty() ? 1 : sz[0];
+  for (int i = 0; i < N; ++i) {
+    G.fm_center[i] = raw0 + 0.5f * (sz[i] - 1.0f);
+    raw0 += sz[i];
+    minRaw = std::min(minRaw, sz[i]);
+  }
+  const int maxRaw = binZ * minRaw;
   int f = 0;
   while (f < N) {
     G.start.push_back(f);
-    int sz = 0, raw = 0;
+    int n = 0, raw = 0;
     while (true) {
-      raw += 1;
-      sz += 1;
+      raw += sz[f];
+      n += 1;
       f += 1;
       if (f >= N) break;
       if (raw >= maxRaw) break;
     }
-    G.size.push_back(sz);
+    G.size.push_back(n);
   }
   for (size_t g = 0; g < G.start.size(); ++g) {
     float s = 0.0f;
-    for (int i = 0; i < G.size[g]; ++i) {
-      const int fm = G.start[g] + i;
-      const float cent = fm + 0.5f * (1 - 1.0f);  // start + 0.5*(size-1)
-      s += cent;
-    }
+    for (int i = 0; i < G.size[g]; ++i) s += G.fm_center[G.start[g] + i];
     G.center.push_back(s / G.size[g]);
   }
   return G;
@@ -465,7 +474,7 @@ Shifts interpolate(Shifts& grp, const Groups& G, int nFrames, bool nearest) {
     return out;
   }
   for (int i = 0; i < nFrames; ++i) {
-    const float fc = (float)i;  // frame centres (CFmIntParam.cpp:423-429)
+    const float fc = G.fm_center[i];  // frame time stamps (CFmIntParam.cpp:276-283)
     int g;
     if (fc <= G.center[0]) g = 1;
     else {
@@ -1047,6 +1056,9 @@ void oracle_default_params(oracle_params* p) {
   p->ft_bin = 1.0f;
   p->out_stack[0] = 0;
   p->out_stack[1] = 1;
+  p->int_size = nullptr;
+  p->acc_dose = nullptr;
+  p->dose_weight = 0;
 }
 
 void oracle_rfft2(const double* img, double* spec, int W, int H, int normalise) {
@@ -1161,7 +1173,7 @@ int oracle_process_movie(const oracle_params* p, const float* frames, int W, int
   const bool forced = out->use_global_shifts != nullptr;
   const float bin = std::fmax(g.xcfBin[0], g.xcfBin[1]);
   const float tol = p->tol / bin;
-  Groups G0 = make_groups(N, p->group[0]);
+  Groups G0 = make_groups(N, p->group[0], p->int_size);
   Shifts xs(N);  // xcf units
   if (!forced) {
     AlignResult ga = iterative_align(xcf.data(), g.xcfCmpX, g.xcfCmpY, N, G0, p->iter, tol,
@@ -1242,7 +1254,7 @@ int oracle_process_movie(const oracle_params* p, const float* frames, int W, int
     const long npat = (long)g.patCmpX * g.patCmpY;
     patShift.assign((size_t)N * P * 2, 0.f);
     patCent.assign((size_t)P * 2, 0.f);
-    Groups G1 = make_groups(N, p->group[1]);
+    Groups G1 = make_groups(N, p->group[1], p->int_size);
     for (int pi = 0; pi < P; ++pi) {
       std::vector<cd> pspec((long)N * npat);
       std::vector<double> win((long)pw * ph);
@@ -1274,13 +1286,14 @@ int oracle_process_movie(const oracle_params* p, const float* frames, int W, int
 
   // ---- correction and sums (Correct/CCorrectFullShift.cpp,
   //      Correct/GCorrectPatchShift.cu) ----
-  const bool dw = !(p->kv < 80 || p->kv > 300) && p->pix_size > 0 && p->fm_dose > 0;
+  const bool dw = !(p->kv < 80 || p->kv > 300) && p->pix_size > 0 &&
+                  (p->fm_dose > 0 || p->dose_weight);
   const bool dws = dw && p->sum_range[0] >= 0 && p->sum_range[1] > 0 &&
                    (p->sum_range[1] - p->sum_range[0]) > 1.0f;
   const int nBase = 1 + (dw ? 1 : 0) + (dws ? 1 : 0);
   const int nSums = nBase + (p->split_sum ? 2 : 0);
   std::vector<float> acc(N);
-  for (int i = 0; i < N; ++i) acc[i] = p->fm_dose * (i + 1);
+  for (int i = 0; i < N; ++i) acc[i] = p->acc_dose ? p->acc_dose[i] : p->fm_dose * (i + 1);
   std::vector<double> wsum;
   double kvf = kv_factor(p->kv);
   if (dw) {
@@ -1371,9 +1384,10 @@ int oracle_process_movie(const oracle_params* p, const float* frames, int W, int
     // CZbinStack::DoIt (Align/CZbinStack.cpp:27-71): FP32 sums in frame
     // order, groups of out_stack[1] frames, the last one shorter
     const int zb = p->out_stack[1] > 1 ? p->out_stack[1] : 1;
+    Groups Z = make_groups(N, zb, p->int_size);
     int ng = 0;
-    for (int f0 = 0; f0 < N; f0 += zb, ++ng) {
-      const int n = std::min(zb, N - f0);
+    for (; ng < (int)Z.start.size(); ++ng) {
+      const int f0 = Z.start[ng], n = Z.size[ng];
       float* dst = out->stack + (long)ng * opx;
       for (long i = 0; i < opx; ++i) {
         float v = out->stack[(long)f0 * opx + i];

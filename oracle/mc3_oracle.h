@@ -40,6 +40,12 @@ typedef struct {
   int split_sum;      /* -SplitSum: odd and even frame sums after the others */
   float ft_bin;       /* -FtBin: Fourier binning of the output sums        */
   int out_stack[2];   /* -OutStack: aligned frames wanted, z-bin            */
+  /* Rendered frames of a frame-integration file (NULL: one raw frame per
+   * frame): raw frames per rendered frame [N] and the accumulated dose [N];
+   * dose_weight turns dose weighting on without fm_dose. */
+  const int* int_size;
+  const float* acc_dose;
+  int dose_weight;
 } oracle_params;
 
 typedef struct {

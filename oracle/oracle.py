@@ -70,6 +70,9 @@ class OracleParams(ctypes.Structure):
         ("split_sum", ctypes.c_int),
         ("ft_bin", ctypes.c_float),
         ("out_stack", ctypes.c_int * 2),
+        ("int_size", _VP),
+        ("acc_dose", _VP),
+        ("dose_weight", ctypes.c_int),
     ]
 
 
@@ -120,10 +123,21 @@ def params(**kw) -> OracleParams:
     return p
 
 
-def process_movie(frames: np.ndarray, gain=None, force=None, **kw) -> dict:
+def process_movie(frames: np.ndarray, gain=None, force=None, int_size=None, acc_dose=None,
+                  **kw) -> dict:
     """Runs the whole oracle path.  `force` may hold global_shifts (and
-    patch_shifts / patch_centers / patch_bad) to correct with given shifts."""
+    patch_shifts / patch_centers / patch_bad) to correct with given shifts;
+    int_size / acc_dose describe rendered frames of a frame-integration file."""
     p = params(**kw)
+    tabs = []
+    if int_size is not None:
+        isz = np.ascontiguousarray(int_size, np.int32)
+        tabs.append(isz)
+        p.int_size = isz.ctypes.data
+    if acc_dose is not None:
+        acc = np.ascontiguousarray(acc_dose, np.float32)
+        tabs.append(acc)
+        p.acc_dose = acc.ctypes.data
     nz, ny, nx = frames.shape
     fr = np.ascontiguousarray(frames, np.float32)
     g = None if gain is None else np.ascontiguousarray(gain, np.float32)

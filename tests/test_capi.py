@@ -5,6 +5,7 @@ import ctypes
 import os
 import re
 
+import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -62,3 +63,92 @@ def test_bad_arguments_rejected(mc3lib):
     assert mc3lib.mc3_create(ctypes.byref(p), ctypes.byref(h)) == api.MC3_EINVAL
     assert mc3lib.mc3_destroy(None) == api.MC3_EINVAL
     assert mc3lib.mc3_fft_forward(None, 64, 64, 1, 1, None) == api.MC3_EINVAL
+
+
+def _write(tmp_path, name, text):
+    f = tmp_path / name
+    f.write_text(text)
+    return str(f)
+
+
+def test_read_fmint_file_parsing(mc3lib, tmp_path):
+    """CReadFmIntFile::DoIt (DataUtil/CReadFmIntFile.cpp:104-170)."""
+    from motioncor3_b200 import api
+    g, n, d = api.read_fmint_file(_write(tmp_path, "a.txt", "40 4 0.5\n20 2 0.5\n"), 9.0)
+    assert g.tolist() == [40, 20] and n.tolist() == [4, 2] and np.allclose(d, 0.5)
+    # two columns: the raw-frame dose is -FmDose
+    g, n, d = api.read_fmint_file(_write(tmp_path, "b.txt", "40 4\n10 1\n"), 0.7)
+    assert g.tolist() == [40, 10] and n.tolist() == [4, 1] and np.allclose(d, 0.7)
+    # three columns: a line that does not scan repeats the previous entry
+    # (the reference compares the scan count instead of assigning it)
+    g, n, d = api.read_fmint_file(_write(tmp_path, "c.txt", "40 4 0.5\n\n20 2 0.5\n"), 0.0)
+    assert g.tolist() == [40, 40, 20]
+    # different raw-frame doses: the file is dropped
+    g, n, d = api.read_fmint_file(_write(tmp_path, "d.txt", "40 4 0.5\n20 2 0.6\n"), 0.0)
+    assert len(g) == 0
+    with pytest.raises(api.MC3Error):
+        api.read_fmint_file(str(tmp_path / "missing.txt"), 0.0)
+
+
+def _tables(entries, n_raw, fm_dose=0.0):
+    """Independent restatement of CFmIntParam::mCalcIntFms (DataUtil/CFmIntParam.cpp:138-229)."""
+    gs = [e[0] for e in entries]
+    isz = [e[1] for e in entries]
+    extra = sum(gs) - n_raw
+    if extra > 0:
+        for i in range(len(gs) - 1, -1, -1):
+            g0 = gs[i]
+            gs[i] -= extra
+            if gs[i] <= 0:
+                gs[i] = 0
+            else:
+                extra -= g0
+            if extra <= 0:
+                break
+    elif extra < 0:
+        gs[-1] -= extra
+    nint = []
+    for i in range(len(gs) - 1):
+        nint.append(gs[i] // isz[i])
+        gs[i + 1] += gs[i] % isz[i]
+    left = gs[-1] % isz[-1]
+    nint.append(gs[-1] // isz[-1])
+    size = [isz[i] for i in range(len(gs)) for _ in range(nint[i])]
+    for i in range(left):
+        size[len(size) - 1 - i] += 1
+    start = [0]
+    for s in size[:-1]:
+        start.append(start[-1] + s)
+    acc = np.cumsum(np.float32(entries[0][2]) * np.array(size, np.float32), dtype=np.float32)
+    return start, size, acc
+
+
+@pytest.mark.parametrize("entries,n_raw", [([(40, 4, 0.5)], 40), ([(40, 4, 0.5)], 42),
+                                           ([(40, 4, 0.5)], 37),
+                                           ([(20, 2, 0.25), (30, 3, 0.25)], 50),
+                                           ([(21, 2, 0.25), (30, 3, 0.25)], 51),
+                                           ([(21, 2, 0.25), (30, 3, 0.25)], 44)])
+def test_frame_integration_tables(mc3lib, entries, n_raw):
+    """CFmIntParam::Setup with a frame-integration file: rendered frames,
+    leftovers moved to the next entry and spread over the last frames."""
+    from motioncor3_b200 import api
+    e = ([x[0] for x in entries], [x[1] for x in entries], [x[2] for x in entries])
+    t = api.frame_integration_tables(e, n_raw)
+    start, size, acc = _tables(entries, n_raw)
+    assert t["size"].tolist() == size and t["start"].tolist() == start
+    assert sum(size) == n_raw
+    assert np.allclose(t["acc_dose"], acc, rtol=1e-6)
+    assert t["dose_weight"] == 1
+
+
+def test_frame_integration_tables_without_integration(mc3lib):
+    """All integration sizes 1 (or no file): one raw frame per frame with
+    -FmDose (CFmIntParam::mSetup); the file's dose still turns dose
+    weighting on (CFmIntParam::bDoseWeight)."""
+    from motioncor3_b200 import api
+    t = api.frame_integration_tables(([30], [1], [0.8]), 30, fm_dose=1.5)
+    assert t["size"].tolist() == [1] * 30 and t["start"].tolist() == list(range(30))
+    assert np.allclose(t["acc_dose"], 1.5 * np.arange(1, 31, dtype=np.float32))
+    assert t["dose_weight"] == 1
+    t = api.frame_integration_tables(None, 12, fm_dose=0.0)
+    assert t["dose_weight"] == 0 and len(t["size"]) == 12

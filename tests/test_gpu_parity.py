@@ -344,6 +344,46 @@ def test_pipeline_four_bit_frames(api, torch_cuda, nx):
         assert np.array_equal(a.sums[i], b.sums[i])
 
 
+def _render(raw, size):
+    """Rendered frames of the reference's 8-bit integration (sums mod 256)."""
+    out, r = [], 0
+    for n in size:
+        out.append(raw[r:r + n].astype(np.uint32).sum(axis=0) % 256)
+        r += n
+    return np.stack(out).astype(np.float32)
+
+
+@pytest.mark.parametrize("packed,high", [(False, False), (False, True), (True, False)])
+def test_pipeline_frame_integration(api, oracle, torch_cuda, packed, high):
+    """-FmIntFile: 26 raw frames rendered as 3+3+...(+leftovers) frames
+    (CFmIntParam::mCalcIntFms), summed modulo 256 as the reference's 8-bit
+    rendered stack (high: counts that wrap), then aligned with groups by
+    raw-frame count and dose-weighted by the file's dose; against the
+    oracle run on the rendered frames with the same tables."""
+    from motioncor3_b200 import mrcio, synthetic as S
+    m = S.make_movie(384, 320, 26, dose=1.0, seed=43, gain=False)
+    raw = np.minimum(np.asarray(m.frames), 15).astype(np.uint8)
+    if high:
+        raw = (raw.astype(np.uint16) * 17 + 40).astype(np.uint8)  # rendered sums wrap
+    tabs = api.frame_integration_tables(([26], [3], [0.4]), 26)
+    assert tabs["size"].tolist() == [3] * 6 + [4, 4]
+    p = api.Params(iter=6, tol=0.2, bft=(300, 100), pix_size=0.9, kv=300, group=(2, 4))
+    with api.MotionCor3(p) as mc:
+        mc.set_frame_integration(tabs, n_raw=26)
+        res = mc.process(mrcio.pack4(raw) if packed else raw, nx4=384 if packed else None)
+    assert res.n_sums == 3 and res.global_shifts.shape == (8, 2)
+    rend = _render(raw, tabs["size"])
+    kw = dict(iter=6, tol=0.2, bft=(300, 100), pix_size=0.9, kv=300, group=(2, 4),
+              dose_weight=1)
+    orc = oracle.process_movie(rend, int_size=tabs["size"], acc_dose=tabs["acc_dose"], **kw)
+    assert np.abs(res.global_shifts - orc["global_shifts"]).max() <= 0.05
+    same = oracle.process_movie(rend, int_size=tabs["size"], acc_dose=tabs["acc_dose"],
+                                force=dict(global_shifts=res.global_shifts), **kw)
+    for i in range(res.n_sums):
+        e = _rel_rms(res.sums[i], same["sums"][i])
+        assert e <= 1e-4, (i, e)
+
+
 def test_pipeline_config1_full_size(api, oracle, torch_cuda):
     """40 frames of 1024x1024, global alignment only (-Patch 0 0 -Iter 7
     -Tol 0.5 -Bft 150 -PixSize 1.0), dose 1 e/px/frame, unit gain."""
