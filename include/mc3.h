@@ -159,6 +159,10 @@ int mc3_host_free(void* ptr);
 /* Gain reference [ny][nx] float (CLoadRefs::LoadGain, CLoadRefs.cpp:82-95);
  * NULL clears it. */
 int mc3_set_gain(mc3_ctx* ctx, const float* gain, int nx, int ny, int on_device);
+/* Dark reference [ny][nx] float (CLoadRefs::LoadDark, CLoadRefs.cpp:161-202),
+ * subtracted before the gain multiplication (GApplyRefsToFrame,
+ * MrcUtil/GApplyRefsToFrame.cu:56-72); NULL clears it. */
+int mc3_set_dark(mc3_ctx* ctx, const float* dark, int nx, int ny, int on_device);
 
 /* ---- whole path ---- */
 /* One movie from raw frames to sums and shift tables: replaces
@@ -265,6 +269,17 @@ int mc3_profile_read(char* buf, size_t len, int reset);
 unsigned long long mc3_kernel_launches(void);
 
 /* ---- host-side bookkeeping (host pointers) ---- */
+/* CLoadRefs::PostProcess (CLoadRefs.cpp:204-229): rotation by rot x 90
+ * degrees (G90Rotate2D, nearest pixel about the centre; odd factors swap the
+ * size), flip (1 upside down, 2 left-right; GFlip2D), then 1/v with 0 kept
+ * (GInverse2D) when inverse is set; out holds nx*ny floats and receives the
+ * image at its new size *out_nx x *out_ny. */
+int mc3_ref_orient(const float* in, int nx, int ny, int rot, int flip, int inverse, float* out,
+                   int* out_nx, int* out_ny);
+/* CLoadRefs::AugmentRefs / GAugmentRef (CLoadRefs.cpp:231-268,
+ * MrcUtil/GAugmentRef.cu:10-23): a reference for frames fact times larger,
+ * every pixel repeated fact x fact; out holds nx*ny*fact*fact floats. */
+int mc3_ref_augment(const float* in, int nx, int ny, int fact, float* out);
 /* CReadFmIntFile::DoIt (DataUtil/CReadFmIntFile.cpp:104-170): up to
  * max_entries (group size, integration size, raw-frame dose) rows of a
  * frame-integration file; two-column files take fm_dose.  MC3_EIO when the

@@ -134,6 +134,9 @@ _SIGS = {
     "mc3_host_alloc": ([ctypes.c_size_t, ctypes.POINTER(_VP)], _I),
     "mc3_host_free": ([_VP], _I),
     "mc3_set_gain": ([_VP, _VP, _I, _I, _I], _I),
+    "mc3_set_dark": ([_VP, _VP, _I, _I, _I], _I),
+    "mc3_ref_orient": ([_VP, _I, _I, _I, _I, _I, _VP, _VP, _VP], _I),
+    "mc3_ref_augment": ([_VP, _I, _I, _I, _VP], _I),
     "mc3_process_movie": ([_VP, ctypes.POINTER(_Movie), ctypes.POINTER(_Result)], _I),
     "mc3_prefetch_movie": ([_VP, ctypes.POINTER(_Movie)], _I),
     "mc3_set_alignment": ([_VP, ctypes.POINTER(_Alignment)], _I),
@@ -314,6 +317,14 @@ class MotionCor3:
         else:
             g = np.ascontiguousarray(gain, dtype=np.float32)
             _check(_lib().mc3_set_gain(self._h, _hp(g), g.shape[1], g.shape[0], 0), "mc3_set_gain")
+
+    def set_dark(self, dark) -> None:
+        """Dark reference [ny][nx] (mc3_set_dark); None clears it."""
+        if dark is None:
+            _check(_lib().mc3_set_dark(self._h, None, 0, 0, 0), "mc3_set_dark")
+            return
+        d = np.ascontiguousarray(dark, dtype=np.float32)
+        _check(_lib().mc3_set_dark(self._h, _hp(d), d.shape[1], d.shape[0], 0), "mc3_set_dark")
 
     @staticmethod
     def _movie(frames, nx4=None):
@@ -507,6 +518,27 @@ def local_gather(src, dst, nx: int, ny: int, centers, shifts, bad=None) -> None:
     _check(_lib().mc3_local_gather(_dp(src), _dp(dst), nx, ny, _dp(centers), _dp(shifts),
                                    _dp(bad) if bad is not None else None, P, _stream()),
            "mc3_local_gather")
+
+
+# ---- reference images (host) ----
+def ref_orient(img: np.ndarray, rot: int = 0, flip: int = 0, inverse: int = 0) -> np.ndarray:
+    """CLoadRefs::PostProcess: rotate by rot x 90 degrees, flip (1 upside
+    down, 2 left-right), invert (mc3_ref_orient)."""
+    a = np.ascontiguousarray(img, np.float32)
+    out = np.zeros(a.size, np.float32)
+    nx, ny = ctypes.c_int(0), ctypes.c_int(0)
+    _check(_lib().mc3_ref_orient(_hp(a), a.shape[1], a.shape[0], rot, flip, inverse, _hp(out),
+                                 ctypes.byref(nx), ctypes.byref(ny)), "mc3_ref_orient")
+    return out.reshape(ny.value, nx.value)
+
+
+def ref_augment(img: np.ndarray, fact: int) -> np.ndarray:
+    """CLoadRefs::AugmentRefs: every pixel repeated fact x fact (mc3_ref_augment)."""
+    a = np.ascontiguousarray(img, np.float32)
+    out = np.zeros((a.shape[0] * fact, a.shape[1] * fact), np.float32)
+    _check(_lib().mc3_ref_augment(_hp(a), a.shape[1], a.shape[0], fact, _hp(out)),
+           "mc3_ref_augment")
+    return out
 
 
 # ---- frame integration (host) ----

@@ -127,6 +127,11 @@ int mc3_host_free(void* ptr) {
   return cudaFreeHost(ptr) == cudaSuccess ? MC3_OK : MC3_ECUDA;
 }
 
+int mc3_set_dark(mc3_ctx* ctx, const float* dark, int nx, int ny, int on_device) {
+  if (!ctx) return MC3_EINVAL;
+  return ctx->eng->set_dark(dark, nx, ny, on_device != 0);
+}
+
 int mc3_set_gain(mc3_ctx* ctx, const float* gain, int nx, int ny, int on_device) {
   if (!ctx) return MC3_EINVAL;
   return ctx->eng->set_gain(gain, nx, ny, on_device != 0);

@@ -10,6 +10,7 @@
 #include <cctype>
 #include <chrono>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -214,6 +215,45 @@ std::string aln_name(const std::string& dir_in, const std::string& movie) {
   return name;
 }
 
+// CLoadRefs::LoadGain / LoadDark (CLoadRefs.cpp:82-202): the gain must be a
+// float (mode 2) MRC image; a dark image in another mode is converted as the
+// reference's mToFloat does (mode 0 read as signed char).  Both must measure
+// 32..32000 pixels per side (sCheckSize).
+bool load_ref(const std::string& path, bool is_gain, std::vector<float>* img, int* nx, int* ny) {
+  const char* what = is_gain ? "Gain" : "Dark";
+  mc3::mrc::Header h;
+  if (!mc3::mrc::read_header(path, &h)) return false;
+  if (is_gain && h.mode != 2) {
+    std::printf("Warning: invalid pixel type of %s reference: %d\n"
+                "   mode 2 (32-bit float) is expected.\n\n%s reference will not be loaded.\n"
+                "   %s correction will be skipped.\n\n", what, h.mode, what, what);
+    return false;
+  }
+  if (is_gain && !(h.nx >= 32 && h.nx <= 32000 && h.ny >= 32 && h.ny <= 32000)) {
+    std::printf("Warning: invalid size of %s reference: %d  %d\n\n", what, h.nx, h.ny);
+    return false;
+  }
+  const int bpp = mc3::mrc::bytes_per_pixel(h.mode);
+  if (!bpp) return false;
+  std::vector<unsigned char> raw((size_t)h.nx * h.ny * bpp);
+  if (!mc3::mrc::read_frames(path, h, 0, 1, raw.data())) return false;
+  const size_t n = (size_t)h.nx * h.ny;
+  img->resize(n);
+  for (size_t i = 0; i < n; ++i) {
+    switch (h.mode) {
+      case 0: (*img)[i] = (float)(signed char)raw[i]; break;
+      case 5: (*img)[i] = raw[i]; break;
+      case 1: (*img)[i] = ((const int16_t*)raw.data())[i]; break;
+      case 6: (*img)[i] = ((const uint16_t*)raw.data())[i]; break;
+      case 2: (*img)[i] = ((const float*)raw.data())[i]; break;
+      default: return false;
+    }
+  }
+  *nx = h.nx;
+  *ny = h.ny;
+  return true;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -226,6 +266,7 @@ int main(int argc, char** argv) {
                 "[-Patch x y] [-Iter n] [-Tol px] [-Bft g p] [-FmDose d] [-PixSize a] "
                 "[-kV kv] [-Group g p] [-FmRef f] [-SumRange lo hi] [-PhaseOnly 0|1] [-SplitSum 0|1] "
                 "[-FtBin b] [-OutAln dir] [-InAln dir] [-OutStack 0|1 zbin] [-FmIntFile file] "
+                "[-Dark dark.mrc] [-RotGain r] [-FlipGain f] [-InvGain 0|1] "
                 "[-LogDir dir] [-Gpu id]\n");
     return eSuccess;
   }
@@ -235,6 +276,11 @@ int main(int argc, char** argv) {
   const std::string in_mrc = A.str("-InMrc");
   const std::string out_mrc = A.str("-OutMrc");
   const std::string gain_mrc = A.str("-Gain");
+  const std::string dark_mrc = A.str("-Dark");
+  int rot_gain = 0, flip_gain = 0, inv_gain = 0;
+  A.ints("-RotGain", &rot_gain, 1);    // CInput.cpp:604-614
+  A.ints("-FlipGain", &flip_gain, 1);
+  A.ints("-InvGain", &inv_gain, 1);
   std::string log_dir = A.str("-LogDir");
   if (!log_dir.empty() && log_dir.back() != '/') log_dir += "/";
   int pt[3] = {0, 0, 0};
@@ -264,10 +310,10 @@ int main(int argc, char** argv) {
   const std::string fmint_file = A.str("-FmIntFile");
   int gpu[8];
   if (A.ints("-Gpu", gpu, 8) > 0) p.gpu = gpu[0];
-  const char* ignored[] = {"-InTiff", "-InEer", "-InSuffix", "-InSkips", "-ArcDir", "-Dark",
+  const char* ignored[] = {"-InTiff", "-InEer", "-InSuffix", "-InSkips", "-ArcDir",
                            "-DefectFile", "-DefectMap", "-FullSum", "-TmpFile",
                            "-StackZ", "-Cs", "-AmpCont", "-ExtPhase", "-Throw", "-Trunc", "-Serial",
-                           "-Tilt", "-Crop", "-RotGain", "-FlipGain", "-InvGain", "-Mag",
+                           "-Tilt", "-Crop", "-Mag",
                            "-InFmMotion", "-GpuMemUsage", "-UseGpus",
                            "-EerSampling", "-OutStar", "-TiffOrder", "-CorrInterp"};
   for (const char* t : ignored) {
@@ -349,10 +395,51 @@ int main(int argc, char** argv) {
     std::fprintf(stderr, "Error: %s\n", mc3_strerror(s));
     return eNoValidGPUs;
   }
-  if (!gain_mrc.empty()) {
-    std::vector<float> gain;
-    int gx = 0, gy = 0;
-    if (!mc3::mrc::read_image_float(gain_mrc, &gain, &gx, &gy)) {
+  // ---- references: CMain::mLoadRefs (CMain.cpp:326-340), CLoadRefs::PostProcess
+  //      and AugmentRefs (CLoadRefs.cpp:82-268), CProcessThread::mCheckGain ----
+  {
+    std::vector<float> gain, dark;
+    int gx = 0, gy = 0, dx = 0, dy = 0;
+    bool have_gain = !gain_mrc.empty() && load_ref(gain_mrc, true, &gain, &gx, &gy);
+    bool have_dark = !dark_mrc.empty() && load_ref(dark_mrc, false, &dark, &dx, &dy);
+    if (have_dark && (!have_gain || dx != gx || dy != gy)) {  // mCheckDarkRef
+      std::printf("Warning: The sizes of Dark and gain references do not match.\n"
+                  "   Dark reference has been removed.\n\n");
+      have_dark = false;
+    }
+    if (have_gain && (rot_gain != 0 || flip_gain != 0 || inv_gain != 0)) {
+      std::vector<float> t(gain.size());
+      mc3_ref_orient(gain.data(), gx, gy, rot_gain, flip_gain, inv_gain, t.data(), &gx, &gy);
+      gain.swap(t);
+      // the reference orients the dark only when (rot != 0 || flip == 0), and never inverts it
+      if (have_dark && (rot_gain != 0 || flip_gain == 0)) {
+        std::vector<float> u(dark.size());
+        mc3_ref_orient(dark.data(), dx, dy, rot_gain, flip_gain, 0, u.data(), &dx, &dy);
+        dark.swap(u);
+      }
+    }
+    // super-resolution frames: references repeated by the common integer factor
+    if (have_gain && (gx != h.nx || gy != h.ny)) {
+      const int fx = h.nx / gx, fy = h.ny / gy;
+      if (fx == 0 || fy == 0 || fx != fy || h.nx % gx || h.ny % gy) {
+        std::fprintf(stderr, "Error: cannot augment gain reference.\n   Frame size: %d  %d\n"
+                             "   Ref size:   %d  %d\n\n", h.nx, h.ny, gx, gy);
+      } else {
+        std::vector<float> t((size_t)h.nx * h.ny);
+        mc3_ref_augment(gain.data(), gx, gy, fx, t.data());
+        gain.swap(t);
+        if (have_dark) {
+          std::vector<float> u((size_t)h.nx * h.ny);
+          mc3_ref_augment(dark.data(), dx, dy, fx, u.data());
+          dark.swap(u);
+          dx *= fx;
+          dy *= fx;
+        }
+        gx *= fx;
+        gy *= fx;
+      }
+    }
+    if (!have_gain) {
       std::printf("Warning: Gain ref not found.\n......   Gain correction will be skipped.\n\n");
     } else if (gx != h.nx || gy != h.ny) {
       std::fprintf(stderr, "Error: Gain and frame dimensions mismatch!\n"
@@ -362,6 +449,7 @@ int main(int argc, char** argv) {
       return eFailProcess;
     } else {
       mc3_set_gain(ctx, gain.data(), gx, gy, 0);
+      if (have_dark) mc3_set_dark(ctx, dark.data(), dx, dy, 0);
     }
   }
   mc3_plan_info info;

@@ -212,6 +212,23 @@ int Engine::set_gain(const float* gain, int w, int h, bool on_device) {
   return kOk;
 }
 
+int Engine::set_dark(const float* dark, int w, int h, bool on_device) {
+  MC3_CUDA(cudaSetDevice(device));
+  if (!dark) {
+    has_dark = false;
+    return kOk;
+  }
+  if (w <= 0 || h <= 0) return kEInval;
+  MC3_TRY(d_dark.ensure(sizeof(float) * (size_t)w * h));
+  MC3_CUDA(cudaMemcpyAsync(d_dark.p, dark, sizeof(float) * (size_t)w * h,
+                           on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream));
+  MC3_CUDA(cudaStreamSynchronize(stream));
+  has_dark = true;
+  dark_w = w;
+  dark_h = h;
+  return kOk;
+}
+
 int Engine::plan(int w, int h, int n, mc3_plan_info* info) {
   Geometry g;
   if (fmint && n != fmint_raw) return kEInval;
@@ -480,6 +497,8 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
     return kEUnsupported;
   }
   if (has_gain && (gain_w != g.W || gain_h != g.H)) return kEInval;  // CProcessThread::mCheckGain
+  if (has_dark && (dark_w != g.W || dark_h != g.H)) return kEInval;
+  const float* dark = has_dark ? d_dark.as<float>() : nullptr;
   const bool loaded = aln_loaded;
   if (loaded && (aln_nz != g.N || aln_P != g.P)) {
     last_error = "loaded alignment does not match the movie (frames or patches)";
@@ -528,10 +547,10 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
     MC3_CUDA(cudaMemcpyAsync(d_istart.p, fi.start.data(), sizeof(int) * N, cudaMemcpyHostToDevice, st));
     MC3_CUDA(cudaMemcpyAsync(d_isize.p, fi.size.data(), sizeof(int) * N, cudaMemcpyHostToDevice, st));
     MC3_TRY(gain_and_sum_int(raw, mv.mode, raw_stride, d_istart.as<int>(), d_isize.as<int>(),
-                             has_gain ? d_gain.as<float>() : nullptr, frames, fr_stride_f,
+                             dark, has_gain ? d_gain.as<float>() : nullptr, frames, fr_stride_f,
                              prm.correct_bad ? d_sum.as<float>() : nullptr, W, H, N, st));
   } else {
-    MC3_TRY(gain_and_sum(raw, mv.mode, raw_stride, has_gain ? d_gain.as<float>() : nullptr, frames,
+    MC3_TRY(gain_and_sum(raw, mv.mode, raw_stride, dark, has_gain ? d_gain.as<float>() : nullptr, frames,
                          fr_stride_f, prm.correct_bad ? d_sum.as<float>() : nullptr, W, H, N, st));
   }
   if (used_slot >= 0) MC3_CUDA(cudaEventRecord(slot_free[used_slot], st));  // raw is read only above

@@ -48,6 +48,7 @@ class Engine {
   int init();
   int set_stream(cudaStream_t s);
   int set_gain(const float* gain, int w, int h, bool on_device);
+  int set_dark(const float* dark, int w, int h, bool on_device);
   int plan(int w, int h, int n, mc3_plan_info* info);
   int process(const mc3_movie& mv, mc3_result* out);
   // Starts the host->device copy of a later movie's raw frames on the copy
@@ -111,6 +112,9 @@ class Engine {
   bool fmint_dose = false;
   host::FmInt fmint_tab;
   DevBuf d_istart, d_isize;
+  DevBuf d_dark;
+  bool has_dark = false;
+  int dark_w = 0, dark_h = 0;
   bool has_gain = false;
   double wn_key[6] = {0, 0, 0, 0, 0, 0};  // geometry and dose options of d_Wn
   bool wn_valid = false;

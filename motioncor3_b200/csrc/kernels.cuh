@@ -8,13 +8,14 @@ namespace mc3 {
 
 // ---- prep.cu ----
 // mode: MRC pixel mode (0 u8, 1 i16, 2 f32, 6 u16).  frames: padded stack.
-int gain_and_sum(const void* raw, int mode, long raw_stride, const float* gain, float* frames,
-                 long fr_stride, float* sum, int W, int H, int N, cudaStream_t st);
+int gain_and_sum(const void* raw, int mode, long raw_stride, const float* dark,
+                 const float* gain, float* frames, long fr_stride, float* sum, int W, int H, int N,
+                 cudaStream_t st);
 // The same with frame integration (modes 0, 5, 101): rendered frame f sums
 // raw frames start[f] .. start[f]+size[f]-1 modulo 256 (device tables).
 int gain_and_sum_int(const void* raw, int mode, long raw_stride, const int* start,
-                     const int* size, const float* gain, float* frames, long fr_stride, float* sum,
-                     int W, int H, int N, cudaStream_t st);
+                     const int* size, const float* dark, const float* gain, float* frames,
+                     long fr_stride, float* sum, int W, int H, int N, cudaStream_t st);
 int moment_grid(int W, int H);
 int image_moment(const float* img, int W, int H, long pitch, int iExp, float* d_part,
                  float* d_out, cudaStream_t st);

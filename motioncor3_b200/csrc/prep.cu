@@ -11,15 +11,18 @@ namespace mc3 {
 // to the padded frame stack and accumulated (in frame order, as the
 // reference's CSumFFTStack does) into the padded sum image.
 template <typename T>
-__global__ void k_gain_sum(const T* __restrict__ raw, long raw_stride, const float* __restrict__ gain,
-                           float* frames, long fr_stride, float* sum, int W, int H, int N, int padX) {
+__global__ void k_gain_sum(const T* __restrict__ raw, long raw_stride, const float* __restrict__ dark,
+                           const float* __restrict__ gain, float* frames, long fr_stride, float* sum,
+                           int W, int H, int N, int padX) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y;
   if (x >= W) return;
   const float g = gain ? gain[(long)y * W + x] : 1.0f;
+  const float d = dark ? dark[(long)y * W + x] : 0.0f;
   float s = 0.0f;
   for (int f = 0; f < N; ++f) {
     float v = (float)raw[(long)f * raw_stride + (long)y * W + x];
+    if (dark) v -= d;  // (raw - dark) * gain, GApplyRefsToFrame.cu:66-70
     if (gain) v *= g;
     frames[(long)f * fr_stride + (long)y * padX + x] = v;
     s += v;
@@ -31,18 +34,21 @@ __global__ void k_gain_sum(const T* __restrict__ raw, long raw_stride, const flo
 // the low nibble of byte x/2 for even x, the high nibble for odd x
 // (GApplyRefsToFrame mGDoPkd, MrcUtil/GApplyRefsToFrame.cu:30-53).
 __global__ void k_gain_sum_pkd(const uint8_t* __restrict__ raw, long raw_stride,
-                               const float* __restrict__ gain, float* frames, long fr_stride,
-                               float* sum, int W, int H, int N, int padX) {
+                               const float* __restrict__ dark, const float* __restrict__ gain,
+                               float* frames, long fr_stride, float* sum, int W, int H, int N,
+                               int padX) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y;
   if (x >= W) return;
   const int pkX = (W + 1) / 2;
   const float g = gain ? gain[(long)y * W + x] : 1.0f;
+  const float d = dark ? dark[(long)y * W + x] : 0.0f;
   float s = 0.0f;
   for (int f = 0; f < N; ++f) {
     int b = raw[(long)f * raw_stride + (long)y * pkX + x / 2];
     if (x & 1) b >>= 4;
     float v = (float)(b & 0xf);
+    if (dark) v -= d;
     if (gain) v *= g;
     frames[(long)f * fr_stride + (long)y * padX + x] = v;
     s += v;
@@ -50,18 +56,19 @@ __global__ void k_gain_sum_pkd(const uint8_t* __restrict__ raw, long raw_stride,
   if (sum) sum[(long)y * padX + x] = s;
 }
 
-int gain_and_sum(const void* raw, int mode, long raw_stride, const float* gain, float* frames,
-                 long fr_stride, float* sum, int W, int H, int N, cudaStream_t st) {
+int gain_and_sum(const void* raw, int mode, long raw_stride, const float* dark,
+                 const float* gain, float* frames, long fr_stride, float* sum, int W, int H, int N,
+                 cudaStream_t st) {
   const int padX = 2 * (W / 2 + 1);
   dim3 grid(ceil_div(W, 256), H);
   const double bpp = mode == 101 ? 0.5 : (mode == 0 || mode == 5) ? 1 : (mode == 2 ? 4 : 2);
   prof::Scope ps("k_gain_sum", (double)W * H * (N * (bpp + 4.0) + (gain ? 4.0 : 0.0) + (sum ? 4.0 : 0.0)), st);
   switch (mode) {
-    case 101: k_gain_sum_pkd<<<grid, 256, 0, st>>>((const uint8_t*)raw, raw_stride, gain, frames, fr_stride, sum, W, H, N, padX); break;
-    case 0: case 5: k_gain_sum<uint8_t><<<grid, 256, 0, st>>>((const uint8_t*)raw, raw_stride, gain, frames, fr_stride, sum, W, H, N, padX); break;
-    case 1: k_gain_sum<int16_t><<<grid, 256, 0, st>>>((const int16_t*)raw, raw_stride, gain, frames, fr_stride, sum, W, H, N, padX); break;
-    case 2: k_gain_sum<float><<<grid, 256, 0, st>>>((const float*)raw, raw_stride, gain, frames, fr_stride, sum, W, H, N, padX); break;
-    case 6: k_gain_sum<uint16_t><<<grid, 256, 0, st>>>((const uint16_t*)raw, raw_stride, gain, frames, fr_stride, sum, W, H, N, padX); break;
+    case 101: k_gain_sum_pkd<<<grid, 256, 0, st>>>((const uint8_t*)raw, raw_stride, dark, gain, frames, fr_stride, sum, W, H, N, padX); break;
+    case 0: case 5: k_gain_sum<uint8_t><<<grid, 256, 0, st>>>((const uint8_t*)raw, raw_stride, dark, gain, frames, fr_stride, sum, W, H, N, padX); break;
+    case 1: k_gain_sum<int16_t><<<grid, 256, 0, st>>>((const int16_t*)raw, raw_stride, dark, gain, frames, fr_stride, sum, W, H, N, padX); break;
+    case 2: k_gain_sum<float><<<grid, 256, 0, st>>>((const float*)raw, raw_stride, dark, gain, frames, fr_stride, sum, W, H, N, padX); break;
+    case 6: k_gain_sum<uint16_t><<<grid, 256, 0, st>>>((const uint16_t*)raw, raw_stride, dark, gain, frames, fr_stride, sum, W, H, N, padX); break;
     default: return kEUnsupported;
   }
   MC3_CHECK_LAUNCH("k_gain_sum");
@@ -77,13 +84,15 @@ int gain_and_sum(const void* raw, int mode, long raw_stride, const float* gain, 
 template <bool PACKED>
 __global__ void k_gain_sum_int(const uint8_t* __restrict__ raw, long raw_stride,
                                const int* __restrict__ start, const int* __restrict__ size,
-                               const float* __restrict__ gain, float* frames, long fr_stride,
-                               float* sum, int W, int H, int N, int padX) {
+                               const float* __restrict__ dark, const float* __restrict__ gain,
+                               float* frames, long fr_stride, float* sum, int W, int H, int N,
+                               int padX) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y;
   if (x >= W) return;
   const long off = PACKED ? (long)y * ((W + 1) / 2) + x / 2 : (long)y * W + x;
   const float g = gain ? gain[(long)y * W + x] : 1.0f;
+  const float d = dark ? dark[(long)y * W + x] : 0.0f;
   float s = 0.0f;
   for (int f = 0; f < N; ++f) {
     const int r0 = start[f], nr = size[f];
@@ -94,6 +103,7 @@ __global__ void k_gain_sum_int(const uint8_t* __restrict__ raw, long raw_stride,
       acc += b;
     }
     float v = (float)(acc & 0xffu);
+    if (dark) v -= d;
     if (gain) v *= g;
     frames[(long)f * fr_stride + (long)y * padX + x] = v;
     s += v;
@@ -102,19 +112,19 @@ __global__ void k_gain_sum_int(const uint8_t* __restrict__ raw, long raw_stride,
 }
 
 int gain_and_sum_int(const void* raw, int mode, long raw_stride, const int* start,
-                     const int* size, const float* gain, float* frames, long fr_stride, float* sum,
-                     int W, int H, int N, cudaStream_t st) {
+                     const int* size, const float* dark, const float* gain, float* frames,
+                     long fr_stride, float* sum, int W, int H, int N, cudaStream_t st) {
   const int padX = 2 * (W / 2 + 1);
   dim3 grid(ceil_div(W, 256), H);
   prof::Scope ps("k_gain_sum_int", (double)W * H * N * 4.0, st);  // rendered-frame writes
   switch (mode) {
     case 101:
-      k_gain_sum_int<true><<<grid, 256, 0, st>>>((const uint8_t*)raw, raw_stride, start, size, gain,
-                                                 frames, fr_stride, sum, W, H, N, padX);
+      k_gain_sum_int<true><<<grid, 256, 0, st>>>((const uint8_t*)raw, raw_stride, start, size, dark,
+                                                 gain, frames, fr_stride, sum, W, H, N, padX);
       break;
     case 0: case 5:
       k_gain_sum_int<false><<<grid, 256, 0, st>>>((const uint8_t*)raw, raw_stride, start, size,
-                                                  gain, frames, fr_stride, sum, W, H, N, padX);
+                                                  dark, gain, frames, fr_stride, sum, W, H, N, padX);
       break;
     default: return kEUnsupported;
   }

@@ -1059,6 +1059,7 @@ void oracle_default_params(oracle_params* p) {
   p->int_size = nullptr;
   p->acc_dose = nullptr;
   p->dose_weight = 0;
+  p->dark = nullptr;
 }
 
 void oracle_rfft2(const double* img, double* spec, int W, int H, int normalise) {
@@ -1143,6 +1144,7 @@ int oracle_process_movie(const oracle_params* p, const float* frames, int W, int
   std::vector<double> fr((long)N * npx);
   for (long i = 0; i < (long)N * npx; ++i) {
     double v = frames[i];
+    if (p->dark) v -= p->dark[i % npx];
     if (gain) v *= gain[i % npx];
     fr[i] = v;
   }

@@ -46,6 +46,7 @@ typedef struct {
   const int* int_size;
   const float* acc_dose;
   int dose_weight;
+  const float* dark;  /* [H][W] dark reference subtracted before the gain, or NULL */
 } oracle_params;
 
 typedef struct {

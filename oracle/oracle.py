@@ -73,6 +73,7 @@ class OracleParams(ctypes.Structure):
         ("int_size", _VP),
         ("acc_dose", _VP),
         ("dose_weight", ctypes.c_int),
+        ("dark", _VP),
     ]
 
 
@@ -124,7 +125,7 @@ def params(**kw) -> OracleParams:
 
 
 def process_movie(frames: np.ndarray, gain=None, force=None, int_size=None, acc_dose=None,
-                  **kw) -> dict:
+                  dark=None, **kw) -> dict:
     """Runs the whole oracle path.  `force` may hold global_shifts (and
     patch_shifts / patch_centers / patch_bad) to correct with given shifts;
     int_size / acc_dose describe rendered frames of a frame-integration file."""
@@ -138,6 +139,10 @@ def process_movie(frames: np.ndarray, gain=None, force=None, int_size=None, acc_
         acc = np.ascontiguousarray(acc_dose, np.float32)
         tabs.append(acc)
         p.acc_dose = acc.ctypes.data
+    if dark is not None:
+        dk = np.ascontiguousarray(dark, np.float32)
+        tabs.append(dk)
+        p.dark = dk.ctypes.data
     nz, ny, nx = frames.shape
     fr = np.ascontiguousarray(frames, np.float32)
     g = None if gain is None else np.ascontiguousarray(gain, np.float32)

@@ -152,3 +152,40 @@ def test_frame_integration_tables_without_integration(mc3lib):
     assert t["dose_weight"] == 1
     t = api.frame_integration_tables(None, 12, fm_dose=0.0)
     assert t["dose_weight"] == 0 and len(t["size"]) == 12
+
+
+@pytest.mark.parametrize("rot", [0, 1, 2, 3])
+@pytest.mark.parametrize("flip", [0, 1, 2])
+def test_ref_orient(mc3lib, rot, flip):
+    """CLoadRefs::PostProcess: G90Rotate2D's nearest-pixel rotation about the
+    centre (restated here from its index formula), GFlip2D, GInverse2D."""
+    from motioncor3_b200 import api
+    rng = np.random.default_rng(rot * 3 + flip)
+    ny, nx = 6, 10
+    a = rng.uniform(0.5, 1.5, (ny, nx)).astype(np.float32)
+    a[2, 3] = 0.0
+    out = api.ref_orient(a, rot, flip, 1)
+    c, s = [(1, 0), (0, 1), (-1, 0), (0, -1)][rot]
+    rx, ry = (ny, nx) if rot % 2 else (nx, ny)
+    ref = np.zeros((ry, rx), np.float32)
+    for y in range(ry):
+        for x in range(rx):
+            fx = (x - (rx - 1) / 2) * c + (y - (ry - 1) / 2) * s
+            fy = -(x - (rx - 1) / 2) * s + (y - (ry - 1) / 2) * c
+            ref[y, x] = a[int(fy + (ny - 1) / 2 + 0.5), int(fx + (nx - 1) / 2 + 0.5)]
+    if flip == 1:
+        ref = ref[::-1]
+    elif flip == 2:
+        ref = ref[:, ::-1]
+    with np.errstate(divide="ignore"):
+        ref = np.where(ref == 0, 0, 1.0 / ref).astype(np.float32)
+    assert out.shape == ref.shape
+    assert np.array_equal(out, ref)
+    if rot == 2 and flip == 0:  # half turn = both flips
+        assert np.array_equal(api.ref_orient(a, 2), a[::-1, ::-1])
+
+
+def test_ref_augment(mc3lib):
+    from motioncor3_b200 import api
+    a = np.arange(12, dtype=np.float32).reshape(3, 4)
+    assert np.array_equal(api.ref_augment(a, 2), np.repeat(np.repeat(a, 2, 0), 2, 1))

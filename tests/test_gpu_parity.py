@@ -384,6 +384,26 @@ def test_pipeline_frame_integration(api, oracle, torch_cuda, packed, high):
         assert e <= 1e-4, (i, e)
 
 
+def test_pipeline_dark_and_gain(api, oracle, torch_cuda):
+    """(raw - dark) * gain (GApplyRefsToFrame, MrcUtil/GApplyRefsToFrame.cu:56-72)."""
+    from motioncor3_b200 import synthetic as S
+    m = S.make_movie(384, 320, 10, dose=4.0, seed=45, gain=True)
+    dark = np.random.default_rng(45).uniform(0.0, 0.6, (320, 384)).astype(np.float32)
+    p = api.Params(iter=6, tol=0.2, bft=(300, 100), fm_dose=1.2, pix_size=0.9)
+    with api.MotionCor3(p) as mc:
+        mc.set_gain(np.asarray(m.gain))
+        mc.set_dark(dark)
+        res = mc.process(np.asarray(m.frames))
+    kw = dict(iter=6, tol=0.2, bft=(300, 100), fm_dose=1.2, pix_size=0.9)
+    orc = oracle.process_movie(np.asarray(m.frames), gain=np.asarray(m.gain), dark=dark, **kw)
+    assert np.abs(res.global_shifts - orc["global_shifts"]).max() <= 0.05
+    same = oracle.process_movie(np.asarray(m.frames), gain=np.asarray(m.gain), dark=dark,
+                                force=dict(global_shifts=res.global_shifts), **kw)
+    for i in range(res.n_sums):
+        e = _rel_rms(res.sums[i], same["sums"][i])
+        assert e <= 1e-4, (i, e)
+
+
 def test_pipeline_config1_full_size(api, oracle, torch_cuda):
     """40 frames of 1024x1024, global alignment only (-Patch 0 0 -Iter 7
     -Tol 0.5 -Bft 150 -PixSize 1.0), dose 1 e/px/frame, unit gain."""

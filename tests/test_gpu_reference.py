@@ -36,11 +36,15 @@ def _read_log(path):
     return np.array(rows)
 
 
-def run_program(binary, workdir, movie, gain, tags, extra=(), four_bit=False):
+def run_program(binary, workdir, movie, gain, tags, extra=(), four_bit=False, dark=None):
     from motioncor3_b200 import mrcio
     os.makedirs(workdir, exist_ok=True)
     mv = os.path.join(workdir, "movie.mrc")
     mrcio.write(mv, movie, four_bit=four_bit)
+    if dark is not None:
+        dp = os.path.join(workdir, "dark.mrc")
+        mrcio.write(dp, dark.astype(np.float32))
+        extra = list(extra) + ["-Dark", dp]
     args = [binary, "-InMrc", mv, "-OutMrc", os.path.join(workdir, "sum.mrc"), "-LogDir",
             workdir + "/", "-OutAln", workdir, "-Gpu", "0", "-Cs", "0"] + tags + list(extra)
     if gain is not None:
@@ -255,3 +259,42 @@ def test_cli_frame_integration_matches_reference_program(tmp_path, mc3lib):
             assert _rel(ref["sums"][suf], ours["sums"][suf]) <= 1e-4, suf
         for f in range(7):
             assert _rel(ref["stack"][f], ours["stack"][f]) <= 1e-4, f
+
+
+@pytest.mark.parametrize("variant", ["rot_flip_inv_dark", "augment"])
+def test_cli_gain_references_match_reference_program(variant, tmp_path, mc3lib):
+    """Gain and dark references as CMain::mLoadRefs prepares them: a gain
+    stored rotated and flipped and as reciprocal (-RotGain 1 -FlipGain 1
+    -InvGain 1) with a dark reference, or a gain at half the frame size
+    repeated 2 x 2 (CLoadRefs::AugmentRefs).  -FlipGain 2 is not run on the
+    reference: its left-right flip kernel touches one row past the image
+    (MrcUtil/GFlip2D.cu mGHorizontal tests y > ny)."""
+    if not os.path.exists(REF_BIN):
+        pytest.skip("reference program not built (oracle/ref_full)")
+    from motioncor3_b200 import api, build, synthetic as S
+    build.build()
+    m = S.make_movie(384, 320, 10, dose=4.0, seed=46, gain=True)
+    tags = "-Iter 6 -Tol 0.2 -Bft 300 -FmDose 1.2 -PixSize 0.9".split()
+    dark = None
+    if variant == "augment":
+        g = np.asarray(m.gain)[::2, ::2].copy()
+        frames = (np.asarray(m.frames) / np.repeat(np.repeat(g, 2, 0), 2, 1)).astype(np.float32)
+        gain_file = g
+    else:
+        frames = np.asarray(m.frames)
+        # the file holds the gain such that rotation, flip and inversion restore it
+        inv = (1.0 / np.asarray(m.gain)).astype(np.float32)
+        stored = api.ref_orient(api.ref_orient(inv, 0, 1, 0), 3, 0, 0)
+        assert np.array_equal(api.ref_orient(stored, 1, 1, 0), inv)
+        gain_file = stored
+        dark = np.random.default_rng(46).uniform(0.0, 0.5, stored.shape).astype(np.float32)
+        tags += "-RotGain 1 -FlipGain 1 -InvGain 1".split()
+    ref = run_program(REF_BIN, str(tmp_path / "ref"), frames, gain_file, tags, dark=dark)
+    ours = run_program(OUR_BIN, str(tmp_path / "ours"), frames, gain_file, tags, dark=dark)
+    assert "mismatch" not in ours["stdout"] and "mismatch" not in ref["stdout"]
+    assert sorted(ref["sums"]) == sorted(ours["sums"])
+    a, b = _read_log(ref["logs"]["-Full.log"]), _read_log(ours["logs"]["-Full.log"])
+    assert np.abs(a - b).max() <= 0.05 + 1e-6
+    if np.array_equal(a, b):
+        for suf in ref["sums"]:
+            assert _rel(ref["sums"][suf], ours["sums"][suf]) <= 1e-4, suf
