@@ -268,6 +268,18 @@ int mc3_profile_read(char* buf, size_t len, int reset);
 /* Kernel launches issued by this library since it was loaded. */
 unsigned long long mc3_kernel_launches(void);
 
+/* ---- movie files (host) ---- */
+/* TiffUtil/CLoadTiffHeader.cpp (size = first directory, frames = number of
+ * directories, mode from bits per sample and sample format: 8 -> 0, 16 -> 1
+ * signed or 6, 32-bit float -> 2).  MC3_EIO when unreadable,
+ * MC3_EUNSUPPORTED for other pixel types or pages of mixed size/type. */
+int mc3_tiff_info(const char* path, int* nx, int* ny, int* nz, int* mode);
+/* TiffUtil/CLoadTiffImage.cpp + CLoadTiffStack (multi-threaded): frames
+ * z0..z0+nz-1 decoded (none, LZW, Deflate, PackBits; horizontal predictor)
+ * into dst [nz][ny][nx] in the file's pixel type, rows bottom-up as the
+ * reference stores them; threads <= 0 uses every host core. */
+int mc3_tiff_read(const char* path, int z0, int nz, void* dst, int threads);
+
 /* ---- host-side bookkeeping (host pointers) ---- */
 /* CLoadRefs::PostProcess (CLoadRefs.cpp:204-229): rotation by rot x 90
  * degrees (G90Rotate2D, nearest pixel about the centre; odd factors swap the

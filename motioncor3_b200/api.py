@@ -137,6 +137,8 @@ _SIGS = {
     "mc3_set_dark": ([_VP, _VP, _I, _I, _I], _I),
     "mc3_ref_orient": ([_VP, _I, _I, _I, _I, _I, _VP, _VP, _VP], _I),
     "mc3_ref_augment": ([_VP, _I, _I, _I, _VP], _I),
+    "mc3_tiff_info": ([ctypes.c_char_p, _VP, _VP, _VP, _VP], _I),
+    "mc3_tiff_read": ([ctypes.c_char_p, _I, _I, _VP, _I], _I),
     "mc3_process_movie": ([_VP, ctypes.POINTER(_Movie), ctypes.POINTER(_Result)], _I),
     "mc3_prefetch_movie": ([_VP, ctypes.POINTER(_Movie)], _I),
     "mc3_set_alignment": ([_VP, ctypes.POINTER(_Alignment)], _I),
@@ -538,6 +540,27 @@ def ref_augment(img: np.ndarray, fact: int) -> np.ndarray:
     out = np.zeros((a.shape[0] * fact, a.shape[1] * fact), np.float32)
     _check(_lib().mc3_ref_augment(_hp(a), a.shape[1], a.shape[0], fact, _hp(out)),
            "mc3_ref_augment")
+    return out
+
+
+# ---- movie files (host) ----
+_TIFF_DT = {0: np.uint8, 1: np.int16, 2: np.float32, 6: np.uint16}
+
+
+def tiff_info(path: str) -> dict:
+    """mc3_tiff_info: size, frame count and MRC-equivalent mode of a TIFF movie."""
+    v = [ctypes.c_int(0) for _ in range(4)]
+    _check(_lib().mc3_tiff_info(path.encode(), *[ctypes.byref(x) for x in v]), "mc3_tiff_info")
+    return dict(nx=v[0].value, ny=v[1].value, nz=v[2].value, mode=v[3].value)
+
+
+def tiff_read(path: str, z0: int = 0, nz: Optional[int] = None, threads: int = 0) -> np.ndarray:
+    """mc3_tiff_read: frames [nz][ny][nx] in the file's pixel type, rows
+    bottom-up as the reference stores them."""
+    info = tiff_info(path)
+    nz = info["nz"] - z0 if nz is None else nz
+    out = np.zeros((nz, info["ny"], info["nx"]), _TIFF_DT[info["mode"]])
+    _check(_lib().mc3_tiff_read(path.encode(), z0, nz, out.ctypes.data, threads), "mc3_tiff_read")
     return out
 
 

@@ -89,7 +89,7 @@ def build(force: bool = False, jobs: int = 8, verbose: bool = False) -> str:
         fh.write("{ global: mc3_*; local: *; };\n")
     if force or cmds or _stale(LIB, objs):
         # only the C ABI is exported; the static CUDA runtime stays private
-        run([nvcc, *ARCH, "-shared", "-ccbin", cxx, "-o", LIB, *objs, "-lpthread",
+        run([nvcc, *ARCH, "-shared", "-ccbin", cxx, "-o", LIB, *objs, "-lpthread", "-lz",
              "-Xlinker", f"--version-script={vscript}"])
     cli_src = [os.path.join(SRC, "cli.cpp"), os.path.join(SRC, "mrc.cpp")]
     if force or _stale(CLI, [*cli_src, LIB, *hdrs]):

@@ -93,10 +93,15 @@ std::string log_stem(const std::string& log_dir, const std::string& in_file) {
   const char* base = std::strrchr(in_file.c_str(), '/');
   base = base ? base + 1 : in_file.c_str();
   std::string s = log_dir + base;
-  const char* p = strcasestr(s.c_str(), ".mrc");
-  if (!p) return std::string();
-  s.resize(p - s.c_str());
-  return s;
+  // CAlignMain::mCreateLogFile (Align/CAlignMain.cpp:77-107)
+  for (const char* ext : {".mrc", ".tif", ".eer"}) {
+    const char* p = strcasestr(s.c_str(), ext);
+    if (p) {
+      s.resize(p - s.c_str());
+      return s;
+    }
+  }
+  return std::string();
 }
 
 void stats(const float* img, size_t n, float* mn, float* mx, float* mean) {
@@ -221,6 +226,27 @@ std::string aln_name(const std::string& dir_in, const std::string& movie) {
 // 32..32000 pixels per side (sCheckSize).
 bool load_ref(const std::string& path, bool is_gain, std::vector<float>* img, int* nx, int* ny) {
   const char* what = is_gain ? "Gain" : "Dark";
+  if (is_gain) {
+    // CLoadRefs::mGetFileType (CLoadRefs.cpp:93-106): by the last extension
+    const size_t dot = path.rfind('.');
+    if (dot == std::string::npos) return false;
+    const std::string ext = path.substr(dot);
+    const bool mrc = strcasestr(ext.c_str(), "mrc") != nullptr;
+    const bool tif = !mrc && (strcasestr(ext.c_str(), "tif") || strcasestr(ext.c_str(), "gain"));
+    if (!mrc && !tif) return false;
+    if (tif) {  // mLoadGainTiff (:125-147): a float TIFF, first directory
+      int m = -1, nz = 0;
+      if (mc3_tiff_info(path.c_str(), nx, ny, &nz, &m) != MC3_OK) return false;
+      if (m != 2) {
+        std::printf("Warning: invalid pixel type of %s reference: %d\n"
+                    "   mode 2 (32-bit float) is expected.\n\n", what, m);
+        return false;
+      }
+      if (!(*nx >= 32 && *nx <= 32000 && *ny >= 32 && *ny <= 32000)) return false;
+      img->resize((size_t)(*nx) * (*ny));
+      return mc3_tiff_read(path.c_str(), 0, 1, img->data(), 1) == MC3_OK;
+    }
+  }
   mc3::mrc::Header h;
   if (!mc3::mrc::read_header(path, &h)) return false;
   if (is_gain && h.mode != 2) {
@@ -262,7 +288,7 @@ int main(int argc, char** argv) {
     return eSuccess;
   }
   if (argc <= 1 || (argc == 2 && strcasecmp(argv[1], "--help") == 0)) {
-    std::printf("Usage: MotionCor3 -InMrc movie.mrc -OutMrc sum.mrc [-Gain gain.mrc] "
+    std::printf("Usage: MotionCor3 -InMrc movie.mrc|-InTiff movie.tif -OutMrc sum.mrc [-Gain gain.mrc] "
                 "[-Patch x y] [-Iter n] [-Tol px] [-Bft g p] [-FmDose d] [-PixSize a] "
                 "[-kV kv] [-Group g p] [-FmRef f] [-SumRange lo hi] [-PhaseOnly 0|1] [-SplitSum 0|1] "
                 "[-FtBin b] [-OutAln dir] [-InAln dir] [-OutStack 0|1 zbin] [-FmIntFile file] "
@@ -273,7 +299,10 @@ int main(int argc, char** argv) {
   Args A{argc, argv};
   mc3_params p;
   mc3_params_default(&p);
-  const std::string in_mrc = A.str("-InMrc");
+  // -InMrc or -InTiff (CInput::IsInTiff, CInput.cpp:697-700); `in_mrc` names
+  // the input file either way (logs, .aln names)
+  const std::string in_tiff = A.str("-InTiff");
+  const std::string in_mrc = in_tiff.empty() ? A.str("-InMrc") : in_tiff;
   const std::string out_mrc = A.str("-OutMrc");
   const std::string gain_mrc = A.str("-Gain");
   const std::string dark_mrc = A.str("-Dark");
@@ -310,7 +339,7 @@ int main(int argc, char** argv) {
   const std::string fmint_file = A.str("-FmIntFile");
   int gpu[8];
   if (A.ints("-Gpu", gpu, 8) > 0) p.gpu = gpu[0];
-  const char* ignored[] = {"-InTiff", "-InEer", "-InSuffix", "-InSkips", "-ArcDir",
+  const char* ignored[] = {"-InEer", "-InSuffix", "-InSkips", "-ArcDir",
                            "-DefectFile", "-DefectMap", "-FullSum", "-TmpFile",
                            "-StackZ", "-Cs", "-AmpCont", "-ExtPhase", "-Throw", "-Trunc", "-Serial",
                            "-Tilt", "-Crop", "-Mag",
@@ -325,11 +354,20 @@ int main(int argc, char** argv) {
   if (in_mrc == out_mrc) return eInputOutputSame;
 
   mc3::mrc::Header h;
-  if (!mc3::mrc::read_header(in_mrc, &h) || mc3::mrc::frame_bytes(h.mode, h.nx, h.ny) == 0) {
-    std::fprintf(stderr, "Error: cannot load %s\n", in_mrc.c_str());
-    return eFailLoad;
+  if (!in_tiff.empty()) {
+    if (mc3_tiff_info(in_tiff.c_str(), &h.nx, &h.ny, &h.nz, &h.mode) != MC3_OK) {
+      std::fprintf(stderr, "CLoadTiffStack: cannot open Tiff file, skip,\n   %s\n\n",
+                   in_tiff.c_str());
+      return eFailLoad;
+    }
+    std::printf("TIFF file size mode: %d  %d  %d  %d\n", h.nx, h.ny, h.nz, h.mode);
+  } else {
+    if (!mc3::mrc::read_header(in_mrc, &h) || mc3::mrc::frame_bytes(h.mode, h.nx, h.ny) == 0) {
+      std::fprintf(stderr, "Error: cannot load %s\n", in_mrc.c_str());
+      return eFailLoad;
+    }
+    std::printf("MRC file size mode: %d  %d  %d  %d\n", h.nx, h.ny, h.nz, h.mode);
   }
-  std::printf("MRC file size mode: %d  %d  %d  %d\n", h.nx, h.ny, h.nz, h.mode);
   // -FmIntFile (CReadFmIntFile::DoIt, CFmIntParam::Setup): rendered-frame
   // tables for this movie's raw frames
   std::vector<int> fi_start, fi_size;
@@ -387,7 +425,14 @@ int main(int argc, char** argv) {
   }
   const size_t frame_bytes = (size_t)mc3::mrc::frame_bytes(h.mode, h.nx, h.ny);
   HostBuf frames(frame_bytes * h.nz);
-  if (!mc3::mrc::read_frames(in_mrc, h, 0, h.nz, frames.as<unsigned char>())) return eFailLoad;
+  if (!in_tiff.empty()) {
+    if (mc3_tiff_read(in_tiff.c_str(), 0, h.nz, frames.p, 0) != MC3_OK) {
+      std::fprintf(stderr, "error: load tiff images of %s\n", in_tiff.c_str());
+      return eFailLoad;
+    }
+  } else if (!mc3::mrc::read_frames(in_mrc, h, 0, h.nz, frames.as<unsigned char>())) {
+    return eFailLoad;
+  }
 
   mc3_ctx* ctx = nullptr;
   int s = mc3_create(&p, &ctx);

@@ -298,3 +298,37 @@ def test_cli_gain_references_match_reference_program(variant, tmp_path, mc3lib):
     if np.array_equal(a, b):
         for suf in ref["sums"]:
             assert _rel(ref["sums"][suf], ours["sums"][suf]) <= 1e-4, suf
+
+
+def test_cli_tiff_movie_matches_mrc_movie(tmp_path, mc3lib):
+    """-InTiff: an LZW-compressed 8-bit TIFF movie (Pillow/libtiff-written)
+    gives the same logs and sums as the MRC movie holding its frames
+    bottom-up (CLoadTiffImage::mReadByStrip row order), with a float TIFF
+    gain (CLoadRefs::mLoadGainTiff) against the same gain as MRC.  The
+    reference program is built without libtiff, so this compares the
+    command line with itself across the two readers."""
+    PIL = pytest.importorskip("PIL.Image")
+    from motioncor3_b200 import build, mrcio, synthetic as S
+    build.build()
+    m = S.make_movie(384, 320, 10, dose=3.0, seed=47, gain=True)
+    u8 = np.minimum(m.frames, 255).astype(np.uint8)
+    gain = np.asarray(m.gain, np.float32)
+    tdir = tmp_path / "tif"
+    tdir.mkdir()
+    tif = str(tdir / "movie.tif")
+    ims = [PIL.fromarray(f) for f in u8]
+    ims[0].save(tif, save_all=True, append_images=ims[1:], compression="tiff_lzw")
+    gtif = str(tdir / "gain.tif")
+    PIL.fromarray(gain).save(gtif)
+    tags = "-Iter 6 -Tol 0.2 -Bft 300 -FmDose 1.2 -PixSize 0.9".split()
+    args = [OUR_BIN, "-InTiff", tif, "-OutMrc", str(tdir / "sum.mrc"), "-LogDir", str(tdir) + "/",
+            "-Gain", gtif, "-Gpu", "0"] + tags
+    p = subprocess.run(args, capture_output=True, text=True, env=_env(), timeout=900)
+    assert p.returncode == 0, (p.stdout + p.stderr)[-3000:]
+    ref = run_program(OUR_BIN, str(tmp_path / "mrc"), u8[:, ::-1], gain[::-1], tags)
+    a = _read_log(str(tdir / "movie-Full.log"))
+    b = _read_log(ref["logs"]["-Full.log"])
+    assert np.array_equal(a, b)
+    for suf in ref["sums"]:
+        t = mrcio.read(str(tdir / f"sum{suf}.mrc")).astype(np.float64)
+        assert np.array_equal(t, ref["sums"][suf]), suf
