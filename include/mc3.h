@@ -58,6 +58,10 @@ typedef struct {
   int out_stack[2];    /* -OutStack (0 1): 1 = also return the aligned frames;
                           second value: sum them in groups of this many frames
                           (CZbinStack, Align/CZbinStack.cpp:27-71)              */
+  float mag[3];        /* -Mag major minor angle (1 1 0): anisotropic
+                          magnification corrected on the sums
+                          (CCorrectFullShift::mCorrectMag,
+                          Correct/CCorrectFullShift.cpp:94-127)               */
 } mc3_params;
 
 /* Sizes a movie will use (CBufferPool::CreateBuffers, CBufferPool.cpp:95-270). */
@@ -69,6 +73,7 @@ typedef struct {
   float xcf_bin[2];    /* binning factors of the alignment image             */
   size_t device_bytes; /* device memory the context holds for this movie     */
   int out_size[2];     /* size of each output sum (binned by -FtBin)          */
+  int n_frames;        /* rendered frames (nz unless frame integration is set) */
 } mc3_plan_info;
 
 typedef struct {

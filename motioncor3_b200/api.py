@@ -52,6 +52,7 @@ class _Params(ctypes.Structure):
         ("gpu", ctypes.c_int),
         ("split_sum", ctypes.c_int),
         ("out_stack", ctypes.c_int * 2),
+        ("mag", ctypes.c_float * 3),
     ]
 
 
@@ -64,6 +65,7 @@ class _PlanInfo(ctypes.Structure):
         ("xcf_bin", ctypes.c_float * 2),
         ("device_bytes", ctypes.c_size_t),
         ("out_size", ctypes.c_int * 2),
+        ("n_frames", ctypes.c_int),
     ]
 
 
@@ -226,6 +228,7 @@ class Params:
     gpu: int = 0
     split_sum: int = 0
     out_stack: tuple = (0, 1)
+    mag: tuple = (1.0, 1.0, 0.0)
 
     def to_c(self) -> _Params:
         p = _Params()
@@ -250,6 +253,8 @@ class Params:
         p.gpu = int(self.gpu)
         p.split_sum = int(self.split_sum)
         p.out_stack[0], p.out_stack[1] = int(self.out_stack[0]), int(self.out_stack[1])
+        for i in range(3):
+            p.mag[i] = float(self.mag[i])
         return p
 
 
@@ -307,7 +312,8 @@ class MotionCor3:
         _check(_lib().mc3_plan(self._h, nx, ny, nz, ctypes.byref(info)), "mc3_plan")
         return dict(n_sums=info.n_sums, n_patches=info.n_patches, xcf_size=tuple(info.xcf_size),
                     patch_size=tuple(info.patch_size), xcf_bin=tuple(info.xcf_bin),
-                    device_bytes=info.device_bytes, out_size=tuple(info.out_size))
+                    device_bytes=info.device_bytes, out_size=tuple(info.out_size),
+                    n_frames=info.n_frames)
 
     def set_gain(self, gain) -> None:
         if gain is None:
@@ -408,6 +414,7 @@ class MotionCor3:
         nx, ny, nz = mv.nx, mv.ny, mv.nz
         info = self.plan(nx, ny, nz)
         ns, P = info["n_sums"], info["n_patches"]
+        nz = info["n_frames"]  # rendered frames: the tables below are per rendered frame
         it = int(self.params.iter)
         gsh = np.zeros((nz, 2), np.float32)
         psh = np.zeros((nz, max(P, 1), 2), np.float32)

@@ -65,6 +65,9 @@ void mc3_params_default(mc3_params* p) {
   p->split_sum = 0;
   p->out_stack[0] = 0;
   p->out_stack[1] = 1;
+  p->mag[0] = 1.0f;
+  p->mag[1] = 1.0f;
+  p->mag[2] = 0.0f;
 }
 
 int mc3_create(const mc3_params* p, mc3_ctx** out) {

@@ -292,7 +292,7 @@ int main(int argc, char** argv) {
                 "[-Patch x y] [-Iter n] [-Tol px] [-Bft g p] [-FmDose d] [-PixSize a] "
                 "[-kV kv] [-Group g p] [-FmRef f] [-SumRange lo hi] [-PhaseOnly 0|1] [-SplitSum 0|1] "
                 "[-FtBin b] [-OutAln dir] [-InAln dir] [-OutStack 0|1 zbin] [-FmIntFile file] "
-                "[-Dark dark.mrc] [-RotGain r] [-FlipGain f] [-InvGain 0|1] "
+                "[-Dark dark.mrc] [-RotGain r] [-FlipGain f] [-InvGain 0|1] [-Mag major minor angle] "
                 "[-LogDir dir] [-Gpu id]\n");
     return eSuccess;
   }
@@ -335,6 +335,13 @@ int main(int argc, char** argv) {
   A.ints("-FmRef", &p.fm_ref, 1);
   A.ints("-SplitSum", &p.split_sum, 1);  // CInput.cpp:657-663
   A.ints("-OutStack", p.out_stack, 2);    // CInput.cpp:590-592
+  {
+    float mg[3];
+    int f0, nmag;
+    // CInput.cpp:640-644: all three values or none
+    if (A.find("-Mag", &f0, &nmag) && nmag == 3 && A.floats("-Mag", mg, 3) == 3)
+      for (int i = 0; i < 3; ++i) p.mag[i] = mg[i];
+  }
   const std::string in_aln = A.str("-InAln");
   const std::string fmint_file = A.str("-FmIntFile");
   int gpu[8];
@@ -342,7 +349,7 @@ int main(int argc, char** argv) {
   const char* ignored[] = {"-InEer", "-InSuffix", "-InSkips", "-ArcDir",
                            "-DefectFile", "-DefectMap", "-FullSum", "-TmpFile",
                            "-StackZ", "-Cs", "-AmpCont", "-ExtPhase", "-Throw", "-Trunc", "-Serial",
-                           "-Tilt", "-Crop", "-Mag",
+                           "-Tilt", "-Crop",
                            "-InFmMotion", "-GpuMemUsage", "-UseGpus",
                            "-EerSampling", "-OutStar", "-TiffOrder", "-CorrInterp"};
   for (const char* t : ignored) {
@@ -566,7 +573,8 @@ int main(int argc, char** argv) {
     exts.push_back("_ODD");
     exts.push_back("_EVN");
   }
-  const float pix = p.pix_size * p.ft_bin;
+  // CInput::GetFinalPixelSize (CInput.cpp:709-715)
+  const float pix = p.pix_size * p.ft_bin / (p.mag[0] > p.mag[1] ? p.mag[0] : p.mag[1]);
   bool saved = true;
   for (int i = 0; i < r.n_sums; ++i) {
     const float* img = sums + (size_t)i * ox * oy;

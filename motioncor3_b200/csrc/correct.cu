@@ -459,6 +459,47 @@ int zbin_frames(float* frames, long fr_stride, int pitch, int W, int H, const in
   return kOk;
 }
 
+// mGStretch (Correct/GStretch.cu:14-44) on n padded real images: the output
+// pixel (x, y) of the W x H image reads the input bilinearly at
+// m * ((x, y) - c) + c, c = (W/2, H/2), m = [m0 m1; m1 m2]; a source outside
+// [1, W-1) x [1, H-1) is folded to (8111 |x| mod (W-1), 8111 |y| mod (H-1)).
+// The padding columns of the output are left as they are.
+__global__ void k_stretch(const float* __restrict__ in, float* __restrict__ out, int pitch,
+                          long stride, int W, int H, float m0, float m1, float m2) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= W) return;
+  const float* src = in + (long)blockIdx.z * stride;
+  const float cx = 0.5f * W, cy = 0.5f * H;
+  const float dx = x - cx, dy = y - cy;
+  float ox = dx * m0 + dy * m1 + cx;
+  float oy = dx * m1 + dy * m2 + cy;
+  if (ox < 1 || oy < 1 || ox >= (W - 1) || oy >= (H - 1)) {
+    // the fold in 64-bit arithmetic (the reference's int product is the same
+    // for sources within a few image widths, and never negative here)
+    const long long ax = (long long)fminf(fabsf(ox), 1.0e9f);
+    const long long ay = (long long)fminf(fabsf(oy), 1.0e9f);
+    ox = (float)((8111LL * ax) % (W - 1));
+    oy = (float)((8111LL * ay) % (H - 1));
+  }
+  const int ix = (int)ox, iy = (int)oy;
+  const float wx = ox - ix, wy = oy - iy;
+  const float* p = src + (long)iy * pitch + ix;
+  out[(long)blockIdx.z * stride + (long)y * pitch + x] =
+      (1 - wx) * (1 - wy) * p[0] + wx * (1 - wy) * p[1] + (1 - wx) * wy * p[pitch] +
+      wx * wy * p[pitch + 1];
+}
+
+int stretch_images(const float* in, float* out, int pitch, long stride, int W, int H, int n,
+                   const float* m, cudaStream_t st) {
+  if (W < 3 || H < 3 || n < 1) return kEInval;
+  dim3 grid(ceil_div(W, 128), H, n);
+  prof::Scope ps("k_stretch", (double)n * W * H * 8.0, st);
+  k_stretch<<<grid, 128, 0, st>>>(in, out, pitch, stride, W, H, m[0], m[1], m[2]);
+  MC3_CHECK_LAUNCH("k_stretch");
+  return kOk;
+}
+
 __global__ void k_unpad_positive(const float* in, long pitch, float* out, int W, int H,
                                  long in_stride) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;

@@ -243,6 +243,7 @@ int Engine::plan(int w, int h, int n, mc3_plan_info* info) {
   info->xcf_bin[1] = g.xcfBin[1];
   info->out_size[0] = g.outW;
   info->out_size[1] = g.outH;
+  info->n_frames = g.N;
   size_t cmp = (size_t)g.cmpX * g.cmpY * sizeof(float2);
   size_t xcf = (size_t)g.xcfCmpX * g.xcfCmpY * sizeof(float2);
   size_t bytes = cmp * g.N + xcf * g.N + cmp * (g.nSums + 2) + (size_t)g.W * g.H * 4 * g.N;
@@ -811,6 +812,29 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
     if (want_stack) MC3_TRY(write_stack(spec, false, g, fi, out));
   }
   if (out && !want_stack) out->stack_frames = 0;
+  // ---- 7b. CCorrectFullShift::mCorrectMag (Correct/CCorrectFullShift.cpp:94-127):
+  //      every sum to real space (unnormalised), stretched, forward again ----
+  float mm[3];
+  if (host::mag_matrix(prm.mag, mm)) {
+    const int n = g.nSums;
+    MC3_TRY(d_mag.ensure(sizeof(float2) * ncmp * n));
+    float2* S = d_sums.as<float2>();
+    Batch b{n, n, (long)ncmp, nullptr, (long)ncmp};
+    ColOps inv{};
+    inv.dir = 1;
+    inv.scale = 1.0f;
+    MC3_TRY(col_fft(S, S, g.cmpX, g.cmpX, H, b, inv, st));
+    Batch br{n, n, (long)ncmp, nullptr, (long)ncmp * 2};
+    MC3_TRY(row_c2r(S, g.cmpX, reinterpret_cast<float*>(S), g.padX, W, H, br, st));
+    MC3_TRY(stretch_images(reinterpret_cast<float*>(S), d_mag.as<float>(), g.padX, (long)ncmp * 2,
+                           W, H, n, mm, st));
+    Batch bf{n, n, (long)ncmp * 2, nullptr, (long)ncmp};
+    MC3_TRY(row_r2c(d_mag.as<float>(), g.padX, S, g.cmpX, W, H, bf, 1.0f, st));
+    ColOps fwd{};
+    fwd.dir = -1;
+    fwd.scale = (float)(1.0 / W / H);
+    MC3_TRY(col_fft(S, S, g.cmpX, g.cmpX, H, b, fwd, st));
+  }
   // ---- 8. sums to real space (CCorrectFullShift::mUnpadSums,
   //      Correct/CCorrectFullShift.cpp:146-185): Fourier crop to the -FtBin
   //      output size, C2R, positivity, unpad ----

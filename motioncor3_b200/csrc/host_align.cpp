@@ -9,6 +9,23 @@
 namespace mc3 {
 namespace host {
 
+// ---- Correct/GStretch.cu:53-72, Align/CAlignParam.cpp:55-72 ------------------
+bool mag_matrix(const float mag[3], float m[3]) {
+  if (!(mag[0] > 0 && mag[1] > 0)) return false;  // no meaningful stretch
+  const float stretch = mag[0] / mag[1];
+  const float axis = -1.0f * mag[2];
+  if (std::fabs(stretch - 1) < 1e-5) return false;
+  const double t2 = 2 * axis * 3.1416 / 180;  // the reference's value of pi
+  const double s2 = std::sin(t2), c2 = std::cos(t2);
+  const double dp = 0.5 * (stretch + 1), dm = 0.5 * (stretch - 1);
+  const float a0 = (float)(dp + dm * c2), a1 = (float)(1 * dm * s2), a2 = (float)(dp - dm * c2);
+  const float det = a0 * a2 - a1 * a1;
+  m[0] = a2 / det;
+  m[1] = -a1 / det;
+  m[2] = a0 / det;
+  return true;
+}
+
 // ---- DataUtil/CFmIntParam.cpp ------------------------------------------------
 void FmInt::plain(int n_raw, float fm_dose) {
   start.resize(n_raw);

@@ -99,6 +99,12 @@ void patch_detect_bads(const float* shifts, const float* centers, int n_frames, 
 void patch_starts(const float* map, int bx, int by, float mean, float m2, int px, int py,
                   int xcf_x, int xcf_y, int pat_x, int pat_y, std::vector<int>& starts);
 
+// GStretch::Setup (Correct/GStretch.cu:53-72) with the stretch and axis of
+// CAlignParam::GetMagStretch (Align/CAlignParam.cpp:55-72): the inverse of
+// the stretch matrix along -angle, as three floats.  Returns false when the
+// stretch is below 1e-5 (no correction).
+bool mag_matrix(const float mag[3], float m[3]);
+
 // Ring template of the defect detector (BadPixel/CTemplate.cpp:20-57).
 void defect_template(int ms, float* tpl);
 

@@ -93,6 +93,10 @@ int crop_frames(const float2* in, int inX, int inY, long in_stride, const float2
 // groups: device [2][n_groups] (starts, then sizes) of consecutive groups.
 int zbin_frames(float* frames, long fr_stride, int pitch, int W, int H, const int* groups,
                 int n_groups, cudaStream_t st);
+// Bilinear anisotropic stretch of n padded real images (GStretch); m: the
+// three entries of the symmetric inverse stretch matrix.
+int stretch_images(const float* in, float* out, int pitch, long stride, int W, int H, int n,
+                   const float* m, cudaStream_t st);
 // out[y*W+x] = max(0, in[y*pitch+x])
 int unpad_positive(const float* in, long pitch, float* out, int W, int H, int n,
                    long in_stride, cudaStream_t st);

@@ -12,7 +12,7 @@ uint32_t bswap32(uint32_t v) {
   return (v >> 24) | ((v >> 8) & 0xff00u) | ((v << 8) & 0xff0000u) | (v << 24);
 }
 uint16_t bswap16(uint16_t v) { return (uint16_t)((v >> 8) | (v << 8)); }
-bool valid_mode(int m) { return m == 0 || m == 1 || m == 2 || m == 6; }
+bool valid_mode(int m) { return m == 0 || m == 1 || m == 2 || m == 5 || m == 6 || m == 101; }
 }  // namespace
 
 int bytes_per_pixel(int mode) {

@@ -1060,6 +1060,8 @@ void oracle_default_params(oracle_params* p) {
   p->acc_dose = nullptr;
   p->dose_weight = 0;
   p->dark = nullptr;
+  p->mag[0] = p->mag[1] = 1.0f;
+  p->mag[2] = 0.0f;
 }
 
 void oracle_rfft2(const double* img, double* spec, int W, int H, int normalise) {
@@ -1368,6 +1370,40 @@ int oracle_process_movie(const oracle_params* p, const float* frames, int W, int
         }
     } else if (split) {
       for (long i = 0; i < ncmp; ++i) split[i] += X[i];
+    }
+  }
+  // CCorrectFullShift::mCorrectMag (Correct/CCorrectFullShift.cpp:94-127):
+  // each sum to real space, stretched (Correct/GStretch.cu), forward again
+  {
+    const float stretch = p->mag[0] / p->mag[1], axis = -1.0f * p->mag[2];
+    if (!(std::fabs(stretch - 1) < 1e-5)) {
+      const double t2 = 2 * axis * 3.1416 / 180;
+      const double dp = 0.5 * (stretch + 1), dm = 0.5 * (stretch - 1);
+      const float a0 = (float)(dp + dm * std::cos(t2)), a1 = (float)(dm * std::sin(t2));
+      const float a2 = (float)(dp - dm * std::cos(t2));
+      const float det = a0 * a2 - a1 * a1;
+      const float m0 = a2 / det, m1 = -a1 / det, m2 = a0 / det;
+      std::vector<double> img(npx), out(npx);
+      for (int s = 0; s < nSums; ++s) {
+        cd* S = &sums[(long)s * ncmp];
+        irfft2(S, img.data(), W, H);
+        const float cx = 0.5f * W, cy = 0.5f * H;
+        for (int y = 0; y < H; ++y)
+          for (int x = 0; x < W; ++x) {
+            const float dx = x - cx, dy = y - cy;
+            float ox = dx * m0 + dy * m1 + cx, oy = dx * m1 + dy * m2 + cy;
+            if (ox < 1 || oy < 1 || ox >= W - 1 || oy >= H - 1) {
+              ox = (float)((8111LL * (long long)std::fabs(ox)) % (W - 1));
+              oy = (float)((8111LL * (long long)std::fabs(oy)) % (H - 1));
+            }
+            const int ix = (int)ox, iy = (int)oy;
+            const double wx = ox - ix, wy = oy - iy;
+            const double* q = &img[(long)iy * W + ix];
+            out[(long)y * W + x] = (1 - wx) * (1 - wy) * q[0] + wx * (1 - wy) * q[1] +
+                                   (1 - wx) * wy * q[W] + wx * wy * q[W + 1];
+          }
+        rfft2(out.data(), S, W, H, true);
+      }
     }
   }
   // mUnpadSums (CCorrectFullShift.cpp:146-185): Fourier crop to the -FtBin

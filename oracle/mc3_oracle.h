@@ -47,6 +47,7 @@ typedef struct {
   const float* acc_dose;
   int dose_weight;
   const float* dark;  /* [H][W] dark reference subtracted before the gain, or NULL */
+  float mag[3];       /* -Mag major minor angle (1 1 0 = none)             */
 } oracle_params;
 
 typedef struct {

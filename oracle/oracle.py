@@ -74,6 +74,7 @@ class OracleParams(ctypes.Structure):
         ("acc_dose", _VP),
         ("dose_weight", ctypes.c_int),
         ("dark", _VP),
+        ("mag", ctypes.c_float * 3),
     ]
 
 
@@ -115,9 +116,9 @@ def params(**kw) -> OracleParams:
     p = OracleParams()
     lib().oracle_default_params(ctypes.byref(p))
     for k, v in kw.items():
-        if k in ("patch", "bft", "group", "sum_range", "out_stack"):
+        if k in ("patch", "bft", "group", "sum_range", "out_stack", "mag"):
             arr = getattr(p, k)
-            for i, x in enumerate(v[:2]):
+            for i, x in enumerate(v[:len(arr)]):
                 arr[i] = x
         else:
             setattr(p, k, v)

