@@ -62,6 +62,9 @@ typedef struct {
                           magnification corrected on the sums
                           (CCorrectFullShift::mCorrectMag,
                           Correct/CCorrectFullShift.cpp:94-127)               */
+  int in_fm_motion;    /* -InFmMotion (0): weight each aligned frame by the
+                          directional sinc of its in-frame motion
+                          (MotionDecon/GMotionWeight.cu, CInFrameMotion)      */
 } mc3_params;
 
 /* Sizes a movie will use (CBufferPool::CreateBuffers, CBufferPool.cpp:95-270). */

@@ -53,6 +53,7 @@ class _Params(ctypes.Structure):
         ("split_sum", ctypes.c_int),
         ("out_stack", ctypes.c_int * 2),
         ("mag", ctypes.c_float * 3),
+        ("in_fm_motion", ctypes.c_int),
     ]
 
 
@@ -229,6 +230,7 @@ class Params:
     split_sum: int = 0
     out_stack: tuple = (0, 1)
     mag: tuple = (1.0, 1.0, 0.0)
+    in_fm_motion: int = 0
 
     def to_c(self) -> _Params:
         p = _Params()
@@ -255,6 +257,7 @@ class Params:
         p.out_stack[0], p.out_stack[1] = int(self.out_stack[0]), int(self.out_stack[1])
         for i in range(3):
             p.mag[i] = float(self.mag[i])
+        p.in_fm_motion = int(self.in_fm_motion)
         return p
 
 

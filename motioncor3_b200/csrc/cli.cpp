@@ -292,7 +292,7 @@ int main(int argc, char** argv) {
                 "[-Patch x y] [-Iter n] [-Tol px] [-Bft g p] [-FmDose d] [-PixSize a] "
                 "[-kV kv] [-Group g p] [-FmRef f] [-SumRange lo hi] [-PhaseOnly 0|1] [-SplitSum 0|1] "
                 "[-FtBin b] [-OutAln dir] [-InAln dir] [-OutStack 0|1 zbin] [-FmIntFile file] "
-                "[-Dark dark.mrc] [-RotGain r] [-FlipGain f] [-InvGain 0|1] [-Mag major minor angle] "
+                "[-Dark dark.mrc] [-RotGain r] [-FlipGain f] [-InvGain 0|1] [-Mag major minor angle] [-InFmMotion 0|1] "
                 "[-LogDir dir] [-Gpu id]\n");
     return eSuccess;
   }
@@ -335,6 +335,7 @@ int main(int argc, char** argv) {
   A.ints("-FmRef", &p.fm_ref, 1);
   A.ints("-SplitSum", &p.split_sum, 1);  // CInput.cpp:657-663
   A.ints("-OutStack", p.out_stack, 2);    // CInput.cpp:590-592
+  A.ints("-InFmMotion", &p.in_fm_motion, 1);
   {
     float mg[3];
     int f0, nmag;
@@ -350,7 +351,7 @@ int main(int argc, char** argv) {
                            "-DefectFile", "-DefectMap", "-FullSum", "-TmpFile",
                            "-StackZ", "-Cs", "-AmpCont", "-ExtPhase", "-Throw", "-Trunc", "-Serial",
                            "-Tilt", "-Crop",
-                           "-InFmMotion", "-GpuMemUsage", "-UseGpus",
+                           "-GpuMemUsage", "-UseGpus",
                            "-EerSampling", "-OutStar", "-TiffOrder", "-CorrInterp"};
   for (const char* t : ignored) {
     int f, n;

@@ -500,6 +500,58 @@ int stretch_images(const float* in, float* out, int pitch, long stride, int W, i
   return kOk;
 }
 
+// GMotionWeight::DirWeight (MotionDecon/GMotionWeight.cu:14-36, 56-68,
+// 92-107): the spectrum of frame f is multiplied by the sinc of its in-frame
+// motion m_f measured along m_f: frequency (x, y) (y signed) lies at distance
+// |s x - y| / sqrt(s^2 + 1), s = -m.x / (m.y + 1e-20), from the line through
+// the origin perpendicular to m (x itself when |s| > 1e5); with
+// d = distance / (2 (cmpX - 1)) the weight is sin(pi |m| d) / (pi |m| d),
+// 0 once |m| d > 1, and 1 when the distance is below 0.1.  DC is left alone;
+// frames whose |m| is below 0.1 px are skipped (flag 0).
+__global__ void k_motion_decon(float2* spec, long fr_stride, int cmpX, int cmpY,
+                               const float4* __restrict__ motion) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  const int f = blockIdx.z;
+  if (x >= cmpX) return;
+  const float4 m = motion[f];  // (m.x, m.y, apply flag, unused)
+  if (m.z == 0.0f || (x == 0 && y == 0)) return;
+  const float shift = sqrtf(m.x * m.x + m.y * m.y);
+  if (shift < 0.1f) return;
+  const float slope = -m.x / (m.y + (float)1e-20);
+  float dist;
+  if (fabsf(slope) > (float)1e5) {
+    dist = (float)x;
+  } else {
+    const int ys = y > cmpY / 2 ? y - cmpY : y;
+    dist = fabsf(slope * x - ys) / sqrtf(slope * slope + 1.0f);
+  }
+  if (dist < 0.1f) return;
+  const float pi = 3.141592654f;
+  dist = dist / (2 * (cmpX - 1));
+  float w;
+  if (shift * dist > 1.0f) {
+    w = 0.0f;
+  } else {
+    w = sinf(pi * shift * dist) / (pi * shift * dist);
+  }
+  float2* p = spec + (long)f * fr_stride + (long)y * cmpX + x;
+  float2 v = *p;
+  v.x *= w;
+  v.y *= w;
+  *p = v;
+}
+
+int motion_decon(float2* spec, long fr_stride, int cmpX, int cmpY, int N, const float4* motion,
+                 cudaStream_t st) {
+  if (N < 1 || N > 65535 || cmpX < 2) return kEInval;
+  dim3 grid(ceil_div(cmpX, 128), cmpY, N);
+  prof::Scope ps("k_motion_decon", (double)N * cmpX * cmpY * 16.0, st);
+  k_motion_decon<<<grid, 128, 0, st>>>(spec, fr_stride, cmpX, cmpY, motion);
+  MC3_CHECK_LAUNCH("k_motion_decon");
+  return kOk;
+}
+
 __global__ void k_unpad_positive(const float* in, long pitch, float* out, int W, int H,
                                  long in_stride) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;

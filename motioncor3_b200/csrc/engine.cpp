@@ -765,6 +765,22 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
     }
   }
   MC3_TRY(global_sums(spec, N, fs, g));
+  if (prm.in_fm_motion) {
+    // -InFmMotion: CCorrectFullShift::mMotionDecon (Correct/CCorrectFullShift.cpp:309-318)
+    // in global mode, CGenRealStack::mMotionDecon (Correct/CGenRealStack.cpp:156-166)
+    // on the globally corrected frames in patch mode; motion of frame f =
+    // s(f+1) - s(f), of the last frame s(N-1) - s(N-2) (CInFrameMotion::GetFullMotion)
+    std::vector<float4> mo(N);
+    for (int f = 0; f < N; ++f) {
+      const int f1 = f == N - 1 ? f - 1 : f, f2 = f == N - 1 ? f : f + 1;
+      const float mx = fs.x(f2) - fs.x(f1), my = fs.y(f2) - fs.y(f1);
+      const double d = sqrtf(mx * mx + my * my);  // GMotionWeight::DirWeight skip test
+      mo[f] = make_float4(mx, my, d < 0.1 ? 0.0f : 1.0f, 0.0f);
+    }
+    MC3_TRY(d_motion.ensure(sizeof(float4) * N));
+    MC3_CUDA(cudaMemcpyAsync(d_motion.p, mo.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, st));
+    MC3_TRY(motion_decon(spec, (long)ncmp, g.cmpX, g.cmpY, N, d_motion.as<float4>(), st));
+  }
   if (!g.patch) {
     MC3_TRY(frame_sums(spec, (long)ncmp, N, g.cmpX, g.cmpY, d_fex.as<float2>(), d_fey.as<float2>(),
                        d_acc.as<float>(), d_Wn.as<float>(), dp, d_sums.as<float2>(), g.nSums, st));

@@ -97,6 +97,10 @@ int zbin_frames(float* frames, long fr_stride, int pitch, int W, int H, const in
 // three entries of the symmetric inverse stretch matrix.
 int stretch_images(const float* in, float* out, int pitch, long stride, int W, int H, int n,
                    const float* m, cudaStream_t st);
+// In-frame motion weighting of N frame spectra; motion[f] = (m.x, m.y,
+// apply, 0) per frame.
+int motion_decon(float2* spec, long fr_stride, int cmpX, int cmpY, int N, const float4* motion,
+                 cudaStream_t st);
 // out[y*W+x] = max(0, in[y*pitch+x])
 int unpad_positive(const float* in, long pitch, float* out, int W, int H, int n,
                    long in_stride, cudaStream_t st);

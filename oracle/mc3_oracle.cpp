@@ -1062,6 +1062,7 @@ void oracle_default_params(oracle_params* p) {
   p->dark = nullptr;
   p->mag[0] = p->mag[1] = 1.0f;
   p->mag[2] = 0.0f;
+  p->in_fm_motion = 0;
 }
 
 void oracle_rfft2(const double* img, double* spec, int W, int H, int normalise) {
@@ -1340,6 +1341,33 @@ int oracle_process_movie(const oracle_params* p, const float* frames, int W, int
     float s[2] = {-fs.x(f), -fs.y(f)};
     double d = (double)std::sqrt((float)(s[0] * s[0] + s[1] * s[1]));
     if (!(d < 0.1)) phase_shift(X, X, g.cmpX, g.cmpY, s[0], s[1], false);
+    if (p->in_fm_motion) {
+      // CInFrameMotion::GetFullMotion + GMotionWeight::DirWeight
+      // (MotionDecon/CInFrameMotion.cpp:78-97, MotionDecon/GMotionWeight.cu:14-36)
+      const int f1 = f == N - 1 ? f - 1 : f, f2 = f == N - 1 ? f : f + 1;
+      const float mx = fs.x(f2) - fs.x(f1), my = fs.y(f2) - fs.y(f1);
+      const double mot = std::sqrt((float)(mx * mx + my * my));
+      if (!(mot < 0.1)) {
+        const float shift = std::sqrt(mx * mx + my * my);
+        const float slope = -mx / (my + (float)1e-20);
+        for (int y = 0; y < g.cmpY; ++y)
+          for (int x = 0; x < g.cmpX; ++x) {
+            if (x == 0 && y == 0) continue;
+            float dist;
+            if (std::fabs(slope) > (float)1e5) {
+              dist = (float)x;
+            } else {
+              const int ys = y > g.cmpY / 2 ? y - g.cmpY : y;
+              dist = std::fabs(slope * x - ys) / std::sqrt(slope * slope + 1.0f);
+            }
+            if (dist < 0.1f) continue;
+            dist = dist / (2 * (g.cmpX - 1));
+            const double a = 3.141592654 * shift * dist;
+            const double w = (shift * dist > 1.0f) ? 0.0 : std::sin(a) / a;
+            X[(long)y * g.cmpX + x] *= w;
+          }
+      }
+    }
     if (patchMode) {
       irfft2(X, realf.data(), W, H);
       local_gather(realf.data(), gath.data(), W, H, patCent.data(), &patShift[(long)f * P * 2],

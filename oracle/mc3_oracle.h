@@ -48,6 +48,7 @@ typedef struct {
   int dose_weight;
   const float* dark;  /* [H][W] dark reference subtracted before the gain, or NULL */
   float mag[3];       /* -Mag major minor angle (1 1 0 = none)             */
+  int in_fm_motion;   /* -InFmMotion: in-frame motion weighting            */
 } oracle_params;
 
 typedef struct {

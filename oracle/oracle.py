@@ -75,6 +75,7 @@ class OracleParams(ctypes.Structure):
         ("dose_weight", ctypes.c_int),
         ("dark", _VP),
         ("mag", ctypes.c_float * 3),
+        ("in_fm_motion", ctypes.c_int),
     ]
 
 

@@ -432,6 +432,37 @@ def test_pipeline_mag_correction(api, oracle, torch_cuda, patch):
         assert e <= 1e-4, (i, e)
 
 
+@pytest.mark.parametrize("patch", [False, True])
+def test_pipeline_in_frame_motion(api, oracle, torch_cuda, patch):
+    """-InFmMotion 1: the directional sinc weight of each frame's motion
+    (CCorrectFullShift::mMotionDecon in global mode, CGenRealStack on the
+    globally corrected frames in patch mode), against the oracle."""
+    from motioncor3_b200 import synthetic as S
+    if patch:
+        m = S.make_movie(512, 512, 12, dose=4.0, seed=33, gain=False, local=True)
+        p = api.Params(patch=(3, 3), iter=5, tol=0.2, bft=(500, 150), fm_dose=1.0, pix_size=1.0,
+                       in_fm_motion=1, out_stack=(1, 1))
+    else:
+        m = S.make_movie(384, 320, 10, dose=3.0, seed=50, gain=False)
+        p = api.Params(iter=6, tol=0.2, bft=(300, 100), fm_dose=1.2, pix_size=0.9,
+                       in_fm_motion=1, out_stack=(1, 1))
+    with api.MotionCor3(p) as mc:
+        res = mc.process(np.asarray(m.frames))
+    force = dict(global_shifts=res.global_shifts)
+    if patch:
+        force.update(patch_shifts=res.patch_shifts, patch_centers=res.patch_centers,
+                     patch_bad=res.patch_bad)
+    kw = _oracle_kw(p)
+    kw["in_fm_motion"] = 1
+    same = oracle.process_movie(np.asarray(m.frames), force=force, **kw)
+    for i in range(res.n_sums):
+        e = _rel_rms(res.sums[i], same["sums"][i])
+        assert e <= 1e-4, (i, e)
+    for f in range(res.stack.shape[0]):
+        e = _rel_rms(res.stack[f], same["stack"][f])
+        assert e <= 1e-4, (f, e)
+
+
 def test_pipeline_config1_full_size(api, oracle, torch_cuda):
     """40 frames of 1024x1024, global alignment only (-Patch 0 0 -Iter 7
     -Tol 0.5 -Bft 150 -PixSize 1.0), dose 1 e/px/frame, unit gain."""

@@ -236,3 +236,21 @@ def test_oracle_mag_stretch_of_the_sums(oracle):
     inner = (slice(4, H - 4), slice(8, W - 8))
     rel = np.abs(st[inner] - ref[inner]).max() / np.abs(ref[inner]).max()
     assert rel < 2e-3, rel
+
+
+def test_oracle_in_frame_motion_weighting(oracle):
+    """-InFmMotion: each aligned frame is damped by the directional sinc of
+    its motion (MotionDecon/GMotionWeight.cu); the DC term (the mean) is
+    untouched and high frequencies lose power."""
+    from motioncor3_b200 import synthetic as S
+    m = S.make_movie(192, 160, 8, dose=20.0, seed=14)
+    kw = dict(iter=4, tol=0.2, bft=(300, 100), pix_size=1.0)
+    a = oracle.process_movie(m.frames, **kw)
+    b = oracle.process_movie(m.frames, in_fm_motion=1, **kw)
+    assert np.array_equal(a["global_shifts"], b["global_shifts"])
+    sa, sb = a["sums"][0].astype(np.float64), b["sums"][0].astype(np.float64)
+    assert abs(sa.mean() - sb.mean()) <= 1e-5 * sa.mean()
+    Fa, Fb = np.abs(np.fft.rfft2(sa)), np.abs(np.fft.rfft2(sb))
+    hi = np.zeros_like(Fa, bool)
+    hi[40:-40, 40:] = True
+    assert Fb[hi].sum() < 0.99 * Fa[hi].sum()
