@@ -137,6 +137,9 @@ typedef struct {
   const int* size;        /* [n_int]                                           */
   const float* acc_dose;  /* [n_int] e/A^2                                     */
   int dose_weight;
+  int rendered;           /* 1: movies already hold the n_int rendered frames
+                             (EER, rendered by mc3_eer_render); the tables then
+                             only give doses, groups and time stamps          */
 } mc3_frame_integration;
 
 /* ---- library ---- */
@@ -287,6 +290,17 @@ int mc3_tiff_info(const char* path, int* nx, int* ny, int* nz, int* mode);
  * into dst [nz][ny][nx] in the file's pixel type, rows bottom-up as the
  * reference stores them; threads <= 0 uses every host core. */
 int mc3_tiff_read(const char* path, int z0, int nz, void* dst, int threads);
+
+/* EerUtil/CLoadEerHeader.cpp:22-51: camera size, number of EER frames (TIFF
+ * directories) and run-length bits (65001 -> 7, 65000 -> 8). */
+int mc3_eer_info(const char* path, int* cam_x, int* cam_y, int* n_frames, int* bits);
+/* EerUtil/CRenderMrcStack.cpp + CDecodeEerFrame.cpp: n_out rendered 8-bit
+ * frames, frame i the electron counts of EER frames start[i] ..
+ * start[i]+size[i]-1, at -EerSampling 1, 2 or 3 (camera size x 1, 2, 4;
+ * super-resolution needs 4096-pixel rows), into dst [n_out][ny][nx]; EER
+ * frames decoded on threads (<= 0: every host core). */
+int mc3_eer_render(const char* path, int sampling, int n_out, const int* start, const int* size,
+                   unsigned char* dst, int threads);
 
 /* ---- host-side bookkeeping (host pointers) ---- */
 /* CLoadRefs::PostProcess (CLoadRefs.cpp:204-229): rotation by rot x 90

@@ -108,6 +108,7 @@ class _FrameIntegration(ctypes.Structure):
         ("size", ctypes.c_void_p),
         ("acc_dose", ctypes.c_void_p),
         ("dose_weight", ctypes.c_int),
+        ("rendered", ctypes.c_int),
     ]
 
 
@@ -142,6 +143,8 @@ _SIGS = {
     "mc3_ref_augment": ([_VP, _I, _I, _I, _VP], _I),
     "mc3_tiff_info": ([ctypes.c_char_p, _VP, _VP, _VP, _VP], _I),
     "mc3_tiff_read": ([ctypes.c_char_p, _I, _I, _VP, _I], _I),
+    "mc3_eer_info": ([ctypes.c_char_p, _VP, _VP, _VP, _VP], _I),
+    "mc3_eer_render": ([ctypes.c_char_p, _I, _I, _VP, _VP, _VP, _I], _I),
     "mc3_process_movie": ([_VP, ctypes.POINTER(_Movie), ctypes.POINTER(_Result)], _I),
     "mc3_prefetch_movie": ([_VP, ctypes.POINTER(_Movie)], _I),
     "mc3_set_alignment": ([_VP, ctypes.POINTER(_Alignment)], _I),
@@ -395,7 +398,8 @@ class MotionCor3:
         _check(_lib().mc3_set_alignment(self._h, ctypes.byref(a)), "mc3_set_alignment")
         del keep  # the library copies the tables
 
-    def set_frame_integration(self, tables: Optional[dict], n_raw: int = 0) -> None:
+    def set_frame_integration(self, tables: Optional[dict], n_raw: int = 0,
+                              rendered: bool = False) -> None:
         """Rendered frames for the following movies of n_raw raw frames
         (mc3_set_frame_integration); tables as frame_integration_tables()
         returns them; None clears."""
@@ -406,7 +410,7 @@ class MotionCor3:
         sz = np.ascontiguousarray(tables["size"], np.int32)
         acc = np.ascontiguousarray(tables["acc_dose"], np.float32)
         fi = _FrameIntegration(n_raw, len(st), st.ctypes.data, sz.ctypes.data, acc.ctypes.data,
-                               int(tables.get("dose_weight", 0)))
+                               int(tables.get("dose_weight", 0)), int(rendered))
         _check(_lib().mc3_set_frame_integration(self._h, ctypes.byref(fi)),
                "mc3_set_frame_integration")
 
@@ -571,6 +575,26 @@ def tiff_read(path: str, z0: int = 0, nz: Optional[int] = None, threads: int = 0
     nz = info["nz"] - z0 if nz is None else nz
     out = np.zeros((nz, info["ny"], info["nx"]), _TIFF_DT[info["mode"]])
     _check(_lib().mc3_tiff_read(path.encode(), z0, nz, out.ctypes.data, threads), "mc3_tiff_read")
+    return out
+
+
+def eer_info(path: str) -> dict:
+    """mc3_eer_info: camera size, EER frame count and run-length bits."""
+    v = [ctypes.c_int(0) for _ in range(4)]
+    _check(_lib().mc3_eer_info(path.encode(), *[ctypes.byref(x) for x in v]), "mc3_eer_info")
+    return dict(cam_x=v[0].value, cam_y=v[1].value, n_frames=v[2].value, bits=v[3].value)
+
+
+def eer_render(path: str, start, size, sampling: int = 1, threads: int = 0) -> np.ndarray:
+    """mc3_eer_render: rendered 8-bit frames, frame i the electrons of EER
+    frames start[i] .. start[i]+size[i]-1."""
+    info = eer_info(path)
+    f = {1: 1, 2: 2, 3: 4}[sampling]
+    st = np.ascontiguousarray(start, np.int32)
+    sz = np.ascontiguousarray(size, np.int32)
+    out = np.zeros((len(st), info["cam_y"] * f, info["cam_x"] * f), np.uint8)
+    _check(_lib().mc3_eer_render(path.encode(), sampling, len(st), st.ctypes.data, sz.ctypes.data,
+                                 out.ctypes.data, threads), "mc3_eer_render")
     return out
 
 

@@ -288,7 +288,8 @@ int main(int argc, char** argv) {
     return eSuccess;
   }
   if (argc <= 1 || (argc == 2 && strcasecmp(argv[1], "--help") == 0)) {
-    std::printf("Usage: MotionCor3 -InMrc movie.mrc|-InTiff movie.tif -OutMrc sum.mrc [-Gain gain.mrc] "
+    std::printf("Usage: MotionCor3 -InMrc movie.mrc|-InTiff movie.tif|-InEer movie.eer "
+                "[-EerSampling 1|2|3] -OutMrc sum.mrc [-Gain gain.mrc] "
                 "[-Patch x y] [-Iter n] [-Tol px] [-Bft g p] [-FmDose d] [-PixSize a] "
                 "[-kV kv] [-Group g p] [-FmRef f] [-SumRange lo hi] [-PhaseOnly 0|1] [-SplitSum 0|1] "
                 "[-FtBin b] [-OutAln dir] [-InAln dir] [-OutStack 0|1 zbin] [-FmIntFile file] "
@@ -302,7 +303,10 @@ int main(int argc, char** argv) {
   // -InMrc or -InTiff (CInput::IsInTiff, CInput.cpp:697-700); `in_mrc` names
   // the input file either way (logs, .aln names)
   const std::string in_tiff = A.str("-InTiff");
-  const std::string in_mrc = in_tiff.empty() ? A.str("-InMrc") : in_tiff;
+  const std::string in_eer = A.str("-InEer");  // CInput::IsInEer (CInput.cpp:703-707)
+  int eer_sampling = 1;
+  A.ints("-EerSampling", &eer_sampling, 1);   // CInput.cpp:502-504
+  const std::string in_mrc = !in_tiff.empty() ? in_tiff : (!in_eer.empty() ? in_eer : A.str("-InMrc"));
   const std::string out_mrc = A.str("-OutMrc");
   const std::string gain_mrc = A.str("-Gain");
   const std::string dark_mrc = A.str("-Dark");
@@ -347,12 +351,12 @@ int main(int argc, char** argv) {
   const std::string fmint_file = A.str("-FmIntFile");
   int gpu[8];
   if (A.ints("-Gpu", gpu, 8) > 0) p.gpu = gpu[0];
-  const char* ignored[] = {"-InEer", "-InSuffix", "-InSkips", "-ArcDir",
+  const char* ignored[] = { "-InSuffix", "-InSkips", "-ArcDir",
                            "-DefectFile", "-DefectMap", "-FullSum", "-TmpFile",
                            "-StackZ", "-Cs", "-AmpCont", "-ExtPhase", "-Throw", "-Trunc", "-Serial",
                            "-Tilt", "-Crop",
                            "-GpuMemUsage", "-UseGpus",
-                           "-EerSampling", "-OutStar", "-TiffOrder", "-CorrInterp"};
+                           "-OutStar", "-TiffOrder", "-CorrInterp"};
   for (const char* t : ignored) {
     int f, n;
     A.find(t, &f, &n);
@@ -362,7 +366,22 @@ int main(int argc, char** argv) {
   if (in_mrc == out_mrc) return eInputOutputSame;
 
   mc3::mrc::Header h;
-  if (!in_tiff.empty()) {
+  int eer_bits = 0;
+  if (!in_eer.empty()) {
+    // EER: the raw frames are the electron-event frames; they are rendered
+    // below at -EerSampling into 8-bit frames (CLoadEerMain / CRenderMrcStack)
+    int cx = 0, cy = 0;
+    if (eer_sampling < 1 || eer_sampling > 3 ||
+        mc3_eer_info(in_eer.c_str(), &cx, &cy, &h.nz, &eer_bits) != MC3_OK) {
+      std::fprintf(stderr, "Error: cannot load EER file %s\n", in_eer.c_str());
+      return eFailLoad;
+    }
+    const int fact = eer_sampling == 2 ? 2 : (eer_sampling == 3 ? 4 : 1);
+    h.nx = cx * fact;
+    h.ny = cy * fact;
+    h.mode = 0;
+    std::printf("EER file size bits: %d  %d  %d  %d\n", cx, cy, h.nz, eer_bits);
+  } else if (!in_tiff.empty()) {
     if (mc3_tiff_info(in_tiff.c_str(), &h.nx, &h.ny, &h.nz, &h.mode) != MC3_OK) {
       std::fprintf(stderr, "CLoadTiffStack: cannot open Tiff file, skip,\n   %s\n\n",
                    in_tiff.c_str());
@@ -406,6 +425,18 @@ int main(int argc, char** argv) {
       }
     }
   }
+  if (!in_eer.empty() && !fi_on) {  // every EER frame rendered on its own
+    fi_start.resize(h.nz);
+    fi_size.assign(h.nz, 1);
+    fi_acc.resize(h.nz);
+    for (int i = 0; i < h.nz; ++i) {
+      fi_start[i] = i;
+      fi_acc[i] = p.fm_dose * (i + 1);  // CFmIntParam::mSetup
+    }
+    fi_dose = 0;
+    fi_on = true;
+  }
+  const int n_raw = h.nz;
   const int n_render = fi_on ? (int)fi_start.size() : h.nz;
   // -InAln (CMain::mOpenInAlnFile, CMain.cpp:382-398): the file's patch
   // grid and throws replace the command line's.
@@ -432,8 +463,15 @@ int main(int argc, char** argv) {
     }
   }
   const size_t frame_bytes = (size_t)mc3::mrc::frame_bytes(h.mode, h.nx, h.ny);
+  if (!in_eer.empty()) h.nz = n_render;  // the movie handed over holds the rendered frames
   HostBuf frames(frame_bytes * h.nz);
-  if (!in_tiff.empty()) {
+  if (!in_eer.empty()) {
+    if (mc3_eer_render(in_eer.c_str(), eer_sampling, n_render, fi_start.data(), fi_size.data(),
+                       frames.as<unsigned char>(), 0) != MC3_OK) {
+      std::fprintf(stderr, "Error: cannot decode EER frames of %s\n", in_eer.c_str());
+      return eFailLoad;
+    }
+  } else if (!in_tiff.empty()) {
     if (mc3_tiff_read(in_tiff.c_str(), 0, h.nz, frames.p, 0) != MC3_OK) {
       std::fprintf(stderr, "error: load tiff images of %s\n", in_tiff.c_str());
       return eFailLoad;
@@ -507,8 +545,8 @@ int main(int argc, char** argv) {
   }
   mc3_plan_info info;
   if (fi_on) {
-    mc3_frame_integration fi{h.nz, (int)fi_start.size(), fi_start.data(), fi_size.data(),
-                             fi_acc.data(), fi_dose};
+    mc3_frame_integration fi{n_raw, (int)fi_start.size(), fi_start.data(), fi_size.data(),
+                             fi_acc.data(), fi_dose, in_eer.empty() ? 0 : 1};
     if ((s = mc3_set_frame_integration(ctx, &fi)) != MC3_OK) {
       std::fprintf(stderr, "Error: %s\n", mc3_strerror(s));
       mc3_destroy(ctx);

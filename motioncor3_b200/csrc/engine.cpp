@@ -231,7 +231,7 @@ int Engine::set_dark(const float* dark, int w, int h, bool on_device) {
 
 int Engine::plan(int w, int h, int n, mc3_plan_info* info) {
   Geometry g;
-  if (fmint && n != fmint_raw) return kEInval;
+  if (fmint && n != (fmint_rendered ? fmint_tab.count() : fmint_raw)) return kEInval;
   MC3_TRY(g.compute(w, h, fmint ? fmint_tab.count() : n, prm, fmint && fmint_dose));
   info->n_sums = g.nSums;
   info->n_patches = g.P;
@@ -413,6 +413,7 @@ int Engine::set_frame_integration(const mc3_frame_integration* fi) {
   fmint_tab = t;
   fmint_raw = fi->n_raw;
   fmint_dose = fi->dose_weight != 0;
+  fmint_rendered = fi->rendered != 0;
   fmint = true;
   return kOk;
 }
@@ -483,7 +484,8 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
   const size_t fbytes = raw_frame_bytes(mv.mode, mv.nx, mv.ny);
   if (!fbytes) return kEUnsupported;
   Geometry g;
-  if (fmint && mv.nz != fmint_raw) {
+  const int expect_nz = fmint ? (fmint_rendered ? fmint_tab.count() : fmint_raw) : mv.nz;
+  if (mv.nz != expect_nz) {
     last_error = "movie frame count differs from the frame-integration table";
     return kEInval;
   }
@@ -491,7 +493,8 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
   MC3_TRY(g.compute(mv.nx, mv.ny, fi.count(), prm, fmint && fmint_dose));
   const int Nraw = mv.nz;
   bool render = false;  // some rendered frame sums several raw frames
-  for (int i = 0; fmint && i < fi.count(); ++i) render = render || fi.size[i] != 1 || fi.start[i] != i;
+  for (int i = 0; fmint && !fmint_rendered && i < fi.count(); ++i)
+    render = render || fi.size[i] != 1 || fi.start[i] != i;
   if (render && !(mv.mode == 0 || mv.mode == 5 || mv.mode == 101)) {
     // the reference renders integrated frames as 8-bit (CLoadCryoEMStack::OpenFile)
     last_error = "frame integration needs an 8-bit or 4-bit movie";

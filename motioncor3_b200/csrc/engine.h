@@ -110,6 +110,7 @@ class Engine {
   bool fmint = false;
   int fmint_raw = 0;
   bool fmint_dose = false;
+  bool fmint_rendered = false;  // the movie holds the rendered frames already
   host::FmInt fmint_tab;
   DevBuf d_istart, d_isize;
   DevBuf d_dark;

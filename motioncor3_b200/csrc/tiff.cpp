@@ -7,7 +7,7 @@
 // mReadMode (:121-148): 8 bits -> MRC mode 0, 16 bits -> 1 (signed sample
 // format) or 6, 32-bit IEEE float -> 2.  Rows are stored bottom-up as
 // CLoadTiffImage::mReadByStrip / mReadByTile write them (TIFF row r lands in
-// frame row ny-1-r).
+// frame row ny-1-r).  EER movies (-InEer) share the container parsing.
 #include <zlib.h>
 
 #include <algorithm>
@@ -354,9 +354,178 @@ bool read_page(FILE* f, const Page& pg, bool be, uint8_t* dst) {
   return true;
 }
 
+// ---- EER (electron-event representation) frames --------------------------
+// One TIFF directory per EER frame, its strips concatenated
+// (EerUtil/CLoadEerFrames.cpp:77-95); compression 65001 = 7-bit run lengths,
+// 65000 = 8-bit run lengths, each followed by a 4-bit sub-pixel code
+// (EerUtil/CLoadEerHeader.cpp:22-51).
+struct EerDecoder {
+  int cam_w = 0, cam_h = 0, bits = 0, sampling = 1;
+  int frm_w = 0;
+  // sub-pixel bit selection of CDecodeEerFrame::Setup (EerUtil/CDecodeEerFrame.cpp:17-41)
+  int sh0 = 0, and0 = 0, sh1 = 0, and1 = 0, sh2 = 0;
+  bool setup(int w, int h, int b, int smp) {
+    cam_w = w;
+    cam_h = h;
+    bits = b;
+    sampling = smp;
+    const int fact = smp == 2 ? 2 : (smp == 3 ? 4 : 1);
+    if (smp == 2) { sh0 = 1; and0 = 2; sh1 = 1; and1 = 8; sh2 = 3; }
+    if (smp == 3) { sh0 = 2; and0 = 3; sh1 = 0; and1 = 12; sh2 = 2; }
+    frm_w = w * fact;
+    // the super-resolution position arithmetic assumes 4096-pixel rows
+    return smp == 1 || w == 4096;
+  }
+  // CDecodeEerFrame::mFindElectron (:167-175)
+  void electron(uint32_t n, unsigned s, uint8_t* frm) const {
+    const uint32_t x = ((n & 4095u) << sh0) | ((s & and0) >> sh1);
+    const uint32_t y = ((n >> 12) << sh0) | ((s & and1) >> sh2);
+    frm[(size_t)y * frm_w + x] += 1;
+  }
+  // Adds the electrons of one EER frame to frm (8-bit counts).
+  void decode(const uint8_t* d, size_t n, uint8_t* frm) const {
+    const uint32_t cam = (uint32_t)cam_w * cam_h;
+    uint32_t pix = 0;
+    if (bits == 7) {  // mDo7BitsCounted / mDo7BitsSuperRes (:55-117)
+      uint64_t pos = 0;
+      const uint64_t end = (uint64_t)n * 8;
+      auto get = [&](int nb) {
+        unsigned v = 0;
+        for (int k = 0; k < nb; ++k, ++pos)
+          if (pos < end) v |= ((d[pos >> 3] >> (pos & 7)) & 1u) << k;
+        return v;
+      };
+      while (pos < end) {
+        const unsigned run = get(7);
+        pix += run;
+        if (pix >= cam) break;
+        if (run == 127) continue;
+        const unsigned sub = get(4) ^ 0x0Au;
+        if (sampling == 1) {
+          frm[(size_t)(pix / frm_w) * frm_w + pix % frm_w] += 1;
+        } else {
+          electron(pix, sub, frm);
+        }
+        pix += 1;
+      }
+      return;
+    }
+    // 8 bits: three bytes carry two (run, sub-pixel) codes (:119-165)
+    for (size_t p = 0; p + 2 < n; p += 3) {
+      const unsigned p1 = d[p];
+      unsigned s1 = d[p + 1] & 0x0Au;
+      pix += p1;
+      if (pix >= cam) break;
+      if (p1 < 255) {
+        if (sampling == 1) frm[(size_t)(pix / frm_w) * frm_w + pix % frm_w] += 1;
+        else electron(pix, s1, frm);
+        pix += 1;
+      }
+      unsigned p2, s2;
+      if (sampling == 1) {
+        p2 = ((d[p + 1] >> 4) | (d[p + 2] << 4)) & 0xFFu;
+        s2 = 0;
+      } else {
+        // the reference's super-resolution branch reads its third byte
+        // from offset 0 of the frame (uiPos2 is never advanced, :150-156)
+        p2 = ((d[p + 1] >> 4) | d[0]) & 0xFFu;
+        s2 = ((unsigned)(d[0] >> 4)) ^ 0x0Au;
+      }
+      pix += p2;
+      if (pix >= cam) break;
+      if (p2 < 255) {
+        if (sampling == 1) frm[(size_t)(pix / frm_w) * frm_w + pix % frm_w] += 1;
+        else electron(pix, s2, frm);
+        pix += 1;
+      }
+    }
+  }
+};
+
+int eer_bits(const Page& p) {
+  if (p.compression == 65001) return 7;
+  if (p.compression == 65000) return 8;
+  return -1;  // 65002 is not decoded by the reference either (CLoadEerHeader.cpp:34-39)
+}
+
 }  // namespace
 
 extern "C" {
+
+int mc3_eer_info(const char* path, int* cam_x, int* cam_y, int* n_frames, int* bits) {
+  if (!path) return MC3_EINVAL;
+  File tf;
+  if (!parse(path, tf)) return MC3_EIO;
+  const Page& p0 = tf.pages[0];
+  const int b = eer_bits(p0);
+  if (b < 0 || p0.nx == 0 || p0.ny == 0) return MC3_EUNSUPPORTED;
+  if (cam_x) *cam_x = (int)p0.nx;
+  if (cam_y) *cam_y = (int)p0.ny;
+  if (n_frames) *n_frames = (int)tf.pages.size();
+  if (bits) *bits = b;
+  return MC3_OK;
+}
+
+int mc3_eer_render(const char* path, int sampling, int n_out, const int* start, const int* size,
+                   unsigned char* dst, int threads) {
+  if (!path || !dst || n_out < 1 || !start || !size) return MC3_EINVAL;
+  if (sampling < 1 || sampling > 3) return MC3_EINVAL;
+  File tf;
+  if (!parse(path, tf)) return MC3_EIO;
+  const Page& p0 = tf.pages[0];
+  EerDecoder dec;
+  const int b = eer_bits(p0);
+  if (b < 0 || !dec.setup((int)p0.nx, (int)p0.ny, b, sampling)) return MC3_EUNSUPPORTED;
+  const int fact = sampling == 2 ? 2 : (sampling == 3 ? 4 : 1);
+  const size_t frame = (size_t)p0.nx * fact * p0.ny * fact;
+  for (int i = 0; i < n_out; ++i)
+    if (start[i] < 0 || size[i] < 1 || start[i] + size[i] > (int)tf.pages.size()) return MC3_EINVAL;
+  // CRenderMrcStack::mRender / mRenderInt (EerUtil/CRenderMrcStack.cpp:30-95):
+  // rendered frame i = the electrons of EER frames start[i] .. start[i]+size[i]-1
+  int nt = threads > 0 ? threads : (int)std::thread::hardware_concurrency();
+  nt = std::max(1, std::min(nt, n_out));
+  std::atomic<int> next{0};
+  std::atomic<int> status{MC3_OK};
+  auto work = [&]() {
+    FILE* f = std::fopen(path, "rb");
+    if (!f) {
+      status = MC3_EIO;
+      return;
+    }
+    std::vector<uint8_t> buf;
+    for (;;) {
+      const int i = next.fetch_add(1);
+      if (i >= n_out || status != MC3_OK) break;
+      uint8_t* frm = dst + frame * i;
+      std::memset(frm, 0, frame);
+      for (int k = 0; k < size[i] && status == MC3_OK; ++k) {
+        const Page& pg = tf.pages[start[i] + k];
+        if (pg.nx != p0.nx || pg.ny != p0.ny || eer_bits(pg) != b) {
+          status = MC3_EUNSUPPORTED;
+          break;
+        }
+        size_t tot = 0;
+        for (size_t s = 0; s < pg.offsets.size() && s < pg.counts.size(); ++s) tot += pg.counts[s];
+        buf.assign(tot + 8, 0);  // zero tail: bit reads past the data see zeros
+        size_t o = 0;
+        for (size_t s = 0; s < pg.offsets.size() && s < pg.counts.size(); ++s) {
+          if (fseeko(f, (off_t)pg.offsets[s], SEEK_SET) != 0 ||
+              std::fread(buf.data() + o, 1, pg.counts[s], f) != pg.counts[s]) {
+            status = MC3_EIO;
+            break;
+          }
+          o += pg.counts[s];
+        }
+        if (status == MC3_OK) dec.decode(buf.data(), tot, frm);
+      }
+    }
+    std::fclose(f);
+  };
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nt; ++t) pool.emplace_back(work);
+  for (auto& t : pool) t.join();
+  return status;
+}
 
 int mc3_tiff_info(const char* path, int* nx, int* ny, int* nz, int* mode) {
   if (!path) return MC3_EINVAL;

@@ -348,3 +348,45 @@ def test_cli_tiff_movie_matches_mrc_movie(tmp_path, mc3lib):
     for suf in ref["sums"]:
         t = mrcio.read(str(tdir / f"sum{suf}.mrc"))[0].astype(np.float64)
         assert np.array_equal(t, ref["sums"][suf]), suf
+
+
+def test_cli_eer_movie_matches_rendered_mrc_movie(tmp_path, mc3lib):
+    """-InEer with -FmIntFile: 30 EER frames (7-bit run lengths) rendered by
+    five (CRenderMrcStack::mRenderInt) and dose-weighted with the file's
+    dose give the same logs and sums as the 8-bit MRC movie of the rendered
+    frames with the equivalent -FmDose.  The reference program is built
+    without libtiff, so this compares the command line across readers."""
+    import importlib.util
+    from motioncor3_b200 import build, mrcio, synthetic as S
+    build.build()
+    spec = importlib.util.spec_from_file_location("eer_t", os.path.join(ROOT, "tests", "test_eer.py"))
+    eer = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(eer)
+    m = S.make_movie(384, 320, 30, dose=0.3, seed=53, gain=False)
+    ev = np.minimum(np.asarray(m.frames), 1).astype(np.uint8)  # at most one electron per pixel
+    cam = 384 * 320
+    rng = np.random.default_rng(53)
+    raws = []
+    for f in range(30):
+        pix = np.flatnonzero(ev[f].ravel())
+        raws.append(eer._encode7(pix, rng.integers(0, 16, pix.size), cam))
+    d = tmp_path / "eer"
+    d.mkdir()
+    path = str(d / "movie.eer")
+    eer._write_eer(path, 384, 320, raws, 65001)
+    fm = d / "fmint.txt"
+    fm.write_text("30 5 0.25\n")
+    tags = "-Iter 6 -Tol 0.2 -Bft 300 -PixSize 0.9 -Group 1 1".split()
+    args = [OUR_BIN, "-InEer", path, "-OutMrc", str(d / "sum.mrc"), "-LogDir", str(d) + "/",
+            "-FmIntFile", str(fm), "-Gpu", "0"] + tags
+    p = subprocess.run(args, capture_output=True, text=True, env=_env(), timeout=900)
+    assert p.returncode == 0, (p.stdout + p.stderr)[-3000:]
+    rendered = ev.reshape(6, 5, 320, 384).sum(axis=1).astype(np.uint8)
+    ref = run_program(OUR_BIN, str(tmp_path / "mrc"), rendered, None, tags + ["-FmDose", "1.25"])
+    a = _read_log(str(d / "movie-Full.log"))
+    b = _read_log(ref["logs"]["-Full.log"])
+    assert a.shape == (6, 3) and np.array_equal(a, b)
+    assert sorted(ref["sums"]) == ["", "_DW", "_DWS"]
+    for suf in ref["sums"]:
+        t = mrcio.read(str(d / f"sum{suf}.mrc"))[0].astype(np.float64)
+        assert np.array_equal(t, ref["sums"][suf]), suf
