@@ -825,6 +825,12 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
       fwd.dir = -1;
       fwd.scale = (float)(1.0 / W / H);
       MC3_TRY(col_fft(spec, spec, g.cmpX, g.cmpX, H, bi, fwd, st));
+      // CCorrectFullShift::mGenSums calls its own (non-virtual) mMotionDecon
+      // on the locally corrected frames too (Correct/CCorrectInc.h:115,
+      // Correct/CCorrectFullShift.cpp:271-274), so in patch mode the weight is
+      // applied a second time
+      if (prm.in_fm_motion)
+        MC3_TRY(motion_decon(spec, (long)ncmp, g.cmpX, g.cmpY, N, d_motion.as<float4>(), st));
     }
     MC3_TRY(frame_sums(spec, (long)ncmp, N, g.cmpX, g.cmpY, nullptr, nullptr, d_acc.as<float>(),
                        d_Wn.as<float>(), dp, d_sums.as<float2>(), g.nSums, st));

@@ -1341,9 +1341,9 @@ int oracle_process_movie(const oracle_params* p, const float* frames, int W, int
     float s[2] = {-fs.x(f), -fs.y(f)};
     double d = (double)std::sqrt((float)(s[0] * s[0] + s[1] * s[1]));
     if (!(d < 0.1)) phase_shift(X, X, g.cmpX, g.cmpY, s[0], s[1], false);
-    if (p->in_fm_motion) {
-      // CInFrameMotion::GetFullMotion + GMotionWeight::DirWeight
-      // (MotionDecon/CInFrameMotion.cpp:78-97, MotionDecon/GMotionWeight.cu:14-36)
+    // CInFrameMotion::GetFullMotion + GMotionWeight::DirWeight
+    // (MotionDecon/CInFrameMotion.cpp:78-97, MotionDecon/GMotionWeight.cu:14-36)
+    auto motion_weight = [&](cd* X) {
       const int f1 = f == N - 1 ? f - 1 : f, f2 = f == N - 1 ? f : f + 1;
       const float mx = fs.x(f2) - fs.x(f1), my = fs.y(f2) - fs.y(f1);
       const double mot = std::sqrt((float)(mx * mx + my * my));
@@ -1367,12 +1367,16 @@ int oracle_process_movie(const oracle_params* p, const float* frames, int W, int
             X[(long)y * g.cmpX + x] *= w;
           }
       }
-    }
+    };
+    if (p->in_fm_motion) motion_weight(X);
     if (patchMode) {
       irfft2(X, realf.data(), W, H);
       local_gather(realf.data(), gath.data(), W, H, patCent.data(), &patShift[(long)f * P * 2],
                    &patBad[(long)f * P], P);
       rfft2(gath.data(), X, W, H, true);
+      // the reference's non-virtual CCorrectFullShift::mMotionDecon runs again
+      // in mGenSums on the locally corrected frame (Correct/CCorrectInc.h:115)
+      if (p->in_fm_motion) motion_weight(X);
     }
     cd* s0 = &sums[0];
     for (long i = 0; i < ncmp; ++i) s0[i] += X[i];
