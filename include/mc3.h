@@ -320,13 +320,16 @@ int mc3_ref_augment(const float* in, int nx, int ny, int fact, float* out);
  * file cannot be opened; *n_entries = 0 when it holds mixed doses. */
 int mc3_read_fmint_file(const char* path, float fm_dose, int max_entries, int* group_size,
                         int* int_size, float* dose, int* n_entries);
-/* CFmIntParam::Setup (DataUtil/CFmIntParam.cpp:29-136): rendered-frame
+/* CFmIntParam::Setup (DataUtil/CFmIntParam.cpp:29-256): rendered-frame
  * tables for n_raw raw frames from n_entries file rows (n_entries = 0: no
- * file); fills up to max_int entries of start/size/acc_dose and returns
- * their count in *n_int, *dose_weight = the file has a dose. */
+ * file), with -Throw / -Trunc frames dropped (raw frames without a file,
+ * rendered frames with one, unless 5 or fewer would be left); fills up to
+ * max_int entries of start/size/acc_dose and returns their count in *n_int,
+ * *dose_weight = the file has a dose. */
 int mc3_frame_integration_tables(const int* group_size, const int* int_size, const float* dose,
-                                 int n_entries, int n_raw, float fm_dose, int max_int, int* n_int,
-                                 int* start, int* size, float* acc_dose, int* dose_weight);
+                                 int n_entries, int n_raw, float fm_dose, int throw_first,
+                                 int throw_last, int max_int, int* n_int, int* start, int* size,
+                                 float* acc_dose, int* dose_weight);
 /* Align::CPeak2D::DoIt (Align/CPeak2D.cpp:39-109). */
 void mc3_peak2d(const float* window, int sea_x, int sea_y, float* shift);
 /* Util::CRemoveSpikes1D::DoIt(x, y, false) (Util/CRemoveSpikes1D.cpp:59-105). */

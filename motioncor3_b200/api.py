@@ -150,7 +150,8 @@ _SIGS = {
     "mc3_set_alignment": ([_VP, ctypes.POINTER(_Alignment)], _I),
     "mc3_set_frame_integration": ([_VP, ctypes.POINTER(_FrameIntegration)], _I),
     "mc3_read_fmint_file": ([ctypes.c_char_p, _F, _I, _VP, _VP, _VP, _VP], _I),
-    "mc3_frame_integration_tables": ([_VP, _VP, _VP, _I, _I, _F, _I, _VP, _VP, _VP, _VP, _VP], _I),
+    "mc3_frame_integration_tables": ([_VP, _VP, _VP, _I, _I, _F, _I, _I, _I, _VP, _VP, _VP, _VP,
+                                      _VP], _I),
     "mc3_fft_forward": ([_VP, _I, _I, _I, _I, _VP], _I),
     "mc3_fft_inverse": ([_VP, _I, _I, _I, _VP], _I),
     "mc3_phase_shift": ([_VP, _VP, _I, _I, _F, _F, _I, _VP], _I),
@@ -612,7 +613,7 @@ def read_fmint_file(path: str, fm_dose: float = 0.0, max_entries: int = 4096):
     return g[:k], n[:k], d[:k]
 
 
-def frame_integration_tables(entries, n_raw: int, fm_dose: float = 0.0) -> dict:
+def frame_integration_tables(entries, n_raw: int, fm_dose: float = 0.0, throw=(0, 0)) -> dict:
     """CFmIntParam::Setup: rendered-frame tables for n_raw raw frames from
     (group_size, int_size, dose) entries (None or empty: no file)."""
     if entries is None or len(entries[0]) == 0:
@@ -628,7 +629,8 @@ def frame_integration_tables(entries, n_raw: int, fm_dose: float = 0.0) -> dict:
     acc = np.zeros(n_raw, np.float32)
     nint = ctypes.c_int(0)
     dwt = ctypes.c_int(0)
-    _check(_lib().mc3_frame_integration_tables(_hp(g), _hp(n), _hp(d), ne, n_raw, fm_dose, n_raw,
+    _check(_lib().mc3_frame_integration_tables(_hp(g), _hp(n), _hp(d), ne, n_raw, fm_dose,
+                                               int(throw[0]), int(throw[1]), n_raw,
                                                ctypes.byref(nint), _hp(start), _hp(size), _hp(acc),
                                                ctypes.byref(dwt)), "mc3_frame_integration_tables")
     k = nint.value

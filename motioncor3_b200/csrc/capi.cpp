@@ -177,9 +177,10 @@ int mc3_read_fmint_file(const char* path, float fm_dose, int max_entries, int* g
 }
 
 int mc3_frame_integration_tables(const int* group_size, const int* int_size, const float* dose,
-                                 int n_entries, int n_raw, float fm_dose, int max_int, int* n_int,
-                                 int* start, int* size, float* acc_dose, int* dose_weight) {
-  if (n_raw < 1 || n_entries < 0 || !n_int) return MC3_EINVAL;
+                                 int n_entries, int n_raw, float fm_dose, int throw_first,
+                                 int throw_last, int max_int, int* n_int, int* start, int* size,
+                                 float* acc_dose, int* dose_weight) {
+  if (n_raw < 1 || n_entries < 0 || !n_int || throw_first < 0 || throw_last < 0) return MC3_EINVAL;
   if (n_entries > 0 && (!group_size || !int_size || !dose)) return MC3_EINVAL;
   for (int i = 0; i < n_entries; ++i)
     if (int_size[i] < 1 || group_size[i] < 0) return MC3_EINVAL;
@@ -188,11 +189,18 @@ int mc3_frame_integration_tables(const int* group_size, const int* int_size, con
   if (n_entries > 0 && std::fabs(dose[0] - dose[n_entries - 1]) < 0.0001f)
     for (int i = 0; i < n_entries; ++i) integrate = integrate || int_size[i] > 1;
   host::FmInt t;
-  if (integrate)
+  if (integrate) {
     t.integrate(std::vector<int>(group_size, group_size + n_entries),
                 std::vector<int>(int_size, int_size + n_entries), dose[0], n_raw);
-  else
-    t.plain(n_raw, fm_dose);
+    t.drop(throw_first, throw_last);  // mThrowIntFrames (:231-256)
+  } else {
+    // CFmIntParam::mSetup (:118-136): the kept raw frames, doses counted from 1
+    const int keep = n_raw - throw_first - throw_last;
+    if (keep < 1) return MC3_EINVAL;
+    t.plain(keep, fm_dose);
+    for (int& st : t.start) st += throw_first;
+    t.centers();
+  }
   *n_int = t.count();
   for (int i = 0; i < t.count() && i < max_int; ++i) {
     if (start) start[i] = t.start[i];

@@ -293,7 +293,7 @@ int main(int argc, char** argv) {
                 "[-Patch x y] [-Iter n] [-Tol px] [-Bft g p] [-FmDose d] [-PixSize a] "
                 "[-kV kv] [-Group g p] [-FmRef f] [-SumRange lo hi] [-PhaseOnly 0|1] [-SplitSum 0|1] "
                 "[-FtBin b] [-OutAln dir] [-InAln dir] [-OutStack 0|1 zbin] [-FmIntFile file] "
-                "[-Dark dark.mrc] [-RotGain r] [-FlipGain f] [-InvGain 0|1] [-Mag major minor angle] [-InFmMotion 0|1] "
+                "[-Dark dark.mrc] [-RotGain r] [-FlipGain f] [-InvGain 0|1] [-Mag major minor angle] [-InFmMotion 0|1] [-Throw n] [-Trunc n] "
                 "[-LogDir dir] [-Gpu id]\n");
     return eSuccess;
   }
@@ -353,7 +353,7 @@ int main(int argc, char** argv) {
   if (A.ints("-Gpu", gpu, 8) > 0) p.gpu = gpu[0];
   const char* ignored[] = { "-InSuffix", "-InSkips", "-ArcDir",
                            "-DefectFile", "-DefectMap", "-FullSum", "-TmpFile",
-                           "-StackZ", "-Cs", "-AmpCont", "-ExtPhase", "-Throw", "-Trunc", "-Serial",
+                           "-StackZ", "-Cs", "-AmpCont", "-ExtPhase", "-Serial",
                            "-Tilt", "-Crop",
                            "-GpuMemUsage", "-UseGpus",
                            "-OutStar", "-TiffOrder", "-CorrInterp"};
@@ -395,6 +395,17 @@ int main(int argc, char** argv) {
     }
     std::printf("MRC file size mode: %d  %d  %d  %d\n", h.nx, h.ny, h.nz, h.mode);
   }
+  // -Throw / -Trunc (CInput.cpp:567-573): frames dropped at the start / end
+  int thr[2] = {0, 0};
+  A.ints("-Throw", &thr[0], 1);
+  A.ints("-Trunc", &thr[1], 1);
+  thr[0] = thr[0] < 0 ? 0 : thr[0];
+  thr[1] = thr[1] < 0 ? 0 : thr[1];
+  if (h.nz - thr[0] - thr[1] < 3) {
+    std::fprintf(stderr, "Error: -Throw %d -Trunc %d leave fewer than 3 of %d frames\n", thr[0],
+                 thr[1], h.nz);
+    return eFailLoad;
+  }
   // -FmIntFile (CReadFmIntFile::DoIt, CFmIntParam::Setup): rendered-frame
   // tables for this movie's raw frames
   std::vector<int> fi_start, fi_size;
@@ -413,9 +424,10 @@ int main(int argc, char** argv) {
       fi_size.resize(h.nz);
       fi_acc.resize(h.nz);
       int nint = 0;
-      if (mc3_frame_integration_tables(eg.data(), en.data(), ed.data(), ne, h.nz, p.fm_dose, h.nz,
-                                       &nint, fi_start.data(), fi_size.data(), fi_acc.data(),
-                                       &fi_dose) == MC3_OK && nint > 0) {
+      if (mc3_frame_integration_tables(eg.data(), en.data(), ed.data(), ne, h.nz, p.fm_dose,
+                                       thr[0], thr[1], h.nz, &nint, fi_start.data(),
+                                       fi_size.data(), fi_acc.data(), &fi_dose) == MC3_OK &&
+          nint > 0) {
         fi_start.resize(nint);
         fi_size.resize(nint);
         fi_acc.resize(nint);
@@ -425,17 +437,22 @@ int main(int argc, char** argv) {
       }
     }
   }
-  if (!in_eer.empty() && !fi_on) {  // every EER frame rendered on its own
-    fi_start.resize(h.nz);
-    fi_size.assign(h.nz, 1);
-    fi_acc.resize(h.nz);
-    for (int i = 0; i < h.nz; ++i) {
-      fi_start[i] = i;
+  if (!in_eer.empty() && !fi_on) {  // every kept EER frame rendered on its own
+    const int keep = h.nz - thr[0] - thr[1];
+    fi_start.resize(keep);
+    fi_size.assign(keep, 1);
+    fi_acc.resize(keep);
+    for (int i = 0; i < keep; ++i) {
+      fi_start[i] = i + thr[0];
       fi_acc[i] = p.fm_dose * (i + 1);  // CFmIntParam::mSetup
     }
     fi_dose = 0;
     fi_on = true;
   }
+  // without rendered-frame tables the throws only select the raw frames read
+  const mc3::mrc::Header h_file = h;  // the file's own frame count, for reading
+  const int z_first = fi_on ? 0 : thr[0];
+  if (!fi_on) h.nz -= thr[0] + thr[1];
   const int n_raw = h.nz;
   const int n_render = fi_on ? (int)fi_start.size() : h.nz;
   // -InAln (CMain::mOpenInAlnFile, CMain.cpp:382-398): the file's patch
@@ -472,11 +489,11 @@ int main(int argc, char** argv) {
       return eFailLoad;
     }
   } else if (!in_tiff.empty()) {
-    if (mc3_tiff_read(in_tiff.c_str(), 0, h.nz, frames.p, 0) != MC3_OK) {
+    if (mc3_tiff_read(in_tiff.c_str(), z_first, h.nz, frames.p, 0) != MC3_OK) {
       std::fprintf(stderr, "error: load tiff images of %s\n", in_tiff.c_str());
       return eFailLoad;
     }
-  } else if (!mc3::mrc::read_frames(in_mrc, h, 0, h.nz, frames.as<unsigned char>())) {
+  } else if (!mc3::mrc::read_frames(in_mrc, h_file, z_first, h.nz, frames.as<unsigned char>())) {
     return eFailLoad;
   }
 
@@ -709,7 +726,7 @@ int main(int argc, char** argv) {
       std::fprintf(f, "setting\n");
       std::fprintf(f, "   stackSize: %d %d %d %d\n", h.nx, h.ny, N, 1);
       std::fprintf(f, "   patches: %d %d %d\n", p.patch[0], p.patch[1], p.patch[2]);
-      std::fprintf(f, "   throw: %d %d\n", 0, 0);
+      std::fprintf(f, "   throw: %d %d\n", thr[0], thr[1]);
       std::fprintf(f, "#    Global Shift\n");
       std::fprintf(f, "#---------------------\n");
       std::fprintf(f, "globalShift\n");

@@ -85,6 +85,22 @@ void FmInt::integrate(const std::vector<int>& gsz_in, const std::vector<int>& is
   centers();
 }
 
+bool FmInt::drop(int t0, int t1) {
+  if (t0 + t1 <= 0) return true;
+  const int keep = count() - t0 - t1;
+  if (keep <= 5) return false;
+  start.erase(start.begin(), start.begin() + t0);
+  size.erase(size.begin(), size.begin() + t0);
+  dose.erase(dose.begin(), dose.begin() + t0);
+  acc.erase(acc.begin(), acc.begin() + t0);
+  start.resize(keep);
+  size.resize(keep);
+  dose.resize(keep);
+  acc.resize(keep);
+  centers();
+  return true;
+}
+
 void FmInt::centers() {
   center.resize(start.size());
   for (size_t i = 0; i < start.size(); ++i) center[i] = start[i] + 0.5f * (size[i] - 1.0f);

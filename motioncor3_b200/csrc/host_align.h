@@ -23,6 +23,11 @@ struct FmInt {
   void integrate(const std::vector<int>& group_size, const std::vector<int>& int_size,
                  float raw_dose, int n_raw);
   void centers();  // CFmIntParam::mCalcIntFmCenters (:276-283)
+  // -Throw / -Trunc on rendered frames (CFmIntParam::mThrowIntFrames,
+  // :231-256): the first t0 and last t1 are dropped, the others keep their
+  // raw-frame starts and accumulated doses; ignored (false) when 5 or fewer
+  // frames would be left.
+  bool drop(int t0, int t1);
 };
 
 // CReadFmIntFile::DoIt (DataUtil/CReadFmIntFile.cpp:104-170): the entries

@@ -135,6 +135,10 @@ def test_frame_integration_tables(mc3lib, entries, n_raw):
     e = ([x[0] for x in entries], [x[1] for x in entries], [x[2] for x in entries])
     t = api.frame_integration_tables(e, n_raw)
     start, size, acc = _tables(entries, n_raw)
+    if len(size) - 3 > 5:  # -Throw 2 -Trunc 1 drop rendered frames, doses kept
+        tt = api.frame_integration_tables(e, n_raw, throw=(2, 1))
+        assert tt["start"].tolist() == start[2:-1] and tt["size"].tolist() == size[2:-1]
+        assert np.allclose(tt["acc_dose"], acc[2:-1], rtol=1e-6)
     assert t["size"].tolist() == size and t["start"].tolist() == start
     assert sum(size) == n_raw
     assert np.allclose(t["acc_dose"], acc, rtol=1e-6)
@@ -189,3 +193,16 @@ def test_ref_augment(mc3lib):
     from motioncor3_b200 import api
     a = np.arange(12, dtype=np.float32).reshape(3, 4)
     assert np.array_equal(api.ref_augment(a, 2), np.repeat(np.repeat(a, 2, 0), 2, 1))
+
+
+def test_frame_tables_with_throws(mc3lib):
+    """CFmIntParam::mSetup with -Throw 2 -Trunc 3: the kept raw frames,
+    doses counted again from the first kept frame; with a file, throwing
+    that would leave 5 or fewer rendered frames is ignored
+    (CFmIntParam::mThrowIntFrames)."""
+    from motioncor3_b200 import api
+    t = api.frame_integration_tables(None, 20, fm_dose=0.5, throw=(2, 3))
+    assert t["start"].tolist() == list(range(2, 17)) and t["size"].tolist() == [1] * 15
+    assert np.allclose(t["acc_dose"], 0.5 * np.arange(1, 16, dtype=np.float32))
+    t = api.frame_integration_tables(([24], [4], [0.5]), 24, throw=(1, 1))
+    assert t["size"].tolist() == [4] * 6  # 6 - 2 = 4 <= 5: throws ignored
