@@ -814,7 +814,8 @@ struct Features {
 
 // CDetectFeatures::DoIt (Align/CDetectFeatures.cpp:58-181) on the aligned
 // xcf sum; the local-variance normalisation reads unmodified input values
-// (GNormByStd2D.cu updates in place while neighbours read).
+// (Align/GNormByStd2D.cu updates in place while neighbouring threads still
+// read, a race whose outcome depends on scheduling).
 Features detect_features(const cd* xsum, int xcfCmpX, int xcfCmpY, int Px, int Py) {
   Features F;
   F.P[0] = Px; F.P[1] = Py;
