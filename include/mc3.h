@@ -65,6 +65,9 @@ typedef struct {
   int in_fm_motion;    /* -InFmMotion (0): weight each aligned frame by the
                           directional sinc of its in-frame motion
                           (MotionDecon/GMotionWeight.cu, CInFrameMotion)      */
+  int corr_interp;     /* -CorrInterp (0): in patch mode divide each globally
+                          corrected frame spectrum by sinc(pi r)^(1/8)
+                          (Util/GCorrLinearInterp.cu)                         */
 } mc3_params;
 
 /* Sizes a movie will use (CBufferPool::CreateBuffers, CBufferPool.cpp:95-270). */

@@ -54,6 +54,7 @@ class _Params(ctypes.Structure):
         ("out_stack", ctypes.c_int * 2),
         ("mag", ctypes.c_float * 3),
         ("in_fm_motion", ctypes.c_int),
+        ("corr_interp", ctypes.c_int),
     ]
 
 
@@ -235,6 +236,7 @@ class Params:
     out_stack: tuple = (0, 1)
     mag: tuple = (1.0, 1.0, 0.0)
     in_fm_motion: int = 0
+    corr_interp: int = 0
 
     def to_c(self) -> _Params:
         p = _Params()
@@ -262,6 +264,7 @@ class Params:
         for i in range(3):
             p.mag[i] = float(self.mag[i])
         p.in_fm_motion = int(self.in_fm_motion)
+        p.corr_interp = int(self.corr_interp)
         return p
 
 

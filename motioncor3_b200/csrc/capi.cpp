@@ -69,6 +69,7 @@ void mc3_params_default(mc3_params* p) {
   p->mag[1] = 1.0f;
   p->mag[2] = 0.0f;
   p->in_fm_motion = 0;
+  p->corr_interp = 0;
 }
 
 int mc3_create(const mc3_params* p, mc3_ctx** out) {

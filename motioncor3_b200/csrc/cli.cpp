@@ -293,7 +293,7 @@ int main(int argc, char** argv) {
                 "[-Patch x y] [-Iter n] [-Tol px] [-Bft g p] [-FmDose d] [-PixSize a] "
                 "[-kV kv] [-Group g p] [-FmRef f] [-SumRange lo hi] [-PhaseOnly 0|1] [-SplitSum 0|1] "
                 "[-FtBin b] [-OutAln dir] [-InAln dir] [-OutStack 0|1 zbin] [-FmIntFile file] "
-                "[-Dark dark.mrc] [-RotGain r] [-FlipGain f] [-InvGain 0|1] [-Mag major minor angle] [-InFmMotion 0|1] [-Throw n] [-Trunc n] "
+                "[-Dark dark.mrc] [-RotGain r] [-FlipGain f] [-InvGain 0|1] [-Mag major minor angle] [-InFmMotion 0|1] [-Throw n] [-Trunc n] [-CorrInterp 0|1] "
                 "[-LogDir dir] [-Gpu id]\n");
     return eSuccess;
   }
@@ -340,6 +340,7 @@ int main(int argc, char** argv) {
   A.ints("-SplitSum", &p.split_sum, 1);  // CInput.cpp:657-663
   A.ints("-OutStack", p.out_stack, 2);    // CInput.cpp:590-592
   A.ints("-InFmMotion", &p.in_fm_motion, 1);
+  A.ints("-CorrInterp", &p.corr_interp, 1);  // CInput.cpp:673-675
   {
     float mg[3];
     int f0, nmag;
@@ -356,7 +357,7 @@ int main(int argc, char** argv) {
                            "-StackZ", "-Cs", "-AmpCont", "-ExtPhase", "-Serial",
                            "-Tilt", "-Crop",
                            "-GpuMemUsage", "-UseGpus",
-                           "-OutStar", "-TiffOrder", "-CorrInterp"};
+                           "-OutStar", "-TiffOrder"};
   for (const char* t : ignored) {
     int f, n;
     A.find(t, &f, &n);

@@ -552,6 +552,35 @@ int motion_decon(float2* spec, long fr_stride, int cmpX, int cmpY, int N, const 
   return kOk;
 }
 
+// GCorrLinearInterp mGCorrectCmp (Util/GCorrLinearInterp.cu:7-22): every
+// frequency but DC of N frame spectra divided by sinc(pi r)^(1/8),
+// r = |(x / (2 (cmpX - 1)), y / cmpY)| with y signed.
+__global__ void k_corr_interp(float2* spec, long fr_stride, int cmpX, int cmpY) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= cmpX || (x == 0 && y == 0)) return;
+  float fx = x * 0.5f / (cmpX - 1);
+  float fy = y / (float)cmpY;
+  if (fy > 0.5f) fy -= 1.0f;
+  fx = sqrtf(fx * fx + fy * fy) * 3.141592654f;
+  fx = sinf(fx) / fx;
+  fx = powf(fx, 0.125f);
+  float2* p = spec + (long)blockIdx.z * fr_stride + (long)y * cmpX + x;
+  float2 v = *p;
+  v.x /= fx;
+  v.y /= fx;
+  *p = v;
+}
+
+int corr_interp(float2* spec, long fr_stride, int cmpX, int cmpY, int N, cudaStream_t st) {
+  if (N < 1 || N > 65535 || cmpX < 2) return kEInval;
+  dim3 grid(ceil_div(cmpX, 128), cmpY, N);
+  prof::Scope ps("k_corr_interp", (double)N * cmpX * cmpY * 16.0, st);
+  k_corr_interp<<<grid, 128, 0, st>>>(spec, fr_stride, cmpX, cmpY);
+  MC3_CHECK_LAUNCH("k_corr_interp");
+  return kOk;
+}
+
 __global__ void k_unpad_positive(const float* in, long pitch, float* out, int W, int H,
                                  long in_stride) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;

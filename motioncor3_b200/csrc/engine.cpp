@@ -768,6 +768,12 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
     }
   }
   MC3_TRY(global_sums(spec, N, fs, g));
+  if (g.patch && prm.corr_interp) {
+    // -CorrInterp: CGenRealStack::mCorrectBilinear on the frames of
+    // CPatchAlign::mCorrectFullShift (Align/CPatchAlign.cpp:52-61), before the
+    // in-frame motion weighting
+    MC3_TRY(corr_interp(spec, (long)ncmp, g.cmpX, g.cmpY, N, st));
+  }
   if (prm.in_fm_motion) {
     // -InFmMotion: CCorrectFullShift::mMotionDecon (Correct/CCorrectFullShift.cpp:309-318)
     // in global mode, CGenRealStack::mMotionDecon (Correct/CGenRealStack.cpp:156-166)

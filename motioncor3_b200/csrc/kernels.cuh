@@ -101,6 +101,8 @@ int stretch_images(const float* in, float* out, int pitch, long stride, int W, i
 // apply, 0) per frame.
 int motion_decon(float2* spec, long fr_stride, int cmpX, int cmpY, int N, const float4* motion,
                  cudaStream_t st);
+// Linear-interpolation correction (-CorrInterp) of N frame spectra.
+int corr_interp(float2* spec, long fr_stride, int cmpX, int cmpY, int N, cudaStream_t st);
 // out[y*W+x] = max(0, in[y*pitch+x])
 int unpad_positive(const float* in, long pitch, float* out, int W, int H, int n,
                    long in_stride, cudaStream_t st);

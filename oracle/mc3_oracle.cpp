@@ -1064,6 +1064,7 @@ void oracle_default_params(oracle_params* p) {
   p->mag[0] = p->mag[1] = 1.0f;
   p->mag[2] = 0.0f;
   p->in_fm_motion = 0;
+  p->corr_interp = 0;
 }
 
 void oracle_rfft2(const double* img, double* spec, int W, int H, int normalise) {
@@ -1369,6 +1370,17 @@ int oracle_process_movie(const oracle_params* p, const float* frames, int W, int
           }
       }
     };
+    if (patchMode && p->corr_interp) {
+      // CGenRealStack::mCorrectBilinear (GCorrLinearInterp, Util/GCorrLinearInterp.cu:7-22)
+      for (int y = 0; y < g.cmpY; ++y)
+        for (int x = 0; x < g.cmpX; ++x) {
+          if (x == 0 && y == 0) continue;
+          float fx = x * 0.5f / (g.cmpX - 1), fy = y / (float)g.cmpY;
+          if (fy > 0.5f) fy -= 1.0f;
+          const double r = std::sqrt((double)fx * fx + (double)fy * fy) * 3.141592654;
+          X[(long)y * g.cmpX + x] /= std::pow(std::sin(r) / r, 0.125);
+        }
+    }
     if (p->in_fm_motion) motion_weight(X);
     if (patchMode) {
       irfft2(X, realf.data(), W, H);

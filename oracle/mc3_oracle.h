@@ -49,6 +49,7 @@ typedef struct {
   const float* dark;  /* [H][W] dark reference subtracted before the gain, or NULL */
   float mag[3];       /* -Mag major minor angle (1 1 0 = none)             */
   int in_fm_motion;   /* -InFmMotion: in-frame motion weighting            */
+  int corr_interp;    /* -CorrInterp: interpolation correction (patch mode) */
 } oracle_params;
 
 typedef struct {

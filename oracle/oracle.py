@@ -76,6 +76,7 @@ class OracleParams(ctypes.Structure):
         ("dark", _VP),
         ("mag", ctypes.c_float * 3),
         ("in_fm_motion", ctypes.c_int),
+        ("corr_interp", ctypes.c_int),
     ]
 
 

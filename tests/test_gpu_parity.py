@@ -441,7 +441,7 @@ def test_pipeline_in_frame_motion(api, oracle, torch_cuda, patch):
     if patch:
         m = S.make_movie(512, 512, 12, dose=4.0, seed=33, gain=False, local=True)
         p = api.Params(patch=(3, 3), iter=5, tol=0.2, bft=(500, 150), fm_dose=1.0, pix_size=1.0,
-                       in_fm_motion=1, out_stack=(1, 1))
+                       in_fm_motion=1, out_stack=(1, 1), corr_interp=1)
     else:
         m = S.make_movie(384, 320, 10, dose=3.0, seed=50, gain=False)
         p = api.Params(iter=6, tol=0.2, bft=(300, 100), fm_dose=1.2, pix_size=0.9,
@@ -454,6 +454,7 @@ def test_pipeline_in_frame_motion(api, oracle, torch_cuda, patch):
                      patch_bad=res.patch_bad)
     kw = _oracle_kw(p)
     kw["in_fm_motion"] = 1
+    kw["corr_interp"] = p.corr_interp
     same = oracle.process_movie(np.asarray(m.frames), force=force, **kw)
     for i in range(res.n_sums):
         e = _rel_rms(res.sums[i], same["sums"][i])

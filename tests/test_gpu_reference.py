@@ -97,6 +97,9 @@ CASES = {
                             tags="-Patch 0 0 -Iter 7 -Tol 0.5 -Bft 150 -PixSize 1.0"),
     "global_throw": dict(shape=(14, 320, 384), dose=3.0, seed=54, gain=False, local=False,
                          tags="-Iter 6 -Tol 0.2 -Bft 300 -FmDose 1.2 -PixSize 0.9 -Throw 2 -Trunc 1"),
+    "patch_corrinterp": dict(shape=(12, 512, 512), dose=4.0, seed=33, gain=True, local=True,
+                             tags="-Patch 3 3 -Iter 5 -Tol 0.2 -Bft 500 150 -FmDose 1 -PixSize 1 "
+                                  "-kV 300 -CorrInterp 1"),
     "global_infmmotion": dict(shape=(10, 320, 384), dose=3.0, seed=51, gain=False, local=False,
                               tags="-Iter 6 -Tol 0.2 -Bft 300 -FmDose 1.2 -PixSize 0.9 -InFmMotion 1"),
     "patch_infmmotion": dict(shape=(12, 512, 512), dose=4.0, seed=33, gain=True, local=True,
