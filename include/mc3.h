@@ -177,6 +177,11 @@ int mc3_set_gain(mc3_ctx* ctx, const float* gain, int nx, int ny, int on_device)
  * subtracted before the gain multiplication (GApplyRefsToFrame,
  * MrcUtil/GApplyRefsToFrame.cu:56-72); NULL clears it. */
 int mc3_set_dark(mc3_ctx* ctx, const float* dark, int nx, int ny, int on_device);
+/* Camera defects known in advance (-DefectFile rectangles, -DefectMap image;
+ * BadPixel/CDetectMain.cpp:146-260): a host [ny][nx] mask whose nonzero
+ * pixels are added to the detected bad pixels before they are filled; NULL
+ * clears it. */
+int mc3_set_defects(mc3_ctx* ctx, const unsigned char* mask, int nx, int ny);
 
 /* ---- whole path ---- */
 /* One movie from raw frames to sums and shift tables: replaces

@@ -140,6 +140,7 @@ _SIGS = {
     "mc3_host_free": ([_VP], _I),
     "mc3_set_gain": ([_VP, _VP, _I, _I, _I], _I),
     "mc3_set_dark": ([_VP, _VP, _I, _I, _I], _I),
+    "mc3_set_defects": ([_VP, _VP, _I, _I], _I),
     "mc3_ref_orient": ([_VP, _I, _I, _I, _I, _I, _VP, _VP, _VP], _I),
     "mc3_ref_augment": ([_VP, _I, _I, _I, _VP], _I),
     "mc3_tiff_info": ([ctypes.c_char_p, _VP, _VP, _VP, _VP], _I),
@@ -343,6 +344,14 @@ class MotionCor3:
             return
         d = np.ascontiguousarray(dark, dtype=np.float32)
         _check(_lib().mc3_set_dark(self._h, _hp(d), d.shape[1], d.shape[0], 0), "mc3_set_dark")
+
+    def set_defects(self, mask) -> None:
+        """Known camera defects [ny][nx] (nonzero = bad; mc3_set_defects); None clears."""
+        if mask is None:
+            _check(_lib().mc3_set_defects(self._h, None, 0, 0), "mc3_set_defects")
+            return
+        m = np.ascontiguousarray(mask, dtype=np.uint8)
+        _check(_lib().mc3_set_defects(self._h, _hp(m), m.shape[1], m.shape[0]), "mc3_set_defects")
 
     @staticmethod
     def _movie(frames, nx4=None):

@@ -137,6 +137,11 @@ int mc3_set_dark(mc3_ctx* ctx, const float* dark, int nx, int ny, int on_device)
   return ctx->eng->set_dark(dark, nx, ny, on_device != 0);
 }
 
+int mc3_set_defects(mc3_ctx* ctx, const unsigned char* mask, int nx, int ny) {
+  if (!ctx) return MC3_EINVAL;
+  return ctx->eng->set_defects(mask, nx, ny);
+}
+
 int mc3_set_gain(mc3_ctx* ctx, const float* gain, int nx, int ny, int on_device) {
   if (!ctx) return MC3_EINVAL;
   return ctx->eng->set_gain(gain, nx, ny, on_device != 0);

@@ -293,7 +293,7 @@ int main(int argc, char** argv) {
                 "[-Patch x y] [-Iter n] [-Tol px] [-Bft g p] [-FmDose d] [-PixSize a] "
                 "[-kV kv] [-Group g p] [-FmRef f] [-SumRange lo hi] [-PhaseOnly 0|1] [-SplitSum 0|1] "
                 "[-FtBin b] [-OutAln dir] [-InAln dir] [-OutStack 0|1 zbin] [-FmIntFile file] "
-                "[-Dark dark.mrc] [-RotGain r] [-FlipGain f] [-InvGain 0|1] [-Mag major minor angle] [-InFmMotion 0|1] [-Throw n] [-Trunc n] [-CorrInterp 0|1] "
+                "[-Dark dark.mrc] [-RotGain r] [-FlipGain f] [-InvGain 0|1] [-Mag major minor angle] [-InFmMotion 0|1] [-Throw n] [-Trunc n] [-CorrInterp 0|1] [-DefectFile f] [-DefectMap f] "
                 "[-LogDir dir] [-Gpu id]\n");
     return eSuccess;
   }
@@ -353,7 +353,7 @@ int main(int argc, char** argv) {
   int gpu[8];
   if (A.ints("-Gpu", gpu, 8) > 0) p.gpu = gpu[0];
   const char* ignored[] = { "-InSuffix", "-InSkips", "-ArcDir",
-                           "-DefectFile", "-DefectMap", "-FullSum", "-TmpFile",
+                           "-FullSum", "-TmpFile",
                            "-StackZ", "-Cs", "-AmpCont", "-ExtPhase", "-Serial",
                            "-Tilt", "-Crop",
                            "-GpuMemUsage", "-UseGpus",
@@ -560,6 +560,51 @@ int main(int argc, char** argv) {
       mc3_set_gain(ctx, gain.data(), gx, gy, 0);
       if (have_dark) mc3_set_dark(ctx, dark.data(), dx, dy, 0);
     }
+  }
+  // ---- known camera defects: CDetectMain::mLoadDefectFile / mLoadDefectMap
+  //      (BadPixel/CDetectMain.cpp:146-260) ----
+  const std::string defect_file = A.str("-DefectFile");
+  const std::string defect_map = A.str("-DefectMap");
+  if (!defect_file.empty() || !defect_map.empty()) {
+    std::vector<unsigned char> mask((size_t)h.nx * h.ny, 0);
+    bool any = false;
+    if (FILE* f = defect_file.empty() ? nullptr : std::fopen(defect_file.c_str(), "rt")) {
+      std::printf("Load camera defects.\n");
+      char line[256];
+      while (std::fgets(line, sizeof(line), f)) {
+        int e[4];
+        if (std::sscanf(line, "%d  %d  %d  %d", e, e + 1, e + 2, e + 3) != 4) continue;
+        std::printf("...... Defect: %6d  %6d  %6d  %6d\n", e[0], e[1], e[2], e[3]);
+        if (e[0] < 0) e[0] = 0;
+        if (e[1] < 0) e[1] = 0;
+        const int ex = e[0] + e[2] > h.nx ? h.nx : e[0] + e[2];
+        const int ey = e[1] + e[3] > h.ny ? h.ny : e[1] + e[3];
+        for (int y = e[1]; y < ey; ++y)
+          for (int x = e[0]; x < ex; ++x) mask[(size_t)y * h.nx + x] = 1;
+        any = true;
+      }
+      std::fclose(f);
+      std::printf("Load camera defects: done.\n\n");
+    }
+    if (!defect_map.empty()) {
+      // an 8-bit MRC image of the frame size, else an 8-bit TIFF (read
+      // bottom-up like every TIFF image); bit 0 marks a defect
+      std::vector<unsigned char> dm((size_t)h.nx * h.ny);
+      bool ok = false;
+      mc3::mrc::Header dh;
+      if (mc3::mrc::read_header(defect_map, &dh) && (dh.mode == 0 || dh.mode == 5) &&
+          dh.nx == h.nx && dh.ny == h.ny)
+        ok = mc3::mrc::read_frames(defect_map, dh, 0, 1, dm.data());
+      int tx = 0, ty = 0, tz = 0, tm = -1;
+      if (!ok && mc3_tiff_info(defect_map.c_str(), &tx, &ty, &tz, &tm) == MC3_OK && tm == 0 &&
+          tx == h.nx && ty == h.ny)
+        ok = mc3_tiff_read(defect_map.c_str(), 0, 1, dm.data(), 1) == MC3_OK;
+      if (ok) {
+        for (size_t i = 0; i < dm.size(); ++i) mask[i] |= dm[i] & 1;
+        any = true;
+      }
+    }
+    if (any) mc3_set_defects(ctx, mask.data(), h.nx, h.ny);
   }
   mc3_plan_info info;
   if (fi_on) {

@@ -229,6 +229,22 @@ int Engine::set_dark(const float* dark, int w, int h, bool on_device) {
   return kOk;
 }
 
+int Engine::set_defects(const unsigned char* mask, int w, int h) {
+  MC3_CUDA(cudaSetDevice(device));
+  if (!mask) {
+    has_defects = false;
+    return kOk;
+  }
+  if (w <= 0 || h <= 0) return kEInval;
+  MC3_TRY(d_defects.ensure((size_t)w * h));
+  MC3_CUDA(cudaMemcpyAsync(d_defects.p, mask, (size_t)w * h, cudaMemcpyHostToDevice, stream));
+  MC3_CUDA(cudaStreamSynchronize(stream));
+  has_defects = true;
+  defects_w = w;
+  defects_h = h;
+  return kOk;
+}
+
 int Engine::plan(int w, int h, int n, mc3_plan_info* info) {
   Geometry g;
   if (fmint && n != (fmint_rendered ? fmint_tab.count() : fmint_raw)) return kEInval;
@@ -502,6 +518,7 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
   }
   if (has_gain && (gain_w != g.W || gain_h != g.H)) return kEInval;  // CProcessThread::mCheckGain
   if (has_dark && (dark_w != g.W || dark_h != g.H)) return kEInval;
+  if (has_defects && (defects_w != g.W || defects_h != g.H)) return kEInval;
   const float* dark = has_dark ? d_dark.as<float>() : nullptr;
   const bool loaded = aln_loaded;
   if (loaded && (aln_nz != g.N || aln_P != g.P)) {
@@ -568,6 +585,8 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
     host::defect_template(6, tpl);
     MC3_TRY(detect_bad_pixels(d_sum.as<float>(), W, H, d_cc.as<float>(), d_part.as<float>(),
                               d_mom.as<float>(), d_bad.as<uint8_t>(), tpl, 6, st));
+    // CDetectMain::mLoadDefectFile / mLoadDefectMap (BadPixel/CDetectMain.cpp:146-260)
+    if (has_defects) MC3_TRY(or_mask(d_bad.as<uint8_t>(), d_defects.as<uint8_t>(), npx, st));
     MC3_TRY(d_badn.ensure(sizeof(int)));
     MC3_TRY(d_badlist.ensure(sizeof(int2) * npx));
     MC3_TRY(correct_bad_pixels(frames, fr_stride_f, N, d_bad.as<uint8_t>(), W, H, d_badn.as<int>(),

@@ -49,6 +49,7 @@ class Engine {
   int set_stream(cudaStream_t s);
   int set_gain(const float* gain, int w, int h, bool on_device);
   int set_dark(const float* dark, int w, int h, bool on_device);
+  int set_defects(const unsigned char* mask, int w, int h);
   int plan(int w, int h, int n, mc3_plan_info* info);
   int process(const mc3_movie& mv, mc3_result* out);
   // Starts the host->device copy of a later movie's raw frames on the copy
@@ -101,7 +102,9 @@ class Engine {
   DevBuf d_xcf, d_sh, d_ex, d_ey, d_S, d_T, d_win, d_gsh, d_act, d_gstart, d_gsize;
   DevBuf d_pat, d_patoff, d_bsum, d_bimg, d_btmp, d_bmap, d_scal;
   DevBuf d_fex, d_fey, d_Wn, d_acc, d_sums, d_real, d_gath, d_pcent, d_pshift, d_pbad, d_pmask, d_out, d_bsums;
-  DevBuf d_stk, d_zgrp, d_mag, d_motion;
+  DevBuf d_stk, d_zgrp, d_mag, d_motion, d_defects;
+  bool has_defects = false;
+  int defects_w = 0, defects_h = 0;
   // loaded alignment (mc3_set_alignment)
   bool aln_loaded = false;
   int aln_nz = 0, aln_P = 0;

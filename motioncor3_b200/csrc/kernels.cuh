@@ -16,6 +16,8 @@ int gain_and_sum(const void* raw, int mode, long raw_stride, const float* dark,
 int gain_and_sum_int(const void* raw, int mode, long raw_stride, const int* start,
                      const int* size, const float* dark, const float* gain, float* frames,
                      long fr_stride, float* sum, int W, int H, int N, cudaStream_t st);
+// bad[i] = 1 where defects[i] != 0 (device, n pixels).
+int or_mask(uint8_t* bad, const uint8_t* defects, size_t n, cudaStream_t st);
 int moment_grid(int W, int H);
 int image_moment(const float* img, int W, int H, long pitch, int iExp, float* d_part,
                  float* d_out, cudaStream_t st);

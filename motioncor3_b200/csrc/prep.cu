@@ -132,6 +132,19 @@ int gain_and_sum_int(const void* raw, int mode, long raw_stride, const int* star
   return kOk;
 }
 
+// Known camera defects added to the detected map: bad |= (defects != 0).
+__global__ void k_or_mask(uint8_t* bad, const uint8_t* __restrict__ defects, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && defects[i]) bad[i] = 1;
+}
+
+int or_mask(uint8_t* bad, const uint8_t* defects, size_t n, cudaStream_t st) {
+  if (n == 0) return kOk;
+  k_or_mask<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(bad, defects, n);
+  MC3_CHECK_LAUNCH("k_or_mask");
+  return kOk;
+}
+
 // ---- moments with the reference's reduction order ------------------------
 // GCalcMoment2D::DoIt (Util/GCalcMoment2D.cu:10-60, 96-114): grid-stride
 // per-thread FP32 sums, shared-memory tree, per-block division by W*H, then

@@ -1065,6 +1065,7 @@ void oracle_default_params(oracle_params* p) {
   p->mag[2] = 0.0f;
   p->in_fm_motion = 0;
   p->corr_interp = 0;
+  p->defects = nullptr;
 }
 
 void oracle_rfft2(const double* img, double* spec, int W, int H, int normalise) {
@@ -1160,6 +1161,10 @@ int oracle_process_movie(const oracle_params* p, const float* frames, int W, int
     for (int f = 0; f < N; ++f)
       for (long i = 0; i < npx; ++i) sum[i] += fr[(long)f * npx + i];
     detect_bad(sum.data(), W, H, bad.data());
+    // CDetectMain::mLoadDefectFile / mLoadDefectMap (BadPixel/CDetectMain.cpp:146-260)
+    if (p->defects)
+      for (long i = 0; i < npx; ++i)
+        if (p->defects[i]) bad[i] = 1;
     parallel_for(N, [&](long f0, long f1) {
       for (long f = f0; f < f1; ++f) correct_bad(&fr[f * npx], bad.data(), W, H);
     });

@@ -50,6 +50,7 @@ typedef struct {
   float mag[3];       /* -Mag major minor angle (1 1 0 = none)             */
   int in_fm_motion;   /* -InFmMotion: in-frame motion weighting            */
   int corr_interp;    /* -CorrInterp: interpolation correction (patch mode) */
+  const unsigned char* defects;  /* [H][W] known camera defects, or NULL */
 } oracle_params;
 
 typedef struct {

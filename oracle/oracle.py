@@ -77,6 +77,7 @@ class OracleParams(ctypes.Structure):
         ("mag", ctypes.c_float * 3),
         ("in_fm_motion", ctypes.c_int),
         ("corr_interp", ctypes.c_int),
+        ("defects", _VP),
     ]
 
 
@@ -128,7 +129,7 @@ def params(**kw) -> OracleParams:
 
 
 def process_movie(frames: np.ndarray, gain=None, force=None, int_size=None, acc_dose=None,
-                  dark=None, **kw) -> dict:
+                  dark=None, defects=None, **kw) -> dict:
     """Runs the whole oracle path.  `force` may hold global_shifts (and
     patch_shifts / patch_centers / patch_bad) to correct with given shifts;
     int_size / acc_dose describe rendered frames of a frame-integration file."""
@@ -146,6 +147,10 @@ def process_movie(frames: np.ndarray, gain=None, force=None, int_size=None, acc_
         dk = np.ascontiguousarray(dark, np.float32)
         tabs.append(dk)
         p.dark = dk.ctypes.data
+    if defects is not None:
+        df = np.ascontiguousarray(defects, np.uint8)
+        tabs.append(df)
+        p.defects = df.ctypes.data
     nz, ny, nx = frames.shape
     fr = np.ascontiguousarray(frames, np.float32)
     g = None if gain is None else np.ascontiguousarray(gain, np.float32)

@@ -464,6 +464,31 @@ def test_pipeline_in_frame_motion(api, oracle, torch_cuda, patch):
         assert e <= 1e-4, (f, e)
 
 
+def test_pipeline_known_defects(api, oracle, torch_cuda):
+    """-DefectFile / -DefectMap: known defects join the detected bad pixels
+    before the fill (BadPixel/CDetectMain.cpp:146-260); the fill itself is
+    the reference's pseudo-random one, so frames and sums agree exactly."""
+    from motioncor3_b200 import synthetic as S
+    m = S.make_movie(384, 320, 10, dose=3.0, seed=55, gain=False)
+    defects = np.zeros((320, 384), np.uint8)
+    defects[100:104, 50:300] = 1   # a few dead rows
+    defects[:, 200] = 1            # a dead column
+    p = api.Params(iter=6, tol=0.2, bft=(300, 100), fm_dose=1.2, pix_size=0.9)
+    with api.MotionCor3(p) as mc:
+        mc.set_defects(defects)
+        res = mc.process(np.asarray(m.frames))
+        mc.set_defects(None)
+        plain = mc.process(np.asarray(m.frames))
+    assert not np.array_equal(res.sums[0], plain.sums[0])
+    kw = dict(iter=6, tol=0.2, bft=(300, 100), fm_dose=1.2, pix_size=0.9)
+    same = oracle.process_movie(np.asarray(m.frames), defects=defects,
+                                force=dict(global_shifts=res.global_shifts), **kw)
+    assert same["bad_map"][defects == 1].all()
+    for i in range(res.n_sums):
+        e = _rel_rms(res.sums[i], same["sums"][i])
+        assert e <= 1e-4, (i, e)
+
+
 def test_pipeline_config1_full_size(api, oracle, torch_cuda):
     """40 frames of 1024x1024, global alignment only (-Patch 0 0 -Iter 7
     -Tol 0.5 -Bft 150 -PixSize 1.0), dose 1 e/px/frame, unit gain."""

@@ -404,3 +404,25 @@ def test_cli_eer_movie_matches_rendered_mrc_movie(tmp_path, mc3lib):
     for suf in ref["sums"]:
         t = mrcio.read(str(d / f"sum{suf}.mrc"))[0].astype(np.float64)
         assert np.array_equal(t, ref["sums"][suf]), suf
+
+
+def test_cli_defect_file_matches_reference_program(tmp_path, mc3lib):
+    """-DefectFile: rectangles of known defects (x y w h per line, clipped to
+    the frame) filled like detected bad pixels (CDetectMain::mLoadDefectFile)."""
+    if not os.path.exists(REF_BIN):
+        pytest.skip("reference program not built (oracle/ref_full)")
+    from motioncor3_b200 import build, synthetic as S
+    build.build()
+    m = S.make_movie(384, 320, 10, dose=3.0, seed=56, gain=False)
+    df = tmp_path / "defects.txt"
+    df.write_text("50 100 250 4\n200 0 1 320\n-5 300 20 40\nnot a defect\n")
+    tags = f"-Iter 6 -Tol 0.2 -Bft 300 -FmDose 1.2 -PixSize 0.9 -DefectFile {df}".split()
+    ref = run_program(REF_BIN, str(tmp_path / "ref"), m.frames, None, tags)
+    ours = run_program(OUR_BIN, str(tmp_path / "ours"), m.frames, None, tags)
+    a, b = _read_log(ref["logs"]["-Full.log"]), _read_log(ours["logs"]["-Full.log"])
+    assert np.abs(a - b).max() <= 0.05 + 1e-6
+    if np.array_equal(a, b):
+        for suf in ref["sums"]:
+            e = _rel(ref["sums"][suf], ours["sums"][suf])
+            print(f"defect file sum{suf}: rel RMS {e:.2e}")
+            assert e <= 1e-4, suf
