@@ -114,6 +114,9 @@ typedef struct {
                               stack_frames slots                               */
   int stack_on_device;     /* 1: `stack` is a device pointer                   */
   int stack_frames;        /* out: frames written to `stack`                   */
+  unsigned char* hot_map;  /* [ny][nx] host: the detected hot pixels (before the
+                              defect patches), as -OutStar lists them
+                              (CGenStarFile::SetHotPixels)                      */
 } mc3_result;
 
 /* A known alignment (the -InAln file of Align/CLoadAlign.cpp:118-250): the

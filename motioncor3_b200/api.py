@@ -98,6 +98,7 @@ class _Result(ctypes.Structure):
         ("stack", ctypes.c_void_p),
         ("stack_on_device", ctypes.c_int),
         ("stack_frames", ctypes.c_int),
+        ("hot_map", ctypes.c_void_p),
     ]
 
 

@@ -293,7 +293,7 @@ int main(int argc, char** argv) {
                 "[-Patch x y] [-Iter n] [-Tol px] [-Bft g p] [-FmDose d] [-PixSize a] "
                 "[-kV kv] [-Group g p] [-FmRef f] [-SumRange lo hi] [-PhaseOnly 0|1] [-SplitSum 0|1] "
                 "[-FtBin b] [-OutAln dir] [-InAln dir] [-OutStack 0|1 zbin] [-FmIntFile file] "
-                "[-Dark dark.mrc] [-RotGain r] [-FlipGain f] [-InvGain 0|1] [-Mag major minor angle] [-InFmMotion 0|1] [-Throw n] [-Trunc n] [-CorrInterp 0|1] [-DefectFile f] [-DefectMap f] "
+                "[-Dark dark.mrc] [-RotGain r] [-FlipGain f] [-InvGain 0|1] [-Mag major minor angle] [-InFmMotion 0|1] [-Throw n] [-Trunc n] [-CorrInterp 0|1] [-DefectFile f] [-DefectMap f] [-OutStar 0|1] "
                 "[-LogDir dir] [-Gpu id]\n");
     return eSuccess;
   }
@@ -341,6 +341,8 @@ int main(int argc, char** argv) {
   A.ints("-OutStack", p.out_stack, 2);    // CInput.cpp:590-592
   A.ints("-InFmMotion", &p.in_fm_motion, 1);
   A.ints("-CorrInterp", &p.corr_interp, 1);  // CInput.cpp:673-675
+  int out_star = 0;
+  A.ints("-OutStar", &out_star, 1);
   {
     float mg[3];
     int f0, nmag;
@@ -357,7 +359,7 @@ int main(int argc, char** argv) {
                            "-StackZ", "-Cs", "-AmpCont", "-ExtPhase", "-Serial",
                            "-Tilt", "-Crop",
                            "-GpuMemUsage", "-UseGpus",
-                           "-OutStar", "-TiffOrder"};
+                           "-TiffOrder"};
   for (const char* t : ignored) {
     int f, n;
     A.find(t, &f, &n);
@@ -651,6 +653,8 @@ int main(int argc, char** argv) {
   r.patch_bad = P ? pb.data() : nullptr;
   r.iterations = iters.data();
   r.errors = errs.data();
+  std::vector<unsigned char> hot((size_t)h.nx * h.ny);
+  if (out_star) r.hot_map = hot.data();
   std::unique_ptr<HostBuf> stack_buf;
   if (p.out_stack[0] != 0) {
     stack_buf.reset(new HostBuf(sizeof(float) * (size_t)N * ox * oy));
@@ -705,6 +709,64 @@ int main(int argc, char** argv) {
     saved = mc3::mrc::write_float_stack(name, r.stack, ox, oy, r.stack_frames, pix, mn, mx,
                                         (float)mean, 32) && saved;
     std::printf("Motion corrected stack done.\n\n");
+  }
+  // ---- RELION star file (-OutStar; CGenStarFile, CGenStarFile.cpp:44-159):
+  //      <OutMrc directory>/<movie name>.star ----
+  if (out_star) {
+    std::string name = out_mrc;
+    const size_t sl = name.rfind('/');
+    name = sl == std::string::npos ? std::string() : name.substr(0, sl + 1);
+    const size_t ms = in_mrc.rfind('/');
+    const std::string in_main = ms == std::string::npos ? in_mrc : in_mrc.substr(ms + 1);
+    std::string main = in_main;
+    const size_t dot = main.rfind('.');
+    main = dot == std::string::npos ? main + ".star" : main.substr(0, dot) + ".star";
+    if (FILE* f = std::fopen((name + main).c_str(), "wt")) {
+      std::fprintf(f, "\n# version 30001\n\n");
+      std::fprintf(f, "data_general\n\n");
+      std::fprintf(f, "%40s %-16d\n", "_rlnImageSizeX", h.nx);
+      std::fprintf(f, "%40s %-16d\n", "_rlnImageSizeY", h.ny);
+      std::fprintf(f, "%40s %-16d\n", "_rlnImageSizeZ", N);
+      std::fprintf(f, "%40s %s\n", "_rlnMicrographMovieName", in_main.c_str());
+      if (gain_mrc.empty()) {
+        std::fprintf(f, "%40s\n", "_rlnMicrographGainName");
+      } else {
+        const size_t gs = gain_mrc.rfind('/');
+        std::fprintf(f, "%40s %s\n", "_rlnMicrographGainName",
+                     (gs == std::string::npos ? gain_mrc : gain_mrc.substr(gs + 1)).c_str());
+      }
+      std::fprintf(f, "%40s %-16.6f\n", "_rlnMicrographOriginalPixelSize", p.pix_size);
+      std::fprintf(f, "%40s %-16.6f\n", "rlnMicrographBinning", p.ft_bin);
+      std::fprintf(f, "%40s %-16.6f\n", "_rlnMicrographDoseRate", p.fm_dose);
+      std::fprintf(f, "%40s %-16.6f\n", "_rlnMicrographPreExposure", 0.0f);
+      std::fprintf(f, "%40s %-16.6f\n", "_rlnVoltage", (float)p.kv);
+      std::fprintf(f, "%40s %-16d\n", "_rlnMicrographStartFrame", thr[0] + 1);
+      std::fprintf(f, "%40s %-16d\n", "_rlnMotionModelVersion", 0);
+      std::fprintf(f, "\n");
+      // SetHotPixels: the reference passes the row as an int to %f; the
+      // intended value, ny - y, is written here
+      std::fprintf(f, "data_hot_pixels\n\n");
+      std::fprintf(f, "loop\n");
+      std::fprintf(f, "_rlnCoordinateX #1\n");
+      std::fprintf(f, "_rlnCoordinateY #2\n");
+      for (int y = 0; y < h.ny; ++y)
+        for (int x = 0; x < h.nx; ++x)
+          if (hot[(size_t)y * h.nx + x])
+            std::fprintf(f, "%13.6f  %13.6f\n", x + 1.0f, (double)(h.ny - y));
+      std::fprintf(f, "\n\n");
+      // SetGlobalShifts: frame shifts relative to the first frame
+      std::fprintf(f, "# version 30001\n\n");
+      std::fprintf(f, "data_global_shift\n\n");
+      std::fprintf(f, "loop\n");
+      std::fprintf(f, "_rlnMicrographFrameNumber #1\n");
+      std::fprintf(f, "_rlnMicrographShiftX #2\n");
+      std::fprintf(f, "_rlnMicrographShiftY #3\n");
+      for (int i = 0; i < N; ++i)
+        std::fprintf(f, "%13d %13.6f %13.6f\n", i + 1, gsh[2 * i] - gsh[0],
+                     gsh[2 * i + 1] - gsh[1]);
+      std::fprintf(f, "\n");
+      std::fclose(f);
+    }
   }
   // ---- logs ----
   const std::string stem = log_stem(log_dir, in_mrc);

@@ -583,8 +583,13 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
     MC3_TRY(d_mom.ensure(sizeof(float) * 16));
     float tpl[36];
     host::defect_template(6, tpl);
+    const bool want_hot = out && out->hot_map;
+    if (want_hot) MC3_TRY(d_hot.ensure(npx));
     MC3_TRY(detect_bad_pixels(d_sum.as<float>(), W, H, d_cc.as<float>(), d_part.as<float>(),
-                              d_mom.as<float>(), d_bad.as<uint8_t>(), tpl, 6, st));
+                              d_mom.as<float>(), d_bad.as<uint8_t>(), tpl, 6, st,
+                              want_hot ? d_hot.as<uint8_t>() : nullptr));
+    if (want_hot)
+      MC3_CUDA(cudaMemcpyAsync(out->hot_map, d_hot.p, npx, cudaMemcpyDeviceToHost, st));
     // CDetectMain::mLoadDefectFile / mLoadDefectMap (BadPixel/CDetectMain.cpp:146-260)
     if (has_defects) MC3_TRY(or_mask(d_bad.as<uint8_t>(), d_defects.as<uint8_t>(), npx, st));
     MC3_TRY(d_badn.ensure(sizeof(int)));

@@ -102,7 +102,7 @@ class Engine {
   DevBuf d_xcf, d_sh, d_ex, d_ey, d_S, d_T, d_win, d_gsh, d_act, d_gstart, d_gsize;
   DevBuf d_pat, d_patoff, d_bsum, d_bimg, d_btmp, d_bmap, d_scal;
   DevBuf d_fex, d_fey, d_Wn, d_acc, d_sums, d_real, d_gath, d_pcent, d_pshift, d_pbad, d_pmask, d_out, d_bsums;
-  DevBuf d_stk, d_zgrp, d_mag, d_motion, d_defects;
+  DevBuf d_stk, d_zgrp, d_mag, d_motion, d_defects, d_hot;
   bool has_defects = false;
   int defects_w = 0, defects_h = 0;
   // loaded alignment (mc3_set_alignment)

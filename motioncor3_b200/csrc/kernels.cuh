@@ -21,8 +21,11 @@ int or_mask(uint8_t* bad, const uint8_t* defects, size_t n, cudaStream_t st);
 int moment_grid(int W, int H);
 int image_moment(const float* img, int W, int H, long pitch, int iExp, float* d_part,
                  float* d_out, cudaStream_t st);
+// hot_copy (optional, device W*H): receives the hot-pixel map before the
+// defect patches are added.
 int detect_bad_pixels(const float* sum, int W, int H, float* cc_buf, float* d_part,
-                      float* d_mom, uint8_t* bad, const float* tpl, int ms, cudaStream_t st);
+                      float* d_mom, uint8_t* bad, const float* tpl, int ms, cudaStream_t st,
+                      uint8_t* hot_copy = nullptr);
 // d_count: 1 int, d_list: W*H int2 of device scratch (bad-pixel list).
 int correct_bad_pixels(float* frames, long fr_stride, int N, const uint8_t* bad, int W, int H,
                        int* d_count, int2* d_list, cudaStream_t st);

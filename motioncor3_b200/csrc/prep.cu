@@ -270,7 +270,7 @@ __global__ void k_mark_defects(const float* cc, long pitch, int W, int H, const 
 
 int detect_bad_pixels(const float* sum, int W, int H, float* cc_buf, float* d_part,
                       float* d_mom /*4 floats*/, uint8_t* bad, const float* tpl, int ms,
-                      cudaStream_t st) {
+                      cudaStream_t st, uint8_t* hot_copy) {
   const long pitch = 2 * (W / 2 + 1);
   MC3_TRY(image_moment(sum, W, H, pitch, 1, d_part, d_mom + 0, st));
   MC3_TRY(image_moment(sum, W, H, pitch, 2, d_part, d_mom + 1, st));
@@ -280,6 +280,9 @@ int detect_bad_pixels(const float* sum, int W, int H, float* cc_buf, float* d_pa
   k_detect_hot<<<grid, 256, 0, st>>>(sum, pitch, W, H, d_mom, 6.0f, bad);
   MC3_CHECK_LAUNCH("k_detect_hot");
   }
+  // the hot pixels alone, as CGenStarFile::SetHotPixels lists them (CDetectMain.cpp:66-67)
+  if (hot_copy)
+    MC3_CUDA(cudaMemcpyAsync(hot_copy, bad, (size_t)W * H, cudaMemcpyDeviceToDevice, st));
   MC3_CUDA(cudaMemcpyToSymbolAsync(c_tpl, tpl, sizeof(float) * ms * ms, 0, cudaMemcpyHostToDevice, st));
   {
   prof::Scope ps("k_local_cc", (double)W * H * 8.0, st);

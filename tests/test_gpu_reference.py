@@ -426,3 +426,39 @@ def test_cli_defect_file_matches_reference_program(tmp_path, mc3lib):
             e = _rel(ref["sums"][suf], ours["sums"][suf])
             print(f"defect file sum{suf}: rel RMS {e:.2e}")
             assert e <= 1e-4, suf
+
+
+def _star_blocks(path):
+    lines = open(path).read().split("\n")
+    i_hot = lines.index("data_hot_pixels")
+    i_gs = lines.index("data_global_shift")
+    head = lines[:i_hot]
+    hot = [l.split() for l in lines[i_hot:i_gs] if re.fullmatch(r"\s*[0-9.+-]+\s+[^\s]+\s*", l)]
+    gs = np.array([[float(v) for v in l.split()] for l in lines[i_gs:]
+                   if re.fullmatch(r"\s*\d+\s+[-0-9.]+\s+[-0-9.]+\s*", l)])
+    return head, hot, gs
+
+
+def test_cli_star_file_matches_reference_program(tmp_path, mc3lib):
+    """-OutStar 1: the RELION star file of CGenStarFile (general block, hot
+    pixels, global shifts relative to the first frame).  The reference prints
+    the hot pixels' row with an int argument to %f, so only their columns and
+    count are compared."""
+    if not os.path.exists(REF_BIN):
+        pytest.skip("reference program not built (oracle/ref_full)")
+    from motioncor3_b200 import build, synthetic as S
+    build.build()
+    m = S.make_movie(384, 320, 10, dose=3.0, seed=57, gain=True)
+    frames = np.array(m.frames)
+    for (y, x) in [(20, 30), (150, 200), (300, 41)]:
+        frames[:, y, x] = 400.0  # hot pixels
+    tags = "-Iter 6 -Tol 0.2 -Bft 300 -FmDose 1.2 -PixSize 0.9 -OutStar 1".split()
+    ref = run_program(REF_BIN, str(tmp_path / "ref"), frames, m.gain, tags)
+    ours = run_program(OUR_BIN, str(tmp_path / "ours"), frames, m.gain, tags)
+    hr, kr, gr = _star_blocks(str(tmp_path / "ref" / "movie.star"))
+    ho, ko, go = _star_blocks(str(tmp_path / "ours" / "movie.star"))
+    assert hr == ho
+    assert len(kr) == len(ko) >= 3
+    assert [r[0] for r in kr] == [o[0] for o in ko]
+    assert gr.shape == go.shape == (10, 3)
+    assert np.abs(gr - go).max() <= 0.05 + 1e-6
