@@ -711,13 +711,15 @@ int main(int argc, char** argv) {
     std::printf("Motion corrected stack done.\n\n");
   }
   // ---- RELION star file (-OutStar; CGenStarFile, CGenStarFile.cpp:44-159):
-  //      <OutMrc directory>/<movie name>.star ----
+  //      <OutMrc directory>/<movie name>.star, where the movie name is the
+  //      -InTiff file's (CMain::mDoSingleCryoEM passes m_acInTifFile, empty for
+  //      MRC and EER input, which therefore write "<OutMrc directory>/.star") ----
   if (out_star) {
     std::string name = out_mrc;
     const size_t sl = name.rfind('/');
     name = sl == std::string::npos ? std::string() : name.substr(0, sl + 1);
-    const size_t ms = in_mrc.rfind('/');
-    const std::string in_main = ms == std::string::npos ? in_mrc : in_mrc.substr(ms + 1);
+    const size_t ms = in_tiff.rfind('/');
+    const std::string in_main = ms == std::string::npos ? in_tiff : in_tiff.substr(ms + 1);
     std::string main = in_main;
     const size_t dot = main.rfind('.');
     main = dot == std::string::npos ? main + ".star" : main.substr(0, dot) + ".star";

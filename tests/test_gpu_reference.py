@@ -455,8 +455,9 @@ def test_cli_star_file_matches_reference_program(tmp_path, mc3lib):
     tags = "-Iter 6 -Tol 0.2 -Bft 300 -FmDose 1.2 -PixSize 0.9 -OutStar 1".split()
     ref = run_program(REF_BIN, str(tmp_path / "ref"), frames, m.gain, tags)
     ours = run_program(OUR_BIN, str(tmp_path / "ours"), frames, m.gain, tags)
-    hr, kr, gr = _star_blocks(str(tmp_path / "ref" / "movie.star"))
-    ho, ko, go = _star_blocks(str(tmp_path / "ours" / "movie.star"))
+    # for MRC input the reference names the file after the (empty) -InTiff name
+    hr, kr, gr = _star_blocks(str(tmp_path / "ref" / ".star"))
+    ho, ko, go = _star_blocks(str(tmp_path / "ours" / ".star"))
     assert hr == ho
     assert len(kr) == len(ko) >= 3
     assert [r[0] for r in kr] == [o[0] for o in ko]
