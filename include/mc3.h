@@ -314,6 +314,13 @@ int mc3_eer_render(const char* path, int sampling, int n_out, const int* start, 
                    unsigned char* dst, int threads);
 
 /* ---- host-side bookkeeping (host pointers) ---- */
+/* CFmGroupParam::Setup (DataUtil/CFmGroupParam.cpp:26-78): groups of the
+ * n rendered frames (start/size in raw frames) for -Group bin_z: runs holding
+ * bin_z x (smallest rendered-frame size) raw frames; writes up to max_groups
+ * group starts, sizes (in rendered frames) and centres (mean frame time
+ * stamps) and their count in *n_groups. */
+int mc3_frame_groups(const int* start, const int* size, int n, int bin_z, int max_groups,
+                     int* n_groups, int* g_start, int* g_size, float* g_center);
 /* CLoadRefs::PostProcess (CLoadRefs.cpp:204-229): rotation by rot x 90
  * degrees (G90Rotate2D, nearest pixel about the centre; odd factors swap the
  * size), flip (1 upside down, 2 left-right; GFlip2D), then 1/v with 0 kept

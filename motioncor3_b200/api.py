@@ -153,6 +153,7 @@ _SIGS = {
     "mc3_set_alignment": ([_VP, ctypes.POINTER(_Alignment)], _I),
     "mc3_set_frame_integration": ([_VP, ctypes.POINTER(_FrameIntegration)], _I),
     "mc3_read_fmint_file": ([ctypes.c_char_p, _F, _I, _VP, _VP, _VP, _VP], _I),
+    "mc3_frame_groups": ([_VP, _VP, _I, _I, _I, _VP, _VP, _VP, _VP], _I),
     "mc3_frame_integration_tables": ([_VP, _VP, _VP, _I, _I, _F, _I, _I, _I, _VP, _VP, _VP, _VP,
                                       _VP], _I),
     "mc3_fft_forward": ([_VP, _I, _I, _I, _I, _VP], _I),
@@ -648,6 +649,21 @@ def frame_integration_tables(entries, n_raw: int, fm_dose: float = 0.0, throw=(0
                                                ctypes.byref(dwt)), "mc3_frame_integration_tables")
     k = nint.value
     return dict(start=start[:k], size=size[:k], acc_dose=acc[:k], dose_weight=dwt.value)
+
+
+def frame_groups(start, size, bin_z: int) -> dict:
+    """CFmGroupParam::Setup over rendered frames (mc3_frame_groups)."""
+    st = np.ascontiguousarray(start, np.int32)
+    sz = np.ascontiguousarray(size, np.int32)
+    n = len(st)
+    gs = np.zeros(n, np.int32)
+    gz = np.zeros(n, np.int32)
+    gc = np.zeros(n, np.float32)
+    ng = ctypes.c_int(0)
+    _check(_lib().mc3_frame_groups(_hp(st), _hp(sz), n, bin_z, n, ctypes.byref(ng), _hp(gs),
+                                   _hp(gz), _hp(gc)), "mc3_frame_groups")
+    k = ng.value
+    return dict(start=gs[:k], size=gz[:k], center=gc[:k])
 
 
 # ---- diagnostics ----

@@ -182,6 +182,26 @@ int mc3_read_fmint_file(const char* path, float fm_dose, int max_entries, int* g
   return MC3_OK;
 }
 
+int mc3_frame_groups(const int* start, const int* size, int n, int bin_z, int max_groups,
+                     int* n_groups, int* g_start, int* g_size, float* g_center) {
+  if (!start || !size || n < 1 || bin_z < 1 || !n_groups) return MC3_EINVAL;
+  host::FmInt t;
+  t.start.assign(start, start + n);
+  t.size.assign(size, size + n);
+  t.dose.assign(n, 0.0f);
+  t.acc.assign(n, 0.0f);
+  t.centers();
+  host::FrameGroups g;
+  g.setup(t, bin_z);
+  *n_groups = g.count();
+  for (int i = 0; i < g.count() && i < max_groups; ++i) {
+    if (g_start) g_start[i] = g.start[i];
+    if (g_size) g_size[i] = g.size[i];
+    if (g_center) g_center[i] = g.center[i];
+  }
+  return MC3_OK;
+}
+
 int mc3_frame_integration_tables(const int* group_size, const int* int_size, const float* dose,
                                  int n_entries, int n_raw, float fm_dose, int throw_first,
                                  int throw_last, int max_int, int* n_int, int* start, int* size,

@@ -14,6 +14,8 @@
 // only to construct inputs and read results.
 #define private public
 #include "Align/CAlignInc.h"
+#include "CMainInc.h"
+#include "DataUtil/CDataUtilInc.h"
 #include "Util/CUtilInc.h"
 #include <Util/Util_LinEqs.h>
 #undef private
@@ -33,16 +35,9 @@ extern "C" cudaError_t cudaMemcpy(void* d, const void* s, size_t n, cudaMemcpyKi
   return cudaSuccess;
 }
 
-// The settings singletons are reached only from CFmIntParam::Setup and the
-// dose/sum-range queries, which this harness never calls; these stand-ins
-// satisfy the linker.
-CInput* CInput::GetInstance(void) { return nullptr; }
-DataUtil::CReadFmIntFile* DataUtil::CReadFmIntFile::GetInstance(void) { return nullptr; }
-int DataUtil::CReadFmIntFile::GetIntSize(int) { return 1; }
-int DataUtil::CReadFmIntFile::GetGroupSize(int) { return 1; }
-bool DataUtil::CReadFmIntFile::NeedIntegrate(void) { return false; }
-float DataUtil::CReadFmIntFile::GetDose(int) { return 0.0f; }
-bool DataUtil::CReadFmIntFile::HasDose(void) { return false; }
+// CInput, CParseArgs and CReadFmIntFile are compiled from the reference too:
+// the frame-integration tables below are set up through the reference's own
+// singletons with the command-line values written into CInput.
 
 extern "C" {
 
@@ -146,6 +141,40 @@ void ref_patch_shifts(const float* raw, const float* centres, int N, int P, int 
       out_shifts[((size_t)f * P + p) * 2 + 1] = v[1];
       out_bad[(size_t)f * P + p] = ps.m_pbBadShifts[(size_t)f * P + p] ? 1 : 0;
     }
+}
+
+// CReadFmIntFile::DoIt, CFmIntParam::Setup and CFmGroupParam::Setup of the
+// reference for n_raw raw frames, with -FmIntFile path (NULL or "" for
+// none), -FmDose and -Throw / -Trunc; tables truncated to max_n entries.
+int ref_fmint(const char* path, float fm_dose, int throw0, int throw1, int n_raw, int bin_z,
+              int max_n, int* n_int, int* start, int* size, float* acc, float* cent,
+              int* n_groups, int* g_start, int* g_size, float* g_cent, int* has_dose) {
+  CInput* in = CInput::GetInstance();
+  std::snprintf(in->m_acFmIntFile, sizeof(in->m_acFmIntFile), "%s", path ? path : "");
+  in->m_fFmDose = fm_dose;
+  in->m_aiThrow[0] = throw0;
+  in->m_aiThrow[1] = throw1;
+  DataUtil::CReadFmIntFile* rf = DataUtil::CReadFmIntFile::GetInstance();
+  rf->DoIt();
+  *has_dose = rf->HasDose() ? 1 : 0;
+  DataUtil::CFmIntParam ip;
+  ip.Setup(n_raw, 0);
+  *n_int = ip.m_iNumIntFms;
+  for (int i = 0; i < ip.m_iNumIntFms && i < max_n; ++i) {
+    start[i] = ip.m_piIntFmStart[i];
+    size[i] = ip.m_piIntFmSize[i];
+    acc[i] = ip.m_pfAccFmDose[i];
+    cent[i] = ip.m_pfIntFmCents[i];
+  }
+  DataUtil::CFmGroupParam gp;
+  gp.Setup(bin_z, &ip);
+  *n_groups = gp.m_iNumGroups;
+  for (int g = 0; g < gp.m_iNumGroups && g < max_n; ++g) {
+    g_start[g] = gp.m_piGroupStart[g];
+    g_size[g] = gp.m_piGroupSize[g];
+    g_cent[g] = gp.m_pfGroupCenters[g];
+  }
+  return 0;
 }
 
 }  // extern "C"

@@ -42,6 +42,8 @@ def ref_host():
     P = ctypes.c_void_p
     L.ref_interpolate.restype = ctypes.c_int
     L.ref_lin_eqs.restype = ctypes.c_int
+    if hasattr(L, "ref_fmint"):
+        L.ref_fmint.restype = ctypes.c_int
     return L
 
 

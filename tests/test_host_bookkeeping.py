@@ -101,3 +101,54 @@ def test_golden_vectors(mc3lib):
         x, y = api.smooth_shifts(np.array(c["x"]), np.array(c["y"]), c["w"])
         assert np.array_equal(x, np.array(c["x_out"], np.float32))
         assert np.array_equal(y, np.array(c["y_out"], np.float32))
+
+
+def _ref_fmint(ref_host, path, fm_dose, throws, n_raw, bin_z):
+    n = n_raw
+    I = lambda: np.zeros(n, np.int32)
+    F = lambda: np.zeros(n, np.float32)
+    st, sz, acc, cen, gs, gz, gc = I(), I(), F(), F(), I(), I(), F()
+    ni, ng, hd = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+    ref_host.ref_fmint(path.encode() if path else None, ctypes.c_float(fm_dose), throws[0],
+                       throws[1], n_raw, bin_z, n, ctypes.byref(ni), fp(st), fp(sz), fp(acc),
+                       fp(cen), ctypes.byref(ng), fp(gs), fp(gz), fp(gc), ctypes.byref(hd))
+    k, g = ni.value, ng.value
+    return dict(start=st[:k], size=sz[:k], acc=acc[:k], center=cen[:k], g_start=gs[:g],
+                g_size=gz[:g], g_center=gc[:g], has_dose=hd.value)
+
+
+@pytest.mark.parametrize("text,fm_dose,n_raw,throws,bin_z", [
+    ("40 4 0.5\n", 0.0, 40, (0, 0), 1),
+    ("40 4 0.5\n", 0.0, 43, (0, 0), 2),
+    ("40 4 0.5\n", 0.0, 37, (1, 2), 3),
+    ("20 2 0.25\n30 3 0.25\n", 0.0, 50, (0, 0), 2),
+    ("21 2 0.25\n30 3 0.25\n", 0.0, 51, (2, 0), 4),
+    ("21 2 0.25\n\n30 3 0.25\n", 0.0, 60, (0, 1), 2),   # blank line: repeated entry
+    ("40 4\n10 1\n", 0.7, 50, (0, 0), 2),                # two columns: -FmDose
+    ("40 4 0.5\n20 2 0.6\n", 1.5, 30, (0, 0), 3),        # mixed doses: file dropped
+    ("30 1 0.8\n", 1.2, 30, (2, 1), 4),                  # no integration: -FmDose doses
+    (None, 0.9, 25, (3, 2), 3),                          # no file at all
+])
+def test_frame_tables_and_groups_match_reference(mc3lib, ref_host, tmp_path, text, fm_dose,
+                                                 n_raw, throws, bin_z):
+    """CReadFmIntFile::DoIt + CFmIntParam::Setup + CFmGroupParam::Setup of the
+    reference, compiled from its sources, against mc3_read_fmint_file +
+    mc3_frame_integration_tables + mc3_frame_groups: same rendered frames,
+    doses, time stamps and groups (bit for bit)."""
+    from motioncor3_b200 import api
+    path = None
+    if text is not None:
+        f = tmp_path / "fmint.txt"
+        f.write_text(text)
+        path = str(f)
+    ref = _ref_fmint(ref_host, path, fm_dose, throws, n_raw, bin_z)
+    entries = api.read_fmint_file(path, fm_dose) if path else None
+    t = api.frame_integration_tables(entries, n_raw, fm_dose=fm_dose, throw=throws)
+    assert t["start"].tolist() == ref["start"].tolist()
+    assert t["size"].tolist() == ref["size"].tolist()
+    assert np.array_equal(t["acc_dose"], ref["acc"])
+    assert t["dose_weight"] == ref["has_dose"]
+    g = api.frame_groups(t["start"], t["size"], bin_z)
+    assert g["start"].tolist() == ref["g_start"].tolist()
+    assert g["size"].tolist() == ref["g_size"].tolist()
+    assert np.array_equal(g["center"], ref["g_center"])
