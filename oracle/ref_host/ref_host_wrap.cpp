@@ -16,6 +16,7 @@
 #include "Align/CAlignInc.h"
 #include "CMainInc.h"
 #include "DataUtil/CDataUtilInc.h"
+#include "EerUtil/CEerUtilInc.h"
 #include "Util/CUtilInc.h"
 #include <Util/Util_LinEqs.h>
 #undef private
@@ -175,6 +176,20 @@ int ref_fmint(const char* path, float fm_dose, int throw0, int throw1, int n_raw
     g_cent[g] = gp.m_pfGroupCenters[g];
   }
   return 0;
+}
+
+// EerUtil::CDecodeEerFrame of the reference on one EER frame (its electrons
+// are added to `frame`, cam x cam y times the sampling factor squared); the
+// buffer is padded because the 7-bit decoder reads whole 32-bit words.
+void ref_eer_decode(const unsigned char* data, int nbytes, int cam_x, int cam_y, int sampling,
+                    int bits, unsigned char* frame) {
+  EerUtil::CDecodeEerFrame d;
+  int cam[2] = {cam_x, cam_y};
+  d.Setup(cam, sampling);
+  std::vector<unsigned char> buf(data, data + nbytes);
+  buf.resize((size_t)nbytes + 8, 0);
+  if (bits == 7) d.Do7Bits(buf.data(), nbytes, frame);
+  else d.Do8Bits(buf.data(), nbytes, frame);
 }
 
 }  // extern "C"
