@@ -509,8 +509,13 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
   MC3_TRY(g.compute(mv.nx, mv.ny, fi.count(), prm, fmint && fmint_dose));
   const int Nraw = mv.nz;
   bool render = false;  // some rendered frame sums several raw frames
-  for (int i = 0; fmint && !fmint_rendered && i < fi.count(); ++i)
-    render = render || fi.size[i] != 1 || fi.start[i] != i;
+  long first_raw = 0;   // one raw frame per frame from here on (-Throw)
+  if (fmint && !fmint_rendered) {
+    for (int i = 0; i < fi.count(); ++i) render = render || fi.size[i] != 1;
+    first_raw = fi.start[0];
+    for (int i = 0; !render && i < fi.count(); ++i) render = fi.start[i] != first_raw + i;
+    if (render) first_raw = 0;
+  }
   if (render && !(mv.mode == 0 || mv.mode == 5 || mv.mode == 101)) {
     // the reference renders integrated frames as 8-bit (CLoadCryoEMStack::OpenFile)
     last_error = "frame integration needs an 8-bit or 4-bit movie";
@@ -571,6 +576,7 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
                              dark, has_gain ? d_gain.as<float>() : nullptr, frames, fr_stride_f,
                              prm.correct_bad ? d_sum.as<float>() : nullptr, W, H, N, st));
   } else {
+    if (first_raw) raw = static_cast<const char*>(raw) + (size_t)first_raw * fbytes;
     MC3_TRY(gain_and_sum(raw, mv.mode, raw_stride, dark, has_gain ? d_gain.as<float>() : nullptr, frames,
                          fr_stride_f, prm.correct_bad ? d_sum.as<float>() : nullptr, W, H, N, st));
   }

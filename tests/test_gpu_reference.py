@@ -463,3 +463,27 @@ def test_cli_star_file_matches_reference_program(tmp_path, mc3lib):
     assert [r[0] for r in kr] == [o[0] for o in ko]
     assert gr.shape == go.shape == (10, 3)
     assert np.abs(gr - go).max() <= 0.05 + 1e-6
+
+
+def test_cli_fmint_file_without_integration_and_throws(tmp_path, mc3lib):
+    """A frame-integration file with integration size 1 (no rendering,
+    CReadFmIntFile::NeedIntegrate false) on a float movie with -Throw 2: the
+    kept raw frames, doses from -FmDose counted from the first kept frame,
+    dose weighting switched on by the file's dose (CFmIntParam::mSetup)."""
+    if not os.path.exists(REF_BIN):
+        pytest.skip("reference program not built (oracle/ref_full)")
+    from motioncor3_b200 import build, synthetic as S
+    build.build()
+    m = S.make_movie(384, 320, 14, dose=3.0, seed=58, gain=False)
+    fm = tmp_path / "fmint.txt"
+    fm.write_text("14 1 0.8\n")
+    tags = f"-Iter 6 -Tol 0.2 -Bft 300 -PixSize 0.9 -FmDose 1.2 -Throw 2 -FmIntFile {fm}".split()
+    ref = run_program(REF_BIN, str(tmp_path / "ref"), m.frames, None, tags)
+    ours = run_program(OUR_BIN, str(tmp_path / "ours"), m.frames, None, tags)
+    assert sorted(ref["sums"]) == sorted(ours["sums"])
+    a, b = _read_log(ref["logs"]["-Full.log"]), _read_log(ours["logs"]["-Full.log"])
+    assert a.shape == b.shape == (12, 3)
+    assert np.abs(a - b).max() <= 0.05 + 1e-6
+    if np.array_equal(a, b):
+        for suf in ref["sums"]:
+            assert _rel(ref["sums"][suf], ours["sums"][suf]) <= 1e-4, suf
