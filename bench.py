@@ -283,6 +283,22 @@ def run_ours(args, wl, world, rank, local):
                 "share_of_step": tot_ms / ms if ms else None,
                 "algorithmic_bytes_per_launch": tot_bytes / n_launch}
 
+    # ---- accuracy of the timed run: full-frame shifts against the drift the
+    #      generator applied (relative to the central frame; the reference's
+    #      two smoothings follow a jittery random walk only to about a pixel) ----
+    accuracy = None
+    try:
+        est = np.asarray(last.global_shifts, np.float64)
+        ref_f = nz // 2
+        est = est - est[ref_f]
+        true = -(np.asarray(mv.drift, np.float64) - np.asarray(mv.drift, np.float64)[ref_f])
+        d = np.abs(est - true)
+        accuracy = {"shift_err_vs_truth_px_max": float(d.max()),
+                    "shift_err_vs_truth_px_rms": float(np.sqrt(np.mean(d ** 2))),
+                    "iterations_global": int(last.iterations[0])}
+    except Exception as exc:  # the report never fails on this extra
+        accuracy = {"error": str(exc)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         n = CPU_SAMPLE_FRAMES
@@ -309,6 +325,7 @@ def run_ours(args, wl, world, rank, local):
             "clocks": clk,
             "roofline": roof,
             "cpu_baseline": cpu,
+            "accuracy": accuracy,
             "kernels": {k: {"launches_per_step": v[0] / args.steps, "ms_per_step": v[1] / args.steps,
                             "GBps": (v[2] / v[1] / 1e6) if v[1] else None}
                         for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
