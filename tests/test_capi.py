@@ -206,3 +206,43 @@ def test_frame_tables_with_throws(mc3lib):
     assert np.allclose(t["acc_dose"], 0.5 * np.arange(1, 16, dtype=np.float32))
     t = api.frame_integration_tables(([24], [4], [0.5]), 24, throw=(1, 1))
     assert t["size"].tolist() == [4] * 6  # 6 - 2 = 4 <= 5: throws ignored
+
+
+def test_argument_checks_without_gpu(mc3lib):
+    """Entry points reject bad arguments with a status code (never abort),
+    before touching a device."""
+    from motioncor3_b200 import api
+    L = api._lib()
+    EINVAL = api.MC3_EINVAL
+    assert L.mc3_set_alignment(None, None) == EINVAL
+    assert L.mc3_set_frame_integration(None, None) == EINVAL
+    assert L.mc3_set_dark(None, None, 0, 0, 0) == EINVAL
+    assert L.mc3_set_defects(None, None, 0, 0) == EINVAL
+    img = np.ones((4, 6), np.float32)
+    out = np.zeros(24, np.float32)
+    nx, ny = ctypes.c_int(0), ctypes.c_int(0)
+    assert L.mc3_ref_orient(img.ctypes.data, 6, 4, 0, 3, 0, out.ctypes.data, ctypes.byref(nx),
+                            ctypes.byref(ny)) == EINVAL  # flip must be 0, 1 or 2
+    assert L.mc3_ref_augment(img.ctypes.data, 6, 4, 0, out.ctypes.data) == EINVAL
+    n = ctypes.c_int(0)
+    assert L.mc3_frame_integration_tables(None, None, None, 0, 10, ctypes.c_float(1.0), -1, 0, 10,
+                                          ctypes.byref(n), None, None, None, None) == EINVAL
+    assert L.mc3_frame_integration_tables(None, None, None, 0, 10, ctypes.c_float(1.0), 6, 5, 10,
+                                          ctypes.byref(n), None, None, None, None) == EINVAL
+    assert L.mc3_frame_groups(None, None, 0, 1, 0, ctypes.byref(n), None, None, None) == EINVAL
+    assert L.mc3_eer_render(None, 1, 1, None, None, None, 0) == EINVAL
+    assert L.mc3_tiff_read(b"x.tif", -1, 1, out.ctypes.data, 1) == EINVAL
+
+
+def test_create_without_a_gpu_fails_cleanly(mc3lib):
+    """Without a CUDA device mc3_create returns an error status instead of
+    aborting the process (CSimpleFuncs.cpp:203-212 resets the device and
+    asserts instead)."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from motioncor3_b200 import api
+    p = api.Params().to_c()
+    h = ctypes.c_void_p()
+    rc = api._lib().mc3_create(ctypes.byref(p), ctypes.byref(h))
+    assert rc != api.MC3_OK and not h.value
