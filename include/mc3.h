@@ -68,6 +68,15 @@ typedef struct {
   int corr_interp;     /* -CorrInterp (0): in patch mode divide each globally
                           corrected frame spectrum by sinc(pi r)^(1/8)
                           (Util/GCorrLinearInterp.cu)                         */
+  float cs;            /* -Cs mm: spherical aberration.  The CTF of the first
+                          sum is estimated when cs > 0.001, kv != 0 and
+                          pix_size != 0 (CFindCtfMain::bEstimate,
+                          FindCtf/CFindCtfMain.cpp:26-40).  Library default 0
+                          (no estimate); the command line's default is the
+                          reference's 2.7                                     */
+  float amp_cont;      /* -AmpCont (0.07): amplitude contrast                 */
+  float ext_phase;     /* -ExtPhase deg (0): the extra phase searched spans
+                          [0, min(2 ext_phase, 180)]                          */
 } mc3_params;
 
 /* Sizes a movie will use (CBufferPool::CreateBuffers, CBufferPool.cpp:95-270). */
@@ -117,6 +126,14 @@ typedef struct {
   unsigned char* hot_map;  /* [ny][nx] host: the detected hot pixels (before the
                               defect patches), as -OutStar lists them
                               (CGenStarFile::SetHotPixels)                      */
+  float ctf[6];            /* out when ctf_done: defocus max, defocus min (A),
+                              astigmatism azimuth (deg), extra phase (deg),
+                              score, fit resolution (A), as the _Ctf.txt line
+                              (CSaveSerialCryoEM::mSaveCtfFit)                 */
+  int ctf_done;            /* out: 1 when the CTF was estimated                */
+  float* ctf_spectrum;     /* [512][512]: the averaged spectrum with the fitted
+                              CTF drawn in (<stem>_Ctf.mrc)                    */
+  int ctf_spectrum_on_device; /* 1: `ctf_spectrum` is a device pointer         */
 } mc3_result;
 
 /* A known alignment (the -InAln file of Align/CLoadAlign.cpp:118-250): the
@@ -193,6 +210,16 @@ int mc3_set_defects(mc3_ctx* ctx, const unsigned char* mask, int nx, int ny);
  * BadPixel::CDetectMain::DoIt, BadPixel::CCorrectMain::DoIt and
  * Align::CAlignMain::DoIt (Align/CAlignMain.cpp:39-75). */
 int mc3_process_movie(mc3_ctx* ctx, const mc3_movie* movie, mc3_result* out);
+/* CTF estimate of one image [ny][nx] (even sizes) at pixel size pix_size A:
+ * the role of FindCtf::CFindCtfMain::DoIt (FindCtf/CFindCtfMain.cpp:49-83),
+ * which the reference runs on the first sum of every movie
+ * (Correct/CCorrectFullShift.cpp:129-144).  result6 as mc3_result::ctf;
+ * spectrum512 (may be NULL) on the host, or on the device when on_device.
+ * MC3_EUNSUPPORTED when the image, rescaled to >= 1.25 A pixels, holds no
+ * 512 x 512 tile. */
+int mc3_estimate_ctf(mc3_ctx* ctx, const float* image, int nx, int ny, int on_device,
+                     float pix_size, float kv, float cs, float amp_cont, float ext_phase,
+                     float* result6, float* spectrum512);
 /* Loading the next movie while the current one is processed, as the
  * reference's loader thread does (MrcUtil/CLoadCryoEMStack.cpp:130-180):
  * starts the host->device copy of `movie`'s raw frames on the context's

@@ -55,6 +55,9 @@ class _Params(ctypes.Structure):
         ("mag", ctypes.c_float * 3),
         ("in_fm_motion", ctypes.c_int),
         ("corr_interp", ctypes.c_int),
+        ("cs", ctypes.c_float),
+        ("amp_cont", ctypes.c_float),
+        ("ext_phase", ctypes.c_float),
     ]
 
 
@@ -99,6 +102,10 @@ class _Result(ctypes.Structure):
         ("stack_on_device", ctypes.c_int),
         ("stack_frames", ctypes.c_int),
         ("hot_map", ctypes.c_void_p),
+        ("ctf", ctypes.c_float * 6),
+        ("ctf_done", ctypes.c_int),
+        ("ctf_spectrum", ctypes.c_void_p),
+        ("ctf_spectrum_on_device", ctypes.c_int),
     ]
 
 
@@ -149,6 +156,7 @@ _SIGS = {
     "mc3_eer_info": ([ctypes.c_char_p, _VP, _VP, _VP, _VP], _I),
     "mc3_eer_render": ([ctypes.c_char_p, _I, _I, _VP, _VP, _VP, _I], _I),
     "mc3_process_movie": ([_VP, ctypes.POINTER(_Movie), ctypes.POINTER(_Result)], _I),
+    "mc3_estimate_ctf": ([_VP, _VP, _I, _I, _I, _F, _F, _F, _F, _F, _VP, _VP], _I),
     "mc3_prefetch_movie": ([_VP, ctypes.POINTER(_Movie)], _I),
     "mc3_set_alignment": ([_VP, ctypes.POINTER(_Alignment)], _I),
     "mc3_set_frame_integration": ([_VP, ctypes.POINTER(_FrameIntegration)], _I),
@@ -240,6 +248,9 @@ class Params:
     mag: tuple = (1.0, 1.0, 0.0)
     in_fm_motion: int = 0
     corr_interp: int = 0
+    cs: float = 0.0          # > 0.001 (with pix_size, kv) turns the CTF estimate on
+    amp_cont: float = 0.07
+    ext_phase: float = 0.0
 
     def to_c(self) -> _Params:
         p = _Params()
@@ -268,6 +279,9 @@ class Params:
             p.mag[i] = float(self.mag[i])
         p.in_fm_motion = int(self.in_fm_motion)
         p.corr_interp = int(self.corr_interp)
+        p.cs = float(self.cs)
+        p.amp_cont = float(self.amp_cont)
+        p.ext_phase = float(self.ext_phase)
         return p
 
 
@@ -284,6 +298,8 @@ class Result:
     n_patches: int
     time_ms: float
     stack: Optional[np.ndarray] = None  # [stack_frames][ny][nx] aligned frames (-OutStack)
+    ctf: Optional[np.ndarray] = None    # dfmax, dfmin (A), azimuth, phase (deg), score, res (A)
+    ctf_spectrum: Optional[np.ndarray] = None  # [512][512] diagnostic spectrum
 
 
 _MODES = {np.dtype(np.uint8): 0, np.dtype(np.int16): 1, np.dtype(np.float32): 2, np.dtype(np.uint16): 6}
@@ -469,6 +485,8 @@ class MotionCor3:
             ox, oy = info["out_size"]
             stack = np.zeros((nz, oy, ox), np.float32)
             r.stack = stack.ctypes.data
+        ctf_img = np.zeros((512, 512), np.float32)
+        r.ctf_spectrum = ctf_img.ctypes.data
         _check(_lib().mc3_process_movie(self._h, ctypes.byref(mv), ctypes.byref(r)),
                "mc3_process_movie")
         if stack is not None:
@@ -479,7 +497,30 @@ class MotionCor3:
         return Result(sums=sums, global_shifts=gsh, patch_shifts=psh if P else None,
                       patch_centers=pc if P else None, patch_bad=pb if P else None,
                       iterations=iters, errors=errs, n_sums=r.n_sums, n_patches=r.n_patches,
-                      time_ms=r.time_ms, stack=stack)
+                      time_ms=r.time_ms, stack=stack,
+                      ctf=np.array(r.ctf[:], np.float32) if r.ctf_done else None,
+                      ctf_spectrum=ctf_img if r.ctf_done else None)
+
+    def estimate_ctf(self, image, pix_size: float, kv: float = 300.0, cs: float = 2.7,
+                     amp_cont: float = 0.07, ext_phase: float = 0.0):
+        """CTF of one image [ny][nx] (numpy float32, or a CUDA tensor):
+        (res6, spectrum512) with res6 = dfmax, dfmin (A), azimuth, phase (deg),
+        score, resolution (A) (mc3_estimate_ctf)."""
+        res = np.zeros(6, np.float32)
+        if hasattr(image, "data_ptr"):
+            import torch
+            ny, nx = image.shape
+            spec = torch.empty((512, 512), dtype=torch.float32, device=image.device)
+            _check(_lib().mc3_estimate_ctf(self._h, _dp(image), nx, ny, 1, pix_size, kv, cs, amp_cont,
+                                           ext_phase, _hp(res), _dp(spec)), "mc3_estimate_ctf")
+            torch.cuda.synchronize()
+            return res, spec.cpu().numpy()
+        img = np.ascontiguousarray(image, np.float32)
+        ny, nx = img.shape
+        spec = np.zeros((512, 512), np.float32)
+        _check(_lib().mc3_estimate_ctf(self._h, _hp(img), nx, ny, 0, pix_size, kv, cs, amp_cont,
+                                       ext_phase, _hp(res), _hp(spec)), "mc3_estimate_ctf")
+        return res, spec
 
     # ---- component entry points needing the context ----
     def iterative_align(self, stack, group: int, max_iter: int, tol: float, bfactor: float,

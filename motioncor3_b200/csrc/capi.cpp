@@ -70,6 +70,9 @@ void mc3_params_default(mc3_params* p) {
   p->mag[2] = 0.0f;
   p->in_fm_motion = 0;
   p->corr_interp = 0;
+  p->cs = 0.0f;
+  p->amp_cont = 0.07f;
+  p->ext_phase = 0.0f;
 }
 
 int mc3_create(const mc3_params* p, mc3_ctx** out) {
@@ -150,6 +153,25 @@ int mc3_set_gain(mc3_ctx* ctx, const float* gain, int nx, int ny, int on_device)
 int mc3_process_movie(mc3_ctx* ctx, const mc3_movie* movie, mc3_result* out) {
   if (!ctx || !movie) return MC3_EINVAL;
   return ctx->eng->process(*movie, out);
+}
+
+int mc3_estimate_ctf(mc3_ctx* ctx, const float* image, int nx, int ny, int on_device, float pix_size,
+                     float kv, float cs, float amp_cont, float ext_phase, float* result6,
+                     float* spectrum512) {
+  if (!ctx || !image || !result6 || nx < 2 || ny < 2 || !(pix_size > 0) || !(kv > 0) ||
+      !(amp_cont >= 0 && amp_cont < 1))
+    return MC3_EINVAL;
+  Engine* e = ctx->eng;
+  MC3_CUDA(cudaSetDevice(e->device));
+  const float* d_img = image;
+  if (!on_device) {
+    MC3_TRY(e->d_out.ensure(sizeof(float) * (size_t)nx * ny));
+    MC3_CUDA(cudaMemcpyAsync(e->d_out.p, image, sizeof(float) * (size_t)nx * ny, cudaMemcpyHostToDevice,
+                             e->stream));
+    d_img = e->d_out.as<float>();
+  }
+  return estimate_ctf(d_img, nx, ny, pix_size, kv, cs, amp_cont, ext_phase, result6, spectrum512,
+                      on_device != 0, e->ctf, e->stream);
 }
 
 int mc3_prefetch_movie(mc3_ctx* ctx, const mc3_movie* movie) {

@@ -341,6 +341,10 @@ int main(int argc, char** argv) {
   A.ints("-OutStack", p.out_stack, 2);    // CInput.cpp:590-592
   A.ints("-InFmMotion", &p.in_fm_motion, 1);
   A.ints("-CorrInterp", &p.corr_interp, 1);  // CInput.cpp:673-675
+  p.cs = 2.7f;  // CInput::CInput (CInput.cpp:96-99): the command line estimates the CTF by default
+  A.floats("-Cs", &p.cs, 1);
+  A.floats("-AmpCont", &p.amp_cont, 1);
+  A.floats("-ExtPhase", &p.ext_phase, 1);
   int out_star = 0;
   A.ints("-OutStar", &out_star, 1);
   {
@@ -356,7 +360,7 @@ int main(int argc, char** argv) {
   if (A.ints("-Gpu", gpu, 8) > 0) p.gpu = gpu[0];
   const char* ignored[] = { "-InSuffix", "-InSkips", "-ArcDir",
                            "-FullSum", "-TmpFile",
-                           "-StackZ", "-Cs", "-AmpCont", "-ExtPhase", "-Serial",
+                           "-StackZ", "-Serial",
                            "-Tilt", "-Crop",
                            "-GpuMemUsage", "-UseGpus",
                            "-TiffOrder"};
@@ -367,6 +371,12 @@ int main(int argc, char** argv) {
   }
   if (in_mrc.empty() || out_mrc.empty()) return eFailLoad;
   if (in_mrc == out_mrc) return eInputOutputSame;
+  if (!(p.cs > 0.001f && p.kv != 0 && p.pix_size != 0)) {  // CFindCtfMain::bEstimate (:26-40)
+    std::printf("Skip CTF estimation. Need the following parameters.\n");
+    std::printf("High tension: %d\n", p.kv);
+    std::printf("Cs value:     %f\n", p.cs);
+    std::printf("Pixel size:   %f\n\n", p.pix_size);
+  }
 
   mc3::mrc::Header h;
   int eer_bits = 0;
@@ -655,6 +665,8 @@ int main(int argc, char** argv) {
   r.errors = errs.data();
   std::vector<unsigned char> hot((size_t)h.nx * h.ny);
   if (out_star) r.hot_map = hot.data();
+  std::vector<float> ctf_img((size_t)512 * 512);
+  r.ctf_spectrum = ctf_img.data();
   std::unique_ptr<HostBuf> stack_buf;
   if (p.out_stack[0] != 0) {
     stack_buf.reset(new HostBuf(sizeof(float) * (size_t)N * ox * oy));
@@ -670,6 +682,12 @@ int main(int argc, char** argv) {
   }
   for (int i = 0; i < iters[0]; ++i)
     std::printf("Iteration %2d  Error: %9.3f\n", i + 1, errs[i]);
+  if (r.ctf_done) {  // CFindCtfMain::DoIt (FindCtf/CFindCtfMain.cpp:65-78)
+    std::printf("CTF estimate\n");
+    std::printf("  Df_max [A]   Df_min [A]  Azimuth [d]  Phase [d]    Score       Res\n");
+    std::printf("  %9.2f    %9.2f  %8.2f    %7.2f    %9.4f  %7.2f\n\n", r.ctf[0], r.ctf[1], r.ctf[2],
+                r.ctf[3], r.ctf[4], r.ctf[5]);
+  }
   std::printf("Computation time: %f sec\n\n", std::chrono::duration<double>(t1 - t0).count());
   // ---- sums ----
   // file name extensions in the order of CAlnSums::Setup (DataUtil/CAlnSums.cpp:18-43)
@@ -709,6 +727,26 @@ int main(int argc, char** argv) {
     saved = mc3::mrc::write_float_stack(name, r.stack, ox, oy, r.stack_frames, pix, mn, mx,
                                         (float)mean, 32) && saved;
     std::printf("Motion corrected stack done.\n\n");
+  }
+  // ---- CTF outputs (CSaveSerialCryoEM::mSaveCtfStack / mSaveCtfFit,
+  //      CSaveSerialCryoEM.cpp:243-297): the 512 x 512 spectrum (pixel size 1,
+  //      header statistics left at their defaults) and the fit line ----
+  if (r.ctf_done) {
+    saved = mc3::mrc::write_float_image(out_name(out_mrc, "_Ctf", ".mrc"), ctf_img.data(), 512, 512, 1.0f,
+                                        0.f, 0.f, 0.f) && saved;
+    const std::string txt = out_name(out_mrc, "_Ctf", ".txt");
+    if (FILE* fh = std::fopen(txt.c_str(), "w")) {
+      std::fprintf(fh, "# Columns: #1 micrograph number; "
+                       "#2 - defocus 1 [A]; #3 - defocus 2; "
+                       "#4 - azimuth of astigmatism; "
+                       "#5 - additional phase shift [radian]; "
+                       "#6 - cross correlation; "
+                       "#7 - spacing (in Angstroms) up to which CTF rings were "
+                       "fit successfully\n");
+      std::fprintf(fh, " %9.2f  %9.2f  %7.2f  %7.2f  %9.5f  %8.4f\n", r.ctf[0], r.ctf[1], r.ctf[2], r.ctf[3],
+                   r.ctf[4], r.ctf[5]);
+      std::fclose(fh);
+    }
   }
   // ---- RELION star file (-OutStar; CGenStarFile, CGenStarFile.cpp:44-159):
   //      <OutMrc directory>/<movie name>.star, where the movie name is the

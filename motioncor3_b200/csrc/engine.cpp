@@ -899,6 +899,7 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
   // ---- 8. sums to real space (CCorrectFullShift::mUnpadSums,
   //      Correct/CCorrectFullShift.cpp:146-185): Fourier crop to the -FtBin
   //      output size, C2R, positivity, unpad ----
+  const float* sum0 = nullptr;  // first output sum, device
   {
     const int oW = g.outW, oH = g.outH;
     const int ocX = oW / 2 + 1;
@@ -928,6 +929,7 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
     }
     MC3_TRY(unpad_positive(reinterpret_cast<float*>(osum), 2 * ocX, dst, oW, oH, g.nSums,
                            (long)ocmp * 2, st));
+    sum0 = dst;
     if (out && out->sums && !out->sums_on_device)
       MC3_CUDA(cudaMemcpyAsync(out->sums, dst, sizeof(float) * opx * g.nSums, cudaMemcpyDeviceToHost, st));
   }
@@ -935,6 +937,19 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
   MC3_CUDA(cudaStreamSynchronize(st));
   float ms = 0.f;
   cudaEventElapsedTime(&ms, ev0, ev1);
+  // ---- 8b. CTF of the first sum, outside the timed region
+  //      (CCorrectFullShift::mEstimateCtf, Correct/CCorrectFullShift.cpp:129-144,179,
+  //      gated as CFindCtfMain::bEstimate, FindCtf/CFindCtfMain.cpp:26-40; pixel
+  //      size CInput::GetFinalPixelSize, CInput.cpp:709-715) ----
+  if (out) out->ctf_done = 0;
+  if (out && prm.cs > 0.001f && prm.kv != 0 && prm.pix_size != 0) {
+    const float pixf = prm.pix_size * prm.ft_bin / (prm.mag[0] > prm.mag[1] ? prm.mag[0] : prm.mag[1]);
+    const int cst = estimate_ctf(sum0, g.outW, g.outH, pixf, (float)prm.kv, prm.cs, prm.amp_cont,
+                                 prm.ext_phase, out->ctf, out->ctf_spectrum,
+                                 out->ctf_spectrum_on_device != 0, ctf, st);
+    if (cst == kOk) out->ctf_done = 1;
+    else if (cst != kEUnsupported) return cst;  // too small for a 512 x 512 tile: no estimate
+  }
   // ---- 9. result tables ----
   if (out) {
     out->n_sums = g.nSums;

@@ -41,6 +41,19 @@ struct Geometry {
   int compute(int w, int h, int n, const mc3_params& p, bool file_dose = false);
 };
 
+// Device scratch of the CTF estimate (ctf.cu), grown on demand.
+struct CtfScratch {
+  DevBuf img, spec, org, stats, tiles, half, full, rad, cand, res, band, ctf, out;
+};
+
+// CTF estimate of the device image d_img [ny][nx] (even sizes) as
+// FindCtf::CFindCtfMain::DoIt makes it: res6 = defocus max, min (A),
+// astigmatism azimuth (deg), extra phase (deg), score, fit resolution (A);
+// image512 (optional, host or device) = the 512 x 512 diagnostic spectrum.
+int estimate_ctf(const float* d_img, int nx, int ny, float pix, float kv, float cs, float ac,
+                 float ext_phase, float* res6, float* image512, bool image_on_device, CtfScratch& s,
+                 cudaStream_t st);
+
 class Engine {
  public:
   explicit Engine(const mc3_params& p);
@@ -117,6 +130,7 @@ class Engine {
   host::FmInt fmint_tab;
   DevBuf d_istart, d_isize;
   DevBuf d_dark;
+  CtfScratch ctf;
   bool has_dark = false;
   int dark_w = 0, dark_h = 0;
   bool has_gain = false;

@@ -17,6 +17,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_build", "libmc3_oracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libmc3ref_host.so")
+REF_CTF_LIB = os.path.join(HERE, "_ref", "libmc3ref_ctf.so")
 REF_TREE = "/root/reference"
 _VP = ctypes.c_void_p
 
@@ -29,7 +30,8 @@ def _cxx_env():
 
 
 def build() -> str:
-    srcs = [os.path.join(HERE, f) for f in ("mc3_oracle.cpp", "mc3_oracle.h", "Makefile")]
+    srcs = [os.path.join(HERE, f) for f in ("mc3_oracle.cpp", "mc3_oracle.h", "ctf_oracle.cpp",
+                                            "Makefile")]
     if not os.path.exists(LIB) or any(os.path.getmtime(s) > os.path.getmtime(LIB) for s in srcs):
         subprocess.run(["make", "-C", HERE], check=True, env=_cxx_env(), capture_output=True)
     return LIB
@@ -305,6 +307,66 @@ def patch_detect_bads(shifts, centers, nx, ny):
     bad = np.zeros(s.shape[:2], np.uint8)
     lib().oracle_patch_detect_bads(_p(s), _p(c), s.shape[0], s.shape[1], nx, ny, _p(bad))
     return bad
+
+
+def ctf_spectrum(img: np.ndarray, pix: float):
+    """(half spectrum [512][257], lowpassed full spectrum [512][512], pixel
+    size) the CTF is fitted to, or None when no 512 x 512 tile fits."""
+    im = np.ascontiguousarray(img, np.float32)
+    avg = np.zeros((512, 257), np.float32)
+    full = np.zeros((512, 512), np.float32)
+    pn = ctypes.c_float(0)
+    if lib().oracle_ctf_spectrum(_p(im), im.shape[1], im.shape[0], ctypes.c_float(pix), _p(avg),
+                                 _p(full), ctypes.byref(pn)):
+        return None
+    return avg, full, pn.value
+
+
+def ctf_search(avg: np.ndarray, pix_n: float, kv=300.0, cs=2.7, ac=0.07, ext_phase=0.0) -> np.ndarray:
+    a = np.ascontiguousarray(avg, np.float32)
+    res = np.zeros(6, np.float32)
+    f = ctypes.c_float
+    lib().oracle_ctf_search(_p(a), f(pix_n), f(kv), f(cs), f(ac), f(ext_phase), _p(res))
+    return res
+
+
+def find_ctf(img: np.ndarray, pix: float, kv=300.0, cs=2.7, ac=0.07, ext_phase=0.0):
+    """(res6, 512 x 512 diagnostic image) or None when no tile fits."""
+    im = np.ascontiguousarray(img, np.float32)
+    res = np.zeros(6, np.float32)
+    out = np.zeros((512, 512), np.float32)
+    f = ctypes.c_float
+    if lib().oracle_find_ctf(_p(im), im.shape[1], im.shape[0], f(pix), f(kv), f(cs), f(ac),
+                             f(ext_phase), _p(res), _p(out)):
+        return None
+    return res, out
+
+
+def ctf_param(kv: float, cs: float, ac: float, pix: float) -> np.ndarray:
+    out = np.zeros(3, np.float32)
+    f = ctypes.c_float
+    lib().oracle_ctf_param(f(kv), f(cs), f(ac), f(pix), _p(out))
+    return out
+
+
+def ctf_model(kv, cs, ac, pix, dfmin_px, dfmax_px, azim_rad, ext_rad) -> np.ndarray:
+    out = np.zeros((512, 257), np.float32)
+    f = ctypes.c_float
+    lib().oracle_ctf_model(f(kv), f(cs), f(ac), f(pix), f(dfmin_px), f(dfmax_px), f(azim_rad),
+                           f(ext_rad), _p(out))
+    return out
+
+
+def ref_ctf():
+    """The reference's CTF fitting drivers with host stand-ins for their
+    kernels (None when neither the tree nor the prebuilt checker exists)."""
+    build_ref_host()
+    if not os.path.exists(REF_CTF_LIB):
+        return None
+    L = ctypes.CDLL(REF_CTF_LIB)
+    L.ref_ctf_param.restype = None
+    L.ref_ctf_search.restype = None
+    return L
 
 
 def ref_host():

@@ -1,0 +1,84 @@
+"""CTF estimation on the corrected sum (FindCtf/, run by
+CCorrectFullShift::mEstimateCtf on the first sum): the oracle restatement
+pinned against the reference's own fitting drivers (CFindCtf2D,
+CFindDefocus1D/2D, CCtfParam compiled unmodified from the reference tree into
+oracle/_ref/libmc3ref_ctf.so, with host stand-ins for the kernels they call),
+and against CTFs planted in synthetic micrographs."""
+import ctypes
+
+import numpy as np
+import pytest
+
+
+@pytest.fixture(scope="module")
+def ref_ctf():
+    from oracle import oracle as O
+    L = O.ref_ctf()
+    if L is None:
+        pytest.skip("reference CTF checker not available")
+    return L
+
+
+def _f(v):
+    return ctypes.c_float(v)
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+@pytest.mark.parametrize("kv,cs,ac,pix", [(300, 2.7, 0.07, 1.25), (200, 2.0, 0.1, 1.6),
+                                          (300, 0.01, 0.0, 2.5)])
+def test_ctf_parameters_match_reference(oracle, ref_ctf, kv, cs, ac, pix):
+    """CCtfParam::Setup: wavelength and Cs in pixels, amplitude-contrast phase."""
+    ref = np.zeros(3, np.float32)
+    ref_ctf.ref_ctf_param(_f(kv), _f(cs), _f(ac), _f(pix), _ptr(ref))
+    assert np.array_equal(oracle.ctf_param(kv, cs, ac, pix), ref)
+
+
+@pytest.mark.parametrize("phase,ext", [(0.0, 0.0), (30.0, 30.0)])
+def test_search_matches_reference_drivers(oracle, ref_ctf, ctf_image, phase, ext):
+    """The 1D brute-force search, the 2D astigmatism / angle / defocus / phase
+    sweeps with their acceptance rules and the fit resolution give the
+    reference's numbers exactly on the same half spectrum (-ExtPhase 30
+    searches the extra phase in [0, 60] degrees)."""
+    img = ctf_image(n=1024, df=12000.0, ast=0.03, ang=-40.0, phase=phase, seed=5)
+    avg, _, pn = oracle.ctf_spectrum(img, 1.0)
+    ref = np.zeros(6, np.float32)
+    ref_ctf.ref_ctf_search(_ptr(np.ascontiguousarray(avg)), _f(pn), _f(300), _f(2.7), _f(0.07),
+                           _f(ext), _ptr(ref))
+    got = oracle.ctf_search(avg, pn, 300, 2.7, 0.07, ext)
+    assert np.array_equal(got, ref), (got, ref)
+    assert abs(0.5 * (ref[0] + ref[1]) - 12000.0) < 250.0
+    if ext:
+        assert abs(ref[3] - phase) < 6.0
+
+
+@pytest.mark.parametrize("pix,n", [(1.0, 2048), (1.6, 2048)])
+def test_oracle_recovers_planted_ctf(oracle, ctf_image, pix, n):
+    """Pixel size 1.0 A is Fourier-rescaled to 1.25 A before tiling
+    (CRescaleImage); 1.6 A is tiled as it is."""
+    img = ctf_image(n=n, pix=pix, df=15000.0, ast=0.02, ang=30.0, seed=1)
+    res, spec = oracle.find_ctf(img, pix)
+    dfmax, dfmin, ang, ph, score, resol = res
+    assert abs(dfmax - 15300.0) < 150.0 and abs(dfmin - 14700.0) < 150.0, res
+    assert abs(ang - 30.0) < 3.0, res
+    assert ph == 0.0 and score > 0.5 and resol < 10.0, res
+    assert spec.shape == (512, 512) and np.isfinite(spec).all()
+
+
+def test_spectrum_needs_a_tile(oracle, ctf_image):
+    img = ctf_image(n=400, pix=1.0)  # 320 px after rescaling: no 512 x 512 tile
+    assert oracle.ctf_spectrum(img, 1.0) is None
+    assert oracle.find_ctf(img, 1.0) is None
+
+
+def test_estimate_ctf_argument_checks(mc3lib):
+    from motioncor3_b200 import api
+    img = np.zeros((600, 600), np.float32)
+    res = np.zeros(6, np.float32)
+    rc = mc3lib.mc3_estimate_ctf(None, _ptr(img), 600, 600, 0, 1.0, 300.0, 2.7, 0.07, 0.0,
+                                 _ptr(res), None)
+    assert rc == api.MC3_EINVAL
+    d = api.Params()
+    assert d.cs == 0.0 and d.amp_cont == 0.07  # the library does not estimate unless asked

@@ -36,7 +36,7 @@ def _read_log(path):
     return np.array(rows)
 
 
-def run_program(binary, workdir, movie, gain, tags, extra=(), four_bit=False, dark=None):
+def run_program(binary, workdir, movie, gain, tags, extra=(), four_bit=False, dark=None, cs="0"):
     from motioncor3_b200 import mrcio
     os.makedirs(workdir, exist_ok=True)
     mv = os.path.join(workdir, "movie.mrc")
@@ -46,7 +46,7 @@ def run_program(binary, workdir, movie, gain, tags, extra=(), four_bit=False, da
         mrcio.write(dp, dark.astype(np.float32))
         extra = list(extra) + ["-Dark", dp]
     args = [binary, "-InMrc", mv, "-OutMrc", os.path.join(workdir, "sum.mrc"), "-LogDir",
-            workdir + "/", "-OutAln", workdir, "-Gpu", "0", "-Cs", "0"] + tags + list(extra)
+            workdir + "/", "-OutAln", workdir, "-Gpu", "0", "-Cs", cs] + tags + list(extra)
     if gain is not None:
         gp = os.path.join(workdir, "gain.mrc")
         mrcio.write(gp, gain.astype(np.float32))
