@@ -15,8 +15,12 @@
 //   * CGenAvgSpectrum::mLowpass (FindCtf/CGenAvgSpectrum.cpp:177-185) copies
 //     the x = Nyquist column from the padding column of the in-place C2R
 //     output; the periodic value (column 0 of the full spectrum) is used.
-// CFindDefocus2D::mIterate's first two correlations use m_fExtPhase before it
-// is set (FindCtf/CFindDefocus2D.cpp:134-141); 0 is used.
+// GRadialAvg (FindCtf/GRadialAvg.cu:11-31) reads row 512, past the half
+// spectrum, for the last angles of radius 256; the index is clamped (that
+// radius lies outside every correlation band).  CFindDefocus2D::mIterate's
+// first two correlations use m_fExtPhase before it is set
+// (FindCtf/CFindDefocus2D.cpp:134-141); 0 is used.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <functional>
@@ -297,8 +301,10 @@ void radial_average(const std::vector<float>& s, std::vector<float>& avg) {
     const float step = 180.0f / n;
     for (int i = 0; i < n; ++i) {
       const float rad = (-90.0f + i * step) * 0.017453f;
-      const int x = (int)(r * std::cos(rad) + 0.5f);
-      const int y = (int)(r * std::sin(rad) + kTile / 2 + 0.5f);
+      int x = (int)(r * std::cos(rad) + 0.5f);
+      int y = (int)(r * std::sin(rad) + kTile / 2 + 0.5f);
+      x = std::min(std::max(x, 0), kCmpX - 1);  // r = 256 reaches row 512 near 90 degrees
+      y = std::min(std::max(y, 0), kTile - 1);
       sum += s[(size_t)y * kCmpX + x];
     }
     avg[r] = sum / n;
@@ -786,6 +792,27 @@ int oracle_ctf_spectrum(const float* img, int nx, int ny, float pix, float* avg_
   lowpass(bg, full);
   std::memcpy(avg_out, bg.data(), sizeof(float) * bg.size());
   if (full_out) std::memcpy(full_out, full.data(), sizeof(float) * full.size());
+  *pix_n = s.pixN;
+  return 0;
+}
+
+// The stages of oracle_ctf_spectrum: the averaged amplitude spectrum before
+// (raw) and after (bg) background removal, the lowpassed half spectrum and
+// full spectrum.  Returns 0, or 1 when no tile fits.
+int oracle_ctf_stages(const float* img, int nx, int ny, float pix, float* raw_out, float* bg_out,
+                      float* half_out, float* full_out, float* pix_n) {
+  Spectrum s;
+  int pitch = 0;
+  std::vector<float> r = rescale(img, nx, ny, pix, s, &pitch);
+  std::vector<float> raw, bg;
+  if (!average_spectrum(r, pitch, s.imgN[0], s.imgN[1], raw)) return 1;
+  remove_background(raw, bg);
+  std::memcpy(raw_out, raw.data(), sizeof(float) * raw.size());
+  std::memcpy(bg_out, bg.data(), sizeof(float) * bg.size());
+  std::vector<float> full;
+  lowpass(bg, full);
+  std::memcpy(half_out, bg.data(), sizeof(float) * bg.size());
+  std::memcpy(full_out, full.data(), sizeof(float) * full.size());
   *pix_n = s.pixN;
   return 0;
 }

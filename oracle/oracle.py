@@ -322,6 +322,20 @@ def ctf_spectrum(img: np.ndarray, pix: float):
     return avg, full, pn.value
 
 
+def ctf_stages(img: np.ndarray, pix: float):
+    """dict(raw, bg, half, full, pix_n) of the spectrum stages, or None."""
+    im = np.ascontiguousarray(img, np.float32)
+    raw = np.zeros((512, 257), np.float32)
+    bg = np.zeros((512, 257), np.float32)
+    half = np.zeros((512, 257), np.float32)
+    full = np.zeros((512, 512), np.float32)
+    pn = ctypes.c_float(0)
+    if lib().oracle_ctf_stages(_p(im), im.shape[1], im.shape[0], ctypes.c_float(pix), _p(raw), _p(bg),
+                               _p(half), _p(full), ctypes.byref(pn)):
+        return None
+    return dict(raw=raw, bg=bg, half=half, full=full, pix_n=pn.value)
+
+
 def ctf_search(avg: np.ndarray, pix_n: float, kv=300.0, cs=2.7, ac=0.07, ext_phase=0.0) -> np.ndarray:
     a = np.ascontiguousarray(avg, np.float32)
     res = np.zeros(6, np.float32)

@@ -54,8 +54,10 @@ void GRadialAvg::DoIt(float* s, float* avg, int* cmp) {
     const float step = 180.0f / n;
     for (int i = 0; i < n; ++i) {
       const float rad = (-90.0f + i * step) * 0.017453f;
-      const int x = (int)(r * cosf(rad) + 0.5f);
-      const int y = (int)(r * sinf(rad) + cmp[1] / 2 + 0.5f);
+      int x = (int)(r * cosf(rad) + 0.5f);
+      int y = (int)(r * sinf(rad) + cmp[1] / 2 + 0.5f);
+      if (y > cmp[1] - 1) y = cmp[1] - 1;  // the kernel reads past the spectrum at r = 256
+      if (x > cmp[0] - 1) x = cmp[0] - 1;
       sum += s[y * cmp[0] + x];
     }
     avg[r] = sum / n;

@@ -36,22 +36,94 @@ def test_ctf_parameters_match_reference(oracle, ref_ctf, kv, cs, ac, pix):
     assert np.array_equal(oracle.ctf_param(kv, cs, ac, pix), ref)
 
 
+_REF_FITS = {}
+
+
+def _ref_fit(oracle, ref_ctf, ctf_image, phase, ext):
+    """(half spectrum, pixel size, the reference drivers' res6), computed once."""
+    if (phase, ext) not in _REF_FITS:
+        img = ctf_image(n=1024, df=12000.0, ast=0.03, ang=-40.0, phase=phase, seed=5)
+        avg, _, pn = oracle.ctf_spectrum(img, 1.0)
+        ref = np.zeros(6, np.float32)
+        ref_ctf.ref_ctf_search(_ptr(np.ascontiguousarray(avg)), _f(pn), _f(300), _f(2.7), _f(0.07),
+                               _f(ext), _ptr(ref))
+        _REF_FITS[(phase, ext)] = (avg, pn, ref)
+    return _REF_FITS[(phase, ext)]
+
+
 @pytest.mark.parametrize("phase,ext", [(0.0, 0.0), (30.0, 30.0)])
 def test_search_matches_reference_drivers(oracle, ref_ctf, ctf_image, phase, ext):
     """The 1D brute-force search, the 2D astigmatism / angle / defocus / phase
     sweeps with their acceptance rules and the fit resolution give the
     reference's numbers exactly on the same half spectrum (-ExtPhase 30
     searches the extra phase in [0, 60] degrees)."""
-    img = ctf_image(n=1024, df=12000.0, ast=0.03, ang=-40.0, phase=phase, seed=5)
-    avg, _, pn = oracle.ctf_spectrum(img, 1.0)
-    ref = np.zeros(6, np.float32)
-    ref_ctf.ref_ctf_search(_ptr(np.ascontiguousarray(avg)), _f(pn), _f(300), _f(2.7), _f(0.07),
-                           _f(ext), _ptr(ref))
+    avg, pn, ref = _ref_fit(oracle, ref_ctf, ctf_image, phase, ext)
     got = oracle.ctf_search(avg, pn, 300, 2.7, 0.07, ext)
     assert np.array_equal(got, ref), (got, ref)
     assert abs(0.5 * (ref[0] + ref[1]) - 12000.0) < 250.0
     if ext:
         assert abs(ref[3] - phase) < 6.0
+
+
+@pytest.mark.parametrize("phase,ext", [(0.0, 0.0), (30.0, 30.0)])
+def test_device_search_logic_matches_reference_drivers(oracle, ref_ctf, ctf_shim, ctf_image, phase, ext):
+    """The device path's search driver and per-candidate expressions
+    (csrc/ctf_core.h: ctf::Search, ctf1d_term, ctf2d_term, make_band,
+    fit_shell), run on the host with a sequential scorer, give the
+    reference's numbers exactly."""
+    avg, pn, ref = _ref_fit(oracle, ref_ctf, ctf_image, phase, ext)
+    res, fit = np.zeros(6, np.float32), np.zeros(4, np.float32)
+    assert ctf_shim.shim_ctf_search(_ptr(np.ascontiguousarray(avg)), _f(pn), _f(300), _f(2.7), _f(0.07),
+                                    _f(ext), _ptr(res), _ptr(fit)) == 0
+    assert np.array_equal(res, ref), (res, ref)
+
+
+def test_device_spectrum_maps_match_oracle(oracle, ctf_shim, ctf_image):
+    """The index maps of the device kernels (csrc/ctf_core.h) on the oracle's
+    intermediate spectra: background removal (exact), the full spectrum,
+    lowpass factors and copy-back (with numpy's FFT between them), the radial
+    average and the diagnostic image."""
+    img = ctf_image(n=2048, pix=1.0, df=15000.0, ast=0.02, ang=30.0, seed=1)
+    st = oracle.ctf_stages(img, 1.0)
+    bg = np.zeros((512, 257), np.float32)
+    ctf_shim.shim_ctf_remove_background(_ptr(st["raw"]), _ptr(bg))
+    assert np.array_equal(bg, st["bg"])
+    full = np.zeros((512, 514), np.float32)
+    ctf_shim.shim_ctf_full(_ptr(bg), _ptr(full))
+    assert not full[:, 512:].any()
+    lp = np.zeros((512, 257), np.float32)
+    ctf_shim.shim_ctf_lowpass_factors(_ptr(lp))
+    spec = np.fft.rfft2(full[:, :512].astype(np.float64)) / (512 * 512) * lp
+    low = np.zeros((512, 514), np.float32)
+    low[:, :512] = np.fft.irfft2(spec, s=(512, 512)) * (512 * 512)
+    assert np.abs(low[:, :512] - st["full"]).max() <= 1e-5 * np.abs(st["full"]).max()
+    half = np.zeros((512, 257), np.float32)
+    ctf_shim.shim_ctf_take_half(_ptr(low), _ptr(half))
+    assert np.abs(half - st["half"]).max() <= 1e-5 * np.abs(st["half"]).max()
+    rad = np.zeros(257, np.float32)
+    ctf_shim.shim_ctf_radial(_ptr(st["half"]), _ptr(rad))
+    ref_rad = np.zeros(257)
+    f32 = np.float32
+    for r in range(257):  # GRadialAvg restated in numpy with its FP32 expressions
+        n = min(max(int(f32(3.1415926) * f32(r) + f32(0.5)), 1), 180)
+        a = (f32(-90.0) + np.arange(n, dtype=f32) * f32(f32(180.0) / f32(n))) * f32(0.017453)
+        x = np.minimum((f32(r) * np.cos(a) + f32(0.5)).astype(int), 256)
+        y = np.minimum((f32(r) * np.sin(a) + f32(256.5)).astype(int), 511)
+        ref_rad[r] = st["half"][y, x].mean()
+    # an index can flip where float32 cos/sin differ by an ulp at a .5 boundary
+    same = np.abs(rad - ref_rad) <= 1e-5 * np.abs(ref_rad).max()
+    assert same.mean() >= 0.97, np.flatnonzero(~same)
+    res, fit = np.zeros(6, np.float32), np.zeros(4, np.float32)
+    ctf_shim.shim_ctf_search(_ptr(st["half"]), _f(st["pix_n"]), _f(300), _f(2.7), _f(0.07), _f(0),
+                             _ptr(res), _ptr(fit))
+    ores, oimg = oracle.find_ctf(img, 1.0)
+    assert np.array_equal(res, ores)
+    out = np.zeros((512, 512), np.float32)
+    fl = np.zeros((512, 514), np.float32)
+    fl[:, :512] = st["full"]
+    ctf_shim.shim_ctf_image(_ptr(fl), _ptr(st["half"]), _f(st["pix_n"]), _f(300), _f(2.7), _f(0.07),
+                            _ptr(fit), _ptr(out))
+    assert np.abs(out - oimg).max() <= 1e-5 * np.abs(oimg).max()
 
 
 @pytest.mark.parametrize("pix,n", [(1.0, 2048), (1.6, 2048)])
