@@ -319,18 +319,17 @@ int estimate_ctf(const float* d_img, int nx, int ny, float pix, float kv, float 
   if (!d_img || !res6 || nx < 2 || ny < 2 || pix <= 0) return kEInval;
   if ((nx | ny) & 1) return kEUnsupported;  // the FFT passes take even sizes
   // ---- CRescaleImage::DoIt (FindCtf/CRescaleImage.cpp:28-68) ----
-  float bin = 1.25f / pix;
-  if (bin <= 1) bin = 1.0f;
-  const float pixN = pix * bin;
-  const int nxN = (int)(nx / bin + 0.5f) / 2 * 2, nyN = (int)(ny / bin + 0.5f) / 2 * 2;
+  int nxN, nyN;
+  float pixN, bin;
+  rescaled_size(nx, ny, pix, &nxN, &nyN, &pixN, &bin);
   const int pitch = (nxN / 2 + 1) * 2, cN = nxN / 2 + 1;
-  // ---- tile grid (CGenAvgSpectrum::SetSizes, FindCtf/CGenAvgSpectrum.cpp:38-63) ----
-  const int overlap = (int)(kTile * 0.50f) / 2 * 2, step = kTile - overlap;
-  const int ntx = (nxN - overlap) / step, nty = (nyN - overlap) / step;
+  // ---- tile grid (CGenAvgSpectrum::SetSizes) ----
+  int nt[2], off[2], step;
+  tile_grid(nxN, nyN, nt, off, &step);
+  const int ntx = nt[0], nty = nt[1];
   if (ntx < 1 || nty < 1) return kEUnsupported;  // no 512 x 512 tile
   const int ntiles = ntx * nty;
-  const int offx = (nxN - ntx * kTile + (ntx - 1) * overlap) / 2;
-  const int offy = (nyN - nty * kTile + (nty - 1) * overlap) / 2;
+  const int offx = off[0], offy = off[1];
   MC3_TRY(s.img.ensure(sizeof(float) * pitch * (size_t)nyN));
   float* img = s.img.as<float>();
   if (bin == 1) {

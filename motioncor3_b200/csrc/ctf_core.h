@@ -28,6 +28,30 @@ constexpr int kNH = kCX * kTile;     // half-spectrum pixels
 constexpr float kD2R = 0.01745329f;  // FindCtf/CCtfTheory.cpp:8, CFindDefocus2D.cpp:13
 constexpr float kD2R1 = 0.0174533f;  // FindCtf/CFindDefocus1D.cpp:12
 
+// ---- geometry -----------------------------------------------------------------
+
+// CRescaleImage::DoIt (FindCtf/CRescaleImage.cpp:28-68): the binning that
+// brings the pixel size to >= 1.25 A and the even rescaled size.
+MC3_HD void rescaled_size(int nx, int ny, float pix, int* nxN, int* nyN, float* pixN, float* bin) {
+  float b = 1.25f / pix;
+  if (b <= 1) b = 1.0f;
+  *bin = b;
+  *pixN = pix * b;
+  *nxN = (int)(nx / b + 0.5f) / 2 * 2;
+  *nyN = (int)(ny / b + 0.5f) / 2 * 2;
+}
+
+// CGenAvgSpectrum::SetSizes (FindCtf/CGenAvgSpectrum.cpp:38-63): tiles per
+// axis, first-tile offsets and the tile step (50 % overlap).
+MC3_HD void tile_grid(int nx, int ny, int* nt, int* off, int* step) {
+  const int overlap = (int)(kTile * 0.50f) / 2 * 2;
+  *step = kTile - overlap;
+  nt[0] = (nx - overlap) / *step;
+  nt[1] = (ny - overlap) / *step;
+  off[0] = (nx - nt[0] * kTile + (nt[0] - 1) * overlap) / 2;
+  off[1] = (ny - nt[1] * kTile + (nt[1] - 1) * overlap) / 2;
+}
+
 // ---- spectrum stages ------------------------------------------------------
 
 // GRoundEdge factor at tile pixel (x, y) (Util/GRoundEdge.cu:8-23 with the

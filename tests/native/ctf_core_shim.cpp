@@ -118,6 +118,33 @@ int shim_ctf_search(const float* half, float pix, float kv, float cs, float ac, 
   return 0;
 }
 
+// Rescaled size and tile grid: out7 = (nxN, nyN, ntx, nty, offx, offy, step);
+// pixN.
+void shim_ctf_geometry(int nx, int ny, float pix, int* out7, float* pix_n) {
+  float bin;
+  rescaled_size(nx, ny, pix, &out7[0], &out7[1], pix_n, &bin);
+  tile_grid(out7[0], out7[1], &out7[2], &out7[4], &out7[6]);
+}
+
+// k_ctf_tile_stats + k_ctf_tile_prep for one tile at (sx, sy) of a padded
+// image: the normalised, edge-rounded tile [512][514].
+void shim_ctf_tile(const float* img, int pitch, int sx, int sy, float* tile) {
+  double a = 0, b = 0;
+  for (int i = 0; i < kTile * kTile; ++i) {
+    const float v = img[(long)(sy + i / kTile) * pitch + sx + (i % kTile)];
+    a += v;
+    b += (double)v * v;
+  }
+  float mean, sd;
+  tile_norm(a, b, &mean, &sd);
+  for (int y = 0; y < kTile; ++y)
+    for (int x = 0; x < kTP; ++x) {
+      const float w = x < kTile ? tile_edge(x, y) : 0.0f;
+      const float* src = img + (long)(sy + y) * pitch + sx;
+      tile[y * kTP + x] = w == 0.0f ? 0.0f : ((src[x] - mean) / sd) * w;
+    }
+}
+
 void shim_ctf_remove_background(const float* raw, float* out) {
   std::vector<float> sq(kNH);
   for (int i = 0; i < kNH; ++i) sq[i] = sqrtf(raw[i]);

@@ -126,6 +126,40 @@ def test_device_spectrum_maps_match_oracle(oracle, ctf_shim, ctf_image):
     assert np.abs(out - oimg).max() <= 1e-5 * np.abs(oimg).max()
 
 
+@pytest.mark.parametrize("pix,nx,ny", [(1.6, 1300, 1100), (1.0, 1280, 1600)])
+def test_device_tile_stage_matches_oracle(oracle, ctf_shim, ctf_image, pix, nx, ny):
+    """The device path's rescaled size, tile grid and tile preparation
+    (csrc/ctf_core.h) with numpy standing in for the FFTs reproduce the
+    oracle's averaged amplitude spectrum (CGenAvgSpectrum::mAverage)."""
+    img = ctf_image(n=nx, ny=ny, pix=pix, seed=9)
+    g = np.zeros(7, np.int32)
+    pn = ctypes.c_float(0)
+    ctf_shim.shim_ctf_geometry(nx, ny, _f(pix), _ptr(g), ctypes.byref(pn))
+    nxN, nyN, ntx, nty, offx, offy, step = (int(v) for v in g)
+    st = oracle.ctf_stages(img, pix)
+    assert abs(pn.value - st["pix_n"]) == 0.0
+    pitch = (nxN // 2 + 1) * 2
+    if nxN == nx and nyN == ny:
+        scaled = img.astype(np.float64)
+    else:  # Fourier crop (GFourierResize2D) between a normalised R2C and a C2R
+        F = np.fft.rfft2(img.astype(np.float64)) / (nx * ny)
+        keep = np.r_[0:nyN // 2 + 1, ny - nyN // 2 + 1:ny]
+        C = F[keep][:, :nxN // 2 + 1]
+        scaled = np.fft.irfft2(C, s=(nyN, nxN)) * (nxN * nyN)
+    pad = np.zeros((nyN, pitch), np.float32)
+    pad[:, :nxN] = scaled
+    acc = np.zeros((512, 257), np.float32)
+    fac = np.float32(1.0 / (ntx * nty))
+    tile = np.zeros((512, 514), np.float32)
+    for t in range(ntx * nty):
+        sx, sy = offx + (t % ntx) * step, offy + (t // ntx) * step
+        ctf_shim.shim_ctf_tile(_ptr(pad), pitch, sx, sy, _ptr(tile))
+        assert not tile[:, 512:].any()
+        amp = np.abs(np.fft.rfft2(tile[:, :512].astype(np.float64))).astype(np.float32)
+        acc = acc + np.roll(amp, 256, axis=0) * fac
+    assert np.abs(acc - st["raw"]).max() <= 1e-4 * np.abs(st["raw"]).max()
+
+
 @pytest.mark.parametrize("pix,n", [(1.0, 2048), (1.6, 2048)])
 def test_oracle_recovers_planted_ctf(oracle, ctf_image, pix, n):
     """Pixel size 1.0 A is Fourier-rescaled to 1.25 A before tiling
