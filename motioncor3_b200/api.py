@@ -485,8 +485,10 @@ class MotionCor3:
             ox, oy = info["out_size"]
             stack = np.zeros((nz, oy, ox), np.float32)
             r.stack = stack.ctypes.data
-        ctf_img = np.zeros((512, 512), np.float32)
-        r.ctf_spectrum = ctf_img.ctypes.data
+        ctf_img = None
+        if float(self.params.cs) > 0.001 and self.params.kv and self.params.pix_size:
+            ctf_img = np.zeros((512, 512), np.float32)  # CFindCtfMain::bEstimate
+            r.ctf_spectrum = ctf_img.ctypes.data
         _check(_lib().mc3_process_movie(self._h, ctypes.byref(mv), ctypes.byref(r)),
                "mc3_process_movie")
         if stack is not None:
