@@ -31,7 +31,7 @@ def _cxx_env():
 
 def build() -> str:
     srcs = [os.path.join(HERE, f) for f in ("mc3_oracle.cpp", "mc3_oracle.h", "ctf_oracle.cpp",
-                                            "Makefile")]
+                                            "cnn_oracle.cpp", "Makefile")]
     if not os.path.exists(LIB) or any(os.path.getmtime(s) > os.path.getmtime(LIB) for s in srcs):
         subprocess.run(["make", "-C", HERE], check=True, env=_cxx_env(), capture_output=True)
     return LIB
@@ -369,6 +369,51 @@ def ctf_model(kv, cs, ac, pix, dfmin_px, dfmax_px, azim_rad, ext_rad) -> np.ndar
     lib().oracle_ctf_model(f(kv), f(cs), f(ac), f(pix), f(dfmin_px), f(dfmax_px), f(azim_rad),
                            f(ext_rad), _p(out))
     return out
+
+
+class ShiftNet:
+    """FP64 oracle of the shift-proposal network (cnn_oracle.cpp): strided
+    convolutions + ReLU, global average pool, linear head."""
+
+    def __init__(self, layers, nout: int, seed: int = 0):
+        L = lib()
+        L.cnn_create.restype = _VP
+        L.cnn_num_params.restype = ctypes.c_long
+        L.cnn_loss_grad.restype = ctypes.c_double
+        spec = np.ascontiguousarray(np.array(layers, np.int32).ravel())
+        self._L = L
+        self._h = _VP(L.cnn_create(len(layers), _p(spec), nout, ctypes.c_uint(seed)))
+        self.nout = nout
+        self.cin = int(layers[0][0])
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._L.cnn_destroy(self._h)
+            self._h = None
+
+    @property
+    def n_params(self) -> int:
+        return int(self._L.cnn_num_params(self._h))
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(self.n_params)
+        self._L.cnn_get_params(self._h, _p(out))
+        return out
+
+    def set_params(self, p: np.ndarray) -> None:
+        self._L.cnn_set_params(self._h, _p(np.ascontiguousarray(p, np.float64)))
+
+    def forward(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float64)
+        out = np.zeros(self.nout)
+        self._L.cnn_loss_grad(self._h, _p(x), *x.shape, None, None, _p(out))
+        return out
+
+    def loss_grad(self, x: np.ndarray, target: np.ndarray, grad: np.ndarray) -> float:
+        """Loss 0.5 |f(x) - target|^2; its gradient is ADDED to grad."""
+        x = np.ascontiguousarray(x, np.float64)
+        t = np.ascontiguousarray(target, np.float64)
+        return float(self._L.cnn_loss_grad(self._h, _p(x), *x.shape, _p(t), _p(grad), None))
 
 
 def ref_ctf():
