@@ -602,8 +602,11 @@ struct AlignResult {
   int iterations;
 };
 
+// init (may be NULL): a first iterate of the per-frame shifts (the learned
+// proposal's warm start); the group totals start at their frames' mean.
 AlignResult iterative_align(const cd* spec, int cmpX, int cmpY, int N, const Groups& G,
-                            int maxIter, float tol, float bfactor, bool phaseOnly) {
+                            int maxIter, float tol, float bfactor, bool phaseOnly,
+                            const float* init = nullptr) {
   const long n = (long)cmpX * cmpY;
   const int nG = (int)G.start.size();
   const int imgX = (cmpX - 1) * 2;
@@ -615,6 +618,21 @@ AlignResult iterative_align(const cd* spec, int cmpX, int cmpY, int N, const Gro
   int iters = 0;
   std::vector<cd> sum(n), gsum(n);
   std::vector<float> win(seaX * seaY);
+  if (init) {
+    for (int f = 0; f < N; ++f) {
+      tmp.x(f) = init[2 * f];
+      tmp.y(f) = init[2 * f + 1];
+    }
+    for (int g = 0; g < nG; ++g) {
+      double sx = 0, sy = 0;
+      for (int i = 0; i < G.size[g]; ++i) {
+        sx += init[2 * (G.start[g] + i)];
+        sy += init[2 * (G.start[g] + i) + 1];
+      }
+      total.x(g) = (float)(sx / G.size[g]);
+      total.y(g) = (float)(sy / G.size[g]);
+    }
+  }
   for (int it = 0; it < maxIter; ++it) {
     // CAlignedSum: sum of all frames shifted by -tmp
     std::fill(sum.begin(), sum.end(), cd(0.0));
@@ -1131,9 +1149,17 @@ void oracle_local_gather(const double* in, double* out, int W, int H, const floa
 
 int oracle_iterative_align(const double* spec, int cmpX, int cmpY, int N, int group_size,
                            int max_iter, float tol, float bfactor, int phase_only, float* shifts) {
+  return oracle_iterative_align_warm(spec, cmpX, cmpY, N, group_size, max_iter, tol, bfactor,
+                                     phase_only, nullptr, shifts);
+}
+
+// The same with a first iterate init[N][2] (NULL: start from zero).
+int oracle_iterative_align_warm(const double* spec, int cmpX, int cmpY, int N, int group_size,
+                                int max_iter, float tol, float bfactor, int phase_only,
+                                const float* init, float* shifts) {
   Groups G = make_groups(N, group_size);
   AlignResult r = iterative_align(reinterpret_cast<const cd*>(spec), cmpX, cmpY, N, G, max_iter,
-                                  tol, bfactor, phase_only != 0);
+                                  tol, bfactor, phase_only != 0, init);
   for (int i = 0; i < N; ++i) {
     shifts[2 * i] = r.shifts.v[i];
     shifts[2 * i + 1] = r.shifts.v[N + i];

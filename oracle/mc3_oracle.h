@@ -128,6 +128,10 @@ void oracle_local_gather(const double* in, double* out, int W, int H, const floa
 int oracle_iterative_align(const double* spec, int cmpX, int cmpY, int N, int group_size,
                            int max_iter, float tol, float bfactor, int phase_only,
                            float* shifts);
+/* oracle_iterative_align with a first iterate init[N][2] (NULL: from zero). */
+int oracle_iterative_align_warm(const double* spec, int cmpX, int cmpY, int N, int group_size,
+                                int max_iter, float tol, float bfactor, int phase_only,
+                                const float* init, float* shifts);
 
 #ifdef __cplusplus
 }

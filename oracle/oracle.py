@@ -254,12 +254,14 @@ def peak2d(win: np.ndarray) -> np.ndarray:
 
 
 def iterative_align(spec: np.ndarray, group: int, max_iter: int, tol: float, bfactor: float,
-                    phase_only: int = 0):
+                    phase_only: int = 0, init=None):
+    """init: optional first iterate [n][2] of the per-frame shifts (warm start)."""
     n, cy, cx = spec.shape
     s = np.ascontiguousarray(spec, np.complex128)
     out = np.zeros((n, 2), np.float32)
-    it = lib().oracle_iterative_align(_p(s), cx, cy, n, group, max_iter, ctypes.c_float(tol),
-                                      ctypes.c_float(bfactor), phase_only, _p(out))
+    ini = None if init is None else np.ascontiguousarray(init, np.float32)
+    it = lib().oracle_iterative_align_warm(_p(s), cx, cy, n, group, max_iter, ctypes.c_float(tol),
+                                           ctypes.c_float(bfactor), phase_only, _p(ini), _p(out))
     return out, it
 
 
