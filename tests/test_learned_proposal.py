@@ -80,10 +80,10 @@ def test_network_learns_frame_pair_shifts(oracle):
 @pytest.mark.parametrize("seed", [21, 24])
 def test_warm_start_keeps_the_cold_result(oracle, seed):
     """The aligner started from a first iterate (the proposal's role) ends
-    at the cold-start shifts within 0.05 px and never needs more iterations;
-    from the converged shifts it stops after the minimum of two.  On these
-    small-drift movies the cold start itself needs only three, so the gain
-    a proposal can bring here is one iteration."""
+    at the cold-start shifts within 0.05 px and never needs more iterations
+    (at least two always run).  On these small-drift movies the cold start
+    itself needs only three, so the gain a proposal can bring here is at most
+    one iteration."""
     from motioncor3_b200 import synthetic as S
     m = S.make_movie(256, 256, 14, dose=5.0, seed=seed)
     spec = np.stack([oracle.rfft2(f.astype(np.float64)) for f in m.frames])
