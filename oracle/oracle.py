@@ -418,6 +418,39 @@ class ShiftNet:
         return float(self._L.cnn_loss_grad(self._h, _p(x), *x.shape, _p(t), _p(grad), None))
 
 
+def bf16(x: np.ndarray) -> np.ndarray:
+    """Round float32 values to bfloat16 (nearest, ties to even), kept as float32."""
+    u = np.ascontiguousarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000).astype(np.uint32)
+    return r.view(np.float32)
+
+
+def split_bf16_matmul(a: np.ndarray, b: np.ndarray, products: int = 3) -> np.ndarray:
+    """a @ b as the tensor-core form computes it: each FP32 operand split into
+    BF16 hi + lo, products hi*hi + hi*lo + lo*hi (products=3) or hi*hi alone
+    (products=1), each exact in FP32 and accumulated in FP32."""
+    a = np.asarray(a, np.float32)
+    b = np.asarray(b, np.float32)
+    ah, bh = bf16(a), bf16(b)
+    out = (ah @ bh).astype(np.float32)
+    if products == 3:
+        al, bl = bf16(a - ah), bf16(b - bh)
+        out = out + (ah @ bl).astype(np.float32) + (al @ bh).astype(np.float32)
+    return out
+
+
+def split_bf16_dft(x: np.ndarray, products: int = 3) -> np.ndarray:
+    """Complex DFT along axis 0 of x [n][m] as four real split-BF16 GEMMs with
+    the FP32 DFT matrix (the form (1) transform of the patch stacks)."""
+    n = x.shape[0]
+    k = np.arange(n)
+    w = np.exp(-2j * np.pi * np.outer(k, k) / n)
+    wr, wi = w.real.astype(np.float32), w.imag.astype(np.float32)
+    xr, xi = x.real.astype(np.float32), x.imag.astype(np.float32)
+    mm = lambda a, b: split_bf16_matmul(a, b, products)
+    return (mm(wr, xr) - mm(wi, xi)) + 1j * (mm(wr, xi) + mm(wi, xr))
+
+
 def ref_ctf():
     """The reference's CTF fitting drivers with host stand-ins for their
     kernels (None when neither the tree nor the prebuilt checker exists)."""
