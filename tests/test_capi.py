@@ -246,3 +246,22 @@ def test_create_without_a_gpu_fails_cleanly(mc3lib):
     h = ctypes.c_void_p()
     rc = api._lib().mc3_create(ctypes.byref(p), ctypes.byref(h))
     assert rc != api.MC3_OK and not h.value
+
+
+def test_cli_ctf_gate(mc3lib, tmp_path):
+    """-Cs defaults to the reference's 2.7 on the command line; with -Cs 0 (or
+    no -PixSize) the reference's 'Skip CTF estimation' notice is printed
+    (CFindCtfMain::bEstimate).  Runs before any GPU work: the movie does not
+    exist."""
+    import subprocess
+    from motioncor3_b200 import build
+    exe = build.CLI
+    base = [exe, "-InMrc", str(tmp_path / "none.mrc"), "-OutMrc", str(tmp_path / "o.mrc")]
+    off = subprocess.run(base + ["-PixSize", "1", "-Cs", "0"], capture_output=True, text=True, timeout=60)
+    assert "Skip CTF estimation" in off.stdout and "Cs value:     0.000000" in off.stdout
+    on = subprocess.run(base + ["-PixSize", "1", "-AmpCont", "0.1", "-ExtPhase", "20"],
+                        capture_output=True, text=True, timeout=60)
+    assert "Skip CTF estimation" not in on.stdout
+    assert "outside the implemented path" not in on.stderr  # the CTF tags are parsed
+    nopix = subprocess.run(base, capture_output=True, text=True, timeout=60)
+    assert "Pixel size:   0.000000" in nopix.stdout
