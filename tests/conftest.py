@@ -96,24 +96,27 @@ def rng():
     return np.random.default_rng(1234)
 
 
-@pytest.fixture(scope="session")
-def ctf_image():
-    """Factory of a seeded micrograph whose power spectrum carries a known
-    CTF: white noise filtered by |CTF| (CCtfTheory convention: defocus
+def make_ctf_image(n=2048, pix=1.0, df=15000.0, ast=0.02, ang=30.0, kv=300.0, cs=2.7, ac=0.07,
+                   phase=0.0, seed=0, ny=None):
+    """A seeded micrograph whose power spectrum carries a known CTF: white
+    noise filtered by |CTF| (CCtfTheory convention: defocus
     df_mean (1 + ast cos 2(theta - angle)), angle in degrees) under a
     Gaussian envelope, plus an offset."""
-    def make(n=2048, pix=1.0, df=15000.0, ast=0.02, ang=30.0, kv=300.0, cs=2.7, ac=0.07,
-             phase=0.0, seed=0, ny=None):
-        ny = ny or n
-        rng = np.random.default_rng(seed)
-        ky = np.fft.fftfreq(ny)[:, None]
-        kx = np.fft.fftfreq(n)[None, :]
-        s2 = (kx ** 2 + ky ** 2) / pix ** 2
-        th = np.arctan2(ky, kx + 1e-30)
-        lam = 12.26 / np.sqrt(kv * 1000 + 0.9784 * kv * kv)
-        dfa = df + df * ast * np.cos(2 * (th - np.deg2rad(ang)))
-        chi = (np.pi * lam * s2 * (dfa - 0.5 * lam ** 2 * s2 * cs * 1e7)
-               + np.arctan(ac / np.sqrt(1 - ac * ac)) + np.deg2rad(phase))
-        F = np.fft.fft2(rng.standard_normal((ny, n))) * (np.abs(np.sin(chi)) * np.exp(-40 * s2) + 0.3)
-        return (np.real(np.fft.ifft2(F)) + 10.0).astype(np.float32)
-    return make
+    ny = ny or n
+    rng = np.random.default_rng(seed)
+    ky = np.fft.fftfreq(ny)[:, None]
+    kx = np.fft.fftfreq(n)[None, :]
+    s2 = (kx ** 2 + ky ** 2) / pix ** 2
+    th = np.arctan2(ky, kx + 1e-30)
+    lam = 12.26 / np.sqrt(kv * 1000 + 0.9784 * kv * kv)
+    dfa = df + df * ast * np.cos(2 * (th - np.deg2rad(ang)))
+    chi = (np.pi * lam * s2 * (dfa - 0.5 * lam ** 2 * s2 * cs * 1e7)
+           + np.arctan(ac / np.sqrt(1 - ac * ac)) + np.deg2rad(phase))
+    F = np.fft.fft2(rng.standard_normal((ny, n))) * (np.abs(np.sin(chi)) * np.exp(-40 * s2) + 0.3)
+    return (np.real(np.fft.ifft2(F)) + 10.0).astype(np.float32)
+
+
+@pytest.fixture(scope="session")
+def ctf_image():
+    """Factory of micrographs with a planted CTF (make_ctf_image)."""
+    return make_ctf_image

@@ -10,6 +10,12 @@ shift bookkeeping (CPeak2D, CRemoveSpikes1D, CStackShift::Smooth,
 CInterpolateShift, CPatchShifts) compiled unmodified from the reference
 sources by oracle/ref_host (seeded random inputs).
 
+ctf_fits.json: the fits of the reference's own CTF drivers (CFindCtf2D,
+CFindDefocus1D/2D, compiled unmodified by oracle/ref_host with host
+stand-ins for their kernels) on the half spectra the oracle makes from
+seeded micrographs with a planted CTF (tests/conftest.py make_ctf_image);
+the inputs are stored as the image parameters.
+
 Run from the repository root: python tests/golden/make_golden.py
 """
 import ctypes
@@ -89,9 +95,38 @@ def host_bookkeeping():
     return cases
 
 
+CTF_CASES = [
+    {"image": {"n": 1024, "df": 12000.0, "ast": 0.03, "ang": -40.0, "phase": 0.0, "seed": 5},
+     "pix": 1.0, "kv": 300.0, "cs": 2.7, "ac": 0.07, "ext_phase": 0.0},
+    {"image": {"n": 1024, "df": 12000.0, "ast": 0.03, "ang": -40.0, "phase": 30.0, "seed": 5},
+     "pix": 1.0, "kv": 300.0, "cs": 2.7, "ac": 0.07, "ext_phase": 30.0},
+    {"image": {"n": 1280, "pix": 1.6, "df": 22000.0, "ast": 0.01, "ang": 70.0, "phase": 0.0, "seed": 6,
+               "kv": 200.0, "cs": 2.0, "ac": 0.1},
+     "pix": 1.6, "kv": 200.0, "cs": 2.0, "ac": 0.1, "ext_phase": 0.0},
+]
+
+
+def ctf_fits():
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from conftest import make_ctf_image
+    from oracle import oracle as O
+    L = O.ref_ctf()
+    f = ctypes.c_float
+    out = []
+    for c in CTF_CASES:
+        avg, _, pn = O.ctf_spectrum(make_ctf_image(**c["image"]), c["pix"])
+        res = np.zeros(6, np.float32)
+        L.ref_ctf_search(np.ascontiguousarray(avg).ctypes.data_as(ctypes.c_void_p), f(pn), f(c["kv"]),
+                         f(c["cs"]), f(c["ac"]), f(c["ext_phase"]), res.ctypes.data_as(ctypes.c_void_p))
+        out.append(dict(c, pix_n=float(pn), res6=[float(v) for v in res]))
+    return {"source": "FindCtf/CFindCtf2D.cpp, CFindDefocus1D.cpp, CFindDefocus2D.cpp", "cases": out}
+
+
 if __name__ == "__main__":
     with open(os.path.join(OUT, "lin_eqs_kat.json"), "w") as fh:
         json.dump(lin_eqs_kat(), fh, indent=1)
     with open(os.path.join(OUT, "host_bookkeeping.json"), "w") as fh:
         json.dump(host_bookkeeping(), fh)
+    with open(os.path.join(OUT, "ctf_fits.json"), "w") as fh:
+        json.dump(ctf_fits(), fh, indent=1)
     print("written")

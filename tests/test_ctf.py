@@ -188,3 +188,26 @@ def test_estimate_ctf_argument_checks(mc3lib):
     assert rc == api.MC3_EINVAL
     d = api.Params()
     assert d.cs == 0.0 and d.amp_cont == 0.07  # the library does not estimate unless asked
+
+
+def test_searches_match_golden_reference_fits(oracle, ctf_shim):
+    """tests/golden/ctf_fits.json holds the reference drivers' fits (made by
+    tests/golden/make_golden.py) of the oracle's spectra of seeded
+    micrographs: the oracle's search and the device path's search driver
+    reproduce every value without the reference tree (three cases: no extra
+    phase, an extra-phase search, 200 kV / 1.6 A)."""
+    import json
+    import os
+    from conftest import make_ctf_image
+    gold = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "ctf_fits.json")))
+    assert len(gold["cases"]) == 3
+    for c in gold["cases"]:
+        avg, _, pn = oracle.ctf_spectrum(make_ctf_image(**c["image"]), c["pix"])
+        assert np.float32(pn) == np.float32(c["pix_n"])
+        ref = np.array(c["res6"], np.float32)
+        got = oracle.ctf_search(avg, pn, c["kv"], c["cs"], c["ac"], c["ext_phase"])
+        assert np.array_equal(got, ref), (c["image"], got, ref)
+        res, fit = np.zeros(6, np.float32), np.zeros(4, np.float32)
+        ctf_shim.shim_ctf_search(_ptr(np.ascontiguousarray(avg)), _f(pn), _f(c["kv"]), _f(c["cs"]),
+                                 _f(c["ac"]), _f(c["ext_phase"]), _ptr(res), _ptr(fit))
+        assert np.array_equal(res, ref), (c["image"], res, ref)
