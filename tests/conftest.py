@@ -80,6 +80,23 @@ def ctf_shim():
 
 
 @pytest.fixture(scope="session")
+def proposal_shim():
+    """libmc3's proposal-network core (csrc/proposal_core.h) compiled for the host."""
+    out_dir = os.path.join(ROOT, "tests", "_build")
+    os.makedirs(out_dir, exist_ok=True)
+    so = os.path.join(out_dir, "proposal_core_shim.so")
+    src = os.path.join(ROOT, "tests", "native", "proposal_core_shim.cpp")
+    hdr = os.path.join(ROOT, "motioncor3_b200", "csrc", "proposal_core.h")
+    if not os.path.exists(so) or os.path.getmtime(so) < max(os.path.getmtime(src), os.path.getmtime(hdr)):
+        cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+        subprocess.run([cxx, "-O2", "-std=c++17", "-shared", "-fPIC", "-I/usr/local/cuda/include",
+                        src, "-o", so], check=True)
+    L = ctypes.CDLL(so)
+    L.shim_proposal_loss_grad.restype = ctypes.c_double
+    return L
+
+
+@pytest.fixture(scope="session")
 def torch_cuda():
     torch = pytest.importorskip("torch")
     if not torch.cuda.is_available():

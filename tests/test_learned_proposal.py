@@ -91,3 +91,31 @@ def test_warm_start_keeps_the_cold_result(oracle, seed):
     warm, it1 = oracle.iterative_align(spec, 1, 15, 0.05, 150.0, init=cold)
     assert it1 <= it0 and it1 >= 2
     assert np.abs(warm - cold).max() <= 0.05
+
+
+@pytest.mark.parametrize("layers,size", [([(2, 4, 3, 2, 1), (4, 6, 3, 2, 1)], 12),
+                                         ([(2, 8, 5, 2, 2), (8, 16, 3, 2, 1), (16, 16, 3, 2, 1)], 32),
+                                         ([(2, 3, 4, 3, 0), (3, 5, 3, 1, 1)], 17)])
+def test_device_core_matches_oracle(oracle, proposal_shim, layers, size):
+    """The per-element gathers the device kernels are built from
+    (csrc/proposal_core.h: conv_fwd_at, conv_dx_at, conv_dw_at, conv_db_at,
+    relu_grad), assembled into a whole pass in double, give the oracle's
+    output, loss and gradient (strides 1-3, padding 0-2, odd sizes)."""
+    import ctypes
+    net = oracle.ShiftNet(layers, 5, seed=4)
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal((2, size, size))
+    t = rng.standard_normal(5)
+    p = net.params()
+    g_ref = np.zeros(net.n_params)
+    loss_ref = net.loss_grad(x, t, g_ref)
+    out_ref = net.forward(x)
+    spec = np.array(layers, np.int32).ravel()
+    g = np.zeros(net.n_params)
+    out = np.zeros(5)
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    loss = proposal_shim.shim_proposal_loss_grad(len(layers), P(spec), 5, P(p), P(x), 2, size, size, P(t),
+                                                 P(g), P(out))
+    assert abs(loss - loss_ref) <= 1e-12 * max(1.0, abs(loss_ref))
+    assert np.allclose(out, out_ref, rtol=1e-12, atol=1e-12)
+    assert np.abs(g - g_ref).max() <= 1e-10 * np.abs(g_ref).max()
