@@ -17,6 +17,16 @@ flush is needed between steps.  Multi-GPU runs are independent replicas
 `--impl reference` times the FP64 CPU restatement of the reference path (the
 reference has no CPU implementation of its own) on all host cores, on a
 bounded sample of the same workload (3 frames of 4096x4096 per step).
+
+`--gpus N` without an outside launcher starts N replica processes itself
+(torch.distributed.run, one per GPU, rendezvous on 127.0.0.1).
+
+Accuracy: the CPU-baseline leg (rank 0, one GPU) also writes the timed movie
+as an MRC file and runs the reference program built from the reference's
+sources (oracle/_ref/MotionCor3, when present) on it with the same options:
+the line reports the timed run's shifts and sums against the reference's,
+and the reference's own shift error against the generator's drift beside
+ours.
 """
 from __future__ import annotations
 
@@ -28,6 +38,8 @@ import subprocess
 import sys
 import threading
 import time
+
+import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
@@ -106,6 +118,37 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
+def max_over_ranks(value: float, dist=None, device="cpu") -> float:
+    """The largest value over all ranks (timings are reported as the slowest
+    rank's); the value itself without a process group."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(ms_local: float, world: int, units_per_rank: int, dist=None,
+                   device="cpu"):
+    """(slowest rank's milliseconds, units of all ranks per second): replicas
+    each process units_per_rank units in ms_local milliseconds."""
+    ms = max_over_ranks(ms_local, dist, device)
+    return ms, world * units_per_rank / (ms / 1000.0)
+
+
+def spawn_replicas(args, argv) -> int:
+    """Re-runs this script under torch.distributed.run with one process per GPU."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={args.gpus}", "--master-addr", "127.0.0.1", "--master-port",
+           str(port), os.path.abspath(__file__)] + list(argv)
+    return subprocess.run(cmd).returncode
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -169,6 +212,87 @@ def run_reference(args, wl, world, rank):
     return 0
 
 
+def _read_log(path):
+    rows = []
+    for line in open(path):
+        if line.startswith("#") or not line.strip():
+            continue
+        rows.append([float(v) for v in line.split()])
+    return np.asarray(rows, np.float64)
+
+
+def _sum_agreement(r, o, frac=1e-3):
+    """Relative RMS over all pixels; fraction of pixels apart by more than
+    `frac` of the RMS (a local-correction gather that moved to the
+    neighbouring pixel); relative RMS over the other pixels."""
+    r = np.asarray(r, np.float64)
+    o = np.asarray(o, np.float64)
+    d = o - r
+    rms = np.sqrt(np.mean(r * r))
+    big = np.abs(d) > frac * rms
+    rest = ~big
+    return (float(np.sqrt(np.mean(d * d)) / rms), float(big.mean()),
+            float(np.sqrt(np.mean(d[rest] ** 2) / np.mean(r[rest] ** 2))))
+
+
+def reference_check(frames, gain, wl, res, sums, drift):
+    """Runs the reference program (built from the reference's sources into
+    oracle/_ref) on the timed movie with the workload's options; returns the
+    timed run's differences from it and both programs' shift errors against
+    the generator's drift."""
+    import tempfile
+    from motioncor3_b200 import mrcio
+    exe = os.path.join(ROOT, "oracle", "_ref", "MotionCor3")
+    if not os.path.exists(exe):
+        return {"skipped": "reference program not built"}
+    pr = wl["params"]
+    tags = ["-Patch", str(pr["patch"][0]), str(pr["patch"][1]), "-Iter", str(pr["iter"]),
+            "-Tol", str(pr["tol"]), "-Bft", str(pr["bft"][0]), str(pr["bft"][1]),
+            "-PixSize", str(pr["pix_size"]), "-Cs", "0"]
+    if pr.get("fm_dose"):
+        tags += ["-FmDose", str(pr["fm_dose"]), "-kV", str(pr.get("kv", 300))]
+    nz = frames.shape[0]
+    with tempfile.TemporaryDirectory() as td:
+        mvp = os.path.join(td, "movie.mrc")
+        if float(frames.max()) <= 255 and np.array_equal(frames, np.round(frames)):
+            mrcio.write(mvp, frames.astype(np.uint8))  # Poisson counts: exact in mode 0
+        else:
+            mrcio.write(mvp, frames)
+        args = [exe, "-InMrc", mvp, "-OutMrc", os.path.join(td, "sum.mrc"), "-LogDir", td + "/",
+                "-Gpu", "0"] + tags
+        if gain is not None:
+            mrcio.write(os.path.join(td, "gain.mrc"), gain.astype(np.float32))
+            args += ["-Gain", os.path.join(td, "gain.mrc")]
+        env = dict(os.environ)
+        env["LD_LIBRARY_PATH"] = "/usr/local/cuda/lib64:" + env.get("LD_LIBRARY_PATH", "")
+        p = subprocess.run(args, capture_output=True, text=True, env=env, timeout=900, cwd=td)
+        if p.returncode != 0:
+            return {"error": "reference program exit " + str(p.returncode)}
+        patch = res.n_patches > 0
+        full = _read_log(os.path.join(td, "movie-Patch-Full.log" if patch else "movie-Full.log"))
+        ref_g = full[:, 1:3]
+        out = {"program": "reference MotionCor3 built from its sources (oracle/_ref)",
+               "global_shift_diff_px_max": float(np.abs(ref_g - res.global_shifts).max())}
+        if patch:
+            pp = _read_log(os.path.join(td, "movie-Patch-Patch.log"))
+            P = res.n_patches
+            ref_p = pp[:, 3:5].reshape(P, nz, 2).transpose(1, 0, 2)
+            cen = pp[:, 1:3].reshape(P, nz, 2)[:, 0]
+            out["patch_centres_identical"] = bool(np.array_equal(cen, res.patch_centers))
+            out["patch_shift_diff_px_max"] = float(np.abs(ref_p - res.patch_shifts).max())
+        for k, suf in enumerate(("", "_DW", "_DWS")[: sums.shape[0]]):
+            r = mrcio.read(os.path.join(td, f"sum{suf}.mrc"))[0]
+            rel, moved, rest = _sum_agreement(r, sums[k])
+            out[f"sum{suf or '_plain'}"] = {"rel_rms": rel, "moved_gather_pixels": moved,
+                                            "rel_rms_other_pixels": rest}
+    ref_f = nz // 2
+    true = -(np.asarray(drift, np.float64) - np.asarray(drift, np.float64)[ref_f])
+    for name, g in (("reference", ref_g), ("ours", np.asarray(res.global_shifts, np.float64))):
+        d = np.abs((g - g[ref_f]) - true)
+        out[f"{name}_err_vs_truth_px_rms"] = float(np.sqrt(np.mean(d ** 2)))
+    return out
+
+
 def run_ours(args, wl, world, rank, local):
     import numpy as np
     import torch
@@ -222,11 +346,7 @@ def run_ours(args, wl, world, rank, local):
     launches = (api.kernel_launches() - launches0) // max(args.steps, 1)
     prof = api.profile_read(reset=True)
     api.profile_enable(False)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * nz * args.steps / (ms / 1000.0)
+    ms, value = aggregate_rate(ms, world, nz * args.steps, dist, "cuda")
 
     # ---- end to end through the C ABI with pinned host buffers ----
     host_frames = frames.cpu().pin_memory()
@@ -251,11 +371,7 @@ def run_ours(args, wl, world, rank, local):
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     e2e_ms = max(f0.elapsed_time(f1), wall * 1000.0)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = world * nz * args.steps / (e2e_ms / 1000.0)
+    e2e_ms, e2e = aggregate_rate(e2e_ms, world, nz * args.steps, dist, "cuda")
     h2d = hf.nbytes
     d2h = hs.nbytes
 
@@ -308,6 +424,13 @@ def run_ours(args, wl, world, rank, local):
         cpu = {"value": n / ts[0], "unit": "frames/s", "cores": os.cpu_count() or 1,
                "kind": "port",
                "sample": f"{n} frames of {nx}x{ny} with the same options (FP64 oracle, all cores)"}
+        # checker: the reference program on the timed movie
+        try:
+            chk = reference_check(host_frames.numpy(), g, wl, last, sums.cpu().numpy(), mv.drift)
+        except Exception as exc:  # the report never fails on this extra
+            chk = {"error": str(exc)[-300:]}
+        if accuracy is not None:
+            accuracy["vs_reference_program"] = chk
 
     if rank == 0:
         line = {
@@ -348,6 +471,8 @@ def main(argv=None):
     ap.add_argument("--frames", type=int, default=0,
                     help="override the frame count (small cases for profiling; not a bench line)")
     args = ap.parse_args(argv)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return spawn_replicas(args, sys.argv[1:] if argv is None else argv)
     world, rank, local = dist_setup()
     wl = workload(args.config)
     if args.frames > 0:

@@ -266,10 +266,13 @@ int mc3_phase_shift(const float* in, float* out, int cmp_x, int cmp_y, float sx,
  * MC3_NOALLOC_MAX_CMP_X and cmp_y at most MC3_NOALLOC_MAX_CMP_Y; larger sizes
  * return MC3_ETOOBIG.  The first call on a device looks up that array's
  * address (once per device, the device current); make that first call before
- * any stream capture.  Every call on a device shares the one array, so calls
- * that overlap on the GPU (other streams, other host threads) race; calls in
- * one stream are ordered.  Asynchronous: unlike mc3_phase_shift it does not
- * synchronise `stream` before returning. */
+ * any stream capture.  The address is kept for the life of the process, so
+ * after a cudaDeviceReset of a device this entry point must not be called on
+ * it again.  Every call on a device shares the one array, so calls that
+ * overlap on the GPU (other streams, other host threads) race; calls in one
+ * stream are ordered.  The shift reaches the device as a kernel argument (no
+ * host memory is read); the call only enqueues work on `stream` and returns
+ * without waiting for it, unlike mc3_phase_shift, which synchronises. */
 #define MC3_NOALLOC_MAX_CMP_X 8193
 #define MC3_NOALLOC_MAX_CMP_Y 16384
 int mc3_phase_shift_noalloc(const float* in, float* out, int cmp_x, int cmp_y, float sx,

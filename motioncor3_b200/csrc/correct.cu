@@ -173,6 +173,19 @@ __device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
   return d;
 }
 
+// Weight of one patch for pixel (x, y) as mGCorrect3D computes it: w =
+// exp(-100 r), r = distance to the patch centre in units of the frame size;
+// false (the patch is skipped) when r > 0.6.
+__device__ __forceinline__ bool patch_weight(int x, int y, int W, int H, float cx, float cy,
+                                             float* w) {
+  float ax = ((float)(unsigned)x - cx) / (float)(unsigned)W;
+  float ay = (y - cy) / H;
+  ax = sqrtf(ax * ax + ay * ay);
+  if (ax > 0.6f) return false;
+  *w = expf(-100.0f * ax);
+  return true;
+}
+
 // Per-pixel patch weights of mGCorrect3D: w = exp(-100 r) for patches with
 // r <= 0.6 (r = distance to the patch centre in units of the frame size),
 // bit p of the returned mask set for those patches; the others weigh 0.
@@ -180,20 +193,12 @@ template <int PMAX, bool EXACT>
 __device__ __forceinline__ unsigned long long gather_weights(int x, int y, int W, int H,
                                                              const float* __restrict__ cent, int P,
                                                              float (&w)[PMAX]) {
-  const float fB = 100.0f;
   unsigned long long inc = 0ull;
 #pragma unroll
   for (int p = 0; p < PMAX; ++p) {
     w[p] = 0.0f;
-    if (x < W && (EXACT || p < P)) {
-      float ax = ((float)(unsigned)x - cent[2 * p]) / (float)(unsigned)W;
-      float ay = (y - cent[2 * p + 1]) / H;
-      ax = sqrtf(ax * ax + ay * ay);
-      if (!(ax > 0.6f)) {
-        w[p] = expf(-fB * ax);
-        inc |= 1ull << p;
-      }
-    }
+    if (x < W && (EXACT || p < P) && patch_weight(x, y, W, H, cent[2 * p], cent[2 * p + 1], &w[p]))
+      inc |= 1ull << p;
   }
   return inc;
 }
@@ -328,6 +333,61 @@ __global__ void __launch_bounds__(128) k_local_gather(
   }
 }
 
+// More than 64 patches (a 64-bit mask per frame no longer covers them):
+// patches in chunks of kWideChunk whose weights are held in registers, frames
+// in groups of kWideFrames whose running sums carry from chunk to chunk, so
+// every (pixel, frame) still adds its good patches in patch order as
+// mGCorrect3D does (Correct/GCorrectPatchShift.cu:32-46).  Bad patches come
+// from the [nb][P] flags.  Weights are evaluated once per frame group.
+constexpr int kWideChunk = 32, kWideFrames = 8;
+__global__ void __launch_bounds__(128) k_local_gather_wide(
+    const float* __restrict__ in, long in_stride, float* out, long out_stride, int W, int H,
+    const float* __restrict__ cent, const float2* __restrict__ sh,
+    const uint8_t* __restrict__ bad, int P, int nb) {
+  const int y = blockIdx.y;
+  const int x = blockIdx.x * 128 + threadIdx.x;
+  if (x >= W) return;
+  const int padX = (W / 2 + 1) * 2;
+  for (int f0 = 0; f0 < nb; f0 += kWideFrames) {
+    const int nf = min(kWideFrames, nb - f0);
+    float sx[kWideFrames], sy[kWideFrames], sw[kWideFrames];
+#pragma unroll
+    for (int b = 0; b < kWideFrames; ++b) sx[b] = sy[b] = sw[b] = 0.0f;
+    for (int p0 = 0; p0 < P; p0 += kWideChunk) {
+      const int np = min(kWideChunk, P - p0);
+      float w[kWideChunk];
+      unsigned inc = 0u;
+#pragma unroll
+      for (int i = 0; i < kWideChunk; ++i) {
+        w[i] = 0.0f;
+        if (i < np && patch_weight(x, y, W, H, cent[2 * (p0 + i)], cent[2 * (p0 + i) + 1], &w[i]))
+          inc |= 1u << i;
+      }
+#pragma unroll
+      for (int b = 0; b < kWideFrames; ++b) {
+        if (b >= nf) break;
+        const long f = f0 + b;
+#pragma unroll
+        for (int i = 0; i < kWideChunk; ++i) {
+          if (((inc >> i) & 1u) && !(bad && bad[f * P + p0 + i])) {
+            const float2 s = sh[f * P + p0 + i];
+            sw[b] += w[i];
+            sx[b] += s.x * w[i];
+            sy[b] += s.y * w[i];
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < kWideFrames; ++b) {
+      if (b >= nf) break;
+      const long f = f0 + b;
+      const int src = gather_src(W, H, padX, x, y, sx[b], sy[b], sw[b]);
+      out[f * out_stride + (long)y * padX + x] = in[f * in_stride + src];
+    }
+  }
+}
+
 template <int PMAX, bool EXACT>
 static void launch_gather(int W, int H, cudaStream_t st, const float* in, long in_stride,
                           float* out, long out_stride, const float* centers,
@@ -355,7 +415,15 @@ int local_gather(const float* in, long in_stride, float* out, long out_stride, i
                  const unsigned long long* masks, const uint8_t* bad, const uint8_t* clean,
                  int P, cudaStream_t st) {
   // `shifts`/`masks`/`bad`/`clean` point at the first frame of the batch.
-  if (P < 1 || P > 64) return kEUnsupported;
+  if (P < 1) return kEInval;
+  if (P > 64) {
+    prof::Scope ps("k_local_gather_wide", (double)nb * W * H * 8.0, st);
+    dim3 grid(ceil_div(W, 128), H);
+    k_local_gather_wide<<<grid, 128, 0, st>>>(in, in_stride, out, out_stride, W, H, centers,
+                                              shifts, bad, P, nb);
+    MC3_CHECK_LAUNCH("k_local_gather_wide");
+    return kOk;
+  }
   prof::Scope ps("k_local_gather", (double)nb * W * H * 8.0, st);
 #define MC3_GATHER(PM, EX) \
   launch_gather<PM, EX>(W, H, st, in, in_stride, out, out_stride, centers, shifts, masks, bad, clean, P, nb)

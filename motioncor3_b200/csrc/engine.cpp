@@ -394,7 +394,7 @@ int Engine::set_alignment(const mc3_alignment* aln) {
     aln_centers.clear();
     return kOk;
   }
-  if (aln->nz < 1 || !aln->global_shifts || aln->n_patches < 0 || aln->n_patches > 64)
+  if (aln->nz < 1 || !aln->global_shifts || aln->n_patches < 0)
     return kEInval;
   if (aln->n_patches > 0 && (!aln->patch_shifts || !aln->patch_centers)) return kEInval;
   aln_nz = aln->nz;
@@ -848,13 +848,19 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
       MC3_TRY(col_fft(spec, spec, g.cmpX, g.cmpX, H, bi, inv, st));
       Batch br{N, N, (long)ncmp, nullptr, (long)ncmp * 2};
       MC3_TRY(row_c2r(spec, g.cmpX, frames, g.padX, W, H, br, st));
-      MC3_TRY(d_pmask.ensure(sizeof(unsigned long long) * N + N));
-      unsigned long long* masks = d_pmask.as<unsigned long long>();
-      uint8_t* clean = reinterpret_cast<uint8_t*>(masks + N);
-      MC3_TRY(patch_masks(d_pbad.as<uint8_t>(), d_pshift.as<float2>(), P, N, masks, clean, st));
-      MC3_TRY(local_gather(frames, (long)ncmp * 2, d_gath.as<float>(), (long)ncmp * 2, N, W, H,
-                           d_pcent.as<float>(), d_pshift.as<float2>(), masks, nullptr, clean, P,
-                           st));
+      if (P <= 64) {
+        MC3_TRY(d_pmask.ensure(sizeof(unsigned long long) * N + N));
+        unsigned long long* masks = d_pmask.as<unsigned long long>();
+        uint8_t* clean = reinterpret_cast<uint8_t*>(masks + N);
+        MC3_TRY(patch_masks(d_pbad.as<uint8_t>(), d_pshift.as<float2>(), P, N, masks, clean, st));
+        MC3_TRY(local_gather(frames, (long)ncmp * 2, d_gath.as<float>(), (long)ncmp * 2, N, W, H,
+                             d_pcent.as<float>(), d_pshift.as<float2>(), masks, nullptr, clean,
+                             P, st));
+      } else {  // bad-patch flags read directly (no 64-bit masks)
+        MC3_TRY(local_gather(frames, (long)ncmp * 2, d_gath.as<float>(), (long)ncmp * 2, N, W, H,
+                             d_pcent.as<float>(), d_pshift.as<float2>(), nullptr,
+                             d_pbad.as<uint8_t>(), nullptr, P, st));
+      }
       Batch bf{N, N, (long)ncmp * 2, nullptr, (long)ncmp};
       MC3_TRY(row_r2c(d_gath.as<float>(), g.padX, spec, g.cmpX, W, H, bf, 1.0f, st));
       ColOps fwd{};

@@ -12,7 +12,11 @@
 //
 // The scratch is one file-scope __device__ array shared by every call on a
 // device.  Its address is looked up once per device (cudaGetSymbolAddress,
-// with that device current) on the first call made on that device.
+// with that device current) on the first call made on that device and kept
+// for the life of the process; a cudaDeviceReset (which ends the context the
+// address belongs to) makes the kept address stale, so a process that resets
+// a device must not call this entry point on it afterwards.  The shift is
+// passed to the device as a kernel argument: no host memory is read.
 #include <mutex>
 
 #include "kernels.cuh"
@@ -47,6 +51,10 @@ int scratch_for_current_device(float2** out) {
   return MC3_OK;
 }
 
+// Writes the shift into its scratch slot from the kernel's own argument, so
+// that no host memory is read by the device.
+__global__ void k_noalloc_store_shift(float2* slot, float2 v) { *slot = v; }
+
 }  // namespace
 
 extern "C" int mc3_phase_shift_noalloc(const float* in, float* out, int cmp_x, int cmp_y,
@@ -62,10 +70,11 @@ extern "C" int mc3_phase_shift_noalloc(const float* in, float* out, int cmp_x, i
   float2* ex = base + kShiftSlots;
   float2* ey = ex + kExSlots;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  const float2 h = make_float2(sx, sy);
-  // Pageable source: the copy has consumed `h` when the call returns.
-  if (cudaMemcpyAsync(sh, &h, sizeof(float2), cudaMemcpyHostToDevice, st) != cudaSuccess)
-    return MC3_ECUDA;
+  {
+    mc3::prof::Scope ps("k_noalloc_store_shift", 8.0, st);
+    k_noalloc_store_shift<<<1, 1, 0, st>>>(sh, make_float2(sx, sy));
+    if (cudaGetLastError() != cudaSuccess) return MC3_ECUDA;
+  }
   s = mc3::phase_tables(sh, 1, cmp_x, cmp_y, ex, ey, false, st);
   if (s != MC3_OK) return s;
   return mc3::phase_apply(reinterpret_cast<const float2*>(in), reinterpret_cast<float2*>(out),

@@ -18,7 +18,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_build", "libmc3_oracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libmc3ref_host.so")
 REF_CTF_LIB = os.path.join(HERE, "_ref", "libmc3ref_ctf.so")
-REF_TREE = "/root/reference"
+# The reference source tree: $MC3_REFERENCE, else a directory named
+# "reference" beside the repository.  Absent on machines that only run the
+# prebuilt checkers.
+REF_TREE = os.environ.get("MC3_REFERENCE") or os.path.normpath(
+    os.path.join(HERE, "..", "..", "reference"))
 _VP = ctypes.c_void_p
 
 

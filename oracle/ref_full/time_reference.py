@@ -1,10 +1,10 @@
 """Times the reference program (built by this directory's Makefile) and the
 mc3-b200 command line on the same synthetic movie on one GPU, and records
 both programs' printed "Computation time" (gain -> bad pixels -> align ->
-sums, CProcessThread.cpp:103-104) plus wall time.  Checker / baseline tool;
-run on the GPU box:
+sums, CProcessThread.cpp:103-104) plus wall time.  Checker / baseline tool,
+run on a machine with a GPU:
 
-  python oracle/ref_full/time_reference.py --config cfg2 --out gpurun_out/ref_cfg2.json
+  python oracle/ref_full/time_reference.py --config cfg2 --out ref_cfg2.json
 """
 import argparse
 import json

@@ -28,7 +28,8 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, ROOT)
-REF = "/root/reference"
+# The reference source tree: $MC3_REFERENCE, else "reference" beside the repository.
+REF = os.environ.get("MC3_REFERENCE") or os.path.normpath(os.path.join(ROOT, "..", "reference"))
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 

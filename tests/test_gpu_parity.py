@@ -122,16 +122,56 @@ def test_bad_pixel_detection_and_fill(api, oracle, torch_cuda):
         assert np.array_equal(got[f], ref.astype(np.float32))
 
 
-def test_local_gather_exact(api, oracle, torch_cuda):
+def _local_shift_f64(nx, ny, cen, sh, bad):
+    """The per-pixel weighted patch shift of mGCorrect3D in FP64."""
+    yy, xx = np.mgrid[0:ny, 0:nx].astype(np.float64)
+    sx = np.zeros((ny, nx))
+    sy = np.zeros((ny, nx))
+    sw = np.zeros((ny, nx))
+    for p in range(len(cen)):
+        if bad[p]:
+            continue
+        r = np.sqrt(((xx - cen[p, 0]) / nx) ** 2 + ((yy - cen[p, 1]) / ny) ** 2)
+        w = np.where(r <= 0.6, np.exp(-100.0 * r), 0.0)
+        sw += w
+        sx += w * sh[p, 0]
+        sy += w * sh[p, 1]
+    ok = sw > 0
+    sx[ok] /= sw[ok]
+    sy[ok] /= sw[ok]
+    return xx - sx, yy - sy
+
+
+def _check_gather(got, ref, nx, ny, cen, sh, bad, limit=1e-4):
+    """Every pixel equal, except where the source coordinate lies within
+    `limit` px of a pixel boundary (the host's expf and unfused FP32 adds in
+    the oracle against the device's expf and FMAs can truncate such a
+    coordinate to the neighbouring pixel).  Returns the mismatch fraction."""
+    mism = got != ref.astype(np.float32)
+    if mism.any():
+        u, v = _local_shift_f64(nx, ny, cen, sh, bad)
+        du = np.abs(u - np.round(u))
+        dv = np.abs(v - np.round(v))
+        near = np.minimum(du, dv)[mism]
+        assert near.max() < limit, (int(mism.sum()), float(near.max()))
+    return float(mism.mean())
+
+
+@pytest.mark.parametrize("P,grid", [(9, 3), (100, 10)])
+def test_local_gather_exact(api, oracle, torch_cuda, P, grid):
+    """mGCorrect3D gathers against the oracle: identical pixels, except at
+    sources on a pixel boundary (checked pixel by pixel).  P = 100 runs the
+    kernel for more than 64 patches (chunked patch loop)."""
     torch = torch_cuda
-    rng = np.random.default_rng(4)
-    ny, nx, P = 384, 512, 9
+    rng = np.random.default_rng(4 + P)
+    ny, nx = 384, 512
     img = rng.standard_normal((ny, nx)).astype(np.float32)
-    cen = np.array([[(i % 3 + 0.5) * nx / 3 + rng.normal(0, 9), (i // 3 + 0.5) * ny / 3 + rng.normal(0, 9)]
-                    for i in range(P)], np.float32)
+    cen = np.array([[(i % grid + 0.5) * nx / grid + rng.normal(0, 9),
+                     (i // grid + 0.5) * ny / grid + rng.normal(0, 9)] for i in range(P)], np.float32)
     sh = rng.normal(0, 2.5, (P, 2)).astype(np.float32)
     bad = np.zeros(P, np.uint8)
     bad[4] = 1
+    bad[P - 3] = 1
     ref = oracle.local_gather(img, cen, sh, bad)
     cx = nx // 2 + 1
     src = torch.zeros((ny, 2 * cx), dtype=torch.float32, device="cuda")
@@ -141,8 +181,8 @@ def test_local_gather_exact(api, oracle, torch_cuda):
                      torch.from_numpy(bad).cuda())
     torch.cuda.synchronize()
     got = dst[:, :nx].cpu().numpy()
-    mism = np.mean(got != ref.astype(np.float32))
-    assert mism < 1e-4, mism
+    frac = _check_gather(got, ref, nx, ny, cen.astype(np.float64), sh.astype(np.float64), bad)
+    assert frac < 1e-4, frac
 
 
 def test_iterative_align_component(api, oracle, torch_cuda):
@@ -496,3 +536,14 @@ def test_pipeline_config1_full_size(api, oracle, torch_cuda):
     m = S.make_movie(1024, 1024, 40, dose=1.0, seed=101)
     p = api.Params(iter=7, tol=0.5, bft=(150, 100), pix_size=1.0)
     _compare_movie(api, oracle, m, p)
+
+
+def test_pipeline_patch_10x10(api, oracle, torch_cuda):
+    """-Patch 10 10 (100 patches: more than a 64-bit patch mask holds), the
+    whole path against the oracle."""
+    from motioncor3_b200 import synthetic as S
+    m = S.make_movie(1024, 1024, 10, dose=3.0, seed=57, gain=False, local=True)
+    p = api.Params(patch=(10, 10), iter=5, tol=0.2, bft=(500, 150), fm_dose=1.0, pix_size=1.0,
+                   kv=300)
+    res, _ = _compare_movie(api, oracle, m, p)
+    assert res.n_patches == 100

@@ -4,9 +4,15 @@ The reference (MotionCor3 1.2.1) is compiled from its own sources for
 sm_100 into oracle/_ref/MotionCor3 by oracle/ref_full/Makefile.  Each case
 writes a seeded synthetic movie (and gain) as MRC, runs the reference and
 the mc3-b200 command line with the same tags, and compares the shift logs
-(within 0.05 px) and the sums (within 1e-4 relative RMS; 1e-3 in patch mode,
-see below).  Skipped when the
-reference binary is not present."""
+(within 0.05 px) and the sums.  Global mode: sums within 1e-4 relative RMS.
+Patch mode: the local correction copies the nearest pixel of a sub-pixel
+source position, so the ~1e-6 px by which two FFT implementations move a
+patch shift moves a few gathers to the neighbouring pixel; those pixels
+differ by a whole count while all others agree to FFT rounding.  Patch-mode
+sums are therefore held to 1e-4 relative RMS on every pixel that no moved
+gather touched, to a bounded fraction of moved pixels, and to 1e-3 overall
+(test_patch_gathers_at_4096_match_reference_frame_by_frame shows the moved
+gathers frame by frame).  Skipped when the reference binary is not present."""
 import os
 import re
 import subprocess
@@ -36,11 +42,14 @@ def _read_log(path):
     return np.array(rows)
 
 
-def run_program(binary, workdir, movie, gain, tags, extra=(), four_bit=False, dark=None, cs="0"):
+def run_program(binary, workdir, movie, gain, tags, extra=(), four_bit=False, dark=None, cs="0",
+                movie_path=None):
+    """movie_path: an MRC movie written already (movie is then not written)."""
     from motioncor3_b200 import mrcio
     os.makedirs(workdir, exist_ok=True)
-    mv = os.path.join(workdir, "movie.mrc")
-    mrcio.write(mv, movie, four_bit=four_bit)
+    mv = movie_path or os.path.join(workdir, "movie.mrc")
+    if movie_path is None:
+        mrcio.write(mv, movie, four_bit=four_bit)
     if dark is not None:
         dp = os.path.join(workdir, "dark.mrc")
         mrcio.write(dp, dark.astype(np.float32))
@@ -62,11 +71,12 @@ def run_program(binary, workdir, movie, gain, tags, extra=(), four_bit=False, da
         if os.path.exists(f):
             sums[suf] = mrcio.read(f)[0].astype(np.float64)
     logs = {}
+    stem = os.path.splitext(os.path.basename(mv))[0]
     for suf in ("-Full.log", "-Patch-Full.log", "-Patch-Patch.log", "-Patch-Frame.log"):
-        f = os.path.join(workdir, "movie" + suf)
+        f = os.path.join(workdir, stem + suf)
         if os.path.exists(f):
             logs[suf] = f
-    aln = os.path.join(workdir, "movie.aln")
+    aln = os.path.join(workdir, stem + ".aln")
     stk = os.path.join(workdir, "sum_Stk.mrc")
     return dict(sums=sums, logs=logs, secs=secs, stdout=out,
                 aln=open(aln).read() if os.path.exists(aln) else None,
@@ -80,6 +90,50 @@ def _aln_parts(text):
     nums = [float(t) for t in toks if re.fullmatch(r"[+-]?\d+(\.\d+)?", t)]
     skel = [t for t in toks if not re.fullmatch(r"[+-]?\d+(\.\d+)?", t)]
     return skel, np.array(nums)
+
+
+def sum_agreement(r, o, frac=1e-3):
+    """Relative RMS of o - r over all pixels; the fraction of pixels whose
+    difference exceeds `frac` of the RMS of r (a gather moved to the
+    neighbouring pixel changes a pixel by about one count); the relative RMS
+    over all other pixels."""
+    r = np.asarray(r, np.float64)
+    o = np.asarray(o, np.float64)
+    d = o - r
+    rms = np.sqrt(np.mean(r * r))
+    big = np.abs(d) > frac * rms
+    rest = ~big
+    rel_rest = float(np.sqrt(np.mean(d[rest] ** 2) / np.mean(r[rest] ** 2)))
+    return float(np.sqrt(np.mean(d * d)) / rms), float(big.mean()), rel_rest
+
+
+def assert_sums(ref, ours, patch_mode, label=""):
+    for suf in ref["sums"]:
+        r, o = ref["sums"][suf], ours["sums"][suf]
+        rel, moved, rest = sum_agreement(r, o)
+        print(f"{label} sum{suf}: rel RMS {rel:.2e}; moved pixels {moved:.2e}, others {rest:.2e}; "
+              f"reference {ref['secs']} s, ours {ours['secs']} s")
+        if patch_mode:
+            assert rest <= 1e-4 and moved <= 2e-3 and rel <= 1e-3, (suf, rel, moved, rest)
+        else:
+            assert rel <= 1e-4, (suf, rel)
+
+
+def run_reference_same_centres(workdir, movie, gain, tags, ours_logs, tries=3, **kw):
+    """Runs the reference, again when its patch centres differ from ours:
+    its feature map is normalised in place while neighbouring threads still
+    read it (Align/GNormByStd2D.cu:7-40), a race that on some inputs moves a
+    centre in some runs.  Returns the run (the last one when every try differs)."""
+    ref = None
+    for t in range(tries):
+        ref = run_program(REF_BIN, f"{workdir}_{t}", movie, gain, tags, **kw)
+        if "-Patch-Patch.log" not in ref["logs"]:
+            return ref
+        a = _read_log(ref["logs"]["-Patch-Patch.log"])[:, 1:3]
+        b = _read_log(ours_logs["-Patch-Patch.log"])[:, 1:3]
+        if a.shape == b.shape and np.array_equal(a, b):
+            return ref
+    return ref
 
 
 CASES = {
@@ -118,26 +172,22 @@ def test_cli_matches_reference_program(name, tmp_path, mc3lib):
     nz, ny, nx = c["shape"]
     m = S.make_movie(nx, ny, nz, dose=c["dose"], seed=c["seed"], gain=c["gain"], local=c["local"])
     tags = c["tags"].split()
-    ref = run_program(REF_BIN, str(tmp_path / "ref"), m.frames, m.gain, tags)
     ours = run_program(OUR_BIN, str(tmp_path / "ours"), m.frames, m.gain, tags)
+    ref = run_reference_same_centres(str(tmp_path / "ref"), m.frames, m.gain, tags, ours["logs"])
     assert sorted(ref["sums"]) == sorted(ours["sums"])
     assert sorted(ref["logs"]) == sorted(ours["logs"])
-    same_shifts = True
-    if "-Patch-Patch.log" in ref["logs"]:
-        # The reference normalises its feature map in place while neighbouring
-        # threads still read it (Align/GNormByStd2D.cu:7-40), so on some inputs
-        # and boxes a patch centre lands elsewhere; the rest is then not comparable.
+    patch_mode = "-Patch-Patch.log" in ref["logs"]
+    if patch_mode:
         a = _read_log(ref["logs"]["-Patch-Patch.log"])[:, 1:3]
         b = _read_log(ours["logs"]["-Patch-Patch.log"])[:, 1:3]
         if a.shape == b.shape and not np.array_equal(a, b):
-            pytest.skip(f"reference patch centres differ by {np.abs(a - b).max()} px "
+            pytest.skip(f"reference patch centres differ by {np.abs(a - b).max()} px in 3 runs "
                         "(feature-map race in the reference)")
     for key in ref["logs"]:
         a, b = _read_log(ref["logs"][key]), _read_log(ours["logs"][key])
         assert a.shape == b.shape, key
         d = np.abs(a - b).max()
         assert d <= 0.05 + 1e-6, (key, d)
-        same_shifts &= d == 0
     # alignment files (-OutAln): same layout, values within the shift tolerance
     assert ref["aln"] is not None and ours["aln"] is not None
     (sr, nr), (so, no) = _aln_parts(ref["aln"]), _aln_parts(ours["aln"])
@@ -148,16 +198,9 @@ def test_cli_matches_reference_program(name, tmp_path, mc3lib):
     # (Align/CMeasurePatches.cpp:79-81 keeps full float precision), so a
     # 1e-6 px difference in patch shifts -- the size that FP32 rounding
     # differences between two FFT implementations leave in the sub-pixel
-    # peak fit -- already moves the sums by ~1e-4 relative RMS
-    # (test_oracle.py::test_patch_sum_sensitivity_to_shift_rounding).  With
-    # every logged shift identical the bound there is 1e-3.
-    tol = 1e-3 if "-Patch-Patch.log" in ref["logs"] else 1e-4
-    for suf in ref["sums"]:
-        r, o = ref["sums"][suf], ours["sums"][suf]
-        rel = np.sqrt(np.mean((r - o) ** 2) / np.mean(r ** 2))
-        print(f"{name} sum{suf}: rel RMS {rel:.2e}; reference {ref['secs']} s, ours {ours['secs']} s")
-        if same_shifts:
-            assert rel <= tol, (suf, rel)
+    # peak fit -- moves a few gathers by a pixel
+    # (test_oracle.py::test_patch_sum_sensitivity_to_shift_rounding).
+    assert_sums(ref, ours, patch_mode, name)
 
 
 def _rel(r, o):
@@ -235,8 +278,9 @@ def test_cli_loaded_alignment_matches_reference_program(name, tmp_path, mc3lib):
         # not found by reading, so patch mode is held to 1e-2 here.
         tol = 1e-2
     for suf in ref["sums"]:
-        e = _rel(ref["sums"][suf], ours["sums"][suf])
-        print(f"{name} -InAln sum{suf}: rel RMS {e:.2e}")
+        e, moved, rest = sum_agreement(ref["sums"][suf], ours["sums"][suf])
+        print(f"{name} -InAln sum{suf}: rel RMS {e:.2e}; moved pixels {moved:.2e}, "
+              f"others {rest:.2e}")
         assert e <= tol, (suf, e)
 
 
@@ -487,3 +531,101 @@ def test_cli_fmint_file_without_integration_and_throws(tmp_path, mc3lib):
     if np.array_equal(a, b):
         for suf in ref["sums"]:
             assert _rel(ref["sums"][suf], ours["sums"][suf]) <= 1e-4, suf
+
+
+def _write_u8_movie(path, frames):
+    """Synthetic frames are Poisson counts: stored exactly as MRC mode 0."""
+    from motioncor3_b200 import mrcio
+    assert float(frames.max()) <= 255 and np.array_equal(frames, np.round(frames))
+    mrcio.write(path, frames.astype(np.uint8))
+
+
+CONFIG2_TAGS = "-Patch 5 5 -Iter 10 -Bft 500 150 -FmDose 1.161 -PixSize 0.83 -kV 300"
+
+
+def test_cli_config2_matches_reference_program(tmp_path, mc3lib):
+    """The benchmark configuration: 60 frames of 4096^2 at 0.8 e/px/frame,
+    -Patch 5 5 -Iter 10 -Bft 500 150 -FmDose 1.161 -PixSize 0.83 -kV 300 and
+    a gain in [0.9, 1.1] (xcf bin 2, 408^2 patches, 25-patch gather), through
+    the reference program and the mc3 command line: every logged global and
+    patch shift within 0.05 px, the sums as the module docstring states."""
+    if not os.path.exists(REF_BIN):
+        pytest.skip("reference program not built (oracle/ref_full)")
+    from motioncor3_b200 import build, synthetic as S
+    build.build()
+    m = S.make_movie(4096, 4096, 60, dose=0.8, seed=1000, gain=True, local=True, backend="torch")
+    frames = m.frames.cpu().numpy()
+    gain = m.gain.cpu().numpy()
+    del m
+    mv = str(tmp_path / "movie.mrc")
+    _write_u8_movie(mv, frames)
+    del frames
+    tags = CONFIG2_TAGS.split()
+    ours = run_program(OUR_BIN, str(tmp_path / "ours"), None, gain, tags, movie_path=mv)
+    ref = run_reference_same_centres(str(tmp_path / "ref"), None, gain, tags, ours["logs"],
+                                     movie_path=mv)
+    assert sorted(ref["sums"]) == ["", "_DW", "_DWS"] and sorted(ours["sums"]) == sorted(ref["sums"])
+    a = _read_log(ref["logs"]["-Patch-Patch.log"])[:, 1:3]
+    b = _read_log(ours["logs"]["-Patch-Patch.log"])[:, 1:3]
+    assert a.shape == b.shape == (60 * 25, 2)
+    if not np.array_equal(a, b):
+        pytest.skip(f"reference patch centres differ by {np.abs(a - b).max()} px in 3 runs "
+                    "(feature-map race in the reference)")
+    for key in ref["logs"]:
+        a, b = _read_log(ref["logs"][key]), _read_log(ours["logs"][key])
+        assert a.shape == b.shape, key
+        d = np.abs(a - b)
+        print(f"config2 {key}: max |d| {d.max():.3f}, identical entries {np.mean(d == 0):.4f}")
+        assert d.max() <= 0.05 + 1e-6, (key, d.max())
+    assert_sums(ref, ours, True, "config2")
+
+
+def test_patch_gathers_at_4096_match_reference_frame_by_frame(tmp_path, mc3lib):
+    """12 frames of the benchmark geometry with -OutStack 1 in both programs:
+    the locally corrected frames compared frame by frame.  Pixels whose
+    gather moved to the neighbouring pixel (about one count apart) are
+    counted; every other pixel agrees to FFT rounding."""
+    if not os.path.exists(REF_BIN):
+        pytest.skip("reference program not built (oracle/ref_full)")
+    from motioncor3_b200 import build, synthetic as S
+    build.build()
+    m = S.make_movie(4096, 4096, 12, dose=0.8, seed=1201, gain=True, local=True, backend="torch")
+    frames = m.frames.cpu().numpy()
+    gain = m.gain.cpu().numpy()
+    mv = str(tmp_path / "movie.mrc")
+    _write_u8_movie(mv, frames)
+    del frames
+    tags = (CONFIG2_TAGS + " -OutStack 1").split()
+    ours = run_program(OUR_BIN, str(tmp_path / "ours"), None, gain, tags, movie_path=mv)
+    ref = run_reference_same_centres(str(tmp_path / "ref"), None, gain, tags, ours["logs"],
+                                     movie_path=mv)
+    a = _read_log(ref["logs"]["-Patch-Patch.log"])[:, 1:3]
+    b = _read_log(ours["logs"]["-Patch-Patch.log"])[:, 1:3]
+    if not np.array_equal(a, b):
+        pytest.skip("reference patch centres differ in 3 runs (feature-map race in the reference)")
+    for key in ref["logs"]:
+        d = np.abs(_read_log(ref["logs"][key]) - _read_log(ours["logs"][key])).max()
+        assert d <= 0.05 + 1e-6, (key, d)
+    R, O = ref["stack"], ours["stack"]
+    assert R.shape == O.shape == (12, 4096, 4096)
+    moved_any = np.zeros(R.shape[1:], bool)
+    worst_rest, fracs = 0.0, []
+    for f in range(R.shape[0]):
+        rel, moved, rest = sum_agreement(R[f], O[f])
+        d = np.abs(O[f] - R[f])
+        mv_px = d > 1e-3 * np.sqrt(np.mean(R[f] ** 2))
+        moved_any |= mv_px
+        fracs.append(moved)
+        worst_rest = max(worst_rest, rest)
+        print(f"frame {f}: rel RMS {rel:.2e}; moved gathers {moved:.2e} "
+              f"({int(mv_px.sum())} px), others {rest:.2e}")
+    print(f"moved gathers: mean {np.mean(fracs):.2e} of the pixels per frame")
+    assert worst_rest <= 1e-5, worst_rest
+    assert np.mean(fracs) <= 1e-4, np.mean(fracs)
+    for suf in ref["sums"]:
+        r, o = ref["sums"][suf], ours["sums"][suf]
+        keep = ~moved_any
+        rest = float(np.sqrt(np.mean((o[keep] - r[keep]) ** 2) / np.mean(r[keep] ** 2)))
+        print(f"sum{suf}: {rest:.2e} relative RMS over the {keep.mean():.5f} of pixels "
+              f"where no frame's gather moved")
+        assert rest <= 1e-4, (suf, rest)
