@@ -77,6 +77,13 @@ typedef struct {
   float amp_cont;      /* -AmpCont (0.07): amplitude contrast                 */
   float ext_phase;     /* -ExtPhase deg (0): the extra phase searched spans
                           [0, min(2 ext_phase, 180)]                          */
+  int dft_gemm;        /* 1: the row transforms of the patch stacks (the
+                          patch pass of CTransformStack,
+                          Align/CMeasurePatches.cpp:55) run as split-
+                          precision BF16 DFT GEMMs on the tensor cores
+                          (hi*hi + hi*lo + lo*hi, FP32 accumulation;
+                          ~1e-5 relative error against 1e-7 for the FP32
+                          FFT).  0 (default): the FP32 FFT                  */
 } mc3_params;
 
 /* Sizes a movie will use (CBufferPool::CreateBuffers, CBufferPool.cpp:95-270). */
@@ -134,6 +141,9 @@ typedef struct {
   float* ctf_spectrum;     /* [512][512]: the averaged spectrum with the fitted
                               CTF drawn in (<stem>_Ctf.mrc)                    */
   int ctf_spectrum_on_device; /* 1: `ctf_spectrum` is a device pointer         */
+  int first_iterate;       /* out: 0 cold start; 1 the first iterate set by
+                              mc3_set_first_iterate converged within its cap;
+                              2 it did not and the plain aligner ran from zero */
 } mc3_result;
 
 /* A known alignment (the -InAln file of Align/CLoadAlign.cpp:118-250): the
@@ -210,6 +220,39 @@ int mc3_set_defects(mc3_ctx* ctx, const unsigned char* mask, int nx, int ny);
  * BadPixel::CDetectMain::DoIt, BadPixel::CCorrectMain::DoIt and
  * Align::CAlignMain::DoIt (Align/CAlignMain.cpp:39-75). */
 int mc3_process_movie(mc3_ctx* ctx, const mc3_movie* movie, mc3_result* out);
+/* Movie queue: the reference's processing thread and its package queue
+ * (CProcessThread::ThreadMain, CProcessThread.cpp:39-80), with the loader
+ * thread's overlap (MrcUtil/CLoadCryoEMStack.cpp:104-152).  mc3_submit
+ * hands a movie to the context's worker thread and returns its ticket at
+ * once; movies are processed in submission order, each one's raw frames
+ * copied to the device while the one before it is processed (pinned host
+ * frames overlap fully).  Movies of any size and frame count may follow one
+ * another.  The movie's frames and the result's buffers must stay valid and
+ * unchanged until mc3_wait has returned for its ticket, and while tickets
+ * are outstanding mc3_process_movie and mc3_prefetch_movie return
+ * MC3_EINVAL (the other entry points of the context must not be called).
+ * mc3_destroy finishes the queued movies first. */
+int mc3_submit(mc3_ctx* ctx, const mc3_movie* movie, mc3_result* out, int* ticket);
+/* Blocks until the movie of `ticket` is done and returns its status (as
+ * mc3_process_movie would); latency_ms (may be NULL) receives the time from
+ * its mc3_submit to the end of its processing.  Each ticket is waited for
+ * once. */
+int mc3_wait(mc3_ctx* ctx, int ticket, double* latency_ms);
+/* Autotuner (no counterpart in the reference, whose launch shapes are
+ * fixed): times every variant of the tunable kernel families -- radix-16 or
+ * radix-8 register FFT passes for power-of-two lengths, two or four columns
+ * per CTA in the 4096-point column pass, one or two pixels per thread in
+ * the local-motion gather -- on a synthetic movie of nx x ny x nz with the
+ * context's options (its device time per movie, best of two runs after a
+ * warm-up), and keeps the fastest for movies of that size and patch grid on
+ * this context.  With json_path the choice (and every candidate's time) is
+ * also written to that JSON file, replacing an earlier entry for the same
+ * size and keeping the others; ms_best (may be NULL) receives the winner's
+ * time.  Takes a few seconds per size. */
+int mc3_autotune(mc3_ctx* ctx, int nx, int ny, int nz, const char* json_path, double* ms_best);
+/* Reads the choices of a file written by mc3_autotune into the context.
+ * MC3_EIO when the file is missing or not such a file. */
+int mc3_load_tuning(mc3_ctx* ctx, const char* json_path);
 /* CTF estimate of one image [ny][nx] (even sizes) at pixel size pix_size A:
  * the role of FindCtf::CFindCtfMain::DoIt (FindCtf/CFindCtfMain.cpp:49-83),
  * which the reference runs on the first sum of every movie
@@ -240,6 +283,16 @@ int mc3_prefetch_movie(mc3_ctx* ctx, const mc3_movie* movie);
  * (-FmRef) and treats every loaded patch shift as good.  n_patches must
  * match the context's -Patch grid (MC3_EINVAL otherwise). */
 int mc3_set_alignment(mc3_ctx* ctx, const mc3_alignment* aln);
+/* Warm start of the next movie's full-frame alignment: CIterativeAlign::DoIt
+ * (Align/CIterativeAlign.cpp:55-97) begins from these per-frame shifts
+ * global_xy [nz][2] (full-frame pixels, as mc3_result.global_shifts) instead
+ * of zero -- each frame group's running total starts at its frames' mean --
+ * and runs at most max_iter iterations (<= 0: 3).  When that has not
+ * converged to -Tol, the plain aligner runs from zero with the full -Iter
+ * budget and its result is used (mc3_result.first_iterate tells which).
+ * Consumed by the next mc3_process_movie; NULL clears it.  This is the entry
+ * of the learned proposal (mc3_proposal_*). */
+int mc3_set_first_iterate(mc3_ctx* ctx, const float* global_xy, int nz, int max_iter);
 /* CFmIntParam / CFmGroupParam set up from a frame-integration table: the
  * following movies (nz = n_raw) are rendered, dose-weighted with acc_dose
  * and grouped by raw-frame counts (CFmGroupParam::mGroupByRawSize,
@@ -250,6 +303,13 @@ int mc3_set_frame_integration(mc3_ctx* ctx, const mc3_frame_integration* fi);
 /* Util::CCufft2D::Forward (Util/CCufft2D.cpp:65-87): in-place R2C of nz
  * padded real frames [nz][ny][2*(nx/2+1)], optionally x 1/(nx*ny). */
 int mc3_fft_forward(float* frames, int nx, int ny, int nz, int normalise, void* stream);
+/* The row pass of Util::CCufft2D::Forward (Util/CCufft2D.cpp:65-78): real
+ * DFT of each of n_rows rows of nx floats (row pitch in_pitch floats) into
+ * nx/2+1 complex values per row (row pitch out_pitch complex), not
+ * normalised.  method 0: the FP32 FFT; 1: the split-precision BF16 DFT GEMM
+ * on the tensor cores (even nx <= 414).  Not in place. */
+int mc3_rfft_rows(const float* in, int in_pitch, float* out, int out_pitch, int nx, int n_rows,
+                  int method, void* stream);
 /* Util::CCufft2D::Inverse (Util/CCufft2D.cpp:105-120): in-place,
  * unnormalised C2R of nz half spectra [nz][ny][nx/2+1] complex. */
 int mc3_fft_inverse(float* frames, int nx, int ny, int nz, void* stream);
@@ -310,6 +370,43 @@ int mc3_local_gather(const float* in, float* out, int nx, int ny, const float* c
  * |s| < 0.1 px skipped) with dose weighting when fm_dose > 0. */
 int mc3_dose_weighted_sums(mc3_ctx* ctx, const float* spectra, int nx, int ny, int nz,
                            const float* shifts_host, float* sums, int* n_sums);
+
+/* ---- learned shift proposal (no counterpart in the reference) ----
+ * A small convolutional network (strided convolutions + ReLU, global
+ * average pool, linear head) that maps a binned frame pair [2][h][w] to a
+ * first iterate of that frame's shift, trained on the GPU by the library's
+ * own forward and backward kernels (FP32, Adam) on shifts that the plain
+ * aligner measured, and used through mc3_set_first_iterate, where the plain
+ * aligner remains the fallback and the judge. */
+typedef struct mc3_proposal mc3_proposal;
+/* spec: n_layers groups of (cin, cout, k, stride, pad), the first cin = 2;
+ * nout outputs; weights He-initialised from seed, on device `gpu`. */
+int mc3_proposal_create(const int* spec, int n_layers, int nout, unsigned seed, int gpu,
+                        mc3_proposal** out);
+int mc3_proposal_destroy(mc3_proposal* p);
+int mc3_proposal_num_params(mc3_proposal* p, long* n);
+/* Parameters in the order: per layer weights [cout][cin][k][k] then biases,
+ * then the head's weights [nout][cout_last] then biases (host floats). */
+int mc3_proposal_get_params(mc3_proposal* p, float* params);
+int mc3_proposal_set_params(mc3_proposal* p, const float* params);
+/* Forward and backward of a batch x [batch][2][h][w] against target
+ * [batch][nout] (host arrays): loss = sum over the batch of
+ * 0.5 |out - target|^2, grad (may be NULL) = its gradient summed over the
+ * batch, out (may be NULL) = the outputs. */
+int mc3_proposal_loss_grad(mc3_proposal* p, const float* x, int batch, int h, int w,
+                           const float* target, double* loss, float* grad, float* out);
+/* One Adam step (learning rate lr) on a batch; x and target on the device
+ * when on_device; *loss receives the batch's mean loss. */
+int mc3_proposal_train_step(mc3_proposal* p, const float* x, const float* target, int batch,
+                            int h, int w, int on_device, float lr, double* loss);
+/* Outputs [batch][nout] (host) for inputs x [batch][2][h][w]. */
+int mc3_proposal_predict(mc3_proposal* p, const float* x, int batch, int h, int w, int on_device,
+                         float* out);
+/* Inputs of n frame pairs from a device movie frames [nz][ny][nx] (float):
+ * pairs [n][2] (host) frame indices, each pair binned by `bin` and normalised
+ * by its mean and standard deviation into x [n][2][ny/bin][nx/bin] (device). */
+int mc3_proposal_pair_inputs(const float* frames, int nx, int ny, int nz, const int* pairs, int n,
+                             int bin, float* x, void* stream);
 
 /* ---- diagnostics (no counterpart in the reference, which reports NVTX
  * ranges and wall-clock prints instead, e.g. CProcessThread.cpp:103-104) ---- */

@@ -58,6 +58,7 @@ class _Params(ctypes.Structure):
         ("cs", ctypes.c_float),
         ("amp_cont", ctypes.c_float),
         ("ext_phase", ctypes.c_float),
+        ("dft_gemm", ctypes.c_int),
     ]
 
 
@@ -106,6 +107,7 @@ class _Result(ctypes.Structure):
         ("ctf_done", ctypes.c_int),
         ("ctf_spectrum", ctypes.c_void_p),
         ("ctf_spectrum_on_device", ctypes.c_int),
+        ("first_iterate", ctypes.c_int),
     ]
 
 
@@ -166,6 +168,21 @@ _SIGS = {
                                       _VP], _I),
     "mc3_fft_forward": ([_VP, _I, _I, _I, _I, _VP], _I),
     "mc3_fft_inverse": ([_VP, _I, _I, _I, _VP], _I),
+    "mc3_rfft_rows": ([_VP, _I, _VP, _I, _I, _I, _I, _VP], _I),
+    "mc3_submit": ([_VP, _VP, _VP, _VP], _I),
+    "mc3_set_first_iterate": ([_VP, _VP, _I, _I], _I),
+    "mc3_proposal_create": ([_VP, _I, _I, ctypes.c_uint, _I, _VP], _I),
+    "mc3_proposal_destroy": ([_VP], _I),
+    "mc3_proposal_num_params": ([_VP, _VP], _I),
+    "mc3_proposal_get_params": ([_VP, _VP], _I),
+    "mc3_proposal_set_params": ([_VP, _VP], _I),
+    "mc3_proposal_loss_grad": ([_VP, _VP, _I, _I, _I, _VP, _VP, _VP, _VP], _I),
+    "mc3_proposal_train_step": ([_VP, _VP, _VP, _I, _I, _I, _I, ctypes.c_float, _VP], _I),
+    "mc3_proposal_predict": ([_VP, _VP, _I, _I, _I, _I, _VP], _I),
+    "mc3_proposal_pair_inputs": ([_VP, _I, _I, _I, _VP, _I, _I, _VP, _VP], _I),
+    "mc3_autotune": ([_VP, _I, _I, _I, ctypes.c_char_p, _VP], _I),
+    "mc3_load_tuning": ([_VP, ctypes.c_char_p], _I),
+    "mc3_wait": ([_VP, _I, _VP], _I),
     "mc3_phase_shift": ([_VP, _VP, _I, _I, _F, _F, _I, _VP], _I),
     "mc3_fourier_crop": ([_VP, _I, _I, _VP, _I, _I, _VP], _I),
     "mc3_correlate": ([_VP, _VP, _I, _I, _F, _I, _I, _I, _VP, _VP, _VP], _I),
@@ -251,6 +268,7 @@ class Params:
     cs: float = 0.0          # > 0.001 (with pix_size, kv) turns the CTF estimate on
     amp_cont: float = 0.07
     ext_phase: float = 0.0
+    dft_gemm: int = 0        # 1: patch row transforms as split-BF16 DFT GEMMs (tensor cores)
 
     def to_c(self) -> _Params:
         p = _Params()
@@ -282,6 +300,7 @@ class Params:
         p.cs = float(self.cs)
         p.amp_cont = float(self.amp_cont)
         p.ext_phase = float(self.ext_phase)
+        p.dft_gemm = int(self.dft_gemm)
         return p
 
 
@@ -297,6 +316,7 @@ class Result:
     n_sums: int
     n_patches: int
     time_ms: float
+    first_iterate: int = 0       # 0 cold start, 1 warm start kept, 2 fell back to cold
     stack: Optional[np.ndarray] = None  # [stack_frames][ny][nx] aligned frames (-OutStack)
     ctf: Optional[np.ndarray] = None    # dfmax, dfmin (A), azimuth, phase (deg), score, res (A)
     ctf_spectrum: Optional[np.ndarray] = None  # [512][512] diagnostic spectrum
@@ -315,6 +335,7 @@ class MotionCor3:
         _check(_lib().mc3_create(ctypes.byref(self._p), ctypes.byref(h)), "mc3_create")
         self._h = h
         self._prefetched = []  # host arrays whose copies are in flight
+        self._queued = {}      # ticket -> buffers of a submitted movie
 
     def close(self) -> None:
         if getattr(self, "_h", None):
@@ -445,21 +466,22 @@ class MotionCor3:
         _check(_lib().mc3_set_frame_integration(self._h, ctypes.byref(fi)),
                "mc3_set_frame_integration")
 
-    def process(self, frames, sums_out=None, nx4=None) -> Result:
-        """frames: [nz][ny][nx] numpy array (host) or torch CUDA tensor; with
-        nx4, packed 4-bit frames [nz][ny][(nx4+1)//2] of width nx4."""
+    def _prepare(self, frames, sums_out, nx4):
+        """The mc3_movie, an mc3_result pointing at freshly allocated host
+        tables, and everything that must stay alive until the call is done."""
         mv, keep = self._movie(frames, nx4)
         nx, ny, nz = mv.nx, mv.ny, mv.nz
         info = self.plan(nx, ny, nz)
         ns, P = info["n_sums"], info["n_patches"]
         nz = info["n_frames"]  # rendered frames: the tables below are per rendered frame
         it = int(self.params.iter)
-        gsh = np.zeros((nz, 2), np.float32)
-        psh = np.zeros((nz, max(P, 1), 2), np.float32)
-        pc = np.zeros((max(P, 1), 2), np.float32)
-        pb = np.zeros((nz, max(P, 1)), np.uint8)
-        iters = np.zeros(1 + P, np.int32)
-        errs = np.zeros((1 + P, it), np.float32)
+        h = dict(keep=keep, mv=mv, P=P,
+                 gsh=np.zeros((nz, 2), np.float32),
+                 psh=np.zeros((nz, max(P, 1), 2), np.float32),
+                 pc=np.zeros((max(P, 1), 2), np.float32),
+                 pb=np.zeros((nz, max(P, 1)), np.uint8),
+                 iters=np.zeros(1 + P, np.int32),
+                 errs=np.zeros((1 + P, it), np.float32), stack=None, ctf_img=None)
         r = _Result()
         if sums_out is not None and hasattr(sums_out, "data_ptr"):
             r.sums = sums_out.data_ptr()
@@ -474,34 +496,86 @@ class MotionCor3:
             sums = np.zeros((ns, oy, ox), np.float32)
             r.sums = sums.ctypes.data
             r.sums_on_device = 0
-        r.global_shifts = gsh.ctypes.data
-        r.patch_shifts = psh.ctypes.data if P else None
-        r.patch_centers = pc.ctypes.data if P else None
-        r.patch_bad = pb.ctypes.data if P else None
-        r.iterations = iters.ctypes.data
-        r.errors = errs.ctypes.data
-        stack = None
+        h["sums"] = sums
+        r.global_shifts = h["gsh"].ctypes.data
+        r.patch_shifts = h["psh"].ctypes.data if P else None
+        r.patch_centers = h["pc"].ctypes.data if P else None
+        r.patch_bad = h["pb"].ctypes.data if P else None
+        r.iterations = h["iters"].ctypes.data
+        r.errors = h["errs"].ctypes.data
         if int(self.params.out_stack[0]):
             ox, oy = info["out_size"]
-            stack = np.zeros((nz, oy, ox), np.float32)
-            r.stack = stack.ctypes.data
-        ctf_img = None
+            h["stack"] = np.zeros((nz, oy, ox), np.float32)
+            r.stack = h["stack"].ctypes.data
         if float(self.params.cs) > 0.001 and self.params.kv and self.params.pix_size:
-            ctf_img = np.zeros((512, 512), np.float32)  # CFindCtfMain::bEstimate
-            r.ctf_spectrum = ctf_img.ctypes.data
-        _check(_lib().mc3_process_movie(self._h, ctypes.byref(mv), ctypes.byref(r)),
-               "mc3_process_movie")
+            h["ctf_img"] = np.zeros((512, 512), np.float32)  # CFindCtfMain::bEstimate
+            r.ctf_spectrum = h["ctf_img"].ctypes.data
+        h["r"] = r
+        return h
+
+    @staticmethod
+    def _finish(h) -> Result:
+        r, P, stack = h["r"], h["P"], h["stack"]
         if stack is not None:
             stack = stack[:r.stack_frames]
-        if not mv.on_device and self._prefetched:
-            self._prefetched.pop(0)
-        del keep
-        return Result(sums=sums, global_shifts=gsh, patch_shifts=psh if P else None,
-                      patch_centers=pc if P else None, patch_bad=pb if P else None,
-                      iterations=iters, errors=errs, n_sums=r.n_sums, n_patches=r.n_patches,
-                      time_ms=r.time_ms, stack=stack,
+        return Result(sums=h["sums"], global_shifts=h["gsh"], patch_shifts=h["psh"] if P else None,
+                      patch_centers=h["pc"] if P else None, patch_bad=h["pb"] if P else None,
+                      iterations=h["iters"], errors=h["errs"], n_sums=r.n_sums,
+                      n_patches=r.n_patches, time_ms=r.time_ms, stack=stack,
+                      first_iterate=r.first_iterate,
                       ctf=np.array(r.ctf[:], np.float32) if r.ctf_done else None,
-                      ctf_spectrum=ctf_img if r.ctf_done else None)
+                      ctf_spectrum=h["ctf_img"] if r.ctf_done else None)
+
+    def process(self, frames, sums_out=None, nx4=None) -> Result:
+        """frames: [nz][ny][nx] numpy array (host) or torch CUDA tensor; with
+        nx4, packed 4-bit frames [nz][ny][(nx4+1)//2] of width nx4."""
+        h = self._prepare(frames, sums_out, nx4)
+        _check(_lib().mc3_process_movie(self._h, ctypes.byref(h["mv"]), ctypes.byref(h["r"])),
+               "mc3_process_movie")
+        if not h["mv"].on_device and self._prefetched:
+            self._prefetched.pop(0)
+        return self._finish(h)
+
+    def submit(self, frames, sums_out=None, nx4=None) -> int:
+        """Queues a movie on the context's worker thread (mc3_submit) and
+        returns its ticket; the frames must not change until wait(ticket)."""
+        h = self._prepare(frames, sums_out, nx4)
+        t = ctypes.c_int()
+        _check(_lib().mc3_submit(self._h, ctypes.byref(h["mv"]), ctypes.byref(h["r"]),
+                                 ctypes.byref(t)), "mc3_submit")
+        self._queued[t.value] = h
+        return t.value
+
+    def autotune(self, nx: int, ny: int, nz: int, json_path: Optional[str] = None) -> float:
+        """Picks the fastest kernel variants for movies of this size
+        (mc3_autotune); returns the winner's device time per movie in ms."""
+        ms = ctypes.c_double()
+        _check(_lib().mc3_autotune(self._h, nx, ny, nz,
+                                   json_path.encode() if json_path else None, ctypes.byref(ms)),
+               "mc3_autotune")
+        return ms.value
+
+    def set_first_iterate(self, global_shifts=None, max_iter: int = 3) -> None:
+        """Warm start of the next movie's full-frame alignment
+        (mc3_set_first_iterate): global_shifts [nz][2] in full-frame pixels;
+        None clears it."""
+        if global_shifts is None:
+            _check(_lib().mc3_set_first_iterate(self._h, None, 0, 0), "mc3_set_first_iterate")
+            return
+        g = np.ascontiguousarray(global_shifts, np.float32)
+        _check(_lib().mc3_set_first_iterate(self._h, g.ctypes.data, g.shape[0], max_iter),
+               "mc3_set_first_iterate")
+
+    def load_tuning(self, json_path: str) -> None:
+        _check(_lib().mc3_load_tuning(self._h, json_path.encode()), "mc3_load_tuning")
+
+    def wait(self, ticket: int):
+        """(Result, latency in ms from submit to done) of a queued movie (mc3_wait)."""
+        lat = ctypes.c_double()
+        code = _lib().mc3_wait(self._h, ticket, ctypes.byref(lat))
+        h = self._queued.pop(ticket)
+        _check(code, "mc3_wait")
+        return self._finish(h), lat.value
 
     def estimate_ctf(self, image, pix_size: float, kv: float = 300.0, cs: float = 2.7,
                      amp_cont: float = 0.07, ext_phase: float = 0.0):
@@ -546,10 +620,105 @@ class MotionCor3:
 
 
 # ---- stateless components (device tensors) ----
+class ShiftProposal:
+    """The learned shift proposal on the GPU (mc3_proposal_*): strided
+    convolutions + ReLU, global average pool and a linear head, trained by
+    the library's own kernels.  spec: [(cin, cout, k, stride, pad), ...]."""
+
+    def __init__(self, spec, nout: int = 2, seed: int = 0, gpu: int = 0):
+        flat = (ctypes.c_int * (5 * len(spec)))(*[int(v) for layer in spec for v in layer])
+        h = _VP()
+        _check(_lib().mc3_proposal_create(flat, len(spec), nout, seed, gpu, ctypes.byref(h)),
+               "mc3_proposal_create")
+        self._h, self.nout = h, nout
+        n = ctypes.c_long()
+        _check(_lib().mc3_proposal_num_params(self._h, ctypes.byref(n)), "mc3_proposal_num_params")
+        self.n_params = n.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib().mc3_proposal_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(self.n_params, np.float32)
+        _check(_lib().mc3_proposal_get_params(self._h, p.ctypes.data), "mc3_proposal_get_params")
+        return p
+
+    def set_params(self, p) -> None:
+        a = np.ascontiguousarray(p, np.float32)
+        _check(_lib().mc3_proposal_set_params(self._h, a.ctypes.data), "mc3_proposal_set_params")
+
+    def loss_grad(self, x, target):
+        """(summed loss, summed gradient, outputs) of a host batch x [n][2][h][w]."""
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(target, np.float32)
+        n, _, h, w = x.shape
+        g = np.zeros(self.n_params, np.float32)
+        out = np.zeros((n, self.nout), np.float32)
+        loss = ctypes.c_double()
+        _check(_lib().mc3_proposal_loss_grad(self._h, x.ctypes.data, n, h, w, t.ctypes.data,
+                                             ctypes.byref(loss), g.ctypes.data, out.ctypes.data),
+               "mc3_proposal_loss_grad")
+        return loss.value, g, out
+
+    def train_step(self, x, target, lr: float = 1e-3) -> float:
+        """One Adam step on a batch (torch CUDA tensors or host arrays); mean loss."""
+        loss = ctypes.c_double()
+        if hasattr(x, "data_ptr"):
+            n, _, h, w = x.shape
+            _check(_lib().mc3_proposal_train_step(self._h, _dp(x), _dp(target), n, h, w, 1, lr,
+                                                  ctypes.byref(loss)), "mc3_proposal_train_step")
+        else:
+            xa = np.ascontiguousarray(x, np.float32)
+            ta = np.ascontiguousarray(target, np.float32)
+            n, _, h, w = xa.shape
+            _check(_lib().mc3_proposal_train_step(self._h, xa.ctypes.data, ta.ctypes.data, n, h, w,
+                                                  0, lr, ctypes.byref(loss)),
+                   "mc3_proposal_train_step")
+        return loss.value
+
+    def predict(self, x) -> np.ndarray:
+        n, _, h, w = x.shape
+        out = np.zeros((n, self.nout), np.float32)
+        if hasattr(x, "data_ptr"):
+            _check(_lib().mc3_proposal_predict(self._h, _dp(x), n, h, w, 1, out.ctypes.data),
+                   "mc3_proposal_predict")
+        else:
+            xa = np.ascontiguousarray(x, np.float32)
+            _check(_lib().mc3_proposal_predict(self._h, xa.ctypes.data, n, h, w, 0, out.ctypes.data),
+                   "mc3_proposal_predict")
+        return out
+
+    @staticmethod
+    def pair_inputs(frames, pairs, bin: int, out):
+        """Inputs of frame pairs from a device movie (torch float32 [nz][ny][nx])
+        into out (torch float32 [n][2][ny/bin][nx/bin])."""
+        nz, ny, nx = frames.shape
+        pr = np.ascontiguousarray(pairs, np.int32)
+        _check(_lib().mc3_proposal_pair_inputs(_dp(frames), nx, ny, nz, pr.ctypes.data, pr.shape[0],
+                                               bin, _dp(out), _stream()), "mc3_proposal_pair_inputs")
+
+
 def fft_forward(frames, nx: int, ny: int, normalise: bool = True) -> None:
     """In place on a float32 CUDA tensor [nz][ny][2*(nx//2+1)]."""
     nz = frames.shape[0]
     _check(_lib().mc3_fft_forward(_dp(frames), nx, ny, nz, int(normalise), _stream()), "mc3_fft_forward")
+
+
+def rfft_rows(src, dst, nx: int, method: int = 0) -> None:
+    """Real DFT of every row of src [rows][>= nx] (float32, device) into dst
+    [rows][>= nx/2+1] (complex64, device): method 0 the FP32 FFT, 1 the
+    split-precision BF16 DFT GEMM on the tensor cores."""
+    rows = src.shape[0]
+    _check(_lib().mc3_rfft_rows(_dp(src), src.stride(0), _dp(dst), dst.stride(0), nx, rows, method,
+                                _stream()), "mc3_rfft_rows")
 
 
 def fft_inverse(frames, nx: int, ny: int) -> None:

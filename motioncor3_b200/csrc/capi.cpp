@@ -2,17 +2,27 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <new>
 #include <vector>
 
 #include <string>
 
+#include "dft_gemm.cuh"
 #include "engine.h"
 #include "profile.h"
+#include "proposal.h"
+#include "queue.h"
+
+struct mc3_proposal {
+  int gpu;
+  mc3::proposal::Net net;
+};
 
 struct mc3_ctx {
   mc3::Engine* eng;
+  mc3::MovieQueue* queue = nullptr;  // created by the first mc3_submit
 };
 
 using namespace mc3;
@@ -73,6 +83,7 @@ void mc3_params_default(mc3_params* p) {
   p->cs = 0.0f;
   p->amp_cont = 0.07f;
   p->ext_phase = 0.0f;
+  p->dft_gemm = 0;
 }
 
 int mc3_create(const mc3_params* p, mc3_ctx** out) {
@@ -104,6 +115,7 @@ int mc3_create(const mc3_params* p, mc3_ctx** out) {
 
 int mc3_destroy(mc3_ctx* ctx) {
   if (!ctx) return MC3_EINVAL;
+  delete ctx->queue;  // finishes the queued movies first
   delete ctx->eng;
   delete ctx;
   return MC3_OK;
@@ -114,8 +126,14 @@ int mc3_set_stream(mc3_ctx* ctx, void* stream) {
   return ctx->eng->set_stream(as_stream(stream));
 }
 
+namespace {
+bool queue_busy(mc3_ctx* ctx);
+}  // namespace
+
 int mc3_plan(mc3_ctx* ctx, int nx, int ny, int nz, mc3_plan_info* info) {
   if (!ctx || !info) return MC3_EINVAL;
+  // while movies are queued the worker owns the buffers: sizes only
+  if (queue_busy(ctx)) return ctx->eng->geometry(nx, ny, nz, info);
   return ctx->eng->plan(nx, ny, nz, info);
 }
 
@@ -150,9 +168,84 @@ int mc3_set_gain(mc3_ctx* ctx, const float* gain, int nx, int ny, int on_device)
   return ctx->eng->set_gain(gain, nx, ny, on_device != 0);
 }
 
+namespace {
+// Movies still queued: the context belongs to its worker thread.
+bool queue_busy(mc3_ctx* ctx) { return ctx->queue && ctx->queue->outstanding() > 0; }
+}  // namespace
+
 int mc3_process_movie(mc3_ctx* ctx, const mc3_movie* movie, mc3_result* out) {
-  if (!ctx || !movie) return MC3_EINVAL;
+  if (!ctx || !movie || queue_busy(ctx)) return MC3_EINVAL;
   return ctx->eng->process(*movie, out);
+}
+
+int mc3_submit(mc3_ctx* ctx, const mc3_movie* movie, mc3_result* out, int* ticket) {
+  if (!ctx || !movie || !ticket || !movie->frames) return MC3_EINVAL;
+  if (!ctx->queue) {
+    ctx->queue = new (std::nothrow) MovieQueue(ctx->eng);
+    if (!ctx->queue) return MC3_ENOMEM;
+  }
+  return ctx->queue->submit(*movie, out, ticket);
+}
+
+int mc3_autotune(mc3_ctx* ctx, int nx, int ny, int nz, const char* json_path, double* ms_best) {
+  if (!ctx || nx < 16 || ny < 16 || nz < 3 || queue_busy(ctx)) return MC3_EINVAL;
+  TuningEntry e;
+  int s = ctx->eng->autotune(nx, ny, nz, &e);
+  if (s != kOk) return s;
+  if (ms_best) *ms_best = e.best_ms;
+  if (json_path) {
+    // the file keeps the entries of other sizes; this size's entry is replaced
+    std::vector<TuningEntry> all;
+    if (FILE* f = std::fopen(json_path, "rb")) {
+      std::string text;
+      char buf[4096];
+      size_t n;
+      while ((n = std::fread(buf, 1, sizeof(buf), f)) > 0) text.append(buf, n);
+      std::fclose(f);
+      parse_tuning_json(text, &all);
+    }
+    for (auto it = all.begin(); it != all.end();)
+      it = (it->nx == e.nx && it->ny == e.ny && it->nz == e.nz && it->px == e.px && it->py == e.py)
+               ? all.erase(it)
+               : it + 1;
+    all.push_back(e);
+    cudaDeviceProp prop;
+    const char* dev = cudaGetDeviceProperties(&prop, ctx->eng->device) == cudaSuccess ? prop.name : "";
+    const std::string js = tuning_json(all, dev);
+    FILE* f = std::fopen(json_path, "wb");
+    if (!f) return MC3_EIO;
+    const bool ok = std::fwrite(js.data(), 1, js.size(), f) == js.size();
+    std::fclose(f);
+    if (!ok) return MC3_EIO;
+  }
+  return MC3_OK;
+}
+
+int mc3_load_tuning(mc3_ctx* ctx, const char* json_path) {
+  if (!ctx || !json_path || queue_busy(ctx)) return MC3_EINVAL;
+  FILE* f = std::fopen(json_path, "rb");
+  if (!f) return MC3_EIO;
+  std::string text;
+  char buf[4096];
+  size_t n;
+  while ((n = std::fread(buf, 1, sizeof(buf), f)) > 0) text.append(buf, n);
+  std::fclose(f);
+  std::vector<TuningEntry> all;
+  if (parse_tuning_json(text, &all) != 0) return MC3_EIO;
+  for (const TuningEntry& e : all) {
+    auto& tab = ctx->eng->tuning_table;
+    for (auto it = tab.begin(); it != tab.end();)
+      it = (it->nx == e.nx && it->ny == e.ny && it->nz == e.nz && it->px == e.px && it->py == e.py)
+               ? tab.erase(it)
+               : it + 1;
+    tab.push_back(e);
+  }
+  return MC3_OK;
+}
+
+int mc3_wait(mc3_ctx* ctx, int ticket, double* latency_ms) {
+  if (!ctx || !ctx->queue) return MC3_EINVAL;
+  return ctx->queue->wait(ticket, latency_ms);
 }
 
 int mc3_estimate_ctf(mc3_ctx* ctx, const float* image, int nx, int ny, int on_device, float pix_size,
@@ -175,8 +268,168 @@ int mc3_estimate_ctf(mc3_ctx* ctx, const float* image, int nx, int ny, int on_de
 }
 
 int mc3_prefetch_movie(mc3_ctx* ctx, const mc3_movie* movie) {
-  if (!ctx || !movie) return MC3_EINVAL;
+  if (!ctx || !movie || queue_busy(ctx)) return MC3_EINVAL;
   return ctx->eng->prefetch(*movie);
+}
+
+int mc3_proposal_create(const int* spec, int n_layers, int nout, unsigned seed, int gpu,
+                        mc3_proposal** out) {
+  if (!spec || !out || n_layers < 1 || nout < 1 || spec[0] != 2) return MC3_EINVAL;
+  *out = nullptr;
+  if (cudaSetDevice(gpu) != cudaSuccess) {
+    cudaGetLastError();
+    return MC3_ECUDA;
+  }
+  mc3_proposal* p = new (std::nothrow) mc3_proposal;
+  if (!p) return MC3_ENOMEM;
+  p->gpu = gpu;
+  const int s = p->net.create(std::vector<int>(spec, spec + 5 * n_layers), nout, seed);
+  if (s != kOk) {
+    delete p;
+    return s;
+  }
+  *out = p;
+  return MC3_OK;
+}
+
+int mc3_proposal_destroy(mc3_proposal* p) {
+  if (!p) return MC3_EINVAL;
+  cudaSetDevice(p->gpu);
+  delete p;
+  return MC3_OK;
+}
+
+int mc3_proposal_num_params(mc3_proposal* p, long* n) {
+  if (!p || !n) return MC3_EINVAL;
+  *n = p->net.nparams;
+  return MC3_OK;
+}
+
+int mc3_proposal_get_params(mc3_proposal* p, float* params) {
+  if (!p || !params) return MC3_EINVAL;
+  MC3_CUDA(cudaSetDevice(p->gpu));
+  MC3_CUDA(cudaMemcpy(params, p->net.d_params, sizeof(float) * p->net.nparams, cudaMemcpyDeviceToHost));
+  return MC3_OK;
+}
+
+int mc3_proposal_set_params(mc3_proposal* p, const float* params) {
+  if (!p || !params) return MC3_EINVAL;
+  MC3_CUDA(cudaSetDevice(p->gpu));
+  MC3_CUDA(cudaMemcpy(p->net.d_params, params, sizeof(float) * p->net.nparams, cudaMemcpyHostToDevice));
+  return MC3_OK;
+}
+
+namespace {
+// Batch inputs on the device: the caller's pointers, or copies into the net's buffers.
+int proposal_inputs(mc3_proposal* p, const float* x, const float* target, int batch, int h, int w,
+                    int on_device, const float** dx, const float** dt, cudaStream_t st) {
+  MC3_TRY(p->net.ensure(batch, h, w, st));
+  if (on_device) {
+    *dx = x;
+    *dt = target;
+    return kOk;
+  }
+  const size_t nx = (size_t)batch * 2 * h * w;
+  MC3_CUDA(cudaMemcpyAsync(p->net.d_x, x, sizeof(float) * nx, cudaMemcpyHostToDevice, st));
+  *dx = p->net.d_x;
+  *dt = nullptr;
+  if (target) {
+    MC3_CUDA(cudaMemcpyAsync(p->net.d_target, target, sizeof(float) * batch * p->net.nout,
+                             cudaMemcpyHostToDevice, st));
+    *dt = p->net.d_target;
+  }
+  return kOk;
+}
+
+double batch_loss(mc3_proposal* p, int batch, int* status) {
+  std::vector<float> l(batch);
+  *status = cudaMemcpy(l.data(), p->net.d_loss, sizeof(float) * batch, cudaMemcpyDeviceToHost) ==
+                    cudaSuccess
+                ? kOk
+                : kECuda;
+  double s = 0.0;
+  for (float v : l) s += v;
+  return s;
+}
+}  // namespace
+
+int mc3_proposal_loss_grad(mc3_proposal* p, const float* x, int batch, int h, int w,
+                           const float* target, double* loss, float* grad, float* out) {
+  if (!p || !x || !target || batch < 1 || h < 1 || w < 1) return MC3_EINVAL;
+  MC3_CUDA(cudaSetDevice(p->gpu));
+  cudaStream_t st = nullptr;
+  const float *dx, *dt;
+  MC3_TRY(proposal_inputs(p, x, target, batch, h, w, 0, &dx, &dt, st));
+  MC3_TRY(p->net.run(dx, batch, h, w, dt, st));
+  MC3_CUDA(cudaStreamSynchronize(st));
+  int s = kOk;
+  const double l = batch_loss(p, batch, &s);
+  if (s) return s;
+  if (loss) *loss = l;
+  if (grad)
+    MC3_CUDA(cudaMemcpy(grad, p->net.d_grad, sizeof(float) * p->net.nparams, cudaMemcpyDeviceToHost));
+  if (out)
+    MC3_CUDA(cudaMemcpy(out, p->net.d_out, sizeof(float) * batch * p->net.nout, cudaMemcpyDeviceToHost));
+  return MC3_OK;
+}
+
+int mc3_proposal_train_step(mc3_proposal* p, const float* x, const float* target, int batch,
+                            int h, int w, int on_device, float lr, double* loss) {
+  if (!p || !x || !target || batch < 1 || h < 1 || w < 1 || !(lr > 0)) return MC3_EINVAL;
+  MC3_CUDA(cudaSetDevice(p->gpu));
+  cudaStream_t st = nullptr;
+  const float *dx, *dt;
+  MC3_TRY(proposal_inputs(p, x, target, batch, h, w, on_device, &dx, &dt, st));
+  MC3_TRY(p->net.run(dx, batch, h, w, dt, st));
+  MC3_TRY(p->net.adam_step(batch, lr, st));
+  MC3_CUDA(cudaStreamSynchronize(st));
+  int s = kOk;
+  const double l = batch_loss(p, batch, &s);
+  if (s) return s;
+  if (loss) *loss = l / batch;
+  return MC3_OK;
+}
+
+int mc3_proposal_predict(mc3_proposal* p, const float* x, int batch, int h, int w, int on_device,
+                         float* out) {
+  if (!p || !x || !out || batch < 1 || h < 1 || w < 1) return MC3_EINVAL;
+  MC3_CUDA(cudaSetDevice(p->gpu));
+  cudaStream_t st = nullptr;
+  const float *dx, *dt;
+  MC3_TRY(proposal_inputs(p, x, nullptr, batch, h, w, on_device, &dx, &dt, st));
+  MC3_TRY(p->net.run(dx, batch, h, w, nullptr, st));
+  MC3_CUDA(cudaMemcpy(out, p->net.d_out, sizeof(float) * batch * p->net.nout, cudaMemcpyDeviceToHost));
+  return MC3_OK;
+}
+
+int mc3_proposal_pair_inputs(const float* frames, int nx, int ny, int nz, const int* pairs, int n,
+                             int bin, float* x, void* stream) {
+  if (!frames || !pairs || !x || n < 1 || nz < 1 || bin < 1 || nx / bin < 1 || ny / bin < 1)
+    return MC3_EINVAL;
+  for (int i = 0; i < 2 * n; ++i)
+    if (pairs[i] < 0 || pairs[i] >= nz) return MC3_EINVAL;
+  cudaStream_t st = as_stream(stream);
+  int* d = nullptr;
+  MC3_CUDA(cudaMalloc(&d, sizeof(int) * 2 * n));
+  int s = cudaMemcpyAsync(d, pairs, sizeof(int) * 2 * n, cudaMemcpyHostToDevice, st) == cudaSuccess
+              ? kOk
+              : kECuda;
+  if (s == kOk) s = proposal::pair_inputs(frames, nx, ny, (long)nx * ny, d, n, bin, x, st);
+  if (s == kOk && cudaStreamSynchronize(st) != cudaSuccess) s = kECuda;
+  cudaFree(d);
+  return s;
+}
+
+int mc3_set_first_iterate(mc3_ctx* ctx, const float* global_xy, int nz, int max_iter) {
+  if (!ctx || queue_busy(ctx)) return MC3_EINVAL;
+  if (!global_xy) {
+    ctx->eng->first_iterate.clear();
+    return MC3_OK;
+  }
+  if (nz < 1) return MC3_EINVAL;
+  ctx->eng->first_iterate.assign(global_xy, global_xy + 2 * (size_t)nz);
+  ctx->eng->first_iterate_max = max_iter > 0 ? max_iter : 3;
+  return MC3_OK;
 }
 
 int mc3_set_alignment(mc3_ctx* ctx, const mc3_alignment* aln) {
@@ -260,6 +513,28 @@ int mc3_frame_integration_tables(const int* group_size, const int* int_size, con
 }
 
 // ---- components ----
+int mc3_rfft_rows(const float* in, int in_pitch, float* out, int out_pitch, int nx, int n_rows,
+                  int method, void* stream) {
+  if (!in || !out || nx < 2 || (nx & 1) || n_rows < 1 || in_pitch < nx ||
+      out_pitch < nx / 2 + 1 || (method != 0 && method != 1))
+    return MC3_EINVAL;
+  cudaStream_t st = as_stream(stream);
+  Batch b{1, 1, 0, nullptr, 0};
+  int s = method == 1 ? dft_rows_r2c(in, in_pitch, reinterpret_cast<float2*>(out), out_pitch, nx,
+                                     n_rows, b, 1.0f, st)
+                      : row_r2c(in, in_pitch, reinterpret_cast<float2*>(out), out_pitch, nx,
+                                n_rows, b, 1.0f, st);
+  if (s) return s;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return MC3_ECUDA;
+  if (method == 1) {
+    int flag = 0;
+    s = dft_gemm_error(true, &flag);
+    if (s) return s;
+    if (flag) return MC3_ETIMEOUT;
+  }
+  return MC3_OK;
+}
+
 int mc3_fft_forward(float* frames, int nx, int ny, int nz, int normalise, void* stream) {
   if (!frames || nx < 2 || (nx & 1) || ny < 1 || nz < 1) return MC3_EINVAL;
   const int cmpX = nx / 2 + 1;

@@ -6,6 +6,7 @@
 #include <cstdlib>
 
 #include "kernels.cuh"
+#include "tuning.h"
 
 namespace mc3 {
 
@@ -395,10 +396,7 @@ static void launch_gather(int W, int H, cudaStream_t st, const float* in, long i
                           const uint8_t* bad, const uint8_t* clean, int P, int nb) {
   // two pixels per thread up to 36 patches (MC3_GATHER_PX=1 forces one,
   // for A/B runs); one above (register budget of the weights)
-  static const bool one = [] {
-    const char* e = getenv("MC3_GATHER_PX");
-    return e && e[0] == '1';
-  }();
+  const bool one = active_tuning().gather_px == 1;
   if (PMAX <= 36 && !one) {
     dim3 grid(ceil_div(W, 256), H);
     k_local_gather<PMAX, EXACT, 2><<<grid, 128, 0, st>>>(in, in_stride, out, out_stride, W, H,

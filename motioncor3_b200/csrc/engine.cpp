@@ -2,6 +2,8 @@
 // (CProcessThread.cpp:82-107) on one GPU stream.
 #include "engine.h"
 
+#include "dft_gemm.cuh"
+
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -190,6 +192,14 @@ int Engine::prefetch(const mc3_movie& mv) {
   return kOk;
 }
 
+void Engine::drop_prefetched() {
+  cudaSetDevice(device);
+  cudaStreamSynchronize(copy_stream);
+  cudaStreamSynchronize(copy_stream2);
+  for (int i = 0; i < 2; ++i) cudaEventRecord(slot_free[i], copy_stream);
+  n_pending = 0;
+}
+
 int Engine::set_stream(cudaStream_t s) {
   stream = s ? s : own_stream;
   return kOk;
@@ -247,24 +257,7 @@ int Engine::set_defects(const unsigned char* mask, int w, int h) {
 
 int Engine::plan(int w, int h, int n, mc3_plan_info* info) {
   Geometry g;
-  if (fmint && n != (fmint_rendered ? fmint_tab.count() : fmint_raw)) return kEInval;
-  MC3_TRY(g.compute(w, h, fmint ? fmint_tab.count() : n, prm, fmint && fmint_dose));
-  info->n_sums = g.nSums;
-  info->n_patches = g.P;
-  info->xcf_size[0] = (g.xcfCmpX - 1) * 2;
-  info->xcf_size[1] = g.xcfCmpY;
-  info->patch_size[0] = g.patch ? (g.patCmpX - 1) * 2 : 0;
-  info->patch_size[1] = g.patch ? g.patCmpY : 0;
-  info->xcf_bin[0] = g.xcfBin[0];
-  info->xcf_bin[1] = g.xcfBin[1];
-  info->out_size[0] = g.outW;
-  info->out_size[1] = g.outH;
-  info->n_frames = g.N;
-  size_t cmp = (size_t)g.cmpX * g.cmpY * sizeof(float2);
-  size_t xcf = (size_t)g.xcfCmpX * g.xcfCmpY * sizeof(float2);
-  size_t bytes = cmp * g.N + xcf * g.N + cmp * (g.nSums + 2) + (size_t)g.W * g.H * 4 * g.N;
-  if (g.patch) bytes += (size_t)g.P * g.N * g.patCmpX * g.patCmpY * sizeof(float2) + 2 * cmp * 32;
-  info->device_bytes = bytes;
+  MC3_TRY(geometry(w, h, n, info, &g));
   // Reserve the large per-movie buffers now, as the reference creates its
   // buffer pool before processing (CMain::mCreateBufferPool, CMain.cpp:400-427);
   // process() reuses them (grow-only, same sizes).
@@ -291,12 +284,37 @@ int Engine::plan(int w, int h, int n, mc3_plan_info* info) {
   return kOk;
 }
 
+int Engine::geometry(int w, int h, int n, mc3_plan_info* info, Geometry* out) const {
+  Geometry g;
+  if (fmint && n != (fmint_rendered ? fmint_tab.count() : fmint_raw)) return kEInval;
+  MC3_TRY(g.compute(w, h, fmint ? fmint_tab.count() : n, prm, fmint && fmint_dose));
+  info->n_sums = g.nSums;
+  info->n_patches = g.P;
+  info->xcf_size[0] = (g.xcfCmpX - 1) * 2;
+  info->xcf_size[1] = g.xcfCmpY;
+  info->patch_size[0] = g.patch ? (g.patCmpX - 1) * 2 : 0;
+  info->patch_size[1] = g.patch ? g.patCmpY : 0;
+  info->xcf_bin[0] = g.xcfBin[0];
+  info->xcf_bin[1] = g.xcfBin[1];
+  info->out_size[0] = g.outW;
+  info->out_size[1] = g.outH;
+  info->n_frames = g.N;
+  size_t cmp = (size_t)g.cmpX * g.cmpY * sizeof(float2);
+  size_t xcf = (size_t)g.xcfCmpX * g.xcfCmpY * sizeof(float2);
+  size_t bytes = cmp * g.N + xcf * g.N + cmp * (g.nSums + 2) + (size_t)g.W * g.H * 4 * g.N;
+  if (g.patch) bytes += (size_t)g.P * g.N * g.patCmpX * g.patCmpY * sizeof(float2) + 2 * cmp * 32;
+  info->device_bytes = bytes;
+  if (out) *out = g;
+  return kOk;
+}
+
 // ---------------------------------------------------------------------------
 // Batched CIterativeAlign::mAlignStack (Align/CIterativeAlign.cpp:99-156).
 int Engine::align_stacks(const float2* spec, long stack_stride, int nstack, int cmpX, int cmpY,
                          int N, const host::FrameGroups& grp, float bf0, float tol,
                          std::vector<host::StackShift>& shifts, std::vector<int>& iters,
-                         std::vector<std::vector<float>>& errors) {
+                         std::vector<std::vector<float>>& errors, const float* init,
+                         int max_iter_init, bool* converged) {
   const int G = grp.count();
   const int imgX = (cmpX - 1) * 2;
   AlignDims d;
@@ -323,11 +341,14 @@ int Engine::align_stacks(const float2* spec, long stack_stride, int nstack, int 
 
   std::vector<host::IterState> st(nstack);
   for (auto& s : st) s.start(N, G, bf0);
+  // a warm start (the learned proposal's first iterate) caps the iterations
+  const int max_iter = init ? std::min(max_iter_init, prm.iter) : prm.iter;
+  if (init) st[0].start_from(init, grp, N, bf0);
   std::vector<int> active(nstack);
   for (int i = 0; i < nstack; ++i) active[i] = i;
   std::vector<float2> hsh((size_t)nstack * N);
   std::vector<float2> hg((size_t)nstack * G);
-  for (int it = 0; it < prm.iter && !active.empty(); ++it) {
+  for (int it = 0; it < max_iter && !active.empty(); ++it) {
     const int A = (int)active.size();
     d.A = A;
     for (int a = 0; a < A; ++a) {
@@ -352,11 +373,12 @@ int Engine::align_stacks(const float2* spec, long stack_stride, int nstack, int 
     std::vector<int> next;
     for (int a = 0; a < A; ++a) {
       host::IterState& s = st[active[a]];
-      const bool fin = s.step(reinterpret_cast<const float*>(&hg[(size_t)a * G]), grp, it, prm.iter, tol);
+      const bool fin = s.step(reinterpret_cast<const float*>(&hg[(size_t)a * G]), grp, it, max_iter, tol);
       if (!fin) next.push_back(active[a]);
     }
     active.swap(next);
   }
+  if (converged) *converged = st[0].max_err < tol && st[0].iterations > 1;
   shifts.resize(nstack);
   iters.resize(nstack);
   errors.resize(nstack);
@@ -493,7 +515,75 @@ int Engine::write_stack(float2* spec, bool phase, const Geometry& g, const host:
 }
 
 // ---------------------------------------------------------------------------
+Tuning Engine::tuning_for(int w, int h, int n) const {
+  // same frame size and patch grid; the nearest frame count
+  const TuningEntry* best = nullptr;
+  for (const TuningEntry& e : tuning_table)
+    if (e.nx == w && e.ny == h && e.px == prm.patch[0] && e.py == prm.patch[1] &&
+        (!best || std::abs(e.nz - n) < std::abs(best->nz - n)))
+      best = &e;
+  return best ? best->best : default_tuning();
+}
+
+int Engine::autotune(int w, int h, int n, TuningEntry* out) {
+  MC3_CUDA(cudaSetDevice(device));
+  mc3_plan_info info;
+  MC3_TRY(plan(w, h, n, &info));
+  DevBuf frames, sums;
+  MC3_TRY(frames.ensure(sizeof(float) * (size_t)w * h * n));
+  MC3_TRY(sums.ensure(sizeof(float) * (size_t)info.out_size[0] * info.out_size[1] * info.n_sums));
+  MC3_TRY(synthetic_counts(frames.as<float>(), (long)w * h * n, stream));
+  mc3_movie mv{frames.p, 2, w, h, n, 1};
+  mc3_result r;
+  std::memset(&r, 0, sizeof(r));
+  r.sums = sums.as<float>();
+  r.sums_on_device = 1;
+  const bool had_gain = has_gain;
+  has_gain = false;  // the tuner's frames need no gain
+  TuningEntry e;
+  e.nx = w;
+  e.ny = h;
+  e.nz = n;
+  e.px = prm.patch[0];
+  e.py = prm.patch[1];
+  int st = kOk;
+  for (const Tuning& t : tuning_candidates()) {
+    TuningScope scope(t);
+    double best = 1e30;
+    for (int rep = 0; rep < 3 && st == kOk; ++rep) {  // first run: warm-up
+      st = process_with(mv, &r, t);
+      if (rep > 0 && r.time_ms < best) best = r.time_ms;
+    }
+    if (st != kOk) break;
+    e.cand.push_back(t);
+    e.cand_ms.push_back(best);
+    if (e.cand.size() == 1 || best < e.best_ms) {
+      e.best = t;
+      e.best_ms = best;
+    }
+  }
+  has_gain = had_gain;
+  if (st != kOk) return st;
+  for (auto it = tuning_table.begin(); it != tuning_table.end();)
+    it = (it->nx == w && it->ny == h && it->nz == n && it->px == e.px && it->py == e.py)
+             ? tuning_table.erase(it)
+             : it + 1;
+  tuning_table.push_back(e);
+  if (out) *out = e;
+  return kOk;
+}
+
 int Engine::process(const mc3_movie& mv, mc3_result* out) {
+  Geometry g0;
+  mc3_plan_info info;
+  const Tuning t = geometry(mv.nx, mv.ny, mv.nz, &info, &g0) == kOk
+                       ? tuning_for(mv.nx, mv.ny, mv.nz)
+                       : default_tuning();
+  return process_with(mv, out, t);
+}
+
+int Engine::process_with(const mc3_movie& mv, mc3_result* out, const Tuning& tune) {
+  TuningScope scope(tune);
   MC3_CUDA(cudaSetDevice(device));
   if (prm.align == 0) return kEUnsupported;
   if (!mv.frames) return kEInval;
@@ -633,7 +723,30 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
     xs[0].setup(N);
     it0.assign(1, 0);
     err0.assign(1, std::vector<float>());
+  } else if ((int)first_iterate.size() == 2 * N) {
+    // Warm start from a first iterate (full-frame pixels -> alignment pixels),
+    // at most first_iterate_max iterations; the plain aligner runs from zero
+    // when that has not converged (the fallback and the judge of the proposal).
+    std::vector<float> init(2 * N);
+    for (int f = 0; f < N; ++f) {
+      init[2 * f] = first_iterate[2 * f] / g.xcfBin[0];
+      init[2 * f + 1] = first_iterate[2 * f + 1] / g.xcfBin[1];
+    }
+    first_iterate.clear();
+    bool conv = false;
+    MC3_TRY(align_stacks(d_xcf.as<float2>(), (long)nxcf * N, 1, g.xcfCmpX, g.xcfCmpY, N, G0,
+                         prm.bft[0], tol, xs, it0, err0, init.data(), first_iterate_max, &conv));
+    first_iterate_used = 1;
+    if (!conv) {
+      const int warm_iters = it0[0];
+      MC3_TRY(align_stacks(d_xcf.as<float2>(), (long)nxcf * N, 1, g.xcfCmpX, g.xcfCmpY, N, G0,
+                           prm.bft[0], tol, xs, it0, err0));
+      it0[0] += warm_iters;  // every iteration run counts
+      first_iterate_used = 2;
+    }
   } else {
+    first_iterate_used = 0;
+    first_iterate.clear();
     MC3_TRY(align_stacks(d_xcf.as<float2>(), (long)nxcf * N, 1, g.xcfCmpX, g.xcfCmpY, N, G0,
                          prm.bft[0], tol, xs, it0, err0));
   }
@@ -719,7 +832,12 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
       MC3_CUDA(cudaMemcpyAsync(d_patoff.p, off.data(), sizeof(long) * P, cudaMemcpyHostToDevice, st));
       const int pw = (g.patCmpX - 1) * 2, ph = g.patCmpY;
       Batch bp{P * N, N, (long)nxcf * 2, d_patoff.as<long>(), (long)npat};
-      MC3_TRY(row_r2c(d_xcf.as<float>(), 2 * g.xcfCmpX, d_pat.as<float2>(), g.patCmpX, pw, ph, bp, 1.0f, st));
+      if (prm.dft_gemm && dft_rows_supported(pw))  // split-BF16 DFT GEMM on the tensor cores
+        MC3_TRY(dft_rows_r2c(d_xcf.as<float>(), 2 * g.xcfCmpX, d_pat.as<float2>(), g.patCmpX, pw,
+                             ph, bp, 1.0f, st));
+      else
+        MC3_TRY(row_r2c(d_xcf.as<float>(), 2 * g.xcfCmpX, d_pat.as<float2>(), g.patCmpX, pw, ph,
+                        bp, 1.0f, st));
       Batch bpc{P * N, P * N, (long)npat, nullptr, (long)npat};
       ColOps fwd{};
       fwd.dir = -1;
@@ -730,6 +848,14 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
       std::vector<host::StackShift> ps;
       MC3_TRY(align_stacks(d_pat.as<float2>(), (long)npat * N, P, g.patCmpX, g.patCmpY, N, G1,
                            prm.bft[1], tol, ps, patIters, patErr));
+      if (prm.dft_gemm) {  // the stream was synchronised by the alignment
+        int flag = 0;
+        MC3_TRY(dft_gemm_error(true, &flag));
+        if (flag) {
+          last_error = "a bounded wait of the DFT-GEMM kernel gave up";
+          return kETimeout;
+        }
+      }
       patShift.assign((size_t)N * P * 2, 0.0f);
       patCent.assign((size_t)P * 2, 0.0f);
       for (int p = 0; p < P; ++p) {
@@ -960,6 +1086,7 @@ int Engine::process(const mc3_movie& mv, mc3_result* out) {
   if (out) {
     out->n_sums = g.nSums;
     out->n_patches = g.P;
+    out->first_iterate = first_iterate_used;
     out->time_ms = ms;
     if (out->global_shifts)
       for (int f = 0; f < N; ++f) {

@@ -10,6 +10,7 @@
 #include "../../include/mc3.h"
 #include "host_align.h"
 #include "kernels.cuh"
+#include "tuning.h"
 
 namespace mc3 {
 
@@ -64,10 +65,23 @@ class Engine {
   int set_dark(const float* dark, int w, int h, bool on_device);
   int set_defects(const unsigned char* mask, int w, int h);
   int plan(int w, int h, int n, mc3_plan_info* info);
+  // Autotuner: times every kernel variant on a synthetic movie of this size
+  // with the context's options, keeps the fastest in the table.
+  int autotune(int w, int h, int n, TuningEntry* out);
+  // The table's choice for a movie size: the entry of the same frame size
+  // and patch grid with the nearest frame count (the defaults when absent).
+  Tuning tuning_for(int w, int h, int n) const;
+  std::vector<TuningEntry> tuning_table;
+  // Sizes of a movie (no allocation, no device work).
+  int geometry(int w, int h, int n, mc3_plan_info* info, Geometry* g = nullptr) const;
   int process(const mc3_movie& mv, mc3_result* out);
+  // process() with the given kernel variants active.
+  int process_with(const mc3_movie& mv, mc3_result* out, const Tuning& t);
   // Starts the host->device copy of a later movie's raw frames on the copy
   // stream (at most two outstanding); process() consumes them in order.
   int prefetch(const mc3_movie& mv);
+  // Waits for the outstanding prefetch copies and forgets them.
+  void drop_prefetched();
   // Known alignment used instead of measuring (NULL clears it).
   int set_alignment(const mc3_alignment* aln);
   int set_frame_integration(const mc3_frame_integration* fi);
@@ -79,11 +93,18 @@ class Engine {
   int write_stack(float2* spec, bool phase, const Geometry& g, const host::FmInt& fi,
                   mc3_result* out);
 
-  // Batched CIterativeAlign over `nstack` stacks of N spectra each.
+  // Batched CIterativeAlign over `nstack` stacks of N spectra each.  init
+  // (optional): a first iterate [N][2] of the first stack's shifts, and
+  // max_iter_init its iteration cap.
   int align_stacks(const float2* spec, long stack_stride, int nstack, int cmpX, int cmpY, int N,
                    const host::FrameGroups& grp, float bf0, float tol,
                    std::vector<host::StackShift>& shifts, std::vector<int>& iters,
-                   std::vector<std::vector<float>>& errors);
+                   std::vector<std::vector<float>>& errors, const float* init = nullptr,
+                   int max_iter_init = 0, bool* converged = nullptr);
+  // First iterate of the next movie's full-frame alignment (mc3_set_first_iterate).
+  std::vector<float> first_iterate;  // [nz][2] full-frame pixels; empty: cold start
+  int first_iterate_max = 3;
+  int first_iterate_used = 0;        // last movie: 1 warm start kept, 2 fell back to cold
   // Sums of spectra shifted by -shifts (global correction) into d_sums_.
   int global_sums(const float2* spec, int N, const host::StackShift& fs, const Geometry& g);
 

@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "fft.cuh"
+#include "tuning.h"
 
 namespace mc3 {
 
@@ -514,13 +515,7 @@ int launch_col_fft_ct(const float2* in, float2* out, long pitch, int cmpX, const
   return kOk;
 }
 // MC3_FFT_COL_WIDE=1 selects the wide 4096-point column form (A/B runs).
-bool col_wide() {
-  static const bool on = [] {
-    const char* e = getenv("MC3_FFT_COL_WIDE");
-    return e && e[0] == '1';
-  }();
-  return on;
-}
+bool col_wide() { return active_tuning().col_wide != 0; }
 // MC3_FFT_RUNTIME_PLAN=1 keeps the runtime-plan in-place kernels (A/B runs).
 bool ct_off() {
   static const bool off = [] {

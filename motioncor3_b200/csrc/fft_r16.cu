@@ -6,6 +6,7 @@
 
 #include "fft.cuh"
 #include "fft_r16.cuh"
+#include "tuning.h"
 
 namespace mc3 {
 
@@ -16,28 +17,25 @@ constexpr int kR16Budget = 72 * 1024;
 __host__ __device__ constexpr int r16_batch(int n) { return kR16Threads / (n / 16); }
 }  // namespace
 
-bool r16_enabled() {
-  static const bool on = [] {
-    const char* e = getenv("MC3_FFT_R16");
-    return !(e && e[0] == '0');
-  }();
-  return on;
-}
+bool r16_enabled() { return active_tuning().fft_r16 != 0; }
 
 // ---------------------------------------------------------------------
 // Column pass: NB adjacent columns per CTA; thread t -> column t % NB,
 // slot t / NB, so a warp's loads cover NB adjacent columns of 32/NB rows.
 // ---------------------------------------------------------------------
 // PHASE / CROP: the phase-shift prologue and the crop epilogue are compiled
-// in only where used.
-template <int H, bool PHASE, bool CROP>
-__global__ void __launch_bounds__(kR16Threads, 2) k_col_fft_r16(const float2* in, float2* out,
+// in only where used.  T threads: 512 (two CTAs per SM) or 1024 (the wide
+// form: twice the columns per CTA, so that each warp's loads and stores
+// cover whole 32-byte sectors at 4096 points; one CTA per SM).
+template <int H, bool PHASE, bool CROP, int T = kR16Threads>
+__global__ void __launch_bounds__(T, kR16Threads * 2 / T) k_col_fft_r16(const float2* in, float2* out,
                                                                 long pitch, int cmpX, Batch bt,
                                                                 const float2* __restrict__ tw,
                                                                 ColOps ops) {
-  constexpr int NB = r16_batch(H);
+  constexpr int NB = T / (H / 16);
   constexpr int LD = spad16_col_stride(H, NB);
-  static_assert(NB * LD * (int)sizeof(float2) <= kR16Budget, "shared memory budget");
+  static_assert(NB * LD * (int)sizeof(float2) <= (T == kR16Threads ? kR16Budget : 2 * kR16Budget),
+                "shared memory budget");
   extern __shared__ float2 sm[];
   const int item = blockIdx.y;
   const int c = threadIdx.x % NB;
@@ -171,18 +169,18 @@ __global__ void __launch_bounds__(kR16Threads, 2) k_row_c2r_r16(const float2* in
 // Launchers (compile-time lengths 256..4096 columns, 128..2048 row pairs).
 // ---------------------------------------------------------------------
 namespace {
-template <int H>
+template <int H, int T = kR16Threads>
 int launch_col(const float2* in, float2* out, long pitch, int cmpX, const Batch& b,
                const float2* tw, const ColOps& ops, const char* name, cudaStream_t st) {
-  constexpr int NB = r16_batch(H);
+  constexpr int NB = T / (H / 16);
   const size_t smem = (size_t)NB * spad16_col_stride(H, NB) * sizeof(float2);
   dim3 grid(ceil_div(cmpX, NB), b.items);
   prof::Scope ps(name, (double)b.items * ((double)cmpX * H * 16.0 + (ops.crop ? (double)ops.crop_x * ops.crop_y * 8.0 : 0.0)), st);
   const bool phase = ops.ex && ops.ey, crop = ops.crop != nullptr;
 #define MC3_COLK(P, C)                                                                   \
   {                                                                                      \
-    MC3_TRY(set_smem_attr(k_col_fft_r16<H, P, C>, smem));                                \
-    k_col_fft_r16<H, P, C><<<grid, kR16Threads, smem, st>>>(in, out, pitch, cmpX, b, tw, ops); \
+    MC3_TRY(set_smem_attr(k_col_fft_r16<H, P, C, T>, smem));                             \
+    k_col_fft_r16<H, P, C, T><<<grid, T, smem, st>>>(in, out, pitch, cmpX, b, tw, ops);  \
   }
   if (phase && crop) MC3_COLK(true, true)
   else if (phase) MC3_COLK(true, false)
@@ -232,7 +230,11 @@ int col_fft_r16(const float2* in, float2* out, long pitch, int cmpX, int H, cons
     case 512: return launch_col<512>(in, out, pitch, cmpX, b, d.tw, ops, "k_col_fft_r16<512>", st);
     case 1024: return launch_col<1024>(in, out, pitch, cmpX, b, d.tw, ops, "k_col_fft_r16<1024>", st);
     case 2048: return launch_col<2048>(in, out, pitch, cmpX, b, d.tw, ops, "k_col_fft_r16<2048>", st);
-    default: return launch_col<4096>(in, out, pitch, cmpX, b, d.tw, ops, "k_col_fft_r16<4096>", st);
+    default:
+      if (active_tuning().col_wide)
+        return launch_col<4096, 2 * kR16Threads>(in, out, pitch, cmpX, b, d.tw, ops,
+                                                 "k_col_fft_r16w<4096>", st);
+      return launch_col<4096>(in, out, pitch, cmpX, b, d.tw, ops, "k_col_fft_r16<4096>", st);
   }
 }
 

@@ -482,6 +482,23 @@ void IterState::start(int n_frames, int n_groups, float bf) {
   errors.clear();
 }
 
+void IterState::start_from(const float* init, const FrameGroups& g, int n_frames, float bf) {
+  start(n_frames, g.count(), bf);
+  for (int f = 0; f < n_frames; ++f) {
+    tmp.x(f) = init[2 * f];
+    tmp.y(f) = init[2 * f + 1];
+  }
+  for (int k = 0; k < g.count(); ++k) {
+    double sx = 0.0, sy = 0.0;
+    for (int i = 0; i < g.size[k]; ++i) {
+      sx += init[2 * (g.start[k] + i)];
+      sy += init[2 * (g.start[k] + i) + 1];
+    }
+    total.x(k) = (float)(sx / g.size[k]);
+    total.y(k) = (float)(sy / g.size[k]);
+  }
+}
+
 bool IterState::step(const float* gxy, const FrameGroups& g, int it, int max_iter, float tol) {
   const int ng = grp.n;
   max_err = 0.0f;

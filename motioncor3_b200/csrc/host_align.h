@@ -87,6 +87,9 @@ struct IterState {
   bool done = false;
   std::vector<float> errors;
   void start(int n_frames, int n_groups, float bf);
+  // start() from a first iterate of the per-frame shifts init[n_frames][2]:
+  // tmp = init, each group's total = the mean of its frames' shifts.
+  void start_from(const float* init, const FrameGroups& g, int n_frames, float bf);
   // Consumes the group shifts measured in iteration `it`; returns true when
   // the stack has finished iterating.
   bool step(const float* grp_xy, const FrameGroups& g, int it, int max_iter, float tol);

@@ -30,6 +30,9 @@ int detect_bad_pixels(const float* sum, int W, int H, float* cc_buf, float* d_pa
 int correct_bad_pixels(float* frames, long fr_stride, int N, const uint8_t* bad, int W, int H,
                        int* d_count, int2* d_list, cudaStream_t st);
 
+// Synthetic counts 0..3 (pixel-index hash) for the autotuner's movie.
+int synthetic_counts(float* f, long n, cudaStream_t st);
+
 // ---- align.cu ----
 // Separable phase tables for shifts sh[item] = (sx, sy) in pixels of an
 // Nx x Ny image: ex[item][kx] = e^{i 2 pi kx sx / Nx}, ey[item][ky] =

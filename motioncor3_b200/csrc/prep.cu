@@ -372,4 +372,22 @@ int correct_bad_pixels(float* frames, long fr_stride, int N, const uint8_t* bad,
   return kOk;
 }
 
+// Synthetic counts 0..3 (a hash of the pixel index) for the autotuner's movie.
+__global__ void k_synthetic_counts(float* f, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x) {
+    unsigned v = (unsigned)i * 2654435761u;
+    v ^= v >> 15;
+    v *= 2246822519u;
+    v ^= v >> 13;
+    f[i] = (float)(v & 3u);
+  }
+}
+
+int synthetic_counts(float* f, long n, cudaStream_t st) {
+  k_synthetic_counts<<<1184, 256, 0, st>>>(f, n);
+  MC3_CHECK_LAUNCH("k_synthetic_counts");
+  return kOk;
+}
+
 }  // namespace mc3

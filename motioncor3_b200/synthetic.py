@@ -86,10 +86,13 @@ def _shift_fourier(img: np.ndarray, dx: float, dy: float) -> np.ndarray:
 
 def make_movie(nx: int, ny: int, nz: int, dose: float = 1.0, seed: int = 0, gain: bool = False,
                local: bool = False, local_amp: float = 2.0, n_blobs: int = 200,
-               backend: str = "numpy", device: str = "cuda") -> Movie:
+               backend: str = "numpy", device: str = "cuda", drift_step: float = 0.7,
+               jump: float = 3.0) -> Movie:
+    """drift_step: standard deviation of the random walk's steps (px); jump:
+    size of the early jump over the first four frames (px)."""
     rng = np.random.default_rng(seed)
     truth = truth_image(nx, ny, rng, n_blobs=n_blobs)
-    drift = drift_trajectory(nz, rng)
+    drift = drift_trajectory(nz, rng, step=drift_step, jump=jump)
     coef = local_coefficients(rng, local_amp) if local else None
     g = rng.uniform(0.9, 1.1, size=(ny, nx)).astype(np.float32) if gain else None
     if backend == "torch":

@@ -265,3 +265,29 @@ def test_cli_ctf_gate(mc3lib, tmp_path):
     assert "outside the implemented path" not in on.stderr  # the CTF tags are parsed
     nopix = subprocess.run(base, capture_output=True, text=True, timeout=60)
     assert "Pixel size:   0.000000" in nopix.stdout
+
+
+def test_queue_entry_points_check_their_arguments(mc3lib):
+    import ctypes
+    from motioncor3_b200 import api
+    L = mc3lib
+    t = ctypes.c_int()
+    assert L.mc3_submit(None, None, None, ctypes.byref(t)) == api.MC3_EINVAL
+    assert L.mc3_wait(None, 1, None) == api.MC3_EINVAL
+    assert L.mc3_rfft_rows(None, 8, None, 5, 8, 1, 1, None) == api.MC3_EINVAL
+
+
+def test_proposal_and_warm_start_entry_points_check_their_arguments(mc3lib):
+    import ctypes
+    from motioncor3_b200 import api
+    L = mc3lib
+    h = ctypes.c_void_p()
+    spec = (ctypes.c_int * 5)(3, 4, 3, 2, 1)   # the first layer must take the two frames
+    assert L.mc3_proposal_create(spec, 1, 2, 0, 0, ctypes.byref(h)) == api.MC3_EINVAL
+    assert L.mc3_proposal_create(None, 1, 2, 0, 0, ctypes.byref(h)) == api.MC3_EINVAL
+    assert L.mc3_proposal_destroy(None) == api.MC3_EINVAL
+    assert L.mc3_proposal_predict(None, None, 1, 8, 8, 0, None) == api.MC3_EINVAL
+    assert L.mc3_proposal_pair_inputs(None, 8, 8, 2, None, 1, 2, None, None) == api.MC3_EINVAL
+    assert L.mc3_set_first_iterate(None, None, 0, 0) == api.MC3_EINVAL
+    assert L.mc3_autotune(None, 64, 64, 4, None, None) == api.MC3_EINVAL
+    assert L.mc3_load_tuning(None, b"x.json") == api.MC3_EINVAL

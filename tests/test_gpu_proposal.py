@@ -1,0 +1,110 @@
+"""The learned shift proposal on the GPU (mc3_proposal_*, csrc/proposal.cu)
+and its use as the warm start of the full-frame alignment
+(mc3_set_first_iterate).
+
+* The device forward and backward (FP32) against the FP64 oracle
+  (oracle/cnn_oracle.cpp) with the same parameters: outputs, loss and every
+  gradient entry.
+* Training on the GPU with the library's kernels on frame pairs of
+  synthetic movies whose labels are the plain aligner's own shifts; on
+  held-out movies the proposal's error against the plain aligner is stated
+  and must beat predicting no motion by a wide margin.
+* The warm start: with the proposal's first iterate the aligner runs at most
+  three iterations, keeps the plain aligner's shifts within 0.05 px (falling
+  back to the plain aligner when it has not converged), and the iterations
+  used are stated beside the cold start's.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SPEC = [(2, 8, 5, 2, 2), (8, 16, 3, 2, 1), (16, 16, 3, 2, 1), (16, 16, 3, 2, 1)]
+
+
+@pytest.mark.parametrize("layers,size,batch", [
+    ([(2, 4, 3, 2, 1), (4, 6, 3, 2, 1)], 12, 3),
+    ([(2, 3, 4, 3, 0), (3, 5, 3, 1, 1)], 17, 2),
+    (SPEC, 64, 4)])
+def test_device_gradients_match_fp64_oracle(mc3lib, oracle, torch_cuda, layers, size, batch):
+    from motioncor3_b200 import api
+    dev = api.ShiftProposal(layers, 5, seed=3)
+    ref = oracle.ShiftNet(layers, 5, seed=3)
+    ref.set_params(dev.params().astype(np.float64))  # the device's FP32 parameters exactly
+    rng = np.random.default_rng(size)
+    x = rng.standard_normal((batch, 2, size, size)).astype(np.float32)
+    t = rng.standard_normal((batch, 5)).astype(np.float32)
+    g_ref = np.zeros(ref.n_params)
+    loss_ref = sum(ref.loss_grad(x[i].astype(np.float64), t[i].astype(np.float64), g_ref)
+                   for i in range(batch))
+    out_ref = np.array([ref.forward(x[i].astype(np.float64)) for i in range(batch)])
+    loss, g, out = dev.loss_grad(x, t)
+    err_g = np.abs(g - g_ref).max() / np.abs(g_ref).max()
+    print(f"{len(layers)} layers, {size}^2 x {batch}: loss {loss:.6g} vs {loss_ref:.6g}, "
+          f"max gradient error {err_g:.2e} of the largest entry")
+    assert abs(loss - loss_ref) <= 1e-5 * max(1.0, abs(loss_ref))
+    assert np.abs(out - out_ref).max() <= 1e-5 * max(1.0, np.abs(out_ref).max())
+    assert err_g <= 1e-4
+
+
+def _movies(n, seed0, nz=16, size=256):
+    """Movies with larger, jumpier drifts than the default generator's."""
+    from motioncor3_b200 import synthetic as S
+    return [S.make_movie(size, size, nz, dose=4.0, seed=seed0 + i, drift_step=1.5, jump=6.0)
+            for i in range(n)]
+
+
+def _pairs_and_labels(torch, api, movies, shifts, bin_):
+    """Inputs (frame f, central frame) and targets s_f - s_ref (px / 4)."""
+    xs, ts = [], []
+    for m, s in zip(movies, shifts):
+        nz, ny, nx = m.frames.shape
+        ref = nz // 2
+        pairs = np.array([[f, ref] for f in range(nz)], np.int32)
+        fr = torch.from_numpy(m.frames).cuda()
+        x = torch.empty((nz, 2, ny // bin_, nx // bin_), dtype=torch.float32, device="cuda")
+        api.ShiftProposal.pair_inputs(fr, pairs, bin_, x)
+        xs.append(x)
+        ts.append(torch.from_numpy(((s - s[ref]) / 4.0).astype(np.float32)).cuda())
+    return torch.cat(xs), torch.cat(ts)
+
+
+def test_trained_proposal_warm_starts_the_aligner(mc3lib, torch_cuda):
+    torch = torch_cuda
+    from motioncor3_b200 import api
+    p = api.Params(iter=15, tol=0.05, bft=(150, 100), pix_size=1.0)
+    train, test = _movies(48, 500), _movies(6, 900)
+    with api.MotionCor3(p) as mc:
+        lab_tr = [mc.process(m.frames).global_shifts for m in train]
+        cold = [mc.process(m.frames) for m in test]
+    bin_ = 4
+    xtr, ttr = _pairs_and_labels(torch, api, train, lab_tr, bin_)
+    xte, tte = _pairs_and_labels(torch, api, test, [c.global_shifts for c in cold], bin_)
+    net = api.ShiftProposal(SPEC, 2, seed=11)
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    for ep in range(40):
+        perm = torch.randperm(xtr.shape[0], device="cuda", generator=gen)
+        for b in range(0, xtr.shape[0], 32):
+            i = perm[b:b + 32]
+            net.train_step(xtr[i].contiguous(), ttr[i].contiguous(), lr=2e-3)
+    pred = net.predict(xte.contiguous()) * 4.0
+    truth = tte.cpu().numpy() * 4.0
+    err = float(np.sqrt(np.mean((pred - truth) ** 2)))
+    base = float(np.sqrt(np.mean(truth ** 2)))
+    print(f"proposal on held-out movies: {err:.3f} px RMS against the plain aligner's shifts "
+          f"(no-motion guess {base:.3f} px)")
+    assert err < 0.5 * base
+    warm_iters, cold_iters, worst = [], [], 0.0
+    with api.MotionCor3(p) as mc:
+        for k, (m, c) in enumerate(zip(test, cold)):
+            nz = m.frames.shape[0]
+            d = pred[k * nz:(k + 1) * nz].astype(np.float64)
+            mc.set_first_iterate((d - d.mean(0)).astype(np.float32), max_iter=3)
+            w = mc.process(m.frames)
+            assert w.first_iterate in (1, 2)
+            worst = max(worst, float(np.abs(w.global_shifts - c.global_shifts).max()))
+            warm_iters.append(int(w.iterations[0]))
+            cold_iters.append(int(c.iterations[0]))
+    print(f"iterations: cold {cold_iters}, warm {warm_iters}; max |warm - cold| {worst:.4f} px")
+    assert worst <= 0.05
+    assert sum(warm_iters) <= sum(cold_iters)
