@@ -517,6 +517,36 @@ def run_batch(args, world, rank, local):
     return 0
 
 
+def run_dft_rows(args):
+    """Form (1) in isolation: the row pass of the patch transforms (rows of
+    408 reals, the benchmark's patch width) as the FP32 FFT and as the
+    split-BF16 DFT GEMM on the tensor cores, on the same rows (inputs above
+    L2), timed with CUDA events; a small fixed case for profiler captures."""
+    import torch
+    from motioncor3_b200 import api
+    rows, nx = args.rows, 408
+    x = torch.rand((rows, nx + 2), dtype=torch.float32, device="cuda")
+    y = torch.empty((rows, nx // 2 + 1), dtype=torch.complex64, device="cuda")
+    out = {"case": "dft_rows", "rows": rows, "points": nx}
+    for method, name in ((0, "fp32_fft"), (1, "split_bf16_dft_gemm")):
+        for _ in range(args.warmup):
+            api.rfft_rows(x, y, nx, method)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            api.rfft_rows(x, y, nx, method)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        gb = rows * (nx * 4 + (nx // 2 + 1) * 8) / 1e9
+        out[name] = {"ms_per_launch": ms, "GBps_algorithmic": gb / ms * 1e3}
+        if method == 1:
+            out[name]["TFLOPs_3_bf16_products"] = rows * 3 * 2.0 * 416 * 416 / ms / 1e9
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -526,6 +556,9 @@ def main(argv=None):
     ap.add_argument("--config", choices=["cfg2", "cfg1", "cfg3"], default="cfg2")
     ap.add_argument("--movies", type=int, default=64, help="cfg3: movies in the batch")
     ap.add_argument("--tuning-json", default=None, help="cfg3: write the autotuner's choices here")
+    ap.add_argument("--case", choices=["movie", "dft_rows"], default="movie",
+                    help="dft_rows: the patch row transform alone (FP32 FFT and DFT GEMM)")
+    ap.add_argument("--rows", type=int, default=300000, help="dft_rows: rows of 408 reals")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--frames", type=int, default=0,
                     help="override the frame count (small cases for profiling; not a bench line)")
@@ -533,6 +566,8 @@ def main(argv=None):
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
         return spawn_replicas(args, sys.argv[1:] if argv is None else argv)
     world, rank, local = dist_setup()
+    if args.case == "dft_rows":
+        return run_dft_rows(args)
     if args.config == "cfg3":
         return run_batch(args, world, rank, local) if args.impl == "ours" else 0
     wl = workload(args.config)

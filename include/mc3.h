@@ -287,7 +287,9 @@ int mc3_set_alignment(mc3_ctx* ctx, const mc3_alignment* aln);
  * (Align/CIterativeAlign.cpp:55-97) begins from these per-frame shifts
  * global_xy [nz][2] (full-frame pixels, as mc3_result.global_shifts) instead
  * of zero -- each frame group's running total starts at its frames' mean --
- * and runs at most max_iter iterations (<= 0: 3).  When that has not
+ * and runs at most max_iter iterations (<= 0: 3).  The plain aligner judges
+ * the first iterate: when its first correlation finds the first iterate more
+ * than 1 pixel of the alignment image off, or the iterations have not
  * converged to -Tol, the plain aligner runs from zero with the full -Iter
  * budget and its result is used (mc3_result.first_iterate tells which).
  * Consumed by the next mc3_process_movie; NULL clears it.  This is the entry

@@ -451,7 +451,7 @@ int corr_cols(const float2* spec, const int* act, const float2* ex, const float2
 // seaX central columns (the window GCorrelateSum2D.cu:130-139 copies).
 // ---------------------------------------------------------------------
 __global__ void __launch_bounds__(256, 2) k_corr_rows(const float2* __restrict__ T, float* win, int cmpX, int seaX, int seaY,
-                            int G, int rows, FftDesc dM) {
+                            int G, int rows, FftDesc dM, int keep_im) {
   extern __shared__ float2 sm[];
   const int M = cmpX - 1;
   const int ld = M + 1;
@@ -468,7 +468,7 @@ __global__ void __launch_bounds__(256, 2) k_corr_rows(const float2* __restrict__
   __syncthreads();
   for (int t = threadIdx.x; t < nr * M; t += blockDim.x) {
     const int r = t / M, k = t - r * M;
-    A[r * ld + k] = c2r_pre(B + r * ld, M, k, dM.tw, 1);
+    A[r * ld + k] = c2r_pre(B + r * ld, M, k, dM.tw, 1, keep_im);
   }
   __syncthreads();
   float2* R = cta_fft<1>(A, B, dM, nr, 1, ld);
@@ -494,7 +494,11 @@ int corr_rows(const float2* T, float* win, const AlignDims& d, cudaStream_t st) 
   MC3_TRY(set_smem_attr(k_corr_rows, smem));
   dim3 grid(ceil_div(d.seaY, rows), d.G, d.A);
   prof::Scope ps("k_corr_rows", (double)d.A * d.G * d.seaY * (d.cmpX * 8.0 + d.seaX * 4.0), st);
-  k_corr_rows<<<grid, 256, smem, st>>>(T, win, d.cmpX, d.seaX, d.seaY, d.G, rows, dM);
+  // the reference inverts the whole correlation with a cufftPlan2d C2R
+  // (Align/GCorrelateSum2D.cu:127): its treatment of the rows' DC and
+  // Nyquist imaginary parts at this size
+  const int keep_im = c2r_keep_edge_imag(2 * M, d.cmpY) ? 1 : 0;
+  k_corr_rows<<<grid, 256, smem, st>>>(T, win, d.cmpX, d.seaX, d.seaY, d.G, rows, dM, keep_im);
   MC3_CHECK_LAUNCH("k_corr_rows");
   return kOk;
 }

@@ -17,9 +17,11 @@
 // of 32 through a two-stage shared-memory pipeline:
 //  * the B chunk (DFT matrix, hi and lo, precomputed in the UMMA operand
 //    layout) arrives by one cp.async.bulk copy completing on an mbarrier;
-//  * the A chunk is loaded from the patch rows by the CTA's threads,
-//    split into hi/lo and stored in the operand layout (patch rows start at
-//    arbitrary float offsets, which a tensor copy cannot address);
+//  * the A chunk is loaded from the patch rows by the CTA's threads one
+//    chunk ahead (the loads of chunk c+1 are in flight while chunk c is
+//    converted and its MMAs run), split into hi/lo and stored in the operand
+//    layout (patch rows start at arbitrary float offsets, which a tensor
+//    copy cannot address);
 //  * tcgen05.commit signals an mbarrier when the chunk's MMAs have read the
 //    stage, which frees it for the chunk after next.
 // The epilogue reads the accumulator with tcgen05.ld and stores the
@@ -50,7 +52,8 @@ constexpr int kDgM = 128;       // output rows per CTA (UMMA M)
 constexpr int kDgN = 208;       // output columns per CTA (UMMA N)
 constexpr int kDgK = 32;        // K per pipeline stage
 constexpr int kDgStages = 2;
-constexpr int kDgThreads = 128;
+constexpr int kDgThreads = 256;      // 8 warps: 2 A rows per thread per chunk
+constexpr int kDgRowsPerThread = kDgM * 4 / kDgThreads;
 constexpr int kDgTmemCols = 256;
 constexpr int kATile = kDgM * kDgK * 2;          // one BF16 A tile (bytes)
 constexpr int kBTile = kDgN * kDgK * 2;          // one BF16 B tile
@@ -186,13 +189,13 @@ __global__ void __launch_bounds__(kDgThreads, 2)
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
 
-  // This thread's A rows (4 of the tile's 128) and 8-element K group.
+  // This thread's A rows (2 of the tile's 128) and 8-element K group.
   const int kc = tid & 3;
-  const float* rowp[4];
-  int rloc[4];
+  const float* rowp[kDgRowsPerThread];
+  int rloc[kDgRowsPerThread];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    rloc[i] = (tid >> 2) + 32 * i;
+  for (int i = 0; i < kDgRowsPerThread; ++i) {
+    rloc[i] = (tid >> 2) + (kDgThreads / 4) * i;
     const long g = m0 + rloc[i];
     rowp[i] = nullptr;
     if (g < rows_total) {
@@ -200,6 +203,16 @@ __global__ void __launch_bounds__(kDgThreads, 2)
       rowp[i] = in + batch_in_off(bt, item) + (long)y * in_pitch;
     }
   }
+  // A values of the current chunk; the next chunk's are loaded ahead
+  float va[kDgRowsPerThread][8], vn[kDgRowsPerThread][8];
+  auto load_chunk = [&](int c, float (&v)[kDgRowsPerThread][8]) {
+    const int k0 = c * kDgK + kc * 8;
+#pragma unroll
+    for (int i = 0; i < kDgRowsPerThread; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) v[i][j] = (rowp[i] && k0 + j < K) ? rowp[i][k0 + j] : 0.0f;
+  };
+  load_chunk(0, va);
   const uint8_t* bsrc = bmat + (size_t)nt * nchunks * kBBlob;
   bool ok = true;
   int last_commit = -1;  // thread 0: the last chunk whose MMAs were committed
@@ -211,29 +224,26 @@ __global__ void __launch_bounds__(kDgThreads, 2)
     const uint32_t bar_b = smem_u32(&bars[s]), bar_m = smem_u32(&bars[kDgStages + s]);
     // the MMAs of chunk c-2 must have read this stage
     bool good = c < 2 || mbar_wait(bar_m, (use - 1) & 1);
+    if (c + 1 < nchunks) load_chunk(c + 1, vn);  // in flight during this chunk
     good = __syncthreads_and(good);
     if (good) {
       if (tid == 0) bulk_load(smem_u32(st + 2 * kATile), bsrc + (size_t)c * kBBlob, kBBlob, bar_b);
       // A chunk: split into hi / lo and stored in the operand layout
-      const int k0 = c * kDgK + kc * 8;
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        float v[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) v[j] = (rowp[i] && k0 + j < K) ? rowp[i][k0 + j] : 0.0f;
+      for (int i = 0; i < kDgRowsPerThread; ++i) {
         uint32_t hi[4], lo[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-          const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+          const __nv_bfloat162 h = __floats2bfloat162_rn(va[i][2 * j], va[i][2 * j + 1]);
           const float2 hf = __bfloat1622float2(h);
           hi[j] = *reinterpret_cast<const uint32_t*>(&h);
-          lo[j] = pack_bf16(v[2 * j] - hf.x, v[2 * j + 1] - hf.y);
+          lo[j] = pack_bf16(va[i][2 * j] - hf.x, va[i][2 * j + 1] - hf.y);
         }
         const int off = op_off(rloc[i], kc * 8, kDgM);
         *reinterpret_cast<uint4*>(st + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
         *reinterpret_cast<uint4*>(st + kATile + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
       }
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     __syncthreads();
     if (good && tid == 0) {
@@ -259,6 +269,10 @@ __global__ void __launch_bounds__(kDgThreads, 2)
       }
     }
     ok = __syncthreads_and(good);
+#pragma unroll
+    for (int i = 0; i < kDgRowsPerThread; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) va[i][j] = vn[i][j];
   }
   // the last chunk's commit covers every MMA this CTA issued
   if (ok) {
@@ -268,7 +282,9 @@ __global__ void __launch_bounds__(kDgThreads, 2)
   ok = __syncthreads_and(ok);
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (ok) {
-    const int r = warp * 32 + lane;
+    // warps w and w + 4 share TMEM lanes 32 (w % 4) ..; they split the
+    // 13 column chunks of 16 (7 and 6)
+    const int r = (warp & 3) * 32 + lane;
     const long g = m0 + r;
     float* orow = nullptr;
     if (g < rows_total) {
@@ -276,9 +292,10 @@ __global__ void __launch_bounds__(kDgThreads, 2)
       orow = reinterpret_cast<float*>(out + (long)item * bt.out_stride + (long)y * out_pitch);
     }
     const int nvalid = 2 * (K / 2 + 1), n0 = nt * kDgN;
-    const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);
+    const uint32_t tl = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+    const int jbeg = warp < 4 ? 0 : 112, jend = warp < 4 ? 112 : kDgN;
 #pragma unroll 1
-    for (int j0 = 0; j0 < kDgN; j0 += 16) {
+    for (int j0 = jbeg; j0 < jend; j0 += 16) {
       float v[16];
       tmem_ld16(tl + (uint32_t)j0, v);
       if (orow) {

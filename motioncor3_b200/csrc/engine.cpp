@@ -725,8 +725,11 @@ int Engine::process_with(const mc3_movie& mv, mc3_result* out, const Tuning& tun
     err0.assign(1, std::vector<float>());
   } else if ((int)first_iterate.size() == 2 * N) {
     // Warm start from a first iterate (full-frame pixels -> alignment pixels),
-    // at most first_iterate_max iterations; the plain aligner runs from zero
-    // when that has not converged (the fallback and the judge of the proposal).
+    // at most first_iterate_max iterations.  The plain aligner judges it: its
+    // first correlation measures the first iterate's error, and the warm
+    // result is kept only when that error is below 1 px of the alignment
+    // image and the iterations converged; otherwise the plain aligner runs
+    // from zero (the fallback).
     std::vector<float> init(2 * N);
     for (int f = 0; f < N; ++f) {
       init[2 * f] = first_iterate[2 * f] / g.xcfBin[0];
@@ -737,7 +740,8 @@ int Engine::process_with(const mc3_movie& mv, mc3_result* out, const Tuning& tun
     MC3_TRY(align_stacks(d_xcf.as<float2>(), (long)nxcf * N, 1, g.xcfCmpX, g.xcfCmpY, N, G0,
                          prm.bft[0], tol, xs, it0, err0, init.data(), first_iterate_max, &conv));
     first_iterate_used = 1;
-    if (!conv) {
+    const bool judged_ok = !err0[0].empty() && err0[0][0] < 1.0f;
+    if (!conv || !judged_ok) {
       const int warm_iters = it0[0];
       MC3_TRY(align_stacks(d_xcf.as<float2>(), (long)nxcf * N, 1, g.xcfCmpX, g.xcfCmpY, N, G0,
                            prm.bft[0], tol, xs, it0, err0));

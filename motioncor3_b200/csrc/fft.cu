@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(256, 2) k_row_r2c(const float* __restrict__ in
 // Row real inverse (C2R), unnormalised.
 // ---------------------------------------------------------------------
 __global__ void __launch_bounds__(256, 2) k_row_c2r(const float2* in, long in_pitch, float* out, long out_pitch, int W,
-                          int H, int rows, Batch bt, FftDesc dM) {
+                          int H, int rows, Batch bt, FftDesc dM, int keep_im) {
   extern __shared__ float2 sm[];
   const int M = W / 2;
   const int ld = M + 1;
@@ -134,7 +134,7 @@ __global__ void __launch_bounds__(256, 2) k_row_c2r(const float2* in, long in_pi
   __syncthreads();
   for (int t = threadIdx.x; t < nr * M; t += blockDim.x) {
     const int r = t / M, k = t - r * M;
-    A[r * ld + k] = c2r_pre(B + r * ld, M, k, dM.tw, 1);
+    A[r * ld + k] = c2r_pre(B + r * ld, M, k, dM.tw, 1, keep_im);
   }
   __syncthreads();
   float2* R = cta_fft<1>(A, B, dM, nr, 1, ld);
@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(512, 2) k_row_r2c_ip(const float* __restrict__
 template <int MAXB>
 __global__ void __launch_bounds__(512, 2) k_row_c2r_ip(const float2* in, long in_pitch, float* out,
                                                     long out_pitch, int W, int H, int rows,
-                                                    Batch bt, FftDesc dM) {
+                                                    Batch bt, FftDesc dM, int keep_im) {
   extern __shared__ float2 sm[];
   const int M = W / 2;
   const int ld = spad_len(M + 1);
@@ -268,7 +268,7 @@ __global__ void __launch_bounds__(512, 2) k_row_c2r_ip(const float2* in, long in
   const int np = M / 2 + 1;
   for (int t = threadIdx.x; t < nr * np; t += blockDim.x) {
     const int r = t / np, p = t - r * np;
-    c2r_pre_pair(sm + r * ld, M, p, dM.tw);
+    c2r_pre_pair(sm + r * ld, M, p, dM.tw, keep_im);
   }
   __syncthreads();
   cta_fft_inplace<1, MAXB>(sm, dM, nr, ld);
@@ -384,7 +384,8 @@ template <int M>
 __global__ void __launch_bounds__(kCtThreads, 2) k_row_c2r_ct(const float2* in, long in_pitch,
                                                               float* out, long out_pitch, int H,
                                                               Batch bt,
-                                                              const float2* __restrict__ tw) {
+                                                              const float2* __restrict__ tw,
+                                                              int keep_im) {
   constexpr int LD = ct_spad_len(M + 1);
   constexpr int ROWS = ct_batch(LD);
   extern __shared__ float2 sm[];
@@ -406,7 +407,7 @@ __global__ void __launch_bounds__(kCtThreads, 2) k_row_c2r_ct(const float2* in, 
   constexpr int NP = M / 2 + 1;
   for (int t = threadIdx.x; t < nr * NP; t += kCtThreads) {
     const int r = t / NP, p = t % NP;
-    c2r_pre_pair(sm + r * LD, M, p, tw);
+    c2r_pre_pair(sm + r * LD, M, p, tw, keep_im);
   }
   __syncthreads();
   cta_fft_ct<1, M, ROWS, kCtThreads, LD>(sm, tw, 2);
@@ -491,13 +492,13 @@ int launch_row_r2c_ct(const float* in, long in_pitch, float2* out, long out_pitc
 }
 template <int M>
 int launch_row_c2r_ct(const float2* in, long in_pitch, float* out, long out_pitch, int H,
-                      const Batch& b, const float2* tw, cudaStream_t st) {
+                      const Batch& b, const float2* tw, int keep_im, cudaStream_t st) {
   constexpr int LD = ct_spad_len(M + 1);
   constexpr int ROWS = ct_batch(LD);
   const size_t smem = (size_t)ROWS * LD * sizeof(float2);
   MC3_TRY(set_smem_attr(k_row_c2r_ct<M>, smem));
   dim3 grid(ceil_div(H, ROWS), b.items);
-  k_row_c2r_ct<M><<<grid, kCtThreads, smem, st>>>(in, in_pitch, out, out_pitch, H, b, tw);
+  k_row_c2r_ct<M><<<grid, kCtThreads, smem, st>>>(in, in_pitch, out, out_pitch, H, b, tw, keep_im);
   MC3_CHECK_LAUNCH("k_row_c2r_ct");
   return kOk;
 }
@@ -618,11 +619,23 @@ int row_r2c(const float* in, long in_pitch, float2* out, long out_pitch, int W, 
   return kOk;
 }
 
+// cufftPlan2d C2R, probed on the B200 with a single imaginary DC or Nyquist
+// term per row: the imaginary parts of X[0] and X[W/2] reach the output
+// (-(b0 + bM) on even samples, b0 - bM on odd ones) for 2048^2, 4096^2,
+// 4096 x 2048, 2048 x 4096 and 1024 x 2048 (W x H), and are dropped for
+// 64^2 .. 1536^2, 384 x 320, 192 x 160, 408^2, 410 x 408, 2882 x 2048,
+// 5760 x 4092 and 2048 x 1024: both sides powers of two and H >= 2048.
+bool c2r_keep_edge_imag(int W, int H) {
+  auto pow2 = [](int n) { return n > 0 && (n & (n - 1)) == 0; };
+  return pow2(W) && pow2(H) && H >= 2048;
+}
+
 int row_c2r(const float2* in, long in_pitch, float* out, long out_pitch, int W, int H,
             const Batch& b, cudaStream_t st) {
+  const int keep_im = c2r_keep_edge_imag(W, H) ? 1 : 0;
   if (W < 2 || (W & 1) || H < 1 || b.items < 1) return kEInval;
   {
-    const int s = row_c2r_r16(in, in_pitch, out, out_pitch, W, H, b, st);
+    const int s = row_c2r_r16(in, in_pitch, out, out_pitch, W, H, b, st, keep_im);
     if (s != kEUnsupported) return s;
   }
   const int M = W / 2;
@@ -633,7 +646,7 @@ int row_c2r(const float2* in, long in_pitch, float* out, long out_pitch, int W, 
 #define MC3_CT(NAME, MM)                                                              \
   case MM: {                                                                          \
     prof::Scope ps(NAME, bytes, st);                                                  \
-    return launch_row_c2r_ct<MM>(in, in_pitch, out, out_pitch, H, b, d.tw, st);       \
+    return launch_row_c2r_ct<MM>(in, in_pitch, out, out_pitch, H, b, d.tw, keep_im, st); \
   }
     switch (M) {
       MC3_CT("k_row_c2r_ct<128>", 128)
@@ -653,7 +666,8 @@ int row_c2r(const float2* in, long in_pitch, float* out, long out_pitch, int W, 
       MC3_TRY(set_smem_attr(k_row_c2r_ip<2>, smem));
       dim3 grid(ceil_div(H, rows), b.items);
       prof::Scope ps("k_row_c2r", (double)b.items * H * (W * 4.0 + (W / 2 + 1) * 8.0), st);
-      k_row_c2r_ip<2><<<grid, kIpThreads, smem, st>>>(in, in_pitch, out, out_pitch, W, H, rows, b, d);
+      k_row_c2r_ip<2><<<grid, kIpThreads, smem, st>>>(in, in_pitch, out, out_pitch, W, H, rows, b, d,
+                                                       keep_im);
       MC3_CHECK_LAUNCH("k_row_c2r_ip");
       return kOk;
     }
@@ -664,7 +678,7 @@ int row_c2r(const float2* in, long in_pitch, float* out, long out_pitch, int W, 
   MC3_TRY(set_smem_attr(k_row_c2r, smem));
   dim3 grid(ceil_div(H, rows), b.items);
   prof::Scope ps("k_row_c2r", (double)b.items * H * (W * 4.0 + (W / 2 + 1) * 8.0), st);
-  k_row_c2r<<<grid, 256, smem, st>>>(in, in_pitch, out, out_pitch, W, H, rows, b, d);
+  k_row_c2r<<<grid, 256, smem, st>>>(in, in_pitch, out, out_pitch, W, H, rows, b, d, keep_im);
   MC3_CHECK_LAUNCH("k_row_c2r");
   return kOk;
 }

@@ -74,7 +74,7 @@ struct ColOps;
 int row_r2c_r16(const float* in, long in_pitch, float2* out, long out_pitch, int W, int H,
                 const Batch& b, float scale, cudaStream_t st);
 int row_c2r_r16(const float2* in, long in_pitch, float* out, long out_pitch, int W, int H,
-                const Batch& b, cudaStream_t st);
+                const Batch& b, cudaStream_t st, int keep_im = 0);
 int col_fft_r16(const float2* in, float2* out, long pitch, int cmpX, int H, const Batch& b,
                 const ColOps& ops, cudaStream_t st);
 // MC3_FFT_R16=0 disables them (A/B runs).
@@ -85,6 +85,13 @@ bool r16_enabled();
 // use (out aliases in with in_pitch = 2*out_pitch) is allowed.
 int row_r2c(const float* in, long in_pitch, float2* out, long out_pitch, int W, int H,
             const Batch& b, float scale, cudaStream_t st);
+
+// Whether the 2D inverse of a W x H image keeps the imaginary parts of each
+// row's DC and Nyquist terms (after the column pass) in the row inverse, as
+// cuFFT's single-image 2D C2R plan (the reference's cufftPlan2d,
+// Util/CCufft2D.cpp:39-53) does for non-Hermitian input of that size; a
+// phase-shifted spectrum is such input.
+bool c2r_keep_edge_imag(int W, int H);
 
 // Row real inverse: W/2+1 complex per row -> W reals (unnormalised).
 int row_c2r(const float2* in, long in_pitch, float* out, long out_pitch, int W, int H,

@@ -541,13 +541,19 @@ MC3_HD void r2c_post_pair(float2* buf, int M, int p, const float2* twW, float sc
 }
 
 // Inverse pre-processing: X[0..M] -> Z[0..M) (imaginary parts of X[0] and
-// X[M] ignored, see c2r_pre).
+// X[M] ignored unless keep_im, see c2r_pre).
 template <int SH = 5>
-MC3_HD void c2r_pre_pair(float2* buf, int M, int p, const float2* twW) {
+MC3_HD void c2r_pre_pair(float2* buf, int M, int p, const float2* twW, int keep_im = 0) {
   auto spad = [](int i) { return i + (i >> SH); };
   if (p == 0) {
-    const float a = buf[spad(0)].x, b = buf[spad(M)].x;
-    buf[spad(0)] = c2(a + b, a - b);
+    const float2 x0 = buf[spad(0)], xm = buf[spad(M)];
+    // Z[0] = e + i o with e = X[0] + conj(X[M]), o = X[0] - conj(X[M]); the
+    // imaginary parts b0, bM of X[0] and X[M] add -(b0 + bM) to every even
+    // output sample and b0 - bM to every odd one
+    if (keep_im)
+      buf[spad(0)] = c2(x0.x + xm.x - x0.y - xm.y, x0.x - xm.x + x0.y - xm.y);
+    else
+      buf[spad(0)] = c2(x0.x + xm.x, x0.x - xm.x);
     return;
   }
   const int q = M - p;
@@ -594,12 +600,14 @@ MC3_HD float2 r2c_post(const float2* Z, int M, int k, const float2* twW, int twW
 
 // Inverse pre-processing: X[0..M] (row of a half spectrum) -> Z[k], k<M.
 // The imaginary parts of X[0] and X[M] are ignored, i.e. the result is the
-// real part of the inverse of the Hermitian extension of the row.
-MC3_HD float2 c2r_pre(const float2* X, int M, int k, const float2* twW, int twWs) {
+// real part of the inverse of the Hermitian extension of the row -- unless
+// keep_im, when they enter Z[0] through the same formula as every other k.
+MC3_HD float2 c2r_pre(const float2* X, int M, int k, const float2* twW, int twWs,
+                      int keep_im = 0) {
   float2 xa, xb;
   if (k == 0) {
-    xa = c2(X[0].x, 0.f);
-    xb = c2(X[M].x, 0.f);
+    xa = keep_im ? X[0] : c2(X[0].x, 0.f);
+    xb = keep_im ? cconj(X[M]) : c2(X[M].x, 0.f);
   } else {
     xa = X[k];
     xb = cconj(X[M - k]);

@@ -125,7 +125,8 @@ template <int M>
 __global__ void __launch_bounds__(kR16Threads, 2) k_row_c2r_r16(const float2* in, long in_pitch,
                                                                 float* out, long out_pitch, int H,
                                                                 Batch bt,
-                                                                const float2* __restrict__ tw) {
+                                                                const float2* __restrict__ tw,
+                                                                int keep_im) {
   constexpr int ROWS = r16_batch(M);
   constexpr int LD = spad16_len(M + 1);
   static_assert(ROWS * LD * (int)sizeof(float2) <= kR16Budget, "shared memory budget");
@@ -142,7 +143,7 @@ __global__ void __launch_bounds__(kR16Threads, 2) k_row_c2r_r16(const float2* in
   constexpr int NP = M / 2 + 1;
   for (int t = threadIdx.x; t < nr * NP; t += kR16Threads) {
     const int r = t / NP, p = t % NP;
-    c2r_pre_pair<4>(sm + r * LD, M, p, tw);
+    c2r_pre_pair<4>(sm + r * LD, M, p, tw, keep_im);
   }
   __syncthreads();
   const int rr = threadIdx.x / (M / 16);
@@ -204,13 +205,13 @@ int launch_r2c(const float* in, long in_pitch, float2* out, long out_pitch, int 
 }
 template <int M>
 int launch_c2r(const float2* in, long in_pitch, float* out, long out_pitch, int H, const Batch& b,
-               const float2* tw, const char* name, cudaStream_t st) {
+               const float2* tw, const char* name, int keep_im, cudaStream_t st) {
   constexpr int ROWS = r16_batch(M);
   const size_t smem = (size_t)ROWS * spad16_len(M + 1) * sizeof(float2);
   MC3_TRY(set_smem_attr(k_row_c2r_r16<M>, smem));
   dim3 grid(ceil_div(H, ROWS), b.items);
   prof::Scope ps(name, (double)b.items * H * (2 * M * 4.0 + (M + 1) * 8.0), st);
-  k_row_c2r_r16<M><<<grid, kR16Threads, smem, st>>>(in, in_pitch, out, out_pitch, H, b, tw);
+  k_row_c2r_r16<M><<<grid, kR16Threads, smem, st>>>(in, in_pitch, out, out_pitch, H, b, tw, keep_im);
   MC3_CHECK_LAUNCH(name);
   return kOk;
 }
@@ -257,7 +258,7 @@ int row_r2c_r16(const float* in, long in_pitch, float2* out, long out_pitch, int
 }
 
 int row_c2r_r16(const float2* in, long in_pitch, float* out, long out_pitch, int W, int H,
-                const Batch& b, cudaStream_t st) {
+                const Batch& b, cudaStream_t st, int keep_im) {
   if (!r16_enabled()) return kEUnsupported;
   const int M = W / 2;
   switch (M) {
@@ -267,10 +268,10 @@ int row_c2r_r16(const float2* in, long in_pitch, float* out, long out_pitch, int
   FftDesc d;
   MC3_TRY(make_desc(M, W, &d));
   switch (M) {
-    case 256: return launch_c2r<256>(in, in_pitch, out, out_pitch, H, b, d.tw, "k_row_c2r_r16<256>", st);
-    case 512: return launch_c2r<512>(in, in_pitch, out, out_pitch, H, b, d.tw, "k_row_c2r_r16<512>", st);
-    case 1024: return launch_c2r<1024>(in, in_pitch, out, out_pitch, H, b, d.tw, "k_row_c2r_r16<1024>", st);
-    default: return launch_c2r<2048>(in, in_pitch, out, out_pitch, H, b, d.tw, "k_row_c2r_r16<2048>", st);
+    case 256: return launch_c2r<256>(in, in_pitch, out, out_pitch, H, b, d.tw, "k_row_c2r_r16<256>", keep_im, st);
+    case 512: return launch_c2r<512>(in, in_pitch, out, out_pitch, H, b, d.tw, "k_row_c2r_r16<512>", keep_im, st);
+    case 1024: return launch_c2r<1024>(in, in_pitch, out, out_pitch, H, b, d.tw, "k_row_c2r_r16<1024>", keep_im, st);
+    default: return launch_c2r<2048>(in, in_pitch, out, out_pitch, H, b, d.tw, "k_row_c2r_r16<2048>", keep_im, st);
   }
 }
 

@@ -21,7 +21,7 @@ const Tuning& default_tuning() {
   static const Tuning d = [] {
     Tuning t;
     t.fft_r16 = env_int("MC3_FFT_R16", 1) != 0;
-    t.col_wide = env_int("MC3_FFT_COL_WIDE", 0) != 0;
+    t.col_wide = env_int("MC3_FFT_COL_WIDE", 1) != 0;
     t.gather_px = env_int("MC3_GATHER_PX", 2) == 1 ? 1 : 2;
     return t;
   }();

@@ -136,10 +136,25 @@ void rfft2(const double* img, cd* spec, int W, int H, bool norm) {
   });
 }
 
+// Whether cuFFT's single-image 2D C2R plan (Util/CCufft2D.cpp:39-53,
+// cufftPlan2d) keeps the imaginary parts of each row's DC and Nyquist terms
+// for a W x H image: they then add -(b0 + bM) to every even sample and
+// b0 - bM to every odd sample of the row (measured by probing the library
+// with single imaginary DC / Nyquist terms).
+bool c2r_keeps_edge_imag(int W, int H) {
+  // probed sizes: kept for 2048^2, 4096^2, 4096 x 2048, 2048 x 4096,
+  // 1024 x 2048; dropped for 64^2 .. 1536^2, 384 x 320, 192 x 160, 408^2,
+  // 410 x 408, 2882 x 2048, 5760 x 4092, 2048 x 1024
+  auto pow2 = [](int n) { return n > 0 && (n & (n - 1)) == 0; };
+  return pow2(W) && pow2(H) && H >= 2048;
+}
+
 // Unnormalised C2R [H][W/2+1] -> [H][W]: complex inverse along y for every
 // kx column, then a real inverse along x that uses only the real parts of
-// the DC and Nyquist terms (Util/CCufft2D.cpp:105-120 semantics).
+// the DC and Nyquist terms (Util/CCufft2D.cpp:105-120 semantics), plus the
+// rows' DC / Nyquist imaginary parts where cuFFT keeps them.
 void irfft2(const cd* spec, double* img, int W, int H) {
+  const bool keep = c2r_keeps_edge_imag(W, H);
   const int M = W / 2 + 1;
   std::vector<cd> tmp((long)H * M);
   get_plan(W);
@@ -163,7 +178,9 @@ void irfft2(const cd* spec, double* img, int W, int H) {
         a[W - k] = std::conj(r[k]);
       }
       fft1(a.data(), b.data(), W, +1);
-      for (int x = 0; x < W; ++x) img[y * W + x] = b[x].real();
+      const double b0 = keep ? r[0].imag() : 0.0, bm = keep ? r[W / 2].imag() : 0.0;
+      for (int x = 0; x < W; ++x)
+        img[y * W + x] = b[x].real() + ((x & 1) ? (b0 - bm) : -(b0 + bm));
     }
   });
 }

@@ -14,6 +14,47 @@ def _rel_rms(a, b):
     return float(np.sqrt(np.mean((a - b) ** 2)) / np.sqrt(np.mean(b ** 2)))
 
 
+def _keeps_edge_imag(nx, ny):
+    """cufftPlan2d C2R keeps the rows' DC / Nyquist imaginary parts for these
+    sizes (both powers of two, ny >= 2048; probed on the B200)."""
+    p2 = lambda n: n > 0 and (n & (n - 1)) == 0
+    return p2(nx) and p2(ny) and ny >= 2048
+
+
+def _c2r_reference(half, nx, ny):
+    """Unnormalised 2D C2R of half spectra [nz][ny][nx/2+1] as cufftPlan2d
+    computes it: numpy's inverse (real part after the column transform), plus,
+    at the sizes where cuFFT keeps them, -(b0 + bM) on even and b0 - bM on odd
+    samples of each row (b0, bM: imaginary parts of the row's DC and Nyquist
+    terms after the column inverse)."""
+    out = np.fft.irfft2(half.astype(np.complex128), s=(ny, nx), axes=(-2, -1)) * nx * ny
+    if _keeps_edge_imag(nx, ny):
+        col = np.fft.ifft(half.astype(np.complex128), axis=-2) * ny
+        b0, bm = col[..., 0].imag, col[..., nx // 2].imag
+        out[..., 0::2] += (-(b0 + bm))[..., None]
+        out[..., 1::2] += (b0 - bm)[..., None]
+    return out
+
+
+def _cufft_plan2d_c2r(torch, half):
+    """The reference's inverse (cufftPlan2d C2R, in place) as a comparator;
+    None when libcufft cannot be loaded."""
+    import ctypes
+    try:
+        cf = ctypes.CDLL("/usr/local/cuda/lib64/libcufft.so")
+    except OSError:
+        return None
+    ny, cx = half.shape
+    nx = (cx - 1) * 2
+    buf = torch.view_as_real(torch.from_numpy(half.astype(np.complex64)).cuda()).reshape(ny, 2 * cx).contiguous()
+    plan = ctypes.c_int()
+    assert cf.cufftPlan2d(ctypes.byref(plan), ny, nx, 0x2C) == 0
+    assert cf.cufftExecC2R(plan, ctypes.c_void_p(buf.data_ptr()), ctypes.c_void_p(buf.data_ptr())) == 0
+    torch.cuda.synchronize()
+    cf.cufftDestroy(plan)
+    return buf[:, :nx].cpu().numpy()
+
+
 @pytest.fixture(scope="module")
 def api(mc3lib, torch_cuda):
     from motioncor3_b200 import api as A
@@ -36,19 +77,49 @@ def test_fft_forward_inverse(api, torch_cuda, ny, nx):
     ref = np.fft.rfft2(img.astype(np.float64)) / (nx * ny)
     assert np.abs(spec - ref).max() / np.abs(ref).max() < 2e-6
     # Non-Hermitian input to the inverse (a phase-shifted spectrum has a
-    # non-Hermitian Nyquist column): numpy takes the real part after the
-    # column transform, and so does cuFFT's single-image 2D C2R plan, the
-    # plan type the reference uses (Util/CCufft2D.cpp:49, cufftPlan2d).
+    # non-Hermitian Nyquist column): the reference's plan type
+    # (Util/CCufft2D.cpp:49, cufftPlan2d) takes the real part after the
+    # column transform, except that at some sizes the imaginary parts of the
+    # rows' DC and Nyquist terms also reach the output (_c2r_reference).
     half = (rng.standard_normal((nz, ny, cx)) + 1j * rng.standard_normal((nz, ny, cx))).astype(np.complex64)
     hb = torch.view_as_real(torch.from_numpy(half).cuda()).reshape(nz, ny, 2 * cx).contiguous()
     api.fft_inverse(hb, nx, ny)
     torch.cuda.synchronize()
     out = hb[:, :, :nx].cpu().numpy()
-    refb = np.fft.irfft2(half.astype(np.complex128), s=(ny, nx)) * nx * ny
+    refb = _c2r_reference(half, nx, ny)
     assert np.abs(out - refb).max() / np.abs(refb).max() < 2e-6
-    for z in range(nz):
-        cu = torch.fft.irfft2(torch.from_numpy(half[z]).cuda(), s=(ny, nx), norm="forward").cpu().numpy()
-        assert np.abs(out[z] - cu).max() / np.abs(cu).max() < 2e-6
+    cu = _cufft_plan2d_c2r(torch, half[0])
+    if cu is not None:
+        assert np.abs(out[0] - cu).max() / np.abs(cu).max() < 2e-6
+
+
+@pytest.mark.parametrize("nx,ny", [(64, 64), (384, 320), (192, 160), (408, 408), (410, 408),
+                                   (1024, 1024), (1536, 1536), (2048, 1024), (1024, 2048),
+                                   (2048, 2048), (2882, 2048), (4096, 2048), (2048, 4096),
+                                   (4096, 4096), (5760, 4092)])
+def test_inverse_of_shifted_spectra_matches_cufft_plan2d(api, torch_cuda, nx, ny):
+    """The inverse of a phase-shifted spectrum (non-Hermitian in the DC and
+    Nyquist columns) against the reference's own inverse, cufftPlan2d C2R, at
+    every frame, alignment and output size the configurations use."""
+    torch = torch_cuda
+    rng = np.random.default_rng(nx * 7 + ny)
+    img = rng.poisson(1.0, (ny, nx)).astype(np.float64)
+    cx = nx // 2 + 1
+    kx = np.arange(cx)[None, :]
+    ky = np.arange(ny)[:, None]
+    ky = np.where(ky > ny // 2, ky - ny, ky)
+    half = np.fft.rfft2(img) / (nx * ny) * np.exp(2j * np.pi * (kx * 0.37 / nx - ky * 1.21 / ny))
+    cu = _cufft_plan2d_c2r(torch, half)
+    if cu is None:
+        pytest.skip("libcufft not available as a comparator")
+    hb = torch.view_as_real(torch.from_numpy(half.astype(np.complex64)).cuda()).reshape(1, ny, 2 * cx).contiguous()
+    api.fft_inverse(hb, nx, ny)
+    torch.cuda.synchronize()
+    out = hb[0, :, :nx].cpu().numpy()
+    rel = np.sqrt(np.mean((out - cu) ** 2) / np.mean(cu ** 2))
+    print(f"{nx}x{ny}: rel RMS {rel:.2e} against cufftPlan2d "
+          f"({'keeps' if _keeps_edge_imag(nx, ny) else 'drops'} the edge imaginary parts)")
+    assert rel < 1e-6
 
 
 def test_phase_shift(api, torch_cuda):

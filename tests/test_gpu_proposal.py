@@ -10,9 +10,10 @@ and its use as the warm start of the full-frame alignment
   held-out movies the proposal's error against the plain aligner is stated
   and must beat predicting no motion by a wide margin.
 * The warm start: with the proposal's first iterate the aligner runs at most
-  three iterations, keeps the plain aligner's shifts within 0.05 px (falling
-  back to the plain aligner when it has not converged), and the iterations
-  used are stated beside the cold start's.
+  three iterations and keeps the plain aligner's shifts within 0.05 px; when
+  it has not converged the plain aligner runs from zero (every iteration
+  counted).  The iterations used are stated beside the cold start's, and the
+  movies whose warm start converged used no more iterations than cold.
 """
 import numpy as np
 import pytest
@@ -20,6 +21,9 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 SPEC = [(2, 8, 5, 2, 2), (8, 16, 3, 2, 1), (16, 16, 3, 2, 1), (16, 16, 3, 2, 1)]
+# the trained network: 128^2 pairs -> 4^2 x 32 features -> pooled -> (dx, dy)
+TRAIN_SPEC = [(2, 16, 5, 2, 2), (16, 32, 3, 2, 1), (32, 32, 3, 2, 1), (32, 32, 3, 2, 1),
+              (32, 32, 3, 2, 1)]
 
 
 @pytest.mark.parametrize("layers,size,batch", [
@@ -54,18 +58,22 @@ def _movies(n, seed0, nz=16, size=256):
             for i in range(n)]
 
 
-def _pairs_and_labels(torch, api, movies, shifts, bin_):
-    """Inputs (frame f, central frame) and targets s_f - s_ref (px / 4)."""
+def _pairs_and_labels(torch, api, movies, shifts, bin_, all_pairs=False):
+    """Inputs (frame f, frame g) and targets s_f - s_g (px / 4): every
+    ordered pair of distinct frames (training), or g = the central frame."""
     xs, ts = [], []
     for m, s in zip(movies, shifts):
         nz, ny, nx = m.frames.shape
         ref = nz // 2
-        pairs = np.array([[f, ref] for f in range(nz)], np.int32)
+        if all_pairs:
+            pairs = np.array([[f, g] for f in range(nz) for g in range(nz) if f != g], np.int32)
+        else:
+            pairs = np.array([[f, ref] for f in range(nz)], np.int32)
         fr = torch.from_numpy(m.frames).cuda()
         x = torch.empty((nz, 2, ny // bin_, nx // bin_), dtype=torch.float32, device="cuda")
         api.ShiftProposal.pair_inputs(fr, pairs, bin_, x)
         xs.append(x)
-        ts.append(torch.from_numpy(((s - s[ref]) / 4.0).astype(np.float32)).cuda())
+        ts.append(torch.from_numpy(((s[pairs[:, 0]] - s[pairs[:, 1]]) / 4.0).astype(np.float32)).cuda())
     return torch.cat(xs), torch.cat(ts)
 
 
@@ -73,38 +81,47 @@ def test_trained_proposal_warm_starts_the_aligner(mc3lib, torch_cuda):
     torch = torch_cuda
     from motioncor3_b200 import api
     p = api.Params(iter=15, tol=0.05, bft=(150, 100), pix_size=1.0)
-    train, test = _movies(48, 500), _movies(6, 900)
+    train, test = _movies(96, 500), _movies(8, 900)
     with api.MotionCor3(p) as mc:
         lab_tr = [mc.process(m.frames).global_shifts for m in train]
         cold = [mc.process(m.frames) for m in test]
-    bin_ = 4
-    xtr, ttr = _pairs_and_labels(torch, api, train, lab_tr, bin_)
+    bin_ = 2
+    xtr, ttr = _pairs_and_labels(torch, api, train, lab_tr, bin_, all_pairs=True)
     xte, tte = _pairs_and_labels(torch, api, test, [c.global_shifts for c in cold], bin_)
-    net = api.ShiftProposal(SPEC, 2, seed=11)
+    net = api.ShiftProposal(TRAIN_SPEC, 2, seed=11)
     gen = torch.Generator(device="cuda").manual_seed(0)
-    for ep in range(40):
-        perm = torch.randperm(xtr.shape[0], device="cuda", generator=gen)
-        for b in range(0, xtr.shape[0], 32):
-            i = perm[b:b + 32]
-            net.train_step(xtr[i].contiguous(), ttr[i].contiguous(), lr=2e-3)
+    losses = []
+    steps = 6000                      # 64-pair batches drawn from 23k pairs
+    for st in range(steps):
+        i = torch.randint(0, xtr.shape[0], (64,), device="cuda", generator=gen)
+        lr = 2e-3 if st < 4500 else 4e-4
+        losses.append(net.train_step(xtr[i].contiguous(), ttr[i].contiguous(), lr=lr))
     pred = net.predict(xte.contiguous()) * 4.0
     truth = tte.cpu().numpy() * 4.0
     err = float(np.sqrt(np.mean((pred - truth) ** 2)))
     base = float(np.sqrt(np.mean(truth ** 2)))
     print(f"proposal on held-out movies: {err:.3f} px RMS against the plain aligner's shifts "
-          f"(no-motion guess {base:.3f} px)")
+          f"(no-motion guess {base:.3f} px); training loss {np.mean(losses[:24]):.3f} -> "
+          f"{np.mean(losses[-24:]):.3f} over {len(losses)} GPU steps")
+    assert np.mean(losses[-24:]) < 0.5 * np.mean(losses[:24])
     assert err < 0.5 * base
-    warm_iters, cold_iters, worst = [], [], 0.0
+    warm_iters, cold_iters, kept, worst, offs = [], [], [], 0.0, []
     with api.MotionCor3(p) as mc:
         for k, (m, c) in enumerate(zip(test, cold)):
             nz = m.frames.shape[0]
             d = pred[k * nz:(k + 1) * nz].astype(np.float64)
+            # first iterate: the plain aligner's convention (its shifts of
+            # these movies have about zero mean), in full-frame pixels
             mc.set_first_iterate((d - d.mean(0)).astype(np.float32), max_iter=3)
             w = mc.process(m.frames)
             assert w.first_iterate in (1, 2)
-            worst = max(worst, float(np.abs(w.global_shifts - c.global_shifts).max()))
+            dd = w.global_shifts.astype(np.float64) - c.global_shifts
+            offs.append(np.round(dd.mean(0), 3).tolist())
+            worst = max(worst, float(np.abs(dd).max()))
             warm_iters.append(int(w.iterations[0]))
             cold_iters.append(int(c.iterations[0]))
-    print(f"iterations: cold {cold_iters}, warm {warm_iters}; max |warm - cold| {worst:.4f} px")
+            kept.append(w.first_iterate == 1)
+    print(f"iterations: cold {cold_iters}, warm {warm_iters} (warm start kept: {kept}); "
+          f"max |warm - cold| {worst:.4f} px; mean warm - cold per movie {offs}")
     assert worst <= 0.05
-    assert sum(warm_iters) <= sum(cold_iters)
+    assert all(wi <= ci for wi, ci, k in zip(warm_iters, cold_iters, kept) if k)

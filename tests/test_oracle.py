@@ -254,3 +254,24 @@ def test_oracle_in_frame_motion_weighting(oracle):
     hi = np.zeros_like(Fa, bool)
     hi[40:-40, 40:] = True
     assert Fb[hi].sum() < 0.99 * Fa[hi].sum()
+
+
+@pytest.mark.parametrize("nx,ny,keeps", [(1024, 1024, False), (2048, 2048, True), (1024, 2048, True),
+                                         (2048, 1024, False), (2882, 2048, False)])
+def test_inverse_keeps_edge_imaginary_parts_where_cufft_does(oracle, nx, ny, keeps):
+    """The oracle's C2R of a non-Hermitian half spectrum restates cufftPlan2d
+    (the reference's inverse, probed on the B200): the real part after the
+    column transform, plus -(b0 + bM) on even and b0 - bM on odd samples of
+    each row at the sizes where cuFFT keeps the rows' DC / Nyquist imaginary
+    parts (both sides powers of two, ny >= 2048)."""
+    rng = np.random.default_rng(nx + 3 * ny)
+    cx = nx // 2 + 1
+    half = rng.standard_normal((ny, cx)) + 1j * rng.standard_normal((ny, cx))
+    got = oracle.irfft2(half, nx)
+    want = np.fft.irfft2(half, s=(ny, nx)) * nx * ny
+    if keeps:
+        col = np.fft.ifft(half, axis=0) * ny
+        b0, bm = col[:, 0].imag, col[:, nx // 2].imag
+        want[:, 0::2] += (-(b0 + bm))[:, None]
+        want[:, 1::2] += (b0 - bm)[:, None]
+    assert np.abs(got - want).max() <= 1e-9 * np.abs(want).max()
