@@ -415,6 +415,40 @@ def run_ours(args, wl, world, rank, local):
     except Exception as exc:  # the report never fails on this extra
         accuracy = {"error": str(exc)}
 
+    # ---- form (1) beside the plain path: the same movie with the patch
+    #      transforms' row pass as split-BF16 DFT GEMMs on the tensor cores ----
+    forms = None
+    if wl["params"].get("patch", (0, 0))[0] > 0 and not args.no_forms:
+        try:
+            mg = api.MotionCor3(api.Params(gpu=local, dft_gemm=1, **wl["params"]))
+            mg.set_stream(stream.cuda_stream)
+            if mv.gain is not None:
+                mg.set_gain(mv.gain)
+            sums_g = torch.empty_like(sums)
+            for _ in range(max(args.warmup, 1)):
+                mg.process(frames, sums_out=sums_g)
+            g0 = torch.cuda.Event(enable_timing=True)
+            g1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            g0.record(stream)
+            for _ in range(args.steps):
+                lg = mg.process(frames, sums_out=sums_g)
+            g1.record(stream)
+            torch.cuda.synchronize()
+            gms = g0.elapsed_time(g1) / args.steps
+            dg = float(np.abs(lg.global_shifts - last.global_shifts).max())
+            dp = float(np.abs(lg.patch_shifts - last.patch_shifts).max()) if last.n_patches else 0.0
+            rel = float(torch.sqrt(torch.mean((sums_g - sums) ** 2) / torch.mean(sums ** 2)))
+            mg.close()
+            forms = {"split_bf16_dft_gemm": {
+                "what": "patch transforms' row pass (408 reals) as 3 BF16 tcgen05 products "
+                        "with FP32 accumulation in tensor memory",
+                "ms_per_step": gms, "value": nz / gms * 1e3, "unit": "frames/s",
+                "max_global_shift_diff_vs_fp32_px": dg, "max_patch_shift_diff_vs_fp32_px": dp,
+                "sums_rel_rms_vs_fp32": rel}}
+        except Exception as exc:  # the report never fails on this extra
+            forms = {"error": str(exc)[-300:]}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         n = CPU_SAMPLE_FRAMES
@@ -449,6 +483,7 @@ def run_ours(args, wl, world, rank, local):
             "roofline": roof,
             "cpu_baseline": cpu,
             "accuracy": accuracy,
+            "forms": forms,
             "kernels": {k: {"launches_per_step": v[0] / args.steps, "ms_per_step": v[1] / args.steps,
                             "GBps": (v[2] / v[1] / 1e6) if v[1] else None}
                         for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
@@ -560,6 +595,8 @@ def main(argv=None):
                     help="dft_rows: the patch row transform alone (FP32 FFT and DFT GEMM)")
     ap.add_argument("--rows", type=int, default=300000, help="dft_rows: rows of 408 reals")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the split-BF16 DFT GEMM rerun of the timed movie")
     ap.add_argument("--frames", type=int, default=0,
                     help="override the frame count (small cases for profiling; not a bench line)")
     args = ap.parse_args(argv)

@@ -2,6 +2,7 @@
 // the first stage reads global memory directly, the last stage writes it
 // directly, and shared memory only carries the exchanges between stages.
 // 512 threads per CTA, up to 72 KB of shared memory, two CTAs per SM.
+#include <algorithm>
 #include <cstdlib>
 
 #include "fft.cuh"
@@ -68,6 +69,123 @@ __global__ void __launch_bounds__(T, kR16Threads * 2 / T) k_col_fft_r16(const fl
   float2* buf = sm + c * LD;
   if (ops.dir < 0) fft_r16<-1, H, false, false>(buf, j, tw, 1, load, store);
   else fft_r16<1, H, false, false>(buf, j, tw, 1, load, store);
+}
+
+// ---------------------------------------------------------------------
+// Pipelined 4096-point column pass (persistent, one 1024-thread CTA per
+// SM).  Work unit = 4 adjacent columns of one item.  While a unit is
+// transformed in registers, the next unit's 4 x 4096 values are copied
+// into a 128 KB staging buffer by 8-byte cp.async (each warp copies 8 rows
+// x 32 bytes: whole sectors), so DRAM reads run under the arithmetic of the
+// previous unit instead of in a separate load phase.  The two exchanges
+// between the three radix-16 stages go through a second buffer that holds
+// two columns at a time (columns 0-1, then 2-3), which keeps the whole CTA
+// within 196 KB of shared memory.  The row pitch of the spectra (W/2+1
+// complex) is odd for every even W, so the rows are not 16-byte aligned
+// and the copies are 8-byte cp.async rather than tensor-map bulk copies.
+// ---------------------------------------------------------------------
+namespace {
+constexpr int kPipeH = 4096;
+constexpr int kPipeNB = 4;
+constexpr int kPipeT = kPipeH / 16 * kPipeNB;  // 1024
+constexpr int kPipeLDX = spad16_col_stride(kPipeH, 2);
+constexpr size_t kPipeSmem =
+    (size_t)kPipeH * kPipeNB * sizeof(float2) + 2 * (size_t)kPipeLDX * sizeof(float2);
+
+__device__ __forceinline__ void cp_async8(float2* dst, const float2* src, int bytes) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Exchange after stage S: the 16 outputs in v (indices base + r*NS) are
+// written to the exchange buffer and the next stage's 16 inputs read back,
+// for columns 0-1 (c < 2) and then columns 2-3.
+template <int S>
+__device__ __forceinline__ void pipe_exchange(float2 (&v)[16], int j, int c, float2* xb) {
+  using St = R16Stage<kPipeH, S>;
+  constexpr int NS = St::NS;
+  const int base = (j / NS) * NS * 16 + j % NS;
+  float2* buf = xb + (c & 1) * kPipeLDX;
+#pragma unroll
+  for (int half = 0; half < 2; ++half) {
+    if ((c >> 1) == half) {
+#pragma unroll
+      for (int r = 0; r < 16; ++r) buf[spad16(base + r * NS)] = v[r];
+    }
+    __syncthreads();
+    if ((c >> 1) == half) {
+#pragma unroll
+      for (int r = 0; r < 16; ++r) v[r] = buf[spad16(r16_in_index<kPipeH, S + 1>(j, 0, r))];
+    }
+    __syncthreads();
+  }
+}
+}  // namespace
+
+template <int DIR, bool PHASE, bool CROP>
+__global__ void __launch_bounds__(kPipeT, 1) k_col_fft_r16p(const float2* in, float2* out,
+                                                            long pitch, int cmpX, Batch bt,
+                                                            const float2* __restrict__ tw,
+                                                            ColOps ops, int ngroups, int nunits) {
+  static_assert(r16_nstages(kPipeH) == 3 && R16Stage<kPipeH, 0>::NB == 1, "three radix-16 stages");
+  extern __shared__ float2 sm[];
+  float2* pre = sm;                         // [kPipeH][kPipeNB]
+  float2* xb = sm + kPipeH * kPipeNB;       // two columns, kPipeLDX apart
+  const int c = threadIdx.x % kPipeNB;
+  const int j = threadIdx.x / kPipeNB;
+  auto prefetch = [&](int u) {
+    const int item = u / ngroups, x = (u % ngroups) * kPipeNB + c;
+    const int bytes = x < cmpX ? 8 : 0;     // columns past cmpX are zero-filled
+    const float2* src = in + batch_in_off(bt, item) + min(x, cmpX - 1) + (long)j * pitch;
+#pragma unroll
+    for (int r = 0; r < 16; ++r)
+      cp_async8(pre + (j + 256 * r) * kPipeNB + c, src + (long)(256 * r) * pitch, bytes);
+    cp_async_commit();
+  };
+  int u = blockIdx.x;
+  if (u < nunits) prefetch(u);
+  for (; u < nunits; u += gridDim.x) {
+    const int item = u / ngroups, x = (u % ngroups) * kPipeNB + c;
+    const bool live = x < cmpX;
+    cp_async_wait_all();
+    __syncthreads();
+    float2 v[16];
+    {
+      const float2* ey = PHASE ? ops.ey + (long)item * kPipeH : nullptr;
+      const float2 exx = (PHASE && live) ? ops.ex[(long)item * cmpX + x] : c2(1.f, 0.f);
+#pragma unroll
+      for (int r = 0; r < 16; ++r) {
+        const int y = r16_in_index<kPipeH, 0>(j, 0, r);
+        v[r] = pre[y * kPipeNB + c];
+        if constexpr (PHASE) v[r] = cmul(v[r], cmul(exx, ey[y]));
+      }
+    }
+    __syncthreads();                        // the staging buffer is free again
+    if (u + (int)gridDim.x < nunits) prefetch(u + gridDim.x);
+    auto none = [](int, float2) {};
+    r16_compute<DIR, kPipeH, 0>(v, j, tw, 1, none);
+    pipe_exchange<0>(v, j, c, xb);
+    r16_compute<DIR, kPipeH, 1>(v, j, tw, 1, none);
+    pipe_exchange<1>(v, j, c, xb);
+    float2* dst = out + (long)item * bt.out_stride + x;
+    float2* crop = CROP ? ops.crop + (long)item * ops.crop_x * ops.crop_y + x : nullptr;
+    const bool in_crop = CROP && x < ops.crop_x;
+    r16_compute<DIR, kPipeH, 2>(v, j, tw, 1, [&](int y, float2 w) {
+      if (!live) return;
+      w = cscale(w, ops.scale);
+      dst[(long)y * pitch] = w;
+      if (CROP && in_crop) {
+        int yo = -1;
+        if (y <= ops.crop_y / 2) yo = y;
+        else if (y > kPipeH - ops.crop_y / 2) yo = y - kPipeH + ops.crop_y;
+        if (yo >= 0) crop[(long)yo * ops.crop_x] = w;
+      }
+    });
+  }
+  cp_async_wait_all();
 }
 
 // ---------------------------------------------------------------------
@@ -191,6 +309,43 @@ int launch_col(const float2* in, float2* out, long pitch, int cmpX, const Batch&
   MC3_CHECK_LAUNCH(name);
   return kOk;
 }
+int sm_count() {
+  int dev = 0, n = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+    n = 148;
+  return n;
+}
+int launch_col_pipe(const float2* in, float2* out, long pitch, int cmpX, const Batch& b,
+                    const float2* tw, const ColOps& ops, const char* name, cudaStream_t st) {
+  const int ngroups = ceil_div(cmpX, kPipeNB);
+  const long nunits_l = (long)ngroups * b.items;
+  if (nunits_l > 0x7fffffffL) return kEUnsupported;
+  const int nunits = (int)nunits_l;
+  const int grid = std::min(nunits, sm_count());
+  prof::Scope ps(name, (double)b.items * ((double)cmpX * kPipeH * 16.0 + (ops.crop ? (double)ops.crop_x * ops.crop_y * 8.0 : 0.0)), st);
+  const bool phase = ops.ex && ops.ey, crop = ops.crop != nullptr;
+#define MC3_PIPEK(D, P, C)                                                                  \
+  {                                                                                         \
+    MC3_TRY(set_smem_attr(k_col_fft_r16p<D, P, C>, kPipeSmem));                             \
+    k_col_fft_r16p<D, P, C><<<grid, kPipeT, kPipeSmem, st>>>(in, out, pitch, cmpX, b, tw,   \
+                                                             ops, ngroups, nunits);         \
+  }
+#define MC3_PIPED(D)                          \
+  if (phase && crop) MC3_PIPEK(D, true, true) \
+  else if (phase) MC3_PIPEK(D, true, false)   \
+  else if (crop) MC3_PIPEK(D, false, true)    \
+  else MC3_PIPEK(D, false, false)
+  if (ops.dir < 0) {
+    MC3_PIPED(-1)
+  } else {
+    MC3_PIPED(1)
+  }
+#undef MC3_PIPED
+#undef MC3_PIPEK
+  MC3_CHECK_LAUNCH(name);
+  return kOk;
+}
 template <int M>
 int launch_r2c(const float* in, long in_pitch, float2* out, long out_pitch, int H, const Batch& b,
                const float2* tw, float scale, const char* name, cudaStream_t st) {
@@ -232,6 +387,8 @@ int col_fft_r16(const float2* in, float2* out, long pitch, int cmpX, int H, cons
     case 1024: return launch_col<1024>(in, out, pitch, cmpX, b, d.tw, ops, "k_col_fft_r16<1024>", st);
     case 2048: return launch_col<2048>(in, out, pitch, cmpX, b, d.tw, ops, "k_col_fft_r16<2048>", st);
     default:
+      if (active_tuning().col_wide == 2)
+        return launch_col_pipe(in, out, pitch, cmpX, b, d.tw, ops, "k_col_fft_r16p<4096>", st);
       if (active_tuning().col_wide)
         return launch_col<4096, 2 * kR16Threads>(in, out, pitch, cmpX, b, d.tw, ops,
                                                  "k_col_fft_r16w<4096>", st);

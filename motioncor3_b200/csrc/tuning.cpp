@@ -2,6 +2,7 @@
 // written by mc3_autotune and read by mc3_load_tuning.
 #include "tuning.h"
 
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -21,7 +22,7 @@ const Tuning& default_tuning() {
   static const Tuning d = [] {
     Tuning t;
     t.fft_r16 = env_int("MC3_FFT_R16", 1) != 0;
-    t.col_wide = env_int("MC3_FFT_COL_WIDE", 1) != 0;
+    t.col_wide = std::min(std::max(env_int("MC3_FFT_COL_WIDE", 1), 0), 2);
     t.gather_px = env_int("MC3_GATHER_PX", 2) == 1 ? 1 : 2;
     return t;
   }();
@@ -41,8 +42,9 @@ TuningScope::~TuningScope() { active_tuning() = saved; }
 
 std::vector<Tuning> tuning_candidates() {
   std::vector<Tuning> c;
+  // the column variants differ only in the radix-16 passes
   for (int r16 = 1; r16 >= 0; --r16)
-    for (int wide = 0; wide <= 1; ++wide)
+    for (int wide = 0; wide <= (r16 ? 2 : 0); ++wide)
       for (int px = 2; px >= 1; --px) {
         Tuning t;
         t.fft_r16 = r16;

@@ -12,7 +12,8 @@ namespace mc3 {
 
 struct Tuning {
   int fft_r16 = 1;    // radix-16 register passes for power-of-two lengths (else radix 8)
-  int col_wide = 1;   // 4096-point column passes with twice the columns per CTA
+  int col_wide = 1;   // 4096-point column passes: 0 two columns per CTA, 1 four columns
+                      // per CTA, 2 persistent with the next columns prefetched
   int gather_px = 2;  // pixels per thread in the local-motion gather (1 or 2)
 };
 

@@ -19,6 +19,7 @@ the inputs are stored as the image parameters.
 Run from the repository root: python tests/golden/make_golden.py
 """
 import ctypes
+import hashlib
 import json
 import os
 import re
@@ -119,7 +120,10 @@ def ctf_fits():
         res = np.zeros(6, np.float32)
         L.ref_ctf_search(np.ascontiguousarray(avg).ctypes.data_as(ctypes.c_void_p), f(pn), f(c["kv"]),
                          f(c["cs"]), f(c["ac"]), f(c["ext_phase"]), res.ctypes.data_as(ctypes.c_void_p))
-        out.append(dict(c, pix_n=float(pn), res6=[float(v) for v in res]))
+        # the spectrum's hash, so that a change of the input (the image is
+        # made with numpy's FFT) is told apart from a change of the search
+        sha = hashlib.sha256(np.ascontiguousarray(avg, np.float32).tobytes()).hexdigest()
+        out.append(dict(c, pix_n=float(pn), spectrum_sha256=sha, res6=[float(v) for v in res]))
     return {"source": "FindCtf/CFindCtf2D.cpp, CFindDefocus1D.cpp, CFindDefocus2D.cpp", "cases": out}
 
 

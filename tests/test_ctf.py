@@ -201,8 +201,15 @@ def test_searches_match_golden_reference_fits(oracle, ctf_shim):
     from conftest import make_ctf_image
     gold = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "ctf_fits.json")))
     assert len(gold["cases"]) == 3
+    import hashlib
     for c in gold["cases"]:
         avg, _, pn = oracle.ctf_spectrum(make_ctf_image(**c["image"]), c["pix"])
+        sha = hashlib.sha256(np.ascontiguousarray(avg, np.float32).tobytes()).hexdigest()
+        # the input first: the micrograph is made with numpy's FFT, and a
+        # changed spectrum is a changed input, not a changed search
+        assert sha == c["spectrum_sha256"], (
+            "averaged spectrum differs from the one the golden fits were made from "
+            "(numpy's FFT changed?); rerun tests/golden/make_golden.py", c["image"])
         assert np.float32(pn) == np.float32(c["pix_n"])
         ref = np.array(c["res6"], np.float32)
         got = oracle.ctf_search(avg, pn, c["kv"], c["cs"], c["ac"], c["ext_phase"])
