@@ -241,6 +241,22 @@ def _dp(t) -> ctypes.c_void_p:
     return ctypes.c_void_p(t.data_ptr())
 
 
+def _need(t, what: str, shape=None, dtype=None) -> None:
+    """Checks a device tensor handed to the library as a raw pointer (the C
+    entry points cannot see its size): a contiguous CUDA tensor, of the given
+    dtype, whose shape equals `shape` (None entries are free)."""
+    if not (hasattr(t, "data_ptr") and getattr(t, "is_cuda", False)):
+        raise ValueError(f"{what}: a CUDA tensor is required")
+    if not t.is_contiguous():
+        raise ValueError(f"{what}: a contiguous tensor is required")
+    if dtype is not None and str(t.dtype) != f"torch.{dtype}":
+        raise ValueError(f"{what}: dtype {t.dtype}, {dtype} required")
+    if shape is not None:
+        if len(t.shape) != len(shape) or any(w is not None and int(g) != int(w)
+                                             for g, w in zip(t.shape, shape)):
+            raise ValueError(f"{what}: shape {tuple(t.shape)}, {tuple(shape)} required")
+
+
 @dataclasses.dataclass
 class Params:
     """In-scope MotionCor3 options; defaults of CInput::CInput (CInput.cpp:82-127)."""
@@ -672,7 +688,9 @@ class ShiftProposal:
         """One Adam step on a batch (torch CUDA tensors or host arrays); mean loss."""
         loss = ctypes.c_double()
         if hasattr(x, "data_ptr"):
+            _need(x, "train_step x", (None, 2, None, None), "float32")
             n, _, h, w = x.shape
+            _need(target, "train_step target", (n, self.nout), "float32")
             _check(_lib().mc3_proposal_train_step(self._h, _dp(x), _dp(target), n, h, w, 1, lr,
                                                   ctypes.byref(loss)), "mc3_proposal_train_step")
         else:
@@ -688,6 +706,7 @@ class ShiftProposal:
         n, _, h, w = x.shape
         out = np.zeros((n, self.nout), np.float32)
         if hasattr(x, "data_ptr"):
+            _need(x, "predict x", (None, 2, None, None), "float32")
             _check(_lib().mc3_proposal_predict(self._h, _dp(x), n, h, w, 1, out.ctypes.data),
                    "mc3_proposal_predict")
         else:
@@ -700,14 +719,17 @@ class ShiftProposal:
     def pair_inputs(frames, pairs, bin: int, out):
         """Inputs of frame pairs from a device movie (torch float32 [nz][ny][nx])
         into out (torch float32 [n][2][ny/bin][nx/bin])."""
+        _need(frames, "pair_inputs frames", (None, None, None), "float32")
         nz, ny, nx = frames.shape
-        pr = np.ascontiguousarray(pairs, np.int32)
+        pr = np.ascontiguousarray(pairs, np.int32).reshape(-1, 2)
+        _need(out, "pair_inputs out", (pr.shape[0], 2, ny // bin, nx // bin), "float32")
         _check(_lib().mc3_proposal_pair_inputs(_dp(frames), nx, ny, nz, pr.ctypes.data, pr.shape[0],
                                                bin, _dp(out), _stream()), "mc3_proposal_pair_inputs")
 
 
 def fft_forward(frames, nx: int, ny: int, normalise: bool = True) -> None:
     """In place on a float32 CUDA tensor [nz][ny][2*(nx//2+1)]."""
+    _need(frames, "fft_forward frames", (None, ny, 2 * (nx // 2 + 1)), "float32")
     nz = frames.shape[0]
     _check(_lib().mc3_fft_forward(_dp(frames), nx, ny, nz, int(normalise), _stream()), "mc3_fft_forward")
 
@@ -717,11 +739,19 @@ def rfft_rows(src, dst, nx: int, method: int = 0) -> None:
     [rows][>= nx/2+1] (complex64, device): method 0 the FP32 FFT, 1 the
     split-precision BF16 DFT GEMM on the tensor cores."""
     rows = src.shape[0]
+    ok = (getattr(src, "is_cuda", False) and getattr(dst, "is_cuda", False) and
+          str(src.dtype) == "torch.float32" and str(dst.dtype) == "torch.complex64" and
+          src.dim() == 2 and dst.dim() == 2 and src.stride(1) == 1 and dst.stride(1) == 1 and
+          src.shape[1] >= nx and dst.shape[0] >= rows and dst.shape[1] >= nx // 2 + 1)
+    if not ok:
+        raise ValueError("rfft_rows: src float32 CUDA [rows][>= nx] and dst complex64 CUDA "
+                         "[>= rows][>= nx/2+1], both with unit inner stride")
     _check(_lib().mc3_rfft_rows(_dp(src), src.stride(0), _dp(dst), dst.stride(0), nx, rows, method,
                                 _stream()), "mc3_rfft_rows")
 
 
 def fft_inverse(frames, nx: int, ny: int) -> None:
+    _need(frames, "fft_inverse frames", (None, ny, 2 * (nx // 2 + 1)), "float32")
     nz = frames.shape[0]
     _check(_lib().mc3_fft_inverse(_dp(frames), nx, ny, nz, _stream()), "mc3_fft_inverse")
 

@@ -291,3 +291,39 @@ def test_proposal_and_warm_start_entry_points_check_their_arguments(mc3lib):
     assert L.mc3_set_first_iterate(None, None, 0, 0) == api.MC3_EINVAL
     assert L.mc3_autotune(None, 64, 64, 4, None, None) == api.MC3_EINVAL
     assert L.mc3_load_tuning(None, b"x.json") == api.MC3_EINVAL
+
+
+class _DeviceTensorStandIn:
+    """Enough of a CUDA tensor for the Python wrappers' argument checks,
+    which run before anything is handed to the library."""
+
+    def __init__(self, shape, dtype="float32"):
+        self.shape, self.dtype, self.is_cuda = tuple(shape), f"torch.{dtype}", True
+
+    def data_ptr(self):
+        return 0
+
+    def is_contiguous(self):
+        return True
+
+
+def test_device_wrappers_check_output_sizes(mc3lib):
+    """The C entry points take raw device pointers and cannot see a buffer's
+    size, so the wrappers compare each tensor's shape with what the call
+    writes: an output sized for fewer frame pairs, a wrong target or a frame
+    of the wrong row length is refused with ValueError."""
+    from motioncor3_b200 import api
+    T = _DeviceTensorStandIn
+    pairs = np.array([[f, g] for f in range(16) for g in range(16) if f != g], np.int32)
+    with pytest.raises(ValueError, match="pair_inputs out"):
+        api.ShiftProposal.pair_inputs(T((16, 256, 256)), pairs, 2, T((16, 2, 128, 128)))
+    with pytest.raises(ValueError, match="pair_inputs out"):
+        api.ShiftProposal.pair_inputs(T((16, 256, 256)), pairs, 2, T((240, 2, 64, 64)))
+    with pytest.raises(ValueError, match="fft_forward"):
+        api.fft_forward(T((2, 64, 64)), 64, 64)
+    with pytest.raises(ValueError, match="fft_inverse"):
+        api.fft_inverse(T((2, 64, 66), "complex64"), 64, 64)
+    net = api.ShiftProposal.__new__(api.ShiftProposal)  # no device state needed for the check
+    net.nout, net._h = 2, None
+    with pytest.raises(ValueError, match="train_step target"):
+        net.train_step(T((8, 2, 32, 32)), T((4, 2)))

@@ -70,7 +70,7 @@ def _pairs_and_labels(torch, api, movies, shifts, bin_, all_pairs=False):
         else:
             pairs = np.array([[f, ref] for f in range(nz)], np.int32)
         fr = torch.from_numpy(m.frames).cuda()
-        x = torch.empty((nz, 2, ny // bin_, nx // bin_), dtype=torch.float32, device="cuda")
+        x = torch.empty((len(pairs), 2, ny // bin_, nx // bin_), dtype=torch.float32, device="cuda")
         api.ShiftProposal.pair_inputs(fr, pairs, bin_, x)
         xs.append(x)
         ts.append(torch.from_numpy(((s[pairs[:, 0]] - s[pairs[:, 1]]) / 4.0).astype(np.float32)).cuda())
