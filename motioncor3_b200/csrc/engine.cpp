@@ -1086,6 +1086,14 @@ int Engine::process_with(const mc3_movie& mv, mc3_result* out, const Tuning& tun
     if (cst == kOk) out->ctf_done = 1;
     else if (cst != kEUnsupported) return cst;  // too small for a 512 x 512 tile: no estimate
   }
+  if (active_tuning().row_pipe) {  // a pipelined pass that gave up waiting for its copies
+    int flag = 0;
+    MC3_TRY(fft_pipe_error(true, &flag));
+    if (flag) {
+      last_error = "a pipelined FFT pass timed out waiting for its bulk copies";
+      return kECuda;
+    }
+  }
   // ---- 9. result tables ----
   if (out) {
     out->n_sums = g.nSums;

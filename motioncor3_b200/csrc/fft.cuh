@@ -79,6 +79,9 @@ int col_fft_r16(const float2* in, float2* out, long pitch, int cmpX, int H, cons
                 const ColOps& ops, cudaStream_t st);
 // MC3_FFT_R16=0 disables them (A/B runs).
 bool r16_enabled();
+// Whether a pipelined pass gave up waiting for its copies (*flag != 0);
+// `reset` clears the record.  Synchronises with the device.
+int fft_pipe_error(bool reset, int* flag);
 
 // Row real FFT: rows of W reals (row pitch in_pitch floats) -> W/2+1
 // complex (row pitch out_pitch complex), multiplied by `scale`.  In-place

@@ -235,6 +235,240 @@ __global__ void __launch_bounds__(kR16Threads, 2) k_row_r2c_r16(const float* __r
 }
 
 // ---------------------------------------------------------------------
+// Pipelined row R2C for rows of 4096 reals (M = 2048 complex points):
+// persistent CTAs of 256 threads, two rows per unit, three CTAs per SM.
+// Each row of the next unit arrives by one bulk copy (cp.async.bulk on the
+// TMA unit, completing on an mbarrier), issued as soon as the current
+// unit's first radix-16 stage has read the staging slots, so the copy runs
+// under the rest of the transform, the post-processing and the stores.
+// The padded rows (W+2 floats) start on 8-byte boundaries, so each copy
+// starts at the 16-byte boundary at or below its row and ends at most 8
+// bytes past the row's data, inside the row's own padding; the leading
+// bytes belong to the previous row and are not used.  Every wait on the
+// mbarrier is bounded; a CTA that gives up records it in g_fft_pipe_error
+// (fft_pipe_error) and leaves.
+// ---------------------------------------------------------------------
+namespace {
+constexpr int kRowPM = 2048;
+constexpr int kRowPRows = 2;
+constexpr int kRowPT = kRowPM / 16 * kRowPRows;  // 256
+constexpr int kRowPSlot = 2 * kRowPM + 8;        // floats per staged row (16-byte multiple)
+constexpr int kRowPLD = spad16_len(kRowPM + 1);
+constexpr size_t kRowPStage = (size_t)kRowPRows * kRowPSlot * sizeof(float);
+constexpr size_t kRowPSmem = 16 + kRowPStage + (size_t)kRowPRows * kRowPLD * sizeof(float2);
+static_assert(kRowPStage % 16 == 0, "bulk copy destinations on 16-byte boundaries");
+// Longest wait on one mbarrier (about 1 s at the B200's clock).
+constexpr long long kPipeWaitCycles = 2000000000ll;
+
+__device__ int g_fft_pipe_error;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Polls the mbarrier phase of the given parity; false after
+// kPipeWaitCycles or once another CTA has recorded an error.
+__device__ __forceinline__ bool pipe_wait(uint32_t bar, uint32_t parity) {
+  const long long t0 = clock64();
+  for (unsigned i = 0;; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if ((i & 255u) == 255u) {
+      if (*reinterpret_cast<volatile int*>(&g_fft_pipe_error)) return false;
+      if (clock64() - t0 > kPipeWaitCycles) return false;
+    }
+  }
+}
+}  // namespace
+
+__global__ void __launch_bounds__(kRowPT, 3) k_row_r2c_r16p(const float* in, long in_pitch,
+                                                            float2* out, long out_pitch, int H,
+                                                            Batch bt, const float2* __restrict__ tw,
+                                                            float scale, int rgroups, int nunits) {
+  constexpr int M = kRowPM;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float* stage = reinterpret_cast<float*>(smraw + 16);
+  float2* A = reinterpret_cast<float2*>(smraw + 16 + kRowPStage);
+  const uint32_t bar = smem_addr(smraw);
+  const int rr = threadIdx.x / (M / 16);
+  const int j = threadIdx.x % (M / 16);
+  // One arrive with the unit's byte count, then one copy per row.
+  auto issue = [&](int u) {
+    const int item = u / rgroups, r0 = (u % rgroups) * kRowPRows;
+    const int nr = min(kRowPRows, H - r0);
+    const float* base = in + batch_in_off(bt, item) + (long)r0 * in_pitch;
+    uint32_t total = 0;
+    for (int r = 0; r < nr; ++r) {
+      const uintptr_t a = reinterpret_cast<uintptr_t>(base + (long)r * in_pitch);
+      total += ((uint32_t)(a & 15) + 2 * M * 4 + 15) & ~15u;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(total)
+                 : "memory");
+    for (int r = 0; r < nr; ++r) {
+      const uintptr_t a = reinterpret_cast<uintptr_t>(base + (long)r * in_pitch);
+      const uint32_t lead = (uint32_t)(a & 15);
+      const uint32_t bytes = (lead + 2 * M * 4 + 15) & ~15u;
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+              smem_addr(stage + r * kRowPSlot)),
+          "l"(a - lead), "r"(bytes), "r"(bar)
+          : "memory");
+    }
+  };
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(1) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  int u = blockIdx.x;
+  if (threadIdx.x == 0 && u < nunits) issue(u);
+  for (int k = 0; u < nunits; u += gridDim.x, ++k) {
+    const bool ok = pipe_wait(bar, (uint32_t)(k & 1));
+    // also the barrier after the previous unit's stores from A
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) atomicOr(&g_fft_pipe_error, 1);
+      return;
+    }
+    const int item = u / rgroups, r0 = (u % rgroups) * kRowPRows;
+    const int nr = min(kRowPRows, H - r0);
+    const bool live = rr < nr;
+    const uintptr_t a = reinterpret_cast<uintptr_t>(in + batch_in_off(bt, item) +
+                                                    (long)(r0 + rr) * in_pitch);
+    const float* srow = stage + rr * kRowPSlot + ((a & 15) >> 2);
+    auto load = [&](int m) {
+      return live ? *reinterpret_cast<const float2*>(srow + 2 * m) : c2(0.f, 0.f);
+    };
+    auto none = [](int, float2) {};
+    const int next = u + (int)gridDim.x;
+    auto after_first = [&]() {
+      if (threadIdx.x == 0 && next < nunits) issue(next);
+    };
+    fft_r16<-1, M, false, true>(A + rr * kRowPLD, j, tw, 2, load, none, after_first);
+    constexpr int NP = M / 2 + 1;
+    for (int t = threadIdx.x; t < nr * NP; t += kRowPT) {
+      const int r = t / NP, p = t % NP;
+      r2c_post_pair<4>(A + r * kRowPLD, M, p, tw, scale);
+    }
+    __syncthreads();
+    float2* dst = out + (long)item * bt.out_stride + (long)r0 * out_pitch;
+    for (int t = threadIdx.x; t < nr * (M + 1); t += kRowPT) {
+      const int r = t / (M + 1), kk = t % (M + 1);
+      dst[(long)r * out_pitch + kk] = A[r * kRowPLD + spad16(kk)];
+    }
+  }
+}
+
+// Pipelined row C2R for rows of 4096 reals, the counterpart of
+// k_row_r2c_r16p: the next unit's half-spectrum rows (2049 complex) arrive
+// by bulk copies issued once the current unit's rows have been moved into
+// the padded work buffer.  A row that starts on a 16-byte boundary is copied
+// without its Nyquist term (2048 values: the whole row would end 8 bytes
+// into the next one), and that term is read directly; a row that starts 8
+// bytes past a boundary is copied with the previous row's last value in
+// front, which is not used.
+__global__ void __launch_bounds__(kRowPT, 3) k_row_c2r_r16p(const float2* in, long in_pitch,
+                                                            float* out, long out_pitch, int H,
+                                                            Batch bt, const float2* __restrict__ tw,
+                                                            int keep_im, int rgroups, int nunits) {
+  constexpr int M = kRowPM;
+  constexpr int SLOT = kRowPSlot / 2;  // float2 per staged row
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float2* stage = reinterpret_cast<float2*>(smraw + 16);
+  float2* A = reinterpret_cast<float2*>(smraw + 16 + kRowPStage);
+  const uint32_t bar = smem_addr(smraw);
+  const int rr = threadIdx.x / (M / 16);
+  const int j = threadIdx.x % (M / 16);
+  auto row_bytes = [](uintptr_t a) -> uint32_t { return (a & 15) ? 8u + 8u * (M + 1) : 8u * M; };
+  auto issue = [&](int u) {
+    const int item = u / rgroups, r0 = (u % rgroups) * kRowPRows;
+    const int nr = min(kRowPRows, H - r0);
+    const float2* base = in + batch_in_off(bt, item) + (long)r0 * in_pitch;
+    uint32_t total = 0;
+    for (int r = 0; r < nr; ++r) total += row_bytes(reinterpret_cast<uintptr_t>(base + (long)r * in_pitch));
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(total)
+                 : "memory");
+    for (int r = 0; r < nr; ++r) {
+      const uintptr_t a = reinterpret_cast<uintptr_t>(base + (long)r * in_pitch);
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+              smem_addr(stage + r * SLOT)),
+          "l"(a & ~(uintptr_t)15), "r"(row_bytes(a)), "r"(bar)
+          : "memory");
+    }
+  };
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(1) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  int u = blockIdx.x;
+  if (threadIdx.x == 0 && u < nunits) issue(u);
+  for (int k = 0; u < nunits; u += gridDim.x, ++k) {
+    const bool ok = pipe_wait(bar, (uint32_t)(k & 1));
+    // also the barrier after the previous unit's last stage read A
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) atomicOr(&g_fft_pipe_error, 1);
+      return;
+    }
+    const int item = u / rgroups, r0 = (u % rgroups) * kRowPRows;
+    const int nr = min(kRowPRows, H - r0);
+    const float2* src = in + batch_in_off(bt, item) + (long)r0 * in_pitch;
+    for (int t = threadIdx.x; t < nr * (M + 1); t += kRowPT) {
+      const int r = t / (M + 1), kk = t % (M + 1);
+      const float2* row = src + (long)r * in_pitch;
+      const bool lead = (reinterpret_cast<uintptr_t>(row) & 15) != 0;
+      A[r * kRowPLD + spad16(kk)] =
+          (kk == M && !lead) ? row[M] : stage[r * SLOT + (lead ? 1 : 0) + kk];
+    }
+    __syncthreads();  // the staging slots are free again
+    const int next = u + (int)gridDim.x;
+    if (threadIdx.x == 0 && next < nunits) issue(next);
+    constexpr int NP = M / 2 + 1;
+    for (int t = threadIdx.x; t < nr * NP; t += kRowPT) {
+      const int r = t / NP, p = t % NP;
+      c2r_pre_pair<4>(A + r * kRowPLD, M, p, tw, keep_im);
+    }
+    __syncthreads();
+    const bool live = rr < nr;
+    float* dst = out + (long)item * bt.out_stride + (long)(r0 + rr) * out_pitch;
+    const bool pair = ((reinterpret_cast<uintptr_t>(out + (long)item * bt.out_stride) & 7) == 0) &&
+                      !(out_pitch & 1);
+    auto none = [](int) { return c2(0.f, 0.f); };
+    auto store = [&](int m, float2 v) {
+      if (!live) return;
+      float* p = dst + 2 * m;
+      if (pair) {
+        *reinterpret_cast<float2*>(p) = v;
+      } else {
+        p[0] = v.x;
+        p[1] = v.y;
+      }
+    };
+    fft_r16<1, M, true, false>(A + rr * kRowPLD, j, tw, 2, none, store);
+  }
+}
+
+int fft_pipe_error(bool reset, int* flag) {
+  int v = 0;
+  MC3_CUDA(cudaMemcpyFromSymbol(&v, g_fft_pipe_error, sizeof(int)));
+  if (reset && v) {
+    const int z = 0;
+    MC3_CUDA(cudaMemcpyToSymbol(g_fft_pipe_error, &z, sizeof(int)));
+  }
+  *flag = v;
+  return kOk;
+}
+
+// ---------------------------------------------------------------------
 // Row C2R (unnormalised): rows loaded to shared memory, paired
 // pre-processing in place, then the transform from shared memory with the
 // last stage storing real pairs straight to global memory.
@@ -358,6 +592,40 @@ int launch_r2c(const float* in, long in_pitch, float2* out, long out_pitch, int 
   MC3_CHECK_LAUNCH(name);
   return kOk;
 }
+// The pipelined R2C's copies need every row to start on an 8-byte boundary
+// of a 16-byte-aligned buffer, with the row's 8 bytes of padding after it.
+bool row_pipe_fits(const float* in, long in_pitch, int W, const Batch& b) {
+  return W == 2 * kRowPM && (reinterpret_cast<uintptr_t>(in) & 15) == 0 && in_pitch % 2 == 0 &&
+         in_pitch >= W + 2 && (b.nf <= 1 || b.in_stride % 2 == 0) && b.patch_off == nullptr;
+}
+int launch_r2c_pipe(const float* in, long in_pitch, float2* out, long out_pitch, int H,
+                    const Batch& b, const float2* tw, float scale, cudaStream_t st) {
+  const int rgroups = ceil_div(H, kRowPRows);
+  const long nunits_l = (long)rgroups * b.items;
+  if (nunits_l > 0x7fffffffL) return kEUnsupported;
+  const int nunits = (int)nunits_l;
+  const int grid = std::min(nunits, 3 * sm_count());
+  MC3_TRY(set_smem_attr(k_row_r2c_r16p, kRowPSmem));
+  prof::Scope ps("k_row_r2c_r16p<2048>", (double)b.items * H * (2 * kRowPM * 4.0 + (kRowPM + 1) * 8.0), st);
+  k_row_r2c_r16p<<<grid, kRowPT, kRowPSmem, st>>>(in, in_pitch, out, out_pitch, H, b, tw, scale,
+                                                  rgroups, nunits);
+  MC3_CHECK_LAUNCH("k_row_r2c_r16p<2048>");
+  return kOk;
+}
+int launch_c2r_pipe(const float2* in, long in_pitch, float* out, long out_pitch, int H,
+                    const Batch& b, const float2* tw, int keep_im, cudaStream_t st) {
+  const int rgroups = ceil_div(H, kRowPRows);
+  const long nunits_l = (long)rgroups * b.items;
+  if (nunits_l > 0x7fffffffL) return kEUnsupported;
+  const int nunits = (int)nunits_l;
+  const int grid = std::min(nunits, 3 * sm_count());
+  MC3_TRY(set_smem_attr(k_row_c2r_r16p, kRowPSmem));
+  prof::Scope ps("k_row_c2r_r16p<2048>", (double)b.items * H * (2 * kRowPM * 4.0 + (kRowPM + 1) * 8.0), st);
+  k_row_c2r_r16p<<<grid, kRowPT, kRowPSmem, st>>>(in, in_pitch, out, out_pitch, H, b, tw, keep_im,
+                                                  rgroups, nunits);
+  MC3_CHECK_LAUNCH("k_row_c2r_r16p<2048>");
+  return kOk;
+}
 template <int M>
 int launch_c2r(const float2* in, long in_pitch, float* out, long out_pitch, int H, const Batch& b,
                const float2* tw, const char* name, int keep_im, cudaStream_t st) {
@@ -410,7 +678,10 @@ int row_r2c_r16(const float* in, long in_pitch, float2* out, long out_pitch, int
     case 256: return launch_r2c<256>(in, in_pitch, out, out_pitch, H, b, d.tw, scale, "k_row_r2c_r16<256>", st);
     case 512: return launch_r2c<512>(in, in_pitch, out, out_pitch, H, b, d.tw, scale, "k_row_r2c_r16<512>", st);
     case 1024: return launch_r2c<1024>(in, in_pitch, out, out_pitch, H, b, d.tw, scale, "k_row_r2c_r16<1024>", st);
-    default: return launch_r2c<2048>(in, in_pitch, out, out_pitch, H, b, d.tw, scale, "k_row_r2c_r16<2048>", st);
+    default:
+      if (active_tuning().row_pipe && row_pipe_fits(in, in_pitch, W, b))
+        return launch_r2c_pipe(in, in_pitch, out, out_pitch, H, b, d.tw, scale, st);
+      return launch_r2c<2048>(in, in_pitch, out, out_pitch, H, b, d.tw, scale, "k_row_r2c_r16<2048>", st);
   }
 }
 
@@ -428,7 +699,12 @@ int row_c2r_r16(const float2* in, long in_pitch, float* out, long out_pitch, int
     case 256: return launch_c2r<256>(in, in_pitch, out, out_pitch, H, b, d.tw, "k_row_c2r_r16<256>", keep_im, st);
     case 512: return launch_c2r<512>(in, in_pitch, out, out_pitch, H, b, d.tw, "k_row_c2r_r16<512>", keep_im, st);
     case 1024: return launch_c2r<1024>(in, in_pitch, out, out_pitch, H, b, d.tw, "k_row_c2r_r16<1024>", keep_im, st);
-    default: return launch_c2r<2048>(in, in_pitch, out, out_pitch, H, b, d.tw, "k_row_c2r_r16<2048>", keep_im, st);
+    default:
+      // the copies need a 16-byte-aligned buffer; rows then start on 8-byte boundaries
+      if (active_tuning().row_pipe && (reinterpret_cast<uintptr_t>(in) & 15) == 0 &&
+          b.patch_off == nullptr)
+        return launch_c2r_pipe(in, in_pitch, out, out_pitch, H, b, d.tw, keep_im, st);
+      return launch_c2r<2048>(in, in_pitch, out, out_pitch, H, b, d.tw, "k_row_c2r_r16<2048>", keep_im, st);
   }
 }
 

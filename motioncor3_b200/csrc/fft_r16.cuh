@@ -186,11 +186,18 @@ __device__ __forceinline__ void fft_r16_rest(float2* buf, int j, const float2* _
 // first stage; store(idx, value) receives the output y[idx] of the last
 // stage (natural order).  With LAST_TO_SMEM the last stage writes buf
 // instead (callers that post-process in shared memory); with
-// FIRST_FROM_SMEM the first stage reads buf (load is not used).  All
-// threads of the CTA must call it.
-template <int DIR, int N, bool FIRST_FROM_SMEM, bool LAST_TO_SMEM, class LoadF, class StoreF>
+// FIRST_FROM_SMEM the first stage reads buf (load is not used).  after_first()
+// runs once the first stage's inputs have all been read (after the barrier
+// that follows the first stage; not called when the first stage is the
+// last).  All threads of the CTA must call it.
+struct NoHook {
+  __device__ void operator()() const {}
+};
+template <int DIR, int N, bool FIRST_FROM_SMEM, bool LAST_TO_SMEM, class LoadF, class StoreF,
+          class HookF = NoHook>
 __device__ __forceinline__ void fft_r16(float2* buf, int j, const float2* __restrict__ tw,
-                                        int tws, LoadF load, StoreF store) {
+                                        int tws, LoadF load, StoreF store,
+                                        HookF after_first = HookF()) {
   auto to_smem = [&](int idx, float2 x) { buf[spad16(idx)] = x; };
   // stage 0
   {
@@ -210,6 +217,7 @@ __device__ __forceinline__ void fft_r16(float2* buf, int j, const float2* __rest
     } else {
       r16_compute<DIR, N, 0>(v, j, tw, tws, to_smem);
       __syncthreads();
+      after_first();
     }
   }
   fft_r16_rest<DIR, N, 1, LAST_TO_SMEM>(buf, j, tw, tws, store);

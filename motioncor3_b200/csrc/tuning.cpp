@@ -24,6 +24,7 @@ const Tuning& default_tuning() {
     t.fft_r16 = env_int("MC3_FFT_R16", 1) != 0;
     t.col_wide = std::min(std::max(env_int("MC3_FFT_COL_WIDE", 1), 0), 2);
     t.gather_px = env_int("MC3_GATHER_PX", 2) == 1 ? 1 : 2;
+    t.row_pipe = env_int("MC3_FFT_ROW_PIPE", 0) != 0;
     return t;
   }();
   return d;
@@ -50,6 +51,7 @@ std::vector<Tuning> tuning_candidates() {
         t.fft_r16 = r16;
         t.col_wide = wide;
         t.gather_px = px;
+        t.row_pipe = wide == 2;  // the persistent passes go together
         c.push_back(t);
       }
   return c;
@@ -121,6 +123,7 @@ int parse_tuning_json(const std::string& text, std::vector<TuningEntry>* out) {
     const char* ms = strstr(p, "\"ms\": ");
     if (ms && ms < end) e.best_ms = atof(ms + 6);
     if (e.best.gather_px != 1) e.best.gather_px = 2;
+    e.best.row_pipe = e.best.col_wide == 2;  // the persistent passes go together
     // the candidates: {"fft_r16": a, "col_wide": b, "gather_px": c, "ms": t} each
     if (cpos != std::string::npos && cpos < eol) {
       const char* q = text.c_str() + cpos;
@@ -131,6 +134,7 @@ int parse_tuning_json(const std::string& text, std::vector<TuningEntry>* out) {
         if (sscanf(q, "{\"fft_r16\": %d, \"col_wide\": %d, \"gather_px\": %d, \"ms\": %lf}",
                    &t.fft_r16, &t.col_wide, &t.gather_px, &tms) != 4)
           return 1;
+        t.row_pipe = t.col_wide == 2;
         e.cand.push_back(t);
         e.cand_ms.push_back(tms);
         ++q;

@@ -3,7 +3,8 @@
 // The launch wrappers read the variant to use from the calling thread's
 // active Tuning; the engine makes its table's entry for the movie's size
 // active for the duration of a movie.  Without an entry the defaults hold
-// (set from MC3_FFT_R16, MC3_FFT_COL_WIDE and MC3_GATHER_PX when present).
+// (set from MC3_FFT_R16, MC3_FFT_COL_WIDE, MC3_GATHER_PX and MC3_FFT_ROW_PIPE when
+// present).
 #pragma once
 #include <string>
 #include <vector>
@@ -15,6 +16,7 @@ struct Tuning {
   int col_wide = 1;   // 4096-point column passes: 0 two columns per CTA, 1 four columns
                       // per CTA, 2 persistent with the next columns prefetched
   int gather_px = 2;  // pixels per thread in the local-motion gather (1 or 2)
+  int row_pipe = 0;   // 4096-real row R2C and C2R: persistent, next rows by bulk copies
 };
 
 // Defaults (environment) and the calling thread's active choices.

@@ -1,7 +1,9 @@
 """The three 4096-point column passes (MC3_FFT_COL_WIDE = 0: two columns per
 CTA, 1: four columns per CTA, 2: persistent CTAs that prefetch the next
-four columns with cp.async while transforming the current ones) run the
-same radix-16 arithmetic in the same order, so their results are
+four columns with cp.async while transforming the current ones) and the two
+4096-real row R2C passes (MC3_FFT_ROW_PIPE = 0: one load phase per CTA, 1:
+persistent CTAs whose next rows arrive by bulk copies on an mbarrier) run
+the same radix-16 arithmetic in the same order, so their results are
 identical bit for bit: the forward and inverse transforms of 4096^2 frames
 (checked against FP64 numpy as well) and a whole 4096^2 movie with 5x5
 patches (shifts and sums).  Each variant runs in its own process, since the
@@ -14,6 +16,9 @@ import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
+
+# (MC3_FFT_COL_WIDE, MC3_FFT_ROW_PIPE)
+VARIANTS = [(1, 0), (0, 0), (2, 0), (2, 1)]
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -53,9 +58,11 @@ def variants(mc3lib, tmp_path_factory):
     script = d / "run.py"
     script.write_text(SCRIPT)
     res = {}
-    for w in (0, 1, 2):
-        env = dict(os.environ, MC3_FFT_COL_WIDE=str(w), MC3_FFT_R16="1")
-        out = d / f"v{w}.npz"
+    for w in VARIANTS:
+        col, row = w
+        env = dict(os.environ, MC3_FFT_COL_WIDE=str(col), MC3_FFT_ROW_PIPE=str(row),
+                   MC3_FFT_R16="1")
+        out = d / f"v{col}{row}.npz"
         p = subprocess.run([sys.executable, str(script), ROOT, str(out)], env=env,
                            capture_output=True, text=True, timeout=900)
         assert p.returncode == 0, p.stderr[-2000:]
@@ -64,17 +71,17 @@ def variants(mc3lib, tmp_path_factory):
 
 
 def test_forward_transform_against_fp64(variants):
-    v = variants[2]
+    v = variants[(2, 1)]
     n, cx = 4096, 2049
     spec = v["spec"][0].view(np.complex64)[:, :cx]
     ref = np.fft.rfft2(v["img0"].astype(np.float64)) / (n * n)
     err = np.abs(spec - ref).max() / np.abs(ref).max()
-    print(f"persistent column pass, 4096^2 forward: {err:.2e} of the spectrum maximum")
+    print(f"persistent column and row passes, 4096^2 forward: {err:.2e} of the spectrum maximum")
     assert err < 2e-6
 
 
 @pytest.mark.parametrize("key", ["spec", "inv", "gsh", "psh", "sums"])
 def test_column_variants_identical(variants, key):
-    a = variants[1][key]
-    for w in (0, 2):
+    a = variants[VARIANTS[0]][key]
+    for w in VARIANTS[1:]:
         assert np.array_equal(variants[w][key], a), (w, key)
