@@ -295,6 +295,17 @@ int mc3_set_alignment(mc3_ctx* ctx, const mc3_alignment* aln);
  * Consumed by the next mc3_process_movie; NULL clears it.  This is the entry
  * of the learned proposal (mc3_proposal_*). */
 int mc3_set_first_iterate(mc3_ctx* ctx, const float* global_xy, int nz, int max_iter);
+/* Patch centres of the following movies, centers_xy [n_patches][2] in
+ * full-frame pixels (as mc3_result.patch_centers), instead of the placement
+ * from the feature map (Align/CDetectFeatures.cpp:58-181, CPatchAlign's
+ * centre search): each patch is cut around the given centre, kept inside the
+ * alignment image.  Used to reproduce another run's patch layout -- for
+ * instance a run of the reference program, whose in-place feature-map
+ * normalisation (Align/GNormByStd2D.cu:7-40) can move its centres -- so that
+ * patch shifts and sums can be compared patch for patch.  Applies while
+ * n_patches equals the movie's patch count; NULL clears it.  No counterpart
+ * option in the reference. */
+int mc3_set_patch_centers(mc3_ctx* ctx, const float* centers_xy, int n_patches);
 /* CFmIntParam / CFmGroupParam set up from a frame-integration table: the
  * following movies (nz = n_raw) are rendered, dose-weighted with acc_dose
  * and grouped by raw-frame counts (CFmGroupParam::mGroupByRawSize,

@@ -171,6 +171,7 @@ _SIGS = {
     "mc3_rfft_rows": ([_VP, _I, _VP, _I, _I, _I, _I, _VP], _I),
     "mc3_submit": ([_VP, _VP, _VP, _VP], _I),
     "mc3_set_first_iterate": ([_VP, _VP, _I, _I], _I),
+    "mc3_set_patch_centers": ([_VP, _VP, _I], _I),
     "mc3_proposal_create": ([_VP, _I, _I, ctypes.c_uint, _I, _VP], _I),
     "mc3_proposal_destroy": ([_VP], _I),
     "mc3_proposal_num_params": ([_VP, _VP], _I),
@@ -581,6 +582,17 @@ class MotionCor3:
         g = np.ascontiguousarray(global_shifts, np.float32)
         _check(_lib().mc3_set_first_iterate(self._h, g.ctypes.data, g.shape[0], max_iter),
                "mc3_set_first_iterate")
+
+    def set_patch_centers(self, centers=None) -> None:
+        """Patch centres [P][2] (full-frame pixels) for the following movies
+        instead of the feature-based placement (mc3_set_patch_centers); None
+        clears them."""
+        if centers is None:
+            _check(_lib().mc3_set_patch_centers(self._h, None, 0), "mc3_set_patch_centers")
+            return
+        c = np.ascontiguousarray(centers, np.float32).reshape(-1, 2)
+        _check(_lib().mc3_set_patch_centers(self._h, c.ctypes.data, c.shape[0]),
+               "mc3_set_patch_centers")
 
     def load_tuning(self, json_path: str) -> None:
         _check(_lib().mc3_load_tuning(self._h, json_path.encode()), "mc3_load_tuning")

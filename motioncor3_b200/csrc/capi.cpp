@@ -432,6 +432,19 @@ int mc3_set_first_iterate(mc3_ctx* ctx, const float* global_xy, int nz, int max_
   return MC3_OK;
 }
 
+int mc3_set_patch_centers(mc3_ctx* ctx, const float* centers_xy, int n_patches) {
+  if (!ctx || queue_busy(ctx)) return MC3_EINVAL;
+  if (!centers_xy) {
+    ctx->eng->patch_centers_given.clear();
+    return MC3_OK;
+  }
+  if (n_patches < 1) return MC3_EINVAL;
+  for (int i = 0; i < 2 * n_patches; ++i)
+    if (!std::isfinite(centers_xy[i])) return MC3_EINVAL;
+  ctx->eng->patch_centers_given.assign(centers_xy, centers_xy + 2 * (size_t)n_patches);
+  return MC3_OK;
+}
+
 int mc3_set_alignment(mc3_ctx* ctx, const mc3_alignment* aln) {
   if (!ctx) return MC3_EINVAL;
   return ctx->eng->set_alignment(aln);

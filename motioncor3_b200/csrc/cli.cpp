@@ -294,7 +294,7 @@ int main(int argc, char** argv) {
                 "[-kV kv] [-Group g p] [-FmRef f] [-SumRange lo hi] [-PhaseOnly 0|1] [-SplitSum 0|1] "
                 "[-FtBin b] [-OutAln dir] [-InAln dir] [-OutStack 0|1 zbin] [-FmIntFile file] "
                 "[-Dark dark.mrc] [-RotGain r] [-FlipGain f] [-InvGain 0|1] [-Mag major minor angle] [-InFmMotion 0|1] [-Throw n] [-Trunc n] [-CorrInterp 0|1] [-DefectFile f] [-DefectMap f] [-OutStar 0|1] "
-                "[-LogDir dir] [-Gpu id]\n");
+                "[-LogDir dir] [-Gpu id] [-PatchCenters file (mc3 only: x y per line)]\n");
     return eSuccess;
   }
   Args A{argc, argv};
@@ -355,6 +355,8 @@ int main(int argc, char** argv) {
       for (int i = 0; i < 3; ++i) p.mag[i] = mg[i];
   }
   const std::string in_aln = A.str("-InAln");
+  // mc3 extension: "x y" per line, full-frame pixels (mc3_set_patch_centers)
+  const std::string patch_centers_file = A.str("-PatchCenters");
   const std::string fmint_file = A.str("-FmIntFile");
   int gpu[8];
   if (A.ints("-Gpu", gpu, 8) > 0) p.gpu = gpu[0];
@@ -643,6 +645,23 @@ int main(int argc, char** argv) {
     al.patch_centers = la.patch.empty() ? nullptr : la.centers.data();
     if ((s = mc3_set_alignment(ctx, &al)) != MC3_OK) {
       std::fprintf(stderr, "Error: %s\n", mc3_strerror(s));
+      mc3_destroy(ctx);
+      return eFailProcess;
+    }
+  }
+  if (!patch_centers_file.empty() && P > 0) {
+    std::vector<float> pcs;
+    if (FILE* fp = std::fopen(patch_centers_file.c_str(), "r")) {
+      float x, y;
+      while (std::fscanf(fp, "%f %f", &x, &y) == 2) {
+        pcs.push_back(x);
+        pcs.push_back(y);
+      }
+      std::fclose(fp);
+    }
+    if ((int)pcs.size() != 2 * P || (s = mc3_set_patch_centers(ctx, pcs.data(), P)) != MC3_OK) {
+      std::fprintf(stderr, "Error: -PatchCenters %s: %d patch centres needed\n",
+                   patch_centers_file.c_str(), P);
       mc3_destroy(ctx);
       return eFailProcess;
     }

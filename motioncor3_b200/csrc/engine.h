@@ -101,6 +101,9 @@ class Engine {
                    std::vector<host::StackShift>& shifts, std::vector<int>& iters,
                    std::vector<std::vector<float>>& errors, const float* init = nullptr,
                    int max_iter_init = 0, bool* converged = nullptr);
+  // Patch centres given by the caller (mc3_set_patch_centers): [P][2]
+  // full-frame pixels replacing the feature-based placement; empty: detect.
+  std::vector<float> patch_centers_given;
   // First iterate of the next movie's full-frame alignment (mc3_set_first_iterate).
   std::vector<float> first_iterate;  // [nz][2] full-frame pixels; empty: cold start
   int first_iterate_max = 3;

@@ -291,6 +291,8 @@ def test_proposal_and_warm_start_entry_points_check_their_arguments(mc3lib):
     assert L.mc3_set_first_iterate(None, None, 0, 0) == api.MC3_EINVAL
     assert L.mc3_autotune(None, 64, 64, 4, None, None) == api.MC3_EINVAL
     assert L.mc3_load_tuning(None, b"x.json") == api.MC3_EINVAL
+    c = (ctypes.c_float * 4)(10.0, 20.0, 30.0, 40.0)
+    assert L.mc3_set_patch_centers(None, c, 2) == api.MC3_EINVAL
 
 
 class _DeviceTensorStandIn:

@@ -5,8 +5,9 @@ and its use as the warm start of the full-frame alignment
 * The device forward and backward (FP32) against the FP64 oracle
   (oracle/cnn_oracle.cpp) with the same parameters: outputs, loss and every
   gradient entry.
-* Training on the GPU with the library's kernels on frame pairs of
-  synthetic movies whose labels are the plain aligner's own shifts; on
+* Training on the GPU with the library's kernels on frame pairs of 512
+  synthetic movies whose labels are the plain aligner's own shifts (each
+  batch flipped or transposed at random, the shift label with it); on
   held-out movies the proposal's error against the plain aligner is stated
   and must beat predicting no motion by a wide margin.
 * The warm start: with the proposal's first iterate the aligner runs at most
@@ -52,24 +53,29 @@ def test_device_gradients_match_fp64_oracle(mc3lib, oracle, torch_cuda, layers, 
 
 
 def _movies(n, seed0, nz=16, size=256):
-    """Movies with larger, jumpier drifts than the default generator's."""
+    """Movies with larger, jumpier drifts than the default generator's,
+    generated on the GPU (frames as CUDA tensors)."""
     from motioncor3_b200 import synthetic as S
-    return [S.make_movie(size, size, nz, dose=4.0, seed=seed0 + i, drift_step=1.5, jump=6.0)
+    return [S.make_movie(size, size, nz, dose=4.0, seed=seed0 + i, drift_step=1.5, jump=6.0,
+                         backend="torch", device="cuda")
             for i in range(n)]
 
 
-def _pairs_and_labels(torch, api, movies, shifts, bin_, all_pairs=False):
-    """Inputs (frame f, frame g) and targets s_f - s_g (px / 4): every
-    ordered pair of distinct frames (training), or g = the central frame."""
+def _pairs_and_labels(torch, api, movies, shifts, bin_, per_movie=None, seed=0):
+    """Inputs (frame f, frame g) and targets s_f - s_g (px / 4): per_movie
+    random ordered pairs of distinct frames (training), or g = the central
+    frame (per_movie None)."""
+    rng = np.random.default_rng(seed)
     xs, ts = [], []
     for m, s in zip(movies, shifts):
         nz, ny, nx = m.frames.shape
         ref = nz // 2
-        if all_pairs:
-            pairs = np.array([[f, g] for f in range(nz) for g in range(nz) if f != g], np.int32)
+        if per_movie:
+            every = np.array([[f, g] for f in range(nz) for g in range(nz) if f != g], np.int32)
+            pairs = every[rng.choice(len(every), per_movie, replace=False)]
         else:
             pairs = np.array([[f, ref] for f in range(nz)], np.int32)
-        fr = torch.from_numpy(m.frames).cuda()
+        fr = m.frames.contiguous()
         x = torch.empty((len(pairs), 2, ny // bin_, nx // bin_), dtype=torch.float32, device="cuda")
         api.ShiftProposal.pair_inputs(fr, pairs, bin_, x)
         xs.append(x)
@@ -81,21 +87,33 @@ def test_trained_proposal_warm_starts_the_aligner(mc3lib, torch_cuda):
     torch = torch_cuda
     from motioncor3_b200 import api
     p = api.Params(iter=15, tol=0.05, bft=(150, 100), pix_size=1.0)
-    train, test = _movies(96, 500), _movies(8, 900)
+    train, test = _movies(512, 500), _movies(8, 900)
     with api.MotionCor3(p) as mc:
         lab_tr = [mc.process(m.frames).global_shifts for m in train]
         cold = [mc.process(m.frames) for m in test]
     bin_ = 2
-    xtr, ttr = _pairs_and_labels(torch, api, train, lab_tr, bin_, all_pairs=True)
+    xtr, ttr = _pairs_and_labels(torch, api, train, lab_tr, bin_, per_movie=64)
     xte, tte = _pairs_and_labels(torch, api, test, [c.global_shifts for c in cold], bin_)
+    frames_test = [m.frames.cpu().numpy() for m in test]
+    del train
     net = api.ShiftProposal(TRAIN_SPEC, 2, seed=11)
     gen = torch.Generator(device="cuda").manual_seed(0)
+    aug = np.random.default_rng(1)
     losses = []
-    steps = 6000                      # 64-pair batches drawn from 23k pairs
+    steps = 6000                      # 64-pair batches drawn from 32k pairs
     for st in range(steps):
         i = torch.randint(0, xtr.shape[0], (64,), device="cuda", generator=gen)
+        xb, tb = xtr[i], ttr[i].clone()
+        # the same flip / transpose of both frames moves the shift with them
+        k = int(aug.integers(0, 8))
+        if k & 1:
+            xb, tb[:, 0] = xb.flip(-1), -tb[:, 0]
+        if k & 2:
+            xb, tb[:, 1] = xb.flip(-2), -tb[:, 1]
+        if k & 4:
+            xb, tb = xb.transpose(-1, -2), tb[:, [1, 0]]
         lr = 2e-3 if st < 4500 else 4e-4
-        losses.append(net.train_step(xtr[i].contiguous(), ttr[i].contiguous(), lr=lr))
+        losses.append(net.train_step(xb.contiguous(), tb.contiguous(), lr=lr))
     pred = net.predict(xte.contiguous()) * 4.0
     truth = tte.cpu().numpy() * 4.0
     err = float(np.sqrt(np.mean((pred - truth) ** 2)))
@@ -107,13 +125,13 @@ def test_trained_proposal_warm_starts_the_aligner(mc3lib, torch_cuda):
     assert err < 0.5 * base
     warm_iters, cold_iters, kept, worst, offs = [], [], [], 0.0, []
     with api.MotionCor3(p) as mc:
-        for k, (m, c) in enumerate(zip(test, cold)):
-            nz = m.frames.shape[0]
+        for k, (fr, c) in enumerate(zip(frames_test, cold)):
+            nz = fr.shape[0]
             d = pred[k * nz:(k + 1) * nz].astype(np.float64)
             # first iterate: the plain aligner's convention (its shifts of
             # these movies have about zero mean), in full-frame pixels
             mc.set_first_iterate((d - d.mean(0)).astype(np.float32), max_iter=3)
-            w = mc.process(m.frames)
+            w = mc.process(fr)
             assert w.first_iterate in (1, 2)
             dd = w.global_shifts.astype(np.float64) - c.global_shifts
             offs.append(np.round(dd.mean(0), 3).tolist())
