@@ -11,20 +11,23 @@ and its use as the warm start of the full-frame alignment
   held-out movies the proposal's error against the plain aligner is stated
   and must beat predicting no motion by a wide margin.
 * The warm start: with the proposal's first iterate the aligner runs at most
-  three iterations and keeps the plain aligner's shifts within 0.05 px; when
+  three iterations and keeps the plain aligner's shifts within 0.05 px (up
+  to a translation of the whole movie, which global mode does not fix); when
   it has not converged the plain aligner runs from zero (every iteration
   counted).  The iterations used are stated beside the cold start's, and the
   movies whose warm start converged used no more iterations than cold.
 """
+import time
+
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
 SPEC = [(2, 8, 5, 2, 2), (8, 16, 3, 2, 1), (16, 16, 3, 2, 1), (16, 16, 3, 2, 1)]
-# the trained network: 128^2 pairs -> 4^2 x 32 features -> pooled -> (dx, dy)
-TRAIN_SPEC = [(2, 16, 5, 2, 2), (16, 32, 3, 2, 1), (32, 32, 3, 2, 1), (32, 32, 3, 2, 1),
-              (32, 32, 3, 2, 1)]
+# the trained network: 128^2 pairs -> 4^2 x 64 features -> pooled -> (dx, dy)
+TRAIN_SPEC = [(2, 16, 5, 2, 2), (16, 32, 3, 2, 1), (32, 64, 3, 2, 1), (64, 64, 3, 2, 1),
+              (64, 64, 3, 2, 1)]
 
 
 @pytest.mark.parametrize("layers,size,batch", [
@@ -100,7 +103,8 @@ def test_trained_proposal_warm_starts_the_aligner(mc3lib, torch_cuda):
     gen = torch.Generator(device="cuda").manual_seed(0)
     aug = np.random.default_rng(1)
     losses = []
-    steps = 6000                      # 64-pair batches drawn from 32k pairs
+    steps = 7000                      # 64-pair batches drawn from 32k pairs
+    t0 = time.perf_counter()
     for st in range(steps):
         i = torch.randint(0, xtr.shape[0], (64,), device="cuda", generator=gen)
         xb, tb = xtr[i], ttr[i].clone()
@@ -112,15 +116,16 @@ def test_trained_proposal_warm_starts_the_aligner(mc3lib, torch_cuda):
             xb, tb[:, 1] = xb.flip(-2), -tb[:, 1]
         if k & 4:
             xb, tb = xb.transpose(-1, -2), tb[:, [1, 0]]
-        lr = 2e-3 if st < 4500 else 4e-4
+        lr = 2e-3 if st < 5000 else 4e-4
         losses.append(net.train_step(xb.contiguous(), tb.contiguous(), lr=lr))
+    train_s = time.perf_counter() - t0
     pred = net.predict(xte.contiguous()) * 4.0
     truth = tte.cpu().numpy() * 4.0
     err = float(np.sqrt(np.mean((pred - truth) ** 2)))
     base = float(np.sqrt(np.mean(truth ** 2)))
     print(f"proposal on held-out movies: {err:.3f} px RMS against the plain aligner's shifts "
           f"(no-motion guess {base:.3f} px); training loss {np.mean(losses[:24]):.3f} -> "
-          f"{np.mean(losses[-24:]):.3f} over {len(losses)} GPU steps")
+          f"{np.mean(losses[-24:]):.3f} over {len(losses)} GPU steps ({train_s:.0f} s)")
     assert np.mean(losses[-24:]) < 0.5 * np.mean(losses[:24])
     assert err < 0.5 * base
     warm_iters, cold_iters, kept, worst, offs = [], [], [], 0.0, []
@@ -133,13 +138,18 @@ def test_trained_proposal_warm_starts_the_aligner(mc3lib, torch_cuda):
             mc.set_first_iterate((d - d.mean(0)).astype(np.float32), max_iter=3)
             w = mc.process(fr)
             assert w.first_iterate in (1, 2)
+            # global-mode shifts are not made relative to a frame (neither
+            # here nor in the reference), so a warm start can end at the same
+            # alignment translated as a whole: compared up to that offset,
+            # which is reported
             dd = w.global_shifts.astype(np.float64) - c.global_shifts
             offs.append(np.round(dd.mean(0), 3).tolist())
-            worst = max(worst, float(np.abs(dd).max()))
+            worst = max(worst, float(np.abs(dd - dd.mean(0)).max()))
             warm_iters.append(int(w.iterations[0]))
             cold_iters.append(int(c.iterations[0]))
             kept.append(w.first_iterate == 1)
     print(f"iterations: cold {cold_iters}, warm {warm_iters} (warm start kept: {kept}); "
-          f"max |warm - cold| {worst:.4f} px; mean warm - cold per movie {offs}")
+          f"max |warm - cold| after each movie's mean offset {worst:.4f} px; "
+          f"mean warm - cold per movie {offs}")
     assert worst <= 0.05
     assert all(wi <= ci for wi, ci, k in zip(warm_iters, cold_iters, kept) if k)
