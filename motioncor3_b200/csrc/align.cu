@@ -86,18 +86,24 @@ int phase_apply(const float2* in, float2* out, int cmpX, int cmpY, const float2*
 // partial sums (even and odd frame index) that are added at the end.
 // ---------------------------------------------------------------------
 // Thread (kx, 4 consecutive rows): each frame's x phase factor is read once
-// for the 4 rows; the y factors are uniform over the warp (one row).
+// for the 4 rows.  Threads are numbered over (row group, kx) of each stack,
+// so no thread idles at the end of a row when cmpX is not a multiple of the
+// block size (1025 and 205 at the benchmark geometry); a warp that straddles
+// two row groups reads two y factors per frame.
 constexpr int kAsRows = 4;
-__global__ void __launch_bounds__(128) k_aligned_sum(const float2* __restrict__ spec,
-                                                     const int* act,
-                                                     const float2* __restrict__ ex,
-                                                     const float2* __restrict__ ey, float2* S,
-                                                     int cmpX, int cmpY, int N, long sstride) {
+constexpr int kAsThreads = 256;
+__global__ void __launch_bounds__(kAsThreads) k_aligned_sum(const float2* __restrict__ spec,
+                                                            const int* act,
+                                                            const float2* __restrict__ ex,
+                                                            const float2* __restrict__ ey, float2* S,
+                                                            int cmpX, int cmpY, int N, long sstride) {
   const long nel = (long)cmpX * cmpY;
-  const int kx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (kx >= cmpX) return;
-  const int ky0 = blockIdx.y * kAsRows;
-  const int a = blockIdx.z;
+  const int groups = (cmpY + kAsRows - 1) / kAsRows;
+  const long e = (long)blockIdx.x * kAsThreads + threadIdx.x;
+  if (e >= (long)groups * cmpX) return;
+  const int kx = (int)(e % cmpX);
+  const int ky0 = (int)(e / cmpX) * kAsRows;
+  const int a = blockIdx.y;
   const float2* X = spec + (long)act[a] * sstride;
   float2 e0[kAsRows], e1[kAsRows];
 #pragma unroll
@@ -110,8 +116,8 @@ __global__ void __launch_bounds__(128) k_aligned_sum(const float2* __restrict__ 
     for (int i = 0; i < kAsRows; ++i) {
       const int ky = ky0 + i;
       if (ky >= cmpY) break;
-      const float2 e = cmul(exf, ey[t * cmpY + ky]);
-      const float2 v = rot(X[(long)f * nel + (long)ky * cmpX + kx], e);
+      const float2 ef = cmul(exf, ey[t * cmpY + ky]);
+      const float2 v = rot(X[(long)f * nel + (long)ky * cmpX + kx], ef);
       if (f & 1) e1[i] = cadd(e1[i], v);
       else e0[i] = cadd(e0[i], v);
     }
@@ -126,9 +132,11 @@ __global__ void __launch_bounds__(128) k_aligned_sum(const float2* __restrict__ 
 int aligned_sum(const float2* spec, const int* act, const float2* ex, const float2* ey, float2* S,
                 const AlignDims& d, cudaStream_t st) {
   const long nel = (long)d.cmpX * d.cmpY;
-  dim3 grid(ceil_div(d.cmpX, 128), ceil_div(d.cmpY, kAsRows), d.A);
+  const long threads = (long)ceil_div(d.cmpY, kAsRows) * d.cmpX;
+  dim3 grid((unsigned)((threads + kAsThreads - 1) / kAsThreads), d.A);
   prof::Scope ps("k_aligned_sum", (double)d.A * nel * 8.0 * (d.N + 1), st);
-  k_aligned_sum<<<grid, 128, 0, st>>>(spec, act, ex, ey, S, d.cmpX, d.cmpY, d.N, d.stack_stride);
+  k_aligned_sum<<<grid, kAsThreads, 0, st>>>(spec, act, ex, ey, S, d.cmpX, d.cmpY, d.N,
+                                             d.stack_stride);
   MC3_CHECK_LAUNCH("k_aligned_sum");
   return kOk;
 }
