@@ -187,6 +187,26 @@ __device__ __forceinline__ bool patch_weight(int x, int y, int W, int H, float c
   return true;
 }
 
+// The same packed FMA on values kept in 64-bit registers (lane 0 in the low
+// half): no packing or unpacking around each instruction.
+__device__ __forceinline__ unsigned long long ffma2_b64(unsigned long long a,
+                                                        unsigned long long b,
+                                                        unsigned long long c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ unsigned long long pack2(float lo, float hi) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ float2 unpack2(unsigned long long v) {
+  float2 d;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(d.x), "=f"(d.y) : "l"(v));
+  return d;
+}
+
 // Per-pixel patch weights of mGCorrect3D: w = exp(-100 r) for patches with
 // r <= 0.6 (r = distance to the patch centre in units of the frame size),
 // bit p of the returned mask set for those patches; the others weigh 0.
@@ -240,9 +260,13 @@ __global__ void __launch_bounds__(128) k_local_gather(
       if ((inc[q] >> p) & 1ull) wsum[q] += w[q][p];
   }
   float2 wp[PMAX];  // (w of pixel 0, w of pixel 1) for the packed FMAs
+  unsigned long long wpb[PMAX];  // the same pairs in 64-bit registers
   if constexpr (PX == 2) {
 #pragma unroll
-    for (int p = 0; p < PMAX; ++p) wp[p] = make_float2(w[0][p], w[1][p]);
+    for (int p = 0; p < PMAX; ++p) {
+      wp[p] = make_float2(w[0][p], w[1][p]);
+      wpb[p] = pack2(w[0][p], w[1][p]);
+    }
   }
   const bool act0 = xb < W;
   const int padX = (W / 2 + 1) * 2;
@@ -270,14 +294,18 @@ __global__ void __launch_bounds__(128) k_local_gather(
         float fSx[PX], fSy[PX], fW[PX];
         if (s_clean[fl]) {
           if constexpr (PX == 2) {
-            float2 Sx = make_float2(0.0f, 0.0f), Sy = Sx;
+            // (sx, sx) and (sy, sy) of each patch come as two 64-bit values
+            unsigned long long Sx = 0ull, Sy = 0ull;  // (+0, +0)
+            const uint32_t sa = (uint32_t)__cvta_generic_to_shared(s);
 #pragma unroll
             for (int p = 0; p < PMAX; ++p) {
-              const float4 sp = s[p];
-              Sx = ffma2(make_float2(sp.x, sp.y), wp[p], Sx);
-              Sy = ffma2(make_float2(sp.z, sp.w), wp[p], Sy);
+              unsigned long long sxx, syy;
+              asm volatile("ld.shared.v2.u64 {%0, %1}, [%2];" : "=l"(sxx), "=l"(syy) : "r"(sa + 16 * p));
+              Sx = ffma2_b64(sxx, wpb[p], Sx);
+              Sy = ffma2_b64(syy, wpb[p], Sy);
             }
-            fSx[0] = Sx.x, fSx[1] = Sx.y, fSy[0] = Sy.x, fSy[1] = Sy.y;
+            const float2 ux = unpack2(Sx), uy = unpack2(Sy);
+            fSx[0] = ux.x, fSx[1] = ux.y, fSy[0] = uy.x, fSy[1] = uy.y;
           } else {
             fSx[0] = fSy[0] = 0.0f;
 #pragma unroll
