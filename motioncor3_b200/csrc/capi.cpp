@@ -439,8 +439,8 @@ int mc3_set_patch_centers(mc3_ctx* ctx, const float* centers_xy, int n_patches) 
     return MC3_OK;
   }
   if (n_patches < 1) return MC3_EINVAL;
-  for (int i = 0; i < 2 * n_patches; ++i)
-    if (!std::isfinite(centers_xy[i])) return MC3_EINVAL;
+  for (int i = 0; i < 2 * n_patches; ++i)  // finite pixel coordinates
+    if (!std::isfinite(centers_xy[i]) || std::fabs(centers_xy[i]) > 1.0e6f) return MC3_EINVAL;
   ctx->eng->patch_centers_given.assign(centers_xy, centers_xy + 2 * (size_t)n_patches);
   return MC3_OK;
 }

@@ -32,7 +32,10 @@ int shim_tuning_roundtrip(char* json_out, int cap) {
     bad += std::abs(a.best_ms - b.best_ms) > 1e-3;
     bad += a.cand.size() != b.cand.size();
     for (size_t k = 0; k < a.cand.size() && k < b.cand.size(); ++k)
-      bad += a.cand[k].col_wide != b.cand[k].col_wide || std::abs(a.cand_ms[k] - b.cand_ms[k]) > 1e-3;
+      bad += a.cand[k].col_wide != b.cand[k].col_wide || a.cand[k].row_pipe != b.cand[k].row_pipe ||
+             std::abs(a.cand_ms[k] - b.cand_ms[k]) > 1e-3;
+    // the persistent row passes go with the persistent column pass
+    bad += b.best.row_pipe != (b.best.col_wide == 2);
   }
   return bad;
 }
@@ -43,4 +46,18 @@ int shim_tuning_parse(const char* text) {
 }
 
 int shim_tuning_candidates() { return (int)mc3::tuning_candidates().size(); }
+
+// Candidates whose persistent row and column passes are not paired, and
+// candidates that differ in nothing: both must be 0.
+int shim_tuning_candidate_faults() {
+  const std::vector<mc3::Tuning> c = mc3::tuning_candidates();
+  int bad = 0;
+  for (size_t i = 0; i < c.size(); ++i) {
+    bad += c[i].row_pipe != (c[i].col_wide == 2);
+    for (size_t k = 0; k < i; ++k)
+      bad += c[i].fft_r16 == c[k].fft_r16 && c[i].col_wide == c[k].col_wide &&
+             c[i].gather_px == c[k].gather_px && c[i].row_pipe == c[k].row_pipe;
+  }
+  return bad;
+}
 }

@@ -45,3 +45,4 @@ def test_tuning_file_rejects_other_text(tshim):
 
 def test_every_variant_is_a_candidate(tshim):
     assert tshim.shim_tuning_candidates() == 8
+    assert tshim.shim_tuning_candidate_faults() == 0
