@@ -502,6 +502,14 @@ void mc3_patch_make_relative(float* shifts, int nz, int n_patches);
 /* Align::CPatchShifts::DetectBads (Align/CPatchShifts.cpp:288-355). */
 void mc3_patch_detect_bads(const float* shifts, const float* centers, int nz, int n_patches,
                            int nx, int ny, unsigned char* bad);
+/* Patch starts [P][2] (alignment-image pixels) that mc3_set_patch_centers
+ * derives from full-frame centres [P][2]: each centre divided by the xcf bin
+ * (bin_x, bin_y) and rounded, minus half the patch (pat_x, pat_y), kept
+ * inside the xcf_x x xcf_y image.  The inverse of the centres the engine
+ * reports ((start + pat/2) * bin, as CPatchCenters::GetCenter scaled by
+ * CFullAlign).  No counterpart in the reference (it has no given centres). */
+int mc3_patch_starts_from_centers(const float* centers, int n_patches, float bin_x, float bin_y,
+                                  int xcf_x, int xcf_y, int pat_x, int pat_y, int* starts);
 
 #ifdef __cplusplus
 }

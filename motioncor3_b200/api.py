@@ -201,6 +201,8 @@ _SIGS = {
     "mc3_smooth_shifts": ([_VP, _VP, _I, _F], None),
     "mc3_patch_make_relative": ([_VP, _I, _I], None),
     "mc3_patch_detect_bads": ([_VP, _VP, _I, _I, _I, _I, _VP], None),
+    "mc3_patch_starts_from_centers": ([_VP, _I, ctypes.c_float, ctypes.c_float, _I, _I, _I, _I,
+                                       _VP], _I),
 }
 
 
@@ -977,3 +979,16 @@ def patch_detect_bads(shifts: np.ndarray, centers: np.ndarray, nx: int, ny: int)
     bad = np.zeros(s.shape[:2], np.uint8)
     _lib().mc3_patch_detect_bads(_hp(s), _hp(c), s.shape[0], s.shape[1], nx, ny, _hp(bad))
     return bad
+
+
+def patch_starts_from_centers(centers, bin_xy, xcf_size, patch_size) -> np.ndarray:
+    """Patch starts [P][2] in the alignment image for full-frame centres
+    [P][2] (mc3_patch_starts_from_centers): what mc3_set_patch_centers uses."""
+    c = np.ascontiguousarray(centers, np.float32).reshape(-1, 2)
+    out = np.zeros((c.shape[0], 2), np.int32)
+    _check(_lib().mc3_patch_starts_from_centers(_hp(c), c.shape[0], float(bin_xy[0]),
+                                                float(bin_xy[1]), int(xcf_size[0]),
+                                                int(xcf_size[1]), int(patch_size[0]),
+                                                int(patch_size[1]), _hp(out)),
+           "mc3_patch_starts_from_centers")
+    return out

@@ -838,4 +838,17 @@ void mc3_patch_detect_bads(const float* shifts, const float* centers, int nz, in
   host::patch_detect_bads(shifts, centers, nz, n_patches, nx, ny, bad);
 }
 
+int mc3_patch_starts_from_centers(const float* centers, int n_patches, float bin_x, float bin_y,
+                                  int xcf_x, int xcf_y, int pat_x, int pat_y, int* starts) {
+  if (!centers || !starts || n_patches < 1 || !(bin_x > 0.0f) || !(bin_y > 0.0f) ||
+      pat_x < 1 || pat_y < 1 || pat_x > xcf_x || pat_y > xcf_y)
+    return MC3_EINVAL;
+  for (int i = 0; i < 2 * n_patches; ++i)
+    if (!std::isfinite(centers[i]) || std::fabs(centers[i]) > 1.0e6f) return MC3_EINVAL;
+  std::vector<int> s;
+  host::patch_starts_from_centers(centers, n_patches, bin_x, bin_y, xcf_x, xcf_y, pat_x, pat_y, s);
+  std::memcpy(starts, s.data(), sizeof(int) * s.size());
+  return MC3_OK;
+}
+
 }  // extern "C"

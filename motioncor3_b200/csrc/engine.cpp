@@ -815,16 +815,9 @@ int Engine::process_with(const mc3_movie& mv, mc3_result* out, const Tuning& tun
       std::vector<int> starts;
       host::patch_starts(map.data(), bx, by, scal[1], scal[2], g.Px, g.Py, xcfX, xcfY,
                          g.patSizeX, g.patSizeY, starts);
-      if (patch_centers_given.size() == 2 * (size_t)g.P) {
-        // caller's centres (full-frame pixels) -> patch starts in the
-        // alignment image, kept inside it
-        for (int p = 0; p < g.P; ++p) {
-          const int cx = (int)lrintf(patch_centers_given[2 * p] / g.xcfBin[0]);
-          const int cy = (int)lrintf(patch_centers_given[2 * p + 1] / g.xcfBin[1]);
-          starts[2 * p] = std::min(std::max(cx - g.patSizeX / 2, 0), xcfX - g.patSizeX);
-          starts[2 * p + 1] = std::min(std::max(cy - g.patSizeY / 2, 0), xcfY - g.patSizeY);
-        }
-      }
+      if (patch_centers_given.size() == 2 * (size_t)g.P)  // the caller's centres
+        host::patch_starts_from_centers(patch_centers_given.data(), g.P, g.xcfBin[0],
+                                        g.xcfBin[1], xcfX, xcfY, g.patSizeX, g.patSizeY, starts);
       // ---- 6b. xcf frames to real space (Correct/CGenRealStack.cpp) ----
       MC3_TRY(phase_tables(d_sh.as<float2>(), N, g.xcfCmpX, g.xcfCmpY, d_ex.as<float2>(), d_ey.as<float2>(), true, st));
       Batch bn{N, N, (long)nxcf, nullptr, (long)nxcf};

@@ -1,6 +1,7 @@
 // Host-side FP32 shift bookkeeping (see host_align.h).
 #include "host_align.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -756,6 +757,18 @@ float kv_factor(int kv) {
   else if (kv < 200 && kv >= 120) f = 0.004375f * (kv - 120) + 0.45f;
   else f = 0.45f;
   return f;
+}
+
+void patch_starts_from_centers(const float* centers, int n_patches, float bin_x, float bin_y,
+                               int xcf_x, int xcf_y, int pat_x, int pat_y,
+                               std::vector<int>& starts) {
+  starts.assign(2 * (size_t)n_patches, 0);
+  for (int p = 0; p < n_patches; ++p) {
+    const int cx = (int)lrintf(centers[2 * p] / bin_x);
+    const int cy = (int)lrintf(centers[2 * p + 1] / bin_y);
+    starts[2 * p] = std::min(std::max(cx - pat_x / 2, 0), xcf_x - pat_x);
+    starts[2 * p + 1] = std::min(std::max(cy - pat_y / 2, 0), xcf_y - pat_y);
+  }
 }
 
 }  // namespace host

@@ -107,6 +107,14 @@ void patch_detect_bads(const float* shifts, const float* centers, int n_frames, 
 void patch_starts(const float* map, int bx, int by, float mean, float m2, int px, int py,
                   int xcf_x, int xcf_y, int pat_x, int pat_y, std::vector<int>& starts);
 
+// Patch starts in the alignment image for given full-frame patch centres
+// (mc3_set_patch_centers): each centre divided by the bin and rounded to the
+// nearest pixel, minus half the patch (the inverse of the centre the engine
+// reports, start + size/2 times the bin), kept inside the image.
+void patch_starts_from_centers(const float* centers, int n_patches, float bin_x, float bin_y,
+                               int xcf_x, int xcf_y, int pat_x, int pat_y,
+                               std::vector<int>& starts);
+
 // GStretch::Setup (Correct/GStretch.cu:53-72) with the stretch and axis of
 // CAlignParam::GetMagStretch (Align/CAlignParam.cpp:55-72): the inverse of
 // the stretch matrix along -angle, as three floats.  Returns false when the
