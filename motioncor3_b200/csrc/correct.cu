@@ -294,7 +294,10 @@ __global__ void __launch_bounds__(128) k_local_gather(
         float fSx[PX], fSy[PX], fW[PX];
         if (s_clean[fl]) {
           if constexpr (PX == 2) {
-            // (sx, sx) and (sy, sy) of each patch come as two 64-bit values
+            // (sx, sx) and (sy, sy) of each patch come as two 64-bit values.
+            // The shared reads need no memory clobber: the chunk's writes
+            // are ordered before them by the __syncthreads() above, and the
+            // next chunk's writes after them by the one at the loop's top.
             unsigned long long Sx = 0ull, Sy = 0ull;  // (+0, +0)
             const uint32_t sa = (uint32_t)__cvta_generic_to_shared(s);
 #pragma unroll
