@@ -390,7 +390,7 @@ int mc3_dose_weighted_sums(mc3_ctx* ctx, const float* spectra, int nx, int ny, i
  * first iterate of that frame's shift, trained on the GPU by the library's
  * own forward and backward kernels (FP32, Adam) on shifts that the plain
  * aligner measured, and used through mc3_set_first_iterate, where the plain
- * aligner remains the fallback and the judge. */
+ * aligner decides whether the warm result is kept and remains the fallback. */
 typedef struct mc3_proposal mc3_proposal;
 /* spec: n_layers groups of (cin, cout, k, stride, pad), the first cin = 2;
  * nout outputs; weights He-initialised from seed, on device `gpu`. */
